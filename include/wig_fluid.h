@@ -1,0 +1,302 @@
+/*
+ * wig_fluid.h — C ABI of the B200 liquid step (worldinagrain_b200).
+ *
+ * This library is a drop-in for the liquid passes that the reference's
+ * `Simulation.encodeFluid(pass, offset)` (js/sim.js:2466-2612) records into a
+ * WebGPU compute pass.  The reference binds one group of 17 bindings
+ * (js/sim.js:407-410, js/sim.js:1155-1159, shaders/fluid.wgsl:116-181,
+ * :2543, :2547); this header takes the same buffers as plain device pointers
+ * in the same layouts, so a host that owns the reference's buffers can hand
+ * them over unchanged:
+ *
+ *   binding 0  Params        -> wig_params (host struct, copied per step)
+ *   binding 1  elems         -> wig_elem table (the liquid's fields only)
+ *   binding 2  cells         -> cells      (vec4<u32> per cell, then gas plane)
+ *   binding 3  air           -> (not bound: the configs carry no air motion)
+ *   binding 4  sorted        -> sorted     (Particles: 16 B header + 3 planes)
+ *   binding 5  parts         -> parts      (Particles)
+ *   binding 6  counters      -> counters   (u32: 11 per cell, 2 per face)
+ *   binding 7  field         -> field      (vec4<f32>: 2 per cell, faces, levels)
+ *   binding 8  blocks        -> blocks     (u32: 5 per 8x8 block + 9 stats)
+ *   binding 9  Level         -> (level, cycle) arguments of wig_fluid_dispatch
+ *   binding 10 gravity       -> (not bound: Earth's pull P.earthG straight down)
+ *   binding 11 airSource     -> (not bound)
+ *   binding 12 bodyMotion    -> (not bound: no free bodies)
+ *   binding 13 occupants     -> (not bound: no people)
+ *   binding 14 bodies        -> (not bound)
+ *   binding 15 fluidCg       -> cg         (vec4<f32>: per cell, per block, sums)
+ *   binding 16 bodyPushes    -> (not bound)
+ *
+ * All entry points return 0 on success and a negative WIG_E* code on error;
+ * wig_fluid_last_error() gives a one-line description of the last error on
+ * the calling thread.  No C++ exception crosses this boundary.  A handle is
+ * not thread-safe and works on the one CUDA stream passed to it.
+ */
+#ifndef WIG_FLUID_H
+#define WIG_FLUID_H
+
+#include <stdint.h>
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define WIG_ABI_VERSION 1u
+
+/* Error codes. */
+#define WIG_OK 0
+#define WIG_E_ARG (-1)        /* bad argument or descriptor */
+#define WIG_E_OOM (-2)        /* device allocation failed */
+#define WIG_E_CUDA (-3)       /* a CUDA call failed (message names it) */
+#define WIG_E_CAPACITY (-4)   /* more particles than the buffers hold */
+#define WIG_E_NOT_CONVERGED (-5) /* solve left more than the tolerance after max_cycles */
+#define WIG_E_STATE (-6)      /* call out of order (e.g. step before bind) */
+#define WIG_E_NO_DEVICE (-7)  /* no CUDA device usable */
+
+/* Layout constants shared with the reference (js/shared.js:263-282). */
+#define WIG_FLUID_BLOCK 8u
+#define WIG_LIQUID_CELL_WORDS 11u
+#define WIG_MG_COARSEST 512u
+#define WIG_MG_LEVELS 8u
+#define WIG_FLUID_STATS 9u
+#define WIG_FLUID_CYCLES 16u
+#define WIG_PARTICLES_HEADER 16u
+#define WIG_PARTICLE_BYTES 48u
+
+/* FLUID_COUNT word offsets (js/shared.js:271). */
+#define WIG_COUNT_ACTIVE 0u
+#define WIG_COUNT_RETIRED 1u
+#define WIG_COUNT_VISCOUS 2u
+#define WIG_COUNT_PARTICLES 3u
+#define WIG_COUNT_RESIDUAL 4u
+#define WIG_COUNT_CYCLES 7u
+#define WIG_COUNT_MOST_CYCLES 8u
+
+/* Element kinds (js/elements.js:8). */
+#define WIG_KIND_SOLID 1u
+#define WIG_KIND_POWDER 2u
+#define WIG_KIND_LIQUID 3u
+#define WIG_KIND_GAS 4u
+
+/* Element ids the liquid step names itself (js/elements.js DEFS order). */
+#define WIG_ELEM_AIR 0u
+#define WIG_ELEM_WALL 1u
+#define WIG_ELEM_SAND 2u
+#define WIG_ELEM_WATER 3u
+#define WIG_MAX_ELEMS 256u
+
+/* Params (shaders/common.wgsl:5-40), 80 bytes, written per step by the host
+ * (js/sim.js:1975-1995).  Field for field the reference's uniform. */
+typedef struct wig_params {
+    uint32_t size[2];
+    uint32_t frame;
+    uint32_t seed;
+    uint32_t offset[2];
+    float support_max;
+    float dx;
+    float day;
+    float day_rate;
+    float hole_pull;
+    float mass_pull;
+    float earth_g;   /* cells/step^2, straight down the screen (+y) */
+    float dt;
+    float day_dt;
+    float clock_span;
+    uint32_t heat_stages;
+    float heat_limit;
+    uint32_t holding;
+    float pad;
+} wig_params;
+
+/* The fields of the reference's Elem (js/elements.js:44-300) that the liquid
+ * step reads, one 80-byte record per element id. */
+typedef struct wig_elem {
+    uint32_t kind;
+    float density;      /* g/cm^3 x 100, water 100 */
+    float weight;       /* cells/step^2 */
+    float heat_cap;
+    float viscosity;
+    float viscosity_t;
+    float viscosity_e;
+    float tension;
+    float expansion;
+    float expansion2;
+    float hi_t;
+    float lo_t;
+    float up_span;
+    float down_span;
+    float down_scale;
+    float sol_density;
+    uint32_t flags;     /* F_* (js/elements.js:10-21); F_IMPACT = 32 */
+    float wetting;
+    float pad[2];
+} wig_elem;
+
+/* A world: its size and the liquid's particles per cell (LIQUID_PER_CELL,
+ * js/shared.js:276; 4 in the reference, a parameter here). */
+typedef struct wig_world_desc {
+    uint32_t width;
+    uint32_t height;
+    uint32_t liquid_per_cell;   /* 0 means the reference's 4 */
+    uint32_t capacity;          /* particle slots; 0 means ceil(W*H*ppc*1.25) */
+} wig_world_desc;
+
+/* Sizes (bytes) and shape the reference derives for a world
+ * (js/sim.js:741-843). */
+typedef struct wig_world_layout {
+    uint32_t width, height, liquid_per_cell, capacity;
+    uint32_t cell_count, face_count, block_count, blocks_wide, edge_tiles;
+    uint32_t levels;                 /* coarse levels (js/sim.js:763-771) */
+    uint32_t level_w[WIG_MG_LEVELS];
+    uint32_t level_h[WIG_MG_LEVELS];
+    uint64_t cells_bytes;            /* C vec4 + ceil(C/2) vec4 gas plane */
+    uint64_t particles_bytes;        /* 16 + 48 * capacity */
+    uint64_t counters_bytes;         /* (11 C + 2 F) * 4 */
+    uint64_t field_bytes;            /* ((C + level cells) * 2 + F + 2 ceil(F/4)) * 16 */
+    uint64_t blocks_bytes;           /* (5 B + 9) * 4 */
+    uint64_t cg_bytes;               /* (C + B + 1) * 16 */
+} wig_world_layout;
+
+/* Device pointers for the bound buffers (layouts as in the comment above).
+ * A null pointer asks the handle to allocate that buffer itself. */
+typedef struct wig_fluid_buffers {
+    void* cells;
+    void* sorted;
+    void* parts;
+    void* counters;
+    void* field;
+    void* blocks;
+    void* cg;
+} wig_fluid_buffers;
+
+/* Step flags. */
+#define WIG_STEP_BOOKKEEPING_ONLY 1u  /* fluidStats.active == 0: syncMarks, compact, retire */
+#define WIG_STEP_SHIFTED_SET 2u       /* take the tiling parity from the next bit */
+#define WIG_STEP_SHIFTED_FIRST 4u     /* (with SHIFTED_SET) the step's first relaxation is shifted */
+#define WIG_STEP_VISCOUS 8u           /* encode viscosity sweeps (fluidStats.viscous) */
+#define WIG_STEP_TOLERANCE 16u        /* stop on ||r||2/||b||2 <= tol (FP64) instead of max|r| < 1e-2 */
+#define WIG_STEP_F64_DOTS 32u         /* CG dot products in FP64 */
+#define WIG_STEP_SYNC_STATS 64u       /* copy the stats to the host at the end of the step */
+
+/* Per-step statistics (the report words, js/sim.js:1882-1900, plus the
+ * solve's residuals). */
+typedef struct wig_fluid_stats {
+    uint32_t count[WIG_FLUID_STATS];  /* FLUID_COUNT words */
+    uint32_t particles;               /* sorted.count after the step */
+    uint32_t cycles;                  /* CG iterations run this step */
+    uint32_t pad;
+    double rel_residual;              /* ||r||2/||b||2 of the CG residual, FP64 (tolerance mode) */
+    double b_norm;                    /* ||b||2 at the solve's start */
+} wig_fluid_stats;
+
+typedef struct wig_fluid wig_fluid;
+
+/* Pass ids, one per reference pipeline dispatched by encodeFluid. */
+enum wig_pass {
+    WIG_PASS_SYNC = 0,            /* fluid.wgsl:637 */
+    WIG_PASS_SYNC_MARKS,          /* fluid.wgsl:652 */
+    WIG_PASS_SYNC_PARTICLES,      /* fluid.wgsl:767 */
+    WIG_PASS_SYNC_SEED,           /* fluid.wgsl:863 */
+    WIG_PASS_COMPACT,             /* fluid.wgsl:896 */
+    WIG_PASS_RETIRE,              /* fluid.wgsl:924 */
+    WIG_PASS_CLEAR,               /* fluid.wgsl:962 */
+    WIG_PASS_GATHER,              /* fluid.wgsl:1017 */
+    WIG_PASS_SEAL_JOIN,           /* fluid.wgsl:1531 */
+    WIG_PASS_SEAL_ANCHOR,         /* fluid.wgsl:1545 */
+    WIG_PASS_CLASSIFY,            /* fluid.wgsl:1578 */
+    WIG_PASS_SET_FACES,           /* fluid.wgsl:1982 */
+    WIG_PASS_VISCOSITY_RED,       /* fluid.wgsl:3458 */
+    WIG_PASS_VISCOSITY_BLACK,     /* fluid.wgsl:3463 */
+    WIG_PASS_UNPRESS,             /* fluid.wgsl:3453 */
+    WIG_PASS_DIVERGENCE,          /* fluid.wgsl:1996 */
+    WIG_PASS_CG_START,            /* fluid.wgsl:2665 */
+    WIG_PASS_CG_JOIN,             /* fluid.wgsl:2677 */
+    WIG_PASS_CG_ANCHOR,           /* fluid.wgsl:2692 */
+    WIG_PASS_CG_RESIDUAL,         /* fluid.wgsl:2708 */
+    WIG_PASS_CG_PREPARE,          /* fluid.wgsl:2721 */
+    WIG_PASS_RELAX_RIMS,          /* fluid.wgsl:2096 */
+    WIG_PASS_RELAX,               /* fluid.wgsl:2184 */
+    WIG_PASS_RELAX_SHIFTED,       /* fluid.wgsl:2189 */
+    WIG_PASS_RESTRICT,            /* fluid.wgsl:2342 */
+    WIG_PASS_SMOOTH_RED,          /* fluid.wgsl:2379 */
+    WIG_PASS_SMOOTH_BLACK,        /* fluid.wgsl:2384 */
+    WIG_PASS_SOLVE,               /* fluid.wgsl:2407 */
+    WIG_PASS_PROLONG,             /* fluid.wgsl:2459 */
+    WIG_PASS_PROLONG_FINE,        /* fluid.wgsl:2500 */
+    WIG_PASS_CG_RHO,              /* fluid.wgsl:2736 */
+    WIG_PASS_CG_BETA,             /* fluid.wgsl:2752 */
+    WIG_PASS_CG_DIRECTION,        /* fluid.wgsl:2767 */
+    WIG_PASS_CG_APPLY,            /* fluid.wgsl:2779 */
+    WIG_PASS_CG_ALPHA,            /* fluid.wgsl:2797 */
+    WIG_PASS_CG_UPDATE,           /* fluid.wgsl:2852 */
+    WIG_PASS_CG_FINISH,           /* fluid.wgsl:2884 */
+    WIG_PASS_PROJECT,             /* fluid.wgsl:2925 */
+    WIG_PASS_EXTRAPOLATE,         /* fluid.wgsl:3267 */
+    WIG_PASS_EXTRAPOLATE_FURTHER, /* fluid.wgsl:3272 */
+    WIG_PASS_ADVECT,              /* fluid.wgsl:3616 */
+    WIG_PASS_SORT_COUNT,          /* fluid.wgsl:3700 */
+    WIG_PASS_SCAN_BLOCKS,         /* fluid.wgsl:3730 */
+    WIG_PASS_SCAN_TOTALS,         /* fluid.wgsl:3757 */
+    WIG_PASS_SCAN_FINISH,         /* fluid.wgsl:3783 */
+    WIG_PASS_SCATTER,             /* fluid.wgsl:3793 */
+    WIG_PASS_RASTER_CLAIMS,       /* fluid.wgsl:3928 */
+    WIG_PASS_RASTER,              /* fluid.wgsl:3983 */
+    WIG_PASS_UNPAINT,             /* fluid.wgsl:4163 */
+    WIG_PASS_COUNT
+};
+
+/* The layout the reference derives for a world (js/sim.js:741-843). */
+int wig_fluid_layout(const wig_world_desc* d, wig_world_layout* out);
+
+/* Replaces `new Simulation(...)`'s liquid allocations (js/sim.js:741-843):
+ * creates a handle on the current CUDA device for world d with element table
+ * elems[n_elems]. */
+int wig_fluid_create(const wig_world_desc* d, const wig_elem* elems, uint32_t n_elems,
+                     wig_fluid** out);
+
+/* Replaces the bind group (js/sim.js:1155-1159): adopts caller-owned device
+ * buffers (null fields are allocated by the handle and zeroed, as
+ * js/sim.js:1259 `clear` leaves them). */
+int wig_fluid_bind(wig_fluid* h, const wig_fluid_buffers* b);
+
+/* The bound (or allocated) device buffers. */
+int wig_fluid_buffers_of(wig_fluid* h, wig_fluid_buffers* out);
+
+/* Replaces encodeFluid (js/sim.js:2466-2612): one liquid step, stream
+ * ordered and asynchronous on `stream` (a cudaStream_t, 0 for the legacy
+ * stream).  max_cycles is fluidCycles (<= 64); flags WIG_STEP_*.
+ * tolerance is used with WIG_STEP_TOLERANCE. */
+int wig_fluid_step(wig_fluid* h, const wig_params* P, uint32_t max_cycles, uint32_t flags,
+                   double tolerance, void* stream);
+
+/* One reference pipeline dispatch (encodeFluid's `run`/`blocks`/`particles`
+ * with its Level slot): pass id, level index and cycle. */
+int wig_fluid_dispatch(wig_fluid* h, const wig_params* P, int pass, uint32_t level,
+                       uint32_t cycle, void* stream);
+
+/* Host <-> device copies of one bound buffer (which: 0 cells, 1 sorted,
+ * 2 parts, 3 counters, 4 field, 5 blocks, 6 cg), stream ordered on the
+ * handle's stream and complete on return: the reference's
+ * device.queue.writeBuffer and mapped readbacks (js/sim.js:1259,
+ * js/snapshot.js:97-164) for worlds loaded or saved by the host. */
+int wig_fluid_upload(wig_fluid* h, int which, const void* host, uint64_t offset, uint64_t bytes, void* stream);
+int wig_fluid_download(wig_fluid* h, int which, void* host, uint64_t offset, uint64_t bytes, void* stream);
+
+/* Replaces readReport (js/sim.js:1882-1900): waits for the stream and reads
+ * the FLUID_COUNT words and the solve's statistics of the last step. */
+int wig_fluid_read_stats(wig_fluid* h, wig_fluid_stats* out);
+
+void wig_fluid_destroy(wig_fluid* h);
+
+/* One-line description of the last error on this thread ("" if none). */
+const char* wig_fluid_last_error(void);
+
+/* Library ABI version (WIG_ABI_VERSION). */
+uint32_t wig_fluid_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* WIG_FLUID_H */

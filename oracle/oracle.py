@@ -1,0 +1,99 @@
+"""TEST INFRASTRUCTURE: ctypes front of the CPU oracle (oracle/wig_oracle.cpp).
+
+The oracle restates the reference's liquid passes on the CPU; it is the
+checker the CUDA path is compared with.  Only tests/, the smoke check and
+bench.py's CPU-baseline leg load it.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+from worldinagrain_b200 import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libwig_oracle.so")
+_lib = None
+
+
+def build():
+    """Compile the oracle (make -C oracle)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        L.wo_layout.argtypes = [C.POINTER(abi.WorldDesc), C.POINTER(abi.WorldLayout)]
+        L.wo_pass.argtypes = [C.POINTER(abi.WorldDesc), C.POINTER(abi.Params), C.POINTER(abi.Elem), C.c_uint32,
+                              C.POINTER(abi.Buffers), C.c_int, C.c_uint32, C.c_uint32]
+        L.wo_step.argtypes = [C.POINTER(abi.WorldDesc), C.POINTER(abi.Params), C.POINTER(abi.Elem), C.c_uint32,
+                              C.POINTER(abi.Buffers), C.c_uint32, C.c_uint32, C.c_double,
+                              C.POINTER(C.c_uint32), C.POINTER(abi.Stats)]
+        L.wo_solve_f64.argtypes = [C.POINTER(abi.WorldDesc), C.POINTER(abi.Params), C.POINTER(abi.Elem), C.c_uint32,
+                                   C.POINTER(abi.Buffers), C.c_double, C.c_uint32, C.c_void_p,
+                                   C.POINTER(C.c_double)]
+        L.wo_true_residual.argtypes = [C.POINTER(abi.WorldDesc), C.POINTER(abi.Params), C.POINTER(abi.Elem),
+                                       C.c_uint32, C.POINTER(abi.Buffers), C.c_void_p]
+        L.wo_true_residual.restype = C.c_double
+        L.wo_sincos.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        _lib = L
+    return _lib
+
+
+def _buffers(world):
+    b = abi.Buffers()
+    for k in abi.BUFFER_NAMES:
+        arr = getattr(world, k)
+        assert arr.flags["C_CONTIGUOUS"]
+        setattr(b, k, arr.ctypes.data)
+    return b
+
+
+class Oracle:
+    """Runs the oracle's passes and steps over a World's host buffers in place."""
+
+    def __init__(self, world, elems):
+        self.world = world
+        self.elems = elems
+        self.shifted = C.c_uint32(0)
+
+    def pass_(self, P, name, level=0, cycle=0):
+        d = self.world.desc()
+        b = _buffers(self.world)
+        rc = lib().wo_pass(C.byref(d), C.byref(P), self.elems, len(self.elems), C.byref(b), abi.PASS[name], level, cycle)
+        assert rc == 0, rc
+
+    def step(self, P, max_cycles=abi.FLUID_CYCLES, flags=0, tolerance=1e-6):
+        d = self.world.desc()
+        b = _buffers(self.world)
+        st = abi.Stats()
+        rc = lib().wo_step(C.byref(d), C.byref(P), self.elems, len(self.elems), C.byref(b), max_cycles, flags,
+                           tolerance, C.byref(self.shifted), C.byref(st))
+        assert rc == 0, rc
+        return st
+
+    def solve_f64(self, P, rel_tol=1e-12, max_iter=100000):
+        d = self.world.desc()
+        b = _buffers(self.world)
+        x = np.zeros(self.world.C, dtype=np.float64)
+        rel = C.c_double(0.0)
+        it = lib().wo_solve_f64(C.byref(d), C.byref(P), self.elems, len(self.elems), C.byref(b), rel_tol, max_iter,
+                                x.ctypes.data, C.byref(rel))
+        return x, it, rel.value
+
+    def true_residual(self, P, x):
+        d = self.world.desc()
+        b = _buffers(self.world)
+        x = np.ascontiguousarray(x, dtype=np.float32)
+        return lib().wo_true_residual(C.byref(d), C.byref(P), self.elems, len(self.elems), C.byref(b), x.ctypes.data)
+
+
+def sincos(a):
+    s, c = C.c_float(), C.c_float()
+    lib().wo_sincos(C.c_float(a), C.byref(s), C.byref(c))
+    return s.value, c.value

@@ -1,0 +1,120 @@
+"""Host side of the liquid step: the reference's Simulation liquid interface
+(js/sim.js:741-843 allocation, :2466-2612 encodeFluid, :1882-1900
+readReport) over the C ABI of libwig_fluid.so.
+
+There is no CPU path here: a missing library or device raises.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import abi
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libwig_fluid.so")
+
+_lib = None
+
+FUNCS = {
+    "wig_fluid_abi_version": ([], C.c_uint32),
+    "wig_fluid_last_error": ([], C.c_char_p),
+    "wig_fluid_layout": ([C.POINTER(abi.WorldDesc), C.POINTER(abi.WorldLayout)], C.c_int),
+    "wig_fluid_create": ([C.POINTER(abi.WorldDesc), C.POINTER(abi.Elem), C.c_uint32, C.POINTER(C.c_void_p)], C.c_int),
+    "wig_fluid_bind": ([C.c_void_p, C.POINTER(abi.Buffers)], C.c_int),
+    "wig_fluid_buffers_of": ([C.c_void_p, C.POINTER(abi.Buffers)], C.c_int),
+    "wig_fluid_step": ([C.c_void_p, C.POINTER(abi.Params), C.c_uint32, C.c_uint32, C.c_double, C.c_void_p], C.c_int),
+    "wig_fluid_dispatch": ([C.c_void_p, C.POINTER(abi.Params), C.c_int, C.c_uint32, C.c_uint32, C.c_void_p], C.c_int),
+    "wig_fluid_upload": ([C.c_void_p, C.c_int, C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p], C.c_int),
+    "wig_fluid_download": ([C.c_void_p, C.c_int, C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p], C.c_int),
+    "wig_fluid_read_stats": ([C.c_void_p, C.POINTER(abi.Stats)], C.c_int),
+    "wig_fluid_destroy": ([C.c_void_p], None),
+}
+
+
+class WigError(RuntimeError):
+    pass
+
+
+def lib(path=None):
+    """Loads libwig_fluid.so (raises if it is missing)."""
+    global _lib
+    if _lib is None:
+        p = path or LIB_PATH
+        if not os.path.exists(p):
+            raise WigError(f"libwig_fluid.so not built ({p}); run worldinagrain_b200/build.py")
+        L = C.CDLL(p)
+        for name, (args, res) in FUNCS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        if L.wig_fluid_abi_version() != abi.ABI_VERSION:
+            raise WigError("libwig_fluid.so ABI version mismatch")
+        _lib = L
+    return _lib
+
+
+def check(rc, what):
+    if rc != 0:
+        msg = lib().wig_fluid_last_error().decode(errors="replace")
+        raise WigError(f"{what}: {abi.ERRORS.get(rc, rc)}: {msg}")
+
+
+class LiquidStep:
+    """One world's liquid on the GPU: its buffers resident in device memory,
+    stepped by wig_fluid_step.  `stream` is a cudaStream_t as an int (0: the
+    legacy stream)."""
+
+    def __init__(self, world, elems, stream=0):
+        self.world = world
+        self.elems = elems
+        self.stream = C.c_void_p(stream or None)
+        L = lib()
+        h = C.c_void_p()
+        d = world.desc()
+        check(L.wig_fluid_create(C.byref(d), elems, len(elems), C.byref(h)), "wig_fluid_create")
+        self.h = h
+        check(L.wig_fluid_bind(h, None), "wig_fluid_bind")
+        self.upload()
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().wig_fluid_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def upload(self, world=None):
+        w = world or self.world
+        for k, name in enumerate(abi.BUFFER_NAMES):
+            arr = np.ascontiguousarray(getattr(w, name))
+            check(lib().wig_fluid_upload(self.h, k, arr.ctypes.data, 0, arr.nbytes, self.stream), f"upload {name}")
+
+    def download(self, world=None, names=abi.BUFFER_NAMES):
+        w = world or self.world
+        for name in names:
+            k = abi.BUFFER_NAMES.index(name)
+            arr = getattr(w, name)
+            assert arr.flags["C_CONTIGUOUS"]
+            check(lib().wig_fluid_download(self.h, k, arr.ctypes.data, 0, arr.nbytes, self.stream), f"download {name}")
+        return w
+
+    def buffers(self):
+        b = abi.Buffers()
+        check(lib().wig_fluid_buffers_of(self.h, C.byref(b)), "buffers_of")
+        return b
+
+    def step(self, P, max_cycles=abi.FLUID_CYCLES, flags=0, tolerance=1e-6):
+        check(lib().wig_fluid_step(self.h, C.byref(P), max_cycles, flags, tolerance, self.stream), "wig_fluid_step")
+
+    def dispatch(self, P, name, level=0, cycle=0):
+        check(lib().wig_fluid_dispatch(self.h, C.byref(P), abi.PASS[name], level, cycle, self.stream), f"dispatch {name}")
+
+    def stats(self):
+        st = abi.Stats()
+        check(lib().wig_fluid_read_stats(self.h, C.byref(st)), "wig_fluid_read_stats")
+        return st

@@ -1,0 +1,250 @@
+"""Host-side world state in the reference's buffer layouts, and the
+synthetic worlds of the benchmark configurations.
+
+A world is the set of buffers `Simulation` allocates for the liquid
+(js/sim.js:741-843) plus the `cells` raster, all as numpy arrays in the exact
+byte layouts the shaders read:
+
+  cells     u32[4 * (C + ceil(C/2))]   vec4 per cell (x word, temp bits, f16x2
+                                       velocity, w), then the gas plane
+  sorted    u32[4 + 12 * cap]          Particles: count, 3 pad, motion/state/affine planes
+  parts     u32[4 + 12 * cap]
+  counters  u32[11 C + 2 F]
+  field     f32[4 * (2 (C + level cells) + F + 2 ceil(F/4))]
+  blocks    u32[5 B + 9]
+  cg        f32[4 * (C + B + 1)]
+
+New liquid is painted as undrawn WATER cells, and the first step's syncSeed
+(shaders/fluid.wgsl:863-890) turns each into LIQUID_PER_CELL particles, as a
+scene painted by js/scenes.js is (`dam`, js/scenes.js:404-407).
+"""
+import math
+import struct
+
+import numpy as np
+
+from . import abi
+
+# ---------------------------------------------------------------- elements
+
+GRAVITY = 9.81 / 3600 / 0.01  # js/elements.js:31, cells/step^2 at 1 cm and 60 steps/s
+T_NEVER = 1e9
+GAS_HEAT_CAP = 1.2e-3 * 1000.0  # order of js/shared.js:174; read by nothing on the liquid's path
+
+
+def element_table():
+    """The element rows the liquid step reads, for AIR, WALL, SAND, WATER
+    (js/elements.js:414-458, with DEFAULTS js/elements.js:316-360)."""
+    rows = [abi.Elem() for _ in range(4)]
+
+    def fill(e, **kw):
+        base = dict(kind=abi.KIND_SOLID, density=1000.0, weight=GRAVITY, heat_cap=2.0, viscosity=0.0,
+                    viscosity_t=20.0, viscosity_e=0.0, tension=0.0, expansion=0.0, expansion2=0.0,
+                    hi_t=T_NEVER, lo_t=-T_NEVER, up_span=1e30, down_span=1e30, down_scale=0.0,
+                    sol_density=0.0, flags=0, wetting=0.5)
+        base.update(kw)
+        for k, v in base.items():
+            setattr(e, k, v)
+
+    fill(rows[abi.AIR], kind=abi.KIND_GAS, density=1.0, weight=0.0, heat_cap=GAS_HEAT_CAP)
+    fill(rows[abi.WALL], flags=4 | 2 | 8, wetting=0.8)
+    fill(rows[abi.SAND], kind=abi.KIND_POWDER, density=265.0, heat_cap=1.3, hi_t=1250.0, wetting=0.95,
+         up_span=220.0 / 1.3)
+    fill(rows[abi.WATER], kind=abi.KIND_LIQUID, density=100.0, heat_cap=4.18, hi_t=100.0, lo_t=0.0,
+         up_span=2257.0 / 4.18, down_span=334.0 / 4.18, down_scale=1.0, expansion=1.42e-4,
+         expansion2=4.45e-6, tension=1.0, flags=2)
+    return (abi.Elem * 4)(*rows)
+
+
+# ---------------------------------------------------------------- cells
+
+def f32_bits(x):
+    return struct.unpack("<I", struct.pack("<f", float(x)))[0]
+
+
+def f16x2(a, b):
+    """pack2x16float of float arrays a, b (round to nearest even)."""
+    lo = np.asarray(a, dtype=np.float32).astype(np.float16).view(np.uint16).astype(np.uint32)
+    hi = np.asarray(b, dtype=np.float32).astype(np.float16).view(np.uint16).astype(np.uint32)
+    return lo | (hi << 16)
+
+
+class World:
+    """The liquid's buffers for one world, host side, zeroed as
+    Simulation.clear leaves them (js/sim.js:1259)."""
+
+    def __init__(self, width, height, liquid_per_cell=4, capacity=0, temperature=20.0):
+        self.L = abi.layout_py(width, height, liquid_per_cell, capacity)
+        L = self.L
+        self.W, self.H = L["width"], L["height"]
+        self.C = L["cell_count"]
+        self.cap = L["capacity"]
+        self.cells = np.zeros(L["cells_bytes"] // 4, dtype=np.uint32)
+        self.sorted = np.zeros(L["particles_bytes"] // 4, dtype=np.uint32)
+        self.parts = np.zeros(L["particles_bytes"] // 4, dtype=np.uint32)
+        self.counters = np.zeros(L["counters_bytes"] // 4, dtype=np.uint32)
+        self.field = np.zeros(L["field_bytes"] // 4, dtype=np.float32)
+        self.blocks = np.zeros(L["blocks_bytes"] // 4, dtype=np.uint32)
+        self.cg = np.zeros(L["cg_bytes"] // 4, dtype=np.float32)
+        cv = self.cell_view()
+        cv[:, 0] = abi.AIR
+        cv[:, 1] = f32_bits(temperature)
+        self.temperature = temperature
+
+    def desc(self):
+        return abi.WorldDesc(self.W, self.H, self.L["liquid_per_cell"], self.cap)
+
+    def cell_view(self):
+        return self.cells[: 4 * self.C].reshape(self.H, self.W, 4)
+
+    def paint(self, mask, elem, vel=None):
+        """Cells under mask (H x W bool) become `elem`, undrawn, at the
+        world's temperature; vel (H x W x 2, cells/step) sets their f16
+        velocity, which syncSeed gives the particles it seeds there."""
+        cv = self.cell_view()
+        cv[mask, 0] = elem
+        cv[mask, 1] = f32_bits(self.temperature)
+        cv[mask, 3] = 0
+        if vel is not None:
+            cv[mask, 2] = f16x2(vel[..., 0][mask], vel[..., 1][mask])
+        else:
+            cv[mask, 2] = 0
+
+    def buffers(self):
+        return {k: getattr(self, k) for k in abi.BUFFER_NAMES}
+
+    def copy(self):
+        w = World.__new__(World)
+        w.__dict__.update(self.__dict__)
+        for k in abi.BUFFER_NAMES:
+            setattr(w, k, getattr(self, k).copy())
+        return w
+
+    # -- views used by the tests
+    def particle_count(self, which="sorted"):
+        return int(getattr(self, which)[0])
+
+    def particles(self, which="sorted"):
+        """(motion f32[n,4], state u32[n,4], affine f32[n,4]) of the live particles."""
+        buf = getattr(self, which)
+        n = min(int(buf[0]), self.cap)
+        items = buf[4:].reshape(3, self.cap, 4)
+        return (items[0, :n].view(np.float32), items[1, :n], items[2, :n].view(np.float32))
+
+    def counters_cells(self):
+        return self.counters[: 11 * self.C].reshape(self.C, 11)
+
+    def field_cells(self):
+        return self.field[: 8 * self.C].reshape(self.C, 2, 4)
+
+    def pressure(self):
+        return self.field_cells()[:, 0, 0].reshape(self.H, self.W)
+
+    def density_class(self):
+        return self.field_cells()[:, 0, 2].reshape(self.H, self.W)
+
+
+def make_params(world, frame, seed, earth_g, dx=1.0, dt=1.0 / 120.0):
+    P = abi.Params()
+    P.size[0], P.size[1] = world.W, world.H
+    P.frame = frame & 0xffffffff
+    P.seed = seed & 0xffffffff
+    P.dx = dx
+    P.earth_g = earth_g
+    P.dt = dt
+    return P
+
+
+# ---------------------------------------------------------------- configurations
+
+def earth_g_cells(g=9.8, dt=1.0 / 120.0, dx=1.0):
+    """|g| dt^2 / dx: the Earth's pull in cells per step^2 (y down)."""
+    return float(np.float32(g * dt * dt / dx))
+
+
+def dam_break(width=256, height=256, seed=1):
+    """Plain 2D dam break: one-cell WALL border, WATER filling the bottom-left
+    40% width x 60% height inside it, at rest (4 particles per cell seeded by
+    syncSeed's jittered quarters)."""
+    w = World(width, height)
+    wall = np.zeros((height, width), dtype=bool)
+    wall[0, :] = wall[-1, :] = True
+    wall[:, 0] = wall[:, -1] = True
+    w.paint(wall, abi.WALL)
+    fw, fh = int(round(0.4 * width)), int(round(0.6 * height))
+    water = np.zeros((height, width), dtype=bool)
+    water[height - 1 - fh:height - 1, 1:1 + fw] = True
+    w.paint(water, abi.WATER)
+    w.config = dict(workload="dam_break", grid=f"{width}x{height}", seed=seed, earth_g=earth_g_cells())
+    return w
+
+
+def disks_world(width=1024, height=1024, n_disks=200, r_lo=4, r_hi=24, sigma=0.5, seed=2):
+    """Single world at scale: WALL disks (centres and radii uniform under the
+    seed), WATER in the top half outside them with Gaussian cell velocities
+    (sigma cells/step per axis, one draw per cell, carried by the cell's f16
+    velocity into the 4 particles syncSeed puts there)."""
+    rng = np.random.default_rng(seed)
+    w = World(width, height)
+    yy, xx = np.mgrid[0:height, 0:width]
+    wall = np.zeros((height, width), dtype=bool)
+    cx = rng.uniform(0, width, n_disks)
+    cy = rng.uniform(0, height, n_disks)
+    r = rng.uniform(r_lo, r_hi, n_disks)
+    for k in range(n_disks):
+        x0, x1 = int(max(0, cx[k] - r[k] - 1)), int(min(width, cx[k] + r[k] + 2))
+        y0, y1 = int(max(0, cy[k] - r[k] - 1)), int(min(height, cy[k] + r[k] + 2))
+        sub = (xx[y0:y1, x0:x1] + 0.5 - cx[k]) ** 2 + (yy[y0:y1, x0:x1] + 0.5 - cy[k]) ** 2 <= r[k] ** 2
+        wall[y0:y1, x0:x1] |= sub
+    w.paint(wall, abi.WALL)
+    water = (yy < height // 2) & ~wall
+    vel = rng.normal(0.0, sigma, (height, width, 2)).astype(np.float32)
+    w.paint(water, abi.WATER, vel=vel)
+    w.config = dict(workload="disks", grid=f"{width}x{height}", seed=seed, earth_g=earth_g_cells(),
+                    disks=n_disks, sigma=sigma)
+    return w
+
+
+def obstacle_column(width=2048, height=2048, p_solid=0.03, fill=0.7, ppc=2, seed=3):
+    """Mixed-precision config: Bernoulli(p) WALL cells dilated once (4-neighbour),
+    WATER in the bottom `fill` of the height outside them, `ppc` particles per
+    cell (LIQUID_PER_CELL as a parameter)."""
+    rng = np.random.default_rng(seed)
+    w = World(width, height, liquid_per_cell=ppc)
+    seedm = rng.random((height, width)) < p_solid
+    wall = seedm.copy()
+    wall[1:, :] |= seedm[:-1, :]
+    wall[:-1, :] |= seedm[1:, :]
+    wall[:, 1:] |= seedm[:, :-1]
+    wall[:, :-1] |= seedm[:, 1:]
+    w.paint(wall, abi.WALL)
+    yy = np.arange(height)[:, None]
+    water = (yy >= height - int(round(fill * height))) & ~wall
+    w.paint(water, abi.WATER)
+    w.config = dict(workload="obstacle_column", grid=f"{width}x{height}", seed=seed, earth_g=earth_g_cells(),
+                    p_solid=p_solid, ppc=ppc)
+    return w
+
+
+def small_world(width=32, height=32, seed=7, kind="dam"):
+    """A small world for parity tests: walls, a block of water and a few
+    obstacles, sized so the oracle finishes in well under a second a step."""
+    rng = np.random.default_rng(seed)
+    w = World(width, height)
+    wall = np.zeros((height, width), dtype=bool)
+    wall[-1, :] = True
+    wall[:, 0] = wall[:, -1] = True
+    if kind == "obstacles":
+        for _ in range(max(1, width * height // 300)):
+            x, y = rng.integers(2, width - 3), rng.integers(height // 2, height - 3)
+            wall[y:y + 2, x:x + 2] = True
+    w.paint(wall, abi.WALL)
+    water = np.zeros((height, width), dtype=bool)
+    water[height // 3:height - 1, 1:width // 2] = True
+    water &= ~wall
+    vel = None
+    if kind in ("obstacles", "moving"):
+        vel = rng.normal(0.0, 0.5, (height, width, 2)).astype(np.float32)
+    w.paint(water, abi.WATER, vel=vel)
+    w.config = dict(workload=f"small_{kind}", grid=f"{width}x{height}", seed=seed, earth_g=earth_g_cells())
+    return w
