@@ -1,0 +1,358 @@
+"""Liquid-step benchmark (one JSON line on rank 0).
+
+Workload: the single world at scale — a 1024 x 1024 MAC grid with 200 WALL
+disks (radii U[4, 24], centres uniform under the seed), WATER in the top half
+at 4 particles per cell with Gaussian cell velocities (sigma 0.5 cells/step),
+Earth's pull at dt 1/120 — stepped by the CUDA liquid step with the pressure
+solved to a 1e-6 relative residual (||r||2/||b||2, FP64 norms).
+
+A step is one liquid step (encodeFluid's whole pass sequence).  `value` is
+grid cells x steps / device time (CUDA events on the launch stream, the
+world resident in HBM, 0.7 GB: larger than L2, so no flush is needed);
+`e2e` is the same through the public API with every step's Params copied
+host->device from pinned memory and the step's report read back.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun) every rank steps its own replica of the world (the
+path does not shard: replicas only), timed as the max over ranks.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+from worldinagrain_b200 import abi  # noqa: E402
+from worldinagrain_b200 import world as W  # noqa: E402
+
+METRIC = "Liquid-step Mcells/s at 1e-6 residual"
+TOL = 1e-6
+MAX_CYCLES = 64
+FLAGS = abi.STEP_TOLERANCE | abi.STEP_F64_DOTS
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.lines = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx.append(float(parts[1]))
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if parts[3 + k].lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_world(args):
+    if args.config == "disks":
+        w = W.disks_world(1024, 1024, seed=args.seed)
+    elif args.config == "dam":
+        w = W.dam_break(256, 256, seed=args.seed)
+    elif args.config == "column":
+        w = W.obstacle_column(2048, 2048, seed=args.seed)
+    else:
+        raise SystemExit(f"unknown config {args.config}")
+    return w
+
+
+def params(world, step, seed):
+    return W.make_params(world, frame=step, seed=seed, earth_g=world.config["earth_g"])
+
+
+# Algorithmic bytes of one launch of each pass: the words the reference
+# layout makes it read and write once (per active cell, fluid cell, face or
+# particle), counted from the world after the step.  Active cells are the
+# active blocks' 64 each.
+def algorithmic_bytes(name, s):
+    A, Cf, N = s["active_cells"], s["fluid_cells"], s["particles"]
+    table = {
+        # 10x10 tile of (field cell z, x; drift x; rim x2; share) in, pot out
+        "RELAX": A * (16 + 4 + 8 + 4 + 4) + Cf * (8 + 8),
+        "RELAX_SHIFTED": A * (16 + 4 + 8 + 4 + 4) + Cf * (8 + 8),
+        # motion + state + affine read, the cell's and its faces' sums updated
+        "GATHER": N * 48 + A * (2 * 4 * 4 + 3 * 4 * 2),
+        "ADVECT": N * (32 + 16 + 16) + A * (2 * 16),
+        "CG_APPLY": Cf * (16 + 4 + 4 + 4 + 4) + A * 4,
+        "CG_UPDATE": Cf * (16 + 16 + 16),
+        "CG_RHO": Cf * (16 + 4 + 4),
+        "CG_DIRECTION": Cf * (8 + 8),
+        "PROLONG_FINE": Cf * (16 + 8) + A * 8 // 4,
+        "SCATTER": N * (48 + 48 + 8),
+        "SYNC_PARTICLES": N * (48 + 48) + A * 16,
+        "CLASSIFY": A * (16 + 32 + 32 + 12),
+        "SET_FACES": A * 2 * (8 + 16 + 16 + 4),
+        "PROJECT": A * 2 * (16 + 16 + 8),
+    }
+    return table.get(name)
+
+
+def world_stats(world):
+    blocks = world.blocks
+    B = world.L["block_count"]
+    active = int(blocks[4 * B + abi.COUNT_ACTIVE])
+    rho = world.field_cells()[:, 0, 2]
+    return {"active_cells": active * 64, "fluid_cells": int(np.sum(rho > 0)), "particles": int(world.sorted[0])}
+
+
+def cpu_baseline(world, args, budget_s):
+    """The CPU oracle (a single-threaded port of the reference's passes) on
+    the same world state, steps until about budget_s of work."""
+    from oracle.oracle import Oracle
+    w = world.copy()
+    o = Oracle(w, W.element_table())
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        o.step(params(w, 10_000 + steps, args.seed), max_cycles=MAX_CYCLES, flags=FLAGS, tolerance=TOL)
+        steps += 1
+        if time.perf_counter() - t0 >= budget_s or steps >= args.cpu_steps_max:
+            break
+    dt = time.perf_counter() - t0
+    return w.C * steps / dt / 1e6, steps, dt
+
+
+def run_reference(args, rank, world_size):
+    """The reference arm: the oracle port timed on the host cores."""
+    if rank != 0:
+        return
+    world = make_world(args)
+    from oracle.oracle import Oracle
+    o = Oracle(world, W.element_table())
+    t_w0 = time.perf_counter()
+    for s in range(1, args.warmup + 1):
+        o.step(params(world, s, args.seed), max_cycles=MAX_CYCLES, flags=FLAGS, tolerance=TOL)
+    budget = args.cpu_budget
+    steps, t0 = 0, time.perf_counter()
+    while steps < args.steps:
+        o.step(params(world, args.warmup + 1 + steps, args.seed), max_cycles=MAX_CYCLES, flags=FLAGS, tolerance=TOL)
+        steps += 1
+        if time.perf_counter() - t0 >= budget:
+            break
+    dt = time.perf_counter() - t0
+    value = world.C * steps / dt / 1e6
+    sample = (f"{steps} of {args.steps} timed steps of the full {world.config['grid']} world after {args.warmup} "
+              f"warm-up steps ({time.perf_counter() - t_w0:.0f} s in all), stopped at a {budget:.0f} s budget")
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "Mcells/s", "n_gpus": world_size,
+        "steps": steps, "warmup": args.warmup, "ms_per_step": round(dt / steps * 1e3, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": config_of(world, args),
+        "cpu_baseline": {"value": round(value, 4), "unit": "Mcells/s", "cores": 1, "kind": "port", "sample": sample},
+        "e2e": {"value": round(value, 4), "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_of(world, args):
+    return {"workload": f"{world.config['workload']}_{world.config['grid']}", "grid": world.config["grid"],
+            "seed": args.seed, "liquid_per_cell": world.L["liquid_per_cell"], "tolerance": TOL,
+            "residual": "||r||2/||b||2 of the CG residual, FP64 norms", "max_cycles": MAX_CYCLES,
+            "form": "plain drop-in (reference layouts), FP32 vectors, FP64 dot products",
+            "l2": "inputs larger than L2 (world resident in HBM, no flush)", "parallelism": "replicas"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="disks")
+    ap.add_argument("--seed", type=int, default=2)
+    ap.add_argument("--profile-steps", type=int, default=2)
+    ap.add_argument("--cpu-budget", type=float, default=20.0)
+    ap.add_argument("--cpu-steps-max", type=int, default=20)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = int(os.environ.get("RANK", "0"))
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        run_reference(args, rank, world_size)
+        return
+
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world_size > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local_rank))
+
+    from worldinagrain_b200 import fluid
+
+    world = make_world(args)
+    stream = torch.cuda.Stream()
+    g = fluid.LiquidStep(world, W.element_table(), stream=stream.cuda_stream)
+    step_no = 0
+    for _ in range(args.warmup):
+        step_no += 1
+        g.step(params(world, step_no, args.seed), max_cycles=MAX_CYCLES, flags=FLAGS, tolerance=TOL)
+    g.stats()
+    torch.cuda.synchronize()
+
+    # ---- device-timed region: K steps, the world resident
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    gpu_index = torch.cuda.current_device()
+    if "CUDA_VISIBLE_DEVICES" in os.environ and os.environ["CUDA_VISIBLE_DEVICES"].strip():
+        try:
+            gpu_index = int(os.environ["CUDA_VISIBLE_DEVICES"].split(",")[local_rank])
+        except ValueError:
+            pass
+    with Clocks(gpu_index) as clk:
+        barrier()
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+        for _ in range(args.steps):
+            step_no += 1
+            g.step(params(world, step_no, args.seed), max_cycles=MAX_CYCLES, flags=FLAGS, tolerance=TOL)
+        with torch.cuda.stream(stream):
+            e1.record(stream)
+        barrier()
+    ms = e0.elapsed_time(e1)
+    st = g.stats()
+    launches_per_step = st.launches
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    cells = world.C
+    value = cells * args.steps * world_size / (ms / 1e3) / 1e6
+
+    # ---- end to end through the public API: params in, report out, every step
+    cycles = []
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step_no += 1
+        g.step(params(world, step_no, args.seed), max_cycles=MAX_CYCLES, flags=FLAGS, tolerance=TOL)
+        s2 = g.stats()
+        cycles.append(s2.cycles)
+        if s2.rel_residual > TOL:
+            raise SystemExit(f"solve left {s2.rel_residual:.3e} > {TOL} after {s2.cycles} iterations")
+    e2e_s = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = cells * args.steps * world_size / e2e_s / 1e6
+
+    # ---- per-pass device times of eagerly launched steps (events on the stream)
+    prof = {}
+    for _ in range(args.profile_steps):
+        step_no += 1
+        for k, (t_ms, n) in g.step_profile(params(world, step_no, args.seed), max_cycles=MAX_CYCLES, flags=FLAGS,
+                                           tolerance=TOL).items():
+            a, b = prof.get(k, (0.0, 0))
+            prof[k] = (a + t_ms, b + n)
+    g.download(world)
+    ws = world_stats(world)
+    total = sum(v[0] for v in prof.values())
+    ranked = sorted(prof.items(), key=lambda kv: -kv[1][0])
+    top = next((k for k, _ in ranked if algorithmic_bytes(k, ws) is not None), ranked[0][0])
+    t_ms, n = prof[top]
+    per_launch_s = t_ms / n / 1e3
+    alg = algorithmic_bytes(top, ws) or 0
+    peak, peak_kind = peaks()
+    achieved = alg / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        v, nsteps, dt = cpu_baseline(world, args, args.cpu_budget)
+        cpu = {"value": round(v, 4), "unit": "Mcells/s", "cores": 1, "kind": "port",
+               "sample": f"{nsteps} steps of the same {world.config['grid']} world state on one host core, {dt:.1f} s"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Mcells/s", "n_gpus": world_size,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_of(world, args),
+            "e2e": {"value": round(e2e, 3), "unit": "Mcells/s", "h2d_bytes_per_step": 152, "d2h_bytes_per_step": 64},
+            "gpu_launches": launches_per_step * args.steps,
+            "roofline": {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                         "algorithmic_bytes_per_launch": alg, "launch_ms": round(per_launch_s * 1e3, 5)},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "solve": {"cycles_mean": round(float(np.mean(cycles)), 2), "cycles_max": int(np.max(cycles)),
+                      "rel_residual_last": s2.rel_residual},
+            "world": ws,
+            "profile_ms_per_step": {k: round(v[0] / args.profile_steps, 4) for k, v in ranked[:12]},
+            "profile_share": {k: round(v[0] / total, 4) for k, v in ranked[:12]},
+        }
+        print(json.dumps(line), flush=True)
+    g.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

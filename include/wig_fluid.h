@@ -185,7 +185,7 @@ typedef struct wig_fluid_stats {
     uint32_t count[WIG_FLUID_STATS];  /* FLUID_COUNT words */
     uint32_t particles;               /* sorted.count after the step */
     uint32_t cycles;                  /* CG iterations run this step */
-    uint32_t pad;
+    uint32_t launches;                /* kernels the last step launched */
     double rel_residual;              /* ||r||2/||b||2 of the CG residual, FP64 (tolerance mode) */
     double b_norm;                    /* ||b||2 at the solve's start */
 } wig_fluid_stats;
@@ -282,6 +282,17 @@ int wig_fluid_dispatch(wig_fluid* h, const wig_params* P, int pass, uint32_t lev
  * js/snapshot.js:97-164) for worlds loaded or saved by the host. */
 int wig_fluid_upload(wig_fluid* h, int which, const void* host, uint64_t offset, uint64_t bytes, void* stream);
 int wig_fluid_download(wig_fluid* h, int which, void* host, uint64_t offset, uint64_t bytes, void* stream);
+
+/* Profile slots: one per pass id, then the tolerance form's norm kernel,
+ * then the report kernel. */
+#define WIG_PROFILE_SLOTS (WIG_PASS_COUNT + 2)
+
+/* One step as wig_fluid_step, but launched pass by pass with CUDA events
+ * around each launch (the reference's per-phase GPU timestamps,
+ * js/timer.js:7-98): per slot, the summed milliseconds in ms_out and the
+ * launches in calls_out (WIG_PROFILE_SLOTS entries each).  Synchronous. */
+int wig_fluid_step_profile(wig_fluid* h, const wig_params* P, uint32_t max_cycles, uint32_t flags, double tolerance,
+                           void* stream, float* ms_out, uint32_t* calls_out);
 
 /* Replaces readReport (js/sim.js:1882-1900): waits for the stream and reads
  * the FLUID_COUNT words and the solve's statistics of the last step. */

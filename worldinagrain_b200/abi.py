@@ -44,6 +44,8 @@ PASSES = [
     "SCAN_FINISH", "SCATTER", "RASTER_CLAIMS", "RASTER", "UNPAINT",
 ]
 PASS = {name: i for i, name in enumerate(PASSES)}
+PROFILE_SLOTS = len(PASSES) + 2
+PROFILE_NAMES = PASSES + ["NORM", "REPORT"]
 
 
 class Params(C.Structure):
@@ -93,7 +95,7 @@ class Buffers(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("count", C.c_uint32 * FLUID_STATS), ("particles", C.c_uint32), ("cycles", C.c_uint32),
-                ("pad", C.c_uint32), ("rel_residual", C.c_double), ("b_norm", C.c_double)]
+                ("launches", C.c_uint32), ("rel_residual", C.c_double), ("b_norm", C.c_double)]
 
 
 BUFFER_NAMES = ("cells", "sorted", "parts", "counters", "field", "blocks", "cg")

@@ -77,6 +77,8 @@ struct wig_fluid {
     cudaStream_t cap = nullptr;      // capture stream
     cudaStream_t last_stream = nullptr;
     std::map<uint64_t, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs;
+    std::map<uint64_t, uint32_t> graph_launches;  // kernels in each graph
+    uint32_t last_launches = 0;
     uint32_t last_cycles_flags = 0;
 };
 
@@ -157,6 +159,7 @@ void drop_graphs(wig_fluid* h) {
         if (kv.second.first) cudaGraphDestroy(kv.second.first);
     }
     h->graphs.clear();
+    h->graph_launches.clear();
 }
 
 // Writes this step's state into the next pinned slot and copies it to the
@@ -180,10 +183,35 @@ int push_state(wig_fluid* h, const wig_params* P, uint32_t flags, double tol, cu
     return WIG_OK;
 }
 
-// Records the step's passes in encodeFluid's order on stream s.
-int record_step(wig_fluid* h, uint32_t max_cycles, uint32_t flags, bool shifted, cudaStream_t s) {
+// Per-pass timing of an eagerly launched step (the reference's per-phase
+// GPU timestamps, js/timer.js:7-98): events around each launch.
+struct Prof {
+    std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+};
+
+// Records the step's passes in encodeFluid's order on stream s; returns the
+// number of kernels launched.
+uint32_t record_step(wig_fluid* h, uint32_t max_cycles, uint32_t flags, bool shifted, cudaStream_t s, Prof* prof) {
     const wig::Dev& D = h->D;
-    auto run = [&](int pass, uint32_t level = 0, uint32_t cycle = 0) { return wig::launch_pass(D, pass, level, cycle, s); };
+    uint32_t launches = 0;
+    auto timed = [&](int id, auto fn) {
+        cudaEvent_t a = nullptr, b = nullptr;
+        if (prof) {
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            cudaEventRecord(a, s);
+        }
+        fn();
+        launches++;
+        if (prof) {
+            cudaEventRecord(b, s);
+            prof->marks.push_back({id, {a, b}});
+        }
+    };
+    auto run = [&](int pass, uint32_t level = 0, uint32_t cycle = 0) {
+        timed(pass, [&] { wig::launch_pass(D, pass, level, cycle, s); });
+    };
+    auto norm = [&](int which, uint32_t cycle) { timed(WIG_PASS_COUNT, [&] { wig::launch_norm(D, which, cycle, s); }); };
     const bool tol = (flags & WIG_STEP_TOLERANCE) != 0u;
     if (flags & WIG_STEP_BOOKKEEPING_ONLY) {
         run(WIG_PASS_SYNC_MARKS);
@@ -213,7 +241,7 @@ int record_step(wig_fluid* h, uint32_t max_cycles, uint32_t flags, bool shifted,
         run(WIG_PASS_CG_JOIN);
         run(WIG_PASS_CG_ANCHOR);
         run(WIG_PASS_CG_RESIDUAL);
-        if (tol) wig::launch_norm(D, 0, 0, s);
+        if (tol) norm(0, 0);
         run(WIG_PASS_CG_PREPARE);
         bool sh = shifted;
         for (uint32_t cycle = 0; cycle < max_cycles; cycle++) {
@@ -243,7 +271,7 @@ int record_step(wig_fluid* h, uint32_t max_cycles, uint32_t flags, bool shifted,
             run(WIG_PASS_CG_APPLY, 0, cycle);
             run(WIG_PASS_CG_ALPHA, 0, cycle);
             run(WIG_PASS_CG_UPDATE, 0, cycle);
-            if (tol) wig::launch_norm(D, 1, cycle, s);
+            if (tol) norm(1, cycle);
         }
         run(WIG_PASS_CG_FINISH);
         run(WIG_PASS_PROJECT);
@@ -259,8 +287,14 @@ int record_step(wig_fluid* h, uint32_t max_cycles, uint32_t flags, bool shifted,
         run(WIG_PASS_RASTER);
         run(WIG_PASS_UNPAINT);
     }
-    k_report<<<1, 32, 0, s>>>(D, h->d_report);
-    return WIG_OK;
+    timed(WIG_PASS_COUNT + 1, [&] { k_report<<<1, 32, 0, s>>>(D, h->d_report); });
+    return launches;
+}
+
+bool step_parity(wig_fluid* h, uint32_t flags) {
+    if (flags & WIG_STEP_SHIFTED_SET) return (flags & WIG_STEP_SHIFTED_FIRST) != 0u;
+    if (!(flags & WIG_STEP_BOOKKEEPING_ONLY)) h->shifted_first = !h->shifted_first;
+    return h->shifted_first;
 }
 
 }  // namespace
@@ -422,15 +456,7 @@ int wig_fluid_step(wig_fluid* h, const wig_params* P, uint32_t max_cycles, uint3
     if (max_cycles == 0 || max_cycles > 64) return fail(WIG_E_ARG, "max_cycles out of range (1..64)");
     if ((flags & WIG_STEP_TOLERANCE) && !(tolerance > 0.0)) return fail(WIG_E_ARG, "tolerance must be positive");
     cudaStream_t s = (cudaStream_t)stream;
-    bool sh;
-    if (flags & WIG_STEP_SHIFTED_SET) {
-        sh = (flags & WIG_STEP_SHIFTED_FIRST) != 0u;
-    } else if (!(flags & WIG_STEP_BOOKKEEPING_ONLY)) {
-        h->shifted_first = !h->shifted_first;
-        sh = h->shifted_first;
-    } else {
-        sh = h->shifted_first;
-    }
+    const bool sh = step_parity(h, flags);
     int rc = push_state(h, P, flags, tolerance, s, false);
     if (rc) return rc;
     const uint32_t shape_flags = flags & (WIG_STEP_BOOKKEEPING_ONLY | WIG_STEP_VISCOUS | WIG_STEP_TOLERANCE | WIG_STEP_F64_DOTS);
@@ -440,7 +466,7 @@ int wig_fluid_step(wig_fluid* h, const wig_params* P, uint32_t max_cycles, uint3
         cudaGraph_t g = nullptr;
         cudaGraphExec_t ge = nullptr;
         CUDA_TRY(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
-        record_step(h, max_cycles, flags, sh, h->cap);
+        uint32_t n = record_step(h, max_cycles, flags, sh, h->cap, nullptr);
         cudaError_t e = cudaStreamEndCapture(h->cap, &g);
         if (e != cudaSuccess) return fail(WIG_E_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
         e = cudaGraphInstantiate(&ge, g, 0);
@@ -449,11 +475,40 @@ int wig_fluid_step(wig_fluid* h, const wig_params* P, uint32_t max_cycles, uint3
             return fail(WIG_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
         }
         it = h->graphs.emplace(key, std::make_pair(g, ge)).first;
+        h->graph_launches[key] = n;
     }
+    h->last_launches = h->graph_launches[key];
     CUDA_TRY(cudaGraphLaunch(it->second.second, s));
     if (flags & WIG_STEP_SYNC_STATS) CUDA_TRY(cudaMemcpyAsync(h->h_report, h->d_report, sizeof(Report), cudaMemcpyDeviceToHost, s));
     h->last_stream = s;
     h->last_cycles_flags = flags;
+    return WIG_OK;
+}
+
+int wig_fluid_step_profile(wig_fluid* h, const wig_params* P, uint32_t max_cycles, uint32_t flags, double tolerance,
+                           void* stream, float* ms_out, uint32_t* calls_out) {
+    if (!h || !P || !ms_out || !calls_out) return fail(WIG_E_ARG, "null argument");
+    if (!h->bound) return fail(WIG_E_STATE, "buffers not bound");
+    if (max_cycles == 0 || max_cycles > 64) return fail(WIG_E_ARG, "max_cycles out of range (1..64)");
+    if ((flags & WIG_STEP_TOLERANCE) && !(tolerance > 0.0)) return fail(WIG_E_ARG, "tolerance must be positive");
+    cudaStream_t s = (cudaStream_t)stream;
+    const bool sh = step_parity(h, flags);
+    int rc = push_state(h, P, flags, tolerance, s, false);
+    if (rc) return rc;
+    Prof prof;
+    h->last_launches = record_step(h, max_cycles, flags, sh, s, &prof);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(s));
+    for (int k = 0; k < WIG_PROFILE_SLOTS; k++) { ms_out[k] = 0.0f; calls_out[k] = 0u; }
+    for (auto& m : prof.marks) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, m.second.first, m.second.second);
+        ms_out[m.first] += ms;
+        calls_out[m.first] += 1u;
+        cudaEventDestroy(m.second.first);
+        cudaEventDestroy(m.second.second);
+    }
+    h->last_stream = s;
     return WIG_OK;
 }
 
@@ -467,6 +522,7 @@ int wig_fluid_read_stats(wig_fluid* h, wig_fluid_stats* out) {
     for (uint32_t k = 0; k < WIG_FLUID_STATS; k++) out->count[k] = r.count[k];
     out->particles = r.particles;
     out->cycles = r.count[WIG_COUNT_CYCLES];
+    out->launches = h->last_launches;
     out->rel_residual = r.rel;
     out->b_norm = r.bnorm2 > 0.0 ? __builtin_sqrt(r.bnorm2) : 0.0;
     if (r.err) return fail(WIG_E_STATE, "a device loop hit its iteration limit (union-find)");

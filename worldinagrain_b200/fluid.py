@@ -28,6 +28,8 @@ FUNCS = {
     "wig_fluid_upload": ([C.c_void_p, C.c_int, C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p], C.c_int),
     "wig_fluid_download": ([C.c_void_p, C.c_int, C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p], C.c_int),
     "wig_fluid_read_stats": ([C.c_void_p, C.POINTER(abi.Stats)], C.c_int),
+    "wig_fluid_step_profile": ([C.c_void_p, C.POINTER(abi.Params), C.c_uint32, C.c_uint32, C.c_double, C.c_void_p,
+                                C.POINTER(C.c_float), C.POINTER(C.c_uint32)], C.c_int),
     "wig_fluid_destroy": ([C.c_void_p], None),
 }
 
@@ -110,6 +112,15 @@ class LiquidStep:
 
     def step(self, P, max_cycles=abi.FLUID_CYCLES, flags=0, tolerance=1e-6):
         check(lib().wig_fluid_step(self.h, C.byref(P), max_cycles, flags, tolerance, self.stream), "wig_fluid_step")
+
+    def step_profile(self, P, max_cycles=abi.FLUID_CYCLES, flags=0, tolerance=1e-6):
+        """One step launched pass by pass with CUDA events around each:
+        {pass name: (ms, launches)}."""
+        ms = (C.c_float * abi.PROFILE_SLOTS)()
+        calls = (C.c_uint32 * abi.PROFILE_SLOTS)()
+        check(lib().wig_fluid_step_profile(self.h, C.byref(P), max_cycles, flags, tolerance, self.stream, ms, calls),
+              "wig_fluid_step_profile")
+        return {abi.PROFILE_NAMES[k]: (ms[k], calls[k]) for k in range(abi.PROFILE_SLOTS) if calls[k]}
 
     def dispatch(self, P, name, level=0, cycle=0):
         check(lib().wig_fluid_dispatch(self.h, C.byref(P), abi.PASS[name], level, cycle, self.stream), f"dispatch {name}")
