@@ -300,6 +300,25 @@ int wig_fluid_read_stats(wig_fluid* h, wig_fluid_stats* out);
 
 void wig_fluid_destroy(wig_fluid* h);
 
+/* No counterpart in the reference.  For hosts that own all device memory
+ * and cannot let a library call cudaMalloc (work recorded into a CUDA graph
+ * while it runs, one pre-reserved pool managed by the host's own allocator,
+ * a real-time path): the squared FP64 norm, over the liquid cells (field's
+ * z > 0) of the blocks worked on, of the pressure solve's residual r (cg's
+ * y per cell), summed in the same order as wig_fluid_step's tolerance form
+ * sums it (so it equals wig_fluid_stats' (rel_residual * b_norm)^2 after a
+ * tolerance-form step).  The caller passes the world's shape, its field,
+ * blocks and cg buffers, and a device double for the result, written on
+ * `stream`.  It allocates nothing: its per-block scratch is a static device
+ * array of WIG_NOALLOC_MAX_BLOCKS doubles (128 KiB held on every GPU that
+ * loads the library until the process exits), so worlds of more blocks are
+ * refused with WIG_E_ARG.  The first call on a device looks up that array's
+ * device address; make it before any stream capture.  Calls share the one
+ * array: calls whose work overlaps on the GPU race. */
+#define WIG_NOALLOC_MAX_BLOCKS 16384u
+int wig_fluid_residual_norm2_noalloc(const wig_world_desc* d, const void* field, const void* blocks, const void* cg,
+                                     double* out, void* stream);
+
 /* One-line description of the last error on this thread ("" if none). */
 const char* wig_fluid_last_error(void);
 

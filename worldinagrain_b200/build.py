@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "libwig_fluid.so")
-SOURCES = ["wig_api.cu", "wig_passes.cu"]
+SOURCES = ["wig_api.cu", "wig_passes.cu", "wig_noalloc.cu"]
 HEADERS = ["wig_device.cuh", "wig_passes.cuh"]
 
 NVCC_FLAGS = [

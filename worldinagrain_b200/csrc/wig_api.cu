@@ -27,6 +27,14 @@ int fail(int code, const std::string& msg) {
     return code;
 }
 
+}  // namespace
+
+namespace wig {
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+}  // namespace wig
+
+namespace {
+
 #define CUDA_TRY(call)                                                                              \
     do {                                                                                            \
         cudaError_t e_ = (call);                                                                    \

@@ -6,12 +6,16 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
 #include "../../include/wig_fluid.h"
 
 namespace wig {
+
+// The message wig_fluid_last_error() returns on this thread.
+void set_last_error(const std::string& msg);
 
 // ---------------------------------------------------------------- constants
 constexpr uint32_t NONE = 0xffffffffu;
