@@ -142,6 +142,14 @@ def algorithmic_bytes(name, s):
         "CLASSIFY": A * (16 + 32 + 32 + 12),
         "SET_FACES": A * 2 * (8 + 16 + 16 + 4),
         "PROJECT": A * 2 * (16 + 16 + 8),
+        # the fast form's structure-of-arrays kernels (a float a cell per array)
+        "F_RELAX": A * (4 + 8) + Cf * (32 + 8),
+        "F_APPLY_ALPHA": A * 4 + Cf * (4 + 16 + 8 + 1 + 4) + (A - Cf) * 8,
+        "F_UPDATE": A * 4 + Cf * (16 + 4 + 24),
+        "F_RHO_BETA": A * 4 + Cf * 12,
+        "F_DIRECTION": A * 8 + Cf * 8,
+        "F_PROLONG_FINE": A * 4 + Cf * (8 + 16) + Cf // 4 * 12,
+        "F_SETUP": A * (32 + 12 + 68),
     }
     return table.get(name)
 
@@ -206,7 +214,7 @@ def config_of(world, args):
     return {"workload": f"{world.config['workload']}_{world.config['grid']}", "grid": world.config["grid"],
             "seed": args.seed, "liquid_per_cell": world.L["liquid_per_cell"], "tolerance": TOL,
             "residual": "||r||2/||b||2 of the CG residual, FP64 norms", "max_cycles": MAX_CYCLES,
-            "form": "plain drop-in (reference layouts), FP32 vectors, FP64 dot products",
+            "form": (f"{args.form} form over the reference's buffer layouts; FP32 vectors, FP64 dot products"),
             "l2": "inputs larger than L2 (world resident in HBM, no flush)", "parallelism": "replicas"}
 
 
@@ -222,8 +230,14 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--cpu-steps-max", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--form", default="fast", choices=["fast", "plain", "persistent"])
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    global FLAGS
+    if args.form == "plain":
+        FLAGS = FLAGS | abi.STEP_PLAIN
+    elif args.form == "persistent":
+        FLAGS = FLAGS | abi.STEP_PERSISTENT
 
     rank = int(os.environ.get("RANK", "0"))
     world_size = int(os.environ.get("WORLD_SIZE", "1"))

@@ -178,6 +178,8 @@ typedef struct wig_fluid_buffers {
 #define WIG_STEP_TOLERANCE 16u        /* stop on ||r||2/||b||2 <= tol (FP64) instead of max|r| < 1e-2 */
 #define WIG_STEP_F64_DOTS 32u         /* CG dot products in FP64 */
 #define WIG_STEP_SYNC_STATS 64u       /* copy the stats to the host at the end of the step */
+#define WIG_STEP_PLAIN 128u           /* the solve as one kernel per reference pass (else the fast form) */
+#define WIG_STEP_PERSISTENT 256u      /* the fast form's iterations as one persistent cooperative kernel (else kernels in a graph WHILE loop) */
 
 /* Per-step statistics (the report words, js/sim.js:1882-1900, plus the
  * solve's residuals). */
@@ -284,8 +286,26 @@ int wig_fluid_upload(wig_fluid* h, int which, const void* host, uint64_t offset,
 int wig_fluid_download(wig_fluid* h, int which, void* host, uint64_t offset, uint64_t bytes, void* stream);
 
 /* Profile slots: one per pass id, then the tolerance form's norm kernel,
- * then the report kernel. */
-#define WIG_PROFILE_SLOTS (WIG_PASS_COUNT + 2)
+ * the report kernel, and the kernels of the fast form of the solve. */
+enum wig_profile_slot {
+    WIG_SLOT_NORM = WIG_PASS_COUNT,
+    WIG_SLOT_REPORT,
+    WIG_SLOT_F_SETUP,
+    WIG_SLOT_F_LOOP,
+    WIG_SLOT_F_RELAX,
+    WIG_SLOT_F_RESTRICT,
+    WIG_SLOT_F_SMOOTH,
+    WIG_SLOT_F_COARSE,
+    WIG_SLOT_F_PROLONG,
+    WIG_SLOT_F_PROLONG_FINE,
+    WIG_SLOT_F_RHO_BETA,
+    WIG_SLOT_F_DIRECTION,
+    WIG_SLOT_F_APPLY_ALPHA,
+    WIG_SLOT_F_UPDATE,
+    WIG_SLOT_F_FINISH,
+    WIG_SLOT_F_SOLVE,
+    WIG_PROFILE_SLOTS
+};
 
 /* One step as wig_fluid_step, but launched pass by pass with CUDA events
  * around each launch (the reference's per-phase GPU timestamps,

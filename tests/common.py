@@ -74,12 +74,35 @@ def canonical_regions(counters, C):
     return out
 
 
-def compare_worlds(x, y, grid=GRID, particles=("sorted", "parts"), skip_parts=False, region_links=False):
+def mask_solve_scratch(world, name, arr):
+    """arr with the pressure solve's scratch words zeroed: what a step writes
+    for its own later passes and the next step overwrites before it reads
+    them — the relaxation's rim snapshot (counters' G_RIM, words 9-10 of a
+    cell), the coarse levels (field past the faces), and cg's per-block
+    partial sums and scalars.  The fast form keeps these in its own scratch."""
+    a = np.array(arr, copy=True)
+    C, L = world.C, world.L
+    if name == "counters":
+        a[: 11 * C].reshape(C, 11)[:, 9:11] = 0
+    elif name == "field":
+        F = L["face_count"]
+        start = 4 * (2 * C + F + 2 * ((F + 3) // 4))
+        a[start:] = 0
+    elif name == "cg":
+        a[4 * C:] = 0
+    return a
+
+
+def compare_worlds(x, y, grid=GRID, particles=("sorted", "parts"), skip_parts=False, region_links=False,
+                   scratch=False):
     """A list of differences between worlds x and y (empty when equal).
-    region_links: compare the G_REGION words by their roots."""
+    region_links: compare the G_REGION words by their roots; scratch: leave
+    out the solve's scratch words (mask_solve_scratch)."""
     out = []
     for name in grid:
         a, b = getattr(x, name), getattr(y, name)
+        if scratch:
+            a, b = mask_solve_scratch(x, name, a), mask_solve_scratch(y, name, b)
         if region_links and name == "counters":
             a, b = canonical_regions(a, x.C), canonical_regions(b, y.C)
         d = diff_words(a, b, name)

@@ -94,10 +94,15 @@ def test_each_pass_matches_oracle(kind, steps):
     g.close()
 
 
+FORMS = {"plain": abi.STEP_PLAIN, "fast": 0, "persistent": abi.STEP_PERSISTENT}
+
+
+@pytest.mark.parametrize("form", ["plain", "fast", "persistent"])
 @pytest.mark.parametrize("kind", ["dam", "obstacles", "moving"])
-def test_steps_match_oracle(kind):
+def test_steps_match_oracle(kind, form):
     """Whole steps (the captured graph) from the first seeding on: grid
-    buffers bit for bit, particles as multisets, every step."""
+    buffers bit for bit (the fast form's solve scratch aside), particles as
+    multisets, every step."""
     fluid = _gpu()
     world = W.small_world(40, 32, seed=3, kind=kind)
     ref = world.copy()
@@ -107,10 +112,10 @@ def test_steps_match_oracle(kind):
     for s in range(1, 13):
         P = params(ref, s)
         o.step(P)
-        g.step(P)
+        g.step(P, flags=FORMS[form])
         st = g.stats()
         g.download(got)
-        diffs = compare_worlds(got, ref)
+        diffs = compare_worlds(got, ref, scratch=form != "plain")
         assert not diffs, f"step {s}: " + "; ".join(diffs)
         assert run_membership(got)
         assert st.particles == int(ref.sorted[0])
@@ -119,8 +124,9 @@ def test_steps_match_oracle(kind):
     g.close()
 
 
+@pytest.mark.parametrize("form", ["plain", "fast", "persistent"])
 @pytest.mark.parametrize("flags", [abi.STEP_TOLERANCE, abi.STEP_TOLERANCE | abi.STEP_F64_DOTS])
-def test_tolerance_forms_match_oracle(flags):
+def test_tolerance_forms_match_oracle(flags, form):
     """The 1e-6 relative-residual forms: same iterations, same buffers."""
     fluid = _gpu()
     world = W.dam_break(64, 64)
@@ -131,10 +137,10 @@ def test_tolerance_forms_match_oracle(flags):
     for s in range(1, 9):
         P = params(ref, s)
         so = o.step(P, max_cycles=48, flags=flags, tolerance=1e-6)
-        g.step(P, max_cycles=48, flags=flags, tolerance=1e-6)
+        g.step(P, max_cycles=48, flags=flags | FORMS[form], tolerance=1e-6)
         sg = g.stats()
         g.download(got)
-        diffs = compare_worlds(got, ref)
+        diffs = compare_worlds(got, ref, scratch=form != "plain")
         assert not diffs, f"step {s}: " + "; ".join(diffs)
         assert sg.cycles == so.cycles
         assert sg.rel_residual <= 1e-6
@@ -161,6 +167,57 @@ def test_coincident_particles_pushed_apart_alike():
     o.step(P)
     g.step(P)
     g.download(got)
-    diffs = compare_worlds(got, ref)
+    diffs = compare_worlds(got, ref, scratch=True)
     assert not diffs, "; ".join(diffs)
     g.close()
+
+
+@pytest.mark.parametrize("form", ["fast", "persistent"])
+@pytest.mark.parametrize("size,seed", [((256, 256), 1), ((200, 136), 4), ((131, 97), 6)])
+def test_fast_form_matches_oracle_on_larger_worlds(size, seed, form):
+    """The fast form on worlds whose levels go down through the per-level
+    kernels into the one-CTA coarse kernel, world sides not multiples of 8
+    included: several steps with the 1e-6 form, against the oracle."""
+    fluid = _gpu()
+    if size == (256, 256):
+        world = W.dam_break(*size, seed=seed)
+    else:
+        world = W.small_world(*size, seed=seed, kind="obstacles")
+    ref = world.copy()
+    o = _oracle(ref)
+    g = fluid.LiquidStep(world, W.element_table())
+    got = world.copy()
+    flags = abi.STEP_TOLERANCE | abi.STEP_F64_DOTS
+    for s in range(1, 5):
+        P = params(ref, s)
+        so = o.step(P, max_cycles=64, flags=flags, tolerance=1e-6)
+        g.step(P, max_cycles=64, flags=flags | FORMS[form], tolerance=1e-6)
+        sg = g.stats()
+        g.download(got)
+        diffs = compare_worlds(got, ref, scratch=True)
+        assert not diffs, f"step {s}: " + "; ".join(diffs)
+        assert sg.cycles == so.cycles
+    g.close()
+
+
+@pytest.mark.parametrize("form", ["fast", "persistent"])
+def test_fast_profile_matches_graph(form):
+    """The profiled (eagerly launched) fast step leaves what the graph leaves."""
+    fluid = _gpu()
+    world = W.small_world(48, 40, seed=2, kind="obstacles")
+    a = fluid.LiquidStep(world.copy(), W.element_table())
+    b = fluid.LiquidStep(world.copy(), W.element_table())
+    wa, wb = world.copy(), world.copy()
+    for s in range(1, 5):
+        P = params(world, s)
+        a.step(P, flags=abi.STEP_TOLERANCE | FORMS[form], tolerance=1e-6, max_cycles=40)
+        prof = b.step_profile(P, flags=abi.STEP_TOLERANCE | FORMS[form], tolerance=1e-6, max_cycles=40)
+        assert ("F_UPDATE" if form == "fast" else "F_SOLVE") in prof
+        sa, sb = a.stats(), b.stats()
+        assert sa.cycles == sb.cycles and sa.launches == sb.launches
+        a.download(wa)
+        b.download(wb)
+        diffs = compare_worlds(wa, wb, scratch=True)
+        assert not diffs, f"step {s}: " + "; ".join(diffs)
+    a.close()
+    b.close()

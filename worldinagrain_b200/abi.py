@@ -33,6 +33,8 @@ STEP_VISCOUS = 8
 STEP_TOLERANCE = 16
 STEP_F64_DOTS = 32
 STEP_SYNC_STATS = 64
+STEP_PLAIN = 128
+STEP_PERSISTENT = 256
 
 PASSES = [
     "SYNC", "SYNC_MARKS", "SYNC_PARTICLES", "SYNC_SEED", "COMPACT", "RETIRE", "CLEAR", "GATHER",
@@ -44,8 +46,10 @@ PASSES = [
     "SCAN_FINISH", "SCATTER", "RASTER_CLAIMS", "RASTER", "UNPAINT",
 ]
 PASS = {name: i for i, name in enumerate(PASSES)}
-PROFILE_SLOTS = len(PASSES) + 2
-PROFILE_NAMES = PASSES + ["NORM", "REPORT"]
+PROFILE_NAMES = PASSES + ["NORM", "REPORT", "F_SETUP", "F_LOOP", "F_RELAX", "F_RESTRICT", "F_SMOOTH", "F_COARSE",
+                          "F_PROLONG", "F_PROLONG_FINE", "F_RHO_BETA", "F_DIRECTION", "F_APPLY_ALPHA", "F_UPDATE",
+                          "F_FINISH", "F_SOLVE"]
+PROFILE_SLOTS = len(PROFILE_NAMES)
 
 
 class Params(C.Structure):

@@ -14,8 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "libwig_fluid.so")
-SOURCES = ["wig_api.cu", "wig_passes.cu", "wig_noalloc.cu"]
-HEADERS = ["wig_device.cuh", "wig_passes.cuh"]
+SOURCES = ["wig_api.cu", "wig_passes.cu", "wig_fast.cu", "wig_noalloc.cu"]
+HEADERS = ["wig_device.cuh", "wig_passes.cuh", "wig_fast.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

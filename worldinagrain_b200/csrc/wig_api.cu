@@ -16,6 +16,7 @@
 #include <vector>
 
 #include "wig_device.cuh"
+#include "wig_fast.cuh"
 #include "wig_passes.cuh"
 
 namespace {
@@ -85,9 +86,16 @@ struct wig_fluid {
     cudaStream_t cap = nullptr;      // capture stream
     cudaStream_t last_stream = nullptr;
     std::map<uint64_t, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs;
-    std::map<uint64_t, uint32_t> graph_launches;  // kernels in each graph
+    std::map<uint64_t, uint32_t> graph_launches;  // kernels in each graph (fast form: outside the loop)
+    std::map<uint64_t, uint32_t> graph_body;      // fast form: kernels per iteration
     uint32_t last_launches = 0;
+    uint32_t last_body = 0;
     uint32_t last_cycles_flags = 0;
+    // the fast form's scratch
+    wig::Fast F{};
+    void* fast_mem = nullptr;
+    bool fast_dirty = true;
+    cudaStream_t cap2 = nullptr;     // capture stream of the iteration loop's body
 };
 
 namespace {
@@ -168,6 +176,7 @@ void drop_graphs(wig_fluid* h) {
     }
     h->graphs.clear();
     h->graph_launches.clear();
+    h->graph_body.clear();
 }
 
 // Writes this step's state into the next pinned slot and copies it to the
@@ -197,12 +206,15 @@ struct Prof {
     std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
 };
 
-// Records the step's passes in encodeFluid's order on stream s; returns the
-// number of kernels launched.
-uint32_t record_step(wig_fluid* h, uint32_t max_cycles, uint32_t flags, bool shifted, cudaStream_t s, Prof* prof) {
-    const wig::Dev& D = h->D;
+// Launch recording with optional per-launch events (Prof).
+struct Rec {
+    wig_fluid* h;
+    cudaStream_t s;
+    Prof* prof;
     uint32_t launches = 0;
-    auto timed = [&](int id, auto fn) {
+    cudaEvent_t pending = nullptr;
+    template <class Fn>
+    void timed(int id, Fn fn) {
         cudaEvent_t a = nullptr, b = nullptr;
         if (prof) {
             cudaEventCreate(&a);
@@ -215,88 +227,189 @@ uint32_t record_step(wig_fluid* h, uint32_t max_cycles, uint32_t flags, bool shi
             cudaEventRecord(b, s);
             prof->marks.push_back({id, {a, b}});
         }
-    };
-    auto run = [&](int pass, uint32_t level = 0, uint32_t cycle = 0) {
-        timed(pass, [&] { wig::launch_pass(D, pass, level, cycle, s); });
-    };
-    auto norm = [&](int which, uint32_t cycle) { timed(WIG_PASS_COUNT, [&] { wig::launch_norm(D, which, cycle, s); }); };
+    }
+    void run(int pass, uint32_t level = 0, uint32_t cycle = 0) {
+        timed(pass, [&] { wig::launch_pass(h->D, pass, level, cycle, s); });
+    }
+    void norm(int which, uint32_t cycle) {
+        timed(WIG_SLOT_NORM, [&] { wig::launch_norm(h->D, which, cycle, s); });
+    }
+    // the fast form's marker hook: events around each of its launches
+    static void mark(void* ctx, int slot, int phase) {
+        Rec* r = static_cast<Rec*>(ctx);
+        if (!r->prof) return;
+        cudaEvent_t e = nullptr;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, r->s);
+        if (phase == 0) {
+            r->pending = e;
+        } else {
+            r->prof->marks.push_back({slot, {r->pending, e}});
+            r->pending = nullptr;
+        }
+    }
+};
+
+// encodeFluid's passes before the solve (js/sim.js:2486-2521).
+void record_pre(Rec& R, uint32_t flags) {
+    R.run(WIG_PASS_SYNC);
+    R.run(WIG_PASS_SYNC_PARTICLES);
+    R.run(WIG_PASS_SYNC_SEED);
+    R.run(WIG_PASS_COMPACT);
+    R.run(WIG_PASS_RETIRE);
+    R.run(WIG_PASS_CLEAR);
+    R.run(WIG_PASS_GATHER);
+    R.run(WIG_PASS_SEAL_JOIN);
+    R.run(WIG_PASS_SEAL_ANCHOR);
+    R.run(WIG_PASS_CLASSIFY);
+    R.run(WIG_PASS_SET_FACES);
+    if (flags & WIG_STEP_VISCOUS)
+        for (int i = 0; i < 8; i++) {
+            R.run(WIG_PASS_VISCOSITY_RED);
+            R.run(WIG_PASS_VISCOSITY_BLACK);
+        }
+    R.run(WIG_PASS_UNPRESS);
+    R.run(WIG_PASS_DIVERGENCE);
+}
+
+// encodeFluid's passes after the solve (js/sim.js:2592-2611) and the report.
+void record_post(Rec& R) {
+    R.run(WIG_PASS_PROJECT);
+    R.run(WIG_PASS_EXTRAPOLATE);
+    R.run(WIG_PASS_EXTRAPOLATE_FURTHER);
+    R.run(WIG_PASS_ADVECT);
+    R.run(WIG_PASS_SORT_COUNT);
+    R.run(WIG_PASS_SCAN_BLOCKS);
+    R.run(WIG_PASS_SCAN_TOTALS);
+    R.run(WIG_PASS_SCAN_FINISH);
+    R.run(WIG_PASS_SCATTER);
+    R.run(WIG_PASS_RASTER_CLAIMS);
+    R.run(WIG_PASS_RASTER);
+    R.run(WIG_PASS_UNPAINT);
+    R.timed(WIG_SLOT_REPORT, [&] { k_report<<<1, 32, 0, R.s>>>(R.h->D, R.h->d_report); });
+}
+
+// Records the plain form's step (one kernel per reference pass, every
+// iteration encoded) on stream s; returns the number of kernels launched.
+uint32_t record_step(wig_fluid* h, uint32_t max_cycles, uint32_t flags, bool shifted, cudaStream_t s, Prof* prof) {
+    Rec R{h, s, prof};
     const bool tol = (flags & WIG_STEP_TOLERANCE) != 0u;
     if (flags & WIG_STEP_BOOKKEEPING_ONLY) {
-        run(WIG_PASS_SYNC_MARKS);
-        run(WIG_PASS_COMPACT);
-        run(WIG_PASS_RETIRE);
-    } else {
-        run(WIG_PASS_SYNC);
-        run(WIG_PASS_SYNC_PARTICLES);
-        run(WIG_PASS_SYNC_SEED);
-        run(WIG_PASS_COMPACT);
-        run(WIG_PASS_RETIRE);
-        run(WIG_PASS_CLEAR);
-        run(WIG_PASS_GATHER);
-        run(WIG_PASS_SEAL_JOIN);
-        run(WIG_PASS_SEAL_ANCHOR);
-        run(WIG_PASS_CLASSIFY);
-        run(WIG_PASS_SET_FACES);
-        if (flags & WIG_STEP_VISCOUS)
-            for (int i = 0; i < 8; i++) {
-                run(WIG_PASS_VISCOSITY_RED);
-                run(WIG_PASS_VISCOSITY_BLACK);
-            }
-        run(WIG_PASS_UNPRESS);
-        run(WIG_PASS_DIVERGENCE);
-        const uint32_t deepest = h->L.levels;
-        run(WIG_PASS_CG_START);
-        run(WIG_PASS_CG_JOIN);
-        run(WIG_PASS_CG_ANCHOR);
-        run(WIG_PASS_CG_RESIDUAL);
-        if (tol) norm(0, 0);
-        run(WIG_PASS_CG_PREPARE);
-        bool sh = shifted;
-        for (uint32_t cycle = 0; cycle < max_cycles; cycle++) {
-            run(WIG_PASS_RELAX_RIMS, 0, cycle);
-            run(sh ? WIG_PASS_RELAX_SHIFTED : WIG_PASS_RELAX, 0, cycle);
-            sh = !sh;
-            for (uint32_t l = 1; l <= deepest; l++) {
-                run(WIG_PASS_RESTRICT, l, cycle);
-                if (l < deepest) {
-                    run(WIG_PASS_SMOOTH_RED, l, cycle);
-                    run(WIG_PASS_SMOOTH_BLACK, l, cycle);
-                }
-            }
-            run(WIG_PASS_SOLVE, deepest, cycle);
-            for (uint32_t l = deepest - 1; l >= 1; l--) {
-                run(WIG_PASS_PROLONG, l, cycle);
-                run(WIG_PASS_SMOOTH_RED, l, cycle);
-                run(WIG_PASS_SMOOTH_BLACK, l, cycle);
-            }
-            run(WIG_PASS_PROLONG_FINE, 0, cycle);
-            run(WIG_PASS_RELAX_RIMS, 0, cycle);
-            run(sh ? WIG_PASS_RELAX_SHIFTED : WIG_PASS_RELAX, 0, cycle);
-            sh = !sh;
-            run(WIG_PASS_CG_RHO, 0, cycle);
-            run(WIG_PASS_CG_BETA, 0, cycle);
-            run(WIG_PASS_CG_DIRECTION, 0, cycle);
-            run(WIG_PASS_CG_APPLY, 0, cycle);
-            run(WIG_PASS_CG_ALPHA, 0, cycle);
-            run(WIG_PASS_CG_UPDATE, 0, cycle);
-            if (tol) norm(1, cycle);
-        }
-        run(WIG_PASS_CG_FINISH);
-        run(WIG_PASS_PROJECT);
-        run(WIG_PASS_EXTRAPOLATE);
-        run(WIG_PASS_EXTRAPOLATE_FURTHER);
-        run(WIG_PASS_ADVECT);
-        run(WIG_PASS_SORT_COUNT);
-        run(WIG_PASS_SCAN_BLOCKS);
-        run(WIG_PASS_SCAN_TOTALS);
-        run(WIG_PASS_SCAN_FINISH);
-        run(WIG_PASS_SCATTER);
-        run(WIG_PASS_RASTER_CLAIMS);
-        run(WIG_PASS_RASTER);
-        run(WIG_PASS_UNPAINT);
+        R.run(WIG_PASS_SYNC_MARKS);
+        R.run(WIG_PASS_COMPACT);
+        R.run(WIG_PASS_RETIRE);
+        R.timed(WIG_SLOT_REPORT, [&] { k_report<<<1, 32, 0, s>>>(h->D, h->d_report); });
+        return R.launches;
     }
-    timed(WIG_PASS_COUNT + 1, [&] { k_report<<<1, 32, 0, s>>>(D, h->d_report); });
-    return launches;
+    record_pre(R, flags);
+    const uint32_t deepest = h->L.levels;
+    R.run(WIG_PASS_CG_START);
+    R.run(WIG_PASS_CG_JOIN);
+    R.run(WIG_PASS_CG_ANCHOR);
+    R.run(WIG_PASS_CG_RESIDUAL);
+    if (tol) R.norm(0, 0);
+    R.run(WIG_PASS_CG_PREPARE);
+    bool sh = shifted;
+    for (uint32_t cycle = 0; cycle < max_cycles; cycle++) {
+        R.run(WIG_PASS_RELAX_RIMS, 0, cycle);
+        R.run(sh ? WIG_PASS_RELAX_SHIFTED : WIG_PASS_RELAX, 0, cycle);
+        sh = !sh;
+        for (uint32_t l = 1; l <= deepest; l++) {
+            R.run(WIG_PASS_RESTRICT, l, cycle);
+            if (l < deepest) {
+                R.run(WIG_PASS_SMOOTH_RED, l, cycle);
+                R.run(WIG_PASS_SMOOTH_BLACK, l, cycle);
+            }
+        }
+        R.run(WIG_PASS_SOLVE, deepest, cycle);
+        for (uint32_t l = deepest - 1; l >= 1; l--) {
+            R.run(WIG_PASS_PROLONG, l, cycle);
+            R.run(WIG_PASS_SMOOTH_RED, l, cycle);
+            R.run(WIG_PASS_SMOOTH_BLACK, l, cycle);
+        }
+        R.run(WIG_PASS_PROLONG_FINE, 0, cycle);
+        R.run(WIG_PASS_RELAX_RIMS, 0, cycle);
+        R.run(sh ? WIG_PASS_RELAX_SHIFTED : WIG_PASS_RELAX, 0, cycle);
+        sh = !sh;
+        R.run(WIG_PASS_CG_RHO, 0, cycle);
+        R.run(WIG_PASS_CG_BETA, 0, cycle);
+        R.run(WIG_PASS_CG_DIRECTION, 0, cycle);
+        R.run(WIG_PASS_CG_APPLY, 0, cycle);
+        R.run(WIG_PASS_CG_ALPHA, 0, cycle);
+        R.run(WIG_PASS_CG_UPDATE, 0, cycle);
+        if (tol) R.norm(1, cycle);
+    }
+    R.run(WIG_PASS_CG_FINISH);
+    record_post(R);
+    return R.launches;
+}
+
+wig::Fast fast_of(wig_fluid* h, uint32_t max_cycles, unsigned long long cond) {
+    wig::Fast F = h->F;
+    F.D = h->D;
+    F.max_cycles = max_cycles;
+    F.cond = cond;
+    return F;
+}
+
+// Records the fast form's step.  With `capture`, s is capturing into a graph
+// and the iterations become a WHILE node whose body is captured on h->cap2;
+// else the iterations are launched from the host, each decided by reading
+// back the device's verdict (the profiler's path).  *outside gets the kernels
+// outside the loop (all of them when not capturing), *body those of one
+// iteration of the loop.
+int record_step_fast(wig_fluid* h, uint32_t max_cycles, uint32_t flags, bool shifted, cudaStream_t s, Prof* prof,
+                     bool capture, uint32_t* outside, uint32_t* body) {
+    Rec R{h, s, prof};
+    record_pre(R, flags);
+    R.run(WIG_PASS_CG_START);
+    R.run(WIG_PASS_CG_JOIN);
+    R.run(WIG_PASS_CG_ANCHOR);
+    wig::Marker mk{&Rec::mark, &R};
+    const wig::Fast F0 = fast_of(h, max_cycles, 0ull);
+    wig::fast_setup(F0, s, prof ? &mk : nullptr);
+    R.launches++;
+    if (flags & WIG_STEP_PERSISTENT) {
+        CUDA_TRY(wig::fast_solve(F0, shifted, s, prof ? &mk : nullptr));
+        R.launches++;
+        *body = 0;
+    } else if (capture) {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t g = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        CUDA_TRY(cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd));
+        cudaGraphConditionalHandle handle;
+        CUDA_TRY(cudaGraphConditionalHandleCreate(&handle, g, 1, cudaGraphCondAssignDefault));
+        cudaGraphNodeParams cp = {};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = handle;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaGraphNode_t cnode;
+        CUDA_TRY(cudaGraphAddNode(&cnode, g, deps, nd, &cp));
+        CUDA_TRY(cudaStreamUpdateCaptureDependencies(s, &cnode, 1, cudaStreamSetCaptureDependencies));
+        cudaGraph_t bodyGraph = cp.conditional.phGraph_out[0];
+        CUDA_TRY(cudaStreamBeginCaptureToGraph(h->cap2, bodyGraph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        const wig::Fast F = fast_of(h, max_cycles, (unsigned long long)handle);
+        *body = wig::fast_cycle(F, shifted, h->cap2, nullptr);
+        cudaGraph_t captured = nullptr;
+        CUDA_TRY(cudaStreamEndCapture(h->cap2, &captured));
+    } else {
+        uint32_t* cont = &h->h_report->pad;
+        for (uint32_t c = 0; c < max_cycles; c++) {
+            R.launches += wig::fast_cycle(F0, shifted, s, prof ? &mk : nullptr);
+            CUDA_TRY(cudaMemcpyAsync(cont, &h->d_st->cont, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            CUDA_TRY(cudaStreamSynchronize(s));
+            if (!*cont) break;
+        }
+        *body = 0;
+    }
+    wig::fast_finish(F0, s, prof ? &mk : nullptr);
+    R.launches++;
+    record_post(R);
+    *outside = R.launches;
+    return WIG_OK;
 }
 
 bool step_parity(wig_fluid* h, uint32_t flags) {
@@ -379,7 +492,47 @@ int wig_fluid_create(const wig_world_desc* d, const wig_elem* elems, uint32_t n_
     D.part64 = h->d_part64;
     D.norm64 = h->d_norm64;
     if (cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking) != cudaSuccess) return cleanup(WIG_E_CUDA, "stream");
+    if (cudaStreamCreateWithFlags(&h->cap2, cudaStreamNonBlocking) != cudaSuccess) return cleanup(WIG_E_CUDA, "stream");
+    {
+        // the fast form's scratch: level 0 (17 floats and a byte a cell), the
+        // coarse levels (10 floats a cell), the block partials
+        auto align = [](size_t x) { return (x + 255u) & ~(size_t)255u; };
+        const size_t C = D.C;
+        size_t bytes = align(C) + 17u * align(C * 4u);
+        for (uint32_t l = 1; l <= D.levels; l++) bytes += 10u * align((size_t)D.level_w[l] * D.level_h[l] * 4u);
+        bytes += align(2u * (size_t)D.B * 4u) + align(2u * (size_t)D.B * 8u);
+        if (cudaMalloc(&h->fast_mem, bytes) != cudaSuccess) return cleanup(WIG_E_OOM, "cudaMalloc fast scratch");
+        cudaMemset(h->fast_mem, 0, bytes);
+        char* p = static_cast<char*>(h->fast_mem);
+        auto take = [&](size_t n) { char* q = p; p += align(n); return q; };
+        wig::Fast& F = h->F;
+        F.fmask = reinterpret_cast<uint8_t*>(take(C));
+        auto fl = [&](size_t n) { return reinterpret_cast<float*>(take(n * 4u)); };
+        for (uint32_t l = 0; l <= D.levels; l++) {
+            const size_t n = l == 0 ? C : (size_t)D.level_w[l] * D.level_h[l];
+            wig::Lvl& V = F.L[l];
+            V.px = fl(n); V.py = fl(n); V.rx = fl(n); V.ry = fl(n); V.rho = fl(n);
+            V.b0 = fl(n); V.b1 = fl(n); V.b2 = fl(n); V.b3 = fl(n); V.diag = fl(n);
+        }
+        F.pin = fl(C); F.rimx = fl(C); F.rimy = fl(C);
+        F.X = fl(C); F.R = fl(C); F.P = fl(C); F.Q = fl(C);
+        F.part32 = fl(2u * (size_t)D.B);
+        F.part64 = reinterpret_cast<double*>(take(2u * (size_t)D.B * 8u));
+        F.lc = D.levels;
+        for (uint32_t l = 1; l <= D.levels; l++)
+            if ((size_t)D.level_w[l] * D.level_h[l] <= wig::COARSE_CTA_CELLS) { F.lc = l; break; }
+        F.lp = D.levels;
+        for (uint32_t l = 1; l <= D.levels; l++)
+            if ((size_t)D.level_w[l] * D.level_h[l] <= wig::PERSISTENT_CTA_CELLS) { F.lp = l; break; }
+        F.D = D;
+        size_t smem = wig::fast_coarse_smem(F);
+        if (smem > 200u * 1024u) return cleanup(WIG_E_ARG, "coarse levels too large for one CTA");
+        if (wig::fast_prepare_attributes(smem) != cudaSuccess) return cleanup(WIG_E_CUDA, "cudaFuncSetAttribute");
+        if (wig::fast_solve_grid(F, &F.solve_grid) != cudaSuccess) return cleanup(WIG_E_CUDA, "occupancy of the persistent solve");
+        h->fast_dirty = true;
+    }
     *out = h;
+
     return WIG_OK;
 }
 
@@ -410,6 +563,7 @@ int wig_fluid_bind(wig_fluid* h, const wig_fluid_buffers* b) {
         }
     }
     h->bound = true;
+    h->fast_dirty = true;
     return WIG_OK;
 }
 
@@ -429,6 +583,7 @@ int wig_fluid_upload(wig_fluid* h, int which, const void* host, uint64_t offset,
     cudaStream_t s = (cudaStream_t)stream;
     CUDA_TRY(cudaMemcpyAsync((char*)*buffer_slot(h, which) + offset, host, bytes, cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaStreamSynchronize(s));
+    h->fast_dirty = true;
     return WIG_OK;
 }
 
@@ -467,14 +622,32 @@ int wig_fluid_step(wig_fluid* h, const wig_params* P, uint32_t max_cycles, uint3
     const bool sh = step_parity(h, flags);
     int rc = push_state(h, P, flags, tolerance, s, false);
     if (rc) return rc;
-    const uint32_t shape_flags = flags & (WIG_STEP_BOOKKEEPING_ONLY | WIG_STEP_VISCOUS | WIG_STEP_TOLERANCE | WIG_STEP_F64_DOTS);
+    const bool plain = (flags & (WIG_STEP_PLAIN | WIG_STEP_BOOKKEEPING_ONLY)) != 0u;
+    if (!plain && h->fast_dirty) {
+        wig::fast_zero_level0(fast_of(h, max_cycles, 0ull), s);
+        h->fast_dirty = false;
+    }
+    const uint32_t shape_flags =
+        flags & (WIG_STEP_BOOKKEEPING_ONLY | WIG_STEP_VISCOUS | WIG_STEP_TOLERANCE | WIG_STEP_F64_DOTS | WIG_STEP_PLAIN |
+                 WIG_STEP_PERSISTENT);
     const uint64_t key = ((uint64_t)max_cycles << 32) | ((uint64_t)shape_flags << 1) | (sh ? 1u : 0u);
     auto it = h->graphs.find(key);
     if (it == h->graphs.end()) {
         cudaGraph_t g = nullptr;
         cudaGraphExec_t ge = nullptr;
         CUDA_TRY(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
-        uint32_t n = record_step(h, max_cycles, flags, sh, h->cap, nullptr);
+        uint32_t n = 0, nb = 0;
+        if (plain) {
+            n = record_step(h, max_cycles, flags, sh, h->cap, nullptr);
+        } else {
+            int rc2 = record_step_fast(h, max_cycles, flags, sh, h->cap, nullptr, true, &n, &nb);
+            if (rc2) {
+                cudaGraph_t junk = nullptr;
+                cudaStreamEndCapture(h->cap, &junk);
+                if (junk) cudaGraphDestroy(junk);
+                return rc2;
+            }
+        }
         cudaError_t e = cudaStreamEndCapture(h->cap, &g);
         if (e != cudaSuccess) return fail(WIG_E_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
         e = cudaGraphInstantiate(&ge, g, 0);
@@ -484,8 +657,10 @@ int wig_fluid_step(wig_fluid* h, const wig_params* P, uint32_t max_cycles, uint3
         }
         it = h->graphs.emplace(key, std::make_pair(g, ge)).first;
         h->graph_launches[key] = n;
+        h->graph_body[key] = nb;
     }
     h->last_launches = h->graph_launches[key];
+    h->last_body = h->graph_body[key];
     CUDA_TRY(cudaGraphLaunch(it->second.second, s));
     if (flags & WIG_STEP_SYNC_STATS) CUDA_TRY(cudaMemcpyAsync(h->h_report, h->d_report, sizeof(Report), cudaMemcpyDeviceToHost, s));
     h->last_stream = s;
@@ -504,7 +679,20 @@ int wig_fluid_step_profile(wig_fluid* h, const wig_params* P, uint32_t max_cycle
     int rc = push_state(h, P, flags, tolerance, s, false);
     if (rc) return rc;
     Prof prof;
-    h->last_launches = record_step(h, max_cycles, flags, sh, s, &prof);
+    const bool plain = (flags & (WIG_STEP_PLAIN | WIG_STEP_BOOKKEEPING_ONLY)) != 0u;
+    h->last_body = 0;
+    if (plain) {
+        h->last_launches = record_step(h, max_cycles, flags, sh, s, &prof);
+    } else {
+        if (h->fast_dirty) {
+            wig::fast_zero_level0(fast_of(h, max_cycles, 0ull), s);
+            h->fast_dirty = false;
+        }
+        uint32_t n = 0, nb = 0;
+        rc = record_step_fast(h, max_cycles, flags, sh, s, &prof, false, &n, &nb);
+        if (rc) return rc;
+        h->last_launches = n;
+    }
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaStreamSynchronize(s));
     for (int k = 0; k < WIG_PROFILE_SLOTS; k++) { ms_out[k] = 0.0f; calls_out[k] = 0u; }
@@ -530,9 +718,10 @@ int wig_fluid_read_stats(wig_fluid* h, wig_fluid_stats* out) {
     for (uint32_t k = 0; k < WIG_FLUID_STATS; k++) out->count[k] = r.count[k];
     out->particles = r.particles;
     out->cycles = r.count[WIG_COUNT_CYCLES];
-    out->launches = h->last_launches;
+    out->launches = h->last_launches + h->last_body * r.count[WIG_COUNT_CYCLES];
     out->rel_residual = r.rel;
     out->b_norm = r.bnorm2 > 0.0 ? __builtin_sqrt(r.bnorm2) : 0.0;
+    if (r.err & wig::ERR_BARRIER) return fail(WIG_E_STATE, "the persistent solve's grid barrier waited past its limit");
     if (r.err) return fail(WIG_E_STATE, "a device loop hit its iteration limit (union-find)");
     if (r.particles > h->L.capacity) return fail(WIG_E_CAPACITY, "more particles than the buffers hold");
     return WIG_OK;
@@ -554,6 +743,8 @@ void wig_fluid_destroy(wig_fluid* h) {
     if (h->d_part64) cudaFree(h->d_part64);
     if (h->d_norm64) cudaFree(h->d_norm64);
     if (h->cap) cudaStreamDestroy(h->cap);
+    if (h->cap2) cudaStreamDestroy(h->cap2);
+    if (h->fast_mem) cudaFree(h->fast_mem);
     delete h;
 }
 

@@ -55,7 +55,10 @@ constexpr uint32_t COUNT_ACTIVE = 0, COUNT_RETIRED = 1, COUNT_VISCOUS = 2, COUNT
 // A bound on any lock-free retry loop (the union-find's): past it the
 // kernel records WIG_ERR_LOOP in the step's error word and gives up.
 constexpr uint32_t LOOP_LIMIT = 1u << 22;
-constexpr uint32_t ERR_LOOP = 1u, ERR_CAPACITY = 2u;
+constexpr uint32_t ERR_LOOP = 1u, ERR_CAPACITY = 2u, ERR_BARRIER = 4u;
+// A grid barrier's wait: at most this many polls of ~64 ns (about half a
+// second), past which the kernel records ERR_BARRIER and returns.
+constexpr uint32_t BARRIER_SPIN_LIMIT = 1u << 23;
 
 // Per-step state in device memory: the step's Params and the solve's
 // scalars (tolerance form and FP64 dots).  Written by the host before each
@@ -74,6 +77,15 @@ struct StepState {
     double pq;
     double alpha;
     double beta;
+    // the fast form's iteration count, loop decision, last-block counters and
+    // f32 scalars (fluid.wgsl's cg sums: r.z, alpha, beta, p.Ap)
+    uint32_t cycle;
+    uint32_t cont;
+    uint32_t fdone[4];
+    float rz32, pq32, alpha32, beta32;
+    // the persistent solve's grid barrier: arrivals and generation
+    uint32_t bar_count;
+    uint32_t bar_gen;
 };
 
 // The world and its buffers, passed by value to every kernel.

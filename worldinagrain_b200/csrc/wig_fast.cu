@@ -1,0 +1,1775 @@
+// wig_fast.cu — the fast form of the liquid's pressure solve (the CG loop
+// of encodeFluid, js/sim.js:2551-2591; fluid.wgsl:2047-2893).
+//
+// Same arithmetic as the reference's passes, operation for operation and in
+// the same order (so every value the step leaves is bit-for-bit the plain
+// form's), arranged for the GPU:
+//   * the stencil's coefficients (fineBeta on the cells, faceBeta on the
+//     coarse levels) are worked out once a step and kept, instead of being
+//     recomputed with their divisions in every sweep;
+//   * the vectors live in structure-of-arrays scratch (a float per cell,
+//     row-major), so a warp's loads are contiguous instead of 32-44 bytes
+//     apart as in the reference's per-cell records;
+//   * the levels of at most 4096 cells, down to the coarsest and back, are
+//     one CTA's work in shared memory, one launch instead of ~15;
+//   * the CG's block sums finish in the last block to write its partial (a
+//     threadfence reduction: the same fixed tree order, one launch fewer);
+//   * the iterations are the body of a CUDA-graph WHILE node: a step runs as
+//     many as it needs, with no launches for the converged ones.
+// The scratch keeps one invariant: level-0 arrays are zero outside the
+// blocks worked on (zeroed at allocation, when a world is uploaded, and as
+// blocks retire), where the reference's field is zero too.
+
+#include "wig_fast.cuh"
+
+namespace wig {
+namespace {
+
+__device__ __forceinline__ uint32_t vld(const uint32_t* p) { return *(const volatile uint32_t*)p; }
+__device__ __forceinline__ double vldd(const double* p) { return *(const volatile double*)p; }
+__device__ __forceinline__ float vldf(const float* p) { return *(const volatile float*)p; }
+
+#define FAST_FOR_ACTIVE(w, wid)                        \
+    const uint32_t na_ = (w).activeCount();           \
+    for (uint32_t wid = blockIdx.x; wid < na_; wid += gridDim.x)
+
+__device__ __forceinline__ I2 lidCell(const W& w, uint32_t wid) {
+    I2 b = w.activeBlock(wid);
+    return I2{b.x * BLOCK + (int)(threadIdx.x & 7u), b.y * BLOCK + (int)(threadIdx.x >> 3)};
+}
+
+// Neighbour d (left, right, up, down: beside, fluid.wgsl:267-269) of cell
+// (x, y) on a w x h level, clamped onto the cell itself past the edge (its
+// coefficient there is 0).
+__device__ __forceinline__ uint32_t nbr(uint32_t i, int x, int y, int w, int h, int d) {
+    switch (d) {
+    case 0: return x > 0 ? i - 1u : i;
+    case 1: return x < w - 1 ? i + 1u : i;
+    case 2: return y > 0 ? i - (uint32_t)w : i;
+    default: return y < h - 1 ? i + (uint32_t)w : i;
+    }
+}
+__device__ __forceinline__ bool nbrIn(int x, int y, int w, int h, int d) {
+    switch (d) {
+    case 0: return x > 0;
+    case 1: return x < w - 1;
+    case 2: return y > 0;
+    default: return y < h - 1;
+    }
+}
+
+// A 256-thread CTA's four trees of 64 (sumBlock's, fluid.wgsl:2628-2641),
+// one per tile of 64 threads; each tile's sum for all its threads.
+template <class T>
+__device__ __forceinline__ T tree64x4(T* s, T v) {
+    const int lane = (int)(threadIdx.x & 63u), base = (int)(threadIdx.x & ~63u);
+    s[threadIdx.x] = v;
+    __syncthreads();
+    for (int h = 32; h > 0; h >>= 1) {
+        if (lane < h) s[base + lane] = s[base + lane] + s[base + lane + h];
+        __syncthreads();
+    }
+    T r = s[base];
+    __syncthreads();
+    return r;
+}
+
+// sumBlocks (fluid.wgsl:2645-2661) by a 256-thread CTA, component comp of 2
+// of the active blocks' partials: thread li adds the partials of blocks li,
+// li + 256, ... in that order (loaded ahead in coalesced batches of 16, the
+// adds kept in order), then the tree over the 256.
+template <class T>
+__device__ T sumBlocks256(const W& w, const T* part, int comp, T* s) {
+    const uint32_t B = w.D.B;
+    const uint32_t* state = w.D.blocks + B;
+    const uint32_t li = threadIdx.x;
+    T acc = T(0);
+    for (uint32_t k0 = li; k0 < B; k0 += 256u * 16u) {
+        T v[16];
+        uint32_t st[16];
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            const uint32_t k = k0 + 256u * (uint32_t)u;
+            st[u] = k < B ? __ldcg(&state[k]) : 0u;
+            v[u] = k < B ? __ldcg(&part[2u * k + (uint32_t)comp]) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 16; u++)
+            if ((st[u] & ACTIVE) != 0u) acc = acc + v[u];
+    }
+    s[li] = acc;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if ((int)li < h) s[li] = s[li] + s[li + h];
+        __syncthreads();
+    }
+    T r = s[0];
+    __syncthreads();
+    return r;
+}
+
+// Whether this CTA counted the last of `total` tiles (its writers fenced
+// their partials before the barrier): a threadfence reduction's test.
+__device__ bool lastOf4(uint32_t* counter, uint32_t inc, uint32_t total) {
+    __shared__ int last;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t old = atomicAdd(counter, inc);
+        last = old + inc == total ? 1 : 0;
+        if (last) {
+            *counter = 0u;
+            __threadfence();
+        }
+    }
+    __syncthreads();
+    return last != 0;
+}
+
+__device__ __forceinline__ I2 tileCell(const W& w, uint32_t wid) {
+    I2 b = w.activeBlock(wid);
+    return I2{b.x * BLOCK + (int)(threadIdx.x & 7u), b.y * BLOCK + (int)((threadIdx.x >> 3) & 7u)};
+}
+
+// ================================================================ set-up
+
+// cgStart, cgResidual, cgPrepare (fluid.wgsl:2665-2732) into the scratch,
+// the cells' coefficients worked out (four tiles a 256-thread CTA), and the
+// blocks that dropped out this step zeroed (the invariant).
+__global__ void __launch_bounds__(256) k_fSetup(Fast F) {
+    const Dev& D = F.D;
+    W w(D);
+    __shared__ double s64[256];
+    const uint32_t na = w.activeCount(), nr = D.blocks[w.countSlot(COUNT_RETIRED)];
+    const bool tol = D.st->tol_mode != 0u;
+    const Lvl& L0 = F.L[0];
+    bool amLast = false;
+    for (uint32_t g = blockIdx.x; g * 4u < na; g += gridDim.x) {
+        const uint32_t wid = g * 4u + (threadIdx.x >> 6);
+        const bool valid = wid < na;
+        double b2 = 0.0;
+        I2 c{-1, -1};
+        if (valid) c = tileCell(w, wid);
+        if (valid && w.inWorld(c)) {
+            const uint32_t i = w.cellIndex(c);
+            const float4 gc = w.f4(2u * i), dr = w.f4(2u * i + 1u);
+            const float rho = gc.z;
+            L0.rho[i] = rho;
+            F.X[i] = gc.x;
+            F.P[i] = 0.0f;
+            F.Q[i] = 0.0f;
+            L0.px[i] = 0.0f;
+            L0.py[i] = dr.x;
+            L0.ry[i] = dr.y;
+            F.rimx[i] = 0.0f;
+            F.rimy[i] = dr.x;
+            float bb[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+            float R = 0.0f, pinv = 0.0f;
+            uint8_t mask = 0;
+            if (rho > 0.0f) {
+                const float share = w.densityAt(c);
+                float sx = 0.0f, dg = 0.0f;
+                for (int d = 0; d < 4; d++) {
+                    I2 n = beside(c, d);
+                    if (!w.inWorld(n)) continue;
+                    float4 gn = w.f4(2u * w.cellIndex(n));
+                    float r = gn.z;
+                    if (r < 0.0f) continue;
+                    float beta = fineBeta(rho, r, share, w.densityAt(n));
+                    bb[d] = beta;
+                    if (r > 0.0f) mask |= (uint8_t)(1u << d);
+                    // the stencil over the warm pressure (cgResidual runs before cgPrepare)
+                    sx = sx + beta * gn.x;
+                    dg = dg + beta;
+                }
+                pinv = (vld(w.gwp(i, G_REGION)) == i) ? PIN : 0.0f;
+                float res = gc.y - (sx - (dg + pinv) * gc.x) / 1.0f;
+                R = -res - 0.0f;
+                double bd = (double)gc.y;
+                b2 = bd * bd;
+            }
+            L0.b0[i] = bb[0]; L0.b1[i] = bb[1]; L0.b2[i] = bb[2]; L0.b3[i] = bb[3];
+            L0.diag[i] = bb[0] + bb[1] + bb[2] + bb[3];
+            F.pin[i] = pinv;
+            F.fmask[i] = mask;
+            F.R[i] = R;
+            L0.rx[i] = rho > 0.0f ? -R : 0.0f;
+        }
+        if (tol) {
+            double v = tree64x4(s64, b2);
+            if (valid && (threadIdx.x & 63u) == 0u) {
+                D.norm64[2u * w.blockIndex(w.activeBlock(wid))] = v;
+                __threadfence();
+            }
+            if (lastOf4(&D.st->fdone[0], min(4u, na - g * 4u), na)) amLast = true;
+        }
+    }
+    if (tol && amLast) {
+        double bn = sumBlocks256(w, D.norm64, 0, s64);
+        if (threadIdx.x == 0) {
+            D.st->bnorm2 = bn;
+            D.st->rel = 1.0;
+        }
+    }
+    // the blocks that dropped out: their level-0 arrays back to zero
+    for (uint32_t j = blockIdx.x * 4u + (threadIdx.x >> 6); j < nr; j += gridDim.x * 4u) {
+        uint32_t n = D.blocks[w.retiredSlot(j)];
+        I2 c{(int)(n % D.BW) * BLOCK + (int)(threadIdx.x & 7u), (int)(n / D.BW) * BLOCK + (int)((threadIdx.x >> 3) & 7u)};
+        if (w.inWorld(c)) {
+            uint32_t i = w.cellIndex(c);
+            L0.px[i] = 0.0f; L0.py[i] = 0.0f; L0.rho[i] = 0.0f;
+            F.rimx[i] = 0.0f; F.rimy[i] = 0.0f; F.P[i] = 0.0f;
+        }
+    }
+}
+
+// Zeroes the level-0 arrays the neighbours read (after an upload).
+__global__ void k_fZero(Fast F) {
+    const uint32_t C = F.D.C;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < C; i += gridDim.x * blockDim.x) {
+        F.L[0].px[i] = 0.0f; F.L[0].py[i] = 0.0f; F.L[0].rho[i] = 0.0f;
+        F.rimx[i] = 0.0f; F.rimy[i] = 0.0f; F.P[i] = 0.0f;
+    }
+}
+
+// ================================================================ relaxation
+
+__device__ I2 tileBlockF(const W& w, uint32_t wid, int shift) {
+    if (wid < w.activeCount()) return w.activeBlock(wid);
+    int wide = (int)w.D.BW, high = (int)(w.D.B / w.D.BW);
+    int j = (int)wid - (int)w.D.B;
+    if (shift == 0 || j < 0 || j > high + wide) return I2{-1, -1};
+    return j <= high ? I2{wide, j} : I2{j - high - 1, high};
+}
+
+// relaxTile (fluid.wgsl:2109-2182) over the scratch: the rim snapshot's
+// values for liquid cells, the potentials (zero) elsewhere.
+__global__ void __launch_bounds__(64) k_fRelax(Fast F, int shift) {
+    const Dev& D = F.D;
+    W w(D);
+    __shared__ float tpx[RIM * RIM], tpy[RIM * RIM];
+    __shared__ int s_live, s_ox, s_oy;
+    const Lvl& L0 = F.L[0];
+    const uint32_t na = w.activeCount();
+    const uint32_t total = na + (shift ? D.edge_tiles : 0u);
+    for (uint32_t j = blockIdx.x; j < total; j += gridDim.x) {
+        uint32_t wid = j < na ? j : D.B + (j - na);
+        if (threadIdx.x == 0) {
+            I2 b = tileBlockF(w, wid, shift);
+            int ox = b.x * BLOCK - shift, oy = b.y * BLOCK - shift;
+            uint32_t live = 0;
+            if (b.x >= 0 && ox < D.W && oy < D.H)
+                live = w.statesOf(I2{ox / BLOCK, oy / BLOCK}, I2{(ox + BLOCK - 1) / BLOCK, (oy + BLOCK - 1) / BLOCK}) & HAS_FLUID;
+            s_live = (int)live;
+            s_ox = ox;
+            s_oy = oy;
+        }
+        __syncthreads();
+        if (s_live) {
+            const int ox = s_ox, oy = s_oy;
+            for (int k = (int)threadIdx.x; k < RIM * RIM; k += 64) {
+                I2 c{ox - 1 + k % RIM, oy - 1 + k / RIM};
+                float px = 0.0f, py = 0.0f;
+                if (w.inWorld(c)) {
+                    uint32_t i = w.cellIndex(c);
+                    if (L0.rho[i] > 0.0f) {
+                        px = F.rimx[i];
+                        py = F.rimy[i];
+                    } else {
+                        px = L0.px[i];
+                        py = L0.py[i];
+                    }
+                }
+                tpx[k] = px;
+                tpy[k] = py;
+            }
+            __syncthreads();
+            const int lx = (int)(threadIdx.x & 7u), ly = (int)(threadIdx.x >> 3);
+            const I2 me{ox + lx, oy + ly};
+            const int t = (ly + 1) * RIM + lx + 1;
+            float rx = 0.0f, ry = 0.0f, bx = 0.0f, by = 0.0f, bz = 0.0f, bw = 0.0f, diag = 0.0f, pinv = 0.0f;
+            uint32_t idx = 0;
+            bool fluid = false;
+            if (w.inWorld(me)) {
+                idx = w.cellIndex(me);
+                fluid = L0.rho[idx] > 0.0f;
+            }
+            if (fluid) {
+                rx = L0.rx[idx];
+                ry = L0.ry[idx];
+                bx = L0.b0[idx];
+                by = L0.b1[idx];
+                bz = L0.b2[idx];
+                bw = L0.b3[idx];
+                diag = L0.diag[idx];
+                pinv = F.pin[idx];
+            }
+            const float dx = diag + pinv, dy = fmaxf(diag, 1e-30f);
+            const bool solving = fluid && dx > 0.0f;
+            const int color = (me.x + me.y) & 1;
+            for (int sw = 0; sw < 2 * SWEEPS; sw++) {
+                if (solving && color == (sw & 1)) {
+                    float sx = bx * tpx[t - 1] + by * tpx[t + 1] + bz * tpx[t - RIM] + bw * tpx[t + RIM];
+                    float sy = bx * tpy[t - 1] + by * tpy[t + 1] + bz * tpy[t - RIM] + bw * tpy[t + RIM];
+                    float nx = mixf(tpx[t], (sx - rx) / dx, SMOOTH_OMEGA);
+                    float ny = mixf(tpy[t], (sy - ry) / dy, SMOOTH_OMEGA);
+                    tpx[t] = nx;
+                    if (diag > 0.0f) tpy[t] = ny;
+                }
+                __syncthreads();
+            }
+            if (solving) {
+                L0.px[idx] = tpx[t];
+                L0.py[idx] = tpy[t];
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// ================================================================ the levels
+
+// residualAt (fluid.wgsl:2306-2315) of cell k on a level held in arrays with
+// stored coefficients (level 0's pinned roots held at PIN).
+__device__ __forceinline__ V2 residualStored(const Lvl& V, const float* pin, uint32_t k, int x, int y, int lw, int lh, float h2) {
+    float sx = 0.0f, sy = 0.0f;
+    const float b[4] = {V.b0[k], V.b1[k], V.b2[k], V.b3[k]};
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+        uint32_t n = nbr(k, x, y, lw, lh, d);
+        sx = sx + b[d] * V.px[n];
+        sy = sy + b[d] * V.py[n];
+    }
+    const float dg = V.diag[k];
+    const float pinx = pin ? pin[k] : 0.0f;
+    return V2{V.rx[k] - (sx - (dg + pinx) * V.px[k]) / h2, V.ry[k] - (sy - (dg + 0.0f) * V.py[k]) / h2};
+}
+
+// restrictLevel (fluid.wgsl:2342-2377) of level l from level l - 1 (both in
+// the scratch): a thread per coarse cell.
+__global__ void k_fRestrict(Fast F, uint32_t l) {
+    const Dev& D = F.D;
+    W w(D);
+    if (w.activeCount() == 0u) return;
+    const int lw = (int)D.level_w[l], lh = (int)D.level_h[l];
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= (uint32_t)(lw * lh)) return;
+    const int cx = (int)(j % (uint32_t)lw), cy = (int)(j / (uint32_t)lw);
+    const Lvl& V = F.L[l];
+    const int span = 1 << l;
+    if (span <= BLOCK) {
+        I2 b{cx * span / BLOCK, cy * span / BLOCK};
+        if (w.inBlocks(b) && (D.blocks[w.stateSlot(w.blockIndex(b))] & ACTIVE) == 0u) {
+            V.px[j] = 0.0f; V.py[j] = 0.0f; V.rx[j] = 0.0f; V.ry[j] = 0.0f; V.rho[j] = 0.0f;
+            return;
+        }
+    }
+    const Lvl& U = F.L[l - 1];
+    const int uw = (int)D.level_w[l - 1], uh = (int)D.level_h[l - 1];
+    const float h2 = (float)(1u << (2u * (l - 1u)));
+    const float* pin = l == 1u ? F.pin : nullptr;
+    float fluid = 0.0f, sum = 0.0f;
+    bool air = false;
+    float rx = 0.0f, ry = 0.0f;
+    for (int q = 0; q < 4; q++) {
+        int kx = 2 * cx + (q & 1), ky = 2 * cy + (q >> 1);
+        if (kx >= uw || ky >= uh) continue;  // rhoAt outside the level: -1
+        uint32_t k = (uint32_t)ky * (uint32_t)uw + (uint32_t)kx;
+        float rho = U.rho[k];
+        if (rho == 0.0f) air = true;
+        else if (rho > 0.0f) {
+            fluid = fluid + 1.0f;
+            sum = sum + rho;
+            V2 r = residualStored(U, pin, k, kx, ky, uw, uh, h2);
+            rx = rx + r.x;
+            ry = ry + r.y;
+        }
+    }
+    const float rho = air ? 0.0f : (fluid > 0.0f ? sum / fluid : -1.0f);
+    V.px[j] = 0.0f;
+    V.py[j] = 0.0f;
+    V.rx[j] = rho > 0.0f ? rx * 0.25f : 0.0f;
+    V.ry[j] = rho > 0.0f ? ry * 0.25f : 0.0f;
+    V.rho[j] = rho;
+}
+
+// smoothAt (fluid.wgsl:2318-2334) on level l >= 1, the coefficients worked
+// out on the step's first iteration and kept.
+__global__ void k_fSmooth(Fast F, uint32_t l, int color) {
+    const Dev& D = F.D;
+    W w(D);
+    if (w.activeCount() == 0u) return;
+    const int lw = (int)D.level_w[l], lh = (int)D.level_h[l];
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= (uint32_t)(lw * lh)) return;
+    const int cx = (int)(j % (uint32_t)lw), cy = (int)(j / (uint32_t)lw);
+    if (((cx + cy) & 1) != color) return;
+    const Lvl& V = F.L[l];
+    const float rho = V.rho[j];
+    if (rho <= 0.0f) return;
+    float b[4];
+    float dg;
+    if (D.st->cycle == 0u) {
+        dg = 0.0f;
+        for (int d = 0; d < 4; d++) {
+            b[d] = 0.0f;
+            if (!nbrIn(cx, cy, lw, lh, d)) continue;
+            float r = V.rho[nbr(j, cx, cy, lw, lh, d)];
+            if (r < 0.0f) continue;
+            b[d] = faceBeta(rho, r);
+            dg = dg + b[d];
+        }
+        V.b0[j] = b[0]; V.b1[j] = b[1]; V.b2[j] = b[2]; V.b3[j] = b[3];
+        V.diag[j] = dg;
+    } else {
+        b[0] = V.b0[j]; b[1] = V.b1[j]; b[2] = V.b2[j]; b[3] = V.b3[j];
+        dg = V.diag[j];
+    }
+    if (dg <= 0.0f) return;
+    float sx = 0.0f, sy = 0.0f;
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+        uint32_t n = nbr(j, cx, cy, lw, lh, d);
+        sx = sx + b[d] * V.px[n];
+        sy = sy + b[d] * V.py[n];
+    }
+    const float h2 = (float)(1u << (2u * l));
+    const float ex = V.px[j], ey = V.py[j];
+    V.px[j] = mixf(ex, (sx - h2 * V.rx[j]) / dg, 1.0f);
+    V.py[j] = mixf(ey, (sy - h2 * V.ry[j]) / dg, 1.0f);
+}
+
+// prolonged (fluid.wgsl:2478-2497) from level l + 1's arrays.
+__device__ __forceinline__ V2 prolongedFrom(const float* rho, const float* px, const float* py, int lw, int lh, int cx, int cy) {
+    const int kx = cx / 2, ky = cy / 2;
+    const int sx = (cx & 1) == 1 ? 1 : -1, sy = (cy & 1) == 1 ? 1 : -1;
+    const int ox[4] = {0, sx, 0, sx}, oy[4] = {0, 0, sy, sy};
+    const float wt[4] = {9.0f, 3.0f, 3.0f, 1.0f};
+    float ax = 0.0f, ay = 0.0f, weight = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        int ax_ = kx + ox[q], ay_ = ky + oy[q];
+        if (ax_ < 0 || ay_ < 0 || ax_ >= lw || ay_ >= lh) continue;
+        uint32_t k = (uint32_t)ay_ * (uint32_t)lw + (uint32_t)ax_;
+        float r = rho[k];
+        if (r < 0.0f) continue;
+        weight = weight + wt[q];
+        if (r > 0.0f) {
+            ax = ax + wt[q] * px[k];
+            ay = ay + wt[q] * py[k];
+        }
+    }
+    const float ww = fmaxf(weight, 1e-6f);
+    return V2{ax / ww, ay / ww};
+}
+
+// prolong (fluid.wgsl:2459-2470) of level l from l + 1.
+__global__ void k_fProlong(Fast F, uint32_t l) {
+    const Dev& D = F.D;
+    W w(D);
+    if (w.activeCount() == 0u) return;
+    const int lw = (int)D.level_w[l], lh = (int)D.level_h[l];
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= (uint32_t)(lw * lh)) return;
+    const Lvl& V = F.L[l];
+    if (V.rho[j] <= 0.0f) return;
+    const Lvl& U = F.L[l + 1];
+    V2 e = prolongedFrom(U.rho, U.px, U.py, (int)D.level_w[l + 1], (int)D.level_h[l + 1], (int)(j % (uint32_t)lw),
+                         (int)(j / (uint32_t)lw));
+    V.px[j] = V.px[j] + e.x;
+    V.py[j] = V.py[j] + e.y;
+}
+
+// The levels from lc down to the coarsest and back up to lc, in one CTA's
+// shared memory: restrictLevel, smoothRed/Black, solve (40 SOR sweep pairs,
+// omega 1.8), prolong (fluid.wgsl:2342-2470), the coefficients worked out
+// from the densities as the reference does.
+struct SL {
+    float *px, *py, *rx, *ry, *rho;
+    int w, h;
+};
+
+__device__ void smem_stencil(const SL& V, int j, int cx, int cy, float rho, float* sx, float* sy, float* dg) {
+    float ax = 0.0f, ay = 0.0f, d0 = 0.0f;
+    for (int d = 0; d < 4; d++) {
+        if (!nbrIn(cx, cy, V.w, V.h, d)) continue;
+        uint32_t n = nbr((uint32_t)j, cx, cy, V.w, V.h, d);
+        float r = V.rho[n];
+        if (r < 0.0f) continue;
+        float beta = faceBeta(rho, r);
+        ax = ax + beta * V.px[n];
+        ay = ay + beta * V.py[n];
+        d0 = d0 + beta;
+    }
+    *sx = ax;
+    *sy = ay;
+    *dg = d0;
+}
+
+__global__ void __launch_bounds__(1024) k_fCoarse(Fast F) {
+    extern __shared__ float sm[];
+    const Dev& D = F.D;
+    W w(D);
+    if (w.activeCount() == 0u) return;
+    const uint32_t lc = F.lc, L = D.levels;
+    SL lv[WIG_MG_LEVELS + 1];
+    {
+        float* p = sm;
+        for (uint32_t l = lc; l <= L; l++) {
+            int n = (int)(D.level_w[l] * D.level_h[l]);
+            lv[l] = SL{p, p + n, p + 2 * n, p + 3 * n, p + 4 * n, (int)D.level_w[l], (int)D.level_h[l]};
+            p += 5 * n;
+        }
+    }
+    const int tid = (int)threadIdx.x, nt = (int)blockDim.x;
+    // down
+    for (uint32_t l = lc; l <= L; l++) {
+        SL& V = lv[l];
+        const int n = V.w * V.h;
+        const int span = 1 << l;
+        const float h2u = (float)(1u << (2u * (l - 1u)));
+        for (int j = tid; j < n; j += nt) {
+            const int cx = j % V.w, cy = j / V.w;
+            if (span <= BLOCK) {
+                I2 b{cx * span / BLOCK, cy * span / BLOCK};
+                if (w.inBlocks(b) && (D.blocks[w.stateSlot(w.blockIndex(b))] & ACTIVE) == 0u) {
+                    V.px[j] = 0.0f; V.py[j] = 0.0f; V.rx[j] = 0.0f; V.ry[j] = 0.0f; V.rho[j] = 0.0f;
+                    continue;
+                }
+            }
+            float fluid = 0.0f, sum = 0.0f, rx = 0.0f, ry = 0.0f;
+            bool air = false;
+            for (int q = 0; q < 4; q++) {
+                int kx = 2 * cx + (q & 1), ky = 2 * cy + (q >> 1);
+                float rho;
+                V2 r;
+                if (l == lc) {
+                    const Lvl& U = F.L[l - 1];
+                    const int uw = (int)D.level_w[l - 1], uh = (int)D.level_h[l - 1];
+                    if (kx >= uw || ky >= uh) continue;
+                    uint32_t k = (uint32_t)ky * (uint32_t)uw + (uint32_t)kx;
+                    rho = U.rho[k];
+                    if (rho > 0.0f) r = residualStored(U, l == 1u ? F.pin : nullptr, k, kx, ky, uw, uh, h2u);
+                } else {
+                    const SL& U = lv[l - 1];
+                    if (kx >= U.w || ky >= U.h) continue;
+                    int k = ky * U.w + kx;
+                    rho = U.rho[k];
+                    if (rho > 0.0f) {
+                        float sx, sy, dg;
+                        smem_stencil(U, k, kx, ky, rho, &sx, &sy, &dg);
+                        r = V2{U.rx[k] - (sx - (dg + 0.0f) * U.px[k]) / h2u, U.ry[k] - (sy - (dg + 0.0f) * U.py[k]) / h2u};
+                    }
+                }
+                if (rho == 0.0f) air = true;
+                else if (rho > 0.0f) {
+                    fluid = fluid + 1.0f;
+                    sum = sum + rho;
+                    rx = rx + r.x;
+                    ry = ry + r.y;
+                }
+            }
+            const float rho = air ? 0.0f : (fluid > 0.0f ? sum / fluid : -1.0f);
+            V.px[j] = 0.0f;
+            V.py[j] = 0.0f;
+            V.rx[j] = rho > 0.0f ? rx * 0.25f : 0.0f;
+            V.ry[j] = rho > 0.0f ? ry * 0.25f : 0.0f;
+            V.rho[j] = rho;
+        }
+        __syncthreads();
+        if (l < L) {
+            const float h2 = (float)(1u << (2u * l));
+            for (int color = 0; color < 2; color++) {
+                for (int j = tid; j < n; j += nt) {
+                    const int cx = j % V.w, cy = j / V.w;
+                    if (((cx + cy) & 1) != color) continue;
+                    const float rho = V.rho[j];
+                    if (rho <= 0.0f) continue;
+                    float sx, sy, dg;
+                    smem_stencil(V, j, cx, cy, rho, &sx, &sy, &dg);
+                    if (dg <= 0.0f) continue;
+                    V.px[j] = mixf(V.px[j], (sx - h2 * V.rx[j]) / dg, 1.0f);
+                    V.py[j] = mixf(V.py[j], (sy - h2 * V.ry[j]) / dg, 1.0f);
+                }
+                __syncthreads();
+            }
+        }
+    }
+    // solve: the coarsest level, a cell a thread (at most 512 cells)
+    {
+        SL& V = lv[L];
+        const int n = min(V.w * V.h, (int)WIG_MG_COARSEST);
+        const float h2 = (float)(1u << (2u * L));
+        const int j = tid;
+        const int cx = j % V.w, cy = j / V.w;
+        float b[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        uint32_t nb[4] = {0u, 0u, 0u, 0u};
+        float dg = 0.0f, r0 = -1.0f;
+        if (j < n) {
+            r0 = V.rho[j];
+            for (int d = 0; d < 4; d++) {
+                nb[d] = nbr((uint32_t)j, cx, cy, V.w, V.h, d);
+                if (!nbrIn(cx, cy, V.w, V.h, d)) continue;
+                float r = V.rho[nb[d]];
+                if (r < 0.0f) continue;
+                b[d] = faceBeta(r0, r);
+                dg = dg + b[d];
+            }
+        }
+        for (int s = 0; s < 2 * COARSE_SWEEPS; s++) {
+            if (j < n && ((cx + cy) & 1) == (s & 1) && r0 > 0.0f) {
+                float sx = 0.0f, sy = 0.0f;
+                for (int d = 0; d < 4; d++) {
+                    sx = sx + b[d] * V.px[nb[d]];
+                    sy = sy + b[d] * V.py[nb[d]];
+                }
+                if (dg > 0.0f) {
+                    V.px[j] = mixf(V.px[j], (sx - h2 * V.rx[j]) / dg, OMEGA);
+                    V.py[j] = mixf(V.py[j], (sy - h2 * V.ry[j]) / dg, OMEGA);
+                }
+            }
+            __syncthreads();
+        }
+    }
+    // up
+    for (int l = (int)L - 1; l >= (int)lc; l--) {
+        SL& V = lv[l];
+        const SL& U = lv[l + 1];
+        const int n = V.w * V.h;
+        for (int j = tid; j < n; j += nt) {
+            if (V.rho[j] <= 0.0f) continue;
+            V2 e = prolongedFrom(U.rho, U.px, U.py, U.w, U.h, j % V.w, j / V.w);
+            V.px[j] = V.px[j] + e.x;
+            V.py[j] = V.py[j] + e.y;
+        }
+        __syncthreads();
+        const float h2 = (float)(1u << (2u * (uint32_t)l));
+        for (int color = 0; color < 2; color++) {
+            for (int j = tid; j < n; j += nt) {
+                const int cx = j % V.w, cy = j / V.w;
+                if (((cx + cy) & 1) != color) continue;
+                const float rho = V.rho[j];
+                if (rho <= 0.0f) continue;
+                float sx, sy, dg;
+                smem_stencil(V, j, cx, cy, rho, &sx, &sy, &dg);
+                if (dg <= 0.0f) continue;
+                V.px[j] = mixf(V.px[j], (sx - h2 * V.rx[j]) / dg, 1.0f);
+                V.py[j] = mixf(V.py[j], (sy - h2 * V.ry[j]) / dg, 1.0f);
+            }
+            __syncthreads();
+        }
+    }
+    // level lc out, for the prolongation into lc - 1
+    {
+        const SL& V = lv[lc];
+        const Lvl& G = F.L[lc];
+        const int n = V.w * V.h;
+        for (int j = tid; j < n; j += nt) {
+            G.px[j] = V.px[j];
+            G.py[j] = V.py[j];
+            G.rho[j] = V.rho[j];
+        }
+    }
+}
+
+// prolongFine (fluid.wgsl:2500-2512), and the rims for the relaxation after.
+__global__ void k_fProlongFine(Fast F) {
+    const Dev& D = F.D;
+    W w(D);
+    const Lvl& L0 = F.L[0];
+    const Lvl& U = F.L[1];
+    FAST_FOR_ACTIVE(w, wid) {
+        I2 c = lidCell(w, wid);
+        if (!w.inWorld(c)) continue;
+        uint32_t i = w.cellIndex(c);
+        if (L0.rho[i] > 0.0f) {
+            V2 e = prolongedFrom(U.rho, U.px, U.py, (int)D.level_w[1], (int)D.level_h[1], c.x, c.y);
+            float px = L0.px[i] + e.x, py = L0.py[i] + e.y;
+            L0.px[i] = px;
+            L0.py[i] = py;
+            F.rimx[i] = px;
+            F.rimy[i] = py;
+        }
+    }
+}
+
+// ================================================================ conjugate gradients
+
+// cgRho + cgBeta (fluid.wgsl:2736-2764): four tiles a 256-thread CTA; the CTA
+// that counts the last tile sums the blocks' partials (sumBlocks' order).
+__global__ void __launch_bounds__(256) k_fRhoBeta(Fast F) {
+    const Dev& D = F.D;
+    W w(D);
+    __shared__ float sx[256], sy[256];
+    __shared__ double s64[256];
+    const bool f64 = D.st->f64 != 0u;
+    const uint32_t cycle = D.st->cycle;
+    const Lvl& L0 = F.L[0];
+    const uint32_t na = w.activeCount();
+    bool amLast = false;
+    for (uint32_t g = blockIdx.x; g * 4u < na; g += gridDim.x) {
+        const uint32_t wid = g * 4u + (threadIdx.x >> 6);
+        const bool valid = wid < na;
+        float vx = 0.0f, vy = 0.0f;
+        double ex = 0.0, ey = 0.0;
+        if (valid) {
+            I2 c = tileCell(w, wid);
+            if (w.inWorld(c)) {
+                uint32_t i = w.cellIndex(c);
+                if (L0.rho[i] > 0.0f) {
+                    float z = L0.px[i];
+                    float r = F.R[i], q = F.Q[i];
+                    vx = r * z;
+                    vy = q * z;
+                    ex = (double)r * (double)z;
+                    ey = (double)q * (double)z;
+                }
+            }
+        }
+        float tx = tree64x4(sx, vx);
+        float ty = tree64x4(sy, vy);
+        double dx = 0.0, dy = 0.0;
+        if (f64) {
+            dx = tree64x4(s64, ex);
+            dy = tree64x4(s64, ey);
+        }
+        if (valid && (threadIdx.x & 63u) == 0u) {
+            const uint32_t b = w.blockIndex(w.activeBlock(wid));
+            F.part32[2u * b] = tx;
+            F.part32[2u * b + 1u] = ty;
+            if (f64) {
+                F.part64[2u * b] = dx;
+                F.part64[2u * b + 1u] = dy;
+            }
+            __threadfence();
+        }
+        if (lastOf4(&D.st->fdone[1], min(4u, na - g * 4u), na)) amLast = true;
+    }
+    if (amLast) {
+        if (f64) {
+            double rz = sumBlocks256(w, F.part64, 0, s64);
+            double zq = sumBlocks256(w, F.part64, 1, s64);
+            if (threadIdx.x == 0) {
+                double beta = (cycle == 0u || D.st->pq <= 0.0) ? 0.0 : -zq / D.st->pq;
+                D.st->rz = rz;
+                D.st->beta = beta;
+            }
+        } else {
+            float rz = sumBlocks256(w, F.part32, 0, sx);
+            float zq = sumBlocks256(w, F.part32, 1, sx);
+            if (threadIdx.x == 0) {
+                float beta = (cycle == 0u || D.st->pq32 <= 0.0f) ? 0.0f : -zq / D.st->pq32;
+                D.st->rz32 = rz;
+                D.st->beta32 = beta;
+            }
+        }
+    }
+}
+
+// cgDirection (fluid.wgsl:2767-2776)
+__global__ void k_fDirection(Fast F) {
+    const Dev& D = F.D;
+    W w(D);
+    const bool f64 = D.st->f64 != 0u;
+    const float beta = vldf(&D.st->beta32);
+    const double beta64 = vldd(&D.st->beta);
+    const Lvl& L0 = F.L[0];
+    FAST_FOR_ACTIVE(w, wid) {
+        I2 c = lidCell(w, wid);
+        if (!w.inWorld(c)) continue;
+        uint32_t i = w.cellIndex(c);
+        float p = 0.0f;
+        if (L0.rho[i] > 0.0f) {
+            float z = L0.px[i];
+            p = f64 ? (float)((double)z + beta64 * (double)F.P[i]) : z + beta * F.P[i];
+        }
+        F.P[i] = p;
+    }
+}
+
+// cgApply + cgAlpha (fluid.wgsl:2779-2814)
+__global__ void __launch_bounds__(256) k_fApplyAlpha(Fast F) {
+    const Dev& D = F.D;
+    W w(D);
+    __shared__ float sx[256];
+    __shared__ double s64[256];
+    const bool f64 = D.st->f64 != 0u;
+    const Lvl& L0 = F.L[0];
+    const uint32_t na = w.activeCount();
+    bool amLast = false;
+    for (uint32_t g = blockIdx.x; g * 4u < na; g += gridDim.x) {
+        const uint32_t wid = g * 4u + (threadIdx.x >> 6);
+        const bool valid = wid < na;
+        float vx = 0.0f;
+        double ex = 0.0;
+        if (valid) {
+            I2 c = tileCell(w, wid);
+            if (w.inWorld(c)) {
+                uint32_t i = w.cellIndex(c);
+                float q = 0.0f;
+                const float p = F.P[i];
+                if (L0.rho[i] > 0.0f) {
+                    const uint8_t m = F.fmask[i];
+                    const float b[4] = {L0.b0[i], L0.b1[i], L0.b2[i], L0.b3[i]};
+                    float sum = 0.0f;
+#pragma unroll
+                    for (int d = 0; d < 4; d++)
+                        if (m & (1u << d)) sum = sum + b[d] * F.P[nbr(i, c.x, c.y, D.W, D.H, d)];
+                    float dg = L0.diag[i] + F.pin[i];
+                    q = dg * p - sum + 0.0f;
+                }
+                F.Q[i] = q;
+                vx = p * q;
+                ex = (double)p * (double)q;
+            }
+        }
+        float tx = tree64x4(sx, vx);
+        double dx = 0.0;
+        if (f64) dx = tree64x4(s64, ex);
+        if (valid && (threadIdx.x & 63u) == 0u) {
+            const uint32_t b = w.blockIndex(w.activeBlock(wid));
+            F.part32[2u * b] = tx;
+            F.part32[2u * b + 1u] = 0.0f;
+            if (f64) {
+                F.part64[2u * b] = dx;
+                F.part64[2u * b + 1u] = 0.0;
+            }
+            __threadfence();
+        }
+        if (lastOf4(&D.st->fdone[2], min(4u, na - g * 4u), na)) amLast = true;
+    }
+    if (amLast) {
+        if (f64) {
+            double pq = sumBlocks256(w, F.part64, 0, s64);
+            if (threadIdx.x == 0) {
+                D.st->pq = pq;
+                D.st->alpha = pq <= 0.0 ? 0.0 : D.st->rz / pq;
+            }
+        } else {
+            float pq = sumBlocks256(w, F.part32, 0, sx);
+            if (threadIdx.x == 0) {
+                D.st->pq32 = pq;
+                D.st->alpha32 = pq <= 0.0f ? 0.0f : D.st->rz32 / pq;
+            }
+        }
+    }
+}
+
+// cgUpdate (fluid.wgsl:2852-2880), the tolerance form's norm, and the loop's
+// condition: the next iteration runs unless the solve has converged
+// (converged, fluid.wgsl:2223-2226) or max_cycles are done.
+__global__ void __launch_bounds__(256) k_fUpdate(Fast F) {
+    const Dev& D = F.D;
+    W w(D);
+    __shared__ uint32_t most[4];
+    __shared__ double s64[256];
+    const uint32_t cycle = D.st->cycle;
+    const bool f64 = D.st->f64 != 0u, tol = D.st->tol_mode != 0u;
+    const float alpha = vldf(&D.st->alpha32);
+    const double alpha64 = vldd(&D.st->alpha);
+    const Lvl& L0 = F.L[0];
+    const uint32_t na = w.activeCount();
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        D.blocks[w.countSlot(COUNT_RESIDUAL + (cycle + 1u) % 3u)] = 0u;
+        D.blocks[w.countSlot(COUNT_CYCLES)] += 1u;
+        if (na == 0u) {
+            D.st->cycle = cycle + 1u;
+            D.st->cont = 0u;
+            if (F.cond) cudaGraphSetConditional(F.cond, 0u);
+        }
+    }
+    bool amLast = false;
+    for (uint32_t g = blockIdx.x; g * 4u < na; g += gridDim.x) {
+        const uint32_t wid = g * 4u + (threadIdx.x >> 6);
+        const bool valid = wid < na;
+        if ((threadIdx.x & 63u) == 0u) most[threadIdx.x >> 6] = 0u;
+        __syncthreads();
+        double r2 = 0.0;
+        if (valid) {
+            I2 c = tileCell(w, wid);
+            if (w.inWorld(c)) {
+                uint32_t i = w.cellIndex(c);
+                if (L0.rho[i] > 0.0f) {
+                    float vx = F.X[i], vy = F.R[i], vz = F.P[i], vw = F.Q[i];
+                    float r, x;
+                    if (f64) {
+                        r = (float)((double)vy - alpha64 * (double)vw);
+                        x = (float)((double)vx + alpha64 * (double)vz);
+                    } else {
+                        r = vy - alpha * vw;
+                        x = vx + alpha * vz;
+                    }
+                    F.X[i] = x;
+                    F.R[i] = r;
+                    L0.px[i] = 0.0f;
+                    L0.rx[i] = -r;
+                    F.rimx[i] = 0.0f;
+                    F.rimy[i] = L0.py[i];
+                    atomicMax(&most[threadIdx.x >> 6], __float_as_uint(fabsf(r)));
+                    r2 = (double)r * (double)r;
+                }
+            }
+        }
+        double t2 = 0.0;
+        if (tol) t2 = tree64x4(s64, r2);
+        __syncthreads();
+        if (valid && (threadIdx.x & 63u) == 0u) {
+            if (tol) D.norm64[2u * w.blockIndex(w.activeBlock(wid))] = t2;
+            atomicMax(&D.blocks[w.countSlot(COUNT_RESIDUAL + cycle % 3u)], most[threadIdx.x >> 6]);
+            __threadfence();
+        }
+        if (lastOf4(&D.st->fdone[3], min(4u, na - g * 4u), na)) amLast = true;
+    }
+    if (amLast) {
+        bool conv;
+        if (tol) {
+            double rr = sumBlocks256(w, D.norm64, 0, s64);
+            double rel = D.st->bnorm2 > 0.0 ? sqrt(rr / D.st->bnorm2) : 0.0;
+            if (threadIdx.x == 0) D.st->rel = rel;
+            conv = rel <= D.st->tol;
+        } else {
+            conv = __uint_as_float(__ldcg(&D.blocks[w.countSlot(COUNT_RESIDUAL + cycle % 3u)])) < LIQUID_TOLERANCE;
+        }
+        if (threadIdx.x == 0) {
+            const uint32_t cont = (!conv && cycle + 1u < F.max_cycles) ? 1u : 0u;
+            D.st->cycle = cycle + 1u;
+            D.st->cont = cont;
+            if (F.cond) cudaGraphSetConditional(F.cond, cont);
+        }
+    }
+}
+
+// The loop's safe default: stop unless k_fUpdate decides otherwise.
+__global__ void k_fLoopStart(Fast F) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        F.D.st->cont = 0u;
+        if (F.cond) cudaGraphSetConditional(F.cond, 0u);
+    }
+}
+
+// cgFinish (fluid.wgsl:2884-2893) and the solve's values back into the
+// reference's buffers: field's pressure, divergence left (-r) and drift
+// potential, cg's (x, r, p, Ap); and the residual slots the converged
+// iterations the reference still dispatches would clear (cgUpdate's first
+// lines run whether or not the iteration is skipped).
+__global__ void k_fFinish(Fast F) {
+    const Dev& D = F.D;
+    W w(D);
+    const Lvl& L0 = F.L[0];
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (uint32_t c = D.st->cycle; c < F.max_cycles; c++) D.blocks[w.countSlot(COUNT_RESIDUAL + (c + 1u) % 3u)] = 0u;
+    }
+    FAST_FOR_ACTIVE(w, wid) {
+        I2 c = lidCell(w, wid);
+        if (!w.inWorld(c)) continue;
+        uint32_t i = w.cellIndex(c);
+        float* f = w.fv(2u * i);
+        f[0] = F.X[i];
+        if (L0.rho[i] > 0.0f) f[1] = L0.rx[i];
+        w.fv(2u * i + 1u)[0] = L0.py[i];
+        reinterpret_cast<float4*>(D.cg)[i] = make_float4(F.X[i], F.R[i], F.P[i], F.Q[i]);
+        *w.gwp(i, G_REGION) = 0u;
+    }
+}
+
+// ================================================================ the persistent solve
+//
+// All the iterations of a step's solve in one cooperative launch: each
+// reference pass of an iteration is a phase, every CTA taking its share of
+// the phase's cells or tiles, the phases separated by a grid barrier; the
+// levels of at most 1024 cells are CTA 0's, in its shared memory; the block
+// sums are finished by CTA 0 after the barrier.  Same cells, same values,
+// same order of every sum as the passes.
+
+// A grid barrier (all CTAs are resident: cooperative launch).  Each wait is
+// bounded: past BARRIER_SPIN_LIMIT polls it records ERR_BARRIER and every CTA
+// returns false from here on.
+__device__ bool gridBarrier(StepState* st, uint32_t nblocks) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        volatile uint32_t* gen = &st->bar_gen;
+        const uint32_t g0 = *gen;
+        __threadfence();
+        const uint32_t arrived = atomicAdd(&st->bar_count, 1u) + 1u;
+        int ok = 1;
+        if (arrived == nblocks) {
+            atomicExch(&st->bar_count, 0u);
+            __threadfence();
+            atomicAdd(&st->bar_gen, 1u);
+        } else {
+            uint32_t it = 0;
+            while (*gen == g0) {
+                if (++it > BARRIER_SPIN_LIMIT) {
+                    atomicOr(&st->err, ERR_BARRIER);
+                    ok = 0;
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        if ((vld(&st->err) & ERR_BARRIER) != 0u) ok = 0;
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// One coarse cell of restrictLevel (fluid.wgsl:2342-2377), level l from l - 1.
+__device__ void restrictCell(const Fast& F, const W& w, uint32_t l, uint32_t j) {
+    const Dev& D = F.D;
+    const int lw = (int)D.level_w[l];
+    const int cx = (int)(j % (uint32_t)lw), cy = (int)(j / (uint32_t)lw);
+    const Lvl& V = F.L[l];
+    const int span = 1 << l;
+    if (span <= BLOCK) {
+        I2 b{cx * span / BLOCK, cy * span / BLOCK};
+        if (w.inBlocks(b) && (D.blocks[w.stateSlot(w.blockIndex(b))] & ACTIVE) == 0u) {
+            V.px[j] = 0.0f; V.py[j] = 0.0f; V.rx[j] = 0.0f; V.ry[j] = 0.0f; V.rho[j] = 0.0f;
+            return;
+        }
+    }
+    const Lvl& U = F.L[l - 1];
+    const int uw = (int)D.level_w[l - 1], uh = (int)D.level_h[l - 1];
+    const float h2 = (float)(1u << (2u * (l - 1u)));
+    const float* pin = l == 1u ? F.pin : nullptr;
+    float fluid = 0.0f, sum = 0.0f, rx = 0.0f, ry = 0.0f;
+    bool air = false;
+    for (int q = 0; q < 4; q++) {
+        int kx = 2 * cx + (q & 1), ky = 2 * cy + (q >> 1);
+        if (kx >= uw || ky >= uh) continue;
+        uint32_t k = (uint32_t)ky * (uint32_t)uw + (uint32_t)kx;
+        float rho = U.rho[k];
+        if (rho == 0.0f) air = true;
+        else if (rho > 0.0f) {
+            fluid = fluid + 1.0f;
+            sum = sum + rho;
+            V2 r = residualStored(U, pin, k, kx, ky, uw, uh, h2);
+            rx = rx + r.x;
+            ry = ry + r.y;
+        }
+    }
+    const float rho = air ? 0.0f : (fluid > 0.0f ? sum / fluid : -1.0f);
+    V.px[j] = 0.0f;
+    V.py[j] = 0.0f;
+    V.rx[j] = rho > 0.0f ? rx * 0.25f : 0.0f;
+    V.ry[j] = rho > 0.0f ? ry * 0.25f : 0.0f;
+    V.rho[j] = rho;
+}
+
+// One cell of smoothAt (fluid.wgsl:2318-2334) on level l >= 1.
+__device__ void smoothCell(const Fast& F, uint32_t l, int color, bool first, uint32_t j) {
+    const Dev& D = F.D;
+    const int lw = (int)D.level_w[l], lh = (int)D.level_h[l];
+    const int cx = (int)(j % (uint32_t)lw), cy = (int)(j / (uint32_t)lw);
+    if (((cx + cy) & 1) != color) return;
+    const Lvl& V = F.L[l];
+    const float rho = V.rho[j];
+    if (rho <= 0.0f) return;
+    float b[4];
+    float dg;
+    if (first) {
+        dg = 0.0f;
+        for (int d = 0; d < 4; d++) {
+            b[d] = 0.0f;
+            if (!nbrIn(cx, cy, lw, lh, d)) continue;
+            float r = V.rho[nbr(j, cx, cy, lw, lh, d)];
+            if (r < 0.0f) continue;
+            b[d] = faceBeta(rho, r);
+            dg = dg + b[d];
+        }
+        V.b0[j] = b[0]; V.b1[j] = b[1]; V.b2[j] = b[2]; V.b3[j] = b[3];
+        V.diag[j] = dg;
+    } else {
+        b[0] = V.b0[j]; b[1] = V.b1[j]; b[2] = V.b2[j]; b[3] = V.b3[j];
+        dg = V.diag[j];
+    }
+    if (dg <= 0.0f) return;
+    float sx = 0.0f, sy = 0.0f;
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+        uint32_t n = nbr(j, cx, cy, lw, lh, d);
+        sx = sx + b[d] * V.px[n];
+        sy = sy + b[d] * V.py[n];
+    }
+    const float h2 = (float)(1u << (2u * l));
+    const float ex = V.px[j], ey = V.py[j];
+    V.px[j] = mixf(ex, (sx - h2 * V.rx[j]) / dg, 1.0f);
+    V.py[j] = mixf(ey, (sy - h2 * V.ry[j]) / dg, 1.0f);
+}
+
+// One cell of prolong (fluid.wgsl:2459-2470), level l from l + 1.
+__device__ void prolongCell(const Fast& F, uint32_t l, uint32_t j) {
+    const Dev& D = F.D;
+    const int lw = (int)D.level_w[l];
+    const Lvl& V = F.L[l];
+    if (V.rho[j] <= 0.0f) return;
+    const Lvl& U = F.L[l + 1];
+    V2 e = prolongedFrom(U.rho, U.px, U.py, (int)D.level_w[l + 1], (int)D.level_h[l + 1], (int)(j % (uint32_t)lw),
+                         (int)(j / (uint32_t)lw));
+    V.px[j] = V.px[j] + e.x;
+    V.py[j] = V.py[j] + e.y;
+}
+
+// The levels from lp (already restricted, in the scratch) down to the
+// coarsest and back up to lp, by one CTA in shared memory sm.
+__device__ void coarseCta(const Fast& F, const W& w, uint32_t lp, float* sm) {
+    const Dev& D = F.D;
+    const uint32_t L = D.levels;
+    const int tid = (int)threadIdx.x, nt = (int)blockDim.x;
+    SL lv[WIG_MG_LEVELS + 1];
+    {
+        float* p = sm;
+        for (uint32_t l = lp; l <= L; l++) {
+            int n = (int)(D.level_w[l] * D.level_h[l]);
+            lv[l] = SL{p, p + n, p + 2 * n, p + 3 * n, p + 4 * n, (int)D.level_w[l], (int)D.level_h[l]};
+            p += 5 * n;
+        }
+    }
+    // level lp in
+    {
+        SL& V = lv[lp];
+        const Lvl& G = F.L[lp];
+        const int n = V.w * V.h;
+        for (int j = tid; j < n; j += nt) {
+            V.px[j] = __ldcg(&G.px[j]);
+            V.py[j] = __ldcg(&G.py[j]);
+            V.rx[j] = __ldcg(&G.rx[j]);
+            V.ry[j] = __ldcg(&G.ry[j]);
+            V.rho[j] = __ldcg(&G.rho[j]);
+        }
+        __syncthreads();
+    }
+    for (uint32_t l = lp; l <= L; l++) {
+        SL& V = lv[l];
+        const int n = V.w * V.h;
+        if (l > lp) {
+            const SL& U = lv[l - 1];
+            const int span = 1 << l;
+            const float h2u = (float)(1u << (2u * (l - 1u)));
+            for (int j = tid; j < n; j += nt) {
+                const int cx = j % V.w, cy = j / V.w;
+                if (span <= BLOCK) {
+                    I2 b{cx * span / BLOCK, cy * span / BLOCK};
+                    if (w.inBlocks(b) && (D.blocks[w.stateSlot(w.blockIndex(b))] & ACTIVE) == 0u) {
+                        V.px[j] = 0.0f; V.py[j] = 0.0f; V.rx[j] = 0.0f; V.ry[j] = 0.0f; V.rho[j] = 0.0f;
+                        continue;
+                    }
+                }
+                float fluid = 0.0f, sum = 0.0f, rx = 0.0f, ry = 0.0f;
+                bool air = false;
+                for (int q = 0; q < 4; q++) {
+                    int kx = 2 * cx + (q & 1), ky = 2 * cy + (q >> 1);
+                    if (kx >= U.w || ky >= U.h) continue;
+                    int k = ky * U.w + kx;
+                    float rho = U.rho[k];
+                    if (rho == 0.0f) air = true;
+                    else if (rho > 0.0f) {
+                        float sx, sy, dg;
+                        smem_stencil(U, k, kx, ky, rho, &sx, &sy, &dg);
+                        fluid = fluid + 1.0f;
+                        sum = sum + rho;
+                        rx = rx + (U.rx[k] - (sx - (dg + 0.0f) * U.px[k]) / h2u);
+                        ry = ry + (U.ry[k] - (sy - (dg + 0.0f) * U.py[k]) / h2u);
+                    }
+                }
+                const float rho = air ? 0.0f : (fluid > 0.0f ? sum / fluid : -1.0f);
+                V.px[j] = 0.0f;
+                V.py[j] = 0.0f;
+                V.rx[j] = rho > 0.0f ? rx * 0.25f : 0.0f;
+                V.ry[j] = rho > 0.0f ? ry * 0.25f : 0.0f;
+                V.rho[j] = rho;
+            }
+            __syncthreads();
+        }
+        if (l < L) {
+            const float h2 = (float)(1u << (2u * l));
+            for (int color = 0; color < 2; color++) {
+                for (int j = tid; j < n; j += nt) {
+                    const int cx = j % V.w, cy = j / V.w;
+                    if (((cx + cy) & 1) != color) continue;
+                    const float rho = V.rho[j];
+                    if (rho <= 0.0f) continue;
+                    float sx, sy, dg;
+                    smem_stencil(V, j, cx, cy, rho, &sx, &sy, &dg);
+                    if (dg <= 0.0f) continue;
+                    V.px[j] = mixf(V.px[j], (sx - h2 * V.rx[j]) / dg, 1.0f);
+                    V.py[j] = mixf(V.py[j], (sy - h2 * V.ry[j]) / dg, 1.0f);
+                }
+                __syncthreads();
+            }
+        }
+    }
+    // solve (fluid.wgsl:2407-2456): the coarsest level's cells, several a thread
+    {
+        SL& V = lv[L];
+        const int n = min(V.w * V.h, (int)WIG_MG_COARSEST);
+        const float h2 = (float)(1u << (2u * L));
+        for (int s = 0; s < 2 * COARSE_SWEEPS; s++) {
+            for (int j = tid; j < n; j += nt) {
+                const int cx = j % V.w, cy = j / V.w;
+                const float r0 = V.rho[j];
+                if (((cx + cy) & 1) != (s & 1) || r0 <= 0.0f) continue;
+                float sx = 0.0f, sy = 0.0f, dg = 0.0f;
+                for (int d = 0; d < 4; d++) {
+                    if (!nbrIn(cx, cy, V.w, V.h, d)) continue;
+                    uint32_t nb = nbr((uint32_t)j, cx, cy, V.w, V.h, d);
+                    float r = V.rho[nb];
+                    if (r < 0.0f) continue;
+                    float beta = faceBeta(r0, r);
+                    sx = sx + beta * V.px[nb];
+                    sy = sy + beta * V.py[nb];
+                    dg = dg + beta;
+                }
+                if (dg > 0.0f) {
+                    V.px[j] = mixf(V.px[j], (sx - h2 * V.rx[j]) / dg, OMEGA);
+                    V.py[j] = mixf(V.py[j], (sy - h2 * V.ry[j]) / dg, OMEGA);
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int l = (int)L - 1; l >= (int)lp; l--) {
+        SL& V = lv[l];
+        const SL& U = lv[l + 1];
+        const int n = V.w * V.h;
+        for (int j = tid; j < n; j += nt) {
+            if (V.rho[j] <= 0.0f) continue;
+            V2 e = prolongedFrom(U.rho, U.px, U.py, U.w, U.h, j % V.w, j / V.w);
+            V.px[j] = V.px[j] + e.x;
+            V.py[j] = V.py[j] + e.y;
+        }
+        __syncthreads();
+        const float h2 = (float)(1u << (2u * (uint32_t)l));
+        for (int color = 0; color < 2; color++) {
+            for (int j = tid; j < n; j += nt) {
+                const int cx = j % V.w, cy = j / V.w;
+                if (((cx + cy) & 1) != color) continue;
+                const float rho = V.rho[j];
+                if (rho <= 0.0f) continue;
+                float sx, sy, dg;
+                smem_stencil(V, j, cx, cy, rho, &sx, &sy, &dg);
+                if (dg <= 0.0f) continue;
+                V.px[j] = mixf(V.px[j], (sx - h2 * V.rx[j]) / dg, 1.0f);
+                V.py[j] = mixf(V.py[j], (sy - h2 * V.ry[j]) / dg, 1.0f);
+            }
+            __syncthreads();
+        }
+    }
+    {
+        const SL& V = lv[lp];
+        const Lvl& G = F.L[lp];
+        const int n = V.w * V.h;
+        for (int j = tid; j < n; j += nt) {
+            G.px[j] = V.px[j];
+            G.py[j] = V.py[j];
+        }
+    }
+}
+
+// relaxTile (fluid.wgsl:2109-2182), four tiles a 256-thread CTA.
+__device__ void relaxGroups(const Fast& F, const W& w, int shift, float (*tpx)[RIM * RIM], float (*tpy)[RIM * RIM],
+                            int* s_live, int* s_ox, int* s_oy) {
+    const Dev& D = F.D;
+    const Lvl& L0 = F.L[0];
+    const uint32_t na = w.activeCount();
+    const uint32_t total = na + (shift ? D.edge_tiles : 0u);
+    const int q = (int)(threadIdx.x >> 6), lane = (int)(threadIdx.x & 63u);
+    for (uint32_t g = blockIdx.x; g * 4u < total; g += gridDim.x) {
+        const uint32_t j = g * 4u + (uint32_t)q;
+        if (lane == 0) {
+            int live = 0, ox = 0, oy = 0;
+            if (j < total) {
+                uint32_t wid = j < na ? j : D.B + (j - na);
+                I2 b = tileBlockF(w, wid, shift);
+                ox = b.x * BLOCK - shift;
+                oy = b.y * BLOCK - shift;
+                if (b.x >= 0 && ox < D.W && oy < D.H)
+                    live = (int)(w.statesOf(I2{ox / BLOCK, oy / BLOCK}, I2{(ox + BLOCK - 1) / BLOCK, (oy + BLOCK - 1) / BLOCK}) & HAS_FLUID);
+            }
+            s_live[q] = live;
+            s_ox[q] = ox;
+            s_oy[q] = oy;
+        }
+        __syncthreads();
+        const bool live = s_live[q] != 0;
+        const int ox = s_ox[q], oy = s_oy[q];
+        if (live) {
+            for (int k = lane; k < RIM * RIM; k += 64) {
+                I2 c{ox - 1 + k % RIM, oy - 1 + k / RIM};
+                float px = 0.0f, py = 0.0f;
+                if (w.inWorld(c)) {
+                    uint32_t i = w.cellIndex(c);
+                    if (__ldcg(&L0.rho[i]) > 0.0f) {
+                        px = __ldcg(&F.rimx[i]);
+                        py = __ldcg(&F.rimy[i]);
+                    } else {
+                        px = __ldcg(&L0.px[i]);
+                        py = __ldcg(&L0.py[i]);
+                    }
+                }
+                tpx[q][k] = px;
+                tpy[q][k] = py;
+            }
+        }
+        __syncthreads();
+        const int lx = lane & 7, ly = lane >> 3;
+        const I2 me{ox + lx, oy + ly};
+        const int t = (ly + 1) * RIM + lx + 1;
+        float rx = 0.0f, ry = 0.0f, bx = 0.0f, by = 0.0f, bz = 0.0f, bw = 0.0f, diag = 0.0f, pinv = 0.0f;
+        uint32_t idx = 0;
+        bool fluid = false;
+        if (live && w.inWorld(me)) {
+            idx = w.cellIndex(me);
+            fluid = __ldcg(&L0.rho[idx]) > 0.0f;
+        }
+        if (fluid) {
+            rx = __ldcg(&L0.rx[idx]);
+            ry = __ldcg(&L0.ry[idx]);
+            bx = L0.b0[idx];
+            by = L0.b1[idx];
+            bz = L0.b2[idx];
+            bw = L0.b3[idx];
+            diag = L0.diag[idx];
+            pinv = F.pin[idx];
+        }
+        const float dx = diag + pinv, dy = fmaxf(diag, 1e-30f);
+        const bool solving = fluid && dx > 0.0f;
+        const int color = (me.x + me.y) & 1;
+        for (int sw = 0; sw < 2 * SWEEPS; sw++) {
+            if (solving && color == (sw & 1)) {
+                float sx = bx * tpx[q][t - 1] + by * tpx[q][t + 1] + bz * tpx[q][t - RIM] + bw * tpx[q][t + RIM];
+                float sy = bx * tpy[q][t - 1] + by * tpy[q][t + 1] + bz * tpy[q][t - RIM] + bw * tpy[q][t + RIM];
+                float nx = mixf(tpx[q][t], (sx - rx) / dx, SMOOTH_OMEGA);
+                float ny = mixf(tpy[q][t], (sy - ry) / dy, SMOOTH_OMEGA);
+                tpx[q][t] = nx;
+                if (diag > 0.0f) tpy[q][t] = ny;
+            }
+            __syncthreads();
+        }
+        if (solving) {
+            L0.px[idx] = tpx[q][t];
+            L0.py[idx] = tpy[q][t];
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(256, 4) k_fSolve(Fast F, int shifted) {
+    extern __shared__ float sm_coarse[];
+    __shared__ float tpx[4][RIM * RIM], tpy[4][RIM * RIM];
+    __shared__ int s_live[4], s_ox[4], s_oy[4];
+    __shared__ float sx[256], sy[256];
+    __shared__ double s64[256];
+    __shared__ uint32_t most[4];
+    const Dev& D = F.D;
+    W w(D);
+    StepState* st = D.st;
+    const uint32_t nb = gridDim.x;
+    const uint32_t gt = blockIdx.x * blockDim.x + threadIdx.x, gn = gridDim.x * blockDim.x;
+    const bool f64 = st->f64 != 0u, tol = st->tol_mode != 0u;
+    const uint32_t na = w.activeCount();
+    const uint32_t lp = F.lp;
+    const Lvl& L0 = F.L[0];
+    if (na == 0u) {
+        // nothing to solve: the first iteration counted, as cgUpdate counts it
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            D.blocks[w.countSlot(COUNT_RESIDUAL + 1u)] = 0u;
+            D.blocks[w.countSlot(COUNT_CYCLES)] += 1u;
+            st->cycle = 1u;
+            st->cont = 0u;
+        }
+        return;
+    }
+    for (uint32_t cycle = 0; cycle < F.max_cycles; cycle++) {
+        // relax (relaxRims's snapshot is the scratch's rims)
+        relaxGroups(F, w, shifted ? BLOCK / 2 : 0, tpx, tpy, s_live, s_ox, s_oy);
+        if (!gridBarrier(st, nb)) return;
+        for (uint32_t l = 1; l < lp; l++) {
+            const uint32_t n = D.level_w[l] * D.level_h[l];
+            for (uint32_t j = gt; j < n; j += gn) restrictCell(F, w, l, j);
+            if (!gridBarrier(st, nb)) return;
+            for (int color = 0; color < 2; color++) {
+                for (uint32_t j = gt; j < n; j += gn) smoothCell(F, l, color, cycle == 0u, j);
+                if (!gridBarrier(st, nb)) return;
+            }
+        }
+        {
+            const uint32_t n = D.level_w[lp] * D.level_h[lp];
+            for (uint32_t j = gt; j < n; j += gn) restrictCell(F, w, lp, j);
+            if (!gridBarrier(st, nb)) return;
+        }
+        if (blockIdx.x == 0) coarseCta(F, w, lp, sm_coarse);
+        if (!gridBarrier(st, nb)) return;
+        for (uint32_t l = lp - 1; l >= 1; l--) {
+            const uint32_t n = D.level_w[l] * D.level_h[l];
+            for (uint32_t j = gt; j < n; j += gn) prolongCell(F, l, j);
+            if (!gridBarrier(st, nb)) return;
+            for (int color = 0; color < 2; color++) {
+                for (uint32_t j = gt; j < n; j += gn) smoothCell(F, l, color, false, j);
+                if (!gridBarrier(st, nb)) return;
+            }
+        }
+        // prolongFine, and the rims of the relaxation after
+        for (uint32_t t = gt; t < na * 64u; t += gn) {
+            const uint32_t wid = t >> 6, lane = t & 63u;
+            I2 b = w.activeBlock(wid);
+            I2 c{b.x * BLOCK + (int)(lane & 7u), b.y * BLOCK + (int)(lane >> 3)};
+            if (!w.inWorld(c)) continue;
+            uint32_t i = w.cellIndex(c);
+            if (L0.rho[i] > 0.0f) {
+                const Lvl& U = F.L[1];
+                V2 e = prolongedFrom(U.rho, U.px, U.py, (int)D.level_w[1], (int)D.level_h[1], c.x, c.y);
+                float px = L0.px[i] + e.x, py = L0.py[i] + e.y;
+                L0.px[i] = px;
+                L0.py[i] = py;
+                F.rimx[i] = px;
+                F.rimy[i] = py;
+            }
+        }
+        if (!gridBarrier(st, nb)) return;
+        relaxGroups(F, w, shifted ? 0 : BLOCK / 2, tpx, tpy, s_live, s_ox, s_oy);
+        if (!gridBarrier(st, nb)) return;
+        // cgRho
+        for (uint32_t g = blockIdx.x; g * 4u < na; g += gridDim.x) {
+            const uint32_t wid = g * 4u + (threadIdx.x >> 6);
+            const bool valid = wid < na;
+            float vx = 0.0f, vy = 0.0f;
+            double ex = 0.0, ey = 0.0;
+            if (valid) {
+                I2 c = tileCell(w, wid);
+                if (w.inWorld(c)) {
+                    uint32_t i = w.cellIndex(c);
+                    if (L0.rho[i] > 0.0f) {
+                        float z = L0.px[i];
+                        float r = F.R[i], q = F.Q[i];
+                        vx = r * z;
+                        vy = q * z;
+                        ex = (double)r * (double)z;
+                        ey = (double)q * (double)z;
+                    }
+                }
+            }
+            float tx = tree64x4(sx, vx);
+            float ty = tree64x4(sy, vy);
+            double dx = 0.0, dy = 0.0;
+            if (f64) {
+                dx = tree64x4(s64, ex);
+                dy = tree64x4(s64, ey);
+            }
+            if (valid && (threadIdx.x & 63u) == 0u) {
+                const uint32_t b = w.blockIndex(w.activeBlock(wid));
+                F.part32[2u * b] = tx;
+                F.part32[2u * b + 1u] = ty;
+                if (f64) {
+                    F.part64[2u * b] = dx;
+                    F.part64[2u * b + 1u] = dy;
+                }
+            }
+        }
+        if (!gridBarrier(st, nb)) return;
+        // cgBeta
+        if (blockIdx.x == 0) {
+            if (f64) {
+                double rz = sumBlocks256(w, F.part64, 0, s64);
+                double zq = sumBlocks256(w, F.part64, 1, s64);
+                if (threadIdx.x == 0) {
+                    double pq = vldd(&st->pq);
+                    st->rz = rz;
+                    st->beta = (cycle == 0u || pq <= 0.0) ? 0.0 : -zq / pq;
+                }
+            } else {
+                float rz = sumBlocks256(w, F.part32, 0, sx);
+                float zq = sumBlocks256(w, F.part32, 1, sx);
+                if (threadIdx.x == 0) {
+                    float pq = vldf(&st->pq32);
+                    st->rz32 = rz;
+                    st->beta32 = (cycle == 0u || pq <= 0.0f) ? 0.0f : -zq / pq;
+                }
+            }
+        }
+        if (!gridBarrier(st, nb)) return;
+        // cgDirection
+        {
+            const float beta = vldf(&st->beta32);
+            const double beta64 = vldd(&st->beta);
+            for (uint32_t t = gt; t < na * 64u; t += gn) {
+                const uint32_t wid = t >> 6, lane = t & 63u;
+                I2 b = w.activeBlock(wid);
+                I2 c{b.x * BLOCK + (int)(lane & 7u), b.y * BLOCK + (int)(lane >> 3)};
+                if (!w.inWorld(c)) continue;
+                uint32_t i = w.cellIndex(c);
+                float p = 0.0f;
+                if (L0.rho[i] > 0.0f) {
+                    float z = L0.px[i];
+                    p = f64 ? (float)((double)z + beta64 * (double)F.P[i]) : z + beta * F.P[i];
+                }
+                F.P[i] = p;
+            }
+        }
+        if (!gridBarrier(st, nb)) return;
+        // cgApply
+        for (uint32_t g = blockIdx.x; g * 4u < na; g += gridDim.x) {
+            const uint32_t wid = g * 4u + (threadIdx.x >> 6);
+            const bool valid = wid < na;
+            float vx = 0.0f;
+            double ex = 0.0;
+            if (valid) {
+                I2 c = tileCell(w, wid);
+                if (w.inWorld(c)) {
+                    uint32_t i = w.cellIndex(c);
+                    float q = 0.0f;
+                    const float p = __ldcg(&F.P[i]);
+                    if (L0.rho[i] > 0.0f) {
+                        const uint8_t m = F.fmask[i];
+                        const float bb[4] = {L0.b0[i], L0.b1[i], L0.b2[i], L0.b3[i]};
+                        float sum = 0.0f;
+#pragma unroll
+                        for (int d = 0; d < 4; d++)
+                            if (m & (1u << d)) sum = sum + bb[d] * __ldcg(&F.P[nbr(i, c.x, c.y, D.W, D.H, d)]);
+                        float dg = L0.diag[i] + F.pin[i];
+                        q = dg * p - sum + 0.0f;
+                    }
+                    F.Q[i] = q;
+                    vx = p * q;
+                    ex = (double)p * (double)q;
+                }
+            }
+            float tx = tree64x4(sx, vx);
+            double dx = 0.0;
+            if (f64) dx = tree64x4(s64, ex);
+            if (valid && (threadIdx.x & 63u) == 0u) {
+                const uint32_t b = w.blockIndex(w.activeBlock(wid));
+                F.part32[2u * b] = tx;
+                F.part32[2u * b + 1u] = 0.0f;
+                if (f64) {
+                    F.part64[2u * b] = dx;
+                    F.part64[2u * b + 1u] = 0.0;
+                }
+            }
+        }
+        if (!gridBarrier(st, nb)) return;
+        // cgAlpha
+        if (blockIdx.x == 0) {
+            if (f64) {
+                double pq = sumBlocks256(w, F.part64, 0, s64);
+                if (threadIdx.x == 0) {
+                    st->pq = pq;
+                    st->alpha = pq <= 0.0 ? 0.0 : vldd(&st->rz) / pq;
+                }
+            } else {
+                float pq = sumBlocks256(w, F.part32, 0, sx);
+                if (threadIdx.x == 0) {
+                    st->pq32 = pq;
+                    st->alpha32 = pq <= 0.0f ? 0.0f : vldf(&st->rz32) / pq;
+                }
+            }
+        }
+        if (!gridBarrier(st, nb)) return;
+        // cgUpdate (its first lines: the next slot cleared, the iteration counted)
+        if (blockIdx.x == 0 && threadIdx.x == 0) {
+            D.blocks[w.countSlot(COUNT_RESIDUAL + (cycle + 1u) % 3u)] = 0u;
+            D.blocks[w.countSlot(COUNT_CYCLES)] += 1u;
+        }
+        {
+            const float alpha = vldf(&st->alpha32);
+            const double alpha64 = vldd(&st->alpha);
+            for (uint32_t g = blockIdx.x; g * 4u < na; g += gridDim.x) {
+                const uint32_t wid = g * 4u + (threadIdx.x >> 6);
+                const bool valid = wid < na;
+                if ((threadIdx.x & 63u) == 0u) most[threadIdx.x >> 6] = 0u;
+                __syncthreads();
+                double r2 = 0.0;
+                if (valid) {
+                    I2 c = tileCell(w, wid);
+                    if (w.inWorld(c)) {
+                        uint32_t i = w.cellIndex(c);
+                        if (L0.rho[i] > 0.0f) {
+                            float vx = F.X[i], vy = F.R[i], vz = __ldcg(&F.P[i]), vw = __ldcg(&F.Q[i]);
+                            float r, x;
+                            if (f64) {
+                                r = (float)((double)vy - alpha64 * (double)vw);
+                                x = (float)((double)vx + alpha64 * (double)vz);
+                            } else {
+                                r = vy - alpha * vw;
+                                x = vx + alpha * vz;
+                            }
+                            F.X[i] = x;
+                            F.R[i] = r;
+                            L0.px[i] = 0.0f;
+                            L0.rx[i] = -r;
+                            F.rimx[i] = 0.0f;
+                            F.rimy[i] = __ldcg(&L0.py[i]);
+                            atomicMax(&most[threadIdx.x >> 6], __float_as_uint(fabsf(r)));
+                            r2 = (double)r * (double)r;
+                        }
+                    }
+                }
+                double t2 = 0.0;
+                if (tol) t2 = tree64x4(s64, r2);
+                __syncthreads();
+                if (valid && (threadIdx.x & 63u) == 0u) {
+                    if (tol) D.norm64[2u * w.blockIndex(w.activeBlock(wid))] = t2;
+                    atomicMax(&D.blocks[w.countSlot(COUNT_RESIDUAL + cycle % 3u)], most[threadIdx.x >> 6]);
+                }
+                __syncthreads();
+            }
+        }
+        if (!gridBarrier(st, nb)) return;
+        // converged (fluid.wgsl:2223-2226) for the next iteration
+        if (blockIdx.x == 0) {
+            bool conv;
+            if (tol) {
+                double rr = sumBlocks256(w, D.norm64, 0, s64);
+                double rel = vldd(&st->bnorm2) > 0.0 ? sqrt(rr / vldd(&st->bnorm2)) : 0.0;
+                if (threadIdx.x == 0) st->rel = rel;
+                conv = rel <= st->tol;
+            } else {
+                conv = __uint_as_float(__ldcg(&D.blocks[w.countSlot(COUNT_RESIDUAL + cycle % 3u)])) < LIQUID_TOLERANCE;
+            }
+            if (threadIdx.x == 0) {
+                st->cycle = cycle + 1u;
+                st->cont = (!conv && cycle + 1u < F.max_cycles) ? 1u : 0u;
+            }
+        }
+        if (!gridBarrier(st, nb)) return;
+        if (vld(&st->cont) == 0u) break;
+    }
+}
+
+unsigned activeGrid(const Dev& D) {
+    unsigned g = 148u * 32u;
+    return D.B < g ? (D.B ? D.B : 1u) : g;
+}
+
+// 256-thread CTAs of four tiles each
+unsigned tileGrid4(const Dev& D) {
+    unsigned n = (D.B + 3u) / 4u, g = 148u * 8u;
+    return n < g ? (n ? n : 1u) : g;
+}
+
+}  // namespace
+
+size_t fast_coarse_smem(const Fast& F) {
+    size_t n = 0;
+    for (uint32_t l = F.lc; l <= F.D.levels; l++) n += (size_t)F.D.level_w[l] * F.D.level_h[l];
+    return 5u * n * sizeof(float);
+}
+
+void fast_zero_level0(const Fast& F, cudaStream_t s) { k_fZero<<<148 * 4, 256, 0, s>>>(F); }
+
+void fast_setup(const Fast& F, cudaStream_t s, const Marker* m) {
+        if (m) m->fn(m->ctx, WIG_SLOT_F_SETUP, 0);
+    k_fSetup<<<tileGrid4(F.D), 256, 0, s>>>(F);
+    if (m) m->fn(m->ctx, WIG_SLOT_F_SETUP, 1);
+}
+
+uint32_t fast_cycle(const Fast& F, bool shifted, cudaStream_t s, const Marker* m) {
+    const Dev& D = F.D;
+    const unsigned G = activeGrid(D);
+    uint32_t launches = 0;
+    auto cells = [&](uint32_t l) { return (D.level_w[l] * D.level_h[l] + 255u) / 256u; };
+    auto mark = [&](int slot, int phase) {
+        if (m) m->fn(m->ctx, slot, phase);
+        if (phase) launches++;
+    };
+    mark(WIG_SLOT_F_LOOP, 0);
+    k_fLoopStart<<<1, 32, 0, s>>>(F);
+    mark(WIG_SLOT_F_LOOP, 1);
+    mark(WIG_SLOT_F_RELAX, 0);
+    k_fRelax<<<G, 64, 0, s>>>(F, shifted ? BLOCK / 2 : 0);
+    mark(WIG_SLOT_F_RELAX, 1);
+    for (uint32_t l = 1; l < F.lc; l++) {
+        mark(WIG_SLOT_F_RESTRICT, 0);
+        k_fRestrict<<<cells(l), 256, 0, s>>>(F, l);
+        mark(WIG_SLOT_F_RESTRICT, 1);
+        mark(WIG_SLOT_F_SMOOTH, 0);
+        k_fSmooth<<<cells(l), 256, 0, s>>>(F, l, 0);
+        mark(WIG_SLOT_F_SMOOTH, 1);
+        mark(WIG_SLOT_F_SMOOTH, 0);
+        k_fSmooth<<<cells(l), 256, 0, s>>>(F, l, 1);
+        mark(WIG_SLOT_F_SMOOTH, 1);
+    }
+    size_t smem = fast_coarse_smem(F);
+    mark(WIG_SLOT_F_COARSE, 0);
+    k_fCoarse<<<1, 1024, smem, s>>>(F);
+    mark(WIG_SLOT_F_COARSE, 1);
+    for (uint32_t l = F.lc - 1; l >= 1; l--) {
+        mark(WIG_SLOT_F_PROLONG, 0);
+        k_fProlong<<<cells(l), 256, 0, s>>>(F, l);
+        mark(WIG_SLOT_F_PROLONG, 1);
+        mark(WIG_SLOT_F_SMOOTH, 0);
+        k_fSmooth<<<cells(l), 256, 0, s>>>(F, l, 0);
+        mark(WIG_SLOT_F_SMOOTH, 1);
+        mark(WIG_SLOT_F_SMOOTH, 0);
+        k_fSmooth<<<cells(l), 256, 0, s>>>(F, l, 1);
+        mark(WIG_SLOT_F_SMOOTH, 1);
+    }
+    mark(WIG_SLOT_F_PROLONG_FINE, 0);
+    k_fProlongFine<<<G, 64, 0, s>>>(F);
+    mark(WIG_SLOT_F_PROLONG_FINE, 1);
+    mark(WIG_SLOT_F_RELAX, 0);
+    k_fRelax<<<G, 64, 0, s>>>(F, shifted ? 0 : BLOCK / 2);
+    mark(WIG_SLOT_F_RELAX, 1);
+    mark(WIG_SLOT_F_RHO_BETA, 0);
+    k_fRhoBeta<<<tileGrid4(D), 256, 0, s>>>(F);
+    mark(WIG_SLOT_F_RHO_BETA, 1);
+    mark(WIG_SLOT_F_DIRECTION, 0);
+    k_fDirection<<<G, 64, 0, s>>>(F);
+    mark(WIG_SLOT_F_DIRECTION, 1);
+    mark(WIG_SLOT_F_APPLY_ALPHA, 0);
+    k_fApplyAlpha<<<tileGrid4(D), 256, 0, s>>>(F);
+    mark(WIG_SLOT_F_APPLY_ALPHA, 1);
+    mark(WIG_SLOT_F_UPDATE, 0);
+    k_fUpdate<<<tileGrid4(D), 256, 0, s>>>(F);
+    mark(WIG_SLOT_F_UPDATE, 1);
+    return launches;
+}
+
+void fast_finish(const Fast& F, cudaStream_t s, const Marker* m) {
+    if (m) m->fn(m->ctx, WIG_SLOT_F_FINISH, 0);
+    k_fFinish<<<activeGrid(F.D), 64, 0, s>>>(F);
+    if (m) m->fn(m->ctx, WIG_SLOT_F_FINISH, 1);
+}
+
+cudaError_t fast_prepare_attributes(size_t smem) {
+    return cudaFuncSetAttribute(k_fCoarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+}
+
+size_t fast_solve_smem(const Fast& F) {
+    size_t n = 0;
+    for (uint32_t l = F.lp; l <= F.D.levels; l++) n += (size_t)F.D.level_w[l] * F.D.level_h[l];
+    return 5u * n * sizeof(float);
+}
+
+cudaError_t fast_solve_grid(const Fast& F, uint32_t* grid) {
+    int dev = 0, sms = 0, per = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_fSolve, 256, fast_solve_smem(F));
+    if (e != cudaSuccess) return e;
+    if (per < 1) return cudaErrorInvalidConfiguration;
+    *grid = (uint32_t)(sms * (per < 4 ? per : 4));
+    return cudaSuccess;
+}
+
+cudaError_t fast_solve(const Fast& F, bool shifted, cudaStream_t s, const Marker* m) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(F.solve_grid);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = fast_solve_smem(F);
+    cfg.stream = s;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (m) m->fn(m->ctx, WIG_SLOT_F_SOLVE, 0);
+    cudaError_t e = cudaLaunchKernelEx(&cfg, k_fSolve, F, shifted ? 1 : 0);
+    if (m) m->fn(m->ctx, WIG_SLOT_F_SOLVE, 1);
+    return e;
+}
+
+}  // namespace wig

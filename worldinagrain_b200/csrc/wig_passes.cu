@@ -934,8 +934,20 @@ __global__ void k_cgPrepare(Dev D) {
 // thread 0.
 __device__ double sumBlocks64(const W& w, const double* buf, int comp, double* s) {
     double acc = 0.0;
-    for (uint32_t k = threadIdx.x; k < w.D.B; k += 256u)
-        if ((w.D.blocks[w.stateSlot(k)] & ACTIVE) != 0u) acc = acc + buf[2u * k + (uint32_t)comp];
+    const uint32_t B = w.D.B;
+    for (uint32_t k0 = threadIdx.x; k0 < B; k0 += 256u * 16u) {
+        double v[16];
+        uint32_t st[16];
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            const uint32_t k = k0 + 256u * (uint32_t)u;
+            st[u] = k < B ? w.D.blocks[w.stateSlot(k)] : 0u;
+            v[u] = k < B ? buf[2u * k + (uint32_t)comp] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 16; u++)
+            if ((st[u] & ACTIVE) != 0u) acc = acc + v[u];
+    }
     s[threadIdx.x] = acc;
     __syncthreads();
     for (int h = 128; h > 0; h >>= 1) {
@@ -1236,11 +1248,24 @@ __device__ __forceinline__ void sumBlock(const W& w, uint32_t wid, float vx, flo
 // sumBlocks (fluid.wgsl:2645-2661): one CTA of 256.
 __device__ V2 sumBlocks(const W& w, float* sx, float* sy) {
     float ax = 0.0f, ay = 0.0f;
-    for (uint32_t k = threadIdx.x; k < w.D.B; k += 256u) {
-        if ((w.D.blocks[w.stateSlot(k)] & ACTIVE) != 0u) {
-            float4 p = reinterpret_cast<const float4*>(w.D.cg)[w.D.C + k];
-            ax = ax + p.x;
-            ay = ay + p.y;
+    const uint32_t B = w.D.B;
+    for (uint32_t k0 = threadIdx.x; k0 < B; k0 += 256u * 8u) {
+        float px[8], py[8];
+        uint32_t st[8];
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            const uint32_t k = k0 + 256u * (uint32_t)u;
+            st[u] = k < B ? w.D.blocks[w.stateSlot(k)] : 0u;
+            float4 p = k < B ? reinterpret_cast<const float4*>(w.D.cg)[w.D.C + k] : make_float4(0, 0, 0, 0);
+            px[u] = p.x;
+            py[u] = p.y;
+        }
+#pragma unroll
+        for (int u = 0; u < 8; u++) {
+            if ((st[u] & ACTIVE) != 0u) {
+                ax = ax + px[u];
+                ay = ay + py[u];
+            }
         }
     }
     sx[threadIdx.x] = ax;
