@@ -266,23 +266,7 @@ __global__ void __launch_bounds__(64) k_fRelax(Fast F, int shift) {
         __syncthreads();
         if (s_live) {
             const int ox = s_ox, oy = s_oy;
-            for (int k = (int)threadIdx.x; k < RIM * RIM; k += 64) {
-                I2 c{ox - 1 + k % RIM, oy - 1 + k / RIM};
-                float px = 0.0f, py = 0.0f;
-                if (w.inWorld(c)) {
-                    uint32_t i = w.cellIndex(c);
-                    if (L0.rho[i] > 0.0f) {
-                        px = F.rimx[i];
-                        py = F.rimy[i];
-                    } else {
-                        px = L0.px[i];
-                        py = L0.py[i];
-                    }
-                }
-                tpx[k] = px;
-                tpy[k] = py;
-            }
-            __syncthreads();
+            // the thread's own cell first (independent of the tile's loads)
             const int lx = (int)(threadIdx.x & 7u), ly = (int)(threadIdx.x >> 3);
             const I2 me{ox + lx, oy + ly};
             const int t = (ly + 1) * RIM + lx + 1;
@@ -292,8 +276,6 @@ __global__ void __launch_bounds__(64) k_fRelax(Fast F, int shift) {
             if (w.inWorld(me)) {
                 idx = w.cellIndex(me);
                 fluid = L0.rho[idx] > 0.0f;
-            }
-            if (fluid) {
                 rx = L0.rx[idx];
                 ry = L0.ry[idx];
                 bx = L0.b0[idx];
@@ -303,6 +285,24 @@ __global__ void __launch_bounds__(64) k_fRelax(Fast F, int shift) {
                 diag = L0.diag[idx];
                 pinv = F.pin[idx];
             }
+            if (!fluid) {
+                rx = 0.0f; ry = 0.0f; bx = 0.0f; by = 0.0f; bz = 0.0f; bw = 0.0f; diag = 0.0f; pinv = 0.0f;
+            }
+            // the tile and its rim: the snapshot's values for liquid cells,
+            // the potentials elsewhere (all five loads issued at once)
+            for (int k = (int)threadIdx.x; k < RIM * RIM; k += 64) {
+                I2 c{ox - 1 + k % RIM, oy - 1 + k / RIM};
+                float px = 0.0f, py = 0.0f;
+                if (w.inWorld(c)) {
+                    uint32_t i = w.cellIndex(c);
+                    const float r = L0.rho[i], ax = F.rimx[i], ay = F.rimy[i], qx = L0.px[i], qy = L0.py[i];
+                    px = r > 0.0f ? ax : qx;
+                    py = r > 0.0f ? ay : qy;
+                }
+                tpx[k] = px;
+                tpy[k] = py;
+            }
+            __syncthreads();
             const float dx = diag + pinv, dy = fmaxf(diag, 1e-30f);
             const bool solving = fluid && dx > 0.0f;
             const int color = (me.x + me.y) & 1;
@@ -479,16 +479,22 @@ __global__ void k_fProlong(Fast F, uint32_t l) {
     V.py[j] = V.py[j] + e.y;
 }
 
-// The levels from lc down to the coarsest and back up to lc, in one CTA's
-// shared memory: restrictLevel, smoothRed/Black, solve (40 SOR sweep pairs,
-// omega 1.8), prolong (fluid.wgsl:2342-2470), the coefficients worked out
-// from the densities as the reference does.
-struct SL {
+// Named barrier over the first `count` threads (a multiple of 32).
+__device__ __forceinline__ void barSub(uint32_t count) { asm volatile("bar.sync 1, %0;" ::"r"(count) : "memory"); }
+
+// Level l (lc <= l <= levels) of the one-CTA kernel's shared memory: five
+// arrays of the level's cells from sm + off[l].
+struct SLv {
     float *px, *py, *rx, *ry, *rho;
     int w, h;
 };
+__device__ __forceinline__ SLv slv(float* sm, const uint32_t* off, const Dev& D, uint32_t l) {
+    const int n = (int)(D.level_w[l] * D.level_h[l]);
+    float* p = sm + off[l];
+    return SLv{p, p + n, p + 2 * n, p + 3 * n, p + 4 * n, (int)D.level_w[l], (int)D.level_h[l]};
+}
 
-__device__ void smem_stencil(const SL& V, int j, int cx, int cy, float rho, float* sx, float* sy, float* dg) {
+__device__ __forceinline__ void slv_stencil(const SLv& V, int j, int cx, int cy, float rho, float* sx, float* sy, float* dg) {
     float ax = 0.0f, ay = 0.0f, d0 = 0.0f;
     for (int d = 0; d < 4; d++) {
         if (!nbrIn(cx, cy, V.w, V.h, d)) continue;
@@ -505,135 +511,162 @@ __device__ void smem_stencil(const SL& V, int j, int cx, int cy, float rho, floa
     *dg = d0;
 }
 
-__global__ void __launch_bounds__(1024) k_fCoarse(Fast F) {
-    extern __shared__ float sm[];
-    const Dev& D = F.D;
-    W w(D);
-    if (w.activeCount() == 0u) return;
-    const uint32_t lc = F.lc, L = D.levels;
-    SL lv[WIG_MG_LEVELS + 1];
-    {
-        float* p = sm;
-        for (uint32_t l = lc; l <= L; l++) {
-            int n = (int)(D.level_w[l] * D.level_h[l]);
-            lv[l] = SL{p, p + n, p + 2 * n, p + 3 * n, p + 4 * n, (int)D.level_w[l], (int)D.level_h[l]};
-            p += 5 * n;
-        }
-    }
-    const int tid = (int)threadIdx.x, nt = (int)blockDim.x;
-    // down
-    for (uint32_t l = lc; l <= L; l++) {
-        SL& V = lv[l];
-        const int n = V.w * V.h;
-        const int span = 1 << l;
-        const float h2u = (float)(1u << (2u * (l - 1u)));
+__device__ void slv_smooth(const SLv& V, uint32_t l, int tid, int nt) {
+    const int n = V.w * V.h;
+    const float h2 = (float)(1u << (2u * l));
+    for (int color = 0; color < 2; color++) {
         for (int j = tid; j < n; j += nt) {
             const int cx = j % V.w, cy = j / V.w;
-            if (span <= BLOCK) {
-                I2 b{cx * span / BLOCK, cy * span / BLOCK};
-                if (w.inBlocks(b) && (D.blocks[w.stateSlot(w.blockIndex(b))] & ACTIVE) == 0u) {
-                    V.px[j] = 0.0f; V.py[j] = 0.0f; V.rx[j] = 0.0f; V.ry[j] = 0.0f; V.rho[j] = 0.0f;
-                    continue;
-                }
-            }
-            float fluid = 0.0f, sum = 0.0f, rx = 0.0f, ry = 0.0f;
-            bool air = false;
-            for (int q = 0; q < 4; q++) {
-                int kx = 2 * cx + (q & 1), ky = 2 * cy + (q >> 1);
-                float rho;
-                V2 r;
-                if (l == lc) {
-                    const Lvl& U = F.L[l - 1];
-                    const int uw = (int)D.level_w[l - 1], uh = (int)D.level_h[l - 1];
-                    if (kx >= uw || ky >= uh) continue;
-                    uint32_t k = (uint32_t)ky * (uint32_t)uw + (uint32_t)kx;
-                    rho = U.rho[k];
-                    if (rho > 0.0f) r = residualStored(U, l == 1u ? F.pin : nullptr, k, kx, ky, uw, uh, h2u);
-                } else {
-                    const SL& U = lv[l - 1];
-                    if (kx >= U.w || ky >= U.h) continue;
-                    int k = ky * U.w + kx;
-                    rho = U.rho[k];
-                    if (rho > 0.0f) {
-                        float sx, sy, dg;
-                        smem_stencil(U, k, kx, ky, rho, &sx, &sy, &dg);
-                        r = V2{U.rx[k] - (sx - (dg + 0.0f) * U.px[k]) / h2u, U.ry[k] - (sy - (dg + 0.0f) * U.py[k]) / h2u};
-                    }
-                }
-                if (rho == 0.0f) air = true;
-                else if (rho > 0.0f) {
-                    fluid = fluid + 1.0f;
-                    sum = sum + rho;
-                    rx = rx + r.x;
-                    ry = ry + r.y;
-                }
-            }
-            const float rho = air ? 0.0f : (fluid > 0.0f ? sum / fluid : -1.0f);
-            V.px[j] = 0.0f;
-            V.py[j] = 0.0f;
-            V.rx[j] = rho > 0.0f ? rx * 0.25f : 0.0f;
-            V.ry[j] = rho > 0.0f ? ry * 0.25f : 0.0f;
-            V.rho[j] = rho;
+            if (((cx + cy) & 1) != color) continue;
+            const float rho = V.rho[j];
+            if (rho <= 0.0f) continue;
+            float sx, sy, dg;
+            slv_stencil(V, j, cx, cy, rho, &sx, &sy, &dg);
+            if (dg <= 0.0f) continue;
+            V.px[j] = mixf(V.px[j], (sx - h2 * V.rx[j]) / dg, 1.0f);
+            V.py[j] = mixf(V.py[j], (sy - h2 * V.ry[j]) / dg, 1.0f);
         }
         __syncthreads();
-        if (l < L) {
-            const float h2 = (float)(1u << (2u * l));
-            for (int color = 0; color < 2; color++) {
+    }
+}
+
+// The levels lc (restricted already, in the scratch) down to the coarsest and
+// back up to lc, in one CTA's shared memory: smoothRed/Black, restrictLevel,
+// solve (40 SOR sweep pairs, omega 1.8), prolong (fluid.wgsl:2318-2470).
+__device__ void coarseLevels(const Fast& F, const W& w, uint32_t lc, float* sm, uint32_t* off) {
+    const Dev& D = F.D;
+    const uint32_t L = D.levels;
+    const int tid = (int)threadIdx.x, nt = (int)blockDim.x;
+    if (tid == 0) {
+        uint32_t o = 0;
+        for (uint32_t l = lc; l <= L; l++) {
+            off[l] = o;
+            o += 5u * D.level_w[l] * D.level_h[l];
+        }
+    }
+    __syncthreads();
+    {
+        const SLv V = slv(sm, off, D, lc);
+        const Lvl& G = F.L[lc];
+        const int n = V.w * V.h;
+        for (int j = tid; j < n; j += nt) {
+            V.px[j] = G.px[j];
+            V.py[j] = G.py[j];
+            V.rx[j] = G.rx[j];
+            V.ry[j] = G.ry[j];
+            V.rho[j] = G.rho[j];
+        }
+        __syncthreads();
+    }
+    for (uint32_t l = lc; l <= L; l++) {
+        const SLv V = slv(sm, off, D, l);
+        const int n = V.w * V.h;
+        if (l > lc) {
+            const SLv U = slv(sm, off, D, l - 1u);
+            const int span = 1 << l;
+            const float h2u = (float)(1u << (2u * (l - 1u)));
+            for (int j = tid; j < n; j += nt) {
+                const int cx = j % V.w, cy = j / V.w;
+                if (span <= BLOCK) {
+                    I2 b{cx * span / BLOCK, cy * span / BLOCK};
+                    if (w.inBlocks(b) && (D.blocks[w.stateSlot(w.blockIndex(b))] & ACTIVE) == 0u) {
+                        V.px[j] = 0.0f; V.py[j] = 0.0f; V.rx[j] = 0.0f; V.ry[j] = 0.0f; V.rho[j] = 0.0f;
+                        continue;
+                    }
+                }
+                float fluid = 0.0f, sum = 0.0f, rx = 0.0f, ry = 0.0f;
+                bool air = false;
+                for (int q = 0; q < 4; q++) {
+                    int kx = 2 * cx + (q & 1), ky = 2 * cy + (q >> 1);
+                    if (kx >= U.w || ky >= U.h) continue;
+                    int k = ky * U.w + kx;
+                    float rho = U.rho[k];
+                    if (rho == 0.0f) air = true;
+                    else if (rho > 0.0f) {
+                        float sx, sy, dg;
+                        slv_stencil(U, k, kx, ky, rho, &sx, &sy, &dg);
+                        fluid = fluid + 1.0f;
+                        sum = sum + rho;
+                        rx = rx + (U.rx[k] - (sx - (dg + 0.0f) * U.px[k]) / h2u);
+                        ry = ry + (U.ry[k] - (sy - (dg + 0.0f) * U.py[k]) / h2u);
+                    }
+                }
+                const float rho = air ? 0.0f : (fluid > 0.0f ? sum / fluid : -1.0f);
+                V.px[j] = 0.0f;
+                V.py[j] = 0.0f;
+                V.rx[j] = rho > 0.0f ? rx * 0.25f : 0.0f;
+                V.ry[j] = rho > 0.0f ? ry * 0.25f : 0.0f;
+                V.rho[j] = rho;
+            }
+            __syncthreads();
+        }
+        if (l < L) slv_smooth(V, l, tid, nt);
+    }
+    // solve: the coarsest level.  When its cells fit the CTA, a cell a thread
+    // of the first warps, the coefficients held in registers across the
+    // sweeps and only those warps synchronised (a named barrier over nsolve
+    // <= blockDim threads); else several cells a thread, the CTA
+    // synchronised.
+    {
+        const SLv V = slv(sm, off, D, L);
+        const int n = min(V.w * V.h, (int)WIG_MG_COARSEST);
+        const float h2 = (float)(1u << (2u * L));
+        const uint32_t nsolve = (uint32_t)((n + 31) & ~31);
+        if (nsolve <= (uint32_t)nt) {
+            if (tid < (int)nsolve) {
+                const int j = tid;
+                const int cx = j % V.w, cy = j / V.w;
+                float b[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+                uint32_t nb[4] = {0u, 0u, 0u, 0u};
+                float dg = 0.0f, r0 = -1.0f, hx = 0.0f, hy = 0.0f;
+                if (j < n) {
+                    r0 = V.rho[j];
+                    hx = h2 * V.rx[j];
+                    hy = h2 * V.ry[j];
+                    for (int d = 0; d < 4; d++) {
+                        nb[d] = nbr((uint32_t)j, cx, cy, V.w, V.h, d);
+                        if (!nbrIn(cx, cy, V.w, V.h, d)) continue;
+                        float r = V.rho[nb[d]];
+                        if (r < 0.0f) continue;
+                        b[d] = faceBeta(r0, r);
+                        dg = dg + b[d];
+                    }
+                }
+                const bool mine = j < n && r0 > 0.0f && dg > 0.0f;
+                const int color = (cx + cy) & 1;
+                float* px = V.px;
+                float* py = V.py;
+                for (int s = 0; s < 2 * COARSE_SWEEPS; s++) {
+                    if (mine && color == (s & 1)) {
+                        float sx = b[0] * px[nb[0]] + b[1] * px[nb[1]] + b[2] * px[nb[2]] + b[3] * px[nb[3]];
+                        float sy = b[0] * py[nb[0]] + b[1] * py[nb[1]] + b[2] * py[nb[2]] + b[3] * py[nb[3]];
+                        px[j] = mixf(px[j], (sx - hx) / dg, OMEGA);
+                        py[j] = mixf(py[j], (sy - hy) / dg, OMEGA);
+                    }
+                    barSub(nsolve);
+                }
+            }
+        } else {
+            for (int s = 0; s < 2 * COARSE_SWEEPS; s++) {
                 for (int j = tid; j < n; j += nt) {
                     const int cx = j % V.w, cy = j / V.w;
-                    if (((cx + cy) & 1) != color) continue;
-                    const float rho = V.rho[j];
-                    if (rho <= 0.0f) continue;
+                    const float r0 = V.rho[j];
+                    if (((cx + cy) & 1) != (s & 1) || r0 <= 0.0f) continue;
                     float sx, sy, dg;
-                    smem_stencil(V, j, cx, cy, rho, &sx, &sy, &dg);
-                    if (dg <= 0.0f) continue;
-                    V.px[j] = mixf(V.px[j], (sx - h2 * V.rx[j]) / dg, 1.0f);
-                    V.py[j] = mixf(V.py[j], (sy - h2 * V.ry[j]) / dg, 1.0f);
+                    slv_stencil(V, j, cx, cy, r0, &sx, &sy, &dg);
+                    if (dg > 0.0f) {
+                        V.px[j] = mixf(V.px[j], (sx - h2 * V.rx[j]) / dg, OMEGA);
+                        V.py[j] = mixf(V.py[j], (sy - h2 * V.ry[j]) / dg, OMEGA);
+                    }
                 }
                 __syncthreads();
             }
         }
+        __syncthreads();
     }
-    // solve: the coarsest level, a cell a thread (at most 512 cells)
-    {
-        SL& V = lv[L];
-        const int n = min(V.w * V.h, (int)WIG_MG_COARSEST);
-        const float h2 = (float)(1u << (2u * L));
-        const int j = tid;
-        const int cx = j % V.w, cy = j / V.w;
-        float b[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-        uint32_t nb[4] = {0u, 0u, 0u, 0u};
-        float dg = 0.0f, r0 = -1.0f;
-        if (j < n) {
-            r0 = V.rho[j];
-            for (int d = 0; d < 4; d++) {
-                nb[d] = nbr((uint32_t)j, cx, cy, V.w, V.h, d);
-                if (!nbrIn(cx, cy, V.w, V.h, d)) continue;
-                float r = V.rho[nb[d]];
-                if (r < 0.0f) continue;
-                b[d] = faceBeta(r0, r);
-                dg = dg + b[d];
-            }
-        }
-        for (int s = 0; s < 2 * COARSE_SWEEPS; s++) {
-            if (j < n && ((cx + cy) & 1) == (s & 1) && r0 > 0.0f) {
-                float sx = 0.0f, sy = 0.0f;
-                for (int d = 0; d < 4; d++) {
-                    sx = sx + b[d] * V.px[nb[d]];
-                    sy = sy + b[d] * V.py[nb[d]];
-                }
-                if (dg > 0.0f) {
-                    V.px[j] = mixf(V.px[j], (sx - h2 * V.rx[j]) / dg, OMEGA);
-                    V.py[j] = mixf(V.py[j], (sy - h2 * V.ry[j]) / dg, OMEGA);
-                }
-            }
-            __syncthreads();
-        }
-    }
-    // up
     for (int l = (int)L - 1; l >= (int)lc; l--) {
-        SL& V = lv[l];
-        const SL& U = lv[l + 1];
+        const SLv V = slv(sm, off, D, (uint32_t)l);
+        const SLv U = slv(sm, off, D, (uint32_t)l + 1u);
         const int n = V.w * V.h;
         for (int j = tid; j < n; j += nt) {
             if (V.rho[j] <= 0.0f) continue;
@@ -642,33 +675,25 @@ __global__ void __launch_bounds__(1024) k_fCoarse(Fast F) {
             V.py[j] = V.py[j] + e.y;
         }
         __syncthreads();
-        const float h2 = (float)(1u << (2u * (uint32_t)l));
-        for (int color = 0; color < 2; color++) {
-            for (int j = tid; j < n; j += nt) {
-                const int cx = j % V.w, cy = j / V.w;
-                if (((cx + cy) & 1) != color) continue;
-                const float rho = V.rho[j];
-                if (rho <= 0.0f) continue;
-                float sx, sy, dg;
-                smem_stencil(V, j, cx, cy, rho, &sx, &sy, &dg);
-                if (dg <= 0.0f) continue;
-                V.px[j] = mixf(V.px[j], (sx - h2 * V.rx[j]) / dg, 1.0f);
-                V.py[j] = mixf(V.py[j], (sy - h2 * V.ry[j]) / dg, 1.0f);
-            }
-            __syncthreads();
-        }
+        slv_smooth(V, (uint32_t)l, tid, nt);
     }
-    // level lc out, for the prolongation into lc - 1
     {
-        const SL& V = lv[lc];
+        const SLv V = slv(sm, off, D, lc);
         const Lvl& G = F.L[lc];
         const int n = V.w * V.h;
         for (int j = tid; j < n; j += nt) {
             G.px[j] = V.px[j];
             G.py[j] = V.py[j];
-            G.rho[j] = V.rho[j];
         }
     }
+}
+
+__global__ void __launch_bounds__(1024) k_fCoarse(Fast F) {
+    extern __shared__ float sm[];
+    __shared__ uint32_t off[WIG_MG_LEVELS + 1];
+    W w(F.D);
+    if (w.activeCount() == 0u) return;
+    coarseLevels(F, w, F.lc, sm, off);
 }
 
 // prolongFine (fluid.wgsl:2500-2512), and the rims for the relaxation after.
@@ -1111,162 +1136,6 @@ __device__ void prolongCell(const Fast& F, uint32_t l, uint32_t j) {
     V.py[j] = V.py[j] + e.y;
 }
 
-// The levels from lp (already restricted, in the scratch) down to the
-// coarsest and back up to lp, by one CTA in shared memory sm.
-__device__ void coarseCta(const Fast& F, const W& w, uint32_t lp, float* sm) {
-    const Dev& D = F.D;
-    const uint32_t L = D.levels;
-    const int tid = (int)threadIdx.x, nt = (int)blockDim.x;
-    SL lv[WIG_MG_LEVELS + 1];
-    {
-        float* p = sm;
-        for (uint32_t l = lp; l <= L; l++) {
-            int n = (int)(D.level_w[l] * D.level_h[l]);
-            lv[l] = SL{p, p + n, p + 2 * n, p + 3 * n, p + 4 * n, (int)D.level_w[l], (int)D.level_h[l]};
-            p += 5 * n;
-        }
-    }
-    // level lp in
-    {
-        SL& V = lv[lp];
-        const Lvl& G = F.L[lp];
-        const int n = V.w * V.h;
-        for (int j = tid; j < n; j += nt) {
-            V.px[j] = __ldcg(&G.px[j]);
-            V.py[j] = __ldcg(&G.py[j]);
-            V.rx[j] = __ldcg(&G.rx[j]);
-            V.ry[j] = __ldcg(&G.ry[j]);
-            V.rho[j] = __ldcg(&G.rho[j]);
-        }
-        __syncthreads();
-    }
-    for (uint32_t l = lp; l <= L; l++) {
-        SL& V = lv[l];
-        const int n = V.w * V.h;
-        if (l > lp) {
-            const SL& U = lv[l - 1];
-            const int span = 1 << l;
-            const float h2u = (float)(1u << (2u * (l - 1u)));
-            for (int j = tid; j < n; j += nt) {
-                const int cx = j % V.w, cy = j / V.w;
-                if (span <= BLOCK) {
-                    I2 b{cx * span / BLOCK, cy * span / BLOCK};
-                    if (w.inBlocks(b) && (D.blocks[w.stateSlot(w.blockIndex(b))] & ACTIVE) == 0u) {
-                        V.px[j] = 0.0f; V.py[j] = 0.0f; V.rx[j] = 0.0f; V.ry[j] = 0.0f; V.rho[j] = 0.0f;
-                        continue;
-                    }
-                }
-                float fluid = 0.0f, sum = 0.0f, rx = 0.0f, ry = 0.0f;
-                bool air = false;
-                for (int q = 0; q < 4; q++) {
-                    int kx = 2 * cx + (q & 1), ky = 2 * cy + (q >> 1);
-                    if (kx >= U.w || ky >= U.h) continue;
-                    int k = ky * U.w + kx;
-                    float rho = U.rho[k];
-                    if (rho == 0.0f) air = true;
-                    else if (rho > 0.0f) {
-                        float sx, sy, dg;
-                        smem_stencil(U, k, kx, ky, rho, &sx, &sy, &dg);
-                        fluid = fluid + 1.0f;
-                        sum = sum + rho;
-                        rx = rx + (U.rx[k] - (sx - (dg + 0.0f) * U.px[k]) / h2u);
-                        ry = ry + (U.ry[k] - (sy - (dg + 0.0f) * U.py[k]) / h2u);
-                    }
-                }
-                const float rho = air ? 0.0f : (fluid > 0.0f ? sum / fluid : -1.0f);
-                V.px[j] = 0.0f;
-                V.py[j] = 0.0f;
-                V.rx[j] = rho > 0.0f ? rx * 0.25f : 0.0f;
-                V.ry[j] = rho > 0.0f ? ry * 0.25f : 0.0f;
-                V.rho[j] = rho;
-            }
-            __syncthreads();
-        }
-        if (l < L) {
-            const float h2 = (float)(1u << (2u * l));
-            for (int color = 0; color < 2; color++) {
-                for (int j = tid; j < n; j += nt) {
-                    const int cx = j % V.w, cy = j / V.w;
-                    if (((cx + cy) & 1) != color) continue;
-                    const float rho = V.rho[j];
-                    if (rho <= 0.0f) continue;
-                    float sx, sy, dg;
-                    smem_stencil(V, j, cx, cy, rho, &sx, &sy, &dg);
-                    if (dg <= 0.0f) continue;
-                    V.px[j] = mixf(V.px[j], (sx - h2 * V.rx[j]) / dg, 1.0f);
-                    V.py[j] = mixf(V.py[j], (sy - h2 * V.ry[j]) / dg, 1.0f);
-                }
-                __syncthreads();
-            }
-        }
-    }
-    // solve (fluid.wgsl:2407-2456): the coarsest level's cells, several a thread
-    {
-        SL& V = lv[L];
-        const int n = min(V.w * V.h, (int)WIG_MG_COARSEST);
-        const float h2 = (float)(1u << (2u * L));
-        for (int s = 0; s < 2 * COARSE_SWEEPS; s++) {
-            for (int j = tid; j < n; j += nt) {
-                const int cx = j % V.w, cy = j / V.w;
-                const float r0 = V.rho[j];
-                if (((cx + cy) & 1) != (s & 1) || r0 <= 0.0f) continue;
-                float sx = 0.0f, sy = 0.0f, dg = 0.0f;
-                for (int d = 0; d < 4; d++) {
-                    if (!nbrIn(cx, cy, V.w, V.h, d)) continue;
-                    uint32_t nb = nbr((uint32_t)j, cx, cy, V.w, V.h, d);
-                    float r = V.rho[nb];
-                    if (r < 0.0f) continue;
-                    float beta = faceBeta(r0, r);
-                    sx = sx + beta * V.px[nb];
-                    sy = sy + beta * V.py[nb];
-                    dg = dg + beta;
-                }
-                if (dg > 0.0f) {
-                    V.px[j] = mixf(V.px[j], (sx - h2 * V.rx[j]) / dg, OMEGA);
-                    V.py[j] = mixf(V.py[j], (sy - h2 * V.ry[j]) / dg, OMEGA);
-                }
-            }
-            __syncthreads();
-        }
-    }
-    for (int l = (int)L - 1; l >= (int)lp; l--) {
-        SL& V = lv[l];
-        const SL& U = lv[l + 1];
-        const int n = V.w * V.h;
-        for (int j = tid; j < n; j += nt) {
-            if (V.rho[j] <= 0.0f) continue;
-            V2 e = prolongedFrom(U.rho, U.px, U.py, U.w, U.h, j % V.w, j / V.w);
-            V.px[j] = V.px[j] + e.x;
-            V.py[j] = V.py[j] + e.y;
-        }
-        __syncthreads();
-        const float h2 = (float)(1u << (2u * (uint32_t)l));
-        for (int color = 0; color < 2; color++) {
-            for (int j = tid; j < n; j += nt) {
-                const int cx = j % V.w, cy = j / V.w;
-                if (((cx + cy) & 1) != color) continue;
-                const float rho = V.rho[j];
-                if (rho <= 0.0f) continue;
-                float sx, sy, dg;
-                smem_stencil(V, j, cx, cy, rho, &sx, &sy, &dg);
-                if (dg <= 0.0f) continue;
-                V.px[j] = mixf(V.px[j], (sx - h2 * V.rx[j]) / dg, 1.0f);
-                V.py[j] = mixf(V.py[j], (sy - h2 * V.ry[j]) / dg, 1.0f);
-            }
-            __syncthreads();
-        }
-    }
-    {
-        const SL& V = lv[lp];
-        const Lvl& G = F.L[lp];
-        const int n = V.w * V.h;
-        for (int j = tid; j < n; j += nt) {
-            G.px[j] = V.px[j];
-            G.py[j] = V.py[j];
-        }
-    }
-}
-
 // relaxTile (fluid.wgsl:2109-2182), four tiles a 256-thread CTA.
 __device__ void relaxGroups(const Fast& F, const W& w, int shift, float (*tpx)[RIM * RIM], float (*tpy)[RIM * RIM],
                             int* s_live, int* s_ox, int* s_oy) {
@@ -1362,6 +1231,7 @@ __global__ void __launch_bounds__(256, 4) k_fSolve(Fast F, int shifted) {
     __shared__ float sx[256], sy[256];
     __shared__ double s64[256];
     __shared__ uint32_t most[4];
+    __shared__ uint32_t s_off[WIG_MG_LEVELS + 1];
     const Dev& D = F.D;
     W w(D);
     StepState* st = D.st;
@@ -1399,7 +1269,7 @@ __global__ void __launch_bounds__(256, 4) k_fSolve(Fast F, int shifted) {
             for (uint32_t j = gt; j < n; j += gn) restrictCell(F, w, lp, j);
             if (!gridBarrier(st, nb)) return;
         }
-        if (blockIdx.x == 0) coarseCta(F, w, lp, sm_coarse);
+        if (blockIdx.x == 0) coarseLevels(F, w, lp, sm_coarse, s_off);
         if (!gridBarrier(st, nb)) return;
         for (uint32_t l = lp - 1; l >= 1; l--) {
             const uint32_t n = D.level_w[l] * D.level_h[l];
@@ -1690,6 +1560,9 @@ uint32_t fast_cycle(const Fast& F, bool shifted, cudaStream_t s, const Marker* m
         k_fSmooth<<<cells(l), 256, 0, s>>>(F, l, 1);
         mark(WIG_SLOT_F_SMOOTH, 1);
     }
+    mark(WIG_SLOT_F_RESTRICT, 0);
+    k_fRestrict<<<cells(F.lc), 256, 0, s>>>(F, F.lc);
+    mark(WIG_SLOT_F_RESTRICT, 1);
     size_t smem = fast_coarse_smem(F);
     mark(WIG_SLOT_F_COARSE, 0);
     k_fCoarse<<<1, 1024, smem, s>>>(F);
