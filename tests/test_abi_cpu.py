@@ -1,0 +1,103 @@
+"""The C ABI's library without a GPU: it loads, exports what
+include/wig_fluid.h declares, agrees on layouts with the oracle and the
+Python mirror, and refuses work without a device."""
+import ctypes as C
+import os
+import re
+
+import pytest
+
+from worldinagrain_b200 import abi
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "wig_fluid.h")
+
+
+def _lib():
+    from worldinagrain_b200 import fluid
+    return fluid.lib()
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"^\s*[a-z_][a-z0-9_ \*]*?\b(wig_[a-z0-9_]+)\s*\(", text, flags=re.M)))
+
+
+def test_library_exports_every_declared_function():
+    names = declared_functions()
+    assert "wig_fluid_step" in names and "wig_fluid_residual_norm2_noalloc" in names
+    L = _lib()
+    for n in names:
+        assert hasattr(L, n), n
+
+
+def test_struct_sizes():
+    assert C.sizeof(abi.Params) == 80
+    assert C.sizeof(abi.Elem) == 80
+    assert C.sizeof(abi.Buffers) == 7 * 8
+    assert C.sizeof(abi.Stats) == 9 * 4 + 3 * 4 + 2 * 8
+
+
+@pytest.mark.parametrize("wh", [(1, 1), (7, 5), (64, 64), (131, 97), (256, 256), (1024, 1024), (2048, 2048), (1000, 300)])
+def test_layouts_agree(wh):
+    from oracle.oracle import lib as olib
+    L = _lib()
+    d = abi.WorldDesc(wh[0], wh[1], 0, 0)
+    a, b = abi.WorldLayout(), abi.WorldLayout()
+    assert L.wig_fluid_layout(C.byref(d), C.byref(a)) == 0
+    assert olib().wo_layout(C.byref(d), C.byref(b)) == 0
+    py = abi.layout_py(*wh)
+    for f, _ in abi.WorldLayout._fields_:
+        va, vb = getattr(a, f), getattr(b, f)
+        if f in ("level_w", "level_h"):
+            va, vb = list(va), list(vb)
+        assert va == vb, f
+    for k in ("capacity", "cell_count", "face_count", "block_count", "cells_bytes", "particles_bytes",
+              "counters_bytes", "field_bytes", "blocks_bytes", "cg_bytes"):
+        assert py[k] == getattr(a, k), k
+    assert a.levels == len(py["levels"])
+    lw, lh = py["levels"][-1]
+    assert lw * lh <= abi.MG_COARSEST
+
+
+def test_layout_rejects_bad_sizes():
+    L = _lib()
+    out = abi.WorldLayout()
+    for w, h in ((0, 5), (5, 0), (40000, 4)):
+        d = abi.WorldDesc(w, h, 0, 0)
+        assert L.wig_fluid_layout(C.byref(d), C.byref(out)) == -1
+        assert L.wig_fluid_last_error()
+
+
+def test_create_without_a_device_fails_loudly():
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    from worldinagrain_b200 import fluid
+    from worldinagrain_b200 import world as W
+    w = W.small_world(16, 16)
+    with pytest.raises(fluid.WigError):
+        fluid.LiquidStep(w, W.element_table())
+
+
+def test_missing_library_raises():
+    from worldinagrain_b200 import fluid
+    saved = fluid._lib
+    try:
+        fluid._lib = None
+        with pytest.raises(fluid.WigError):
+            fluid.lib("/nonexistent/libwig_fluid.so")
+    finally:
+        fluid._lib = saved
+
+
+def test_noalloc_refuses_large_worlds_without_touching_the_device():
+    L = _lib()
+    f = L.wig_fluid_residual_norm2_noalloc
+    f.argtypes = [C.POINTER(abi.WorldDesc), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    f.restype = C.c_int
+    d = abi.WorldDesc(2048, 2048, 4, 0)
+    one = C.c_void_p(16)
+    assert f(C.byref(d), one, one, one, one, None) == -1
+    assert b"at most 16384" in L.wig_fluid_last_error()

@@ -1,0 +1,143 @@
+"""The CPU oracle (oracle/wig_oracle.cpp) on its own: the invariants the
+reference's scenes state, integer invariants of the splat, the FP64 solve,
+determinism, and the committed golden fixtures.  No GPU."""
+import json
+import math
+import os
+
+import numpy as np
+import pytest
+
+from oracle.oracle import Oracle, sincos
+from worldinagrain_b200 import abi
+from worldinagrain_b200 import world as W
+
+from .common import params
+from .golden.make_golden import CASES, world_digests
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _run(world, steps, flags=0, max_cycles=16, tol=1e-6):
+    o = Oracle(world, W.element_table())
+    stats = []
+    for s in range(1, steps + 1):
+        stats.append(o.step(params(world, s), max_cycles=max_cycles, flags=flags, tolerance=tol))
+    return o, stats
+
+
+def test_own_sincos_matches_numpy():
+    for a in np.linspace(0.0, 2 * math.pi, 2001, endpoint=False):
+        s, c = sincos(float(np.float32(a)))
+        assert abs(s - math.sin(np.float32(a))) < 2e-6
+        assert abs(c - math.cos(np.float32(a))) < 2e-6
+
+
+def test_dam_break_loses_no_particle():
+    """js/scenes.js:1089-1090, `dam`: "Not a drop is lost"."""
+    world = W.dam_break(64, 64)
+    n0 = None
+    o = Oracle(world, W.element_table())
+    for s in range(1, 41):
+        st = o.step(params(world, s))
+        if n0 is None:
+            n0 = st.particles
+            water = int(np.sum(world.cell_view()[..., 0] & 0xff == abi.WATER))
+            assert n0 == 4 * water
+        assert st.particles == n0
+        m, _, _ = world.particles()
+        assert np.all(np.isfinite(m))
+        # every particle inside the world and out of the walls' cells
+        cx = np.floor(m[:, 0]).astype(int)
+        cy = np.floor(m[:, 1]).astype(int)
+        assert np.all((cx >= 1) & (cx < 63) & (cy >= 1) & (cy < 63))
+
+
+def test_still_tank_pressure_grows_with_depth():
+    """js/scenes.js:1085-1086, `still-tank`: it comes to rest, its pressure
+    growing with depth (columnWeight, fluid.wgsl:1566-1575: rho g (depth + 1/2))."""
+    world = W.World(32, 40)
+    wall = np.zeros((40, 32), dtype=bool)
+    wall[-1, :] = True
+    wall[:, 0] = wall[:, -1] = True
+    world.paint(wall, abi.WALL)
+    water = np.zeros((40, 32), dtype=bool)
+    water[20:39, 1:31] = True
+    world.paint(water, abi.WATER)
+    world.config = {"earth_g": W.earth_g_cells()}
+    g = world.config["earth_g"]
+    _run(world, 60, flags=abi.STEP_TOLERANCE | abi.STEP_F64_DOTS, max_cycles=48)
+    p = world.pressure()
+    m, _, _ = world.particles()
+    assert np.abs(m[:, 2:]).max() < 0.05 * g * 60  # far below free fall over the run
+    col = p[24:38, 15]
+    assert np.all(np.diff(col) > 0)  # deeper, higher
+    slope = np.mean(np.diff(col))
+    assert abs(slope - g) < 0.1 * g
+
+
+def test_splat_integer_invariants():
+    """gather's fixed-point sums (fluid.wgsl:1000-1087): a cell's count and
+    mass are its particles', water's density 1 at 20 C a unit of 2^16 each."""
+    world = W.small_world(40, 32, seed=3, kind="obstacles")
+    o = Oracle(world, W.element_table())
+    for s in range(1, 4):
+        o.step(params(world, s))
+    P = params(world, 4)
+    for name in ("SYNC", "SYNC_PARTICLES", "SYNC_SEED", "COMPACT", "RETIRE", "CLEAR", "GATHER"):
+        o.pass_(P, name)
+    cc = world.counters_cells()
+    n = world.particle_count("parts")
+    assert int(cc[:, 0].sum()) == n
+    assert np.array_equal(cc[:, 7].astype(np.int64), cc[:, 0].astype(np.int64) * 65536)
+    # each particle's four density shares sum to 2^16 (up to rounding of each)
+    assert abs(int(cc[:, 6].astype(np.int64).sum()) - n * 65536) <= 4 * n
+
+
+def test_oracle_is_deterministic():
+    a = W.small_world(40, 32, seed=3, kind="moving")
+    b = a.copy()
+    _run(a, 5)
+    _run(b, 5)
+    for name in abi.BUFFER_NAMES:
+        assert np.array_equal(getattr(a, name), getattr(b, name)), name
+
+
+def test_fp32_solve_against_fp64_solve():
+    """The oracle's FP32 CG (1e-6 form) against an FP64 solve of the same
+    operator at 1e-12: the pressure's relative L2 error."""
+    world = W.dam_break(64, 64)
+    o, _ = _run(world, 3, flags=abi.STEP_TOLERANCE | abi.STEP_F64_DOTS, max_cycles=48)
+    P = params(world, 4)
+    seq = ("SYNC", "SYNC_PARTICLES", "SYNC_SEED", "COMPACT", "RETIRE", "CLEAR", "GATHER", "SEAL_JOIN",
+           "SEAL_ANCHOR", "CLASSIFY", "SET_FACES", "UNPRESS", "DIVERGENCE", "CG_START", "CG_JOIN", "CG_ANCHOR")
+    probe = world.copy()
+    po = Oracle(probe, W.element_table())
+    for name in seq:
+        po.pass_(P, name)
+    x64, it, rel = po.solve_f64(P, rel_tol=1e-12)
+    assert rel <= 1e-12
+    o.step(P, max_cycles=48, flags=abi.STEP_TOLERANCE | abi.STEP_F64_DOTS, tolerance=1e-6)
+    x32 = world.field_cells()[:, 0, 0].astype(np.float64)
+    fluid = world.field_cells()[:, 0, 2] > 0
+    err = np.linalg.norm(x32[fluid] - x64[fluid]) / np.linalg.norm(x64[fluid])
+    assert err < 1e-4, err
+    true_rel = po.true_residual(P, world.field_cells()[:, 0, 0])
+    assert true_rel < 1e-3
+
+
+@pytest.mark.parametrize("case", [c[0] for c in CASES])
+def test_oracle_matches_golden_fixtures(case):
+    with open(os.path.join(HERE, "golden", "oracle_steps.json")) as f:
+        fixtures = json.load(f)
+    name, builder, flags, max_cycles, record = next(c for c in CASES if c[0] == case)
+    world = builder()
+    o = Oracle(world, W.element_table())
+    want = fixtures[case]["steps"]
+    for s in range(1, max(record) + 1):
+        P = W.make_params(world, frame=s, seed=0x1234, earth_g=world.config["earth_g"])
+        st = o.step(P, max_cycles=max_cycles, flags=flags, tolerance=1e-6)
+        if str(s) in want:
+            got = world_digests(world)
+            got["cycles"] = int(st.cycles)
+            assert got == want[str(s)], f"{case} step {s}"

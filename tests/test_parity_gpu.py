@@ -12,7 +12,11 @@ import pytest
 from worldinagrain_b200 import abi
 from worldinagrain_b200 import world as W
 
+import json
+import os
+
 from .common import busy_world, compare_worlds, params, run_membership
+from .golden.make_golden import CASES, world_digests
 
 pytestmark = pytest.mark.gpu
 
@@ -221,3 +225,56 @@ def test_fast_profile_matches_graph(form):
         assert not diffs, f"step {s}: " + "; ".join(diffs)
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize("form", ["plain", "fast", "persistent"])
+@pytest.mark.parametrize("case", [c[0] for c in CASES])
+def test_gpu_matches_golden_fixtures(case, form):
+    """The committed fixtures (the oracle's digests, tests/golden): the
+    plain form's every buffer, the fast forms' observable ones."""
+    fluid = _gpu()
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "golden", "oracle_steps.json")) as f:
+        want = json.load(f)[case]["steps"]
+    name, builder, flags, max_cycles, record = next(c for c in CASES if c[0] == case)
+    world = builder()
+    g = fluid.LiquidStep(world, W.element_table())
+    got = world.copy()
+    for s in range(1, max(record) + 1):
+        P = W.make_params(world, frame=s, seed=0x1234, earth_g=world.config["earth_g"])
+        g.step(P, max_cycles=max_cycles, flags=flags | FORMS[form], tolerance=1e-6)
+        st = g.stats()
+        if str(s) in want:
+            g.download(got)
+            d = world_digests(got)
+            w = want[str(s)]
+            keys = ["cells", "blocks", "sorted", "parts", "sorted_count", "parts_count"]
+            keys += ["counters", "field", "cg"] if form == "plain" else ["counters_observable", "field_observable"]
+            for k in keys:
+                assert d[k] == w[k], f"{case} step {s} {k}"
+            assert st.cycles == w["cycles"]
+    g.close()
+
+
+@pytest.mark.parametrize("form", ["plain", "fast"])
+def test_two_liquids_with_viscosity(form):
+    """Water and a viscous liquid: viscosity's sweeps and unpress
+    (fluid.wgsl:3277-3466), two liquids' cells drawn by the most numerous
+    (raster, fluid.wgsl:4029-4066), slip between them (fluid.wgsl:3605-3614)."""
+    fluid = _gpu()
+    world = W.two_liquids()
+    ref = world.copy()
+    o = _oracle(ref)
+    g = fluid.LiquidStep(world, W.element_table())
+    got = world.copy()
+    flags = abi.STEP_VISCOUS
+    for s in range(1, 11):
+        P = params(ref, s)
+        so = o.step(P, flags=flags)
+        g.step(P, flags=flags | FORMS[form])
+        sg = g.stats()
+        g.download(got)
+        diffs = compare_worlds(got, ref, scratch=form != "plain")
+        assert not diffs, f"step {s}: " + "; ".join(diffs)
+        assert sg.count[abi.COUNT_VISCOUS] == so.count[abi.COUNT_VISCOUS] == 1
+    g.close()

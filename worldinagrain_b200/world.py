@@ -32,10 +32,15 @@ T_NEVER = 1e9
 GAS_HEAT_CAP = 1.2e-3 * 1000.0  # order of js/shared.js:174; read by nothing on the liquid's path
 
 
+MUD = 4  # a viscous liquid of this table's own (not the reference's id)
+
+
 def element_table():
     """The element rows the liquid step reads, for AIR, WALL, SAND, WATER
-    (js/elements.js:414-458, with DEFAULTS js/elements.js:316-360)."""
-    rows = [abi.Elem() for _ in range(4)]
+    (js/elements.js:414-458, with DEFAULTS js/elements.js:316-360), and a
+    fifth, a viscous liquid denser than water (on the lines of the
+    reference's mud, js/elements.js:510-514) for the viscosity passes."""
+    rows = [abi.Elem() for _ in range(5)]
 
     def fill(e, **kw):
         base = dict(kind=abi.KIND_SOLID, density=1000.0, weight=GRAVITY, heat_cap=2.0, viscosity=0.0,
@@ -53,7 +58,8 @@ def element_table():
     fill(rows[abi.WATER], kind=abi.KIND_LIQUID, density=100.0, heat_cap=4.18, hi_t=100.0, lo_t=0.0,
          up_span=2257.0 / 4.18, down_span=334.0 / 4.18, down_scale=1.0, expansion=1.42e-4,
          expansion2=4.45e-6, tension=1.0, flags=2)
-    return (abi.Elem * 4)(*rows)
+    fill(rows[MUD], kind=abi.KIND_LIQUID, density=160.0, heat_cap=3.3, viscosity=0.8, hi_t=T_NEVER, lo_t=-T_NEVER)
+    return (abi.Elem * 5)(*rows)
 
 
 # ---------------------------------------------------------------- cells
@@ -223,6 +229,27 @@ def obstacle_column(width=2048, height=2048, p_solid=0.03, fill=0.7, ppc=2, seed
     w.paint(water, abi.WATER)
     w.config = dict(workload="obstacle_column", grid=f"{width}x{height}", seed=seed, earth_g=earth_g_cells(),
                     p_solid=p_solid, ppc=ppc)
+    return w
+
+
+def two_liquids(width=40, height=32, seed=5):
+    """Water on the left and a viscous liquid (MUD) on the right of a walled
+    box, moving: two liquids in contact, their cells rasterised by the most
+    numerous, the viscous one's faces swept (viscosityRed/Black, unpress)."""
+    rng = np.random.default_rng(seed)
+    w = World(width, height)
+    wall = np.zeros((height, width), dtype=bool)
+    wall[-1, :] = True
+    wall[:, 0] = wall[:, -1] = True
+    w.paint(wall, abi.WALL)
+    vel = rng.normal(0.0, 0.3, (height, width, 2)).astype(np.float32)
+    water = np.zeros((height, width), dtype=bool)
+    water[height // 3:height - 1, 1:width // 2] = True
+    w.paint(water, abi.WATER, vel=vel)
+    mud = np.zeros((height, width), dtype=bool)
+    mud[height // 2:height - 1, width // 2:width - 1] = True
+    w.paint(mud, MUD, vel=vel)
+    w.config = dict(workload="two_liquids", grid=f"{width}x{height}", seed=seed, earth_g=earth_g_cells())
     return w
 
 
