@@ -304,6 +304,7 @@ enum wig_profile_slot {
     WIG_SLOT_F_UPDATE,
     WIG_SLOT_F_FINISH,
     WIG_SLOT_F_SOLVE,
+    WIG_SLOT_SCHED,        /* writing a batch's work lists */
     WIG_PROFILE_SLOTS
 };
 

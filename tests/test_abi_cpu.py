@@ -1,6 +1,6 @@
 """The C ABI's library without a GPU: it loads, exports what
-include/wig_fluid.h declares, agrees on layouts with the oracle and the
-Python mirror, and refuses work without a device."""
+include/*.h declare, agrees on layouts with the oracle and the Python
+mirror, and refuses work without a device."""
 import ctypes as C
 import os
 import re
@@ -10,7 +10,7 @@ import pytest
 from worldinagrain_b200 import abi
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-HEADER = os.path.join(ROOT, "include", "wig_fluid.h")
+HEADERS = [os.path.join(ROOT, "include", h) for h in sorted(os.listdir(os.path.join(ROOT, "include"))) if h.endswith(".h")]
 
 
 def _lib():
@@ -19,14 +19,18 @@ def _lib():
 
 
 def declared_functions():
-    text = open(HEADER).read()
-    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"^\s*[a-z_][a-z0-9_ \*]*?\b(wig_[a-z0-9_]+)\s*\(", text, flags=re.M)))
+    names = set()
+    for h in HEADERS:
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        names |= set(re.findall(r"^\s*[a-z_][a-z0-9_ \*]*?\b(wig_[a-z0-9_]+)\s*\(", text, flags=re.M))
+    return sorted(names)
 
 
 def test_library_exports_every_declared_function():
     names = declared_functions()
     assert "wig_fluid_step" in names and "wig_fluid_residual_norm2_noalloc" in names
+    assert "wig_batch_step" in names and "wig_batch_create" in names
     L = _lib()
     for n in names:
         assert hasattr(L, n), n

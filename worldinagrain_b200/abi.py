@@ -48,7 +48,7 @@ PASSES = [
 PASS = {name: i for i, name in enumerate(PASSES)}
 PROFILE_NAMES = PASSES + ["NORM", "REPORT", "F_SETUP", "F_LOOP", "F_RELAX", "F_RESTRICT", "F_SMOOTH", "F_COARSE",
                           "F_PROLONG", "F_PROLONG_FINE", "F_RHO_BETA", "F_DIRECTION", "F_APPLY_ALPHA", "F_UPDATE",
-                          "F_FINISH", "F_SOLVE"]
+                          "F_FINISH", "F_SOLVE", "SCHED"]
 PROFILE_SLOTS = len(PROFILE_NAMES)
 
 

@@ -14,8 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(LIB_DIR, "libwig_fluid.so")
-SOURCES = ["wig_api.cu", "wig_passes.cu", "wig_fast.cu", "wig_noalloc.cu"]
-HEADERS = ["wig_device.cuh", "wig_passes.cuh", "wig_fast.cuh"]
+SOURCES = ["wig_api.cu", "wig_passes.cu", "wig_fast.cu", "wig_sched.cu", "wig_noalloc.cu"]
+HEADERS = ["wig_device.cuh", "wig_passes.cuh", "wig_fast.cuh", "wig_sched.cuh"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -38,6 +38,7 @@ def _stale():
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
     deps.append(os.path.join(HERE, "..", "include", "wig_fluid.h"))
+    deps.append(os.path.join(HERE, "..", "include", "wig_batch.h"))
     deps.append(os.path.abspath(__file__))
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 

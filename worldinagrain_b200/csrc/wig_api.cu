@@ -1,23 +1,30 @@
-// wig_api.cu — the C ABI (include/wig_fluid.h): world handles, bound
-// buffers, and the step driver that replaces Simulation.encodeFluid
-// (js/sim.js:2466-2612).
+// wig_api.cu — the C ABI (include/wig_fluid.h, include/wig_batch.h): world
+// handles and batches, bound buffers, and the step driver that replaces
+// Simulation.encodeFluid (js/sim.js:2466-2612).
 //
-// A step is the reference's pass sequence, recorded once per shape (max
-// cycles, flags, the tiling parity it starts on) into a CUDA graph and
-// replayed: the per-step inputs (the Params uniform) reach the device as one
-// small copy from pinned host memory ahead of the graph, and the report words
-// come back as one small copy after it, the reference's writeBuffer and
-// mapped report buffer (js/sim.js:1975-1995, :1763, :1882-1900).
+// Every handle is a batch: a table of worlds in device memory and, per step
+// lane, the work lists the kernels take their items from.  A single-world
+// handle (wig_fluid) is a batch of one.  A step is the reference's pass
+// sequence, recorded once per shape (max cycles, flags) into a CUDA graph
+// and replayed: the per-step inputs (each world's Params uniform and its
+// part of the step) reach the device as one small copy from pinned host
+// memory ahead of the graph, and the report words come back as one small
+// copy after it, the reference's writeBuffer and mapped report buffer
+// (js/sim.js:1975-1995, :1763, :1882-1900).
 
+#include <algorithm>
+#include <array>
 #include <cstdio>
 #include <cstring>
 #include <map>
 #include <string>
 #include <vector>
 
+#include "../../include/wig_batch.h"
 #include "wig_device.cuh"
 #include "wig_fast.cuh"
 #include "wig_passes.cuh"
+#include "wig_sched.cuh"
 
 namespace {
 
@@ -42,8 +49,8 @@ namespace {
         if (e_ != cudaSuccess) return fail(WIG_E_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
     } while (0)
 
-// Device-side report: the FLUID_COUNT words, the particle count and the
-// solve's residuals, gathered by k_report at the end of a step.
+// Device-side report of a world: the FLUID_COUNT words, the particle count
+// and the solve's residuals, gathered by k_report at the end of a step.
 struct Report {
     uint32_t count[WIG_FLUID_STATS];
     uint32_t particles;
@@ -53,49 +60,84 @@ struct Report {
     double bnorm2;
 };
 
-__global__ void k_report(wig::Dev D, Report* out) {
-    if (threadIdx.x == 0) {
-        for (uint32_t k = 0; k < WIG_FLUID_STATS; k++) out->count[k] = D.blocks[4u * D.B + k];
-        out->particles = D.sorted[0];
-        out->err = D.st->err;
-        out->rel = D.st->rel;
-        out->bnorm2 = D.st->bnorm2;
+// Each world's report into its slot (by world) and the lane's (by the
+// world's place in the step's list).
+__global__ void k_report(wig::Batch Bt, Report* by_world, Report* by_entry) {
+    if (threadIdx.x != 0) return;
+    FOR_ITEMS(Bt, wig::L_ONE_ALL, it) {
+        const uint32_t k = (uint32_t)((uint64_t)it >> Bt.lbits);
+        const wig::Dev& D = Bt.worlds[k].D;
+        Report r;
+        for (uint32_t c = 0; c < WIG_FLUID_STATS; c++) r.count[c] = D.blocks[4u * D.B + c];
+        r.particles = D.sorted[0];
+        r.err = D.st->err;
+        r.pad = 0u;
+        r.rel = D.st->rel;
+        r.bnorm2 = D.st->bnorm2;
+        by_world[k] = r;
+        by_entry[g_it] = r;
     }
 }
 
 constexpr int RING = 8;
 
+struct Graph {
+    cudaGraph_t g = nullptr;
+    cudaGraphExec_t ge = nullptr;
+    uint32_t outside = 0;  // kernels outside the iteration loop
+    uint32_t body = 0;     // kernels of one iteration
+};
+
+// A step lane: its work lists, its per-step upload ring, its graphs.
+struct Lane {
+    uint32_t* d_items = nullptr;
+    uint32_t* d_count = nullptr;
+    uint32_t* d_off = nullptr;
+    uint32_t* d_loop = nullptr;
+    char* d_up = nullptr;          // nsub, sub[], heads[]
+    char* h_up = nullptr;          // pinned, RING slots
+    cudaEvent_t up_ev[RING] = {};
+    int up_at = 0;
+    Report* d_rsub = nullptr;
+    Report* h_rsub = nullptr;      // pinned
+    wig::Batch Bt{};
+    wig::SchedCtl ctl{};
+    std::map<uint64_t, Graph> graphs;
+    cudaStream_t cap = nullptr, cap2 = nullptr;
+    cudaStream_t last_stream = nullptr;
+    uint32_t last_launches = 0, last_body = 0;
+};
+
+size_t align256(size_t x) { return (x + 255u) & ~(size_t)255u; }
+
 }  // namespace
 
-struct wig_fluid {
-    wig_world_layout L{};
-    wig::Dev D{};
+struct wig_batch {
+    uint32_t K = 0;
     int device = 0;
-    void* own[7] = {nullptr};
-    bool bound = false;
+    std::vector<wig_world_layout> L;
+    std::vector<wig::World> hw;       // host copy of the world table
+    wig::World* d_worlds = nullptr;
     wig_elem* d_elems = nullptr;
-    wig::StepState* d_st = nullptr;
-    wig::StepState* h_st = nullptr;  // pinned ring of RING
-    cudaEvent_t st_ev[RING] = {};
-    int st_at = 0;
-    Report* d_report = nullptr;
-    Report* h_report = nullptr;      // pinned
-    double* d_part64 = nullptr;
-    double* d_norm64 = nullptr;
-    bool shifted_first = false;
-    cudaStream_t cap = nullptr;      // capture stream
-    cudaStream_t last_stream = nullptr;
-    std::map<uint64_t, std::pair<cudaGraph_t, cudaGraphExec_t>> graphs;
-    std::map<uint64_t, uint32_t> graph_launches;  // kernels in each graph (fast form: outside the loop)
-    std::map<uint64_t, uint32_t> graph_body;      // fast form: kernels per iteration
-    uint32_t last_launches = 0;
-    uint32_t last_body = 0;
-    uint32_t last_cycles_flags = 0;
-    // the fast form's scratch
-    wig::Fast F{};
-    void* fast_mem = nullptr;
-    bool fast_dirty = true;
-    cudaStream_t cap2 = nullptr;     // capture stream of the iteration loop's body
+    wig::StepState* d_st = nullptr;   // K
+    Report* d_report = nullptr;       // K
+    Report* h_report = nullptr;       // K, pinned
+    void* scratch = nullptr;          // the fast form's scratch and FP64 partials of every world
+    void* arena = nullptr;            // the worlds' buffers (batches made by wig_batch_create)
+    std::vector<std::array<void*, 7>> own;  // buffers a single-world handle allocated at bind
+    std::vector<char> bound, dirty;
+    std::vector<char> shifted_first;
+    std::vector<cudaStream_t> stepped_on;   // the stream of each world's last step
+    std::vector<int> stepped_lane;
+    wig::BatchShape S{};
+    uint32_t lbits = 31;
+    uint32_t solve_grid = 0;          // the persistent solve's CTAs (a batch of one world)
+    Lane lane[WIG_BATCH_LANES];
+    size_t up_bytes = 0;              // one upload slot
+};
+
+struct wig_fluid {
+    wig_batch* b = nullptr;
 };
 
 namespace {
@@ -111,8 +153,8 @@ int layout_of(const wig_world_desc* d, wig_world_layout* L) {
     L->height = (uint32_t)H;
     L->liquid_per_cell = d->liquid_per_cell ? d->liquid_per_cell : 4u;
     if (L->liquid_per_cell > 64) return fail(WIG_E_ARG, "liquid_per_cell out of range (1..64)");
-    uint64_t cap = d->capacity ? d->capacity : (uint64_t)((double)C * L->liquid_per_cell * 1.25 + 0.999999);
-    if (!d->capacity) {
+    uint64_t cap = d->capacity;
+    if (!cap) {
         // ceil(C * ppc * 1.25) exactly (js/sim.js:747)
         uint64_t num = C * L->liquid_per_cell * 5ull;
         cap = (num + 3ull) / 4ull;
@@ -156,49 +198,324 @@ uint64_t buffer_bytes(const wig_world_layout& L, int which) {
     }
 }
 
-void** buffer_slot(wig_fluid* h, int which) {
+void** buffer_slot(wig::Dev& D, int which) {
     switch (which) {
-    case 0: return (void**)&h->D.cells;
-    case 1: return (void**)&h->D.sorted;
-    case 2: return (void**)&h->D.parts;
-    case 3: return (void**)&h->D.counters;
-    case 4: return (void**)&h->D.field;
-    case 5: return (void**)&h->D.blocks;
-    case 6: return (void**)&h->D.cg;
+    case 0: return (void**)&D.cells;
+    case 1: return (void**)&D.sorted;
+    case 2: return (void**)&D.parts;
+    case 3: return (void**)&D.counters;
+    case 4: return (void**)&D.field;
+    case 5: return (void**)&D.blocks;
+    case 6: return (void**)&D.cg;
     default: return nullptr;
     }
 }
 
-void drop_graphs(wig_fluid* h) {
-    for (auto& kv : h->graphs) {
-        if (kv.second.second) cudaGraphExecDestroy(kv.second.second);
-        if (kv.second.first) cudaGraphDestroy(kv.second.first);
+// The shape fields of a world's descriptor.
+void dev_shape(wig::Dev& D, const wig_world_layout& L) {
+    D.W = (int)L.width;
+    D.H = (int)L.height;
+    D.C = L.cell_count;
+    D.F = L.face_count;
+    D.B = L.block_count;
+    D.BW = L.blocks_wide;
+    D.BH = L.block_count / L.blocks_wide;
+    D.cap = L.capacity;
+    D.ppc = L.liquid_per_cell;
+    D.edge_tiles = L.edge_tiles;
+    D.levels = L.levels;
+    D.level_w[0] = L.width;
+    D.level_h[0] = L.height;
+    uint32_t at = 2u * D.C + D.F + 2u * ((D.F + 3u) / 4u);
+    D.level_start[0] = 0;
+    for (uint32_t l = 1; l <= WIG_MG_LEVELS; l++) {
+        D.level_w[l] = l <= L.levels ? L.level_w[l - 1] : 0u;
+        D.level_h[l] = l <= L.levels ? L.level_h[l - 1] : 0u;
+        D.level_start[l] = at;
+        at += 2u * D.level_w[l] * D.level_h[l];
     }
-    h->graphs.clear();
-    h->graph_launches.clear();
-    h->graph_body.clear();
 }
 
-// Writes this step's state into the next pinned slot and copies it to the
-// device on stream s.
-int push_state(wig_fluid* h, const wig_params* P, uint32_t flags, double tol, cudaStream_t s, bool params_only) {
-    int k = h->st_at;
-    h->st_at = (h->st_at + 1) % RING;
-    CUDA_TRY(cudaEventSynchronize(h->st_ev[k]));
-    wig::StepState* st = h->h_st + k;
-    std::memset(st, 0, sizeof(*st));
-    st->P = *P;
-    st->P.size[0] = h->L.width;
-    st->P.size[1] = h->L.height;
-    st->tol_mode = (flags & WIG_STEP_TOLERANCE) ? 1u : 0u;
-    st->f64 = (flags & WIG_STEP_F64_DOTS) ? 1u : 0u;
-    st->tol = tol;
-    st->rel = 1.0;
-    size_t bytes = params_only ? sizeof(wig_params) : sizeof(wig::StepState);
-    CUDA_TRY(cudaMemcpyAsync(h->d_st, st, bytes, cudaMemcpyHostToDevice, s));
-    CUDA_TRY(cudaEventRecord(h->st_ev[k], s));
+// Bytes of a world's fast scratch and FP64 partials.
+size_t scratch_bytes(const wig::Dev& D) {
+    const size_t C = D.C;
+    size_t bytes = align256(C) + 17u * align256(C * 4u);
+    for (uint32_t l = 1; l <= D.levels; l++) bytes += 10u * align256((size_t)D.level_w[l] * D.level_h[l] * 4u);
+    bytes += align256(2u * (size_t)D.B * 4u) + 3u * align256(2u * (size_t)D.B * 8u);
+    return bytes;
+}
+
+// Lays a world's scratch out from p (scratch_bytes of it).
+void scratch_take(wig::World& Wd, char* p) {
+    wig::Dev& D = Wd.D;
+    wig::FastW& F = Wd.S;
+    auto take = [&](size_t n) { char* q = p; p += align256(n); return q; };
+    auto fl = [&](size_t n) { return reinterpret_cast<float*>(take(n * 4u)); };
+    const size_t C = D.C;
+    F.fmask = reinterpret_cast<uint8_t*>(take(C));
+    for (uint32_t l = 0; l <= D.levels; l++) {
+        const size_t n = l == 0 ? C : (size_t)D.level_w[l] * D.level_h[l];
+        wig::Lvl& V = F.L[l];
+        V.px = fl(n); V.py = fl(n); V.rx = fl(n); V.ry = fl(n); V.rho = fl(n);
+        V.b0 = fl(n); V.b1 = fl(n); V.b2 = fl(n); V.b3 = fl(n); V.diag = fl(n);
+    }
+    F.pin = fl(C); F.rimx = fl(C); F.rimy = fl(C);
+    F.X = fl(C); F.R = fl(C); F.P = fl(C); F.Q = fl(C);
+    F.part32 = fl(2u * (size_t)D.B);
+    F.part64 = reinterpret_cast<double*>(take(2u * (size_t)D.B * 8u));
+    D.part64 = reinterpret_cast<double*>(take(2u * (size_t)D.B * 8u));
+    D.norm64 = reinterpret_cast<double*>(take(2u * (size_t)D.B * 8u));
+    F.lc = D.levels;
+    for (uint32_t l = 1; l <= D.levels; l++)
+        if ((size_t)D.level_w[l] * D.level_h[l] <= wig::COARSE_CTA_CELLS) { F.lc = l; break; }
+    F.lp = D.levels;
+    for (uint32_t l = 1; l <= D.levels; l++)
+        if ((size_t)D.level_w[l] * D.level_h[l] <= wig::PERSISTENT_CTA_CELLS) { F.lp = l; break; }
+}
+
+uint64_t world_buffers_bytes(const wig_world_layout& L) {
+    uint64_t n = 0;
+    for (int k = 0; k < 7; k++) n += align256(buffer_bytes(L, k));
+    return n;
+}
+
+uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
+
+void destroy_batch(wig_batch* b);
+
+// Frees a lane's graphs.
+void drop_graphs(Lane& ln) {
+    for (auto& kv : ln.graphs) {
+        if (kv.second.ge) cudaGraphExecDestroy(kv.second.ge);
+        if (kv.second.g) cudaGraphDestroy(kv.second.g);
+    }
+    ln.graphs.clear();
+}
+
+int upload_world_entry(wig_batch* b, uint32_t k) {
+    CUDA_TRY(cudaMemcpy(b->d_worlds + k, &b->hw[k], sizeof(wig::World), cudaMemcpyHostToDevice));
     return WIG_OK;
 }
+
+// A batch of n worlds with their shapes, scratch, lanes and (alloc_buffers)
+// the worlds' buffers in one packed allocation.
+int make_batch(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, uint32_t n_elems, bool alloc_buffers,
+               wig_batch** out) {
+    if (!out) return fail(WIG_E_ARG, "null output handle");
+    *out = nullptr;
+    if (!descs || n == 0 || n > WIG_BATCH_MAX_WORLDS) return fail(WIG_E_ARG, "world count out of range");
+    if (!elems || n_elems == 0 || n_elems > WIG_MAX_ELEMS) return fail(WIG_E_ARG, "element table empty or too long");
+    if (n_elems <= WIG_ELEM_WATER) return fail(WIG_E_ARG, "element table must reach WATER (id 3)");
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(WIG_E_NO_DEVICE, "no CUDA device");
+    }
+    wig_batch* b = new (std::nothrow) wig_batch();
+    if (!b) return fail(WIG_E_OOM, "host allocation failed");
+    auto bail = [&](int code, const std::string& m) {
+        std::string keep = m;
+        destroy_batch(b);
+        return fail(code, keep);
+    };
+    b->K = n;
+    cudaGetDevice(&b->device);
+    b->L.resize(n);
+    b->hw.assign(n, wig::World{});
+    b->own.assign(n, std::array<void*, 7>{});
+    b->bound.assign(n, 0);
+    b->dirty.assign(n, 1);
+    b->shifted_first.assign(n, 0);
+    b->stepped_on.assign(n, nullptr);
+    b->stepped_lane.assign(n, -1);
+    for (uint32_t k = 0; k < n; k++) {
+        int rc = layout_of(&descs[k], &b->L[k]);
+        if (rc) {
+            std::string m = g_last_error;
+            destroy_batch(b);
+            return fail(rc, "world " + std::to_string(k) + ": " + m);
+        }
+        dev_shape(b->hw[k].D, b->L[k]);
+    }
+    // the shape: list sizes, coarse kernel's memory, item bits
+    wig::BatchShape& S = b->S;
+    std::memset(&S, 0, sizeof(S));
+    S.worlds = n;
+    uint64_t most_units = 1, max_items[wig::L_COUNT] = {0};
+    size_t scratch_total = 0;
+    for (uint32_t k = 0; k < n; k++) {
+        wig::World& Wd = b->hw[k];
+        const wig::Dev& D = Wd.D;
+        scratch_total += scratch_bytes(D);
+        // lc for the shape (scratch_take sets it again on the real layout)
+        uint32_t lc = D.levels;
+        for (uint32_t l = 1; l <= D.levels; l++)
+            if ((size_t)D.level_w[l] * D.level_h[l] <= wig::COARSE_CTA_CELLS) { lc = l; break; }
+        Wd.S.lc = lc;
+        const uint64_t pch = cdiv(D.cap, 256);
+        max_items[wig::L_WB] += D.B;
+        max_items[wig::L_PS] += pch;
+        max_items[wig::L_PP] += pch;
+        max_items[wig::L_ACT] += D.B;
+        max_items[wig::L_RET] += D.B;
+        max_items[wig::L_ACT4] += cdiv(D.B, 4);
+        max_items[wig::L_RELAX] += D.B + D.edge_tiles;
+        max_items[wig::L_ONE_ALL] += 1;
+        max_items[wig::L_ONE] += 1;
+        for (uint32_t l = 1; l <= WIG_MG_LEVELS; l++) {
+            const uint64_t ch = cdiv((uint64_t)D.level_w[l] * D.level_h[l], 256);
+            if (l <= lc && l <= D.levels) max_items[wig::L_RES + l - 1] += ch;
+            if (l < lc) max_items[wig::L_SM + l - 1] += ch;
+            if (l <= D.levels) most_units = std::max<uint64_t>(most_units, ch);
+        }
+        most_units = std::max<uint64_t>(most_units, std::max<uint64_t>(D.B + D.edge_tiles, pch));
+        S.levels = std::max(S.levels, D.levels);
+        S.lc_max = std::max(S.lc_max, lc);
+        S.coarse_smem = std::max(S.coarse_smem, wig::fast_coarse_smem(D, lc));
+    }
+    uint32_t bits = 1;
+    while (bits < 31 && (1ull << bits) <= most_units) bits++;
+    if ((1ull << bits) <= most_units) return bail(WIG_E_ARG, "a world is too large for the work lists");
+    if (bits < 31 && (uint64_t)n > (1ull << (32 - bits))) return bail(WIG_E_ARG, "too many worlds of this size in one batch");
+    b->lbits = bits;
+    uint64_t items_total = 0;
+    uint32_t base[wig::L_COUNT];
+    for (uint32_t l = 0; l < wig::L_COUNT; l++) {
+        if (max_items[l] > 0xffffffffull) return bail(WIG_E_ARG, "work lists too long");
+        S.max_items[l] = (uint32_t)max_items[l];
+        base[l] = (uint32_t)items_total;
+        items_total += max_items[l];
+    }
+    if (items_total > 0xffffffffull) return bail(WIG_E_ARG, "work lists too long");
+    if (S.coarse_smem > 200u * 1024u) return bail(WIG_E_ARG, "coarse levels too large for one CTA");
+    if (wig::fast_prepare_attributes(S.coarse_smem) != cudaSuccess) return bail(WIG_E_CUDA, "cudaFuncSetAttribute");
+
+    // device memory: elements, step states, reports, world table, scratch
+    if (cudaMalloc(&b->d_elems, sizeof(wig_elem) * n_elems) != cudaSuccess) return bail(WIG_E_OOM, "cudaMalloc elems");
+    if (cudaMemcpy(b->d_elems, elems, sizeof(wig_elem) * n_elems, cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(WIG_E_CUDA, "cudaMemcpy elems");
+    if (cudaMalloc(&b->d_st, sizeof(wig::StepState) * n) != cudaSuccess) return bail(WIG_E_OOM, "cudaMalloc step states");
+    cudaMemset(b->d_st, 0, sizeof(wig::StepState) * n);
+    if (cudaMalloc(&b->d_report, sizeof(Report) * n) != cudaSuccess) return bail(WIG_E_OOM, "cudaMalloc reports");
+    cudaMemset(b->d_report, 0, sizeof(Report) * n);
+    if (cudaMallocHost(&b->h_report, sizeof(Report) * n) != cudaSuccess) return bail(WIG_E_OOM, "cudaMallocHost reports");
+    std::memset(b->h_report, 0, sizeof(Report) * n);
+    if (cudaMalloc(&b->d_worlds, sizeof(wig::World) * n) != cudaSuccess) return bail(WIG_E_OOM, "cudaMalloc world table");
+    if (cudaMalloc(&b->scratch, scratch_total) != cudaSuccess) return bail(WIG_E_OOM, "cudaMalloc fast scratch");
+    cudaMemset(b->scratch, 0, scratch_total);
+    {
+        char* p = static_cast<char*>(b->scratch);
+        for (uint32_t k = 0; k < n; k++) {
+            wig::World& Wd = b->hw[k];
+            scratch_take(Wd, p);
+            p += scratch_bytes(Wd.D);
+            Wd.D.elems = b->d_elems;
+            Wd.D.n_elems = n_elems;
+            Wd.D.st = b->d_st + k;
+        }
+    }
+    if (alloc_buffers) {
+        uint64_t total = 0;
+        for (uint32_t k = 0; k < n; k++) total += world_buffers_bytes(b->L[k]);
+        if (cudaMalloc(&b->arena, total) != cudaSuccess) {
+            cudaGetLastError();
+            return bail(WIG_E_OOM, "cudaMalloc of the worlds' buffers failed");
+        }
+        if (cudaMemset(b->arena, 0, total) != cudaSuccess) return bail(WIG_E_CUDA, "cudaMemset of the worlds' buffers");
+        char* p = static_cast<char*>(b->arena);
+        for (uint32_t k = 0; k < n; k++) {
+            for (int w = 0; w < 7; w++) {
+                *buffer_slot(b->hw[k].D, w) = p;
+                p += align256(buffer_bytes(b->L[k], w));
+            }
+            b->bound[k] = 1;
+        }
+    }
+    if (cudaMemcpy(b->d_worlds, b->hw.data(), sizeof(wig::World) * n, cudaMemcpyHostToDevice) != cudaSuccess)
+        return bail(WIG_E_CUDA, "cudaMemcpy world table");
+    if (n == 1) {
+        wig::Fast F0;
+        static_cast<wig::FastW&>(F0) = b->hw[0].S;
+        F0.D = b->hw[0].D;
+        if (wig::fast_solve_grid(F0, &b->solve_grid) != cudaSuccess) return bail(WIG_E_CUDA, "occupancy of the persistent solve");
+    }
+
+    // lanes
+    b->up_bytes = 8u + ((4u * (size_t)n + 7u) & ~(size_t)7u) + sizeof(wig::StepHead) * n;
+    for (uint32_t li = 0; li < WIG_BATCH_LANES; li++) {
+        Lane& ln = b->lane[li];
+        if (cudaMalloc(&ln.d_items, 4u * (size_t)std::max<uint64_t>(items_total, 1)) != cudaSuccess)
+            return bail(WIG_E_OOM, "cudaMalloc work lists");
+        if (cudaMalloc(&ln.d_count, 4u * wig::L_COUNT) != cudaSuccess) return bail(WIG_E_OOM, "cudaMalloc list counts");
+        cudaMemset(ln.d_count, 0, 4u * wig::L_COUNT);
+        if (cudaMalloc(&ln.d_off, 4u * (size_t)wig::L_COUNT * (n + 1u)) != cudaSuccess)
+            return bail(WIG_E_OOM, "cudaMalloc list offsets");
+        if (cudaMalloc(&ln.d_loop, 4u) != cudaSuccess) return bail(WIG_E_OOM, "cudaMalloc loop word");
+        cudaMemset(ln.d_loop, 0, 4u);
+        if (cudaMalloc(&ln.d_up, b->up_bytes) != cudaSuccess) return bail(WIG_E_OOM, "cudaMalloc step inputs");
+        cudaMemset(ln.d_up, 0, b->up_bytes);
+        if (cudaMallocHost(&ln.h_up, b->up_bytes * RING) != cudaSuccess) return bail(WIG_E_OOM, "cudaMallocHost step inputs");
+        for (int r = 0; r < RING; r++)
+            if (cudaEventCreateWithFlags(&ln.up_ev[r], cudaEventDisableTiming) != cudaSuccess) return bail(WIG_E_CUDA, "event");
+        if (cudaMalloc(&ln.d_rsub, sizeof(Report) * n) != cudaSuccess) return bail(WIG_E_OOM, "cudaMalloc lane reports");
+        if (cudaMallocHost(&ln.h_rsub, sizeof(Report) * n) != cudaSuccess) return bail(WIG_E_OOM, "cudaMallocHost lane reports");
+        if (cudaStreamCreateWithFlags(&ln.cap, cudaStreamNonBlocking) != cudaSuccess) return bail(WIG_E_CUDA, "stream");
+        if (cudaStreamCreateWithFlags(&ln.cap2, cudaStreamNonBlocking) != cudaSuccess) return bail(WIG_E_CUDA, "stream");
+        wig::Batch& Bt = ln.Bt;
+        Bt.worlds = b->d_worlds;
+        Bt.items = ln.d_items;
+        Bt.count = ln.d_count;
+        for (uint32_t l = 0; l < wig::L_COUNT; l++) Bt.base[l] = base[l];
+        Bt.lbits = b->lbits;
+        Bt.max_cycles = 1;
+        Bt.cond = 0;
+        Bt.loop = ln.d_loop;
+        wig::SchedCtl& c = ln.ctl;
+        c.nsub = reinterpret_cast<const uint32_t*>(ln.d_up);
+        c.sub = reinterpret_cast<const uint32_t*>(ln.d_up + 8);
+        c.heads = reinterpret_cast<const wig::StepHead*>(ln.d_up + 8 + ((4u * (size_t)n + 7u) & ~(size_t)7u));
+        c.off = ln.d_off;
+        c.items = ln.d_items;
+        c.count = ln.d_count;
+        c.max_worlds = n;
+    }
+    *out = b;
+    return WIG_OK;
+}
+
+void destroy_batch(wig_batch* b) {
+    if (!b) return;
+    cudaDeviceSynchronize();
+    for (uint32_t li = 0; li < WIG_BATCH_LANES; li++) {
+        Lane& ln = b->lane[li];
+        drop_graphs(ln);
+        if (ln.d_items) cudaFree(ln.d_items);
+        if (ln.d_count) cudaFree(ln.d_count);
+        if (ln.d_off) cudaFree(ln.d_off);
+        if (ln.d_loop) cudaFree(ln.d_loop);
+        if (ln.d_up) cudaFree(ln.d_up);
+        if (ln.h_up) cudaFreeHost(ln.h_up);
+        for (int r = 0; r < RING; r++)
+            if (ln.up_ev[r]) cudaEventDestroy(ln.up_ev[r]);
+        if (ln.d_rsub) cudaFree(ln.d_rsub);
+        if (ln.h_rsub) cudaFreeHost(ln.h_rsub);
+        if (ln.cap) cudaStreamDestroy(ln.cap);
+        if (ln.cap2) cudaStreamDestroy(ln.cap2);
+    }
+    for (auto& o : b->own)
+        for (void* p : o)
+            if (p) cudaFree(p);
+    if (b->arena) cudaFree(b->arena);
+    if (b->scratch) cudaFree(b->scratch);
+    if (b->d_worlds) cudaFree(b->d_worlds);
+    if (b->d_elems) cudaFree(b->d_elems);
+    if (b->d_st) cudaFree(b->d_st);
+    if (b->d_report) cudaFree(b->d_report);
+    if (b->h_report) cudaFreeHost(b->h_report);
+    delete b;
+}
+
+// ---------------------------------------------------------------- recording
 
 // Per-pass timing of an eagerly launched step (the reference's per-phase
 // GPU timestamps, js/timer.js:7-98): events around each launch.
@@ -208,31 +525,51 @@ struct Prof {
 
 // Launch recording with optional per-launch events (Prof).
 struct Rec {
-    wig_fluid* h;
+    wig_batch* b;
+    Lane& ln;
     cudaStream_t s;
     Prof* prof;
     uint32_t launches = 0;
     cudaEvent_t pending = nullptr;
     template <class Fn>
     void timed(int id, Fn fn) {
-        cudaEvent_t a = nullptr, b = nullptr;
+        cudaEvent_t a = nullptr, e = nullptr;
         if (prof) {
             cudaEventCreate(&a);
-            cudaEventCreate(&b);
+            cudaEventCreate(&e);
             cudaEventRecord(a, s);
         }
         fn();
         launches++;
         if (prof) {
-            cudaEventRecord(b, s);
-            prof->marks.push_back({id, {a, b}});
+            cudaEventRecord(e, s);
+            prof->marks.push_back({id, {a, e}});
         }
     }
     void run(int pass, uint32_t level = 0, uint32_t cycle = 0) {
-        timed(pass, [&] { wig::launch_pass(h->D, pass, level, cycle, s); });
+        timed(pass, [&] { wig::launch_pass(ln.Bt, b->S, b->hw[0].D, pass, level, cycle, s); });
     }
     void norm(int which, uint32_t cycle) {
-        timed(WIG_SLOT_NORM, [&] { wig::launch_norm(h->D, which, cycle, s); });
+        timed(WIG_SLOT_NORM, [&] { wig::launch_norm(b->hw[0].D, which, cycle, s); });
+    }
+    void sched(int phase) {
+        cudaEvent_t a = nullptr, e = nullptr;
+        if (prof) {
+            cudaEventCreate(&a);
+            cudaEventCreate(&e);
+            cudaEventRecord(a, s);
+        }
+        wig::sched_lists(ln.Bt, ln.ctl, b->S, phase, s);
+        launches += 2;
+        if (prof) {
+            cudaEventRecord(e, s);
+            prof->marks.push_back({WIG_SLOT_SCHED, {a, e}});
+        }
+    }
+    void report() {
+        timed(WIG_SLOT_REPORT, [&] {
+            k_report<<<wig::list_grid(b->S, wig::L_ONE_ALL, 4), 32, 0, s>>>(ln.Bt, b->d_report, ln.d_rsub);
+        });
     }
     // the fast form's marker hook: events around each of its launches
     static void mark(void* ctx, int slot, int phase) {
@@ -250,12 +587,15 @@ struct Rec {
     }
 };
 
-// encodeFluid's passes before the solve (js/sim.js:2486-2521).
-void record_pre(Rec& R, uint32_t flags) {
+// encodeFluid's passes before the solve (js/sim.js:2486-2521), with the
+// work lists written at the step's start and after compact.
+void record_pre(Rec& R, bool viscous) {
+    R.sched(0);
     R.run(WIG_PASS_SYNC);
     R.run(WIG_PASS_SYNC_PARTICLES);
     R.run(WIG_PASS_SYNC_SEED);
     R.run(WIG_PASS_COMPACT);
+    R.sched(1);
     R.run(WIG_PASS_RETIRE);
     R.run(WIG_PASS_CLEAR);
     R.run(WIG_PASS_GATHER);
@@ -263,7 +603,7 @@ void record_pre(Rec& R, uint32_t flags) {
     R.run(WIG_PASS_SEAL_ANCHOR);
     R.run(WIG_PASS_CLASSIFY);
     R.run(WIG_PASS_SET_FACES);
-    if (flags & WIG_STEP_VISCOUS)
+    if (viscous)
         for (int i = 0; i < 8; i++) {
             R.run(WIG_PASS_VISCOSITY_RED);
             R.run(WIG_PASS_VISCOSITY_BLACK);
@@ -286,23 +626,28 @@ void record_post(Rec& R) {
     R.run(WIG_PASS_RASTER_CLAIMS);
     R.run(WIG_PASS_RASTER);
     R.run(WIG_PASS_UNPAINT);
-    R.timed(WIG_SLOT_REPORT, [&] { k_report<<<1, 32, 0, R.s>>>(R.h->D, R.h->d_report); });
+    R.report();
 }
 
-// Records the plain form's step (one kernel per reference pass, every
-// iteration encoded) on stream s; returns the number of kernels launched.
-uint32_t record_step(wig_fluid* h, uint32_t max_cycles, uint32_t flags, bool shifted, cudaStream_t s, Prof* prof) {
-    Rec R{h, s, prof};
+// A single world's bookkeeping-only step (js/sim.js:2480-2485).
+uint32_t record_book(Rec& R) {
+    R.sched(0);
+    R.run(WIG_PASS_SYNC_MARKS);
+    R.run(WIG_PASS_COMPACT);
+    R.sched(1);
+    R.run(WIG_PASS_RETIRE);
+    R.report();
+    return R.launches;
+}
+
+// Records the plain form's step of world 0 (one kernel per reference pass,
+// every iteration encoded) on stream s; returns the kernels launched.
+uint32_t record_step(wig_batch* b, Lane& ln, uint32_t max_cycles, uint32_t flags, bool shifted, cudaStream_t s, Prof* prof) {
+    Rec R{b, ln, s, prof};
     const bool tol = (flags & WIG_STEP_TOLERANCE) != 0u;
-    if (flags & WIG_STEP_BOOKKEEPING_ONLY) {
-        R.run(WIG_PASS_SYNC_MARKS);
-        R.run(WIG_PASS_COMPACT);
-        R.run(WIG_PASS_RETIRE);
-        R.timed(WIG_SLOT_REPORT, [&] { k_report<<<1, 32, 0, s>>>(h->D, h->d_report); });
-        return R.launches;
-    }
-    record_pre(R, flags);
-    const uint32_t deepest = h->L.levels;
+    if (flags & WIG_STEP_BOOKKEEPING_ONLY) return record_book(R);
+    record_pre(R, (flags & WIG_STEP_VISCOUS) != 0u);
+    const uint32_t deepest = b->L[0].levels;
     R.run(WIG_PASS_CG_START);
     R.run(WIG_PASS_CG_JOIN);
     R.run(WIG_PASS_CG_ANCHOR);
@@ -344,32 +689,37 @@ uint32_t record_step(wig_fluid* h, uint32_t max_cycles, uint32_t flags, bool shi
     return R.launches;
 }
 
-wig::Fast fast_of(wig_fluid* h, uint32_t max_cycles, unsigned long long cond) {
-    wig::Fast F = h->F;
-    F.D = h->D;
-    F.max_cycles = max_cycles;
-    F.cond = cond;
-    return F;
-}
-
-// Records the fast form's step.  With `capture`, s is capturing into a graph
-// and the iterations become a WHILE node whose body is captured on h->cap2;
-// else the iterations are launched from the host, each decided by reading
-// back the device's verdict (the profiler's path).  *outside gets the kernels
-// outside the loop (all of them when not capturing), *body those of one
-// iteration of the loop.
-int record_step_fast(wig_fluid* h, uint32_t max_cycles, uint32_t flags, bool shifted, cudaStream_t s, Prof* prof,
-                     bool capture, uint32_t* outside, uint32_t* body) {
-    Rec R{h, s, prof};
-    record_pre(R, flags);
+// Records the fast form's step of the lane's worlds.  With `capture`, s is
+// capturing into a graph and the iterations become a WHILE node whose body
+// is captured on the lane's second stream; else the iterations are launched
+// from the host, each decided by reading back the device's verdict (the
+// profiler's path).  *outside gets the kernels outside the loop (all of
+// them when not capturing), *body those of one iteration of the loop.  The
+// persistent form (one world) runs the iterations in one cooperative kernel.
+int record_step_fast(wig_batch* b, Lane& ln, uint32_t max_cycles, uint32_t flags, bool shifted, cudaStream_t s,
+                     Prof* prof, bool capture, uint32_t* outside, uint32_t* body) {
+    Rec R{b, ln, s, prof};
+    if ((flags & WIG_STEP_BOOKKEEPING_ONLY) && b->K == 1) {
+        *outside = record_book(R);
+        *body = 0;
+        return WIG_OK;
+    }
+    record_pre(R, (flags & WIG_STEP_VISCOUS) != 0u);
     R.run(WIG_PASS_CG_START);
     R.run(WIG_PASS_CG_JOIN);
     R.run(WIG_PASS_CG_ANCHOR);
     wig::Marker mk{&Rec::mark, &R};
-    const wig::Fast F0 = fast_of(h, max_cycles, 0ull);
-    wig::fast_setup(F0, s, prof ? &mk : nullptr);
+    ln.Bt.max_cycles = max_cycles;
+    ln.Bt.cond = 0;
+    wig::fast_setup(ln.Bt, b->S, s, prof ? &mk : nullptr);
     R.launches++;
     if (flags & WIG_STEP_PERSISTENT) {
+        wig::Fast F0;
+        static_cast<wig::FastW&>(F0) = b->hw[0].S;
+        F0.D = b->hw[0].D;
+        F0.max_cycles = max_cycles;
+        F0.solve_grid = b->solve_grid;
+        if (F0.solve_grid == 0u) return fail(WIG_E_STATE, "no grid for the persistent solve");
         CUDA_TRY(wig::fast_solve(F0, shifted, s, prof ? &mk : nullptr));
         R.launches++;
         *body = 0;
@@ -390,32 +740,273 @@ int record_step_fast(wig_fluid* h, uint32_t max_cycles, uint32_t flags, bool shi
         CUDA_TRY(cudaGraphAddNode(&cnode, g, deps, nd, &cp));
         CUDA_TRY(cudaStreamUpdateCaptureDependencies(s, &cnode, 1, cudaStreamSetCaptureDependencies));
         cudaGraph_t bodyGraph = cp.conditional.phGraph_out[0];
-        CUDA_TRY(cudaStreamBeginCaptureToGraph(h->cap2, bodyGraph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-        const wig::Fast F = fast_of(h, max_cycles, (unsigned long long)handle);
-        *body = wig::fast_cycle(F, shifted, h->cap2, nullptr);
+        CUDA_TRY(cudaStreamBeginCaptureToGraph(ln.cap2, bodyGraph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
+        wig::Batch Bc = ln.Bt;
+        Bc.cond = (unsigned long long)handle;
+        *body = wig::fast_cycle(Bc, b->S, ln.cap2, nullptr);
         cudaGraph_t captured = nullptr;
-        CUDA_TRY(cudaStreamEndCapture(h->cap2, &captured));
+        CUDA_TRY(cudaStreamEndCapture(ln.cap2, &captured));
     } else {
-        uint32_t* cont = &h->h_report->pad;
+        uint32_t* cont = reinterpret_cast<uint32_t*>(ln.h_rsub);  // a word of pinned scratch
         for (uint32_t c = 0; c < max_cycles; c++) {
-            R.launches += wig::fast_cycle(F0, shifted, s, prof ? &mk : nullptr);
-            CUDA_TRY(cudaMemcpyAsync(cont, &h->d_st->cont, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
+            R.launches += wig::fast_cycle(ln.Bt, b->S, s, prof ? &mk : nullptr);
+            CUDA_TRY(cudaMemcpyAsync(cont, ln.d_loop, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
             CUDA_TRY(cudaStreamSynchronize(s));
             if (!*cont) break;
         }
         *body = 0;
     }
-    wig::fast_finish(F0, s, prof ? &mk : nullptr);
+    wig::fast_finish(ln.Bt, b->S, s, prof ? &mk : nullptr);
     R.launches++;
     record_post(R);
     *outside = R.launches;
     return WIG_OK;
 }
 
-bool step_parity(wig_fluid* h, uint32_t flags) {
-    if (flags & WIG_STEP_SHIFTED_SET) return (flags & WIG_STEP_SHIFTED_FIRST) != 0u;
-    if (!(flags & WIG_STEP_BOOKKEEPING_ONLY)) h->shifted_first = !h->shifted_first;
-    return h->shifted_first;
+// ---------------------------------------------------------------- stepping
+
+struct StepArgs {
+    uint32_t lane;
+    const uint32_t* worlds;
+    uint32_t count;
+    const wig_params* P;
+    const uint32_t* world_flags;  // null: `flags`' per-world bits for all
+    uint32_t max_cycles;
+    uint32_t flags;
+    double tol;
+    cudaStream_t s;
+};
+
+constexpr uint32_t WORLD_BITS = WIG_STEP_BOOKKEEPING_ONLY | WIG_STEP_VISCOUS | WIG_STEP_SHIFTED_SET | WIG_STEP_SHIFTED_FIRST;
+
+int check_step(wig_batch* b, const StepArgs& a) {
+    if (!b || !a.worlds || !a.P) return fail(WIG_E_ARG, "null argument");
+    if (a.lane >= WIG_BATCH_LANES) return fail(WIG_E_ARG, "lane out of range");
+    if (a.count == 0 || a.count > b->K) return fail(WIG_E_ARG, "world count out of range");
+    if (a.max_cycles == 0 || a.max_cycles > 64) return fail(WIG_E_ARG, "max_cycles out of range (1..64)");
+    if ((a.flags & WIG_STEP_TOLERANCE) && !(a.tol > 0.0)) return fail(WIG_E_ARG, "tolerance must be positive");
+    if ((a.flags & (WIG_STEP_PLAIN | WIG_STEP_PERSISTENT)) && b->K != 1)
+        return fail(WIG_E_ARG, "the plain and persistent forms step one world");
+    std::vector<char> seen(b->K, 0);
+    for (uint32_t i = 0; i < a.count; i++) {
+        const uint32_t k = a.worlds[i];
+        if (k >= b->K) return fail(WIG_E_ARG, "world index out of range");
+        if (seen[k]) return fail(WIG_E_ARG, "a world listed twice");
+        seen[k] = 1;
+        if (!b->bound[k]) return fail(WIG_E_STATE, "buffers not bound");
+    }
+    return WIG_OK;
+}
+
+// Writes the step's inputs into the lane's next pinned slot and copies them
+// to the device; returns the batch-wide viscous bit and (one world) the
+// tiling parity of its step.
+int push_inputs(wig_batch* b, Lane& ln, const StepArgs& a, bool* viscous, bool* shifted0) {
+    const int r = ln.up_at;
+    ln.up_at = (ln.up_at + 1) % RING;
+    CUDA_TRY(cudaEventSynchronize(ln.up_ev[r]));
+    char* slot = ln.h_up + b->up_bytes * r;
+    const size_t sub_bytes = (4u * (size_t)b->K + 7u) & ~(size_t)7u;
+    uint32_t* hdr = reinterpret_cast<uint32_t*>(slot);
+    uint32_t* sub = reinterpret_cast<uint32_t*>(slot + 8);
+    wig::StepHead* heads = reinterpret_cast<wig::StepHead*>(slot + 8 + sub_bytes);
+    hdr[0] = a.count;
+    hdr[1] = 0u;
+    *viscous = false;
+    *shifted0 = false;
+    for (uint32_t i = 0; i < a.count; i++) {
+        const uint32_t k = a.worlds[i];
+        const uint32_t wf = (a.world_flags ? a.world_flags[i] : a.flags) & WORLD_BITS;
+        sub[i] = k;
+        wig::StepHead& h = heads[i];
+        std::memset(&h, 0, sizeof(h));
+        h.P = a.P[i];
+        h.P.size[0] = b->L[k].width;
+        h.P.size[1] = b->L[k].height;
+        h.tol_mode = (a.flags & WIG_STEP_TOLERANCE) ? 1u : 0u;
+        h.f64 = (a.flags & WIG_STEP_F64_DOTS) ? 1u : 0u;
+        h.book = (wf & WIG_STEP_BOOKKEEPING_ONLY) ? 1u : 0u;
+        h.viscous = (wf & WIG_STEP_VISCOUS) ? 1u : 0u;
+        bool sh;
+        if (wf & WIG_STEP_SHIFTED_SET) {
+            sh = (wf & WIG_STEP_SHIFTED_FIRST) != 0u;
+        } else {
+            if (!h.book) b->shifted_first[k] = !b->shifted_first[k];
+            sh = b->shifted_first[k] != 0;
+        }
+        h.shift_first = sh ? 1u : 0u;
+        h.tol = a.tol;
+        *viscous = *viscous || h.viscous;
+        if (i == 0) *shifted0 = sh;
+    }
+    const size_t bytes = 8u + sub_bytes + sizeof(wig::StepHead) * a.count;
+    // the heads sit after the full sub array, so copy the slot's prefix
+    // through the last head written
+    CUDA_TRY(cudaMemcpyAsync(ln.d_up, slot, bytes, cudaMemcpyHostToDevice, a.s));
+    CUDA_TRY(cudaEventRecord(ln.up_ev[r], a.s));
+    return WIG_OK;
+}
+
+// Level 0 of the listed worlds whose buffers the host has written since
+// their last step, zeroed (the fast form's invariant).
+void zero_dirty(wig_batch* b, const StepArgs& a) {
+    for (uint32_t i = 0; i < a.count; i++) {
+        const uint32_t k = a.worlds[i];
+        if (!b->dirty[k]) continue;
+        wig::fast_zero_level0(b->hw[k].S, b->hw[k].D.C, a.s);
+        b->dirty[k] = 0;
+    }
+}
+
+int batch_step(wig_batch* b, const StepArgs& a) {
+    int rc = check_step(b, a);
+    if (rc) return rc;
+    Lane& ln = b->lane[a.lane];
+    bool viscous = false, sh = false;
+    rc = push_inputs(b, ln, a, &viscous, &sh);
+    if (rc) return rc;
+    const bool plain = (a.flags & WIG_STEP_PLAIN) != 0u;
+    if (!plain) zero_dirty(b, a);
+    const bool book1 = b->K == 1 && ((a.world_flags ? a.world_flags[0] : a.flags) & WIG_STEP_BOOKKEEPING_ONLY) != 0u;
+    uint32_t shape = a.flags & (WIG_STEP_TOLERANCE | WIG_STEP_F64_DOTS | WIG_STEP_PLAIN | WIG_STEP_PERSISTENT);
+    if (viscous) shape |= WIG_STEP_VISCOUS;
+    if (book1) shape |= WIG_STEP_BOOKKEEPING_ONLY;
+    const bool parity_keyed = plain || (a.flags & WIG_STEP_PERSISTENT);
+    const uint64_t key = ((uint64_t)a.max_cycles << 32) | ((uint64_t)shape << 1) | ((parity_keyed && sh) ? 1u : 0u);
+    auto it = ln.graphs.find(key);
+    if (it == ln.graphs.end()) {
+        Graph G;
+        CUDA_TRY(cudaStreamBeginCapture(ln.cap, cudaStreamCaptureModeThreadLocal));
+        uint32_t n = 0, nb = 0;
+        if (plain) {
+            n = record_step(b, ln, a.max_cycles, shape, sh, ln.cap, nullptr);
+        } else {
+            int rc2 = record_step_fast(b, ln, a.max_cycles, shape, sh, ln.cap, nullptr, true, &n, &nb);
+            if (rc2) {
+                std::string m = g_last_error;
+                cudaGraph_t junk = nullptr;
+                cudaStreamEndCapture(ln.cap, &junk);
+                if (junk) cudaGraphDestroy(junk);
+                return fail(rc2, m);
+            }
+        }
+        cudaError_t e = cudaStreamEndCapture(ln.cap, &G.g);
+        if (e != cudaSuccess) return fail(WIG_E_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&G.ge, G.g, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(G.g);
+            return fail(WIG_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        }
+        G.outside = n;
+        G.body = nb;
+        it = ln.graphs.emplace(key, G).first;
+    }
+    ln.last_launches = it->second.outside;
+    ln.last_body = it->second.body;
+    CUDA_TRY(cudaGraphLaunch(it->second.ge, a.s));
+    if (a.flags & WIG_STEP_SYNC_STATS)
+        CUDA_TRY(cudaMemcpyAsync(ln.h_rsub, ln.d_rsub, sizeof(Report) * a.count, cudaMemcpyDeviceToHost, a.s));
+    ln.last_stream = a.s;
+    for (uint32_t i = 0; i < a.count; i++) {
+        b->stepped_on[a.worlds[i]] = a.s;
+        b->stepped_lane[a.worlds[i]] = (int)a.lane;
+    }
+    return WIG_OK;
+}
+
+int batch_step_profile(wig_batch* b, const StepArgs& a, float* ms_out, uint32_t* calls_out) {
+    if (!ms_out || !calls_out) return fail(WIG_E_ARG, "null argument");
+    int rc = check_step(b, a);
+    if (rc) return rc;
+    Lane& ln = b->lane[a.lane];
+    bool viscous = false, sh = false;
+    rc = push_inputs(b, ln, a, &viscous, &sh);
+    if (rc) return rc;
+    const bool plain = (a.flags & WIG_STEP_PLAIN) != 0u;
+    const bool book1 = b->K == 1 && ((a.world_flags ? a.world_flags[0] : a.flags) & WIG_STEP_BOOKKEEPING_ONLY) != 0u;
+    uint32_t shape = a.flags & (WIG_STEP_TOLERANCE | WIG_STEP_F64_DOTS | WIG_STEP_PLAIN | WIG_STEP_PERSISTENT);
+    if (viscous) shape |= WIG_STEP_VISCOUS;
+    if (book1) shape |= WIG_STEP_BOOKKEEPING_ONLY;
+    Prof prof;
+    ln.last_body = 0;
+    if (plain) {
+        ln.last_launches = record_step(b, ln, a.max_cycles, shape, sh, a.s, &prof);
+    } else {
+        zero_dirty(b, a);
+        uint32_t n = 0, nb = 0;
+        rc = record_step_fast(b, ln, a.max_cycles, shape, sh, a.s, &prof, false, &n, &nb);
+        if (rc) return rc;
+        ln.last_launches = n;
+    }
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(a.s));
+    for (int k = 0; k < WIG_PROFILE_SLOTS; k++) { ms_out[k] = 0.0f; calls_out[k] = 0u; }
+    for (auto& m : prof.marks) {
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, m.second.first, m.second.second);
+        ms_out[m.first] += ms;
+        calls_out[m.first] += 1u;
+        cudaEventDestroy(m.second.first);
+        cudaEventDestroy(m.second.second);
+    }
+    ln.last_stream = a.s;
+    for (uint32_t i = 0; i < a.count; i++) {
+        b->stepped_on[a.worlds[i]] = a.s;
+        b->stepped_lane[a.worlds[i]] = (int)a.lane;
+    }
+    return WIG_OK;
+}
+
+int batch_read_stats(wig_batch* b, const uint32_t* worlds, uint32_t count, wig_fluid_stats* out) {
+    if (!b || !worlds || !out) return fail(WIG_E_ARG, "null argument");
+    std::vector<cudaStream_t> waited;
+    for (uint32_t i = 0; i < count; i++) {
+        if (worlds[i] >= b->K) return fail(WIG_E_ARG, "world index out of range");
+        cudaStream_t s = b->stepped_on[worlds[i]];
+        bool done = false;
+        for (cudaStream_t w : waited) done = done || w == s;
+        if (!done) {
+            CUDA_TRY(cudaStreamSynchronize(s));
+            waited.push_back(s);
+        }
+    }
+    int rc = WIG_OK;
+    for (uint32_t i = 0; i < count; i++) {
+        const uint32_t k = worlds[i];
+        CUDA_TRY(cudaMemcpy(&b->h_report[k], &b->d_report[k], sizeof(Report), cudaMemcpyDeviceToHost));
+        const Report& r = b->h_report[k];
+        wig_fluid_stats& o = out[i];
+        std::memset(&o, 0, sizeof(o));
+        for (uint32_t c = 0; c < WIG_FLUID_STATS; c++) o.count[c] = r.count[c];
+        o.particles = r.particles;
+        o.cycles = r.count[WIG_COUNT_CYCLES];
+        const int li = b->stepped_lane[k];
+        if (li >= 0) o.launches = b->lane[li].last_launches + b->lane[li].last_body * r.count[WIG_COUNT_CYCLES];
+        o.rel_residual = r.rel;
+        o.b_norm = r.bnorm2 > 0.0 ? __builtin_sqrt(r.bnorm2) : 0.0;
+        if (rc == WIG_OK) {
+            if (r.err & wig::ERR_BARRIER) rc = fail(WIG_E_STATE, "the persistent solve's grid barrier waited past its limit");
+            else if (r.err) rc = fail(WIG_E_STATE, "a device loop hit its iteration limit (union-find)");
+            else if (r.particles > b->L[k].capacity) rc = fail(WIG_E_CAPACITY, "more particles than the buffers hold");
+        }
+    }
+    return rc;
+}
+
+int copy_world(wig_batch* b, uint32_t k, int which, void* host, uint64_t offset, uint64_t bytes, void* stream, bool up) {
+    if (!b || !host) return fail(WIG_E_ARG, "null argument");
+    if (k >= b->K) return fail(WIG_E_ARG, "world index out of range");
+    if (!b->bound[k]) return fail(WIG_E_STATE, "buffers not bound");
+    uint64_t size = buffer_bytes(b->L[k], which);
+    if (!size || offset > size || bytes > size - offset)
+        return fail(WIG_E_ARG, up ? "upload out of the buffer's range" : "download out of the buffer's range");
+    cudaStream_t s = (cudaStream_t)stream;
+    char* dev = (char*)*buffer_slot(b->hw[k].D, which) + offset;
+    if (up) CUDA_TRY(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, s));
+    else CUDA_TRY(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (up) b->dirty[k] = 1;
+    return WIG_OK;
 }
 
 }  // namespace
@@ -431,321 +1022,201 @@ int wig_fluid_layout(const wig_world_desc* d, wig_world_layout* out) { return la
 int wig_fluid_create(const wig_world_desc* d, const wig_elem* elems, uint32_t n_elems, wig_fluid** out) {
     if (!out) return fail(WIG_E_ARG, "null output handle");
     *out = nullptr;
-    if (!elems || n_elems == 0 || n_elems > WIG_MAX_ELEMS) return fail(WIG_E_ARG, "element table empty or too long");
-    if (n_elems <= WIG_ELEM_WATER) return fail(WIG_E_ARG, "element table must reach WATER (id 3)");
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-        cudaGetLastError();
-        return fail(WIG_E_NO_DEVICE, "no CUDA device");
-    }
+    if (!d) return fail(WIG_E_ARG, "null descriptor");
     wig_fluid* h = new (std::nothrow) wig_fluid();
     if (!h) return fail(WIG_E_OOM, "host allocation failed");
-    int rc = layout_of(d, &h->L);
-    if (rc) { delete h; return rc; }
-    cudaGetDevice(&h->device);
-    const wig_world_layout& L = h->L;
-    wig::Dev& D = h->D;
-    D.W = (int)L.width;
-    D.H = (int)L.height;
-    D.C = L.cell_count;
-    D.F = L.face_count;
-    D.B = L.block_count;
-    D.BW = L.blocks_wide;
-    D.BH = L.block_count / L.blocks_wide;
-    D.cap = L.capacity;
-    D.ppc = L.liquid_per_cell;
-    D.edge_tiles = L.edge_tiles;
-    D.levels = L.levels;
-    D.level_w[0] = L.width;
-    D.level_h[0] = L.height;
-    uint32_t at = 2u * D.C + D.F + 2u * ((D.F + 3u) / 4u);
-    D.level_start[0] = 0;
-    for (uint32_t l = 1; l <= WIG_MG_LEVELS; l++) {
-        D.level_w[l] = l <= L.levels ? L.level_w[l - 1] : 0u;
-        D.level_h[l] = l <= L.levels ? L.level_h[l - 1] : 0u;
-        D.level_start[l] = at;
-        at += 2u * D.level_w[l] * D.level_h[l];
-    }
-    D.n_elems = n_elems;
-    auto cleanup = [&](int code, const std::string& m) {
-        wig_fluid_destroy(h);
-        return fail(code, m);
-    };
-    if (cudaMalloc(&h->d_elems, sizeof(wig_elem) * n_elems) != cudaSuccess) return cleanup(WIG_E_OOM, "cudaMalloc elems");
-    if (cudaMemcpy(h->d_elems, elems, sizeof(wig_elem) * n_elems, cudaMemcpyHostToDevice) != cudaSuccess)
-        return cleanup(WIG_E_CUDA, "cudaMemcpy elems");
-    D.elems = h->d_elems;
-    if (cudaMalloc(&h->d_st, sizeof(wig::StepState)) != cudaSuccess) return cleanup(WIG_E_OOM, "cudaMalloc step state");
-    cudaMemset(h->d_st, 0, sizeof(wig::StepState));
-    D.st = h->d_st;
-    if (cudaMallocHost(&h->h_st, sizeof(wig::StepState) * RING) != cudaSuccess) return cleanup(WIG_E_OOM, "cudaMallocHost");
-    for (int k = 0; k < RING; k++)
-        if (cudaEventCreateWithFlags(&h->st_ev[k], cudaEventDisableTiming) != cudaSuccess) return cleanup(WIG_E_CUDA, "event");
-    if (cudaMalloc(&h->d_report, sizeof(Report)) != cudaSuccess) return cleanup(WIG_E_OOM, "cudaMalloc report");
-    cudaMemset(h->d_report, 0, sizeof(Report));
-    if (cudaMallocHost(&h->h_report, sizeof(Report)) != cudaSuccess) return cleanup(WIG_E_OOM, "cudaMallocHost report");
-    std::memset(h->h_report, 0, sizeof(Report));
-    if (cudaMalloc(&h->d_part64, sizeof(double) * 2 * D.B) != cudaSuccess) return cleanup(WIG_E_OOM, "cudaMalloc part64");
-    if (cudaMalloc(&h->d_norm64, sizeof(double) * 2 * D.B) != cudaSuccess) return cleanup(WIG_E_OOM, "cudaMalloc norm64");
-    cudaMemset(h->d_part64, 0, sizeof(double) * 2 * D.B);
-    cudaMemset(h->d_norm64, 0, sizeof(double) * 2 * D.B);
-    D.part64 = h->d_part64;
-    D.norm64 = h->d_norm64;
-    if (cudaStreamCreateWithFlags(&h->cap, cudaStreamNonBlocking) != cudaSuccess) return cleanup(WIG_E_CUDA, "stream");
-    if (cudaStreamCreateWithFlags(&h->cap2, cudaStreamNonBlocking) != cudaSuccess) return cleanup(WIG_E_CUDA, "stream");
-    {
-        // the fast form's scratch: level 0 (17 floats and a byte a cell), the
-        // coarse levels (10 floats a cell), the block partials
-        auto align = [](size_t x) { return (x + 255u) & ~(size_t)255u; };
-        const size_t C = D.C;
-        size_t bytes = align(C) + 17u * align(C * 4u);
-        for (uint32_t l = 1; l <= D.levels; l++) bytes += 10u * align((size_t)D.level_w[l] * D.level_h[l] * 4u);
-        bytes += align(2u * (size_t)D.B * 4u) + align(2u * (size_t)D.B * 8u);
-        if (cudaMalloc(&h->fast_mem, bytes) != cudaSuccess) return cleanup(WIG_E_OOM, "cudaMalloc fast scratch");
-        cudaMemset(h->fast_mem, 0, bytes);
-        char* p = static_cast<char*>(h->fast_mem);
-        auto take = [&](size_t n) { char* q = p; p += align(n); return q; };
-        wig::Fast& F = h->F;
-        F.fmask = reinterpret_cast<uint8_t*>(take(C));
-        auto fl = [&](size_t n) { return reinterpret_cast<float*>(take(n * 4u)); };
-        for (uint32_t l = 0; l <= D.levels; l++) {
-            const size_t n = l == 0 ? C : (size_t)D.level_w[l] * D.level_h[l];
-            wig::Lvl& V = F.L[l];
-            V.px = fl(n); V.py = fl(n); V.rx = fl(n); V.ry = fl(n); V.rho = fl(n);
-            V.b0 = fl(n); V.b1 = fl(n); V.b2 = fl(n); V.b3 = fl(n); V.diag = fl(n);
-        }
-        F.pin = fl(C); F.rimx = fl(C); F.rimy = fl(C);
-        F.X = fl(C); F.R = fl(C); F.P = fl(C); F.Q = fl(C);
-        F.part32 = fl(2u * (size_t)D.B);
-        F.part64 = reinterpret_cast<double*>(take(2u * (size_t)D.B * 8u));
-        F.lc = D.levels;
-        for (uint32_t l = 1; l <= D.levels; l++)
-            if ((size_t)D.level_w[l] * D.level_h[l] <= wig::COARSE_CTA_CELLS) { F.lc = l; break; }
-        F.lp = D.levels;
-        for (uint32_t l = 1; l <= D.levels; l++)
-            if ((size_t)D.level_w[l] * D.level_h[l] <= wig::PERSISTENT_CTA_CELLS) { F.lp = l; break; }
-        F.D = D;
-        size_t smem = wig::fast_coarse_smem(F);
-        if (smem > 200u * 1024u) return cleanup(WIG_E_ARG, "coarse levels too large for one CTA");
-        if (wig::fast_prepare_attributes(smem) != cudaSuccess) return cleanup(WIG_E_CUDA, "cudaFuncSetAttribute");
-        if (wig::fast_solve_grid(F, &F.solve_grid) != cudaSuccess) return cleanup(WIG_E_CUDA, "occupancy of the persistent solve");
-        h->fast_dirty = true;
+    int rc = make_batch(d, 1, elems, n_elems, false, &h->b);
+    if (rc) {
+        delete h;
+        return rc;
     }
     *out = h;
-
     return WIG_OK;
 }
 
-int wig_fluid_bind(wig_fluid* h, const wig_fluid_buffers* b) {
-    if (!h) return fail(WIG_E_ARG, "null handle");
-    drop_graphs(h);
+int wig_fluid_bind(wig_fluid* h, const wig_fluid_buffers* bufs) {
+    if (!h || !h->b) return fail(WIG_E_ARG, "null handle");
+    wig_batch* b = h->b;
+    for (auto& ln : b->lane) drop_graphs(ln);
     void* given[7] = {nullptr};
-    if (b) {
-        given[0] = b->cells; given[1] = b->sorted; given[2] = b->parts; given[3] = b->counters;
-        given[4] = b->field; given[5] = b->blocks; given[6] = b->cg;
+    if (bufs) {
+        given[0] = bufs->cells; given[1] = bufs->sorted; given[2] = bufs->parts; given[3] = bufs->counters;
+        given[4] = bufs->field; given[5] = bufs->blocks; given[6] = bufs->cg;
     }
+    wig::Dev& D = b->hw[0].D;
     for (int k = 0; k < 7; k++) {
-        void** slot = buffer_slot(h, k);
+        void** slot = buffer_slot(D, k);
         if (given[k]) {
             if (((uintptr_t)given[k] & 15u) != 0u) return fail(WIG_E_ARG, "buffer not 16-byte aligned");
-            if (h->own[k]) { cudaFree(h->own[k]); h->own[k] = nullptr; }
+            if (b->own[0][k]) { cudaFree(b->own[0][k]); b->own[0][k] = nullptr; }
             *slot = given[k];
-        } else if (!h->own[k]) {
-            uint64_t bytes = buffer_bytes(h->L, k);
+        } else if (!b->own[0][k]) {
+            uint64_t bytes = buffer_bytes(b->L[0], k);
             void* p = nullptr;
             if (cudaMalloc(&p, bytes) != cudaSuccess) {
                 cudaGetLastError();
                 return fail(WIG_E_OOM, "cudaMalloc of a world buffer failed");
             }
             CUDA_TRY(cudaMemset(p, 0, bytes));
-            h->own[k] = p;
+            b->own[0][k] = p;
             *slot = p;
         }
     }
-    h->bound = true;
-    h->fast_dirty = true;
+    int rc = upload_world_entry(b, 0);
+    if (rc) return rc;
+    b->bound[0] = 1;
+    b->dirty[0] = 1;
     return WIG_OK;
 }
 
 int wig_fluid_buffers_of(wig_fluid* h, wig_fluid_buffers* out) {
-    if (!h || !out) return fail(WIG_E_ARG, "null argument");
-    if (!h->bound) return fail(WIG_E_STATE, "buffers not bound");
-    out->cells = h->D.cells; out->sorted = h->D.sorted; out->parts = h->D.parts; out->counters = h->D.counters;
-    out->field = h->D.field; out->blocks = h->D.blocks; out->cg = h->D.cg;
-    return WIG_OK;
+    if (!h || !h->b) return fail(WIG_E_ARG, "null argument");
+    return wig_batch_buffers_of(h->b, 0, out);
 }
 
 int wig_fluid_upload(wig_fluid* h, int which, const void* host, uint64_t offset, uint64_t bytes, void* stream) {
-    if (!h || !host) return fail(WIG_E_ARG, "null argument");
-    if (!h->bound) return fail(WIG_E_STATE, "buffers not bound");
-    uint64_t size = buffer_bytes(h->L, which);
-    if (!size || offset > size || bytes > size - offset) return fail(WIG_E_ARG, "upload out of the buffer's range");
-    cudaStream_t s = (cudaStream_t)stream;
-    CUDA_TRY(cudaMemcpyAsync((char*)*buffer_slot(h, which) + offset, host, bytes, cudaMemcpyHostToDevice, s));
-    CUDA_TRY(cudaStreamSynchronize(s));
-    h->fast_dirty = true;
-    return WIG_OK;
+    if (!h || !h->b) return fail(WIG_E_ARG, "null argument");
+    return copy_world(h->b, 0, which, const_cast<void*>(host), offset, bytes, stream, true);
 }
 
 int wig_fluid_download(wig_fluid* h, int which, void* host, uint64_t offset, uint64_t bytes, void* stream) {
-    if (!h || !host) return fail(WIG_E_ARG, "null argument");
-    if (!h->bound) return fail(WIG_E_STATE, "buffers not bound");
-    uint64_t size = buffer_bytes(h->L, which);
-    if (!size || offset > size || bytes > size - offset) return fail(WIG_E_ARG, "download out of the buffer's range");
-    cudaStream_t s = (cudaStream_t)stream;
-    CUDA_TRY(cudaMemcpyAsync(host, (const char*)*buffer_slot(h, which) + offset, bytes, cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaStreamSynchronize(s));
-    return WIG_OK;
+    if (!h || !h->b) return fail(WIG_E_ARG, "null argument");
+    return copy_world(h->b, 0, which, host, offset, bytes, stream, false);
 }
 
 int wig_fluid_dispatch(wig_fluid* h, const wig_params* P, int pass, uint32_t level, uint32_t cycle, void* stream) {
-    if (!h || !P) return fail(WIG_E_ARG, "null argument");
-    if (!h->bound) return fail(WIG_E_STATE, "buffers not bound");
+    if (!h || !h->b || !P) return fail(WIG_E_ARG, "null argument");
+    wig_batch* b = h->b;
+    if (!b->bound[0]) return fail(WIG_E_STATE, "buffers not bound");
     if (pass < 0 || pass >= WIG_PASS_COUNT) return fail(WIG_E_ARG, "unknown pass");
-    if (level > h->L.levels) return fail(WIG_E_ARG, "level past the coarsest");
+    if (level > b->L[0].levels) return fail(WIG_E_ARG, "level past the coarsest");
     cudaStream_t s = (cudaStream_t)stream;
-    int rc = push_state(h, P, 0u, 0.0, s, true);
-    if (rc) return rc;
-    rc = wig::launch_pass(h->D, pass, level, cycle, s);
+    Lane& ln = b->lane[0];
+    // the pass runs as asked: Params written, world 0 the whole subset, not
+    // bookkeeping-only, with its viscosity sweeps
+    wig_params p = *P;
+    p.size[0] = b->L[0].width;
+    p.size[1] = b->L[0].height;
+    const int r = ln.up_at;
+    ln.up_at = (ln.up_at + 1) % RING;
+    CUDA_TRY(cudaEventSynchronize(ln.up_ev[r]));
+    char* slot = ln.h_up + b->up_bytes * r;
+    uint32_t* hdr = reinterpret_cast<uint32_t*>(slot);
+    hdr[0] = 1u;
+    hdr[1] = 0u;
+    hdr[2] = 0u;
+    std::memcpy(slot + 16, &p, sizeof(p));
+    const uint32_t flags2[2] = {0u, 1u};  // book, viscous
+    std::memcpy(slot + 16 + sizeof(p), flags2, sizeof(flags2));
+    CUDA_TRY(cudaMemcpyAsync(ln.d_up, slot, 12, cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(&b->d_st[0].P, slot + 16, sizeof(p), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaMemcpyAsync(&b->d_st[0].book, slot + 16 + sizeof(p), sizeof(flags2), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaEventRecord(ln.up_ev[r], s));
+    wig::SchedCtl c = ln.ctl;
+    c.heads = nullptr;
+    wig::sched_lists(ln.Bt, c, b->S, 0, s);
+    wig::sched_lists(ln.Bt, c, b->S, 1, s);
+    int rc = wig::launch_pass(ln.Bt, b->S, b->hw[0].D, pass, level, cycle, s);
     if (rc) return fail(rc, "launch");
     CUDA_TRY(cudaGetLastError());
-    h->last_stream = s;
+    ln.last_stream = s;
+    b->stepped_on[0] = s;
     return WIG_OK;
 }
 
 int wig_fluid_step(wig_fluid* h, const wig_params* P, uint32_t max_cycles, uint32_t flags, double tolerance, void* stream) {
-    if (!h || !P) return fail(WIG_E_ARG, "null argument");
-    if (!h->bound) return fail(WIG_E_STATE, "buffers not bound");
-    if (max_cycles == 0 || max_cycles > 64) return fail(WIG_E_ARG, "max_cycles out of range (1..64)");
-    if ((flags & WIG_STEP_TOLERANCE) && !(tolerance > 0.0)) return fail(WIG_E_ARG, "tolerance must be positive");
-    cudaStream_t s = (cudaStream_t)stream;
-    const bool sh = step_parity(h, flags);
-    int rc = push_state(h, P, flags, tolerance, s, false);
-    if (rc) return rc;
-    const bool plain = (flags & (WIG_STEP_PLAIN | WIG_STEP_BOOKKEEPING_ONLY)) != 0u;
-    if (!plain && h->fast_dirty) {
-        wig::fast_zero_level0(fast_of(h, max_cycles, 0ull), s);
-        h->fast_dirty = false;
-    }
-    const uint32_t shape_flags =
-        flags & (WIG_STEP_BOOKKEEPING_ONLY | WIG_STEP_VISCOUS | WIG_STEP_TOLERANCE | WIG_STEP_F64_DOTS | WIG_STEP_PLAIN |
-                 WIG_STEP_PERSISTENT);
-    const uint64_t key = ((uint64_t)max_cycles << 32) | ((uint64_t)shape_flags << 1) | (sh ? 1u : 0u);
-    auto it = h->graphs.find(key);
-    if (it == h->graphs.end()) {
-        cudaGraph_t g = nullptr;
-        cudaGraphExec_t ge = nullptr;
-        CUDA_TRY(cudaStreamBeginCapture(h->cap, cudaStreamCaptureModeThreadLocal));
-        uint32_t n = 0, nb = 0;
-        if (plain) {
-            n = record_step(h, max_cycles, flags, sh, h->cap, nullptr);
-        } else {
-            int rc2 = record_step_fast(h, max_cycles, flags, sh, h->cap, nullptr, true, &n, &nb);
-            if (rc2) {
-                cudaGraph_t junk = nullptr;
-                cudaStreamEndCapture(h->cap, &junk);
-                if (junk) cudaGraphDestroy(junk);
-                return rc2;
-            }
-        }
-        cudaError_t e = cudaStreamEndCapture(h->cap, &g);
-        if (e != cudaSuccess) return fail(WIG_E_CUDA, std::string("stream capture: ") + cudaGetErrorString(e));
-        e = cudaGraphInstantiate(&ge, g, 0);
-        if (e != cudaSuccess) {
-            cudaGraphDestroy(g);
-            return fail(WIG_E_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-        }
-        it = h->graphs.emplace(key, std::make_pair(g, ge)).first;
-        h->graph_launches[key] = n;
-        h->graph_body[key] = nb;
-    }
-    h->last_launches = h->graph_launches[key];
-    h->last_body = h->graph_body[key];
-    CUDA_TRY(cudaGraphLaunch(it->second.second, s));
-    if (flags & WIG_STEP_SYNC_STATS) CUDA_TRY(cudaMemcpyAsync(h->h_report, h->d_report, sizeof(Report), cudaMemcpyDeviceToHost, s));
-    h->last_stream = s;
-    h->last_cycles_flags = flags;
-    return WIG_OK;
+    if (!h || !h->b || !P) return fail(WIG_E_ARG, "null argument");
+    const uint32_t w0 = 0;
+    StepArgs a{0, &w0, 1, P, nullptr, max_cycles, flags, tolerance, (cudaStream_t)stream};
+    return batch_step(h->b, a);
 }
 
 int wig_fluid_step_profile(wig_fluid* h, const wig_params* P, uint32_t max_cycles, uint32_t flags, double tolerance,
                            void* stream, float* ms_out, uint32_t* calls_out) {
-    if (!h || !P || !ms_out || !calls_out) return fail(WIG_E_ARG, "null argument");
-    if (!h->bound) return fail(WIG_E_STATE, "buffers not bound");
-    if (max_cycles == 0 || max_cycles > 64) return fail(WIG_E_ARG, "max_cycles out of range (1..64)");
-    if ((flags & WIG_STEP_TOLERANCE) && !(tolerance > 0.0)) return fail(WIG_E_ARG, "tolerance must be positive");
-    cudaStream_t s = (cudaStream_t)stream;
-    const bool sh = step_parity(h, flags);
-    int rc = push_state(h, P, flags, tolerance, s, false);
-    if (rc) return rc;
-    Prof prof;
-    const bool plain = (flags & (WIG_STEP_PLAIN | WIG_STEP_BOOKKEEPING_ONLY)) != 0u;
-    h->last_body = 0;
-    if (plain) {
-        h->last_launches = record_step(h, max_cycles, flags, sh, s, &prof);
-    } else {
-        if (h->fast_dirty) {
-            wig::fast_zero_level0(fast_of(h, max_cycles, 0ull), s);
-            h->fast_dirty = false;
-        }
-        uint32_t n = 0, nb = 0;
-        rc = record_step_fast(h, max_cycles, flags, sh, s, &prof, false, &n, &nb);
-        if (rc) return rc;
-        h->last_launches = n;
-    }
-    CUDA_TRY(cudaGetLastError());
-    CUDA_TRY(cudaStreamSynchronize(s));
-    for (int k = 0; k < WIG_PROFILE_SLOTS; k++) { ms_out[k] = 0.0f; calls_out[k] = 0u; }
-    for (auto& m : prof.marks) {
-        float ms = 0.0f;
-        cudaEventElapsedTime(&ms, m.second.first, m.second.second);
-        ms_out[m.first] += ms;
-        calls_out[m.first] += 1u;
-        cudaEventDestroy(m.second.first);
-        cudaEventDestroy(m.second.second);
-    }
-    h->last_stream = s;
-    return WIG_OK;
+    if (!h || !h->b || !P) return fail(WIG_E_ARG, "null argument");
+    const uint32_t w0 = 0;
+    StepArgs a{0, &w0, 1, P, nullptr, max_cycles, flags, tolerance, (cudaStream_t)stream};
+    return batch_step_profile(h->b, a, ms_out, calls_out);
 }
 
 int wig_fluid_read_stats(wig_fluid* h, wig_fluid_stats* out) {
-    if (!h || !out) return fail(WIG_E_ARG, "null argument");
-    cudaStream_t s = h->last_stream;
-    CUDA_TRY(cudaMemcpyAsync(h->h_report, h->d_report, sizeof(Report), cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaStreamSynchronize(s));
-    const Report& r = *h->h_report;
-    std::memset(out, 0, sizeof(*out));
-    for (uint32_t k = 0; k < WIG_FLUID_STATS; k++) out->count[k] = r.count[k];
-    out->particles = r.particles;
-    out->cycles = r.count[WIG_COUNT_CYCLES];
-    out->launches = h->last_launches + h->last_body * r.count[WIG_COUNT_CYCLES];
-    out->rel_residual = r.rel;
-    out->b_norm = r.bnorm2 > 0.0 ? __builtin_sqrt(r.bnorm2) : 0.0;
-    if (r.err & wig::ERR_BARRIER) return fail(WIG_E_STATE, "the persistent solve's grid barrier waited past its limit");
-    if (r.err) return fail(WIG_E_STATE, "a device loop hit its iteration limit (union-find)");
-    if (r.particles > h->L.capacity) return fail(WIG_E_CAPACITY, "more particles than the buffers hold");
-    return WIG_OK;
+    if (!h || !h->b) return fail(WIG_E_ARG, "null argument");
+    const uint32_t w0 = 0;
+    return batch_read_stats(h->b, &w0, 1, out);
 }
 
 void wig_fluid_destroy(wig_fluid* h) {
     if (!h) return;
-    if (h->last_stream || true) cudaDeviceSynchronize();
-    drop_graphs(h);
-    for (int k = 0; k < 7; k++)
-        if (h->own[k]) cudaFree(h->own[k]);
-    if (h->d_elems) cudaFree(h->d_elems);
-    if (h->d_st) cudaFree(h->d_st);
-    if (h->h_st) cudaFreeHost(h->h_st);
-    for (int k = 0; k < RING; k++)
-        if (h->st_ev[k]) cudaEventDestroy(h->st_ev[k]);
-    if (h->d_report) cudaFree(h->d_report);
-    if (h->h_report) cudaFreeHost(h->h_report);
-    if (h->d_part64) cudaFree(h->d_part64);
-    if (h->d_norm64) cudaFree(h->d_norm64);
-    if (h->cap) cudaStreamDestroy(h->cap);
-    if (h->cap2) cudaStreamDestroy(h->cap2);
-    if (h->fast_mem) cudaFree(h->fast_mem);
+    destroy_batch(h->b);
     delete h;
 }
+
+// ---------------------------------------------------------------- batches
+
+int wig_batch_world_bytes(const wig_world_desc* d, uint64_t* out) {
+    if (!out) return fail(WIG_E_ARG, "null argument");
+    wig_world_layout L;
+    int rc = layout_of(d, &L);
+    if (rc) return rc;
+    wig::Dev D{};
+    dev_shape(D, L);
+    *out = world_buffers_bytes(L) + scratch_bytes(D) + sizeof(wig::StepState) + sizeof(wig::World) + 3u * sizeof(Report);
+    return WIG_OK;
+}
+
+int wig_batch_create(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, uint32_t n_elems, wig_batch** out) {
+    return make_batch(descs, n, elems, n_elems, true, out);
+}
+
+uint32_t wig_batch_worlds(const wig_batch* b) { return b ? b->K : 0u; }
+
+int wig_batch_layout(const wig_batch* b, uint32_t world, wig_world_layout* out) {
+    if (!b || !out) return fail(WIG_E_ARG, "null argument");
+    if (world >= b->K) return fail(WIG_E_ARG, "world index out of range");
+    *out = b->L[world];
+    return WIG_OK;
+}
+
+int wig_batch_buffers_of(wig_batch* b, uint32_t world, wig_fluid_buffers* out) {
+    if (!b || !out) return fail(WIG_E_ARG, "null argument");
+    if (world >= b->K) return fail(WIG_E_ARG, "world index out of range");
+    if (!b->bound[world]) return fail(WIG_E_STATE, "buffers not bound");
+    const wig::Dev& D = b->hw[world].D;
+    out->cells = D.cells; out->sorted = D.sorted; out->parts = D.parts; out->counters = D.counters;
+    out->field = D.field; out->blocks = D.blocks; out->cg = D.cg;
+    return WIG_OK;
+}
+
+int wig_batch_upload(wig_batch* b, uint32_t world, int which, const void* host, uint64_t offset, uint64_t bytes,
+                     void* stream) {
+    return copy_world(b, world, which, const_cast<void*>(host), offset, bytes, stream, true);
+}
+
+int wig_batch_download(wig_batch* b, uint32_t world, int which, void* host, uint64_t offset, uint64_t bytes,
+                       void* stream) {
+    return copy_world(b, world, which, host, offset, bytes, stream, false);
+}
+
+int wig_batch_step(wig_batch* b, uint32_t lane, const uint32_t* worlds, uint32_t count, const wig_params* P,
+                   const uint32_t* world_flags, uint32_t max_cycles, uint32_t flags, double tolerance, void* stream) {
+    if (flags & (WIG_STEP_PLAIN | WIG_STEP_PERSISTENT)) return fail(WIG_E_ARG, "a batch steps in the fast form");
+    StepArgs a{lane, worlds, count, P, world_flags, max_cycles, flags & ~WORLD_BITS, tolerance, (cudaStream_t)stream};
+    if (!world_flags) a.world_flags = nullptr;
+    return batch_step(b, a);
+}
+
+int wig_batch_read_stats(wig_batch* b, const uint32_t* worlds, uint32_t count, wig_fluid_stats* out) {
+    return batch_read_stats(b, worlds, count, out);
+}
+
+int wig_batch_step_profile(wig_batch* b, uint32_t lane, const uint32_t* worlds, uint32_t count, const wig_params* P,
+                           const uint32_t* world_flags, uint32_t max_cycles, uint32_t flags, double tolerance,
+                           void* stream, float* ms_out, uint32_t* calls_out) {
+    if (flags & (WIG_STEP_PLAIN | WIG_STEP_PERSISTENT)) return fail(WIG_E_ARG, "a batch steps in the fast form");
+    StepArgs a{lane, worlds, count, P, world_flags, max_cycles, flags & ~WORLD_BITS, tolerance, (cudaStream_t)stream};
+    return batch_step_profile(b, a, ms_out, calls_out);
+}
+
+void wig_batch_destroy(wig_batch* b) { destroy_batch(b); }
 
 }  // extern "C"

@@ -5,6 +5,7 @@
 // js/shared.js:63-110).
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 #include <string>
 #include <cuda_fp16.h>
@@ -60,17 +61,36 @@ constexpr uint32_t ERR_LOOP = 1u, ERR_CAPACITY = 2u, ERR_BARRIER = 4u;
 // second), past which the kernel records ERR_BARRIER and returns.
 constexpr uint32_t BARRIER_SPIN_LIMIT = 1u << 23;
 
-// Per-step state in device memory: the step's Params and the solve's
-// scalars (tolerance form and FP64 dots).  Written by the host before each
-// step (one small H2D copy), read by every kernel, so a captured graph replays
-// with the new values.
+// What the host writes for a world before each step: its Params, the
+// solve's stopping rule, and its part of the step (a batch steps worlds with
+// different flags): bookkeeping only, viscosity sweeps, the tiling the
+// step's first relaxation is on.
+struct StepHead {
+    wig_params P;
+    uint32_t tol_mode;
+    uint32_t f64;
+    uint32_t book;
+    uint32_t viscous;
+    uint32_t shift_first;
+    uint32_t pad_;
+    double tol;
+};
+
+// Per-step state of a world in device memory: its head, then the solve's
+// scalars (tolerance form and FP64 dots), set by the step itself.  Read by
+// every kernel, so a captured graph replays with new values.
 struct StepState {
     wig_params P;
     uint32_t tol_mode;
     uint32_t f64;
+    uint32_t book;
+    uint32_t viscous;
+    uint32_t shift_first;
+    uint32_t pad_;
+    double tol;
+    // set at the step's start: error word, residuals
     uint32_t err;
     uint32_t cycles_run;
-    double tol;
     double rel;
     double bnorm2;
     double rz;
@@ -87,8 +107,9 @@ struct StepState {
     uint32_t bar_count;
     uint32_t bar_gen;
 };
+static_assert(sizeof(StepHead) == offsetof(StepState, err), "StepHead is StepState's prefix");
 
-// The world and its buffers, passed by value to every kernel.
+// A world and its buffers (an entry of a batch's world table).
 struct Dev {
     int W, H;
     uint32_t C, F, B, BW, BH, cap, ppc, edge_tiles, levels;
@@ -319,5 +340,83 @@ __device__ __forceinline__ float fineBeta(float a, float b, float da, float db) 
     if (b > 0.0f && a == 0.0f) return beta / (db > 0.0f ? surfaceShare(db, da) : 0.5f);
     return beta;
 }
+
+// ---------------------------------------------------------------- batches
+
+// One multigrid level's arrays in the fast form's scratch, a float per cell
+// (row-major, the level's width): potentials and right-hand sides (pressure
+// x, drift y), density, and the stencil's coefficients to the left, right,
+// upper and lower neighbours (0 past an obstacle or the edge) with their sum.
+struct Lvl {
+    float *px, *py, *rx, *ry, *rho;
+    float *b0, *b1, *b2, *b3, *diag;
+};
+
+// A world's fast-form scratch.
+struct FastW {
+    Lvl L[WIG_MG_LEVELS + 1];  // level 0 (the cells) .. levels
+    float* pin;                // level 0: PIN at a pinned root, else 0
+    uint8_t* fmask;            // level 0: bit d set when neighbour d is liquid
+    float *rimx, *rimy;        // level 0: the relaxation's rim snapshot
+    float *X, *R, *P, *Q;      // level 0: CG's x, r, p, A p
+    float* part32;             // 2 per block
+    double* part64;            // 2 per block
+    uint32_t lc;               // first level the one-CTA coarse kernel solves
+    uint32_t lp;               // first level CTA 0 of the persistent solve holds
+};
+
+// An entry of a batch's world table (device memory).
+struct World {
+    Dev D;
+    FastW S;
+};
+
+// Work lists.  A kernel's CTAs take the items of one list in turn (grid
+// stride); an item is a world of the batch (its index in the world table, the
+// high bits) and a unit of that world's work (the low Batch::lbits bits):
+enum List : uint32_t {
+    L_WB = 0,     // every 8x8 block of the world (sync, syncSeed)
+    L_PS,         // 256 particles of `sorted` (syncParticles)
+    L_PP,         // 256 particles of `parts` (gather, advect, sortCount, scatter)
+    L_ACT,        // an active block (the passes over the blocks worked on)
+    L_RET,        // a retired block
+    L_ACT4,       // four active blocks (the fast form's 256-thread CG kernels)
+    L_RELAX,      // a relaxation tile: the active blocks, then the shifted tiling's edge tiles
+    L_ONE_ALL,    // the world (per-world single-CTA work: compact, report)
+    L_ONE,        // the world when it runs the full step (scanTotals, the coarse levels, ...)
+    L_RES,        // + l - 1: 256 cells of level l when the fast form restricts it by itself (l <= lc)
+    L_SM = L_RES + WIG_MG_LEVELS,  // + l - 1: 256 cells of level l below the coarse kernel's (l < lc)
+    L_COUNT = L_SM + WIG_MG_LEVELS
+};
+
+// A batch as every kernel sees it: the world table and the work lists
+// (list L's items at items + base[L], count[L] of them, written on the
+// device by the schedule kernels).
+struct Batch {
+    const World* __restrict__ worlds;
+    const uint32_t* __restrict__ items;
+    const uint32_t* __restrict__ count;
+    uint32_t base[L_COUNT];
+    uint32_t lbits;           // bits of an item's unit
+    uint32_t max_cycles;
+    unsigned long long cond;  // cudaGraphConditionalHandle of the iteration loop (0: none)
+    uint32_t* loop;           // the loop's verdict: 1 when a world iterates again
+
+    __device__ __forceinline__ uint32_t n(uint32_t list) const { return count[list]; }
+    __device__ __forceinline__ uint32_t item(uint32_t list, uint32_t g) const { return items[base[list] + g]; }
+    __device__ __forceinline__ const World& world(uint32_t it) const { return worlds[(uint64_t)it >> lbits]; }
+    __device__ __forceinline__ uint32_t unit(uint32_t it) const { return it & ((1u << lbits) - 1u); }
+};
+
+// The CTAs of a kernel over list L, one item per CTA at a time:
+//   FOR_ITEMS(Bt, L, it) { const World& Wd = Bt.world(it); uint32_t j = Bt.unit(it); ... }
+#define FOR_ITEMS(Bt, L, it)                                                         \
+    for (uint32_t g_##it = blockIdx.x, n_##it = (Bt).n(L), it = 0;                    \
+         g_##it < n_##it && ((it = (Bt).item((L), g_##it)), true); g_##it += gridDim.x)
+// An item's world D (with its accessors w) and unit j.
+#define ITEM_WORLD(Bt, it, D, w, j)              \
+    const Dev& D = (Bt).world(it).D;             \
+    const W w(D);                                \
+    const uint32_t j = (Bt).unit(it)
 
 }  // namespace wig

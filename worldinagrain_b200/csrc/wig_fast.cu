@@ -29,10 +29,6 @@ __device__ __forceinline__ uint32_t vld(const uint32_t* p) { return *(const vola
 __device__ __forceinline__ double vldd(const double* p) { return *(const volatile double*)p; }
 __device__ __forceinline__ float vldf(const float* p) { return *(const volatile float*)p; }
 
-#define FAST_FOR_ACTIVE(w, wid)                        \
-    const uint32_t na_ = (w).activeCount();           \
-    for (uint32_t wid = blockIdx.x; wid < na_; wid += gridDim.x)
-
 __device__ __forceinline__ I2 lidCell(const W& w, uint32_t wid) {
     I2 b = w.activeBlock(wid);
     return I2{b.x * BLOCK + (int)(threadIdx.x & 7u), b.y * BLOCK + (int)(threadIdx.x >> 3)};
@@ -130,20 +126,28 @@ __device__ __forceinline__ I2 tileCell(const W& w, uint32_t wid) {
     return I2{b.x * BLOCK + (int)(threadIdx.x & 7u), b.y * BLOCK + (int)((threadIdx.x >> 3) & 7u)};
 }
 
+// An item's world: its descriptor D, fast scratch F, accessors w, unit j.
+#define FAST_ITEM(Bt, it, D, F, w, j)            \
+    const World& Wd_##it = (Bt).world(it);       \
+    const Dev& D = Wd_##it.D;                    \
+    const FastW& F = Wd_##it.S;                  \
+    const W w(D);                                \
+    const uint32_t j = (Bt).unit(it)
+
 // ================================================================ set-up
 
 // cgStart, cgResidual, cgPrepare (fluid.wgsl:2665-2732) into the scratch,
-// the cells' coefficients worked out (four tiles a 256-thread CTA), and the
-// blocks that dropped out this step zeroed (the invariant).
-__global__ void __launch_bounds__(256) k_fSetup(Fast F) {
-    const Dev& D = F.D;
-    W w(D);
+// the cells' coefficients worked out (four tiles a 256-thread CTA, a world's
+// group of four active blocks an item; the CTA that counts a world's last
+// tile sums its ||b||^2), and the blocks that dropped out this step zeroed
+// (the invariant).
+__global__ void __launch_bounds__(256) k_fSetup(Batch Bt) {
     __shared__ double s64[256];
-    const uint32_t na = w.activeCount(), nr = D.blocks[w.countSlot(COUNT_RETIRED)];
-    const bool tol = D.st->tol_mode != 0u;
-    const Lvl& L0 = F.L[0];
-    bool amLast = false;
-    for (uint32_t g = blockIdx.x; g * 4u < na; g += gridDim.x) {
+    FOR_ITEMS(Bt, L_ACT4, it) {
+        FAST_ITEM(Bt, it, D, F, w, g);
+        const uint32_t na = w.activeCount();
+        const bool tol = D.st->tol_mode != 0u;
+        const Lvl& L0 = F.L[0];
         const uint32_t wid = g * 4u + (threadIdx.x >> 6);
         const bool valid = wid < na;
         double b2 = 0.0;
@@ -200,22 +204,26 @@ __global__ void __launch_bounds__(256) k_fSetup(Fast F) {
                 D.norm64[2u * w.blockIndex(w.activeBlock(wid))] = v;
                 __threadfence();
             }
-            if (lastOf4(&D.st->fdone[0], min(4u, na - g * 4u), na)) amLast = true;
+            if (lastOf4(&D.st->fdone[0], min(4u, na - g * 4u), na)) {
+                double bn = sumBlocks256(w, D.norm64, 0, s64);
+                if (threadIdx.x == 0) {
+                    D.st->bnorm2 = bn;
+                    D.st->rel = 1.0;
+                }
+            }
         }
     }
-    if (tol && amLast) {
-        double bn = sumBlocks256(w, D.norm64, 0, s64);
-        if (threadIdx.x == 0) {
-            D.st->bnorm2 = bn;
-            D.st->rel = 1.0;
-        }
-    }
-    // the blocks that dropped out: their level-0 arrays back to zero
-    for (uint32_t j = blockIdx.x * 4u + (threadIdx.x >> 6); j < nr; j += gridDim.x * 4u) {
+    // the blocks that dropped out: their level-0 arrays back to zero (a
+    // retired block a quarter of the CTA)
+    const uint32_t nr = Bt.n(L_RET);
+    for (uint32_t t = blockIdx.x * 4u + (threadIdx.x >> 6); t < nr; t += gridDim.x * 4u) {
+        const uint32_t it = Bt.item(L_RET, t);
+        FAST_ITEM(Bt, it, D, F, w, j);
         uint32_t n = D.blocks[w.retiredSlot(j)];
         I2 c{(int)(n % D.BW) * BLOCK + (int)(threadIdx.x & 7u), (int)(n / D.BW) * BLOCK + (int)((threadIdx.x >> 3) & 7u)};
         if (w.inWorld(c)) {
             uint32_t i = w.cellIndex(c);
+            const Lvl& L0 = F.L[0];
             L0.px[i] = 0.0f; L0.py[i] = 0.0f; L0.rho[i] = 0.0f;
             F.rimx[i] = 0.0f; F.rimy[i] = 0.0f; F.P[i] = 0.0f;
         }
@@ -223,8 +231,7 @@ __global__ void __launch_bounds__(256) k_fSetup(Fast F) {
 }
 
 // Zeroes the level-0 arrays the neighbours read (after an upload).
-__global__ void k_fZero(Fast F) {
-    const uint32_t C = F.D.C;
+__global__ void k_fZero(FastW F, uint32_t C) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < C; i += gridDim.x * blockDim.x) {
         F.L[0].px[i] = 0.0f; F.L[0].py[i] = 0.0f; F.L[0].rho[i] = 0.0f;
         F.rimx[i] = 0.0f; F.rimy[i] = 0.0f; F.P[i] = 0.0f;
@@ -242,17 +249,19 @@ __device__ I2 tileBlockF(const W& w, uint32_t wid, int shift) {
 }
 
 // relaxTile (fluid.wgsl:2109-2182) over the scratch: the rim snapshot's
-// values for liquid cells, the potentials (zero) elsewhere.
-__global__ void __launch_bounds__(64) k_fRelax(Fast F, int shift) {
-    const Dev& D = F.D;
-    W w(D);
+// values for liquid cells, the potentials (zero) elsewhere.  `second`: the
+// iteration's relaxation after the V-cycle, on the other tiling from the
+// first (each world's first tiling is its step's).
+__global__ void __launch_bounds__(64) k_fRelax(Batch Bt, int second) {
     __shared__ float tpx[RIM * RIM], tpy[RIM * RIM];
     __shared__ int s_live, s_ox, s_oy;
-    const Lvl& L0 = F.L[0];
-    const uint32_t na = w.activeCount();
-    const uint32_t total = na + (shift ? D.edge_tiles : 0u);
-    for (uint32_t j = blockIdx.x; j < total; j += gridDim.x) {
-        uint32_t wid = j < na ? j : D.B + (j - na);
+    FOR_ITEMS(Bt, L_RELAX, it) {
+        FAST_ITEM(Bt, it, D, F, w, j);
+        if (D.st->cont == 0u) continue;
+        const int shift = ((D.st->shift_first ^ (uint32_t)second) & 1u) ? BLOCK / 2 : 0;
+        const Lvl& L0 = F.L[0];
+        const uint32_t na = w.activeCount();
+        const uint32_t wid = j < na ? j : D.B + (j - na);
         if (threadIdx.x == 0) {
             I2 b = tileBlockF(w, wid, shift);
             int ox = b.x * BLOCK - shift, oy = b.y * BLOCK - shift;
@@ -344,15 +353,9 @@ __device__ __forceinline__ V2 residualStored(const Lvl& V, const float* pin, uin
     return V2{V.rx[k] - (sx - (dg + pinx) * V.px[k]) / h2, V.ry[k] - (sy - (dg + 0.0f) * V.py[k]) / h2};
 }
 
-// restrictLevel (fluid.wgsl:2342-2377) of level l from level l - 1 (both in
-// the scratch): a thread per coarse cell.
-__global__ void k_fRestrict(Fast F, uint32_t l) {
-    const Dev& D = F.D;
-    W w(D);
-    if (w.activeCount() == 0u) return;
-    const int lw = (int)D.level_w[l], lh = (int)D.level_h[l];
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= (uint32_t)(lw * lh)) return;
+// One coarse cell of restrictLevel (fluid.wgsl:2342-2377), level l from l - 1.
+__device__ void restrictCell(const Dev& D, const FastW& F, const W& w, uint32_t l, uint32_t j) {
+    const int lw = (int)D.level_w[l];
     const int cx = (int)(j % (uint32_t)lw), cy = (int)(j / (uint32_t)lw);
     const Lvl& V = F.L[l];
     const int span = 1 << l;
@@ -367,9 +370,8 @@ __global__ void k_fRestrict(Fast F, uint32_t l) {
     const int uw = (int)D.level_w[l - 1], uh = (int)D.level_h[l - 1];
     const float h2 = (float)(1u << (2u * (l - 1u)));
     const float* pin = l == 1u ? F.pin : nullptr;
-    float fluid = 0.0f, sum = 0.0f;
+    float fluid = 0.0f, sum = 0.0f, rx = 0.0f, ry = 0.0f;
     bool air = false;
-    float rx = 0.0f, ry = 0.0f;
     for (int q = 0; q < 4; q++) {
         int kx = 2 * cx + (q & 1), ky = 2 * cy + (q >> 1);
         if (kx >= uw || ky >= uh) continue;  // rhoAt outside the level: -1
@@ -392,15 +394,10 @@ __global__ void k_fRestrict(Fast F, uint32_t l) {
     V.rho[j] = rho;
 }
 
-// smoothAt (fluid.wgsl:2318-2334) on level l >= 1, the coefficients worked
-// out on the step's first iteration and kept.
-__global__ void k_fSmooth(Fast F, uint32_t l, int color) {
-    const Dev& D = F.D;
-    W w(D);
-    if (w.activeCount() == 0u) return;
+// One cell of smoothAt (fluid.wgsl:2318-2334) on level l >= 1, the
+// coefficients worked out on the step's first iteration and kept.
+__device__ void smoothCell(const Dev& D, const FastW& F, uint32_t l, int color, bool first, uint32_t j) {
     const int lw = (int)D.level_w[l], lh = (int)D.level_h[l];
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= (uint32_t)(lw * lh)) return;
     const int cx = (int)(j % (uint32_t)lw), cy = (int)(j / (uint32_t)lw);
     if (((cx + cy) & 1) != color) return;
     const Lvl& V = F.L[l];
@@ -408,7 +405,7 @@ __global__ void k_fSmooth(Fast F, uint32_t l, int color) {
     if (rho <= 0.0f) return;
     float b[4];
     float dg;
-    if (D.st->cycle == 0u) {
+    if (first) {
         dg = 0.0f;
         for (int d = 0; d < 4; d++) {
             b[d] = 0.0f;
@@ -462,14 +459,9 @@ __device__ __forceinline__ V2 prolongedFrom(const float* rho, const float* px, c
     return V2{ax / ww, ay / ww};
 }
 
-// prolong (fluid.wgsl:2459-2470) of level l from l + 1.
-__global__ void k_fProlong(Fast F, uint32_t l) {
-    const Dev& D = F.D;
-    W w(D);
-    if (w.activeCount() == 0u) return;
-    const int lw = (int)D.level_w[l], lh = (int)D.level_h[l];
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= (uint32_t)(lw * lh)) return;
+// One cell of prolong (fluid.wgsl:2459-2470), level l from l + 1.
+__device__ void prolongCell(const Dev& D, const FastW& F, uint32_t l, uint32_t j) {
+    const int lw = (int)D.level_w[l];
     const Lvl& V = F.L[l];
     if (V.rho[j] <= 0.0f) return;
     const Lvl& U = F.L[l + 1];
@@ -477,6 +469,37 @@ __global__ void k_fProlong(Fast F, uint32_t l) {
                          (int)(j / (uint32_t)lw));
     V.px[j] = V.px[j] + e.x;
     V.py[j] = V.py[j] + e.y;
+}
+
+// restrictLevel of level l from level l - 1 (both in the scratch): a thread
+// per coarse cell, 256 cells an item.
+__global__ void k_fRestrict(Batch Bt, uint32_t l) {
+    FOR_ITEMS(Bt, L_RES + l - 1u, it) {
+        FAST_ITEM(Bt, it, D, F, w, chunk);
+        if (D.st->cont == 0u) continue;
+        const uint32_t j = chunk * blockDim.x + threadIdx.x;
+        if (j < D.level_w[l] * D.level_h[l]) restrictCell(D, F, w, l, j);
+    }
+}
+
+// smoothAt on level l >= 1, one colour.
+__global__ void k_fSmooth(Batch Bt, uint32_t l, int color) {
+    FOR_ITEMS(Bt, L_SM + l - 1u, it) {
+        FAST_ITEM(Bt, it, D, F, w, chunk);
+        if (D.st->cont == 0u) continue;
+        const uint32_t j = chunk * blockDim.x + threadIdx.x;
+        if (j < D.level_w[l] * D.level_h[l]) smoothCell(D, F, l, color, D.st->cycle == 0u, j);
+    }
+}
+
+// prolong of level l from l + 1.
+__global__ void k_fProlong(Batch Bt, uint32_t l) {
+    FOR_ITEMS(Bt, L_SM + l - 1u, it) {
+        FAST_ITEM(Bt, it, D, F, w, chunk);
+        if (D.st->cont == 0u) continue;
+        const uint32_t j = chunk * blockDim.x + threadIdx.x;
+        if (j < D.level_w[l] * D.level_h[l]) prolongCell(D, F, l, j);
+    }
 }
 
 // Named barrier over the first `count` threads (a multiple of 32).
@@ -533,8 +556,7 @@ __device__ void slv_smooth(const SLv& V, uint32_t l, int tid, int nt) {
 // The levels lc (restricted already, in the scratch) down to the coarsest and
 // back up to lc, in one CTA's shared memory: smoothRed/Black, restrictLevel,
 // solve (40 SOR sweep pairs, omega 1.8), prolong (fluid.wgsl:2318-2470).
-__device__ void coarseLevels(const Fast& F, const W& w, uint32_t lc, float* sm, uint32_t* off) {
-    const Dev& D = F.D;
+__device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t lc, float* sm, uint32_t* off) {
     const uint32_t L = D.levels;
     const int tid = (int)threadIdx.x, nt = (int)blockDim.x;
     if (tid == 0) {
@@ -688,21 +710,25 @@ __device__ void coarseLevels(const Fast& F, const W& w, uint32_t lc, float* sm, 
     }
 }
 
-__global__ void __launch_bounds__(1024) k_fCoarse(Fast F) {
+__global__ void __launch_bounds__(1024) k_fCoarse(Batch Bt) {
     extern __shared__ float sm[];
     __shared__ uint32_t off[WIG_MG_LEVELS + 1];
-    W w(F.D);
-    if (w.activeCount() == 0u) return;
-    coarseLevels(F, w, F.lc, sm, off);
+    FOR_ITEMS(Bt, L_ONE, it) {
+        FAST_ITEM(Bt, it, D, F, w, unused_);
+        (void)unused_;
+        if (D.st->cont == 0u) continue;
+        coarseLevels(D, F, w, F.lc, sm, off);
+        __syncthreads();
+    }
 }
 
 // prolongFine (fluid.wgsl:2500-2512), and the rims for the relaxation after.
-__global__ void k_fProlongFine(Fast F) {
-    const Dev& D = F.D;
-    W w(D);
-    const Lvl& L0 = F.L[0];
-    const Lvl& U = F.L[1];
-    FAST_FOR_ACTIVE(w, wid) {
+__global__ void k_fProlongFine(Batch Bt) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        FAST_ITEM(Bt, it, D, F, w, wid);
+        if (D.st->cont == 0u) continue;
+        const Lvl& L0 = F.L[0];
+        const Lvl& U = F.L[1];
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         uint32_t i = w.cellIndex(c);
@@ -720,18 +746,17 @@ __global__ void k_fProlongFine(Fast F) {
 // ================================================================ conjugate gradients
 
 // cgRho + cgBeta (fluid.wgsl:2736-2764): four tiles a 256-thread CTA; the CTA
-// that counts the last tile sums the blocks' partials (sumBlocks' order).
-__global__ void __launch_bounds__(256) k_fRhoBeta(Fast F) {
-    const Dev& D = F.D;
-    W w(D);
+// that counts a world's last tile sums its blocks' partials (sumBlocks' order).
+__global__ void __launch_bounds__(256) k_fRhoBeta(Batch Bt) {
     __shared__ float sx[256], sy[256];
     __shared__ double s64[256];
-    const bool f64 = D.st->f64 != 0u;
-    const uint32_t cycle = D.st->cycle;
-    const Lvl& L0 = F.L[0];
-    const uint32_t na = w.activeCount();
-    bool amLast = false;
-    for (uint32_t g = blockIdx.x; g * 4u < na; g += gridDim.x) {
+    FOR_ITEMS(Bt, L_ACT4, it) {
+        FAST_ITEM(Bt, it, D, F, w, g);
+        if (D.st->cont == 0u) continue;
+        const bool f64 = D.st->f64 != 0u;
+        const uint32_t cycle = D.st->cycle;
+        const Lvl& L0 = F.L[0];
+        const uint32_t na = w.activeCount();
         const uint32_t wid = g * 4u + (threadIdx.x >> 6);
         const bool valid = wid < na;
         float vx = 0.0f, vy = 0.0f;
@@ -767,38 +792,37 @@ __global__ void __launch_bounds__(256) k_fRhoBeta(Fast F) {
             }
             __threadfence();
         }
-        if (lastOf4(&D.st->fdone[1], min(4u, na - g * 4u), na)) amLast = true;
-    }
-    if (amLast) {
-        if (f64) {
-            double rz = sumBlocks256(w, F.part64, 0, s64);
-            double zq = sumBlocks256(w, F.part64, 1, s64);
-            if (threadIdx.x == 0) {
-                double beta = (cycle == 0u || D.st->pq <= 0.0) ? 0.0 : -zq / D.st->pq;
-                D.st->rz = rz;
-                D.st->beta = beta;
-            }
-        } else {
-            float rz = sumBlocks256(w, F.part32, 0, sx);
-            float zq = sumBlocks256(w, F.part32, 1, sx);
-            if (threadIdx.x == 0) {
-                float beta = (cycle == 0u || D.st->pq32 <= 0.0f) ? 0.0f : -zq / D.st->pq32;
-                D.st->rz32 = rz;
-                D.st->beta32 = beta;
+        if (lastOf4(&D.st->fdone[1], min(4u, na - g * 4u), na)) {
+            if (f64) {
+                double rz = sumBlocks256(w, F.part64, 0, s64);
+                double zq = sumBlocks256(w, F.part64, 1, s64);
+                if (threadIdx.x == 0) {
+                    double beta = (cycle == 0u || D.st->pq <= 0.0) ? 0.0 : -zq / D.st->pq;
+                    D.st->rz = rz;
+                    D.st->beta = beta;
+                }
+            } else {
+                float rz = sumBlocks256(w, F.part32, 0, sx);
+                float zq = sumBlocks256(w, F.part32, 1, sx);
+                if (threadIdx.x == 0) {
+                    float beta = (cycle == 0u || D.st->pq32 <= 0.0f) ? 0.0f : -zq / D.st->pq32;
+                    D.st->rz32 = rz;
+                    D.st->beta32 = beta;
+                }
             }
         }
     }
 }
 
 // cgDirection (fluid.wgsl:2767-2776)
-__global__ void k_fDirection(Fast F) {
-    const Dev& D = F.D;
-    W w(D);
-    const bool f64 = D.st->f64 != 0u;
-    const float beta = vldf(&D.st->beta32);
-    const double beta64 = vldd(&D.st->beta);
-    const Lvl& L0 = F.L[0];
-    FAST_FOR_ACTIVE(w, wid) {
+__global__ void k_fDirection(Batch Bt) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        FAST_ITEM(Bt, it, D, F, w, wid);
+        if (D.st->cont == 0u) continue;
+        const bool f64 = D.st->f64 != 0u;
+        const float beta = D.st->beta32;
+        const double beta64 = D.st->beta;
+        const Lvl& L0 = F.L[0];
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         uint32_t i = w.cellIndex(c);
@@ -812,16 +836,15 @@ __global__ void k_fDirection(Fast F) {
 }
 
 // cgApply + cgAlpha (fluid.wgsl:2779-2814)
-__global__ void __launch_bounds__(256) k_fApplyAlpha(Fast F) {
-    const Dev& D = F.D;
-    W w(D);
+__global__ void __launch_bounds__(256) k_fApplyAlpha(Batch Bt) {
     __shared__ float sx[256];
     __shared__ double s64[256];
-    const bool f64 = D.st->f64 != 0u;
-    const Lvl& L0 = F.L[0];
-    const uint32_t na = w.activeCount();
-    bool amLast = false;
-    for (uint32_t g = blockIdx.x; g * 4u < na; g += gridDim.x) {
+    FOR_ITEMS(Bt, L_ACT4, it) {
+        FAST_ITEM(Bt, it, D, F, w, g);
+        if (D.st->cont == 0u) continue;
+        const bool f64 = D.st->f64 != 0u;
+        const Lvl& L0 = F.L[0];
+        const uint32_t na = w.activeCount();
         const uint32_t wid = g * 4u + (threadIdx.x >> 6);
         const bool valid = wid < na;
         float vx = 0.0f;
@@ -860,50 +883,40 @@ __global__ void __launch_bounds__(256) k_fApplyAlpha(Fast F) {
             }
             __threadfence();
         }
-        if (lastOf4(&D.st->fdone[2], min(4u, na - g * 4u), na)) amLast = true;
-    }
-    if (amLast) {
-        if (f64) {
-            double pq = sumBlocks256(w, F.part64, 0, s64);
-            if (threadIdx.x == 0) {
-                D.st->pq = pq;
-                D.st->alpha = pq <= 0.0 ? 0.0 : D.st->rz / pq;
-            }
-        } else {
-            float pq = sumBlocks256(w, F.part32, 0, sx);
-            if (threadIdx.x == 0) {
-                D.st->pq32 = pq;
-                D.st->alpha32 = pq <= 0.0f ? 0.0f : D.st->rz32 / pq;
+        if (lastOf4(&D.st->fdone[2], min(4u, na - g * 4u), na)) {
+            if (f64) {
+                double pq = sumBlocks256(w, F.part64, 0, s64);
+                if (threadIdx.x == 0) {
+                    D.st->pq = pq;
+                    D.st->alpha = pq <= 0.0 ? 0.0 : D.st->rz / pq;
+                }
+            } else {
+                float pq = sumBlocks256(w, F.part32, 0, sx);
+                if (threadIdx.x == 0) {
+                    D.st->pq32 = pq;
+                    D.st->alpha32 = pq <= 0.0f ? 0.0f : D.st->rz32 / pq;
+                }
             }
         }
     }
 }
 
 // cgUpdate (fluid.wgsl:2852-2880), the tolerance form's norm, and the loop's
-// condition: the next iteration runs unless the solve has converged
-// (converged, fluid.wgsl:2223-2226) or max_cycles are done.
-__global__ void __launch_bounds__(256) k_fUpdate(Fast F) {
-    const Dev& D = F.D;
-    W w(D);
+// condition: a world iterates again unless its solve has converged
+// (converged, fluid.wgsl:2223-2226) or max_cycles are done; the loop runs on
+// while any world does.
+__global__ void __launch_bounds__(256) k_fUpdate(Batch Bt) {
     __shared__ uint32_t most[4];
     __shared__ double s64[256];
-    const uint32_t cycle = D.st->cycle;
-    const bool f64 = D.st->f64 != 0u, tol = D.st->tol_mode != 0u;
-    const float alpha = vldf(&D.st->alpha32);
-    const double alpha64 = vldd(&D.st->alpha);
-    const Lvl& L0 = F.L[0];
-    const uint32_t na = w.activeCount();
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        D.blocks[w.countSlot(COUNT_RESIDUAL + (cycle + 1u) % 3u)] = 0u;
-        D.blocks[w.countSlot(COUNT_CYCLES)] += 1u;
-        if (na == 0u) {
-            D.st->cycle = cycle + 1u;
-            D.st->cont = 0u;
-            if (F.cond) cudaGraphSetConditional(F.cond, 0u);
-        }
-    }
-    bool amLast = false;
-    for (uint32_t g = blockIdx.x; g * 4u < na; g += gridDim.x) {
+    FOR_ITEMS(Bt, L_ACT4, it) {
+        FAST_ITEM(Bt, it, D, F, w, g);
+        if (D.st->cont == 0u) continue;
+        const uint32_t cycle = D.st->cycle;
+        const bool f64 = D.st->f64 != 0u, tol = D.st->tol_mode != 0u;
+        const float alpha = D.st->alpha32;
+        const double alpha64 = D.st->alpha;
+        const Lvl& L0 = F.L[0];
+        const uint32_t na = w.activeCount();
         const uint32_t wid = g * 4u + (threadIdx.x >> 6);
         const bool valid = wid < na;
         if ((threadIdx.x & 63u) == 0u) most[threadIdx.x >> 6] = 0u;
@@ -942,32 +955,53 @@ __global__ void __launch_bounds__(256) k_fUpdate(Fast F) {
             atomicMax(&D.blocks[w.countSlot(COUNT_RESIDUAL + cycle % 3u)], most[threadIdx.x >> 6]);
             __threadfence();
         }
-        if (lastOf4(&D.st->fdone[3], min(4u, na - g * 4u), na)) amLast = true;
-    }
-    if (amLast) {
-        bool conv;
-        if (tol) {
-            double rr = sumBlocks256(w, D.norm64, 0, s64);
-            double rel = D.st->bnorm2 > 0.0 ? sqrt(rr / D.st->bnorm2) : 0.0;
-            if (threadIdx.x == 0) D.st->rel = rel;
-            conv = rel <= D.st->tol;
-        } else {
-            conv = __uint_as_float(__ldcg(&D.blocks[w.countSlot(COUNT_RESIDUAL + cycle % 3u)])) < LIQUID_TOLERANCE;
-        }
-        if (threadIdx.x == 0) {
-            const uint32_t cont = (!conv && cycle + 1u < F.max_cycles) ? 1u : 0u;
-            D.st->cycle = cycle + 1u;
-            D.st->cont = cont;
-            if (F.cond) cudaGraphSetConditional(F.cond, cont);
+        if (lastOf4(&D.st->fdone[3], min(4u, na - g * 4u), na)) {
+            bool conv;
+            if (tol) {
+                double rr = sumBlocks256(w, D.norm64, 0, s64);
+                double rel = D.st->bnorm2 > 0.0 ? sqrt(rr / D.st->bnorm2) : 0.0;
+                if (threadIdx.x == 0) D.st->rel = rel;
+                conv = rel <= D.st->tol;
+            } else {
+                conv = __uint_as_float(__ldcg(&D.blocks[w.countSlot(COUNT_RESIDUAL + cycle % 3u)])) < LIQUID_TOLERANCE;
+            }
+            if (threadIdx.x == 0) {
+                const uint32_t cont = (!conv && cycle + 1u < Bt.max_cycles) ? 1u : 0u;
+                D.st->cycle = cycle + 1u;
+                D.st->cont = cont;
+                if (cont) {
+                    *Bt.loop = 1u;
+                    if (Bt.cond) cudaGraphSetConditional(Bt.cond, 1u);
+                }
+            }
         }
     }
 }
 
-// The loop's safe default: stop unless k_fUpdate decides otherwise.
-__global__ void k_fLoopStart(Fast F) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) {
-        F.D.st->cont = 0u;
-        if (F.cond) cudaGraphSetConditional(F.cond, 0u);
+// An iteration's start: the loop stops unless a world's k_fUpdate says
+// otherwise; each world still iterating (all of them on the first
+// iteration) clears its next residual slot and counts the iteration
+// (cgUpdate's first lines, fluid.wgsl:2852-2856), and one with no block
+// worked on stops there, as cgUpdate's converged test stops it.
+__global__ void k_fLoopStart(Batch Bt) {
+    if (threadIdx.x != 0) return;
+    if (blockIdx.x == 0) {
+        *Bt.loop = 0u;
+        if (Bt.cond) cudaGraphSetConditional(Bt.cond, 0u);
+    }
+    FOR_ITEMS(Bt, L_ONE, it) {
+        ITEM_WORLD(Bt, it, D, w, unused_);
+        (void)unused_;
+        StepState* st = D.st;
+        if (st->cycle == 0u) st->cont = 1u;
+        if (st->cont == 0u) continue;
+        const uint32_t cycle = st->cycle;
+        D.blocks[w.countSlot(COUNT_RESIDUAL + (cycle + 1u) % 3u)] = 0u;
+        D.blocks[w.countSlot(COUNT_CYCLES)] += 1u;
+        if (w.activeCount() == 0u) {
+            st->cycle = cycle + 1u;
+            st->cont = 0u;
+        }
     }
 }
 
@@ -976,14 +1010,18 @@ __global__ void k_fLoopStart(Fast F) {
 // potential, cg's (x, r, p, Ap); and the residual slots the converged
 // iterations the reference still dispatches would clear (cgUpdate's first
 // lines run whether or not the iteration is skipped).
-__global__ void k_fFinish(Fast F) {
-    const Dev& D = F.D;
-    W w(D);
-    const Lvl& L0 = F.L[0];
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        for (uint32_t c = D.st->cycle; c < F.max_cycles; c++) D.blocks[w.countSlot(COUNT_RESIDUAL + (c + 1u) % 3u)] = 0u;
+__global__ void k_fFinish(Batch Bt) {
+    if (threadIdx.x == 0) {
+        FOR_ITEMS(Bt, L_ONE, ot) {
+            ITEM_WORLD(Bt, ot, D, w, unused_);
+            (void)unused_;
+            for (uint32_t c = D.st->cycle; c < Bt.max_cycles; c++)
+                D.blocks[w.countSlot(COUNT_RESIDUAL + (c + 1u) % 3u)] = 0u;
+        }
     }
-    FAST_FOR_ACTIVE(w, wid) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        FAST_ITEM(Bt, it, D, F, w, wid);
+        const Lvl& L0 = F.L[0];
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         uint32_t i = w.cellIndex(c);
@@ -995,6 +1033,7 @@ __global__ void k_fFinish(Fast F) {
         *w.gwp(i, G_REGION) = 0u;
     }
 }
+
 
 // ================================================================ the persistent solve
 //
@@ -1038,102 +1077,6 @@ __device__ bool gridBarrier(StepState* st, uint32_t nblocks) {
     }
     __syncthreads();
     return s_ok != 0;
-}
-
-// One coarse cell of restrictLevel (fluid.wgsl:2342-2377), level l from l - 1.
-__device__ void restrictCell(const Fast& F, const W& w, uint32_t l, uint32_t j) {
-    const Dev& D = F.D;
-    const int lw = (int)D.level_w[l];
-    const int cx = (int)(j % (uint32_t)lw), cy = (int)(j / (uint32_t)lw);
-    const Lvl& V = F.L[l];
-    const int span = 1 << l;
-    if (span <= BLOCK) {
-        I2 b{cx * span / BLOCK, cy * span / BLOCK};
-        if (w.inBlocks(b) && (D.blocks[w.stateSlot(w.blockIndex(b))] & ACTIVE) == 0u) {
-            V.px[j] = 0.0f; V.py[j] = 0.0f; V.rx[j] = 0.0f; V.ry[j] = 0.0f; V.rho[j] = 0.0f;
-            return;
-        }
-    }
-    const Lvl& U = F.L[l - 1];
-    const int uw = (int)D.level_w[l - 1], uh = (int)D.level_h[l - 1];
-    const float h2 = (float)(1u << (2u * (l - 1u)));
-    const float* pin = l == 1u ? F.pin : nullptr;
-    float fluid = 0.0f, sum = 0.0f, rx = 0.0f, ry = 0.0f;
-    bool air = false;
-    for (int q = 0; q < 4; q++) {
-        int kx = 2 * cx + (q & 1), ky = 2 * cy + (q >> 1);
-        if (kx >= uw || ky >= uh) continue;
-        uint32_t k = (uint32_t)ky * (uint32_t)uw + (uint32_t)kx;
-        float rho = U.rho[k];
-        if (rho == 0.0f) air = true;
-        else if (rho > 0.0f) {
-            fluid = fluid + 1.0f;
-            sum = sum + rho;
-            V2 r = residualStored(U, pin, k, kx, ky, uw, uh, h2);
-            rx = rx + r.x;
-            ry = ry + r.y;
-        }
-    }
-    const float rho = air ? 0.0f : (fluid > 0.0f ? sum / fluid : -1.0f);
-    V.px[j] = 0.0f;
-    V.py[j] = 0.0f;
-    V.rx[j] = rho > 0.0f ? rx * 0.25f : 0.0f;
-    V.ry[j] = rho > 0.0f ? ry * 0.25f : 0.0f;
-    V.rho[j] = rho;
-}
-
-// One cell of smoothAt (fluid.wgsl:2318-2334) on level l >= 1.
-__device__ void smoothCell(const Fast& F, uint32_t l, int color, bool first, uint32_t j) {
-    const Dev& D = F.D;
-    const int lw = (int)D.level_w[l], lh = (int)D.level_h[l];
-    const int cx = (int)(j % (uint32_t)lw), cy = (int)(j / (uint32_t)lw);
-    if (((cx + cy) & 1) != color) return;
-    const Lvl& V = F.L[l];
-    const float rho = V.rho[j];
-    if (rho <= 0.0f) return;
-    float b[4];
-    float dg;
-    if (first) {
-        dg = 0.0f;
-        for (int d = 0; d < 4; d++) {
-            b[d] = 0.0f;
-            if (!nbrIn(cx, cy, lw, lh, d)) continue;
-            float r = V.rho[nbr(j, cx, cy, lw, lh, d)];
-            if (r < 0.0f) continue;
-            b[d] = faceBeta(rho, r);
-            dg = dg + b[d];
-        }
-        V.b0[j] = b[0]; V.b1[j] = b[1]; V.b2[j] = b[2]; V.b3[j] = b[3];
-        V.diag[j] = dg;
-    } else {
-        b[0] = V.b0[j]; b[1] = V.b1[j]; b[2] = V.b2[j]; b[3] = V.b3[j];
-        dg = V.diag[j];
-    }
-    if (dg <= 0.0f) return;
-    float sx = 0.0f, sy = 0.0f;
-#pragma unroll
-    for (int d = 0; d < 4; d++) {
-        uint32_t n = nbr(j, cx, cy, lw, lh, d);
-        sx = sx + b[d] * V.px[n];
-        sy = sy + b[d] * V.py[n];
-    }
-    const float h2 = (float)(1u << (2u * l));
-    const float ex = V.px[j], ey = V.py[j];
-    V.px[j] = mixf(ex, (sx - h2 * V.rx[j]) / dg, 1.0f);
-    V.py[j] = mixf(ey, (sy - h2 * V.ry[j]) / dg, 1.0f);
-}
-
-// One cell of prolong (fluid.wgsl:2459-2470), level l from l + 1.
-__device__ void prolongCell(const Fast& F, uint32_t l, uint32_t j) {
-    const Dev& D = F.D;
-    const int lw = (int)D.level_w[l];
-    const Lvl& V = F.L[l];
-    if (V.rho[j] <= 0.0f) return;
-    const Lvl& U = F.L[l + 1];
-    V2 e = prolongedFrom(U.rho, U.px, U.py, (int)D.level_w[l + 1], (int)D.level_h[l + 1], (int)(j % (uint32_t)lw),
-                         (int)(j / (uint32_t)lw));
-    V.px[j] = V.px[j] + e.x;
-    V.py[j] = V.py[j] + e.y;
 }
 
 // relaxTile (fluid.wgsl:2109-2182), four tiles a 256-thread CTA.
@@ -1257,26 +1200,26 @@ __global__ void __launch_bounds__(256, 4) k_fSolve(Fast F, int shifted) {
         if (!gridBarrier(st, nb)) return;
         for (uint32_t l = 1; l < lp; l++) {
             const uint32_t n = D.level_w[l] * D.level_h[l];
-            for (uint32_t j = gt; j < n; j += gn) restrictCell(F, w, l, j);
+            for (uint32_t j = gt; j < n; j += gn) restrictCell(F.D, F, w, l, j);
             if (!gridBarrier(st, nb)) return;
             for (int color = 0; color < 2; color++) {
-                for (uint32_t j = gt; j < n; j += gn) smoothCell(F, l, color, cycle == 0u, j);
+                for (uint32_t j = gt; j < n; j += gn) smoothCell(F.D, F, l, color, cycle == 0u, j);
                 if (!gridBarrier(st, nb)) return;
             }
         }
         {
             const uint32_t n = D.level_w[lp] * D.level_h[lp];
-            for (uint32_t j = gt; j < n; j += gn) restrictCell(F, w, lp, j);
+            for (uint32_t j = gt; j < n; j += gn) restrictCell(F.D, F, w, lp, j);
             if (!gridBarrier(st, nb)) return;
         }
-        if (blockIdx.x == 0) coarseLevels(F, w, lp, sm_coarse, s_off);
+        if (blockIdx.x == 0) coarseLevels(F.D, F, w, lp, sm_coarse, s_off);
         if (!gridBarrier(st, nb)) return;
         for (uint32_t l = lp - 1; l >= 1; l--) {
             const uint32_t n = D.level_w[l] * D.level_h[l];
-            for (uint32_t j = gt; j < n; j += gn) prolongCell(F, l, j);
+            for (uint32_t j = gt; j < n; j += gn) prolongCell(F.D, F, l, j);
             if (!gridBarrier(st, nb)) return;
             for (int color = 0; color < 2; color++) {
-                for (uint32_t j = gt; j < n; j += gn) smoothCell(F, l, color, false, j);
+                for (uint32_t j = gt; j < n; j += gn) smoothCell(F.D, F, l, color, false, j);
                 if (!gridBarrier(st, nb)) return;
             }
         }
@@ -1507,101 +1450,89 @@ __global__ void __launch_bounds__(256, 4) k_fSolve(Fast F, int shifted) {
     }
 }
 
-unsigned activeGrid(const Dev& D) {
-    unsigned g = 148u * 32u;
-    return D.B < g ? (D.B ? D.B : 1u) : g;
-}
-
-// 256-thread CTAs of four tiles each
-unsigned tileGrid4(const Dev& D) {
-    unsigned n = (D.B + 3u) / 4u, g = 148u * 8u;
-    return n < g ? (n ? n : 1u) : g;
-}
-
 }  // namespace
 
-size_t fast_coarse_smem(const Fast& F) {
+size_t fast_coarse_smem(const Dev& D, uint32_t lc) {
     size_t n = 0;
-    for (uint32_t l = F.lc; l <= F.D.levels; l++) n += (size_t)F.D.level_w[l] * F.D.level_h[l];
+    for (uint32_t l = lc; l <= D.levels; l++) n += (size_t)D.level_w[l] * D.level_h[l];
     return 5u * n * sizeof(float);
 }
 
-void fast_zero_level0(const Fast& F, cudaStream_t s) { k_fZero<<<148 * 4, 256, 0, s>>>(F); }
+void fast_zero_level0(const FastW& F, uint32_t cells, cudaStream_t s) { k_fZero<<<148 * 4, 256, 0, s>>>(F, cells); }
 
-void fast_setup(const Fast& F, cudaStream_t s, const Marker* m) {
-        if (m) m->fn(m->ctx, WIG_SLOT_F_SETUP, 0);
-    k_fSetup<<<tileGrid4(F.D), 256, 0, s>>>(F);
+void fast_setup(const Batch& Bt, const BatchShape& S, cudaStream_t s, const Marker* m) {
+    if (m) m->fn(m->ctx, WIG_SLOT_F_SETUP, 0);
+    k_fSetup<<<list_grid(S, L_ACT4, 8), 256, 0, s>>>(Bt);
     if (m) m->fn(m->ctx, WIG_SLOT_F_SETUP, 1);
 }
 
-uint32_t fast_cycle(const Fast& F, bool shifted, cudaStream_t s, const Marker* m) {
-    const Dev& D = F.D;
-    const unsigned G = activeGrid(D);
+uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, cudaStream_t s, const Marker* m) {
+    const unsigned G = list_grid(S, L_ACT, 32), G4 = list_grid(S, L_ACT4, 8), GR = list_grid(S, L_RELAX, 32);
     uint32_t launches = 0;
-    auto cells = [&](uint32_t l) { return (D.level_w[l] * D.level_h[l] + 255u) / 256u; };
     auto mark = [&](int slot, int phase) {
         if (m) m->fn(m->ctx, slot, phase);
         if (phase) launches++;
     };
+    auto cells = [&](uint32_t list) { return list_grid(S, list, 8); };
     mark(WIG_SLOT_F_LOOP, 0);
-    k_fLoopStart<<<1, 32, 0, s>>>(F);
+    k_fLoopStart<<<list_grid(S, L_ONE, 1), 32, 0, s>>>(Bt);
     mark(WIG_SLOT_F_LOOP, 1);
     mark(WIG_SLOT_F_RELAX, 0);
-    k_fRelax<<<G, 64, 0, s>>>(F, shifted ? BLOCK / 2 : 0);
+    k_fRelax<<<GR, 64, 0, s>>>(Bt, 0);
     mark(WIG_SLOT_F_RELAX, 1);
-    for (uint32_t l = 1; l < F.lc; l++) {
+    // down: each world restricts its levels 1..lc by themselves and smooths
+    // those above lc, then its levels from lc are the coarse kernel's
+    for (uint32_t l = 1; l <= S.lc_max; l++) {
         mark(WIG_SLOT_F_RESTRICT, 0);
-        k_fRestrict<<<cells(l), 256, 0, s>>>(F, l);
+        k_fRestrict<<<cells(L_RES + l - 1u), 256, 0, s>>>(Bt, l);
         mark(WIG_SLOT_F_RESTRICT, 1);
+        if (S.max_items[L_SM + l - 1u] == 0u) continue;
         mark(WIG_SLOT_F_SMOOTH, 0);
-        k_fSmooth<<<cells(l), 256, 0, s>>>(F, l, 0);
+        k_fSmooth<<<cells(L_SM + l - 1u), 256, 0, s>>>(Bt, l, 0);
         mark(WIG_SLOT_F_SMOOTH, 1);
         mark(WIG_SLOT_F_SMOOTH, 0);
-        k_fSmooth<<<cells(l), 256, 0, s>>>(F, l, 1);
+        k_fSmooth<<<cells(L_SM + l - 1u), 256, 0, s>>>(Bt, l, 1);
         mark(WIG_SLOT_F_SMOOTH, 1);
     }
-    mark(WIG_SLOT_F_RESTRICT, 0);
-    k_fRestrict<<<cells(F.lc), 256, 0, s>>>(F, F.lc);
-    mark(WIG_SLOT_F_RESTRICT, 1);
-    size_t smem = fast_coarse_smem(F);
     mark(WIG_SLOT_F_COARSE, 0);
-    k_fCoarse<<<1, 1024, smem, s>>>(F);
+    k_fCoarse<<<list_grid(S, L_ONE, 1), 1024, S.coarse_smem, s>>>(Bt);
     mark(WIG_SLOT_F_COARSE, 1);
-    for (uint32_t l = F.lc - 1; l >= 1; l--) {
+    for (uint32_t l = S.lc_max; l >= 1; l--) {
+        if (S.max_items[L_SM + l - 1u] == 0u) continue;
         mark(WIG_SLOT_F_PROLONG, 0);
-        k_fProlong<<<cells(l), 256, 0, s>>>(F, l);
+        k_fProlong<<<cells(L_SM + l - 1u), 256, 0, s>>>(Bt, l);
         mark(WIG_SLOT_F_PROLONG, 1);
         mark(WIG_SLOT_F_SMOOTH, 0);
-        k_fSmooth<<<cells(l), 256, 0, s>>>(F, l, 0);
+        k_fSmooth<<<cells(L_SM + l - 1u), 256, 0, s>>>(Bt, l, 0);
         mark(WIG_SLOT_F_SMOOTH, 1);
         mark(WIG_SLOT_F_SMOOTH, 0);
-        k_fSmooth<<<cells(l), 256, 0, s>>>(F, l, 1);
+        k_fSmooth<<<cells(L_SM + l - 1u), 256, 0, s>>>(Bt, l, 1);
         mark(WIG_SLOT_F_SMOOTH, 1);
     }
     mark(WIG_SLOT_F_PROLONG_FINE, 0);
-    k_fProlongFine<<<G, 64, 0, s>>>(F);
+    k_fProlongFine<<<G, 64, 0, s>>>(Bt);
     mark(WIG_SLOT_F_PROLONG_FINE, 1);
     mark(WIG_SLOT_F_RELAX, 0);
-    k_fRelax<<<G, 64, 0, s>>>(F, shifted ? 0 : BLOCK / 2);
+    k_fRelax<<<GR, 64, 0, s>>>(Bt, 1);
     mark(WIG_SLOT_F_RELAX, 1);
     mark(WIG_SLOT_F_RHO_BETA, 0);
-    k_fRhoBeta<<<tileGrid4(D), 256, 0, s>>>(F);
+    k_fRhoBeta<<<G4, 256, 0, s>>>(Bt);
     mark(WIG_SLOT_F_RHO_BETA, 1);
     mark(WIG_SLOT_F_DIRECTION, 0);
-    k_fDirection<<<G, 64, 0, s>>>(F);
+    k_fDirection<<<G, 64, 0, s>>>(Bt);
     mark(WIG_SLOT_F_DIRECTION, 1);
     mark(WIG_SLOT_F_APPLY_ALPHA, 0);
-    k_fApplyAlpha<<<tileGrid4(D), 256, 0, s>>>(F);
+    k_fApplyAlpha<<<G4, 256, 0, s>>>(Bt);
     mark(WIG_SLOT_F_APPLY_ALPHA, 1);
     mark(WIG_SLOT_F_UPDATE, 0);
-    k_fUpdate<<<tileGrid4(D), 256, 0, s>>>(F);
+    k_fUpdate<<<G4, 256, 0, s>>>(Bt);
     mark(WIG_SLOT_F_UPDATE, 1);
     return launches;
 }
 
-void fast_finish(const Fast& F, cudaStream_t s, const Marker* m) {
+void fast_finish(const Batch& Bt, const BatchShape& S, cudaStream_t s, const Marker* m) {
     if (m) m->fn(m->ctx, WIG_SLOT_F_FINISH, 0);
-    k_fFinish<<<activeGrid(F.D), 64, 0, s>>>(F);
+    k_fFinish<<<list_grid(S, L_ACT, 32), 64, 0, s>>>(Bt);
     if (m) m->fn(m->ctx, WIG_SLOT_F_FINISH, 1);
 }
 
@@ -1609,11 +1540,7 @@ cudaError_t fast_prepare_attributes(size_t smem) {
     return cudaFuncSetAttribute(k_fCoarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-size_t fast_solve_smem(const Fast& F) {
-    size_t n = 0;
-    for (uint32_t l = F.lp; l <= F.D.levels; l++) n += (size_t)F.D.level_w[l] * F.D.level_h[l];
-    return 5u * n * sizeof(float);
-}
+size_t fast_solve_smem(const Fast& F) { return fast_coarse_smem(F.D, F.lp); }
 
 cudaError_t fast_solve_grid(const Fast& F, uint32_t* grid) {
     int dev = 0, sms = 0, per = 0;

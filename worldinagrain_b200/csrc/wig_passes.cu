@@ -189,10 +189,14 @@ __device__ V2 prolonged(const W& w, uint32_t l, I2 c) {
 
 // ================================================================ bookkeeping
 
-// sync / syncMarks (fluid.wgsl:608-659): a CTA per block of the world.
-__global__ void k_sync(Dev D, int claims) {
-    W w(D);
-    I2 c{(int)blockIdx.x * BLOCK + (int)(threadIdx.x & 7u), (int)blockIdx.y * BLOCK + (int)(threadIdx.x >> 3)};
+// sync / syncMarks (fluid.wgsl:608-659): a CTA per block of the world
+// (syncMarks: no claims, as a world's bookkeeping-only step takes it).
+__global__ void k_sync(Batch Bt, int sync_claims) {
+  FOR_ITEMS(Bt, L_WB, it) {
+    ITEM_WORLD(Bt, it, D, w, n);
+    const bool claims = sync_claims && D.st->book == 0u;
+    const I2 b{(int)(n % D.BW), (int)(n / D.BW)};
+    I2 c{b.x * BLOCK + (int)(threadIdx.x & 7u), b.y * BLOCK + (int)(threadIdx.x >> 3)};
     bool here = false;
     if (w.inWorld(c)) {
         uint32_t i = w.cellIndex(c);
@@ -209,7 +213,8 @@ __global__ void k_sync(Dev D, int claims) {
             here = true;
         }
     }
-    if (__syncthreads_or(here) && threadIdx.x == 0) atomicOr(&D.blocks[w.blockIndex(I2{(int)blockIdx.x, (int)blockIdx.y})], MARK_LIQUID);
+    if (__syncthreads_or(here) && threadIdx.x == 0) atomicOr(&D.blocks[n], MARK_LIQUID);
+  }
 }
 
 __device__ void markBlockOf(const W& w, float px, float py) {
@@ -306,11 +311,12 @@ __device__ __forceinline__ void storeParticle(const W& w, uint32_t m, V2 pos, V2
 }
 
 // syncParticles (fluid.wgsl:767-831): a thread per particle of `sorted`.
-__global__ void k_syncParticles(Dev D) {
-    W w(D);
+__global__ void k_syncParticles(Batch Bt) {
+  FOR_ITEMS(Bt, L_PS, qi) {
+    ITEM_WORLD(Bt, qi, D, w, chunk);
     uint32_t live = min(D.sorted[0], D.cap);
-    uint32_t k0 = blockIdx.x * blockDim.x;
-    if (k0 >= live) return;  // whole CTA past the particles (uniform)
+    uint32_t k0 = chunk * blockDim.x;
+    if (k0 >= live) continue;  // whole CTA past the particles (uniform)
     uint32_t k = k0 + threadIdx.x;
     bool keep = false;
     V2 pos{0, 0}, vel{0, 0};
@@ -361,6 +367,7 @@ __global__ void k_syncParticles(Dev D) {
     }
     uint32_t m = takePlaces(&D.parts[0], keep ? 1u : 0u);
     if (keep && m < D.cap) storeParticle(w, m, pos, vel, word, temp, id, aff);
+  }
 }
 
 // seedId, seedPos (fluid.wgsl:835-855)
@@ -373,9 +380,11 @@ __device__ uint32_t seedId(const Dev& D, I2 c, uint32_t j) {
 }
 
 // syncSeed (fluid.wgsl:863-890): a CTA per block of the world.
-__global__ void k_syncSeed(Dev D) {
-    W w(D);
-    I2 c{(int)blockIdx.x * BLOCK + (int)(threadIdx.x & 7u), (int)blockIdx.y * BLOCK + (int)(threadIdx.x >> 3)};
+__global__ void k_syncSeed(Batch Bt) {
+  FOR_ITEMS(Bt, L_WB, qi) {
+    ITEM_WORLD(Bt, qi, D, w, blk);
+    if (D.st->book) continue;
+    I2 c{(int)(blk % D.BW) * BLOCK + (int)(threadIdx.x & 7u), (int)(blk / D.BW) * BLOCK + (int)(threadIdx.x >> 3)};
     uint32_t n = 0;
     uint4 v = make_uint4(0, 0, 0, 0);
     Rng g;
@@ -414,13 +423,16 @@ __global__ void k_syncSeed(Dev D) {
                           make_float4(0, 0, 0, 0));
         }
     }
+  }
 }
 
 // compact (fluid.wgsl:896-921): one CTA of 1024 threads, a contiguous run of
 // blocks each, so the lists come out in block-index order.
-__global__ void __launch_bounds__(1024) k_compact(Dev D) {
-    W w(D);
-    __shared__ uint32_t sa[1024], sr[1024];
+__global__ void __launch_bounds__(1024) k_compact(Batch Bt) {
+  __shared__ uint32_t sa[1024], sr[1024];
+  FOR_ITEMS(Bt, L_ONE_ALL, it) {
+    ITEM_WORLD(Bt, it, D, w, unused_);
+    (void)unused_;
     const uint32_t per = (D.B + 1023u) / 1024u;
     const uint32_t lo = min(threadIdx.x * per, D.B), hi = min(lo + per, D.B);
     uint32_t na = 0, nr = 0;
@@ -470,13 +482,14 @@ __global__ void __launch_bounds__(1024) k_compact(Dev D) {
         D.blocks[w.countSlot(COUNT_ACTIVE)] = sa[1023];
         D.blocks[w.countSlot(COUNT_RETIRED)] = sr[1023];
     }
+    __syncthreads();
+  }
 }
 
 // retire (fluid.wgsl:924-951)
-__global__ void k_retire(Dev D) {
-    W w(D);
-    const uint32_t nr = D.blocks[w.countSlot(COUNT_RETIRED)];
-    for (uint32_t wid = blockIdx.x; wid < nr; wid += gridDim.x) {
+__global__ void k_retire(Batch Bt) {
+    FOR_ITEMS(Bt, L_RET, it) {
+        ITEM_WORLD(Bt, it, D, w, wid);
         uint32_t n = D.blocks[w.retiredSlot(wid)];
         I2 c{(int)(n % D.BW) * BLOCK + (int)(threadIdx.x & 7u), (int)(n / D.BW) * BLOCK + (int)(threadIdx.x >> 3)};
         if (!w.inWorld(c)) continue;
@@ -499,9 +512,9 @@ __global__ void k_retire(Dev D) {
 }
 
 // clear (fluid.wgsl:962-985)
-__global__ void k_clear(Dev D) {
-    W w(D);
-    FOR_ACTIVE(D, w, wid) {
+__global__ void k_clear(Batch Bt) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        ITEM_WORLD(Bt, it, D, w, wid);
         I2 b = w.activeBlock(wid);
         if (threadIdx.x == 0) D.blocks[w.blockIndex(b)] = 0u;
         I2 c = lidCell(w, wid);
@@ -567,10 +580,9 @@ __device__ __forceinline__ void splatDensity(const W& w, float px, float py, flo
 }
 
 // gather (fluid.wgsl:1017-1039), no air bound: no air push.
-__global__ void k_gather(Dev D) {
-    W w(D);
+__device__ __forceinline__ void gatherOne(const Dev& D, const W& w, uint32_t chunk) {
     uint32_t live = min(D.parts[0], D.cap);
-    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t k = chunk * blockDim.x + threadIdx.x;
     if (k >= live) return;
     const uint4* it = w.items(D.parts);
     uint4 mo = it[k], stt = it[D.cap + k], af = it[2u * D.cap + k];
@@ -583,6 +595,12 @@ __global__ void k_gather(Dev D) {
     atomicAdd(w.gwp(home, G_COUNT), 1u);
     atomicAdd(w.gwp(home, G_MASS), f2u(rnd_even(w.liquidDensity(stt.x, temp) * FIX)));
     splatDensity(w, px, py, w.liquidVolume(stt.x, temp));
+}
+__global__ void k_gather(Batch Bt) {
+    FOR_ITEMS(Bt, L_PP, qi) {
+        ITEM_WORLD(Bt, qi, D, w, chunk);
+        gatherOne(D, w, chunk);
+    }
 }
 
 // ================================================================ classify
@@ -599,9 +617,9 @@ __device__ bool wasOpen(const W& w, I2 q) {
 }
 
 // sealJoin (fluid.wgsl:1531-1543)
-__global__ void k_sealJoin(Dev D) {
-    W w(D);
-    FOR_ACTIVE(D, w, wid) {
+__global__ void k_sealJoin(Batch Bt) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        ITEM_WORLD(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c) || !mayBeSealed(w, c)) continue;
         for (int d = 0; d < 2; d++) {
@@ -611,9 +629,9 @@ __global__ void k_sealJoin(Dev D) {
     }
 }
 // sealAnchor (fluid.wgsl:1545-1554)
-__global__ void k_sealAnchor(Dev D) {
-    W w(D);
-    FOR_ACTIVE(D, w, wid) {
+__global__ void k_sealAnchor(Batch Bt) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        ITEM_WORLD(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c) || !mayBeSealed(w, c)) continue;
         if (wasOpen(w, beside(c, 0)) || wasOpen(w, beside(c, 1)) || wasOpen(w, beside(c, 2)) || wasOpen(w, beside(c, 3)))
@@ -633,12 +651,12 @@ __device__ float columnWeight(const W& w, I2 p, float density) {
 }
 
 // classify (fluid.wgsl:1578-1696), no bodies.
-__global__ void k_classify(Dev D) {
-    W w(D);
+__global__ void k_classify(Batch Bt) {
     __shared__ uint32_t blockBits;
-    const uint32_t frame = D.st->P.frame;
-    const uint32_t mine = 1u << (frame & 1u), fall0 = 4u << (frame & 1u);
-    FOR_ACTIVE(D, w, wid) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        ITEM_WORLD(Bt, it, D, w, wid);
+        const uint32_t frame = D.st->P.frame;
+        const uint32_t mine = 1u << (frame & 1u), fall0 = 4u << (frame & 1u);
         if (threadIdx.x == 0) blockBits = 0u;
         __syncthreads();
         I2 p = lidCell(w, wid);
@@ -753,9 +771,9 @@ __device__ void setFace(const W& w, I2 at, bool isU) {
 }
 
 // setFaces (fluid.wgsl:1982-1994)
-__global__ void k_setFaces(Dev D) {
-    W w(D);
-    FOR_ACTIVE(D, w, wid) {
+__global__ void k_setFaces(Batch Bt) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        ITEM_WORLD(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         int fs[4][3];
@@ -792,9 +810,10 @@ __device__ void viscousFace(const W& w, I2 at, bool isU, int color) {
 }
 
 // viscosityRed / viscosityBlack / unpress (fluid.wgsl:3409-3466)
-__global__ void k_viscosity(Dev D, int color) {
-    W w(D);
-    FOR_ACTIVE(D, w, wid) {
+__global__ void k_viscosity(Batch Bt, int color) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        ITEM_WORLD(Bt, it, D, w, wid);
+        if (color < 2 && D.st->viscous == 0u) continue;  // this world's step has no sweeps
         I2 b = w.activeBlock(wid);
         if ((w.statesOf(I2{b.x - 1, b.y - 1}, I2{b.x + 1, b.y + 1}) & HAS_VISCOUS) == 0u) continue;
         I2 c = lidCell(w, wid);
@@ -824,13 +843,18 @@ __global__ void k_viscosity(Dev D, int color) {
 }
 
 // divergence (fluid.wgsl:1996-2025), posedRoom 1 with no bodies.
-__global__ void k_divergence(Dev D) {
-    W w(D);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        D.blocks[w.countSlot(COUNT_RESIDUAL)] = 0u;
-        D.blocks[w.countSlot(COUNT_CYCLES)] = 0u;
+__global__ void k_divergence(Batch Bt) {
+    // once a world: its residual and iteration words cleared
+    if (threadIdx.x == 0) {
+        FOR_ITEMS(Bt, L_ONE, ot) {
+            ITEM_WORLD(Bt, ot, D, w, unused_);
+            (void)unused_;
+            D.blocks[w.countSlot(COUNT_RESIDUAL)] = 0u;
+            D.blocks[w.countSlot(COUNT_CYCLES)] = 0u;
+        }
     }
-    FOR_ACTIVE(D, w, wid) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        ITEM_WORLD(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         uint32_t i = w.cellIndex(c);
@@ -847,9 +871,9 @@ __global__ void k_divergence(Dev D) {
 // ================================================================ the solve's start
 
 // cgStart (fluid.wgsl:2665-2674)
-__global__ void k_cgStart(Dev D) {
-    W w(D);
-    FOR_ACTIVE(D, w, wid) {
+__global__ void k_cgStart(Batch Bt) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        ITEM_WORLD(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         uint32_t i = w.cellIndex(c);
@@ -858,9 +882,9 @@ __global__ void k_cgStart(Dev D) {
     }
 }
 // cgJoin (fluid.wgsl:2677-2689)
-__global__ void k_cgJoin(Dev D) {
-    W w(D);
-    FOR_ACTIVE(D, w, wid) {
+__global__ void k_cgJoin(Batch Bt) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        ITEM_WORLD(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c) || w.gridAt(c).z <= 0.0f) continue;
         for (int d = 0; d < 2; d++) {
@@ -870,9 +894,9 @@ __global__ void k_cgJoin(Dev D) {
     }
 }
 // cgAnchor (fluid.wgsl:2692-2705)
-__global__ void k_cgAnchor(Dev D) {
-    W w(D);
-    FOR_ACTIVE(D, w, wid) {
+__global__ void k_cgAnchor(Batch Bt) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        ITEM_WORLD(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c) || w.gridAt(c).z <= 0.0f) continue;
         for (int d = 0; d < 4; d++) {
@@ -1505,13 +1529,18 @@ __global__ void k_cgFinish(Dev D) {
 // ================================================================ projection, extrapolation
 
 // project / projectFace (fluid.wgsl:2897-2942), no bodies.
-__global__ void k_project(Dev D) {
-    W w(D);
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        uint32_t cyc = D.blocks[w.countSlot(COUNT_CYCLES)];
-        atomicMax(&D.blocks[w.countSlot(COUNT_MOST_CYCLES)], cyc);
+__global__ void k_project(Batch Bt) {
+    // once a world: the most iterations any step took
+    if (threadIdx.x == 0) {
+        FOR_ITEMS(Bt, L_ONE, ot) {
+            ITEM_WORLD(Bt, ot, D, w, unused_);
+            (void)unused_;
+            uint32_t cyc = D.blocks[w.countSlot(COUNT_CYCLES)];
+            atomicMax(&D.blocks[w.countSlot(COUNT_MOST_CYCLES)], cyc);
+        }
     }
-    FOR_ACTIVE(D, w, wid) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        ITEM_WORLD(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         int fs[4][3];
@@ -1536,9 +1565,9 @@ __global__ void k_project(Dev D) {
 }
 
 // extrapolate / extrapolateFurther (fluid.wgsl:3226-3275)
-__global__ void k_extrapolate(Dev D, uint32_t layer) {
-    W w(D);
-    FOR_ACTIVE(D, w, wid) {
+__global__ void k_extrapolate(Batch Bt, uint32_t layer) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        ITEM_WORLD(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         int fs[4][3];
@@ -1649,10 +1678,9 @@ __device__ __forceinline__ V2 clampSpeed(V2 v) {
 }
 
 // advect (fluid.wgsl:3616-3694)
-__global__ void k_advect(Dev D) {
-    W w(D);
+__device__ __forceinline__ void advectOne(const Dev& D, const W& w, uint32_t chunk) {
     uint32_t live = min(D.parts[0], D.cap);
-    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t k = chunk * blockDim.x + threadIdx.x;
     if (k >= live) return;
     uint4* it = w.items(D.parts);
     uint4 mo = it[k], stt = it[D.cap + k];
@@ -1719,27 +1747,38 @@ __global__ void k_advect(Dev D) {
     }
     if ((w.elem(wordType(stt.x)).flags & F_IMPACT) != 0u && impact > IMPACT_SPEED) it[D.cap + k].x = wordWith(stt.x, FL_BURN);
 }
+__global__ void k_advect(Batch Bt) {
+    FOR_ITEMS(Bt, L_PP, qi) {
+        ITEM_WORLD(Bt, qi, D, w, chunk);
+        advectOne(D, w, chunk);
+    }
+}
 
 // ================================================================ sort
 
 // sortCount (fluid.wgsl:3700-3708)
-__global__ void k_sortCount(Dev D) {
-    W w(D);
+__device__ __forceinline__ void sortCountOne(const Dev& D, const W& w, uint32_t chunk) {
     uint32_t live = min(D.parts[0], D.cap);
-    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t k = chunk * blockDim.x + threadIdx.x;
     if (k >= live) return;
     uint4* it = w.items(D.parts);
     uint4 mo = it[k];
     uint32_t i = w.cellIndex(w.cellOf(__uint_as_float(mo.x), __uint_as_float(mo.y)));
     it[D.cap + k].w = atomicAdd(w.gwp(i, G_SORT), 1u);
 }
+__global__ void k_sortCount(Batch Bt) {
+    FOR_ITEMS(Bt, L_PP, qi) {
+        ITEM_WORLD(Bt, qi, D, w, chunk);
+        sortCountOne(D, w, chunk);
+    }
+}
 
 // scanBlocks (fluid.wgsl:3730-3753)
-__global__ void __launch_bounds__(64) k_scanBlocks(Dev D) {
-    W w(D);
+__global__ void __launch_bounds__(64) k_scanBlocks(Batch Bt) {
     __shared__ uint32_t tile[64];
-    const uint32_t fall0 = 4u << (D.st->P.frame & 1u);
-    FOR_ACTIVE(D, w, wid) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        ITEM_WORLD(Bt, it, D, w, wid);
+        const uint32_t fall0 = 4u << (D.st->P.frame & 1u);
         I2 c = lidCell(w, wid);
         uint32_t n = 0;
         if (w.inWorld(c)) n = w.gw(w.cellIndex(c), G_SORT);
@@ -1766,9 +1805,11 @@ __global__ void __launch_bounds__(64) k_scanBlocks(Dev D) {
 }
 
 // scanTotals (fluid.wgsl:3757-3780): one CTA of 256.
-__global__ void __launch_bounds__(256) k_scanTotals(Dev D) {
-    W w(D);
-    __shared__ uint32_t tile[256];
+__global__ void __launch_bounds__(256) k_scanTotals(Batch Bt) {
+  __shared__ uint32_t tile[256];
+  FOR_ITEMS(Bt, L_ONE, ot) {
+    ITEM_WORLD(Bt, ot, D, w, unused_);
+    (void)unused_;
     const uint32_t n = w.activeCount();
     const uint32_t per = (n + 255u) / 256u;
     const uint32_t lo = min(threadIdx.x * per, n), hi = min(lo + per, n);
@@ -1792,12 +1833,14 @@ __global__ void __launch_bounds__(256) k_scanTotals(Dev D) {
         D.sorted[0] = tile[255];
         D.blocks[w.countSlot(COUNT_PARTICLES)] = tile[255];
     }
+    __syncthreads();
+  }
 }
 
 // scanFinish (fluid.wgsl:3783-3790)
-__global__ void k_scanFinish(Dev D) {
-    W w(D);
-    FOR_ACTIVE(D, w, wid) {
+__global__ void k_scanFinish(Batch Bt) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        ITEM_WORLD(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         *w.gwp(w.cellIndex(c), G_START) += D.blocks[w.totalSlot(wid)];
@@ -1805,10 +1848,9 @@ __global__ void k_scanFinish(Dev D) {
 }
 
 // scatter (fluid.wgsl:3793-3808)
-__global__ void k_scatter(Dev D) {
-    W w(D);
+__device__ __forceinline__ void scatterOne(const Dev& D, const W& w, uint32_t chunk) {
     uint32_t live = min(D.parts[0], D.cap);
-    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t k = chunk * blockDim.x + threadIdx.x;
     if (k >= live) return;
     const uint4* it = w.items(D.parts);
     uint4 mo = it[k], stt = it[D.cap + k];
@@ -1819,6 +1861,12 @@ __global__ void k_scatter(Dev D) {
         so[m] = mo;
         so[D.cap + m] = stt;
         so[2u * D.cap + m] = it[2u * D.cap + k];
+    }
+}
+__global__ void k_scatter(Batch Bt) {
+    FOR_ITEMS(Bt, L_PP, qi) {
+        ITEM_WORLD(Bt, qi, D, w, chunk);
+        scatterOne(D, w, chunk);
     }
 }
 
@@ -1841,9 +1889,9 @@ __device__ uint32_t airTo(const W& w, I2 c, bool gas) {
     return NONE;
 }
 // rasterClaims (fluid.wgsl:3928-3948), no people.
-__global__ void k_rasterClaims(Dev D) {
-    W w(D);
-    FOR_ACTIVE(D, w, wid) {
+__global__ void k_rasterClaims(Batch Bt) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        ITEM_WORLD(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         uint32_t i = w.cellIndex(c);
@@ -1884,9 +1932,9 @@ __device__ __forceinline__ float exact_value(unsigned long long wsum, float scal
 }
 
 // raster (fluid.wgsl:3983-4119), no people, the air source unbound.
-__global__ void k_raster(Dev D) {
-    W w(D);
-    FOR_ACTIVE(D, w, wid) {
+__global__ void k_raster(Batch Bt) {
+    FOR_ITEMS(Bt, L_ACT, qi) {
+        ITEM_WORLD(Bt, qi, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         uint32_t i = w.cellIndex(c);
@@ -1988,9 +2036,9 @@ __global__ void k_raster(Dev D) {
 }
 
 // unpaint (fluid.wgsl:4163-4182)
-__global__ void k_unpaint(Dev D) {
-    W w(D);
-    FOR_ACTIVE(D, w, wid) {
+__global__ void k_unpaint(Batch Bt) {
+    FOR_ITEMS(Bt, L_ACT, it) {
+        ITEM_WORLD(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         uint32_t i = w.cellIndex(c);
@@ -2006,38 +2054,48 @@ __global__ void k_unpaint(Dev D) {
 
 // ================================================================ launch
 
-static inline unsigned particle_groups(const Dev& D) { return (D.cap + 255u) / 256u; }
 static inline unsigned block_grid(const Dev& D, unsigned per_sm) {
     unsigned g = 148u * per_sm;
     return D.B < g ? (D.B ? D.B : 1u) : g;
 }
 
-int launch_pass(const Dev& D, int pass, uint32_t level, uint32_t cycle, cudaStream_t s) {
-    const dim3 world((unsigned)D.BW, (unsigned)D.BH);
-    const unsigned G = block_grid(D, 32), P = particle_groups(D);
+unsigned list_grid(const BatchShape& S, uint32_t list, unsigned per_sm) {
+    const unsigned g = 148u * per_sm, n = S.max_items[list];
+    return n < g ? (n ? n : 1u) : g;
+}
+
+int launch_pass(const Batch& Bt, const BatchShape& S, const Dev& D0, int pass, uint32_t level, uint32_t cycle,
+                cudaStream_t s) {
+    // the passes shared by every form: over the batch's work lists
+    const unsigned A = list_grid(S, L_ACT, 32), WB = list_grid(S, L_WB, 32);
+    const unsigned PS = list_grid(S, L_PS, 8), PP = list_grid(S, L_PP, 8);
+    const unsigned RET = list_grid(S, L_RET, 32), ONE = list_grid(S, L_ONE, 2), ALL = list_grid(S, L_ONE_ALL, 2);
+    // the plain form's solve: world 0 alone
+    const unsigned G = block_grid(D0, 32);
     auto lvl = [&](uint32_t l) {
-        return dim3((D.level_w[l] + 7u) / 8u, (D.level_h[l] + 7u) / 8u);
+        return dim3((D0.level_w[l] + 7u) / 8u, (D0.level_h[l] + 7u) / 8u);
     };
+    const Dev& D = D0;
     switch (pass) {
-    case WIG_PASS_SYNC: k_sync<<<world, 64, 0, s>>>(D, 1); break;
-    case WIG_PASS_SYNC_MARKS: k_sync<<<world, 64, 0, s>>>(D, 0); break;
-    case WIG_PASS_SYNC_PARTICLES: k_syncParticles<<<P, 256, 0, s>>>(D); break;
-    case WIG_PASS_SYNC_SEED: k_syncSeed<<<world, 64, 0, s>>>(D); break;
-    case WIG_PASS_COMPACT: k_compact<<<1, 1024, 0, s>>>(D); break;
-    case WIG_PASS_RETIRE: k_retire<<<G, 64, 0, s>>>(D); break;
-    case WIG_PASS_CLEAR: k_clear<<<G, 64, 0, s>>>(D); break;
-    case WIG_PASS_GATHER: k_gather<<<P, 256, 0, s>>>(D); break;
-    case WIG_PASS_SEAL_JOIN: k_sealJoin<<<G, 64, 0, s>>>(D); break;
-    case WIG_PASS_SEAL_ANCHOR: k_sealAnchor<<<G, 64, 0, s>>>(D); break;
-    case WIG_PASS_CLASSIFY: k_classify<<<G, 64, 0, s>>>(D); break;
-    case WIG_PASS_SET_FACES: k_setFaces<<<G, 64, 0, s>>>(D); break;
-    case WIG_PASS_VISCOSITY_RED: k_viscosity<<<G, 64, 0, s>>>(D, 0); break;
-    case WIG_PASS_VISCOSITY_BLACK: k_viscosity<<<G, 64, 0, s>>>(D, 1); break;
-    case WIG_PASS_UNPRESS: k_viscosity<<<G, 64, 0, s>>>(D, 2); break;
-    case WIG_PASS_DIVERGENCE: k_divergence<<<G, 64, 0, s>>>(D); break;
-    case WIG_PASS_CG_START: k_cgStart<<<G, 64, 0, s>>>(D); break;
-    case WIG_PASS_CG_JOIN: k_cgJoin<<<G, 64, 0, s>>>(D); break;
-    case WIG_PASS_CG_ANCHOR: k_cgAnchor<<<G, 64, 0, s>>>(D); break;
+    case WIG_PASS_SYNC: k_sync<<<WB, 64, 0, s>>>(Bt, 1); break;
+    case WIG_PASS_SYNC_MARKS: k_sync<<<WB, 64, 0, s>>>(Bt, 0); break;
+    case WIG_PASS_SYNC_PARTICLES: k_syncParticles<<<PS, 256, 0, s>>>(Bt); break;
+    case WIG_PASS_SYNC_SEED: k_syncSeed<<<WB, 64, 0, s>>>(Bt); break;
+    case WIG_PASS_COMPACT: k_compact<<<ALL, 1024, 0, s>>>(Bt); break;
+    case WIG_PASS_RETIRE: k_retire<<<RET, 64, 0, s>>>(Bt); break;
+    case WIG_PASS_CLEAR: k_clear<<<A, 64, 0, s>>>(Bt); break;
+    case WIG_PASS_GATHER: k_gather<<<PP, 256, 0, s>>>(Bt); break;
+    case WIG_PASS_SEAL_JOIN: k_sealJoin<<<A, 64, 0, s>>>(Bt); break;
+    case WIG_PASS_SEAL_ANCHOR: k_sealAnchor<<<A, 64, 0, s>>>(Bt); break;
+    case WIG_PASS_CLASSIFY: k_classify<<<A, 64, 0, s>>>(Bt); break;
+    case WIG_PASS_SET_FACES: k_setFaces<<<A, 64, 0, s>>>(Bt); break;
+    case WIG_PASS_VISCOSITY_RED: k_viscosity<<<A, 64, 0, s>>>(Bt, 0); break;
+    case WIG_PASS_VISCOSITY_BLACK: k_viscosity<<<A, 64, 0, s>>>(Bt, 1); break;
+    case WIG_PASS_UNPRESS: k_viscosity<<<A, 64, 0, s>>>(Bt, 2); break;
+    case WIG_PASS_DIVERGENCE: k_divergence<<<A, 64, 0, s>>>(Bt); break;
+    case WIG_PASS_CG_START: k_cgStart<<<A, 64, 0, s>>>(Bt); break;
+    case WIG_PASS_CG_JOIN: k_cgJoin<<<A, 64, 0, s>>>(Bt); break;
+    case WIG_PASS_CG_ANCHOR: k_cgAnchor<<<A, 64, 0, s>>>(Bt); break;
     case WIG_PASS_CG_RESIDUAL: k_cgResidual<<<G, 64, 0, s>>>(D); break;
     case WIG_PASS_CG_PREPARE: k_cgPrepare<<<G, 64, 0, s>>>(D); break;
     case WIG_PASS_RELAX_RIMS: k_relaxRims<<<G, 64, 0, s>>>(D, cycle); break;
@@ -2056,18 +2114,18 @@ int launch_pass(const Dev& D, int pass, uint32_t level, uint32_t cycle, cudaStre
     case WIG_PASS_CG_ALPHA: k_cgAlpha<<<1, 256, 0, s>>>(D, cycle); break;
     case WIG_PASS_CG_UPDATE: k_cgUpdate<<<G, 64, 0, s>>>(D, cycle); break;
     case WIG_PASS_CG_FINISH: k_cgFinish<<<G, 64, 0, s>>>(D); break;
-    case WIG_PASS_PROJECT: k_project<<<G, 64, 0, s>>>(D); break;
-    case WIG_PASS_EXTRAPOLATE: k_extrapolate<<<G, 64, 0, s>>>(D, 1u); break;
-    case WIG_PASS_EXTRAPOLATE_FURTHER: k_extrapolate<<<G, 64, 0, s>>>(D, 2u); break;
-    case WIG_PASS_ADVECT: k_advect<<<P, 256, 0, s>>>(D); break;
-    case WIG_PASS_SORT_COUNT: k_sortCount<<<P, 256, 0, s>>>(D); break;
-    case WIG_PASS_SCAN_BLOCKS: k_scanBlocks<<<G, 64, 0, s>>>(D); break;
-    case WIG_PASS_SCAN_TOTALS: k_scanTotals<<<1, 256, 0, s>>>(D); break;
-    case WIG_PASS_SCAN_FINISH: k_scanFinish<<<G, 64, 0, s>>>(D); break;
-    case WIG_PASS_SCATTER: k_scatter<<<P, 256, 0, s>>>(D); break;
-    case WIG_PASS_RASTER_CLAIMS: k_rasterClaims<<<G, 64, 0, s>>>(D); break;
-    case WIG_PASS_RASTER: k_raster<<<G, 64, 0, s>>>(D); break;
-    case WIG_PASS_UNPAINT: k_unpaint<<<G, 64, 0, s>>>(D); break;
+    case WIG_PASS_PROJECT: k_project<<<A, 64, 0, s>>>(Bt); break;
+    case WIG_PASS_EXTRAPOLATE: k_extrapolate<<<A, 64, 0, s>>>(Bt, 1u); break;
+    case WIG_PASS_EXTRAPOLATE_FURTHER: k_extrapolate<<<A, 64, 0, s>>>(Bt, 2u); break;
+    case WIG_PASS_ADVECT: k_advect<<<PP, 256, 0, s>>>(Bt); break;
+    case WIG_PASS_SORT_COUNT: k_sortCount<<<PP, 256, 0, s>>>(Bt); break;
+    case WIG_PASS_SCAN_BLOCKS: k_scanBlocks<<<A, 64, 0, s>>>(Bt); break;
+    case WIG_PASS_SCAN_TOTALS: k_scanTotals<<<ONE, 256, 0, s>>>(Bt); break;
+    case WIG_PASS_SCAN_FINISH: k_scanFinish<<<A, 64, 0, s>>>(Bt); break;
+    case WIG_PASS_SCATTER: k_scatter<<<PP, 256, 0, s>>>(Bt); break;
+    case WIG_PASS_RASTER_CLAIMS: k_rasterClaims<<<A, 64, 0, s>>>(Bt); break;
+    case WIG_PASS_RASTER: k_raster<<<A, 64, 0, s>>>(Bt); break;
+    case WIG_PASS_UNPAINT: k_unpaint<<<A, 64, 0, s>>>(Bt); break;
     default: return WIG_E_ARG;
     }
     return WIG_OK;

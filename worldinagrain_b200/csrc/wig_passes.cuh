@@ -3,8 +3,26 @@
 #include "wig_device.cuh"
 
 namespace wig {
-// One reference pass (enum wig_pass) at Level (level, cycle), on stream s.
-int launch_pass(const Dev& D, int pass, uint32_t level, uint32_t cycle, cudaStream_t s);
-// The tolerance form's norms: which 0 = ||b||^2 after cgResidual, 1 = ||r||/||b|| after cgUpdate.
+
+// Host-side shape of a batch: the most items each work list can hold (grid
+// sizes of the kernels over it).
+struct BatchShape {
+    uint32_t max_items[L_COUNT];
+    uint32_t worlds;
+    uint32_t levels;       // deepest coarse level of any world
+    uint32_t lc_max;       // deepest level any world restricts by itself
+    size_t coarse_smem;    // the coarse kernel's shared memory for the largest world
+};
+
+// CTAs for a kernel over list `list` with `per_sm` CTAs a multiprocessor.
+unsigned list_grid(const BatchShape& S, uint32_t list, unsigned per_sm);
+
+// One reference pass (enum wig_pass) at Level (level, cycle), on stream s:
+// over the batch's work lists, or (the plain form's solve passes) over
+// world 0, whose descriptor D0 is.
+int launch_pass(const Batch& Bt, const BatchShape& S, const Dev& D0, int pass, uint32_t level, uint32_t cycle,
+                cudaStream_t s);
+// The plain form's tolerance norms on world 0: which 0 = ||b||^2 after
+// cgResidual, 1 = ||r||/||b|| after cgUpdate.
 int launch_norm(const Dev& D, int which, uint32_t cycle, cudaStream_t s);
 }  // namespace wig

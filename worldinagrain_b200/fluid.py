@@ -31,6 +31,21 @@ FUNCS = {
     "wig_fluid_step_profile": ([C.c_void_p, C.POINTER(abi.Params), C.c_uint32, C.c_uint32, C.c_double, C.c_void_p,
                                 C.POINTER(C.c_float), C.POINTER(C.c_uint32)], C.c_int),
     "wig_fluid_destroy": ([C.c_void_p], None),
+    "wig_batch_world_bytes": ([C.POINTER(abi.WorldDesc), C.POINTER(C.c_uint64)], C.c_int),
+    "wig_batch_create": ([C.POINTER(abi.WorldDesc), C.c_uint32, C.POINTER(abi.Elem), C.c_uint32, C.POINTER(C.c_void_p)],
+                         C.c_int),
+    "wig_batch_worlds": ([C.c_void_p], C.c_uint32),
+    "wig_batch_layout": ([C.c_void_p, C.c_uint32, C.POINTER(abi.WorldLayout)], C.c_int),
+    "wig_batch_buffers_of": ([C.c_void_p, C.c_uint32, C.POINTER(abi.Buffers)], C.c_int),
+    "wig_batch_upload": ([C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p], C.c_int),
+    "wig_batch_download": ([C.c_void_p, C.c_uint32, C.c_int, C.c_void_p, C.c_uint64, C.c_uint64, C.c_void_p], C.c_int),
+    "wig_batch_step": ([C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(abi.Params),
+                        C.POINTER(C.c_uint32), C.c_uint32, C.c_uint32, C.c_double, C.c_void_p], C.c_int),
+    "wig_batch_read_stats": ([C.c_void_p, C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(abi.Stats)], C.c_int),
+    "wig_batch_step_profile": ([C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32), C.c_uint32, C.POINTER(abi.Params),
+                                C.POINTER(C.c_uint32), C.c_uint32, C.c_uint32, C.c_double, C.c_void_p,
+                                C.POINTER(C.c_float), C.POINTER(C.c_uint32)], C.c_int),
+    "wig_batch_destroy": ([C.c_void_p], None),
 }
 
 
@@ -129,3 +144,98 @@ class LiquidStep:
         st = abi.Stats()
         check(lib().wig_fluid_read_stats(self.h, C.byref(st)), "wig_fluid_read_stats")
         return st
+
+
+def world_bytes(width, height, liquid_per_cell=4, capacity=0):
+    """Device bytes a world of this shape holds in a batch."""
+    d = abi.WorldDesc(width, height, liquid_per_cell, capacity)
+    out = C.c_uint64()
+    check(lib().wig_batch_world_bytes(C.byref(d), C.byref(out)), "wig_batch_world_bytes")
+    return out.value
+
+
+def _u32s(seq):
+    seq = list(seq)
+    return (C.c_uint32 * max(len(seq), 1))(*seq)
+
+
+class Batch:
+    """Many worlds resident on the GPU in one packed allocation, stepped
+    together: each pass one launch over all the worlds listed (the
+    reference's Simulation holds one world; this has no counterpart there).
+    `worlds` are World objects (their numpy buffers uploaded at creation)."""
+
+    LANES = 2
+
+    def __init__(self, worlds, elems):
+        self.worlds = list(worlds)
+        self.elems = elems
+        L = lib()
+        descs = (abi.WorldDesc * len(self.worlds))(*[w.desc() for w in self.worlds])
+        h = C.c_void_p()
+        check(L.wig_batch_create(descs, len(self.worlds), elems, len(elems), C.byref(h)), "wig_batch_create")
+        self.h = h
+        for k in range(len(self.worlds)):
+            self.upload(k)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().wig_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __len__(self):
+        return len(self.worlds)
+
+    def upload(self, k, world=None, stream=0):
+        w = world or self.worlds[k]
+        for which, name in enumerate(abi.BUFFER_NAMES):
+            arr = np.ascontiguousarray(getattr(w, name))
+            check(lib().wig_batch_upload(self.h, k, which, arr.ctypes.data, 0, arr.nbytes, C.c_void_p(stream or None)),
+                  f"upload {name} of world {k}")
+
+    def download(self, k, world=None, names=abi.BUFFER_NAMES, stream=0):
+        w = world or self.worlds[k]
+        for name in names:
+            which = abi.BUFFER_NAMES.index(name)
+            arr = getattr(w, name)
+            assert arr.flags["C_CONTIGUOUS"]
+            check(lib().wig_batch_download(self.h, k, which, arr.ctypes.data, 0, arr.nbytes, C.c_void_p(stream or None)),
+                  f"download {name} of world {k}")
+        return w
+
+    def buffers(self, k):
+        b = abi.Buffers()
+        check(lib().wig_batch_buffers_of(self.h, k, C.byref(b)), "wig_batch_buffers_of")
+        return b
+
+    def step(self, ids, params, world_flags=None, max_cycles=abi.FLUID_CYCLES, flags=0, tolerance=1e-6, lane=0,
+             stream=0):
+        """One step of the worlds `ids` (params[i] for ids[i]), asynchronous."""
+        ids = list(ids)
+        P = (abi.Params * len(ids))(*params)
+        wf = _u32s(world_flags) if world_flags is not None else None
+        check(lib().wig_batch_step(self.h, lane, _u32s(ids), len(ids), P, wf, max_cycles, flags, tolerance,
+                                   C.c_void_p(stream or None)), "wig_batch_step")
+
+    def step_profile(self, ids, params, world_flags=None, max_cycles=abi.FLUID_CYCLES, flags=0, tolerance=1e-6,
+                     lane=0, stream=0):
+        ids = list(ids)
+        P = (abi.Params * len(ids))(*params)
+        wf = _u32s(world_flags) if world_flags is not None else None
+        ms = (C.c_float * abi.PROFILE_SLOTS)()
+        calls = (C.c_uint32 * abi.PROFILE_SLOTS)()
+        check(lib().wig_batch_step_profile(self.h, lane, _u32s(ids), len(ids), P, wf, max_cycles, flags, tolerance,
+                                           C.c_void_p(stream or None), ms, calls), "wig_batch_step_profile")
+        return {abi.PROFILE_NAMES[k]: (ms[k], calls[k]) for k in range(abi.PROFILE_SLOTS) if calls[k]}
+
+    def stats(self, ids):
+        ids = list(ids)
+        out = (abi.Stats * len(ids))()
+        check(lib().wig_batch_read_stats(self.h, _u32s(ids), len(ids), out), "wig_batch_read_stats")
+        return list(out)
