@@ -210,6 +210,152 @@ def run_reference(args, rank, world_size):
     print(json.dumps(line), flush=True)
 
 
+def gpu_index_of(torch, local_rank):
+    gpu_index = torch.cuda.current_device()
+    if "CUDA_VISIBLE_DEVICES" in os.environ and os.environ["CUDA_VISIBLE_DEVICES"].strip():
+        try:
+            gpu_index = int(os.environ["CUDA_VISIBLE_DEVICES"].split(",")[local_rank])
+        except ValueError:
+            pass
+    return gpu_index
+
+
+def run_batched(args, rank, world_size, local_rank, dist, torch):
+    """The batched multi-world workload: args.worlds independent worlds of
+    uneven sizes (multi_worlds) resident together, every step one
+    wig_batch_step of all of them (each pass one launch over all the
+    worlds), solved to the same 1e-6 relative residual."""
+    from worldinagrain_b200 import fluid
+    import ctypes as C
+    worlds = W.multi_worlds(n=args.worlds, seed=args.seed)
+    n = len(worlds)
+    cells = sum(w.C for w in worlds)
+    stream = torch.cuda.Stream()
+    b = fluid.Batch(worlds, W.element_table())
+    ids = (C.c_uint32 * n)(*range(n))
+    P = (abi.Params * n)(*[params(w, 0, args.seed) for w in worlds])
+    step_no = 0
+
+    def step(extra=0):
+        nonlocal step_no
+        step_no += 1
+        for k in range(n):
+            P[k].frame = step_no
+        b.step(ids, P, max_cycles=MAX_CYCLES, flags=FLAGS | extra, tolerance=TOL, stream=stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with Clocks(gpu_index_of(torch, local_rank)) as clk:
+        barrier()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        barrier()
+    ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = cells * args.steps * world_size / (ms / 1e3) / 1e6
+    st = b.stats(range(n))
+    launches_per_step = st[0].launches
+
+    # end to end: every step's inputs in, every world's report out
+    cycles, worst = [], 0.0
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
+        sts = b.stats(range(n))
+        cycles.append(max(x.cycles for x in sts))
+        worst = max(worst, max(x.rel_residual for x in sts))
+    e2e_s = time.perf_counter() - t0
+    if worst > TOL:
+        raise SystemExit(f"a world's solve left {worst:.3e} > {TOL}")
+    if dist:
+        t = torch.tensor([e2e_s], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e = cells * args.steps * world_size / e2e_s / 1e6
+    h2d = 8 + ((4 * n + 7) // 8) * 8 + 136 * n
+    d2h = 64 * n
+
+    prof = {}
+    for _ in range(args.profile_steps):
+        step_no += 1
+        for k in range(n):
+            P[k].frame = step_no
+        for key, (t_ms, cnt) in b.step_profile(range(n), list(P), max_cycles=MAX_CYCLES, flags=FLAGS, tolerance=TOL,
+                                               stream=stream.cuda_stream).items():
+            a0, c0 = prof.get(key, (0.0, 0))
+            prof[key] = (a0 + t_ms, c0 + cnt)
+    ws = {"active_cells": 0, "fluid_cells": 0, "particles": 0}
+    for k, w in enumerate(worlds):
+        b.download(k, names=("blocks", "field"))
+        B = w.L["block_count"]
+        ws["active_cells"] += int(w.blocks[4 * B + abi.COUNT_ACTIVE]) * 64
+        ws["fluid_cells"] += int(np.sum(w.field_cells()[:, 0, 2] > 0))
+    ws["particles"] = int(sum(x.particles for x in b.stats(range(n))))
+    total = sum(v[0] for v in prof.values())
+    ranked = sorted(prof.items(), key=lambda kv: -kv[1][0])
+    top = next((k for k, _ in ranked if algorithmic_bytes(k, ws) is not None), ranked[0][0])
+    t_ms, cnt = prof[top]
+    per_launch_s = t_ms / cnt / 1e3
+    alg = algorithmic_bytes(top, ws) or 0
+    peak, peak_kind = peaks()
+    achieved = alg / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        from oracle.oracle import Oracle
+        done_cells, steps_done, t0 = 0, 0, time.perf_counter()
+        for w in worlds:
+            o = Oracle(w.copy(), W.element_table())
+            o.step(params(w, 1, args.seed), max_cycles=MAX_CYCLES, flags=FLAGS, tolerance=TOL)
+            done_cells += w.C
+            steps_done += 1
+            if time.perf_counter() - t0 >= args.cpu_budget:
+                break
+        dt = time.perf_counter() - t0
+        cpu = {"value": round(done_cells / dt / 1e6, 4), "unit": "Mcells/s", "cores": 1, "kind": "port",
+               "sample": f"the first step of {steps_done} of the {n} worlds on one host core, {dt:.1f} s"}
+    b.close()
+    if rank == 0:
+        sides = sorted(w.W for w in worlds)
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Mcells/s", "n_gpus": world_size,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": f"multi_worlds_{n}", "worlds": n, "cells": cells,
+                       "sides": f"log-uniform {sides[0]}..{sides[-1]}, median {sides[n // 2]}", "seed": args.seed,
+                       "liquid_per_cell": 4, "tolerance": TOL, "max_cycles": MAX_CYCLES,
+                       "form": "batched fast form: one launch a pass over all worlds, CG loop in a graph WHILE node",
+                       "l2": "inputs larger than L2 (worlds resident in HBM, no flush)", "parallelism": "replicas"},
+            "e2e": {"value": round(e2e, 3), "unit": "Mcells/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": launches_per_step * args.steps,
+            "roofline": {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                         "algorithmic_bytes_per_launch": alg, "launch_ms": round(per_launch_s * 1e3, 5)},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+            "solve": {"cycles_max_mean": round(float(np.mean(cycles)), 2), "cycles_max": int(np.max(cycles)),
+                      "rel_residual_worst": worst},
+            "world": ws,
+            "profile_ms_per_step": {k: round(v[0] / args.profile_steps, 4) for k, v in ranked[:12]},
+            "profile_share": {k: round(v[0] / total, 4) for k, v in ranked[:12]},
+        }
+        print(json.dumps(line), flush=True)
+
+
 def config_of(world, args):
     return {"workload": f"{world.config['workload']}_{world.config['grid']}", "grid": world.config["grid"],
             "seed": args.seed, "liquid_per_cell": world.L["liquid_per_cell"], "tolerance": TOL,
@@ -231,6 +377,8 @@ def main():
     ap.add_argument("--cpu-steps-max", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--form", default="fast", choices=["fast", "plain", "persistent"])
+    ap.add_argument("--workload", default="single", choices=["single", "batched"])
+    ap.add_argument("--worlds", type=int, default=512)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     global FLAGS
@@ -257,6 +405,12 @@ def main():
 
     from worldinagrain_b200 import fluid
 
+    if args.workload == "batched":
+        run_batched(args, rank, world_size, local_rank, dist, torch)
+        if dist:
+            dist.destroy_process_group()
+        return
+
     world = make_world(args)
     stream = torch.cuda.Stream()
     g = fluid.LiquidStep(world, W.element_table(), stream=stream.cuda_stream)
@@ -274,13 +428,7 @@ def main():
         torch.cuda.synchronize()
 
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    gpu_index = torch.cuda.current_device()
-    if "CUDA_VISIBLE_DEVICES" in os.environ and os.environ["CUDA_VISIBLE_DEVICES"].strip():
-        try:
-            gpu_index = int(os.environ["CUDA_VISIBLE_DEVICES"].split(",")[local_rank])
-        except ValueError:
-            pass
-    with Clocks(gpu_index) as clk:
+    with Clocks(gpu_index_of(torch, local_rank)) as clk:
         barrier()
         with torch.cuda.stream(stream):
             e0.record(stream)

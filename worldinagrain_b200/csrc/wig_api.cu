@@ -467,6 +467,7 @@ int make_batch(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, u
         Bt.count = ln.d_count;
         for (uint32_t l = 0; l < wig::L_COUNT; l++) Bt.base[l] = base[l];
         Bt.lbits = b->lbits;
+        Bt.single = n == 1 ? 1u : 0u;
         Bt.max_cycles = 1;
         Bt.cond = 0;
         Bt.loop = ln.d_loop;
@@ -711,7 +712,8 @@ int record_step_fast(wig_batch* b, Lane& ln, uint32_t max_cycles, uint32_t flags
     wig::Marker mk{&Rec::mark, &R};
     ln.Bt.max_cycles = max_cycles;
     ln.Bt.cond = 0;
-    wig::fast_setup(ln.Bt, b->S, s, prof ? &mk : nullptr);
+    const wig::World* one = b->K == 1 ? &b->hw[0] : nullptr;
+    wig::fast_setup(ln.Bt, b->S, one, s, prof ? &mk : nullptr);
     R.launches++;
     if (flags & WIG_STEP_PERSISTENT) {
         wig::Fast F0;
@@ -743,20 +745,20 @@ int record_step_fast(wig_batch* b, Lane& ln, uint32_t max_cycles, uint32_t flags
         CUDA_TRY(cudaStreamBeginCaptureToGraph(ln.cap2, bodyGraph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
         wig::Batch Bc = ln.Bt;
         Bc.cond = (unsigned long long)handle;
-        *body = wig::fast_cycle(Bc, b->S, ln.cap2, nullptr);
+        *body = wig::fast_cycle(Bc, b->S, one, ln.cap2, nullptr);
         cudaGraph_t captured = nullptr;
         CUDA_TRY(cudaStreamEndCapture(ln.cap2, &captured));
     } else {
         uint32_t* cont = reinterpret_cast<uint32_t*>(ln.h_rsub);  // a word of pinned scratch
         for (uint32_t c = 0; c < max_cycles; c++) {
-            R.launches += wig::fast_cycle(ln.Bt, b->S, s, prof ? &mk : nullptr);
+            R.launches += wig::fast_cycle(ln.Bt, b->S, one, s, prof ? &mk : nullptr);
             CUDA_TRY(cudaMemcpyAsync(cont, ln.d_loop, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
             CUDA_TRY(cudaStreamSynchronize(s));
             if (!*cont) break;
         }
         *body = 0;
     }
-    wig::fast_finish(ln.Bt, b->S, s, prof ? &mk : nullptr);
+    wig::fast_finish(ln.Bt, b->S, one, s, prof ? &mk : nullptr);
     R.launches++;
     record_post(R);
     *outside = R.launches;
@@ -971,9 +973,12 @@ int batch_read_stats(wig_batch* b, const uint32_t* worlds, uint32_t count, wig_f
         }
     }
     int rc = WIG_OK;
+    // one copy of every world's report when more than a few are asked for
+    const bool all = count > 4;
+    if (all) CUDA_TRY(cudaMemcpy(b->h_report, b->d_report, sizeof(Report) * b->K, cudaMemcpyDeviceToHost));
     for (uint32_t i = 0; i < count; i++) {
         const uint32_t k = worlds[i];
-        CUDA_TRY(cudaMemcpy(&b->h_report[k], &b->d_report[k], sizeof(Report), cudaMemcpyDeviceToHost));
+        if (!all) CUDA_TRY(cudaMemcpy(&b->h_report[k], &b->d_report[k], sizeof(Report), cudaMemcpyDeviceToHost));
         const Report& r = b->h_report[k];
         wig_fluid_stats& o = out[i];
         std::memset(&o, 0, sizeof(o));

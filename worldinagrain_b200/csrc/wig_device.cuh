@@ -366,10 +366,11 @@ struct FastW {
 };
 
 // An entry of a batch's world table (device memory).
-struct World {
+struct alignas(16) World {
     Dev D;
     FastW S;
 };
+static_assert(sizeof(World) % 16 == 0, "World copies in 16-byte words");
 
 // Work lists.  A kernel's CTAs take the items of one list in turn (grid
 // stride); an item is a world of the batch (its index in the world table, the
@@ -398,24 +399,60 @@ struct Batch {
     const uint32_t* __restrict__ count;
     uint32_t base[L_COUNT];
     uint32_t lbits;           // bits of an item's unit
+    uint32_t single;          // a batch of one world: item g of any list is unit g of world 0
     uint32_t max_cycles;
     unsigned long long cond;  // cudaGraphConditionalHandle of the iteration loop (0: none)
     uint32_t* loop;           // the loop's verdict: 1 when a world iterates again
 
     __device__ __forceinline__ uint32_t n(uint32_t list) const { return count[list]; }
-    __device__ __forceinline__ uint32_t item(uint32_t list, uint32_t g) const { return items[base[list] + g]; }
+    __device__ __forceinline__ uint32_t item(uint32_t list, uint32_t g) const {
+        return single ? g : items[base[list] + g];
+    }
     __device__ __forceinline__ const World& world(uint32_t it) const { return worlds[(uint64_t)it >> lbits]; }
     __device__ __forceinline__ uint32_t unit(uint32_t it) const { return it & ((1u << lbits) - 1u); }
 };
 
-// The CTAs of a kernel over list L, one item per CTA at a time:
+// The CTAs of a kernel over list L, one item per CTA at a time, each CTA a
+// contiguous run of the list (so its items are mostly of one world):
 //   FOR_ITEMS(Bt, L, it) { const World& Wd = Bt.world(it); uint32_t j = Bt.unit(it); ... }
-#define FOR_ITEMS(Bt, L, it)                                                         \
-    for (uint32_t g_##it = blockIdx.x, n_##it = (Bt).n(L), it = 0;                    \
-         g_##it < n_##it && ((it = (Bt).item((L), g_##it)), true); g_##it += gridDim.x)
-// An item's world D (with its accessors w) and unit j.
+#define FOR_ITEMS(Bt, L, it)                                                                       \
+    for (uint32_t n_##it = (Bt).n(L), p_##it = (n_##it + gridDim.x - 1u) / gridDim.x,              \
+                  g_##it = blockIdx.x * p_##it, e_##it = min(g_##it + p_##it, n_##it), it = 0;     \
+         g_##it < e_##it && ((it = (Bt).item((L), g_##it)), true); g_##it++)
+// A CTA's copy of the world of its current item, in shared memory: copied
+// when the item's world changes (uniformly across the CTA), so the world's
+// fields cost a shared-memory read instead of a chain of global loads.
+struct WorldCopy {
+    World w;
+    uint32_t k;
+};
+__device__ __forceinline__ void worldCopyInit(WorldCopy& c) {
+    if (threadIdx.x == 0) c.k = 0xffffffffu;
+    __syncthreads();
+}
+__device__ __forceinline__ const World& worldOf(const Batch& Bt, uint32_t it, WorldCopy& c) {
+    const uint32_t k = (uint32_t)((uint64_t)it >> Bt.lbits);
+    if (k != c.k) {
+        __syncthreads();  // the CTA is done with the last world's copy
+        const uint4* src = reinterpret_cast<const uint4*>(&Bt.worlds[k]);
+        uint4* dst = reinterpret_cast<uint4*>(&c.w);
+        for (uint32_t i = threadIdx.x; i < sizeof(World) / 16u; i += blockDim.x) dst[i] = src[i];
+        if (threadIdx.x == 0) c.k = k;  // read again only after the barrier below
+        __syncthreads();
+    }
+    return c.w;
+}
+
+// An item's world D (with its accessors w) and unit j, read from the world
+// table (any thread, any loop).
 #define ITEM_WORLD(Bt, it, D, w, j)              \
     const Dev& D = (Bt).world(it).D;             \
+    const W w(D);                                \
+    const uint32_t j = (Bt).unit(it)
+// The same from the CTA's copy (every thread of the CTA, each item in turn;
+// the kernel declares `__shared__ WorldCopy wc_;` and calls worldCopyInit).
+#define ITEM_WORLD_C(Bt, it, D, w, j)            \
+    const Dev& D = worldOf((Bt), (it), wc_).D;   \
     const W w(D);                                \
     const uint32_t j = (Bt).unit(it)
 

@@ -126,8 +126,34 @@ __device__ __forceinline__ I2 tileCell(const W& w, uint32_t wid) {
     return I2{b.x * BLOCK + (int)(threadIdx.x & 7u), b.y * BLOCK + (int)((threadIdx.x >> 3) & 7u)};
 }
 
-// An item's world: its descriptor D, fast scratch F, accessors w, unit j.
+// Where a kernel finds its items' world: in a batch of one, the world
+// itself, a kernel parameter (read as constants, with no load at a CTA's
+// start); else the CTA's shared copy of the world-table entry.
+template <bool ONE>
+struct WorldSrc;
+template <>
+struct WorldSrc<true> {
+    World w;
+    __device__ __forceinline__ const World& get(const Batch&, uint32_t, WorldCopy&) const { return w; }
+};
+template <>
+struct WorldSrc<false> {
+    __device__ __forceinline__ const World& get(const Batch& Bt, uint32_t it, WorldCopy& c) const {
+        return worldOf(Bt, it, c);
+    }
+};
+
+// An item's world: its descriptor D, fast scratch F, accessors w, unit j,
+// from the CTA's copy of the world (every thread of the CTA, each item in
+// turn; the kernel declares `__shared__ WorldCopy wc_;`) or (FAST_ITEM_G)
+// from the world table.
 #define FAST_ITEM(Bt, it, D, F, w, j)            \
+    const World& Wd_##it = src.get((Bt), (it), wc_); \
+    const Dev& D = Wd_##it.D;                    \
+    const FastW& F = Wd_##it.S;                  \
+    const W w(D);                                \
+    const uint32_t j = (Bt).unit(it)
+#define FAST_ITEM_G(Bt, it, D, F, w, j)          \
     const World& Wd_##it = (Bt).world(it);       \
     const Dev& D = Wd_##it.D;                    \
     const FastW& F = Wd_##it.S;                  \
@@ -141,7 +167,10 @@ __device__ __forceinline__ I2 tileCell(const W& w, uint32_t wid) {
 // group of four active blocks an item; the CTA that counts a world's last
 // tile sums its ||b||^2), and the blocks that dropped out this step zeroed
 // (the invariant).
-__global__ void __launch_bounds__(256) k_fSetup(Batch Bt) {
+template <bool ONE>
+__global__ void __launch_bounds__(256) k_fSetup(Batch Bt, const __grid_constant__ WorldSrc<ONE> src) {
+    __shared__ WorldCopy wc_;
+    if (!ONE) worldCopyInit(wc_);
     __shared__ double s64[256];
     FOR_ITEMS(Bt, L_ACT4, it) {
         FAST_ITEM(Bt, it, D, F, w, g);
@@ -218,7 +247,7 @@ __global__ void __launch_bounds__(256) k_fSetup(Batch Bt) {
     const uint32_t nr = Bt.n(L_RET);
     for (uint32_t t = blockIdx.x * 4u + (threadIdx.x >> 6); t < nr; t += gridDim.x * 4u) {
         const uint32_t it = Bt.item(L_RET, t);
-        FAST_ITEM(Bt, it, D, F, w, j);
+        FAST_ITEM_G(Bt, it, D, F, w, j);
         uint32_t n = D.blocks[w.retiredSlot(j)];
         I2 c{(int)(n % D.BW) * BLOCK + (int)(threadIdx.x & 7u), (int)(n / D.BW) * BLOCK + (int)((threadIdx.x >> 3) & 7u)};
         if (w.inWorld(c)) {
@@ -252,7 +281,10 @@ __device__ I2 tileBlockF(const W& w, uint32_t wid, int shift) {
 // values for liquid cells, the potentials (zero) elsewhere.  `second`: the
 // iteration's relaxation after the V-cycle, on the other tiling from the
 // first (each world's first tiling is its step's).
-__global__ void __launch_bounds__(64) k_fRelax(Batch Bt, int second) {
+template <bool ONE>
+__global__ void __launch_bounds__(64) k_fRelax(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, int second) {
+    __shared__ WorldCopy wc_;
+    if (!ONE) worldCopyInit(wc_);
     __shared__ float tpx[RIM * RIM], tpy[RIM * RIM];
     __shared__ int s_live, s_ox, s_oy;
     FOR_ITEMS(Bt, L_RELAX, it) {
@@ -473,7 +505,10 @@ __device__ void prolongCell(const Dev& D, const FastW& F, uint32_t l, uint32_t j
 
 // restrictLevel of level l from level l - 1 (both in the scratch): a thread
 // per coarse cell, 256 cells an item.
-__global__ void k_fRestrict(Batch Bt, uint32_t l) {
+template <bool ONE>
+__global__ void k_fRestrict(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
+    __shared__ WorldCopy wc_;
+    if (!ONE) worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_RES + l - 1u, it) {
         FAST_ITEM(Bt, it, D, F, w, chunk);
         if (D.st->cont == 0u) continue;
@@ -483,7 +518,10 @@ __global__ void k_fRestrict(Batch Bt, uint32_t l) {
 }
 
 // smoothAt on level l >= 1, one colour.
-__global__ void k_fSmooth(Batch Bt, uint32_t l, int color) {
+template <bool ONE>
+__global__ void k_fSmooth(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l, int color) {
+    __shared__ WorldCopy wc_;
+    if (!ONE) worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_SM + l - 1u, it) {
         FAST_ITEM(Bt, it, D, F, w, chunk);
         if (D.st->cont == 0u) continue;
@@ -493,7 +531,10 @@ __global__ void k_fSmooth(Batch Bt, uint32_t l, int color) {
 }
 
 // prolong of level l from l + 1.
-__global__ void k_fProlong(Batch Bt, uint32_t l) {
+template <bool ONE>
+__global__ void k_fProlong(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
+    __shared__ WorldCopy wc_;
+    if (!ONE) worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_SM + l - 1u, it) {
         FAST_ITEM(Bt, it, D, F, w, chunk);
         if (D.st->cont == 0u) continue;
@@ -710,7 +751,10 @@ __device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t 
     }
 }
 
-__global__ void __launch_bounds__(1024) k_fCoarse(Batch Bt) {
+template <bool ONE>
+__global__ void __launch_bounds__(1024) k_fCoarse(Batch Bt, const __grid_constant__ WorldSrc<ONE> src) {
+    __shared__ WorldCopy wc_;
+    if (!ONE) worldCopyInit(wc_);
     extern __shared__ float sm[];
     __shared__ uint32_t off[WIG_MG_LEVELS + 1];
     FOR_ITEMS(Bt, L_ONE, it) {
@@ -723,7 +767,10 @@ __global__ void __launch_bounds__(1024) k_fCoarse(Batch Bt) {
 }
 
 // prolongFine (fluid.wgsl:2500-2512), and the rims for the relaxation after.
-__global__ void k_fProlongFine(Batch Bt) {
+template <bool ONE>
+__global__ void k_fProlongFine(Batch Bt, const __grid_constant__ WorldSrc<ONE> src) {
+    __shared__ WorldCopy wc_;
+    if (!ONE) worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_ACT, it) {
         FAST_ITEM(Bt, it, D, F, w, wid);
         if (D.st->cont == 0u) continue;
@@ -747,7 +794,10 @@ __global__ void k_fProlongFine(Batch Bt) {
 
 // cgRho + cgBeta (fluid.wgsl:2736-2764): four tiles a 256-thread CTA; the CTA
 // that counts a world's last tile sums its blocks' partials (sumBlocks' order).
-__global__ void __launch_bounds__(256) k_fRhoBeta(Batch Bt) {
+template <bool ONE>
+__global__ void __launch_bounds__(256) k_fRhoBeta(Batch Bt, const __grid_constant__ WorldSrc<ONE> src) {
+    __shared__ WorldCopy wc_;
+    if (!ONE) worldCopyInit(wc_);
     __shared__ float sx[256], sy[256];
     __shared__ double s64[256];
     FOR_ITEMS(Bt, L_ACT4, it) {
@@ -815,7 +865,10 @@ __global__ void __launch_bounds__(256) k_fRhoBeta(Batch Bt) {
 }
 
 // cgDirection (fluid.wgsl:2767-2776)
-__global__ void k_fDirection(Batch Bt) {
+template <bool ONE>
+__global__ void k_fDirection(Batch Bt, const __grid_constant__ WorldSrc<ONE> src) {
+    __shared__ WorldCopy wc_;
+    if (!ONE) worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_ACT, it) {
         FAST_ITEM(Bt, it, D, F, w, wid);
         if (D.st->cont == 0u) continue;
@@ -836,7 +889,10 @@ __global__ void k_fDirection(Batch Bt) {
 }
 
 // cgApply + cgAlpha (fluid.wgsl:2779-2814)
-__global__ void __launch_bounds__(256) k_fApplyAlpha(Batch Bt) {
+template <bool ONE>
+__global__ void __launch_bounds__(256) k_fApplyAlpha(Batch Bt, const __grid_constant__ WorldSrc<ONE> src) {
+    __shared__ WorldCopy wc_;
+    if (!ONE) worldCopyInit(wc_);
     __shared__ float sx[256];
     __shared__ double s64[256];
     FOR_ITEMS(Bt, L_ACT4, it) {
@@ -905,7 +961,10 @@ __global__ void __launch_bounds__(256) k_fApplyAlpha(Batch Bt) {
 // condition: a world iterates again unless its solve has converged
 // (converged, fluid.wgsl:2223-2226) or max_cycles are done; the loop runs on
 // while any world does.
-__global__ void __launch_bounds__(256) k_fUpdate(Batch Bt) {
+template <bool ONE>
+__global__ void __launch_bounds__(256) k_fUpdate(Batch Bt, const __grid_constant__ WorldSrc<ONE> src) {
+    __shared__ WorldCopy wc_;
+    if (!ONE) worldCopyInit(wc_);
     __shared__ uint32_t most[4];
     __shared__ double s64[256];
     FOR_ITEMS(Bt, L_ACT4, it) {
@@ -1010,7 +1069,10 @@ __global__ void k_fLoopStart(Batch Bt) {
 // potential, cg's (x, r, p, Ap); and the residual slots the converged
 // iterations the reference still dispatches would clear (cgUpdate's first
 // lines run whether or not the iteration is skipped).
-__global__ void k_fFinish(Batch Bt) {
+template <bool ONE>
+__global__ void k_fFinish(Batch Bt, const __grid_constant__ WorldSrc<ONE> src) {
+    __shared__ WorldCopy wc_;
+    if (!ONE) worldCopyInit(wc_);
     if (threadIdx.x == 0) {
         FOR_ITEMS(Bt, L_ONE, ot) {
             ITEM_WORLD(Bt, ot, D, w, unused_);
@@ -1460,13 +1522,21 @@ size_t fast_coarse_smem(const Dev& D, uint32_t lc) {
 
 void fast_zero_level0(const FastW& F, uint32_t cells, cudaStream_t s) { k_fZero<<<148 * 4, 256, 0, s>>>(F, cells); }
 
-void fast_setup(const Batch& Bt, const BatchShape& S, cudaStream_t s, const Marker* m) {
+// Launches kernel K's instance for the batch: the single-world one with
+// the world as a parameter when `one` is given, else the table one.
+#define LAUNCH(K, grid, block, smem, ...)                                                      \
+    do {                                                                                       \
+        if (one) K<true><<<(grid), (block), (smem), s>>>(Bt, WorldSrc<true>{*one}, ##__VA_ARGS__); \
+        else K<false><<<(grid), (block), (smem), s>>>(Bt, WorldSrc<false>{}, ##__VA_ARGS__);       \
+    } while (0)
+
+void fast_setup(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m) {
     if (m) m->fn(m->ctx, WIG_SLOT_F_SETUP, 0);
-    k_fSetup<<<list_grid(S, L_ACT4, 8), 256, 0, s>>>(Bt);
+    LAUNCH(k_fSetup, list_grid(S, L_ACT4, 8), 256, 0);
     if (m) m->fn(m->ctx, WIG_SLOT_F_SETUP, 1);
 }
 
-uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, cudaStream_t s, const Marker* m) {
+uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m) {
     const unsigned G = list_grid(S, L_ACT, 32), G4 = list_grid(S, L_ACT4, 8), GR = list_grid(S, L_RELAX, 32);
     uint32_t launches = 0;
     auto mark = [&](int slot, int phase) {
@@ -1478,66 +1548,68 @@ uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, cudaStream_t s, const 
     k_fLoopStart<<<list_grid(S, L_ONE, 1), 32, 0, s>>>(Bt);
     mark(WIG_SLOT_F_LOOP, 1);
     mark(WIG_SLOT_F_RELAX, 0);
-    k_fRelax<<<GR, 64, 0, s>>>(Bt, 0);
+    LAUNCH(k_fRelax, GR, 64, 0, 0);
     mark(WIG_SLOT_F_RELAX, 1);
     // down: each world restricts its levels 1..lc by themselves and smooths
     // those above lc, then its levels from lc are the coarse kernel's
     for (uint32_t l = 1; l <= S.lc_max; l++) {
         mark(WIG_SLOT_F_RESTRICT, 0);
-        k_fRestrict<<<cells(L_RES + l - 1u), 256, 0, s>>>(Bt, l);
+        LAUNCH(k_fRestrict, cells(L_RES + l - 1u), 256, 0, l);
         mark(WIG_SLOT_F_RESTRICT, 1);
         if (S.max_items[L_SM + l - 1u] == 0u) continue;
         mark(WIG_SLOT_F_SMOOTH, 0);
-        k_fSmooth<<<cells(L_SM + l - 1u), 256, 0, s>>>(Bt, l, 0);
+        LAUNCH(k_fSmooth, cells(L_SM + l - 1u), 256, 0, l, 0);
         mark(WIG_SLOT_F_SMOOTH, 1);
         mark(WIG_SLOT_F_SMOOTH, 0);
-        k_fSmooth<<<cells(L_SM + l - 1u), 256, 0, s>>>(Bt, l, 1);
+        LAUNCH(k_fSmooth, cells(L_SM + l - 1u), 256, 0, l, 1);
         mark(WIG_SLOT_F_SMOOTH, 1);
     }
     mark(WIG_SLOT_F_COARSE, 0);
-    k_fCoarse<<<list_grid(S, L_ONE, 1), 1024, S.coarse_smem, s>>>(Bt);
+    LAUNCH(k_fCoarse, list_grid(S, L_ONE, 1), 1024, S.coarse_smem);
     mark(WIG_SLOT_F_COARSE, 1);
     for (uint32_t l = S.lc_max; l >= 1; l--) {
         if (S.max_items[L_SM + l - 1u] == 0u) continue;
         mark(WIG_SLOT_F_PROLONG, 0);
-        k_fProlong<<<cells(L_SM + l - 1u), 256, 0, s>>>(Bt, l);
+        LAUNCH(k_fProlong, cells(L_SM + l - 1u), 256, 0, l);
         mark(WIG_SLOT_F_PROLONG, 1);
         mark(WIG_SLOT_F_SMOOTH, 0);
-        k_fSmooth<<<cells(L_SM + l - 1u), 256, 0, s>>>(Bt, l, 0);
+        LAUNCH(k_fSmooth, cells(L_SM + l - 1u), 256, 0, l, 0);
         mark(WIG_SLOT_F_SMOOTH, 1);
         mark(WIG_SLOT_F_SMOOTH, 0);
-        k_fSmooth<<<cells(L_SM + l - 1u), 256, 0, s>>>(Bt, l, 1);
+        LAUNCH(k_fSmooth, cells(L_SM + l - 1u), 256, 0, l, 1);
         mark(WIG_SLOT_F_SMOOTH, 1);
     }
     mark(WIG_SLOT_F_PROLONG_FINE, 0);
-    k_fProlongFine<<<G, 64, 0, s>>>(Bt);
+    LAUNCH(k_fProlongFine, G, 64, 0);
     mark(WIG_SLOT_F_PROLONG_FINE, 1);
     mark(WIG_SLOT_F_RELAX, 0);
-    k_fRelax<<<GR, 64, 0, s>>>(Bt, 1);
+    LAUNCH(k_fRelax, GR, 64, 0, 1);
     mark(WIG_SLOT_F_RELAX, 1);
     mark(WIG_SLOT_F_RHO_BETA, 0);
-    k_fRhoBeta<<<G4, 256, 0, s>>>(Bt);
+    LAUNCH(k_fRhoBeta, G4, 256, 0);
     mark(WIG_SLOT_F_RHO_BETA, 1);
     mark(WIG_SLOT_F_DIRECTION, 0);
-    k_fDirection<<<G, 64, 0, s>>>(Bt);
+    LAUNCH(k_fDirection, G, 64, 0);
     mark(WIG_SLOT_F_DIRECTION, 1);
     mark(WIG_SLOT_F_APPLY_ALPHA, 0);
-    k_fApplyAlpha<<<G4, 256, 0, s>>>(Bt);
+    LAUNCH(k_fApplyAlpha, G4, 256, 0);
     mark(WIG_SLOT_F_APPLY_ALPHA, 1);
     mark(WIG_SLOT_F_UPDATE, 0);
-    k_fUpdate<<<G4, 256, 0, s>>>(Bt);
+    LAUNCH(k_fUpdate, G4, 256, 0);
     mark(WIG_SLOT_F_UPDATE, 1);
     return launches;
 }
 
-void fast_finish(const Batch& Bt, const BatchShape& S, cudaStream_t s, const Marker* m) {
+void fast_finish(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m) {
     if (m) m->fn(m->ctx, WIG_SLOT_F_FINISH, 0);
-    k_fFinish<<<list_grid(S, L_ACT, 32), 64, 0, s>>>(Bt);
+    LAUNCH(k_fFinish, list_grid(S, L_ACT, 32), 64, 0);
     if (m) m->fn(m->ctx, WIG_SLOT_F_FINISH, 1);
 }
 
 cudaError_t fast_prepare_attributes(size_t smem) {
-    return cudaFuncSetAttribute(k_fCoarse, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_fCoarse<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_fCoarse<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
 size_t fast_solve_smem(const Fast& F) { return fast_coarse_smem(F.D, F.lp); }

@@ -27,11 +27,12 @@ struct Marker {
     void* ctx;
 };
 
-// Launchers over a batch (stream-ordered; all capturable).  fast_cycle
-// returns its launches.
-void fast_setup(const Batch& Bt, const BatchShape& S, cudaStream_t s, const Marker* m);
-uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, cudaStream_t s, const Marker* m);
-void fast_finish(const Batch& Bt, const BatchShape& S, cudaStream_t s, const Marker* m);
+// Launchers over a batch (stream-ordered; all capturable).  `one`: the
+// batch's only world (host copy), passed to the kernels as a parameter; null
+// for a batch of several.  fast_cycle returns its launches.
+void fast_setup(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m);
+uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m);
+void fast_finish(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m);
 // Level 0's arrays of one world zeroed (after its buffers are written by the host).
 void fast_zero_level0(const FastW& F, uint32_t cells, cudaStream_t s);
 // Shared memory of the coarse kernel for a world, and the kernel's limit set.

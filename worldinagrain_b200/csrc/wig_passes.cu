@@ -192,8 +192,10 @@ __device__ V2 prolonged(const W& w, uint32_t l, I2 c) {
 // sync / syncMarks (fluid.wgsl:608-659): a CTA per block of the world
 // (syncMarks: no claims, as a world's bookkeeping-only step takes it).
 __global__ void k_sync(Batch Bt, int sync_claims) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
   FOR_ITEMS(Bt, L_WB, it) {
-    ITEM_WORLD(Bt, it, D, w, n);
+    ITEM_WORLD_C(Bt, it, D, w, n);
     const bool claims = sync_claims && D.st->book == 0u;
     const I2 b{(int)(n % D.BW), (int)(n / D.BW)};
     I2 c{b.x * BLOCK + (int)(threadIdx.x & 7u), b.y * BLOCK + (int)(threadIdx.x >> 3)};
@@ -312,8 +314,10 @@ __device__ __forceinline__ void storeParticle(const W& w, uint32_t m, V2 pos, V2
 
 // syncParticles (fluid.wgsl:767-831): a thread per particle of `sorted`.
 __global__ void k_syncParticles(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
   FOR_ITEMS(Bt, L_PS, qi) {
-    ITEM_WORLD(Bt, qi, D, w, chunk);
+    ITEM_WORLD_C(Bt, qi, D, w, chunk);
     uint32_t live = min(D.sorted[0], D.cap);
     uint32_t k0 = chunk * blockDim.x;
     if (k0 >= live) continue;  // whole CTA past the particles (uniform)
@@ -381,8 +385,10 @@ __device__ uint32_t seedId(const Dev& D, I2 c, uint32_t j) {
 
 // syncSeed (fluid.wgsl:863-890): a CTA per block of the world.
 __global__ void k_syncSeed(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
   FOR_ITEMS(Bt, L_WB, qi) {
-    ITEM_WORLD(Bt, qi, D, w, blk);
+    ITEM_WORLD_C(Bt, qi, D, w, blk);
     if (D.st->book) continue;
     I2 c{(int)(blk % D.BW) * BLOCK + (int)(threadIdx.x & 7u), (int)(blk / D.BW) * BLOCK + (int)(threadIdx.x >> 3)};
     uint32_t n = 0;
@@ -429,9 +435,11 @@ __global__ void k_syncSeed(Batch Bt) {
 // compact (fluid.wgsl:896-921): one CTA of 1024 threads, a contiguous run of
 // blocks each, so the lists come out in block-index order.
 __global__ void __launch_bounds__(1024) k_compact(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
   __shared__ uint32_t sa[1024], sr[1024];
   FOR_ITEMS(Bt, L_ONE_ALL, it) {
-    ITEM_WORLD(Bt, it, D, w, unused_);
+    ITEM_WORLD_C(Bt, it, D, w, unused_);
     (void)unused_;
     const uint32_t per = (D.B + 1023u) / 1024u;
     const uint32_t lo = min(threadIdx.x * per, D.B), hi = min(lo + per, D.B);
@@ -488,8 +496,10 @@ __global__ void __launch_bounds__(1024) k_compact(Batch Bt) {
 
 // retire (fluid.wgsl:924-951)
 __global__ void k_retire(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_RET, it) {
-        ITEM_WORLD(Bt, it, D, w, wid);
+        ITEM_WORLD_C(Bt, it, D, w, wid);
         uint32_t n = D.blocks[w.retiredSlot(wid)];
         I2 c{(int)(n % D.BW) * BLOCK + (int)(threadIdx.x & 7u), (int)(n / D.BW) * BLOCK + (int)(threadIdx.x >> 3)};
         if (!w.inWorld(c)) continue;
@@ -513,8 +523,10 @@ __global__ void k_retire(Batch Bt) {
 
 // clear (fluid.wgsl:962-985)
 __global__ void k_clear(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_ACT, it) {
-        ITEM_WORLD(Bt, it, D, w, wid);
+        ITEM_WORLD_C(Bt, it, D, w, wid);
         I2 b = w.activeBlock(wid);
         if (threadIdx.x == 0) D.blocks[w.blockIndex(b)] = 0u;
         I2 c = lidCell(w, wid);
@@ -597,8 +609,10 @@ __device__ __forceinline__ void gatherOne(const Dev& D, const W& w, uint32_t chu
     splatDensity(w, px, py, w.liquidVolume(stt.x, temp));
 }
 __global__ void k_gather(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_PP, qi) {
-        ITEM_WORLD(Bt, qi, D, w, chunk);
+        ITEM_WORLD_C(Bt, qi, D, w, chunk);
         gatherOne(D, w, chunk);
     }
 }
@@ -618,8 +632,10 @@ __device__ bool wasOpen(const W& w, I2 q) {
 
 // sealJoin (fluid.wgsl:1531-1543)
 __global__ void k_sealJoin(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_ACT, it) {
-        ITEM_WORLD(Bt, it, D, w, wid);
+        ITEM_WORLD_C(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c) || !mayBeSealed(w, c)) continue;
         for (int d = 0; d < 2; d++) {
@@ -630,8 +646,10 @@ __global__ void k_sealJoin(Batch Bt) {
 }
 // sealAnchor (fluid.wgsl:1545-1554)
 __global__ void k_sealAnchor(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_ACT, it) {
-        ITEM_WORLD(Bt, it, D, w, wid);
+        ITEM_WORLD_C(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c) || !mayBeSealed(w, c)) continue;
         if (wasOpen(w, beside(c, 0)) || wasOpen(w, beside(c, 1)) || wasOpen(w, beside(c, 2)) || wasOpen(w, beside(c, 3)))
@@ -652,9 +670,11 @@ __device__ float columnWeight(const W& w, I2 p, float density) {
 
 // classify (fluid.wgsl:1578-1696), no bodies.
 __global__ void k_classify(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     __shared__ uint32_t blockBits;
     FOR_ITEMS(Bt, L_ACT, it) {
-        ITEM_WORLD(Bt, it, D, w, wid);
+        ITEM_WORLD_C(Bt, it, D, w, wid);
         const uint32_t frame = D.st->P.frame;
         const uint32_t mine = 1u << (frame & 1u), fall0 = 4u << (frame & 1u);
         if (threadIdx.x == 0) blockBits = 0u;
@@ -772,8 +792,10 @@ __device__ void setFace(const W& w, I2 at, bool isU) {
 
 // setFaces (fluid.wgsl:1982-1994)
 __global__ void k_setFaces(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_ACT, it) {
-        ITEM_WORLD(Bt, it, D, w, wid);
+        ITEM_WORLD_C(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         int fs[4][3];
@@ -811,8 +833,10 @@ __device__ void viscousFace(const W& w, I2 at, bool isU, int color) {
 
 // viscosityRed / viscosityBlack / unpress (fluid.wgsl:3409-3466)
 __global__ void k_viscosity(Batch Bt, int color) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_ACT, it) {
-        ITEM_WORLD(Bt, it, D, w, wid);
+        ITEM_WORLD_C(Bt, it, D, w, wid);
         if (color < 2 && D.st->viscous == 0u) continue;  // this world's step has no sweeps
         I2 b = w.activeBlock(wid);
         if ((w.statesOf(I2{b.x - 1, b.y - 1}, I2{b.x + 1, b.y + 1}) & HAS_VISCOUS) == 0u) continue;
@@ -844,6 +868,8 @@ __global__ void k_viscosity(Batch Bt, int color) {
 
 // divergence (fluid.wgsl:1996-2025), posedRoom 1 with no bodies.
 __global__ void k_divergence(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     // once a world: its residual and iteration words cleared
     if (threadIdx.x == 0) {
         FOR_ITEMS(Bt, L_ONE, ot) {
@@ -854,7 +880,7 @@ __global__ void k_divergence(Batch Bt) {
         }
     }
     FOR_ITEMS(Bt, L_ACT, it) {
-        ITEM_WORLD(Bt, it, D, w, wid);
+        ITEM_WORLD_C(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         uint32_t i = w.cellIndex(c);
@@ -872,8 +898,10 @@ __global__ void k_divergence(Batch Bt) {
 
 // cgStart (fluid.wgsl:2665-2674)
 __global__ void k_cgStart(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_ACT, it) {
-        ITEM_WORLD(Bt, it, D, w, wid);
+        ITEM_WORLD_C(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         uint32_t i = w.cellIndex(c);
@@ -883,8 +911,10 @@ __global__ void k_cgStart(Batch Bt) {
 }
 // cgJoin (fluid.wgsl:2677-2689)
 __global__ void k_cgJoin(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_ACT, it) {
-        ITEM_WORLD(Bt, it, D, w, wid);
+        ITEM_WORLD_C(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c) || w.gridAt(c).z <= 0.0f) continue;
         for (int d = 0; d < 2; d++) {
@@ -895,8 +925,10 @@ __global__ void k_cgJoin(Batch Bt) {
 }
 // cgAnchor (fluid.wgsl:2692-2705)
 __global__ void k_cgAnchor(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_ACT, it) {
-        ITEM_WORLD(Bt, it, D, w, wid);
+        ITEM_WORLD_C(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c) || w.gridAt(c).z <= 0.0f) continue;
         for (int d = 0; d < 4; d++) {
@@ -1530,6 +1562,8 @@ __global__ void k_cgFinish(Dev D) {
 
 // project / projectFace (fluid.wgsl:2897-2942), no bodies.
 __global__ void k_project(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     // once a world: the most iterations any step took
     if (threadIdx.x == 0) {
         FOR_ITEMS(Bt, L_ONE, ot) {
@@ -1540,7 +1574,7 @@ __global__ void k_project(Batch Bt) {
         }
     }
     FOR_ITEMS(Bt, L_ACT, it) {
-        ITEM_WORLD(Bt, it, D, w, wid);
+        ITEM_WORLD_C(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         int fs[4][3];
@@ -1566,8 +1600,10 @@ __global__ void k_project(Batch Bt) {
 
 // extrapolate / extrapolateFurther (fluid.wgsl:3226-3275)
 __global__ void k_extrapolate(Batch Bt, uint32_t layer) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_ACT, it) {
-        ITEM_WORLD(Bt, it, D, w, wid);
+        ITEM_WORLD_C(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         int fs[4][3];
@@ -1748,8 +1784,10 @@ __device__ __forceinline__ void advectOne(const Dev& D, const W& w, uint32_t chu
     if ((w.elem(wordType(stt.x)).flags & F_IMPACT) != 0u && impact > IMPACT_SPEED) it[D.cap + k].x = wordWith(stt.x, FL_BURN);
 }
 __global__ void k_advect(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_PP, qi) {
-        ITEM_WORLD(Bt, qi, D, w, chunk);
+        ITEM_WORLD_C(Bt, qi, D, w, chunk);
         advectOne(D, w, chunk);
     }
 }
@@ -1767,17 +1805,21 @@ __device__ __forceinline__ void sortCountOne(const Dev& D, const W& w, uint32_t 
     it[D.cap + k].w = atomicAdd(w.gwp(i, G_SORT), 1u);
 }
 __global__ void k_sortCount(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_PP, qi) {
-        ITEM_WORLD(Bt, qi, D, w, chunk);
+        ITEM_WORLD_C(Bt, qi, D, w, chunk);
         sortCountOne(D, w, chunk);
     }
 }
 
 // scanBlocks (fluid.wgsl:3730-3753)
 __global__ void __launch_bounds__(64) k_scanBlocks(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     __shared__ uint32_t tile[64];
     FOR_ITEMS(Bt, L_ACT, it) {
-        ITEM_WORLD(Bt, it, D, w, wid);
+        ITEM_WORLD_C(Bt, it, D, w, wid);
         const uint32_t fall0 = 4u << (D.st->P.frame & 1u);
         I2 c = lidCell(w, wid);
         uint32_t n = 0;
@@ -1839,8 +1881,10 @@ __global__ void __launch_bounds__(256) k_scanTotals(Batch Bt) {
 
 // scanFinish (fluid.wgsl:3783-3790)
 __global__ void k_scanFinish(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_ACT, it) {
-        ITEM_WORLD(Bt, it, D, w, wid);
+        ITEM_WORLD_C(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         *w.gwp(w.cellIndex(c), G_START) += D.blocks[w.totalSlot(wid)];
@@ -1864,8 +1908,10 @@ __device__ __forceinline__ void scatterOne(const Dev& D, const W& w, uint32_t ch
     }
 }
 __global__ void k_scatter(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_PP, qi) {
-        ITEM_WORLD(Bt, qi, D, w, chunk);
+        ITEM_WORLD_C(Bt, qi, D, w, chunk);
         scatterOne(D, w, chunk);
     }
 }
@@ -1890,8 +1936,10 @@ __device__ uint32_t airTo(const W& w, I2 c, bool gas) {
 }
 // rasterClaims (fluid.wgsl:3928-3948), no people.
 __global__ void k_rasterClaims(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_ACT, it) {
-        ITEM_WORLD(Bt, it, D, w, wid);
+        ITEM_WORLD_C(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         uint32_t i = w.cellIndex(c);
@@ -1933,8 +1981,10 @@ __device__ __forceinline__ float exact_value(unsigned long long wsum, float scal
 
 // raster (fluid.wgsl:3983-4119), no people, the air source unbound.
 __global__ void k_raster(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_ACT, qi) {
-        ITEM_WORLD(Bt, qi, D, w, wid);
+        ITEM_WORLD_C(Bt, qi, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         uint32_t i = w.cellIndex(c);
@@ -2037,8 +2087,10 @@ __global__ void k_raster(Batch Bt) {
 
 // unpaint (fluid.wgsl:4163-4182)
 __global__ void k_unpaint(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
     FOR_ITEMS(Bt, L_ACT, it) {
-        ITEM_WORLD(Bt, it, D, w, wid);
+        ITEM_WORLD_C(Bt, it, D, w, wid);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         uint32_t i = w.cellIndex(c);

@@ -216,11 +216,15 @@ class Batch:
 
     def step(self, ids, params, world_flags=None, max_cycles=abi.FLUID_CYCLES, flags=0, tolerance=1e-6, lane=0,
              stream=0):
-        """One step of the worlds `ids` (params[i] for ids[i]), asynchronous."""
-        ids = list(ids)
-        P = (abi.Params * len(ids))(*params)
-        wf = _u32s(world_flags) if world_flags is not None else None
-        check(lib().wig_batch_step(self.h, lane, _u32s(ids), len(ids), P, wf, max_cycles, flags, tolerance,
+        """One step of the worlds `ids` (params[i] for ids[i]), asynchronous.
+        ids, params and world_flags may be prebuilt ctypes arrays."""
+        n = len(ids)
+        ids_a = ids if isinstance(ids, C.Array) else _u32s(ids)
+        P = params if isinstance(params, C.Array) else (abi.Params * n)(*params)
+        wf = None
+        if world_flags is not None:
+            wf = world_flags if isinstance(world_flags, C.Array) else _u32s(world_flags)
+        check(lib().wig_batch_step(self.h, lane, ids_a, n, P, wf, max_cycles, flags, tolerance,
                                    C.c_void_p(stream or None)), "wig_batch_step")
 
     def step_profile(self, ids, params, world_flags=None, max_cycles=abi.FLUID_CYCLES, flags=0, tolerance=1e-6,

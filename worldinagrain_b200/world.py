@@ -232,6 +232,41 @@ def obstacle_column(width=2048, height=2048, p_solid=0.03, fill=0.7, ppc=2, seed
     return w
 
 
+def multi_worlds(n=512, lo=64, hi=512, seed=4, ppc=4):
+    """Batched multi-world config: n independent square worlds, sides
+    log-uniform in [lo, hi] rounded to a multiple of 16, each a dam break
+    (WATER against the left wall, about 1.5 times as high as wide) or a
+    column (the bottom rows, full width), fluid fraction U(0.2, 0.7) of the
+    inside, at rest, ppc particles per fluid cell, one-cell WALL border.  The
+    particle buffers are sized to the liquid (1.25 times its particles), not
+    to the whole grid."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for k in range(n):
+        s = int(16 * round(lo * (hi / lo) ** rng.uniform() / 16))
+        kind = "dam" if rng.uniform() < 0.5 else "column"
+        f = rng.uniform(0.2, 0.7)
+        inner = s - 2
+        if kind == "dam":
+            fh = min(inner, int(round(inner * min(0.95, (1.5 * f) ** 0.5))))
+            fw = min(inner, int(round(f * inner * inner / max(fh, 1))))
+        else:
+            fw, fh = inner, min(inner, int(round(f * inner)))
+        cap = int(np.ceil(fw * fh * ppc * 1.25)) + 256
+        w = World(s, s, ppc, cap)
+        wall = np.zeros((s, s), dtype=bool)
+        wall[0, :] = wall[-1, :] = True
+        wall[:, 0] = wall[:, -1] = True
+        w.paint(wall, abi.WALL)
+        water = np.zeros((s, s), dtype=bool)
+        water[s - 1 - fh:s - 1, 1:1 + fw] = True
+        w.paint(water, abi.WATER)
+        w.config = dict(workload=f"multi_{kind}", grid=f"{s}x{s}", seed=seed, earth_g=earth_g_cells(), fill=float(f),
+                        index=k)
+        out.append(w)
+    return out
+
+
 def two_liquids(width=40, height=32, seed=5):
     """Water on the left and a viscous liquid (MUD) on the right of a walled
     box, moving: two liquids in contact, their cells rasterised by the most
