@@ -356,6 +356,63 @@ def run_batched(args, rank, world_size, local_rank, dist, torch):
         print(json.dumps(line), flush=True)
 
 
+def run_served(args, rank, world_size, local_rank, dist, torch):
+    """The served stream: args.worlds resident worlds (sides log-uniform
+    64..1024), Poisson step requests at each rate of args.rates, admitted
+    under a device-memory budget into two-lane continuously batched steps
+    (lane pools lend each step its per-step memory); p50/p99 latency and
+    Mcells/s per rate, beside the same stream served one world a launch."""
+    from worldinagrain_b200 import serve
+    t0 = time.perf_counter()
+    worlds = W.multi_worlds(n=args.worlds, lo=64, hi=1024, seed=args.seed)
+    t_build = time.perf_counter() - t0
+    cells_of = [w.C for w in worlds]
+    budget = int(args.budget_gb * 1e9)
+    pool = int(args.pool_gb * 1e9)
+    be = serve.GpuBackend(worlds, W.element_table(), FLAGS, MAX_CYCLES, TOL, pool_bytes=pool)
+    srv = serve.Server(be, len(worlds), budget - 2 * pool)
+    t0 = time.perf_counter()
+    srv.preload()
+    t_preload = time.perf_counter() - t0
+    resident = len(srv.resident)
+    srv.run(serve.poisson_arrivals(1000.0, 200, len(worlds), seed=99))  # graphs captured, first steps seeded
+    rates = [float(r) for r in args.rates.split(",")]
+    points = []
+    with Clocks(gpu_index_of(torch, local_rank)) as clk:
+        for rate in rates:
+            n_req = int(min(max(rate * args.serve_seconds, 500), args.serve_max_requests))
+            done = srv.run(serve.poisson_arrivals(rate, n_req, len(worlds), seed=args.seed + int(rate)))
+            pt = serve.latency_summary(done, lambda k: cells_of[k])
+            pt["rate"] = rate
+            points.append(pt)
+    # the one-world-at-a-time baseline (same kernels, one world a launch) at the lowest rate
+    one = serve.Server(be, len(worlds), budget - 2 * pool, one_at_a_time=True)
+    one.resident, one.resident_bytes = srv.resident, srv.resident_bytes
+    rate0 = rates[0]
+    arr = serve.poisson_arrivals(rate0, int(min(max(rate0 * args.serve_seconds, 300), 1500)), len(worlds),
+                                 seed=args.seed + 7)
+    base = serve.latency_summary(one.run(arr), lambda k: cells_of[k])
+    base["rate"] = rate0
+    be.close()
+    best = max(points, key=lambda p: p["mcells_per_s"])
+    if rank == 0:
+        line = {
+            "metric": METRIC + "; served p50/p99 step latency", "value": best["mcells_per_s"], "unit": "Mcells/s",
+            "n_gpus": world_size, "steps": sum(p["requests"] for p in points), "warmup": 200,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": f"served_{len(worlds)}_worlds", "worlds": len(worlds), "cells": sum(cells_of),
+                       "sides": "log-uniform 64..1024", "budget_gb": args.budget_gb, "lane_pool_gb": args.pool_gb,
+                       "resident_worlds": resident, "resident_gb": round(srv.resident_bytes / 1e9, 2),
+                       "build_s": round(t_build, 1), "preload_s": round(t_preload, 1), "tolerance": TOL,
+                       "arrivals": "Poisson, worlds uniform", "parallelism": "replicas"},
+            "served": points,
+            "one_at_a_time": base,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+
+
 def config_of(world, args):
     return {"workload": f"{world.config['workload']}_{world.config['grid']}", "grid": world.config["grid"],
             "seed": args.seed, "liquid_per_cell": world.L["liquid_per_cell"], "tolerance": TOL,
@@ -377,8 +434,13 @@ def main():
     ap.add_argument("--cpu-steps-max", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--form", default="fast", choices=["fast", "plain", "persistent"])
-    ap.add_argument("--workload", default="single", choices=["single", "batched"])
-    ap.add_argument("--worlds", type=int, default=512)
+    ap.add_argument("--workload", default="single", choices=["single", "batched", "served"])
+    ap.add_argument("--worlds", type=int, default=None)
+    ap.add_argument("--rates", default="1000,2000,5000,10000,20000,50000")
+    ap.add_argument("--budget-gb", type=float, default=120.0)
+    ap.add_argument("--pool-gb", type=float, default=7.0)
+    ap.add_argument("--serve-seconds", type=float, default=2.0)
+    ap.add_argument("--serve-max-requests", type=int, default=4000)
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     global FLAGS
@@ -405,8 +467,10 @@ def main():
 
     from worldinagrain_b200 import fluid
 
-    if args.workload == "batched":
-        run_batched(args, rank, world_size, local_rank, dist, torch)
+    if args.workload in ("batched", "served"):
+        if args.worlds is None:
+            args.worlds = 512 if args.workload == "batched" else 2000
+        (run_batched if args.workload == "batched" else run_served)(args, rank, world_size, local_rank, dist, torch)
         if dist:
             dist.destroy_process_group()
         return

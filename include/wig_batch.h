@@ -77,6 +77,30 @@ int wig_batch_step_profile(wig_batch* b, uint32_t lane, const uint32_t* worlds, 
 
 void wig_batch_destroy(wig_batch* b);
 
+/* Serving: a batch whose worlds hold no device memory until admitted.
+ * wig_batch_admit allocates one world's memory (zeroed; the host uploads
+ * its state after) from the device's stream-ordered pool; wig_batch_evict
+ * returns it (download the state first; the world's step counter and tiling
+ * parity carry on when it is admitted again).  Only admitted worlds step.
+ * wig_batch_resident_bytes: the admitted worlds' bytes. */
+int wig_batch_create_deferred(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, uint32_t n_elems,
+                              wig_batch** out);
+int wig_batch_admit(wig_batch* b, uint32_t world, void* stream);
+int wig_batch_evict(wig_batch* b, uint32_t world, void* stream);
+uint64_t wig_batch_resident_bytes(const wig_batch* b);
+
+/* Pooled serving: each lane gets a pool of `bytes` that lends every world
+ * of a step on that lane its per-step memory (its `parts` particle buffer,
+ * which the step refills, its `cg` buffer, which the step writes before any
+ * pass reads it, and the fast form's scratch); an admitted world then holds
+ * only its persistent buffers, `field` without its coarse levels (copies of
+ * field stop there; copies of parts and cg are refused).  Set both lanes'
+ * pools before admitting any world.  A step whose worlds' per-step memory
+ * exceeds the lane's pool is refused (WIG_E_OOM).
+ * wig_batch_world_bytes_split gives a world's persistent and per-step bytes. */
+int wig_batch_set_lane_pool(wig_batch* b, uint32_t lane, uint64_t bytes);
+int wig_batch_world_bytes_split(const wig_world_desc* d, uint64_t* persistent, uint64_t* transient);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,133 @@
+"""The serving loop's scheduling on the CPU, over a fake device: every
+request served once, a world never in two steps at once, the memory
+budget and the lane pools never exceeded, least-recently-used eviction,
+both lanes used."""
+import collections
+
+import pytest
+
+from worldinagrain_b200 import serve
+
+
+class FakeBackend:
+    """Steps finish after `step_s` of the fake clock; records everything."""
+
+    def __init__(self, sizes, step_s, clock, step_sizes=None, pool=None):
+        self.sizes = sizes
+        self.step_sizes = step_sizes or [0] * len(sizes)
+        self.pool = pool
+        self.step_s = step_s
+        self.clock = clock
+        self.resident = set()
+        self.log = []
+        self.inflight = collections.Counter()
+
+    def world_bytes(self, k):
+        return self.sizes[k]
+
+    def step_bytes(self, k):
+        return self.step_sizes[k]
+
+    def lane_capacity(self, lane):
+        return self.pool
+
+    def admit(self, k):
+        assert k not in self.resident
+        self.resident.add(k)
+        self.log.append(("admit", k))
+
+    def evict(self, k):
+        assert k in self.resident and self.inflight[k] == 0
+        self.resident.remove(k)
+        self.log.append(("evict", k))
+
+    def launch(self, lane, ids):
+        for k in ids:
+            assert k in self.resident
+            assert self.inflight[k] == 0, "a world in two steps at once"
+            self.inflight[k] += 1
+        if self.pool is not None:
+            assert sum(self.step_sizes[k] for k in ids) <= self.pool
+        self.log.append(("step", lane, tuple(ids)))
+        return [self.clock.t + self.step_s, ids]
+
+    def done(self, token):
+        if self.clock.t >= token[0]:
+            for k in token[1]:
+                self.inflight[k] -= 1
+            token[1] = []
+            return True
+        return False
+
+
+class FakeClock:
+    def __init__(self):
+        self.t = 0.0
+
+    def __call__(self):
+        self.t += 1e-4  # every look at the clock moves it on
+        return self.t
+
+
+@pytest.mark.parametrize("budget", [10_000, 450])
+def test_every_request_served_once_within_budget(budget):
+    clock = FakeClock()
+    sizes = [50 + 10 * (k % 7) for k in range(20)]
+    be = FakeBackend(sizes, step_s=0.003, clock=clock)
+    srv = serve.Server(be, len(sizes), budget, clock=clock)
+    srv.preload()
+    arr = serve.poisson_arrivals(rate=2000.0, n_requests=300, n_worlds=len(sizes), seed=3)
+    done = srv.run(arr)
+    assert sorted(r.rid for r in done) == list(range(300))
+    assert all(r.t_done >= r.t_start >= r.t_arrival for r in done)
+    used = 0
+    for ev in be.log:
+        if ev[0] == "admit":
+            used += sizes[ev[1]]
+            assert used <= budget
+        elif ev[0] == "evict":
+            used -= sizes[ev[1]]
+    assert {ev[1] for ev in be.log if ev[0] == "step"} == {0, 1}
+    if budget < sum(sizes):
+        assert srv.swaps_out > 0 and srv.swaps_in > 0
+
+
+def test_lane_pool_bounds_each_step():
+    clock = FakeClock()
+    be = FakeBackend([10] * 12, step_s=0.002, clock=clock, step_sizes=[3 + k % 4 for k in range(12)], pool=12)
+    srv = serve.Server(be, 12, 10_000, clock=clock)
+    srv.preload()
+    done = srv.run(serve.poisson_arrivals(5000.0, 200, 12, seed=4))
+    assert len(done) == 200
+    steps = [ev for ev in be.log if ev[0] == "step"]
+    assert max(len(ev[2]) for ev in steps) > 1
+
+
+def test_requests_of_one_world_run_in_order():
+    clock = FakeClock()
+    be = FakeBackend([10] * 3, step_s=0.002, clock=clock)
+    srv = serve.Server(be, 3, 1000, clock=clock)
+    srv.preload()
+    done = sorted(srv.run([(0.0001 * i, 1) for i in range(10)]), key=lambda r: r.rid)
+    for a, b in zip(done, done[1:]):
+        assert b.t_start >= a.t_done
+
+
+def test_one_at_a_time_baseline_steps_single_worlds():
+    clock = FakeClock()
+    be = FakeBackend([10] * 5, step_s=0.001, clock=clock)
+    srv = serve.Server(be, 5, 1000, one_at_a_time=True, clock=clock)
+    srv.preload()
+    done = srv.run(serve.poisson_arrivals(1000.0, 50, 5, seed=1))
+    assert len(done) == 50
+    assert all(len(ev[2]) == 1 and ev[1] == 0 for ev in be.log if ev[0] == "step")
+
+
+def test_eviction_is_least_recently_used():
+    clock = FakeClock()
+    be = FakeBackend([100] * 4, step_s=0.001, clock=clock)
+    srv = serve.Server(be, 4, 300, clock=clock)
+    srv.preload()  # worlds 0, 1, 2
+    assert list(srv.resident) == [0, 1, 2]
+    srv.run([(0.0, 1), (0.01, 0), (0.02, 3)])
+    assert [ev[1] for ev in be.log if ev[0] == "evict"] == [2]

@@ -100,6 +100,11 @@ struct Lane {
     int up_at = 0;
     Report* d_rsub = nullptr;
     Report* h_rsub = nullptr;      // pinned
+    // pooled batches: the lane's own world table and its pool of the
+    // per-step memory (each stepping world's borrowed buffers and scratch)
+    wig::World* d_table = nullptr;
+    char* d_pool = nullptr;
+    uint64_t pool_bytes = 0;
     wig::Batch Bt{};
     wig::SchedCtl ctl{};
     std::map<uint64_t, Graph> graphs;
@@ -124,6 +129,8 @@ struct wig_batch {
     Report* h_report = nullptr;       // K, pinned
     void* scratch = nullptr;          // the fast form's scratch and FP64 partials of every world
     void* arena = nullptr;            // the worlds' buffers (batches made by wig_batch_create)
+    std::vector<void*> wmem;          // each world's allocation (batches made by wig_batch_create_deferred)
+    uint64_t resident = 0;            // bytes of the admitted worlds' allocations
     std::vector<std::array<void*, 7>> own;  // buffers a single-world handle allocated at bind
     std::vector<char> bound, dirty;
     std::vector<char> shifted_first;
@@ -134,6 +141,8 @@ struct wig_batch {
     uint32_t solve_grid = 0;          // the persistent solve's CTAs (a batch of one world)
     Lane lane[WIG_BATCH_LANES];
     size_t up_bytes = 0;              // one upload slot
+    size_t entries_at = 0;            // offset of the staged world entries in a slot (pooled batches)
+    bool pooled = false;              // per-step memory from the lanes' pools
 };
 
 struct wig_fluid {
@@ -279,6 +288,30 @@ uint64_t world_buffers_bytes(const wig_world_layout& L) {
     return n;
 }
 
+// A pooled world's split: what stays on the device between its steps and
+// what a step borrows from its lane's pool.  Borrowed: `parts` (syncParticles
+// refills it every step), `cg` (cgStart and the solve's finish write it, no
+// pass reads it across steps) and the fast form's scratch (the step zeroes
+// it where it is read before written).  Kept: the other buffers, `field`
+// without its coarse levels (the fast form keeps those in its scratch).
+bool borrowed(int which) { return which == 2 || which == 6; }
+uint64_t persistent_buffer_bytes(const wig_world_layout& L, int which) {
+    if (borrowed(which)) return 0;
+    if (which == 4) {
+        const uint64_t F = L.face_count;
+        return 16ull * (2ull * L.cell_count + F + 2ull * ((F + 3) / 4));
+    }
+    return buffer_bytes(L, which);
+}
+uint64_t persistent_bytes(const wig_world_layout& L) {
+    uint64_t n = 0;
+    for (int k = 0; k < 7; k++) n += align256(persistent_buffer_bytes(L, k));
+    return n;
+}
+uint64_t transient_bytes(const wig_world_layout& L, const wig::Dev& D) {
+    return align256(buffer_bytes(L, 2)) + align256(buffer_bytes(L, 6)) + scratch_bytes(D);
+}
+
 uint32_t cdiv(uint64_t a, uint64_t b) { return (uint32_t)((a + b - 1) / b); }
 
 void destroy_batch(wig_batch* b);
@@ -297,9 +330,14 @@ int upload_world_entry(wig_batch* b, uint32_t k) {
     return WIG_OK;
 }
 
-// A batch of n worlds with their shapes, scratch, lanes and (alloc_buffers)
-// the worlds' buffers in one packed allocation.
-int make_batch(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, uint32_t n_elems, bool alloc_buffers,
+// How a batch holds its worlds' device memory: a single world's scratch with
+// its buffers bound later (wig_fluid_bind); every world's buffers and
+// scratch packed in two allocations; or each world's own allocation, made
+// when it is admitted and freed when it is evicted (serving).
+enum class Alloc { Single, Packed, Deferred };
+
+// A batch of n worlds with their shapes, lanes and (per `how`) memory.
+int make_batch(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, uint32_t n_elems, Alloc how,
                wig_batch** out) {
     if (!out) return fail(WIG_E_ARG, "null output handle");
     *out = nullptr;
@@ -401,20 +439,31 @@ int make_batch(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, u
     if (cudaMallocHost(&b->h_report, sizeof(Report) * n) != cudaSuccess) return bail(WIG_E_OOM, "cudaMallocHost reports");
     std::memset(b->h_report, 0, sizeof(Report) * n);
     if (cudaMalloc(&b->d_worlds, sizeof(wig::World) * n) != cudaSuccess) return bail(WIG_E_OOM, "cudaMalloc world table");
-    if (cudaMalloc(&b->scratch, scratch_total) != cudaSuccess) return bail(WIG_E_OOM, "cudaMalloc fast scratch");
-    cudaMemset(b->scratch, 0, scratch_total);
-    {
+    for (uint32_t k = 0; k < n; k++) {
+        wig::World& Wd = b->hw[k];
+        Wd.D.elems = b->d_elems;
+        Wd.D.n_elems = n_elems;
+        Wd.D.st = b->d_st + k;
+    }
+    if (how != Alloc::Deferred) {
+        if (cudaMalloc(&b->scratch, scratch_total) != cudaSuccess) return bail(WIG_E_OOM, "cudaMalloc fast scratch");
+        cudaMemset(b->scratch, 0, scratch_total);
         char* p = static_cast<char*>(b->scratch);
         for (uint32_t k = 0; k < n; k++) {
-            wig::World& Wd = b->hw[k];
-            scratch_take(Wd, p);
-            p += scratch_bytes(Wd.D);
-            Wd.D.elems = b->d_elems;
-            Wd.D.n_elems = n_elems;
-            Wd.D.st = b->d_st + k;
+            scratch_take(b->hw[k], p);
+            p += scratch_bytes(b->hw[k].D);
+        }
+    } else {
+        b->wmem.assign(n, nullptr);
+        // stream-ordered allocations that stay with the pool when freed, so
+        // admitting a world after an eviction is a pool hit
+        cudaMemPool_t pool;
+        if (cudaDeviceGetDefaultMemPool(&pool, b->device) == cudaSuccess) {
+            uint64_t keep = ~0ull;
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
         }
     }
-    if (alloc_buffers) {
+    if (how == Alloc::Packed) {
         uint64_t total = 0;
         for (uint32_t k = 0; k < n; k++) total += world_buffers_bytes(b->L[k]);
         if (cudaMalloc(&b->arena, total) != cudaSuccess) {
@@ -442,6 +491,11 @@ int make_batch(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, u
 
     // lanes
     b->up_bytes = 8u + ((4u * (size_t)n + 7u) & ~(size_t)7u) + sizeof(wig::StepHead) * n;
+    if (how == Alloc::Deferred) {
+        // room for the stepping worlds' table entries of a pooled step
+        b->entries_at = (b->up_bytes + 15u) & ~(size_t)15u;
+        b->up_bytes = b->entries_at + sizeof(wig::World) * n;
+    }
     for (uint32_t li = 0; li < WIG_BATCH_LANES; li++) {
         Lane& ln = b->lane[li];
         if (cudaMalloc(&ln.d_items, 4u * (size_t)std::max<uint64_t>(items_total, 1)) != cudaSuccess)
@@ -479,6 +533,8 @@ int make_batch(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, u
         c.items = ln.d_items;
         c.count = ln.d_count;
         c.max_worlds = n;
+        c.entries = nullptr;
+        c.table = nullptr;
     }
     *out = b;
     return WIG_OK;
@@ -502,11 +558,15 @@ void destroy_batch(wig_batch* b) {
         if (ln.h_rsub) cudaFreeHost(ln.h_rsub);
         if (ln.cap) cudaStreamDestroy(ln.cap);
         if (ln.cap2) cudaStreamDestroy(ln.cap2);
+        if (ln.d_table) cudaFree(ln.d_table);
+        if (ln.d_pool) cudaFree(ln.d_pool);
     }
     for (auto& o : b->own)
         for (void* p : o)
             if (p) cudaFree(p);
     if (b->arena) cudaFree(b->arena);
+    for (void* p : b->wmem)
+        if (p) cudaFree(p);
     if (b->scratch) cudaFree(b->scratch);
     if (b->d_worlds) cudaFree(b->d_worlds);
     if (b->d_elems) cudaFree(b->d_elems);
@@ -713,6 +773,10 @@ int record_step_fast(wig_batch* b, Lane& ln, uint32_t max_cycles, uint32_t flags
     ln.Bt.max_cycles = max_cycles;
     ln.Bt.cond = 0;
     const wig::World* one = b->K == 1 ? &b->hw[0] : nullptr;
+    if (b->pooled) {
+        wig::fast_zero_idle(ln.Bt, b->S, s);
+        R.launches++;
+    }
     wig::fast_setup(ln.Bt, b->S, one, s, prof ? &mk : nullptr);
     R.launches++;
     if (flags & WIG_STEP_PERSISTENT) {
@@ -842,6 +906,27 @@ int push_inputs(wig_batch* b, Lane& ln, const StepArgs& a, bool* viscous, bool* 
         if (i == 0) *shifted0 = sh;
     }
     const size_t bytes = 8u + sub_bytes + sizeof(wig::StepHead) * a.count;
+    if (b->pooled) {
+        // each stepping world's per-step memory from the lane's pool
+        if (!ln.d_pool) return fail(WIG_E_STATE, "the lane has no pool");
+        wig::World* ent = reinterpret_cast<wig::World*>(slot + b->entries_at);
+        uint64_t at = 0;
+        for (uint32_t i = 0; i < a.count; i++) {
+            const uint32_t k = a.worlds[i];
+            const uint64_t need = transient_bytes(b->L[k], b->hw[k].D);
+            if (at + need > ln.pool_bytes) return fail(WIG_E_OOM, "the step's worlds do not fit the lane's pool");
+            wig::World e = b->hw[k];
+            char* q = ln.d_pool + at;
+            e.D.parts = reinterpret_cast<uint32_t*>(q);
+            q += align256(buffer_bytes(b->L[k], 2));
+            e.D.cg = reinterpret_cast<float*>(q);
+            q += align256(buffer_bytes(b->L[k], 6));
+            scratch_take(e, q);
+            ent[i] = e;
+            at += need;
+        }
+        CUDA_TRY(cudaMemcpyAsync(ln.d_up + b->entries_at, ent, sizeof(wig::World) * a.count, cudaMemcpyHostToDevice, a.s));
+    }
     // the heads sit after the full sub array, so copy the slot's prefix
     // through the last head written
     CUDA_TRY(cudaMemcpyAsync(ln.d_up, slot, bytes, cudaMemcpyHostToDevice, a.s));
@@ -852,6 +937,7 @@ int push_inputs(wig_batch* b, Lane& ln, const StepArgs& a, bool* viscous, bool* 
 // Level 0 of the listed worlds whose buffers the host has written since
 // their last step, zeroed (the fast form's invariant).
 void zero_dirty(wig_batch* b, const StepArgs& a) {
+    if (b->pooled) return;  // the step zeroes its lent scratch itself
     for (uint32_t i = 0; i < a.count; i++) {
         const uint32_t k = a.worlds[i];
         if (!b->dirty[k]) continue;
@@ -1005,6 +1091,13 @@ int copy_world(wig_batch* b, uint32_t k, int which, void* host, uint64_t offset,
     uint64_t size = buffer_bytes(b->L[k], which);
     if (!size || offset > size || bytes > size - offset)
         return fail(WIG_E_ARG, up ? "upload out of the buffer's range" : "download out of the buffer's range");
+    if (b->pooled && borrowed(which)) return fail(WIG_E_STATE, "`parts` and `cg` are per-step memory in a pooled batch");
+    if (b->pooled && which == 4) {
+        // a pooled world's field ends before its coarse levels
+        const uint64_t kept = persistent_buffer_bytes(b->L[k], 4);
+        if (offset > kept) return fail(WIG_E_ARG, "field past a pooled world's kept part");
+        if (bytes > kept - offset) bytes = kept - offset;
+    }
     cudaStream_t s = (cudaStream_t)stream;
     char* dev = (char*)*buffer_slot(b->hw[k].D, which) + offset;
     if (up) CUDA_TRY(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyHostToDevice, s));
@@ -1030,7 +1123,7 @@ int wig_fluid_create(const wig_world_desc* d, const wig_elem* elems, uint32_t n_
     if (!d) return fail(WIG_E_ARG, "null descriptor");
     wig_fluid* h = new (std::nothrow) wig_fluid();
     if (!h) return fail(WIG_E_OOM, "host allocation failed");
-    int rc = make_batch(d, 1, elems, n_elems, false, &h->b);
+    int rc = make_batch(d, 1, elems, n_elems, Alloc::Single, &h->b);
     if (rc) {
         delete h;
         return rc;
@@ -1170,7 +1263,7 @@ int wig_batch_world_bytes(const wig_world_desc* d, uint64_t* out) {
 }
 
 int wig_batch_create(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, uint32_t n_elems, wig_batch** out) {
-    return make_batch(descs, n, elems, n_elems, true, out);
+    return make_batch(descs, n, elems, n_elems, Alloc::Packed, out);
 }
 
 uint32_t wig_batch_worlds(const wig_batch* b) { return b ? b->K : 0u; }
@@ -1223,5 +1316,104 @@ int wig_batch_step_profile(wig_batch* b, uint32_t lane, const uint32_t* worlds, 
 }
 
 void wig_batch_destroy(wig_batch* b) { destroy_batch(b); }
+
+int wig_batch_create_deferred(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, uint32_t n_elems,
+                              wig_batch** out) {
+    return make_batch(descs, n, elems, n_elems, Alloc::Deferred, out);
+}
+
+int wig_batch_admit(wig_batch* b, uint32_t world, void* stream) {
+    if (!b) return fail(WIG_E_ARG, "null batch");
+    if (world >= b->K) return fail(WIG_E_ARG, "world index out of range");
+    if (b->wmem.empty()) return fail(WIG_E_STATE, "not a deferred batch");
+    if (b->wmem[world]) return fail(WIG_E_STATE, "world already admitted");
+    cudaStream_t s = (cudaStream_t)stream;
+    wig::World& Wd = b->hw[world];
+    const uint64_t bytes = b->pooled ? persistent_bytes(b->L[world])
+                                     : world_buffers_bytes(b->L[world]) + scratch_bytes(Wd.D);
+    void* p = nullptr;
+    if (cudaMallocAsync(&p, bytes, s) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(WIG_E_OOM, "device memory for the world");
+    }
+    CUDA_TRY(cudaMemsetAsync(p, 0, bytes, s));
+    char* q = static_cast<char*>(p);
+    for (int w = 0; w < 7; w++) {
+        if (b->pooled && borrowed(w)) {
+            *buffer_slot(Wd.D, w) = nullptr;  // the lane's pool at each step
+            continue;
+        }
+        *buffer_slot(Wd.D, w) = q;
+        q += align256(b->pooled ? persistent_buffer_bytes(b->L[world], w) : buffer_bytes(b->L[world], w));
+    }
+    if (!b->pooled) scratch_take(Wd, q);
+    CUDA_TRY(cudaMemcpyAsync(b->d_worlds + world, &Wd, sizeof(wig::World), cudaMemcpyHostToDevice, s));
+    for (auto& ln : b->lane)
+        if (ln.d_table) CUDA_TRY(cudaMemcpyAsync(ln.d_table + world, &Wd, sizeof(wig::World), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    b->wmem[world] = p;
+    b->resident += bytes;
+    b->bound[world] = 1;
+    b->dirty[world] = 1;  // (its tiling parity carries on from its last step)
+    return WIG_OK;
+}
+
+int wig_batch_evict(wig_batch* b, uint32_t world, void* stream) {
+    if (!b) return fail(WIG_E_ARG, "null batch");
+    if (world >= b->K) return fail(WIG_E_ARG, "world index out of range");
+    if (b->wmem.empty() || !b->wmem[world]) return fail(WIG_E_STATE, "world not admitted");
+    cudaStream_t s = (cudaStream_t)stream;
+    // its last step done before its memory goes back to the pool
+    if (b->stepped_on[world] != s) CUDA_TRY(cudaStreamSynchronize(b->stepped_on[world]));
+    wig::World& Wd = b->hw[world];
+    const uint64_t bytes = b->pooled ? persistent_bytes(b->L[world])
+                                     : world_buffers_bytes(b->L[world]) + scratch_bytes(Wd.D);
+    CUDA_TRY(cudaFreeAsync(b->wmem[world], s));
+    for (int w = 0; w < 7; w++) *buffer_slot(Wd.D, w) = nullptr;
+    b->wmem[world] = nullptr;
+    b->resident -= bytes;
+    b->bound[world] = 0;
+    return WIG_OK;
+}
+
+uint64_t wig_batch_resident_bytes(const wig_batch* b) { return b ? b->resident : 0u; }
+
+int wig_batch_world_bytes_split(const wig_world_desc* d, uint64_t* persistent, uint64_t* transient) {
+    if (!persistent || !transient) return fail(WIG_E_ARG, "null argument");
+    wig_world_layout L;
+    int rc = layout_of(d, &L);
+    if (rc) return rc;
+    wig::Dev D{};
+    dev_shape(D, L);
+    *persistent = persistent_bytes(L);
+    *transient = transient_bytes(L, D);
+    return WIG_OK;
+}
+
+int wig_batch_set_lane_pool(wig_batch* b, uint32_t lane, uint64_t bytes) {
+    if (!b) return fail(WIG_E_ARG, "null batch");
+    if (lane >= WIG_BATCH_LANES) return fail(WIG_E_ARG, "lane out of range");
+    if (b->wmem.empty()) return fail(WIG_E_STATE, "not a deferred batch");
+    for (uint32_t k = 0; k < b->K; k++)
+        if (b->wmem[k]) return fail(WIG_E_STATE, "set the pools before admitting worlds");
+    Lane& ln = b->lane[lane];
+    CUDA_TRY(cudaDeviceSynchronize());
+    if (ln.d_pool) { cudaFree(ln.d_pool); ln.d_pool = nullptr; ln.pool_bytes = 0; }
+    if (cudaMalloc(&ln.d_pool, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(WIG_E_OOM, "cudaMalloc of a lane pool");
+    }
+    ln.pool_bytes = bytes;
+    if (!ln.d_table) {
+        if (cudaMalloc(&ln.d_table, sizeof(wig::World) * b->K) != cudaSuccess) return fail(WIG_E_OOM, "cudaMalloc lane table");
+        CUDA_TRY(cudaMemcpy(ln.d_table, b->hw.data(), sizeof(wig::World) * b->K, cudaMemcpyHostToDevice));
+    }
+    ln.Bt.worlds = ln.d_table;
+    ln.ctl.table = ln.d_table;
+    ln.ctl.entries = reinterpret_cast<const wig::World*>(ln.d_up + b->entries_at);
+    drop_graphs(ln);
+    b->pooled = true;
+    return WIG_OK;
+}
 
 }  // extern "C"

@@ -259,6 +259,23 @@ __global__ void __launch_bounds__(256) k_fSetup(Batch Bt, const __grid_constant_
     }
 }
 
+// The level-0 arrays neighbours read, zeroed in the blocks not worked on
+// (the invariant), for worlds whose scratch is lent by a pool for the step:
+// a CTA per block of the world.
+__global__ void k_fZeroIdle(Batch Bt) {
+    FOR_ITEMS(Bt, L_WB, it) {
+        FAST_ITEM_G(Bt, it, D, F, w, n);
+        if (D.st->book != 0u || (D.blocks[w.stateSlot(n)] & ACTIVE) != 0u) continue;
+        for (uint32_t t = threadIdx.x; t < 64u; t += blockDim.x) {
+            I2 c{(int)(n % D.BW) * BLOCK + (int)(t & 7u), (int)(n / D.BW) * BLOCK + (int)(t >> 3)};
+            if (!w.inWorld(c)) continue;
+            const uint32_t i = w.cellIndex(c);
+            F.L[0].px[i] = 0.0f; F.L[0].py[i] = 0.0f; F.L[0].rho[i] = 0.0f;
+            F.rimx[i] = 0.0f; F.rimy[i] = 0.0f; F.P[i] = 0.0f;
+        }
+    }
+}
+
 // Zeroes the level-0 arrays the neighbours read (after an upload).
 __global__ void k_fZero(FastW F, uint32_t C) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < C; i += gridDim.x * blockDim.x) {
@@ -1521,6 +1538,10 @@ size_t fast_coarse_smem(const Dev& D, uint32_t lc) {
 }
 
 void fast_zero_level0(const FastW& F, uint32_t cells, cudaStream_t s) { k_fZero<<<148 * 4, 256, 0, s>>>(F, cells); }
+
+void fast_zero_idle(const Batch& Bt, const BatchShape& S, cudaStream_t s) {
+    k_fZeroIdle<<<list_grid(S, L_WB, 32), 64, 0, s>>>(Bt);
+}
 
 // Launches kernel K's instance for the batch: the single-world one with
 // the world as a parameter when `one` is given, else the table one.

@@ -35,6 +35,9 @@ uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, const World* one, cuda
 void fast_finish(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m);
 // Level 0's arrays of one world zeroed (after its buffers are written by the host).
 void fast_zero_level0(const FastW& F, uint32_t cells, cudaStream_t s);
+// The same for the blocks not worked on, of every world of the step whose
+// scratch a pool lends (after compact).
+void fast_zero_idle(const Batch& Bt, const BatchShape& S, cudaStream_t s);
 // Shared memory of the coarse kernel for a world, and the kernel's limit set.
 size_t fast_coarse_smem(const Dev& D, uint32_t lc);
 cudaError_t fast_prepare_attributes(size_t smem);

@@ -118,6 +118,13 @@ __global__ void __launch_bounds__(256) k_schedFill(Batch Bt, SchedCtl c, int pha
             st->bar_count = 0u;
             st->bar_gen = 0u;
         }
+        if (phase == 0 && c.entries && q == 0u) {
+            // the world's table entry for this step (the scan above read only
+            // its shape and persistent buffers, the same in every entry)
+            const uint4* src = reinterpret_cast<const uint4*>(&c.entries[s]);
+            uint4* dst = reinterpret_cast<uint4*>(&c.table[k]);
+            for (uint32_t i = threadIdx.x; i < sizeof(World) / 16u; i += blockDim.x) dst[i] = src[i];
+        }
         for (uint32_t li = 0; li < nl; li++) {
             const uint32_t L = phase == 0 ? kPhaseA[li] : kPhaseB[li];
             const uint32_t* off = c.off + (size_t)L * (c.max_worlds + 1u);
