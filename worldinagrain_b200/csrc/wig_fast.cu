@@ -20,6 +20,8 @@
 // blocks worked on (zeroed at allocation, when a world is uploaded, and as
 // blocks retire), where the reference's field is zero too.
 
+#include <algorithm>
+
 #include "wig_fast.cuh"
 
 namespace wig {
@@ -135,12 +137,15 @@ template <>
 struct WorldSrc<true> {
     World w;
     __device__ __forceinline__ const World& get(const Batch&, uint32_t, WorldCopy&) const { return w; }
+    __device__ __forceinline__ const World& getG(const Batch&, uint32_t) const { return w; }
 };
 template <>
 struct WorldSrc<false> {
     __device__ __forceinline__ const World& get(const Batch& Bt, uint32_t it, WorldCopy& c) const {
         return worldOf(Bt, it, c);
     }
+    // without the CTA's copy (a warp's own item)
+    __device__ __forceinline__ const World& getG(const Batch& Bt, uint32_t it) const { return Bt.world(it); }
 };
 
 // An item's world: its descriptor D, fast scratch F, accessors w, unit j,
@@ -295,92 +300,111 @@ __device__ I2 tileBlockF(const W& w, uint32_t wid, int shift) {
 }
 
 // relaxTile (fluid.wgsl:2109-2182) over the scratch: the rim snapshot's
-// values for liquid cells, the potentials (zero) elsewhere.  `second`: the
-// iteration's relaxation after the V-cycle, on the other tiling from the
-// first (each world's first tiling is its step's).
+// values for liquid cells, the potentials (zero) elsewhere.  A warp a tile
+// (four a CTA, each warp its own run of the list): lane l holds the red and
+// the black cell of quarter l % 4 of row l / 4, so every lane works in every
+// sweep and a sweep ends at a warp barrier.  Within a colour the cells are
+// independent, so each keeps the reference's arithmetic and order.
+// `second`: the iteration's relaxation after the V-cycle, on the other
+// tiling from the first (each world's first tiling is its step's).
 template <bool ONE>
-__global__ void __launch_bounds__(64) k_fRelax(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, int second) {
-    __shared__ WorldCopy wc_;
-    if (!ONE) worldCopyInit(wc_);
-    __shared__ float tpx[RIM * RIM], tpy[RIM * RIM];
-    __shared__ int s_live, s_ox, s_oy;
-    FOR_ITEMS(Bt, L_RELAX, it) {
-        FAST_ITEM(Bt, it, D, F, w, j);
+__global__ void __launch_bounds__(128) k_fRelax(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, int second) {
+    __shared__ float tpx[4][RIM * RIM], tpy[4][RIM * RIM];
+    const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+    float* sx_ = tpx[warp];
+    float* sy_ = tpy[warp];
+    const uint32_t n = Bt.n(L_RELAX);
+    const uint32_t warps = gridDim.x * 4u, per = (n + warps - 1u) / warps;
+    const uint32_t first = (blockIdx.x * 4u + warp) * per, last = min(first + per, n);
+    for (uint32_t g = first; g < last; g++) {
+        const uint32_t it = Bt.item(L_RELAX, g);
+        const World& Wd = src.getG(Bt, it);
+        const Dev& D = Wd.D;
+        const FastW& F = Wd.S;
+        const W w(D);
+        const uint32_t j = Bt.unit(it);
         if (D.st->cont == 0u) continue;
         const int shift = ((D.st->shift_first ^ (uint32_t)second) & 1u) ? BLOCK / 2 : 0;
         const Lvl& L0 = F.L[0];
         const uint32_t na = w.activeCount();
         const uint32_t wid = j < na ? j : D.B + (j - na);
-        if (threadIdx.x == 0) {
-            I2 b = tileBlockF(w, wid, shift);
-            int ox = b.x * BLOCK - shift, oy = b.y * BLOCK - shift;
-            uint32_t live = 0;
-            if (b.x >= 0 && ox < D.W && oy < D.H)
-                live = w.statesOf(I2{ox / BLOCK, oy / BLOCK}, I2{(ox + BLOCK - 1) / BLOCK, (oy + BLOCK - 1) / BLOCK}) & HAS_FLUID;
-            s_live = (int)live;
-            s_ox = ox;
-            s_oy = oy;
-        }
-        __syncthreads();
-        if (s_live) {
-            const int ox = s_ox, oy = s_oy;
-            // the thread's own cell first (independent of the tile's loads)
-            const int lx = (int)(threadIdx.x & 7u), ly = (int)(threadIdx.x >> 3);
+        const I2 b = tileBlockF(w, wid, shift);
+        const int ox = b.x * BLOCK - shift, oy = b.y * BLOCK - shift;
+        if (b.x < 0 || ox >= D.W || oy >= D.H) continue;
+        if ((w.statesOf(I2{ox / BLOCK, oy / BLOCK}, I2{(ox + BLOCK - 1) / BLOCK, (oy + BLOCK - 1) / BLOCK}) & HAS_FLUID) == 0u)
+            continue;
+        // the lane's two cells first (independent of the tile's loads)
+        const int ly = (int)(lane >> 2), q = (int)(lane & 3u);
+        const int p0 = (ox + oy + ly) & 1;
+        int t[2];
+        uint32_t idx[2];
+        bool solving[2], visc[2];
+        float rx[2], ry[2], bx[2], by[2], bz[2], bw[2], dxx[2], dyy[2];
+#pragma unroll
+        for (int c = 0; c < 2; c++) {
+            const int lx = 2 * q + (c == 0 ? p0 : 1 - p0);
             const I2 me{ox + lx, oy + ly};
-            const int t = (ly + 1) * RIM + lx + 1;
-            float rx = 0.0f, ry = 0.0f, bx = 0.0f, by = 0.0f, bz = 0.0f, bw = 0.0f, diag = 0.0f, pinv = 0.0f;
-            uint32_t idx = 0;
+            t[c] = (ly + 1) * RIM + lx + 1;
+            float r_x = 0.0f, r_y = 0.0f, b0 = 0.0f, b1 = 0.0f, b2 = 0.0f, b3 = 0.0f, dg = 0.0f, pv = 0.0f;
+            uint32_t id = 0;
             bool fluid = false;
             if (w.inWorld(me)) {
-                idx = w.cellIndex(me);
-                fluid = L0.rho[idx] > 0.0f;
-                rx = L0.rx[idx];
-                ry = L0.ry[idx];
-                bx = L0.b0[idx];
-                by = L0.b1[idx];
-                bz = L0.b2[idx];
-                bw = L0.b3[idx];
-                diag = L0.diag[idx];
-                pinv = F.pin[idx];
+                id = w.cellIndex(me);
+                fluid = L0.rho[id] > 0.0f;
+                r_x = L0.rx[id];
+                r_y = L0.ry[id];
+                b0 = L0.b0[id];
+                b1 = L0.b1[id];
+                b2 = L0.b2[id];
+                b3 = L0.b3[id];
+                dg = L0.diag[id];
+                pv = F.pin[id];
             }
             if (!fluid) {
-                rx = 0.0f; ry = 0.0f; bx = 0.0f; by = 0.0f; bz = 0.0f; bw = 0.0f; diag = 0.0f; pinv = 0.0f;
+                r_x = 0.0f; r_y = 0.0f; b0 = 0.0f; b1 = 0.0f; b2 = 0.0f; b3 = 0.0f; dg = 0.0f; pv = 0.0f;
             }
-            // the tile and its rim: the snapshot's values for liquid cells,
-            // the potentials elsewhere (all five loads issued at once)
-            for (int k = (int)threadIdx.x; k < RIM * RIM; k += 64) {
-                I2 c{ox - 1 + k % RIM, oy - 1 + k / RIM};
-                float px = 0.0f, py = 0.0f;
-                if (w.inWorld(c)) {
-                    uint32_t i = w.cellIndex(c);
-                    const float r = L0.rho[i], ax = F.rimx[i], ay = F.rimy[i], qx = L0.px[i], qy = L0.py[i];
-                    px = r > 0.0f ? ax : qx;
-                    py = r > 0.0f ? ay : qy;
-                }
-                tpx[k] = px;
-                tpy[k] = py;
-            }
-            __syncthreads();
-            const float dx = diag + pinv, dy = fmaxf(diag, 1e-30f);
-            const bool solving = fluid && dx > 0.0f;
-            const int color = (me.x + me.y) & 1;
-            for (int sw = 0; sw < 2 * SWEEPS; sw++) {
-                if (solving && color == (sw & 1)) {
-                    float sx = bx * tpx[t - 1] + by * tpx[t + 1] + bz * tpx[t - RIM] + bw * tpx[t + RIM];
-                    float sy = bx * tpy[t - 1] + by * tpy[t + 1] + bz * tpy[t - RIM] + bw * tpy[t + RIM];
-                    float nx = mixf(tpx[t], (sx - rx) / dx, SMOOTH_OMEGA);
-                    float ny = mixf(tpy[t], (sy - ry) / dy, SMOOTH_OMEGA);
-                    tpx[t] = nx;
-                    if (diag > 0.0f) tpy[t] = ny;
-                }
-                __syncthreads();
-            }
-            if (solving) {
-                L0.px[idx] = tpx[t];
-                L0.py[idx] = tpy[t];
-            }
+            idx[c] = id;
+            rx[c] = r_x; ry[c] = r_y; bx[c] = b0; by[c] = b1; bz[c] = b2; bw[c] = b3;
+            dxx[c] = dg + pv;
+            dyy[c] = fmaxf(dg, 1e-30f);
+            solving[c] = fluid && dxx[c] > 0.0f;
+            visc[c] = dg > 0.0f;
         }
-        __syncthreads();
+        // the tile and its rim: the snapshot's values for liquid cells, the
+        // potentials elsewhere
+        for (int k = (int)lane; k < RIM * RIM; k += 32) {
+            I2 c{ox - 1 + k % RIM, oy - 1 + k / RIM};
+            float px = 0.0f, py = 0.0f;
+            if (w.inWorld(c)) {
+                uint32_t i = w.cellIndex(c);
+                const float r = L0.rho[i], ax = F.rimx[i], ay = F.rimy[i], qx = L0.px[i], qy = L0.py[i];
+                px = r > 0.0f ? ax : qx;
+                py = r > 0.0f ? ay : qy;
+            }
+            sx_[k] = px;
+            sy_[k] = py;
+        }
+        __syncwarp();
+        for (int sw = 0; sw < 2 * SWEEPS; sw++) {
+            const int c = sw & 1;
+            if (solving[c]) {
+                const int tc = t[c];
+                float sx = bx[c] * sx_[tc - 1] + by[c] * sx_[tc + 1] + bz[c] * sx_[tc - RIM] + bw[c] * sx_[tc + RIM];
+                float sy = bx[c] * sy_[tc - 1] + by[c] * sy_[tc + 1] + bz[c] * sy_[tc - RIM] + bw[c] * sy_[tc + RIM];
+                float nx = mixf(sx_[tc], (sx - rx[c]) / dxx[c], SMOOTH_OMEGA);
+                float ny = mixf(sy_[tc], (sy - ry[c]) / dyy[c], SMOOTH_OMEGA);
+                sx_[tc] = nx;
+                if (visc[c]) sy_[tc] = ny;
+            }
+            __syncwarp();
+        }
+#pragma unroll
+        for (int c = 0; c < 2; c++)
+            if (solving[c]) {
+                L0.px[idx[c]] = sx_[t[c]];
+                L0.py[idx[c]] = sy_[t[c]];
+            }
+        __syncwarp();
     }
 }
 
@@ -1558,7 +1582,9 @@ void fast_setup(const Batch& Bt, const BatchShape& S, const World* one, cudaStre
 }
 
 uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m) {
-    const unsigned G = list_grid(S, L_ACT, 32), G4 = list_grid(S, L_ACT4, 8), GR = list_grid(S, L_RELAX, 32);
+    const unsigned G = list_grid(S, L_ACT, 32), G4 = list_grid(S, L_ACT4, 8);
+    const unsigned GR = (S.max_items[L_RELAX] + 3u) / 4u < 148u * 16u ? std::max((S.max_items[L_RELAX] + 3u) / 4u, 1u)
+                                                                      : 148u * 16u;
     uint32_t launches = 0;
     auto mark = [&](int slot, int phase) {
         if (m) m->fn(m->ctx, slot, phase);
@@ -1569,7 +1595,7 @@ uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, const World* one, cuda
     k_fLoopStart<<<list_grid(S, L_ONE, 1), 32, 0, s>>>(Bt);
     mark(WIG_SLOT_F_LOOP, 1);
     mark(WIG_SLOT_F_RELAX, 0);
-    LAUNCH(k_fRelax, GR, 64, 0, 0);
+    LAUNCH(k_fRelax, GR, 128, 0, 0);
     mark(WIG_SLOT_F_RELAX, 1);
     // down: each world restricts its levels 1..lc by themselves and smooths
     // those above lc, then its levels from lc are the coarse kernel's
@@ -1604,7 +1630,7 @@ uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, const World* one, cuda
     LAUNCH(k_fProlongFine, G, 64, 0);
     mark(WIG_SLOT_F_PROLONG_FINE, 1);
     mark(WIG_SLOT_F_RELAX, 0);
-    LAUNCH(k_fRelax, GR, 64, 0, 1);
+    LAUNCH(k_fRelax, GR, 128, 0, 1);
     mark(WIG_SLOT_F_RELAX, 1);
     mark(WIG_SLOT_F_RHO_BETA, 0);
     LAUNCH(k_fRhoBeta, G4, 256, 0);
