@@ -106,6 +106,46 @@ __device__ T sumBlocks256(const W& w, const T* part, int comp, T* s) {
     return r;
 }
 
+// sumBlocks of both components of the partials in one pass (each component
+// in sumBlocks256's order).
+template <class T>
+__device__ void sumBlocks256x2(const W& w, const T* part, T* s0, T* s1, T* out0, T* out1) {
+    const uint32_t B = w.D.B;
+    const uint32_t* state = w.D.blocks + B;
+    const uint32_t li = threadIdx.x;
+    T a0 = T(0), a1 = T(0);
+    for (uint32_t k0 = li; k0 < B; k0 += 256u * 16u) {
+        T v0[16], v1[16];
+        uint32_t st[16];
+#pragma unroll
+        for (int u = 0; u < 16; u++) {
+            const uint32_t k = k0 + 256u * (uint32_t)u;
+            st[u] = k < B ? __ldcg(&state[k]) : 0u;
+            v0[u] = k < B ? __ldcg(&part[2u * k]) : T(0);
+            v1[u] = k < B ? __ldcg(&part[2u * k + 1u]) : T(0);
+        }
+#pragma unroll
+        for (int u = 0; u < 16; u++)
+            if ((st[u] & ACTIVE) != 0u) {
+                a0 = a0 + v0[u];
+                a1 = a1 + v1[u];
+            }
+    }
+    s0[li] = a0;
+    s1[li] = a1;
+    __syncthreads();
+    for (int h = 128; h > 0; h >>= 1) {
+        if ((int)li < h) {
+            s0[li] = s0[li] + s0[li + h];
+            s1[li] = s1[li] + s1[li + h];
+        }
+        __syncthreads();
+    }
+    *out0 = s0[0];
+    *out1 = s1[0];
+    __syncthreads();
+}
+
 // Whether this CTA counted the last of `total` tiles (its writers fenced
 // their partials before the barrier): a threadfence reduction's test.
 __device__ bool lastOf4(uint32_t* counter, uint32_t inc, uint32_t total) {
@@ -121,6 +161,24 @@ __device__ bool lastOf4(uint32_t* counter, uint32_t inc, uint32_t total) {
     }
     __syncthreads();
     return last != 0;
+}
+
+// Whether a CTA's run over a list ends its share of a world at item g (the
+// run's last item, or the next item is another world's): where it counts
+// the tiles it finished, one atomic per world a CTA instead of one per item.
+__device__ __forceinline__ bool worldRunEnds(const Batch& Bt, uint32_t list, uint32_t g, uint32_t e, uint32_t it) {
+    if (g + 1u >= e) return true;
+    return ((uint64_t)Bt.item(list, g + 1u) >> Bt.lbits) != ((uint64_t)it >> Bt.lbits);
+}
+
+// At the end of a world's run: counts the CTA's pending tiles of that world;
+// true in the CTA that counted the world's last tile.
+__device__ __forceinline__ bool flushTiles(const Batch& Bt, uint32_t g, uint32_t e, uint32_t it, uint32_t& pend,
+                                           uint32_t* counter, uint32_t total) {
+    if (!worldRunEnds(Bt, L_ACT4, g, e, it)) return false;
+    const uint32_t inc = pend;
+    pend = 0u;
+    return lastOf4(counter, inc, total);
 }
 
 __device__ __forceinline__ I2 tileCell(const W& w, uint32_t wid) {
@@ -177,6 +235,7 @@ __global__ void __launch_bounds__(256) k_fSetup(Batch Bt, const __grid_constant_
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
     __shared__ double s64[256];
+    uint32_t pend_ = 0;  // tiles finished of the current world, not yet counted
     FOR_ITEMS(Bt, L_ACT4, it) {
         FAST_ITEM(Bt, it, D, F, w, g);
         const uint32_t na = w.activeCount();
@@ -238,7 +297,8 @@ __global__ void __launch_bounds__(256) k_fSetup(Batch Bt, const __grid_constant_
                 D.norm64[2u * w.blockIndex(w.activeBlock(wid))] = v;
                 __threadfence();
             }
-            if (lastOf4(&D.st->fdone[0], min(4u, na - g * 4u), na)) {
+            pend_ += min(4u, na - g * 4u);
+            if (flushTiles(Bt, g_it, e_it, it, pend_, &D.st->fdone[0], na)) {
                 double bn = sumBlocks256(w, D.norm64, 0, s64);
                 if (threadIdx.x == 0) {
                     D.st->bnorm2 = bn;
@@ -840,7 +900,8 @@ __global__ void __launch_bounds__(256) k_fRhoBeta(Batch Bt, const __grid_constan
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
     __shared__ float sx[256], sy[256];
-    __shared__ double s64[256];
+    __shared__ double s64[256], s64b[256];
+    uint32_t pend_ = 0;  // tiles finished of the current world, not yet counted
     FOR_ITEMS(Bt, L_ACT4, it) {
         FAST_ITEM(Bt, it, D, F, w, g);
         if (D.st->cont == 0u) continue;
@@ -883,18 +944,19 @@ __global__ void __launch_bounds__(256) k_fRhoBeta(Batch Bt, const __grid_constan
             }
             __threadfence();
         }
-        if (lastOf4(&D.st->fdone[1], min(4u, na - g * 4u), na)) {
+        pend_ += min(4u, na - g * 4u);
+        if (flushTiles(Bt, g_it, e_it, it, pend_, &D.st->fdone[1], na)) {
             if (f64) {
-                double rz = sumBlocks256(w, F.part64, 0, s64);
-                double zq = sumBlocks256(w, F.part64, 1, s64);
+                double rz, zq;
+                sumBlocks256x2(w, F.part64, s64, s64b, &rz, &zq);
                 if (threadIdx.x == 0) {
                     double beta = (cycle == 0u || D.st->pq <= 0.0) ? 0.0 : -zq / D.st->pq;
                     D.st->rz = rz;
                     D.st->beta = beta;
                 }
             } else {
-                float rz = sumBlocks256(w, F.part32, 0, sx);
-                float zq = sumBlocks256(w, F.part32, 1, sx);
+                float rz, zq;
+                sumBlocks256x2(w, F.part32, sx, sy, &rz, &zq);
                 if (threadIdx.x == 0) {
                     float beta = (cycle == 0u || D.st->pq32 <= 0.0f) ? 0.0f : -zq / D.st->pq32;
                     D.st->rz32 = rz;
@@ -936,6 +998,7 @@ __global__ void __launch_bounds__(256) k_fApplyAlpha(Batch Bt, const __grid_cons
     if (!ONE) worldCopyInit(wc_);
     __shared__ float sx[256];
     __shared__ double s64[256];
+    uint32_t pend_ = 0;  // tiles finished of the current world, not yet counted
     FOR_ITEMS(Bt, L_ACT4, it) {
         FAST_ITEM(Bt, it, D, F, w, g);
         if (D.st->cont == 0u) continue;
@@ -980,7 +1043,8 @@ __global__ void __launch_bounds__(256) k_fApplyAlpha(Batch Bt, const __grid_cons
             }
             __threadfence();
         }
-        if (lastOf4(&D.st->fdone[2], min(4u, na - g * 4u), na)) {
+        pend_ += min(4u, na - g * 4u);
+        if (flushTiles(Bt, g_it, e_it, it, pend_, &D.st->fdone[2], na)) {
             if (f64) {
                 double pq = sumBlocks256(w, F.part64, 0, s64);
                 if (threadIdx.x == 0) {
@@ -1008,6 +1072,7 @@ __global__ void __launch_bounds__(256) k_fUpdate(Batch Bt, const __grid_constant
     if (!ONE) worldCopyInit(wc_);
     __shared__ uint32_t most[4];
     __shared__ double s64[256];
+    uint32_t pend_ = 0;  // tiles finished of the current world, not yet counted
     FOR_ITEMS(Bt, L_ACT4, it) {
         FAST_ITEM(Bt, it, D, F, w, g);
         if (D.st->cont == 0u) continue;
@@ -1055,7 +1120,8 @@ __global__ void __launch_bounds__(256) k_fUpdate(Batch Bt, const __grid_constant
             atomicMax(&D.blocks[w.countSlot(COUNT_RESIDUAL + cycle % 3u)], most[threadIdx.x >> 6]);
             __threadfence();
         }
-        if (lastOf4(&D.st->fdone[3], min(4u, na - g * 4u), na)) {
+        pend_ += min(4u, na - g * 4u);
+        if (flushTiles(Bt, g_it, e_it, it, pend_, &D.st->fdone[3], na)) {
             bool conv;
             if (tol) {
                 double rr = sumBlocks256(w, D.norm64, 0, s64);
