@@ -1071,7 +1071,9 @@ __global__ void __launch_bounds__(256) k_fUpdate(Batch Bt, const __grid_constant
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
     __shared__ uint32_t most[4];
+    __shared__ uint32_t runMost;  // the largest |r| of the current world's run (bits of a non-negative float)
     __shared__ double s64[256];
+    if (threadIdx.x == 0) runMost = 0u;
     uint32_t pend_ = 0;  // tiles finished of the current world, not yet counted
     FOR_ITEMS(Bt, L_ACT4, it) {
         FAST_ITEM(Bt, it, D, F, w, g);
@@ -1117,10 +1119,20 @@ __global__ void __launch_bounds__(256) k_fUpdate(Batch Bt, const __grid_constant
         __syncthreads();
         if (valid && (threadIdx.x & 63u) == 0u) {
             if (tol) D.norm64[2u * w.blockIndex(w.activeBlock(wid))] = t2;
-            atomicMax(&D.blocks[w.countSlot(COUNT_RESIDUAL + cycle % 3u)], most[threadIdx.x >> 6]);
+            atomicMax(&runMost, most[threadIdx.x >> 6]);
             __threadfence();
         }
         pend_ += min(4u, na - g * 4u);
+        if (worldRunEnds(Bt, L_ACT4, g_it, e_it, it)) {
+            // the run's largest |r| into the world's residual slot (a max of
+            // maxima: the same word), before its tiles are counted
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                atomicMax(&D.blocks[w.countSlot(COUNT_RESIDUAL + cycle % 3u)], runMost);
+                runMost = 0u;
+                __threadfence();
+            }
+        }
         if (flushTiles(Bt, g_it, e_it, it, pend_, &D.st->fdone[3], na)) {
             bool conv;
             if (tol) {
