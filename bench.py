@@ -433,7 +433,7 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=20.0)
     ap.add_argument("--cpu-steps-max", type=int, default=20)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--form", default="fast", choices=["fast", "plain", "persistent"])
+    ap.add_argument("--form", default="fast", choices=["fast", "plain", "persistent", "mixed"])
     ap.add_argument("--workload", default="single", choices=["single", "batched", "served"])
     ap.add_argument("--worlds", type=int, default=None)
     ap.add_argument("--rates", default="1000,2000,5000,10000,20000,50000")
@@ -448,6 +448,8 @@ def main():
         FLAGS = FLAGS | abi.STEP_PLAIN
     elif args.form == "persistent":
         FLAGS = FLAGS | abi.STEP_PERSISTENT
+    elif args.form == "mixed":
+        FLAGS = FLAGS | abi.STEP_MIXED
 
     rank = int(os.environ.get("RANK", "0"))
     world_size = int(os.environ.get("WORLD_SIZE", "1"))

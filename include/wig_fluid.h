@@ -42,7 +42,7 @@
 extern "C" {
 #endif
 
-#define WIG_ABI_VERSION 1u
+#define WIG_ABI_VERSION 2u
 
 /* Error codes. */
 #define WIG_OK 0
@@ -180,6 +180,12 @@ typedef struct wig_fluid_buffers {
 #define WIG_STEP_SYNC_STATS 64u       /* copy the stats to the host at the end of the step */
 #define WIG_STEP_PLAIN 128u           /* the solve as one kernel per reference pass (else the fast form) */
 #define WIG_STEP_PERSISTENT 256u      /* the fast form's iterations as one persistent cooperative kernel (else kernels in a graph WHILE loop) */
+#define WIG_STEP_MIXED 512u           /* mixed precision (fast form, with TOLERANCE and F64_DOTS): each coarse level's
+                                         operator (density, stencil coefficients) stored in binary16 and worked in FP32,
+                                         potentials, right-hand sides and CG vectors FP32, dots and norms FP64; every 8th
+                                         iteration and before the solve stops, the true residual b + A x worked in FP64
+                                         and put in for the recursive one when it has drifted above it and above the
+                                         FP32 rounding floor of A x; not bit-exact with the other forms */
 
 /* Per-step statistics (the report words, js/sim.js:1882-1900, plus the
  * solve's residuals). */
@@ -188,8 +194,9 @@ typedef struct wig_fluid_stats {
     uint32_t particles;               /* sorted.count after the step */
     uint32_t cycles;                  /* CG iterations run this step */
     uint32_t launches;                /* kernels the last step launched */
-    double rel_residual;              /* ||r||2/||b||2 of the CG residual, FP64 (tolerance mode) */
+    double rel_residual;              /* ||r||2/||b||2 of the CG (recursive) residual, FP64 (tolerance mode) */
     double b_norm;                    /* ||b||2 at the solve's start */
+    double true_residual;             /* the mixed form: ||b + A x||2/||b||2 worked in FP64 at its last check (else 0) */
 } wig_fluid_stats;
 
 typedef struct wig_fluid wig_fluid;

@@ -40,7 +40,7 @@ def test_struct_sizes():
     assert C.sizeof(abi.Params) == 80
     assert C.sizeof(abi.Elem) == 80
     assert C.sizeof(abi.Buffers) == 7 * 8
-    assert C.sizeof(abi.Stats) == 9 * 4 + 3 * 4 + 2 * 8
+    assert C.sizeof(abi.Stats) == 9 * 4 + 3 * 4 + 3 * 8
 
 
 @pytest.mark.parametrize("wh", [(1, 1), (7, 5), (64, 64), (131, 97), (256, 256), (1024, 1024), (2048, 2048), (1000, 300)])

@@ -5,7 +5,7 @@ Python host side and the tests.
 """
 import ctypes as C
 
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 FLUID_BLOCK = 8
 LIQUID_CELL_WORDS = 11
@@ -35,6 +35,7 @@ STEP_F64_DOTS = 32
 STEP_SYNC_STATS = 64
 STEP_PLAIN = 128
 STEP_PERSISTENT = 256
+STEP_MIXED = 512
 
 PASSES = [
     "SYNC", "SYNC_MARKS", "SYNC_PARTICLES", "SYNC_SEED", "COMPACT", "RETIRE", "CLEAR", "GATHER",
@@ -99,7 +100,8 @@ class Buffers(C.Structure):
 
 class Stats(C.Structure):
     _fields_ = [("count", C.c_uint32 * FLUID_STATS), ("particles", C.c_uint32), ("cycles", C.c_uint32),
-                ("launches", C.c_uint32), ("rel_residual", C.c_double), ("b_norm", C.c_double)]
+                ("launches", C.c_uint32), ("rel_residual", C.c_double), ("b_norm", C.c_double),
+                ("true_residual", C.c_double)]
 
 
 BUFFER_NAMES = ("cells", "sorted", "parts", "counters", "field", "blocks", "cg")

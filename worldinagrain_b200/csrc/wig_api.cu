@@ -58,6 +58,7 @@ struct Report {
     uint32_t pad;
     double rel;
     double bnorm2;
+    double rel_true;
 };
 
 // Each world's report into its slot (by world) and the lane's (by the
@@ -74,6 +75,7 @@ __global__ void k_report(wig::Batch Bt, Report* by_world, Report* by_entry) {
         r.pad = 0u;
         r.rel = D.st->rel;
         r.bnorm2 = D.st->bnorm2;
+        r.rel_true = D.st->rel_true;
         by_world[k] = r;
         by_entry[g_it] = r;
     }
@@ -249,7 +251,10 @@ void dev_shape(wig::Dev& D, const wig_world_layout& L) {
 size_t scratch_bytes(const wig::Dev& D) {
     const size_t C = D.C;
     size_t bytes = align256(C) + 17u * align256(C * 4u);
-    for (uint32_t l = 1; l <= D.levels; l++) bytes += 10u * align256((size_t)D.level_w[l] * D.level_h[l] * 4u);
+    for (uint32_t l = 1; l <= D.levels; l++) {
+        bytes += 10u * align256((size_t)D.level_w[l] * D.level_h[l] * 4u);
+        bytes += align256(5u * (size_t)D.level_w[l] * D.level_h[l] * 2u);  // the binary16 operator
+    }
     bytes += align256(2u * (size_t)D.B * 4u) + 3u * align256(2u * (size_t)D.B * 8u);
     return bytes;
 }
@@ -267,6 +272,11 @@ void scratch_take(wig::World& Wd, char* p) {
         wig::Lvl& V = F.L[l];
         V.px = fl(n); V.py = fl(n); V.rx = fl(n); V.ry = fl(n); V.rho = fl(n);
         V.b0 = fl(n); V.b1 = fl(n); V.b2 = fl(n); V.b3 = fl(n); V.diag = fl(n);
+    }
+    F.H[0] = wig::LvlH{nullptr, 0u, 0u};
+    for (uint32_t l = 1; l <= D.levels; l++) {
+        const size_t n = (size_t)D.level_w[l] * D.level_h[l];
+        F.H[l] = wig::LvlH{reinterpret_cast<__half*>(take(5u * n * 2u)), (uint32_t)n, 0u};
     }
     F.pin = fl(C); F.rimx = fl(C); F.rimy = fl(C);
     F.X = fl(C); F.R = fl(C); F.P = fl(C); F.Q = fl(C);
@@ -772,6 +782,7 @@ int record_step_fast(wig_batch* b, Lane& ln, uint32_t max_cycles, uint32_t flags
     wig::Marker mk{&Rec::mark, &R};
     ln.Bt.max_cycles = max_cycles;
     ln.Bt.cond = 0;
+    ln.Bt.mixed = (flags & WIG_STEP_MIXED) ? 1u : 0u;
     const wig::World* one = b->K == 1 ? &b->hw[0] : nullptr;
     if (b->pooled) {
         wig::fast_zero_idle(ln.Bt, b->S, s);
@@ -853,6 +864,10 @@ int check_step(wig_batch* b, const StepArgs& a) {
     if ((a.flags & WIG_STEP_TOLERANCE) && !(a.tol > 0.0)) return fail(WIG_E_ARG, "tolerance must be positive");
     if ((a.flags & (WIG_STEP_PLAIN | WIG_STEP_PERSISTENT)) && b->K != 1)
         return fail(WIG_E_ARG, "the plain and persistent forms step one world");
+    if ((a.flags & WIG_STEP_MIXED) &&
+        ((a.flags & (WIG_STEP_PLAIN | WIG_STEP_PERSISTENT)) ||
+         (a.flags & (WIG_STEP_TOLERANCE | WIG_STEP_F64_DOTS)) != (WIG_STEP_TOLERANCE | WIG_STEP_F64_DOTS)))
+        return fail(WIG_E_ARG, "the mixed form is a fast form with WIG_STEP_TOLERANCE and WIG_STEP_F64_DOTS");
     std::vector<char> seen(b->K, 0);
     for (uint32_t i = 0; i < a.count; i++) {
         const uint32_t k = a.worlds[i];
@@ -956,7 +971,7 @@ int batch_step(wig_batch* b, const StepArgs& a) {
     const bool plain = (a.flags & WIG_STEP_PLAIN) != 0u;
     if (!plain) zero_dirty(b, a);
     const bool book1 = b->K == 1 && ((a.world_flags ? a.world_flags[0] : a.flags) & WIG_STEP_BOOKKEEPING_ONLY) != 0u;
-    uint32_t shape = a.flags & (WIG_STEP_TOLERANCE | WIG_STEP_F64_DOTS | WIG_STEP_PLAIN | WIG_STEP_PERSISTENT);
+    uint32_t shape = a.flags & (WIG_STEP_TOLERANCE | WIG_STEP_F64_DOTS | WIG_STEP_PLAIN | WIG_STEP_PERSISTENT | WIG_STEP_MIXED);
     if (viscous) shape |= WIG_STEP_VISCOUS;
     if (book1) shape |= WIG_STEP_BOOKKEEPING_ONLY;
     const bool parity_keyed = plain || (a.flags & WIG_STEP_PERSISTENT);
@@ -1012,7 +1027,7 @@ int batch_step_profile(wig_batch* b, const StepArgs& a, float* ms_out, uint32_t*
     if (rc) return rc;
     const bool plain = (a.flags & WIG_STEP_PLAIN) != 0u;
     const bool book1 = b->K == 1 && ((a.world_flags ? a.world_flags[0] : a.flags) & WIG_STEP_BOOKKEEPING_ONLY) != 0u;
-    uint32_t shape = a.flags & (WIG_STEP_TOLERANCE | WIG_STEP_F64_DOTS | WIG_STEP_PLAIN | WIG_STEP_PERSISTENT);
+    uint32_t shape = a.flags & (WIG_STEP_TOLERANCE | WIG_STEP_F64_DOTS | WIG_STEP_PLAIN | WIG_STEP_PERSISTENT | WIG_STEP_MIXED);
     if (viscous) shape |= WIG_STEP_VISCOUS;
     if (book1) shape |= WIG_STEP_BOOKKEEPING_ONLY;
     Prof prof;
@@ -1075,6 +1090,7 @@ int batch_read_stats(wig_batch* b, const uint32_t* worlds, uint32_t count, wig_f
         if (li >= 0) o.launches = b->lane[li].last_launches + b->lane[li].last_body * r.count[WIG_COUNT_CYCLES];
         o.rel_residual = r.rel;
         o.b_norm = r.bnorm2 > 0.0 ? __builtin_sqrt(r.bnorm2) : 0.0;
+        o.true_residual = r.rel_true;
         if (rc == WIG_OK) {
             if (r.err & wig::ERR_BARRIER) rc = fail(WIG_E_STATE, "the persistent solve's grid barrier waited past its limit");
             else if (r.err) rc = fail(WIG_E_STATE, "a device loop hit its iteration limit (union-find)");

@@ -8,6 +8,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <string>
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -101,7 +102,10 @@ struct StepState {
     // f32 scalars (fluid.wgsl's cg sums: r.z, alpha, beta, p.Ap)
     uint32_t cycle;
     uint32_t cont;
-    uint32_t fdone[4];
+    uint32_t fdone[6];
+    uint32_t check;     // the mixed form: this iteration's true residual is to be checked
+    uint32_t drift;     // the mixed form: the true residual is to be put in for the recursive one
+    double rel_true;    // the mixed form: the last check's ||b + A x||2/||b||2
     float rz32, pq32, alpha32, beta32;
     // the persistent solve's grid barrier: arrivals and generation
     uint32_t bar_count;
@@ -352,9 +356,19 @@ struct Lvl {
     float *b0, *b1, *b2, *b3, *diag;
 };
 
+// A coarse level's operator in binary16 (the mixed-precision form): its
+// density and four stencil coefficients (rho, b0, b1, b2, b3), n values each,
+// from base; its potentials and right-hand sides stay in Lvl's f32 arrays.
+struct LvlH {
+    __half* base;
+    uint32_t n;
+    uint32_t pad_;
+};
+
 // A world's fast-form scratch.
 struct FastW {
     Lvl L[WIG_MG_LEVELS + 1];  // level 0 (the cells) .. levels
+    LvlH H[WIG_MG_LEVELS + 1]; // levels 1 .. levels: the operator in binary16 (the mixed form)
     float* pin;                // level 0: PIN at a pinned root, else 0
     uint8_t* fmask;            // level 0: bit d set when neighbour d is liquid
     float *rimx, *rimy;        // level 0: the relaxation's rim snapshot
@@ -400,6 +414,7 @@ struct Batch {
     uint32_t base[L_COUNT];
     uint32_t lbits;           // bits of an item's unit
     uint32_t single;          // a batch of one world: item g of any list is unit g of world 0
+    uint32_t mixed;           // the mixed-precision form (coarse operators in binary16, true-residual checks)
     uint32_t max_cycles;
     unsigned long long cond;  // cudaGraphConditionalHandle of the iteration loop (0: none)
     uint32_t* loop;           // the loop's verdict: 1 when a world iterates again

@@ -470,36 +470,79 @@ __global__ void __launch_bounds__(128) k_fRelax(Batch Bt, const __grid_constant_
 
 // ================================================================ the levels
 
+// A level's arrays as stored: the potentials and right-hand sides in f32,
+// the operator (density, stencil coefficients, diagonal) in T: f32 (the
+// plain precision) or binary16 (the coarse levels of the mixed form); values
+// are read into and worked in f32.
+template <class T>
+struct LRef {
+    float *px, *py, *rx, *ry;
+    T *rho, *b0, *b1, *b2, *b3, *diag;
+};
+__device__ __forceinline__ float ld(const float* p) { return *p; }
+__device__ __forceinline__ float ld(const __half* p) { return __half2float(*p); }
+__device__ __forceinline__ void st(float* p, float v) { *p = v; }
+__device__ __forceinline__ void st(__half* p, float v) { *p = __float2half_rn(v); }
+
+template <class T>
+__device__ __forceinline__ LRef<T> lref(const FastW& F, uint32_t l);
+template <>
+__device__ __forceinline__ LRef<float> lref<float>(const FastW& F, uint32_t l) {
+    const Lvl& V = F.L[l];
+    return LRef<float>{V.px, V.py, V.rx, V.ry, V.rho, V.b0, V.b1, V.b2, V.b3, V.diag};
+}
+template <>
+__device__ __forceinline__ LRef<__half> lref<__half>(const FastW& F, uint32_t l) {
+    const Lvl& V = F.L[l];
+    __half* b = F.H[l].base;
+    const uint32_t n = F.H[l].n;
+    return LRef<__half>{V.px, V.py, V.rx, V.ry, b, b + n, b + 2u * n, b + 3u * n, b + 4u * n, nullptr};
+}
+
+// A cell's diagonal: stored in f32 (the sum of its four coefficients, in
+// that order); in binary16 not stored but the sum of the rounded
+// coefficients, so the rounded operator keeps its diagonal equal to the sum
+// of its off-diagonals (a separately rounded diagonal could fall below it
+// and make a region with no free surface indefinite).
+__device__ __forceinline__ float diagAt(const LRef<float>& V, uint32_t k) { return V.diag[k]; }
+__device__ __forceinline__ float diagAt(const LRef<__half>& V, uint32_t k) {
+    return ((ld(V.b0 + k) + ld(V.b1 + k)) + ld(V.b2 + k)) + ld(V.b3 + k);
+}
+
 // residualAt (fluid.wgsl:2306-2315) of cell k on a level held in arrays with
 // stored coefficients (level 0's pinned roots held at PIN).
-__device__ __forceinline__ V2 residualStored(const Lvl& V, const float* pin, uint32_t k, int x, int y, int lw, int lh, float h2) {
+template <class T>
+__device__ __forceinline__ V2 residualStored(const LRef<T>& V, const float* pin, uint32_t k, int x, int y, int lw, int lh,
+                                             float h2) {
     float sx = 0.0f, sy = 0.0f;
-    const float b[4] = {V.b0[k], V.b1[k], V.b2[k], V.b3[k]};
+    const float b[4] = {ld(V.b0 + k), ld(V.b1 + k), ld(V.b2 + k), ld(V.b3 + k)};
 #pragma unroll
     for (int d = 0; d < 4; d++) {
         uint32_t n = nbr(k, x, y, lw, lh, d);
-        sx = sx + b[d] * V.px[n];
-        sy = sy + b[d] * V.py[n];
+        sx = sx + b[d] * ld(V.px + n);
+        sy = sy + b[d] * ld(V.py + n);
     }
-    const float dg = V.diag[k];
+    const float dg = diagAt(V, k);
     const float pinx = pin ? pin[k] : 0.0f;
-    return V2{V.rx[k] - (sx - (dg + pinx) * V.px[k]) / h2, V.ry[k] - (sy - (dg + 0.0f) * V.py[k]) / h2};
+    return V2{ld(V.rx + k) - (sx - (dg + pinx) * ld(V.px + k)) / h2, ld(V.ry + k) - (sy - (dg + 0.0f) * ld(V.py + k)) / h2};
 }
 
-// One coarse cell of restrictLevel (fluid.wgsl:2342-2377), level l from l - 1.
-__device__ void restrictCell(const Dev& D, const FastW& F, const W& w, uint32_t l, uint32_t j) {
+// One coarse cell of restrictLevel (fluid.wgsl:2342-2377), level l (stored
+// as TV) from l - 1 (stored as TU).
+template <class TU, class TV>
+__device__ void restrictCellT(const Dev& D, const FastW& F, const W& w, uint32_t l, uint32_t j) {
     const int lw = (int)D.level_w[l];
     const int cx = (int)(j % (uint32_t)lw), cy = (int)(j / (uint32_t)lw);
-    const Lvl& V = F.L[l];
+    const LRef<TV> V = lref<TV>(F, l);
     const int span = 1 << l;
     if (span <= BLOCK) {
         I2 b{cx * span / BLOCK, cy * span / BLOCK};
         if (w.inBlocks(b) && (D.blocks[w.stateSlot(w.blockIndex(b))] & ACTIVE) == 0u) {
-            V.px[j] = 0.0f; V.py[j] = 0.0f; V.rx[j] = 0.0f; V.ry[j] = 0.0f; V.rho[j] = 0.0f;
+            st(V.px + j, 0.0f); st(V.py + j, 0.0f); st(V.rx + j, 0.0f); st(V.ry + j, 0.0f); st(V.rho + j, 0.0f);
             return;
         }
     }
-    const Lvl& U = F.L[l - 1];
+    const LRef<TU> U = lref<TU>(F, l - 1u);
     const int uw = (int)D.level_w[l - 1], uh = (int)D.level_h[l - 1];
     const float h2 = (float)(1u << (2u * (l - 1u)));
     const float* pin = l == 1u ? F.pin : nullptr;
@@ -509,7 +552,7 @@ __device__ void restrictCell(const Dev& D, const FastW& F, const W& w, uint32_t 
         int kx = 2 * cx + (q & 1), ky = 2 * cy + (q >> 1);
         if (kx >= uw || ky >= uh) continue;  // rhoAt outside the level: -1
         uint32_t k = (uint32_t)ky * (uint32_t)uw + (uint32_t)kx;
-        float rho = U.rho[k];
+        float rho = ld(U.rho + k);
         if (rho == 0.0f) air = true;
         else if (rho > 0.0f) {
             fluid = fluid + 1.0f;
@@ -520,21 +563,28 @@ __device__ void restrictCell(const Dev& D, const FastW& F, const W& w, uint32_t 
         }
     }
     const float rho = air ? 0.0f : (fluid > 0.0f ? sum / fluid : -1.0f);
-    V.px[j] = 0.0f;
-    V.py[j] = 0.0f;
-    V.rx[j] = rho > 0.0f ? rx * 0.25f : 0.0f;
-    V.ry[j] = rho > 0.0f ? ry * 0.25f : 0.0f;
-    V.rho[j] = rho;
+    st(V.px + j, 0.0f);
+    st(V.py + j, 0.0f);
+    st(V.rx + j, rho > 0.0f ? rx * 0.25f : 0.0f);
+    st(V.ry + j, rho > 0.0f ? ry * 0.25f : 0.0f);
+    st(V.rho + j, rho);
+}
+// Level l from l - 1 with the levels stored as T (level 0 always f32).
+template <class T = float>
+__device__ __forceinline__ void restrictCell(const Dev& D, const FastW& F, const W& w, uint32_t l, uint32_t j) {
+    if (l == 1u) restrictCellT<float, T>(D, F, w, l, j);
+    else restrictCellT<T, T>(D, F, w, l, j);
 }
 
 // One cell of smoothAt (fluid.wgsl:2318-2334) on level l >= 1, the
 // coefficients worked out on the step's first iteration and kept.
+template <class T = float>
 __device__ void smoothCell(const Dev& D, const FastW& F, uint32_t l, int color, bool first, uint32_t j) {
     const int lw = (int)D.level_w[l], lh = (int)D.level_h[l];
     const int cx = (int)(j % (uint32_t)lw), cy = (int)(j / (uint32_t)lw);
     if (((cx + cy) & 1) != color) return;
-    const Lvl& V = F.L[l];
-    const float rho = V.rho[j];
+    const LRef<T> V = lref<T>(F, l);
+    const float rho = ld(V.rho + j);
     if (rho <= 0.0f) return;
     float b[4];
     float dg;
@@ -543,33 +593,37 @@ __device__ void smoothCell(const Dev& D, const FastW& F, uint32_t l, int color, 
         for (int d = 0; d < 4; d++) {
             b[d] = 0.0f;
             if (!nbrIn(cx, cy, lw, lh, d)) continue;
-            float r = V.rho[nbr(j, cx, cy, lw, lh, d)];
+            float r = ld(V.rho + nbr(j, cx, cy, lw, lh, d));
             if (r < 0.0f) continue;
             b[d] = faceBeta(rho, r);
             dg = dg + b[d];
         }
-        V.b0[j] = b[0]; V.b1[j] = b[1]; V.b2[j] = b[2]; V.b3[j] = b[3];
-        V.diag[j] = dg;
+        st(V.b0 + j, b[0]); st(V.b1 + j, b[1]); st(V.b2 + j, b[2]); st(V.b3 + j, b[3]);
+        if (V.diag) st(V.diag + j, dg);
+        // worked in what is stored, as later iterations read it
+        b[0] = ld(V.b0 + j); b[1] = ld(V.b1 + j); b[2] = ld(V.b2 + j); b[3] = ld(V.b3 + j);
+        dg = diagAt(V, j);
     } else {
-        b[0] = V.b0[j]; b[1] = V.b1[j]; b[2] = V.b2[j]; b[3] = V.b3[j];
-        dg = V.diag[j];
+        b[0] = ld(V.b0 + j); b[1] = ld(V.b1 + j); b[2] = ld(V.b2 + j); b[3] = ld(V.b3 + j);
+        dg = diagAt(V, j);
     }
     if (dg <= 0.0f) return;
     float sx = 0.0f, sy = 0.0f;
 #pragma unroll
     for (int d = 0; d < 4; d++) {
         uint32_t n = nbr(j, cx, cy, lw, lh, d);
-        sx = sx + b[d] * V.px[n];
-        sy = sy + b[d] * V.py[n];
+        sx = sx + b[d] * ld(V.px + n);
+        sy = sy + b[d] * ld(V.py + n);
     }
     const float h2 = (float)(1u << (2u * l));
-    const float ex = V.px[j], ey = V.py[j];
-    V.px[j] = mixf(ex, (sx - h2 * V.rx[j]) / dg, 1.0f);
-    V.py[j] = mixf(ey, (sy - h2 * V.ry[j]) / dg, 1.0f);
+    const float ex = ld(V.px + j), ey = ld(V.py + j);
+    st(V.px + j, mixf(ex, (sx - h2 * ld(V.rx + j)) / dg, 1.0f));
+    st(V.py + j, mixf(ey, (sy - h2 * ld(V.ry + j)) / dg, 1.0f));
 }
 
 // prolonged (fluid.wgsl:2478-2497) from level l + 1's arrays.
-__device__ __forceinline__ V2 prolongedFrom(const float* rho, const float* px, const float* py, int lw, int lh, int cx, int cy) {
+template <class T>
+__device__ __forceinline__ V2 prolongedFrom(const T* rho, const float* px, const float* py, int lw, int lh, int cx, int cy) {
     const int kx = cx / 2, ky = cy / 2;
     const int sx = (cx & 1) == 1 ? 1 : -1, sy = (cy & 1) == 1 ? 1 : -1;
     const int ox[4] = {0, sx, 0, sx}, oy[4] = {0, 0, sy, sy};
@@ -580,12 +634,12 @@ __device__ __forceinline__ V2 prolongedFrom(const float* rho, const float* px, c
         int ax_ = kx + ox[q], ay_ = ky + oy[q];
         if (ax_ < 0 || ay_ < 0 || ax_ >= lw || ay_ >= lh) continue;
         uint32_t k = (uint32_t)ay_ * (uint32_t)lw + (uint32_t)ax_;
-        float r = rho[k];
+        float r = ld(rho + k);
         if (r < 0.0f) continue;
         weight = weight + wt[q];
         if (r > 0.0f) {
-            ax = ax + wt[q] * px[k];
-            ay = ay + wt[q] * py[k];
+            ax = ax + wt[q] * ld(px + k);
+            ay = ay + wt[q] * ld(py + k);
         }
     }
     const float ww = fmaxf(weight, 1e-6f);
@@ -593,20 +647,21 @@ __device__ __forceinline__ V2 prolongedFrom(const float* rho, const float* px, c
 }
 
 // One cell of prolong (fluid.wgsl:2459-2470), level l from l + 1.
+template <class T = float>
 __device__ void prolongCell(const Dev& D, const FastW& F, uint32_t l, uint32_t j) {
     const int lw = (int)D.level_w[l];
-    const Lvl& V = F.L[l];
-    if (V.rho[j] <= 0.0f) return;
-    const Lvl& U = F.L[l + 1];
+    const LRef<T> V = lref<T>(F, l);
+    if (ld(V.rho + j) <= 0.0f) return;
+    const LRef<T> U = lref<T>(F, l + 1u);
     V2 e = prolongedFrom(U.rho, U.px, U.py, (int)D.level_w[l + 1], (int)D.level_h[l + 1], (int)(j % (uint32_t)lw),
                          (int)(j / (uint32_t)lw));
-    V.px[j] = V.px[j] + e.x;
-    V.py[j] = V.py[j] + e.y;
+    st(V.px + j, ld(V.px + j) + e.x);
+    st(V.py + j, ld(V.py + j) + e.y);
 }
 
 // restrictLevel of level l from level l - 1 (both in the scratch): a thread
 // per coarse cell, 256 cells an item.
-template <bool ONE>
+template <bool ONE, class T>
 __global__ void k_fRestrict(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
@@ -614,12 +669,12 @@ __global__ void k_fRestrict(Batch Bt, const __grid_constant__ WorldSrc<ONE> src,
         FAST_ITEM(Bt, it, D, F, w, chunk);
         if (D.st->cont == 0u) continue;
         const uint32_t j = chunk * blockDim.x + threadIdx.x;
-        if (j < D.level_w[l] * D.level_h[l]) restrictCell(D, F, w, l, j);
+        if (j < D.level_w[l] * D.level_h[l]) restrictCell<T>(D, F, w, l, j);
     }
 }
 
 // smoothAt on level l >= 1, one colour.
-template <bool ONE>
+template <bool ONE, class T>
 __global__ void k_fSmooth(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l, int color) {
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
@@ -627,12 +682,12 @@ __global__ void k_fSmooth(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, u
         FAST_ITEM(Bt, it, D, F, w, chunk);
         if (D.st->cont == 0u) continue;
         const uint32_t j = chunk * blockDim.x + threadIdx.x;
-        if (j < D.level_w[l] * D.level_h[l]) smoothCell(D, F, l, color, D.st->cycle == 0u, j);
+        if (j < D.level_w[l] * D.level_h[l]) smoothCell<T>(D, F, l, color, D.st->cycle == 0u, j);
     }
 }
 
 // prolong of level l from l + 1.
-template <bool ONE>
+template <bool ONE, class T>
 __global__ void k_fProlong(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
@@ -640,7 +695,7 @@ __global__ void k_fProlong(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, 
         FAST_ITEM(Bt, it, D, F, w, chunk);
         if (D.st->cont == 0u) continue;
         const uint32_t j = chunk * blockDim.x + threadIdx.x;
-        if (j < D.level_w[l] * D.level_h[l]) prolongCell(D, F, l, j);
+        if (j < D.level_w[l] * D.level_h[l]) prolongCell<T>(D, F, l, j);
     }
 }
 
@@ -698,6 +753,7 @@ __device__ void slv_smooth(const SLv& V, uint32_t l, int tid, int nt) {
 // The levels lc (restricted already, in the scratch) down to the coarsest and
 // back up to lc, in one CTA's shared memory: smoothRed/Black, restrictLevel,
 // solve (40 SOR sweep pairs, omega 1.8), prolong (fluid.wgsl:2318-2470).
+template <class T = float>
 __device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t lc, float* sm, uint32_t* off) {
     const uint32_t L = D.levels;
     const int tid = (int)threadIdx.x, nt = (int)blockDim.x;
@@ -711,14 +767,14 @@ __device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t 
     __syncthreads();
     {
         const SLv V = slv(sm, off, D, lc);
-        const Lvl& G = F.L[lc];
+        const LRef<T> G = lref<T>(F, lc);
         const int n = V.w * V.h;
         for (int j = tid; j < n; j += nt) {
-            V.px[j] = G.px[j];
-            V.py[j] = G.py[j];
-            V.rx[j] = G.rx[j];
-            V.ry[j] = G.ry[j];
-            V.rho[j] = G.rho[j];
+            V.px[j] = ld(G.px + j);
+            V.py[j] = ld(G.py + j);
+            V.rx[j] = ld(G.rx + j);
+            V.ry[j] = ld(G.ry + j);
+            V.rho[j] = ld(G.rho + j);
         }
         __syncthreads();
     }
@@ -843,16 +899,16 @@ __device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t 
     }
     {
         const SLv V = slv(sm, off, D, lc);
-        const Lvl& G = F.L[lc];
+        const LRef<T> G = lref<T>(F, lc);
         const int n = V.w * V.h;
         for (int j = tid; j < n; j += nt) {
-            G.px[j] = V.px[j];
-            G.py[j] = V.py[j];
+            st(G.px + j, V.px[j]);
+            st(G.py + j, V.py[j]);
         }
     }
 }
 
-template <bool ONE>
+template <bool ONE, class T>
 __global__ void __launch_bounds__(1024) k_fCoarse(Batch Bt, const __grid_constant__ WorldSrc<ONE> src) {
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
@@ -862,13 +918,13 @@ __global__ void __launch_bounds__(1024) k_fCoarse(Batch Bt, const __grid_constan
         FAST_ITEM(Bt, it, D, F, w, unused_);
         (void)unused_;
         if (D.st->cont == 0u) continue;
-        coarseLevels(D, F, w, F.lc, sm, off);
+        coarseLevels<T>(D, F, w, F.lc, sm, off);
         __syncthreads();
     }
 }
 
 // prolongFine (fluid.wgsl:2500-2512), and the rims for the relaxation after.
-template <bool ONE>
+template <bool ONE, class T>
 __global__ void k_fProlongFine(Batch Bt, const __grid_constant__ WorldSrc<ONE> src) {
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
@@ -876,7 +932,7 @@ __global__ void k_fProlongFine(Batch Bt, const __grid_constant__ WorldSrc<ONE> s
         FAST_ITEM(Bt, it, D, F, w, wid);
         if (D.st->cont == 0u) continue;
         const Lvl& L0 = F.L[0];
-        const Lvl& U = F.L[1];
+        const LRef<T> U = lref<T>(F, 1u);
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         uint32_t i = w.cellIndex(c);
@@ -1144,15 +1200,124 @@ __global__ void __launch_bounds__(256) k_fUpdate(Batch Bt, const __grid_constant
                 conv = __uint_as_float(__ldcg(&D.blocks[w.countSlot(COUNT_RESIDUAL + cycle % 3u)])) < LIQUID_TOLERANCE;
             }
             if (threadIdx.x == 0) {
-                const uint32_t cont = (!conv && cycle + 1u < Bt.max_cycles) ? 1u : 0u;
-                D.st->cycle = cycle + 1u;
+                const uint32_t next = cycle + 1u;
+                // the mixed form checks the true residual every 8th iteration
+                // and before it stops (k_fTrueCheck may then go on)
+                const bool check = Bt.mixed != 0u && tol && (conv || (next % 8u) == 0u || next >= Bt.max_cycles);
+                const uint32_t cont = (!conv && next < Bt.max_cycles) ? 1u : 0u;
+                D.st->cycle = next;
                 D.st->cont = cont;
+                D.st->check = check ? 1u : 0u;
                 if (cont) {
                     *Bt.loop = 1u;
                     if (Bt.cond) cudaGraphSetConditional(Bt.cond, 1u);
                 }
             }
         }
+    }
+}
+
+// The true residual -(b + A x) of liquid cell i at c, worked in FP64 from the
+// FP32 solution, and (floor2) the square of the FP32 rounding of A x there:
+// u (|d x| + sum |beta x_n|), u = 2^-24 (the CG's own residual cannot stay
+// below that floor's norm).
+__device__ __forceinline__ double trueResidualAt(const Dev& D, const FastW& F, I2 c, uint32_t i, double* floor2) {
+    const Lvl& L0 = F.L[0];
+    const uint8_t m = F.fmask[i];
+    const float bb[4] = {L0.b0[i], L0.b1[i], L0.b2[i], L0.b3[i]};
+    const double dx = (double)(L0.diag[i] + F.pin[i]) * (double)F.X[i];
+    double ax = dx, mag = fabs(dx);
+#pragma unroll
+    for (int d = 0; d < 4; d++)
+        if (m & (1u << d)) {
+            const double t = (double)bb[d] * (double)F.X[nbr(i, c.x, c.y, D.W, D.H, d)];
+            ax = ax - t;
+            mag = mag + fabs(t);
+        }
+    const double f = mag * 5.9604644775390625e-8;
+    *floor2 = f * f;
+    return -((double)D.field[8u * (size_t)i + 1u] + ax);
+}
+
+// The mixed form's guard, over the worlds k_fUpdate flagged: the FP64 norm
+// of the true residual and of the FP32 rounding floor; when the true one
+// has drifted above twice the recursive one plus four floors (the
+// low-precision preconditioner's rounding lost the recursion's accuracy),
+// the world goes on with the true residual put in (k_fTrueFix), else it
+// stops or goes on as k_fUpdate decided.
+template <bool ONE>
+__global__ void __launch_bounds__(256) k_fTrueCheck(Batch Bt, const __grid_constant__ WorldSrc<ONE> src) {
+    __shared__ WorldCopy wc_;
+    if (!ONE) worldCopyInit(wc_);
+    __shared__ double s64[256], s64b[256];
+    uint32_t pend_ = 0;
+    FOR_ITEMS(Bt, L_ACT4, it) {
+        FAST_ITEM(Bt, it, D, F, w, g);
+        if (D.st->check == 0u) continue;
+        const Lvl& L0 = F.L[0];
+        const uint32_t na = w.activeCount();
+        const uint32_t wid = g * 4u + (threadIdx.x >> 6);
+        const bool valid = wid < na;
+        double r2 = 0.0, f2 = 0.0;
+        if (valid) {
+            I2 c = tileCell(w, wid);
+            if (w.inWorld(c)) {
+                const uint32_t i = w.cellIndex(c);
+                if (L0.rho[i] > 0.0f) {
+                    const double r = trueResidualAt(D, F, c, i, &f2);
+                    r2 = r * r;
+                }
+            }
+        }
+        const double t2 = tree64x4(s64, r2);
+        const double u2 = tree64x4(s64, f2);
+        if (valid && (threadIdx.x & 63u) == 0u) {
+            const uint32_t b = w.blockIndex(w.activeBlock(wid));
+            D.norm64[2u * b] = t2;
+            D.norm64[2u * b + 1u] = u2;
+            __threadfence();
+        }
+        pend_ += min(4u, na - g * 4u);
+        if (flushTiles(Bt, g_it, e_it, it, pend_, &D.st->fdone[4], na)) {
+            double rr, ff;
+            sumBlocks256x2(w, D.norm64, s64, s64b, &rr, &ff);
+            if (threadIdx.x == 0) {
+                const double bn = D.st->bnorm2;
+                const double rel = bn > 0.0 ? sqrt(rr / bn) : 0.0, flo = bn > 0.0 ? sqrt(ff / bn) : 0.0;
+                D.st->rel_true = rel;
+                D.st->check = 0u;
+                if (rel > 2.0 * D.st->rel + 4.0 * flo) {
+                    D.st->drift = 1u;
+                    const uint32_t cont = D.st->cycle < Bt.max_cycles ? 1u : 0u;
+                    D.st->cont = cont;
+                    if (cont) {
+                        *Bt.loop = 1u;
+                        if (Bt.cond) cudaGraphSetConditional(Bt.cond, 1u);
+                    }
+                }
+            }
+        }
+    }
+}
+
+// The true residual put in for the recursive one (CG's r and the
+// smoother's -r), for the worlds k_fTrueCheck found drifted.
+template <bool ONE>
+__global__ void k_fTrueFix(Batch Bt, const __grid_constant__ WorldSrc<ONE> src) {
+    __shared__ WorldCopy wc_;
+    if (!ONE) worldCopyInit(wc_);
+    FOR_ITEMS(Bt, L_ACT, it) {
+        FAST_ITEM(Bt, it, D, F, w, wid);
+        if (D.st->drift == 0u) continue;
+        const Lvl& L0 = F.L[0];
+        I2 c = lidCell(w, wid);
+        if (!w.inWorld(c)) continue;
+        const uint32_t i = w.cellIndex(c);
+        if (L0.rho[i] <= 0.0f) continue;
+        double f2;
+        const float rf = (float)trueResidualAt(D, F, c, i, &f2);
+        F.R[i] = rf;
+        L0.rx[i] = -rf;
     }
 }
 
@@ -1171,6 +1336,7 @@ __global__ void k_fLoopStart(Batch Bt) {
         ITEM_WORLD(Bt, it, D, w, unused_);
         (void)unused_;
         StepState* st = D.st;
+        st->drift = 0u;
         if (st->cycle == 0u) st->cont = 1u;
         if (st->cont == 0u) continue;
         const uint32_t cycle = st->cycle;
@@ -1652,6 +1818,12 @@ void fast_zero_idle(const Batch& Bt, const BatchShape& S, cudaStream_t s) {
         if (one) K<true><<<(grid), (block), (smem), s>>>(Bt, WorldSrc<true>{*one}, ##__VA_ARGS__); \
         else K<false><<<(grid), (block), (smem), s>>>(Bt, WorldSrc<false>{}, ##__VA_ARGS__);       \
     } while (0)
+// The same for a kernel over levels stored as T.
+#define LAUNCH_T(K, T, grid, block, smem, ...)                                                        \
+    do {                                                                                              \
+        if (one) K<true, T><<<(grid), (block), (smem), s>>>(Bt, WorldSrc<true>{*one}, ##__VA_ARGS__);   \
+        else K<false, T><<<(grid), (block), (smem), s>>>(Bt, WorldSrc<false>{}, ##__VA_ARGS__);         \
+    } while (0)
 
 void fast_setup(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m) {
     if (m) m->fn(m->ctx, WIG_SLOT_F_SETUP, 0);
@@ -1659,7 +1831,8 @@ void fast_setup(const Batch& Bt, const BatchShape& S, const World* one, cudaStre
     if (m) m->fn(m->ctx, WIG_SLOT_F_SETUP, 1);
 }
 
-uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m) {
+template <class T>
+uint32_t fast_cycle_t(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m) {
     const unsigned G = list_grid(S, L_ACT, 32), G4 = list_grid(S, L_ACT4, 8);
     const unsigned GR = (S.max_items[L_RELAX] + 3u) / 4u < 148u * 16u ? std::max((S.max_items[L_RELAX] + 3u) / 4u, 1u)
                                                                       : 148u * 16u;
@@ -1679,33 +1852,33 @@ uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, const World* one, cuda
     // those above lc, then its levels from lc are the coarse kernel's
     for (uint32_t l = 1; l <= S.lc_max; l++) {
         mark(WIG_SLOT_F_RESTRICT, 0);
-        LAUNCH(k_fRestrict, cells(L_RES + l - 1u), 256, 0, l);
+        LAUNCH_T(k_fRestrict, T, cells(L_RES + l - 1u), 256, 0, l);
         mark(WIG_SLOT_F_RESTRICT, 1);
         if (S.max_items[L_SM + l - 1u] == 0u) continue;
         mark(WIG_SLOT_F_SMOOTH, 0);
-        LAUNCH(k_fSmooth, cells(L_SM + l - 1u), 256, 0, l, 0);
+        LAUNCH_T(k_fSmooth, T, cells(L_SM + l - 1u), 256, 0, l, 0);
         mark(WIG_SLOT_F_SMOOTH, 1);
         mark(WIG_SLOT_F_SMOOTH, 0);
-        LAUNCH(k_fSmooth, cells(L_SM + l - 1u), 256, 0, l, 1);
+        LAUNCH_T(k_fSmooth, T, cells(L_SM + l - 1u), 256, 0, l, 1);
         mark(WIG_SLOT_F_SMOOTH, 1);
     }
     mark(WIG_SLOT_F_COARSE, 0);
-    LAUNCH(k_fCoarse, list_grid(S, L_ONE, 1), 1024, S.coarse_smem);
+    LAUNCH_T(k_fCoarse, T, list_grid(S, L_ONE, 1), 1024, S.coarse_smem);
     mark(WIG_SLOT_F_COARSE, 1);
     for (uint32_t l = S.lc_max; l >= 1; l--) {
         if (S.max_items[L_SM + l - 1u] == 0u) continue;
         mark(WIG_SLOT_F_PROLONG, 0);
-        LAUNCH(k_fProlong, cells(L_SM + l - 1u), 256, 0, l);
+        LAUNCH_T(k_fProlong, T, cells(L_SM + l - 1u), 256, 0, l);
         mark(WIG_SLOT_F_PROLONG, 1);
         mark(WIG_SLOT_F_SMOOTH, 0);
-        LAUNCH(k_fSmooth, cells(L_SM + l - 1u), 256, 0, l, 0);
+        LAUNCH_T(k_fSmooth, T, cells(L_SM + l - 1u), 256, 0, l, 0);
         mark(WIG_SLOT_F_SMOOTH, 1);
         mark(WIG_SLOT_F_SMOOTH, 0);
-        LAUNCH(k_fSmooth, cells(L_SM + l - 1u), 256, 0, l, 1);
+        LAUNCH_T(k_fSmooth, T, cells(L_SM + l - 1u), 256, 0, l, 1);
         mark(WIG_SLOT_F_SMOOTH, 1);
     }
     mark(WIG_SLOT_F_PROLONG_FINE, 0);
-    LAUNCH(k_fProlongFine, G, 64, 0);
+    LAUNCH_T(k_fProlongFine, T, G, 64, 0);
     mark(WIG_SLOT_F_PROLONG_FINE, 1);
     mark(WIG_SLOT_F_RELAX, 0);
     LAUNCH(k_fRelax, GR, 128, 0, 1);
@@ -1722,7 +1895,19 @@ uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, const World* one, cuda
     mark(WIG_SLOT_F_UPDATE, 0);
     LAUNCH(k_fUpdate, G4, 256, 0);
     mark(WIG_SLOT_F_UPDATE, 1);
+    if (Bt.mixed) {
+        mark(WIG_SLOT_F_UPDATE, 0);
+        LAUNCH(k_fTrueCheck, G4, 256, 0);
+        mark(WIG_SLOT_F_UPDATE, 1);
+        mark(WIG_SLOT_F_UPDATE, 0);
+        LAUNCH(k_fTrueFix, G, 64, 0);
+        mark(WIG_SLOT_F_UPDATE, 1);
+    }
     return launches;
+}
+
+uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m) {
+    return Bt.mixed ? fast_cycle_t<__half>(Bt, S, one, s, m) : fast_cycle_t<float>(Bt, S, one, s, m);
 }
 
 void fast_finish(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m) {
@@ -1732,9 +1917,12 @@ void fast_finish(const Batch& Bt, const BatchShape& S, const World* one, cudaStr
 }
 
 cudaError_t fast_prepare_attributes(size_t smem) {
-    cudaError_t e = cudaFuncSetAttribute(k_fCoarse<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(k_fCoarse<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const int b = (int)smem;
+    cudaError_t e = cudaFuncSetAttribute(k_fCoarse<true, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fCoarse<false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fCoarse<true, __half>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fCoarse<false, __half>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    return e;
 }
 
 size_t fast_solve_smem(const Fast& F) { return fast_coarse_smem(F.D, F.lp); }

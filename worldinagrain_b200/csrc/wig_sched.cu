@@ -113,7 +113,10 @@ __global__ void __launch_bounds__(256) k_schedFill(Batch Bt, SchedCtl c, int pha
             st->rz = 0.0; st->pq = 0.0; st->alpha = 0.0; st->beta = 0.0;
             st->cycle = 0u;
             st->cont = 0u;
-            for (int f = 0; f < 4; f++) st->fdone[f] = 0u;
+            for (int f = 0; f < 6; f++) st->fdone[f] = 0u;
+            st->check = 0u;
+            st->drift = 0u;
+            st->rel_true = 0.0;
             st->rz32 = 0.0f; st->pq32 = 0.0f; st->alpha32 = 0.0f; st->beta32 = 0.0f;
             st->bar_count = 0u;
             st->bar_gen = 0u;
