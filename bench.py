@@ -225,11 +225,16 @@ def run_batched(args, rank, world_size, local_rank, dist, torch):
     uneven sizes (multi_worlds) resident together, every step one
     wig_batch_step of all of them (each pass one launch over all the
     worlds), solved to the same 1e-6 relative residual."""
-    from worldinagrain_b200 import fluid
+    from worldinagrain_b200 import fluid, shard
     import ctypes as C
-    worlds = W.multi_worlds(n=args.worlds, seed=args.seed)
+    # N ranks: N times the worlds, each rank its cell-balanced share (weak
+    # scaling, no collective on the data path)
+    n_all = args.worlds * world_size
+    specs = W.multi_world_specs(n=n_all, seed=args.seed)
+    all_cells = [s_[0] * s_[0] for s_ in specs]
+    mine = shard.share_of(all_cells, rank, world_size)
+    worlds = W.multi_worlds(n=n_all, seed=args.seed, only=mine)
     n = len(worlds)
-    cells = sum(w.C for w in worlds)
     stream = torch.cuda.Stream()
     b = fluid.Batch(worlds, W.element_table())
     ids = (C.c_uint32 * n)(*range(n))
@@ -265,7 +270,7 @@ def run_batched(args, rank, world_size, local_rank, dist, torch):
         t = torch.tensor([ms], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
-    value = cells * args.steps * world_size / (ms / 1e3) / 1e6
+    value = sum(all_cells) * args.steps / (ms / 1e3) / 1e6
     st = b.stats(range(n))
     launches_per_step = st[0].launches
 
@@ -285,7 +290,7 @@ def run_batched(args, rank, world_size, local_rank, dist, torch):
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
-    e2e = cells * args.steps * world_size / e2e_s / 1e6
+    e2e = sum(all_cells) * args.steps / e2e_s / 1e6
     h2d = 8 + ((4 * n + 7) // 8) * 8 + 136 * n
     d2h = 64 * n
 
@@ -335,7 +340,8 @@ def run_batched(args, rank, world_size, local_rank, dist, torch):
             "metric": METRIC, "value": round(value, 3), "unit": "Mcells/s", "n_gpus": world_size,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": f"multi_worlds_{n}", "worlds": n, "cells": cells,
+            "config": {"workload": f"multi_worlds_{args.worlds}_per_gpu", "worlds": n_all, "cells": sum(all_cells),
+                       "worlds_on_rank0": n, "sharding": "cell-balanced greedy partition, no data-path collective",
                        "sides": f"log-uniform {sides[0]}..{sides[-1]}, median {sides[n // 2]}", "seed": args.seed,
                        "liquid_per_cell": 4, "tolerance": TOL, "max_cycles": MAX_CYCLES,
                        "form": "batched fast form: one launch a pass over all worlds, CG loop in a graph WHILE node",
@@ -362,9 +368,15 @@ def run_served(args, rank, world_size, local_rank, dist, torch):
     under a device-memory budget into two-lane continuously batched steps
     (lane pools lend each step its per-step memory); p50/p99 latency and
     Mcells/s per rate, beside the same stream served one world a launch."""
-    from worldinagrain_b200 import serve
+    from worldinagrain_b200 import serve, shard
     t0 = time.perf_counter()
-    worlds = W.multi_worlds(n=args.worlds, lo=64, hi=1024, seed=args.seed)
+    # N ranks: N times the worlds, each rank serving its cell-balanced share
+    # and the requests for it (weak scaling; the ranks share only the
+    # latencies, gathered on the host for the percentiles)
+    n_all = args.worlds * world_size
+    specs = W.multi_world_specs(n=n_all, lo=64, hi=1024, seed=args.seed)
+    mine = shard.share_of([s_[0] * s_[0] for s_ in specs], rank, world_size)
+    worlds = W.multi_worlds(n=n_all, lo=64, hi=1024, seed=args.seed, only=mine)
     t_build = time.perf_counter() - t0
     cells_of = [w.C for w in worlds]
     budget = int(args.budget_gb * 1e9)
@@ -381,9 +393,14 @@ def run_served(args, rank, world_size, local_rank, dist, torch):
     with Clocks(gpu_index_of(torch, local_rank)) as clk:
         for rate in rates:
             n_req = int(min(max(rate * args.serve_seconds, 500), args.serve_max_requests))
-            done = srv.run(serve.poisson_arrivals(rate, n_req, len(worlds), seed=args.seed + int(rate)))
-            pt = serve.latency_summary(done, lambda k: cells_of[k])
-            pt["rate"] = rate
+            done = srv.run(serve.poisson_arrivals(rate, n_req, len(worlds), seed=args.seed + int(rate) + 7919 * rank))
+            part = serve.latency_part(done, lambda k: cells_of[k])
+            parts = [part]
+            if dist:
+                parts = [None] * world_size
+                dist.all_gather_object(parts, part)
+            pt = serve.merge_parts(parts)
+            pt["rate"] = rate * world_size
             points.append(pt)
     # the one-world-at-a-time baseline (same kernels, one world a launch) at the lowest rate
     one = serve.Server(be, len(worlds), budget - 2 * pool, one_at_a_time=True)
@@ -391,8 +408,13 @@ def run_served(args, rank, world_size, local_rank, dist, torch):
     rate0 = rates[0]
     arr = serve.poisson_arrivals(rate0, int(min(max(rate0 * args.serve_seconds, 300), 1500)), len(worlds),
                                  seed=args.seed + 7)
-    base = serve.latency_summary(one.run(arr), lambda k: cells_of[k])
-    base["rate"] = rate0
+    part = serve.latency_part(one.run(arr), lambda k: cells_of[k])
+    parts = [part]
+    if dist:
+        parts = [None] * world_size
+        dist.all_gather_object(parts, part)
+    base = serve.merge_parts(parts)
+    base["rate"] = rate0 * world_size
     be.close()
     best = max(points, key=lambda p: p["mcells_per_s"])
     if rank == 0:
@@ -401,7 +423,8 @@ def run_served(args, rank, world_size, local_rank, dist, torch):
             "n_gpus": world_size, "steps": sum(p["requests"] for p in points), "warmup": 200,
             "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": f"served_{len(worlds)}_worlds", "worlds": len(worlds), "cells": sum(cells_of),
+            "config": {"workload": f"served_{args.worlds}_worlds_per_gpu", "worlds": n_all,
+                       "cells": sum(s_[0] * s_[0] for s_ in specs), "worlds_on_rank0": len(worlds),
                        "sides": "log-uniform 64..1024", "budget_gb": args.budget_gb, "lane_pool_gb": args.pool_gb,
                        "resident_worlds": resident, "resident_gb": round(srv.resident_bytes / 1e9, 2),
                        "build_s": round(t_build, 1), "preload_s": round(t_preload, 1), "tolerance": TOL,

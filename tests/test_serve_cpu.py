@@ -131,3 +131,13 @@ def test_eviction_is_least_recently_used():
     assert list(srv.resident) == [0, 1, 2]
     srv.run([(0.0, 1), (0.01, 0), (0.02, 3)])
     assert [ev[1] for ev in be.log if ev[0] == "evict"] == [2]
+
+
+def test_merge_parts_pools_latencies_and_sums_throughput():
+    a = {"lat_ms": [1.0, 2.0, 3.0], "swapped": [False] * 3, "cells": 300, "t0": 0.0, "t1": 1.0}
+    b = {"lat_ms": [10.0], "swapped": [True], "cells": 100, "t0": 0.5, "t1": 1.0}
+    m = serve.merge_parts([a, b])
+    assert m["requests"] == 4
+    assert m["p50_ms"] == 2.5
+    assert m["mcells_per_s"] == round((300 / 1.0 + 100 / 0.5) / 1e6, 3)
+    assert m["swapped_requests"] == 1 and m["p50_ms_resident"] == 2.0

@@ -359,3 +359,36 @@ def latency_summary(finished, cells_of):
         out["p50_ms_resident"] = round(float(np.percentile(lat[hit], 50)), 3)
         out["p99_ms_resident"] = round(float(np.percentile(lat[hit], 99)), 3)
     return out
+
+
+def latency_part(finished, cells_of):
+    """One rank's raw results, for merge_parts on rank 0: latencies (ms),
+    swapped flags, cells stepped, and the run's first arrival and last
+    completion (the ranks' clocks start together at a barrier)."""
+    return {
+        "lat_ms": [(r.t_done - r.t_arrival) * 1e3 for r in finished],
+        "swapped": [bool(r.swapped) for r in finished],
+        "cells": int(sum(cells_of(r.world) for r in finished)),
+        "t0": min(r.t_arrival for r in finished),
+        "t1": max(r.t_done for r in finished),
+    }
+
+
+def merge_parts(parts):
+    """latency_summary over several ranks' latency_part results: the
+    percentiles of all requests, the throughput summed over the ranks."""
+    lat = np.concatenate([np.asarray(p["lat_ms"]) for p in parts])
+    hit = ~np.concatenate([np.asarray(p["swapped"], dtype=bool) for p in parts])
+    out = {
+        "requests": int(lat.size),
+        "p50_ms": round(float(np.percentile(lat, 50)), 3),
+        "p99_ms": round(float(np.percentile(lat, 99)), 3),
+        "mean_ms": round(float(lat.mean()), 3),
+        "mcells_per_s": round(sum(p["cells"] / max(p["t1"] - p["t0"], 1e-9) for p in parts) / 1e6, 3),
+        "steps_per_s": round(sum(len(p["lat_ms"]) / max(p["t1"] - p["t0"], 1e-9) for p in parts), 1),
+        "swapped_requests": int((~hit).sum()),
+    }
+    if hit.any() and not hit.all():
+        out["p50_ms_resident"] = round(float(np.percentile(lat[hit], 50)), 3)
+        out["p99_ms_resident"] = round(float(np.percentile(lat[hit], 99)), 3)
+    return out

@@ -232,14 +232,10 @@ def obstacle_column(width=2048, height=2048, p_solid=0.03, fill=0.7, ppc=2, seed
     return w
 
 
-def multi_worlds(n=512, lo=64, hi=512, seed=4, ppc=4):
-    """Batched multi-world config: n independent square worlds, sides
-    log-uniform in [lo, hi] rounded to a multiple of 16, each a dam break
-    (WATER against the left wall, about 1.5 times as high as wide) or a
-    column (the bottom rows, full width), fluid fraction U(0.2, 0.7) of the
-    inside, at rest, ppc particles per fluid cell, one-cell WALL border.  The
-    particle buffers are sized to the liquid (1.25 times its particles), not
-    to the whole grid."""
+def multi_world_specs(n=512, lo=64, hi=512, seed=4, ppc=4):
+    """The shapes multi_worlds draws, without building the worlds: per world
+    (side, kind, fluid fraction, fluid block width and height, particle
+    capacity)."""
     rng = np.random.default_rng(seed)
     out = []
     for k in range(n):
@@ -253,6 +249,22 @@ def multi_worlds(n=512, lo=64, hi=512, seed=4, ppc=4):
         else:
             fw, fh = inner, min(inner, int(round(f * inner)))
         cap = int(np.ceil(fw * fh * ppc * 1.25)) + 256
+        out.append((s, kind, float(f), fw, fh, cap))
+    return out
+
+
+def multi_worlds(n=512, lo=64, hi=512, seed=4, ppc=4, only=None):
+    """Batched multi-world config: n independent square worlds, sides
+    log-uniform in [lo, hi] rounded to a multiple of 16, each a dam break
+    (WATER against the left wall, about 1.5 times as high as wide) or a
+    column (the bottom rows, full width), fluid fraction U(0.2, 0.7) of the
+    inside, at rest, ppc particles per fluid cell, one-cell WALL border.  The
+    particle buffers are sized to the liquid (1.25 times its particles), not
+    to the whole grid.  `only`: build just these of the n worlds."""
+    specs = multi_world_specs(n, lo, hi, seed, ppc)
+    out = []
+    for k in (range(n) if only is None else only):
+        s, kind, f, fw, fh, cap = specs[k]
         w = World(s, s, ppc, cap)
         wall = np.zeros((s, s), dtype=bool)
         wall[0, :] = wall[-1, :] = True
@@ -261,8 +273,7 @@ def multi_worlds(n=512, lo=64, hi=512, seed=4, ppc=4):
         water = np.zeros((s, s), dtype=bool)
         water[s - 1 - fh:s - 1, 1:1 + fw] = True
         w.paint(water, abi.WATER)
-        w.config = dict(workload=f"multi_{kind}", grid=f"{s}x{s}", seed=seed, earth_g=earth_g_cells(), fill=float(f),
-                        index=k)
+        w.config = dict(workload=f"multi_{kind}", grid=f"{s}x{s}", seed=seed, earth_g=earth_g_cells(), fill=f, index=k)
         out.append(w)
     return out
 
