@@ -4,18 +4,26 @@ Workload: the single world at scale — a 1024 x 1024 MAC grid with 200 WALL
 disks (radii U[4, 24], centres uniform under the seed), WATER in the top half
 at 4 particles per cell with Gaussian cell velocities (sigma 0.5 cells/step),
 Earth's pull at dt 1/120 — stepped by the CUDA liquid step with the pressure
-solved to a 1e-6 relative residual (||r||2/||b||2, FP64 norms).
+solved to a 1e-6 relative residual (||r||2/||b||2 of the CG residual, FP64
+norms).
 
 A step is one liquid step (encodeFluid's whole pass sequence).  `value` is
 grid cells x steps / device time (CUDA events on the launch stream, the
 world resident in HBM, 0.7 GB: larger than L2, so no flush is needed);
 `e2e` is the same through the public API with every step's Params copied
-host->device from pinned memory and the step's report read back.
+host->device from pinned memory and the step's report read back, stepped
+from the same saved state over the same trajectory.  A one-GPU run adds
+`forms`: the batched workload (512 worlds of 64..512, every pass one launch
+over all of them) and the served one (2000 resident worlds of 64..1024
+under a 120 GB budget, Poisson requests, p50/p99 latency beside one world
+a launch); --workload batched|served runs either alone.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--form fast|plain|persistent|mixed] [--workload single|batched|served]
 
-With N > 1 (torchrun) every rank steps its own replica of the world (the
-path does not shard: replicas only), timed as the max over ranks.
+With N > 1 (torchrun) every rank steps its own replica of the single world
+(it does not shard: replicas only), or its cell-balanced share of N times
+the batched or served worlds; timed as the max over ranks.
 """
 import argparse
 import json
@@ -122,9 +130,56 @@ def params(world, step, seed):
 # Algorithmic bytes of one launch of each pass: the words the reference
 # layout makes it read and write once (per active cell, fluid cell, face or
 # particle), counted from the world after the step.  Active cells are the
-# active blocks' 64 each.
+# active blocks' 64 each.  The fast form's level kernels: per launch on a
+# level of n cells, smoothing one colour 32 n (the colour's cells read their
+# density, four coefficients, diagonal, potentials and right-hand sides and
+# write their potentials, the other colour's potentials read once),
+# restriction 180 n (the four finer cells' ten arrays, the five of the
+# coarse cell written), prolongation 23 n, the one-CTA coarse kernel 28 n on
+# its first level; averaged over the launches of an iteration (s["levels"]:
+# per level, its cells summed over the worlds and whether it is smoothed,
+# restricted by itself, or the coarse kernel's first).
+def level_bytes(name, s):
+    L = s.get("levels")
+    if not L:
+        return None
+    sm = [n for n, kind in L if kind == "smooth"]
+    rs = [n for n, kind in L if kind in ("smooth", "restrict")]
+    co = [n for n, kind in L if kind == "restrict"]
+    if name == "F_SMOOTH" and sm:
+        return sum(32 * n for n in sm) // len(sm)
+    if name == "F_RESTRICT" and rs:
+        return sum(180 * n for n in rs) // len(rs)
+    if name == "F_PROLONG" and sm:
+        return sum(23 * n for n in sm) // len(sm)
+    if name == "F_COARSE" and co:
+        return sum(28 * n for n in co)
+    return None
+
+
+def level_stats(worlds):
+    """Per level index: (cells over the worlds, what the fast form does there)."""
+    from collections import defaultdict
+    cells, kind = defaultdict(int), {}
+    for w in worlds:
+        lv = w.L["levels"]
+        lc = next((i + 1 for i, (a, b) in enumerate(lv) if a * b <= 4096), len(lv))
+        for i, (a, b) in enumerate(lv):
+            l = i + 1
+            if l < lc:
+                cells[l] += a * b
+                kind[l] = "smooth"
+            elif l == lc:
+                cells[l] += a * b
+                kind.setdefault(l, "restrict")
+    return [(cells[l], kind[l]) for l in sorted(cells)]
+
+
 def algorithmic_bytes(name, s):
     A, Cf, N = s["active_cells"], s["fluid_cells"], s["particles"]
+    lb = level_bytes(name, s)
+    if lb is not None:
+        return lb
     table = {
         # 10x10 tile of (field cell z, x; drift x; rim x2; share) in, pot out
         "RELAX": A * (16 + 4 + 8 + 4 + 4) + Cf * (8 + 8),
@@ -159,7 +214,8 @@ def world_stats(world):
     B = world.L["block_count"]
     active = int(blocks[4 * B + abi.COUNT_ACTIVE])
     rho = world.field_cells()[:, 0, 2]
-    return {"active_cells": active * 64, "fluid_cells": int(np.sum(rho > 0)), "particles": int(world.sorted[0])}
+    return {"active_cells": active * 64, "fluid_cells": int(np.sum(rho > 0)), "particles": int(world.sorted[0]),
+            "levels": level_stats([world])}
 
 
 def cpu_baseline(world, args, budget_s):
@@ -220,7 +276,7 @@ def gpu_index_of(torch, local_rank):
     return gpu_index
 
 
-def run_batched(args, rank, world_size, local_rank, dist, torch):
+def run_batched(args, rank, world_size, local_rank, dist, torch, emit=True):
     """The batched multi-world workload: args.worlds independent worlds of
     uneven sizes (multi_worlds) resident together, every step one
     wig_batch_step of all of them (each pass one launch over all the
@@ -310,6 +366,7 @@ def run_batched(args, rank, world_size, local_rank, dist, torch):
         ws["active_cells"] += int(w.blocks[4 * B + abi.COUNT_ACTIVE]) * 64
         ws["fluid_cells"] += int(np.sum(w.field_cells()[:, 0, 2] > 0))
     ws["particles"] = int(sum(x.particles for x in b.stats(range(n))))
+    ws["levels"] = level_stats(worlds)
     total = sum(v[0] for v in prof.values())
     ranked = sorted(prof.items(), key=lambda kv: -kv[1][0])
     top = next((k for k, _ in ranked if algorithmic_bytes(k, ws) is not None), ranked[0][0])
@@ -359,10 +416,12 @@ def run_batched(args, rank, world_size, local_rank, dist, torch):
             "profile_ms_per_step": {k: round(v[0] / args.profile_steps, 4) for k, v in ranked[:12]},
             "profile_share": {k: round(v[0] / total, 4) for k, v in ranked[:12]},
         }
-        print(json.dumps(line), flush=True)
+        if emit:
+            print(json.dumps(line), flush=True)
+        return line
 
 
-def run_served(args, rank, world_size, local_rank, dist, torch):
+def run_served(args, rank, world_size, local_rank, dist, torch, emit=True):
     """The served stream: args.worlds resident worlds (sides log-uniform
     64..1024), Poisson step requests at each rate of args.rates, admitted
     under a device-memory budget into two-lane continuously batched steps
@@ -433,7 +492,9 @@ def run_served(args, rank, world_size, local_rank, dist, torch):
             "one_at_a_time": base,
             "clocks": clk.summary(),
         }
-        print(json.dumps(line), flush=True)
+        if emit:
+            print(json.dumps(line), flush=True)
+        return line
 
 
 def config_of(world, args):
@@ -464,6 +525,8 @@ def main():
     ap.add_argument("--pool-gb", type=float, default=7.0)
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--serve-max-requests", type=int, default=4000)
+    ap.add_argument("--no-forms", action="store_true",
+                    help="the single world alone, without the batched and served summaries a one-GPU run adds")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     global FLAGS
@@ -503,12 +566,22 @@ def main():
     world = make_world(args)
     stream = torch.cuda.Stream()
     g = fluid.LiquidStep(world, W.element_table(), stream=stream.cuda_stream)
+
+    def flags_of(step):
+        # the tiling parity fixed by the step's number, so a trajectory
+        # replayed from a saved state repeats itself
+        return FLAGS | abi.STEP_SHIFTED_SET | (abi.STEP_SHIFTED_FIRST if step % 2 else 0)
+
     step_no = 0
     for _ in range(args.warmup):
         step_no += 1
-        g.step(params(world, step_no, args.seed), max_cycles=MAX_CYCLES, flags=FLAGS, tolerance=TOL)
+        g.step(params(world, step_no, args.seed), max_cycles=MAX_CYCLES, flags=flags_of(step_no), tolerance=TOL)
     g.stats()
     torch.cuda.synchronize()
+    # the state after warm-up: the device-timed and the end-to-end runs both
+    # step from it, over the same trajectory
+    saved = g.download(world.copy())
+    step_saved = step_no
 
     # ---- device-timed region: K steps, the world resident
     def barrier():
@@ -523,7 +596,7 @@ def main():
             e0.record(stream)
         for _ in range(args.steps):
             step_no += 1
-            g.step(params(world, step_no, args.seed), max_cycles=MAX_CYCLES, flags=FLAGS, tolerance=TOL)
+            g.step(params(world, step_no, args.seed), max_cycles=MAX_CYCLES, flags=flags_of(step_no), tolerance=TOL)
         with torch.cuda.stream(stream):
             e1.record(stream)
         barrier()
@@ -537,13 +610,16 @@ def main():
     cells = world.C
     value = cells * args.steps * world_size / (ms / 1e3) / 1e6
 
-    # ---- end to end through the public API: params in, report out, every step
+    # ---- end to end through the public API: params in, report out, every
+    # step, from the same saved state
+    g.upload(saved)
+    step_no = step_saved
     cycles = []
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         step_no += 1
-        g.step(params(world, step_no, args.seed), max_cycles=MAX_CYCLES, flags=FLAGS, tolerance=TOL)
+        g.step(params(world, step_no, args.seed), max_cycles=MAX_CYCLES, flags=flags_of(step_no), tolerance=TOL)
         s2 = g.stats()
         cycles.append(s2.cycles)
         if s2.rel_residual > TOL:
@@ -599,10 +675,36 @@ def main():
             "profile_ms_per_step": {k: round(v[0] / args.profile_steps, 4) for k, v in ranked[:12]},
             "profile_share": {k: round(v[0] / total, 4) for k, v in ranked[:12]},
         }
-        print(json.dumps(line), flush=True)
     g.close()
+    if rank == 0 and world_size == 1 and not args.no_forms:
+        line["forms"] = run_forms(args, rank, world_size, local_rank, dist, torch)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
+
+
+def run_forms(args, rank, world_size, local_rank, dist, torch):
+    """The one-GPU run's summaries of the batched and served forms, beside
+    the single world: each its own workload (run_batched, run_served), made
+    smaller in steps and rates so the whole run stays within minutes."""
+    import argparse as ap_
+    out = {}
+    b = ap_.Namespace(**vars(args))
+    b.worlds, b.steps, b.warmup, b.no_cpu, b.profile_steps = 512, 10, 3, True, 1
+    s = ap_.Namespace(**vars(args))
+    s.worlds, s.rates, s.no_cpu = 2000, "1000,2000,20000", True
+    for name, fn, a in (("batched", run_batched, b), ("served", run_served, s)):
+        try:
+            ln = fn(a, rank, world_size, local_rank, dist, torch, emit=False)
+            keep = ("value", "unit", "ms_per_step", "e2e", "config", "roofline", "solve", "served", "one_at_a_time",
+                    "gpu_launches", "clocks")
+            out[name] = {k: ln[k] for k in keep if k in ln}
+        except Exception as e:  # a form that cannot run here is reported, not fatal
+            out[name] = {"error": f"{type(e).__name__}: {e}"}
+        torch.cuda.synchronize()
+        torch.cuda.empty_cache()
+    return out
 
 
 if __name__ == "__main__":
