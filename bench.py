@@ -130,15 +130,15 @@ def params(world, step, seed):
 # Algorithmic bytes of one launch of each pass: the words the reference
 # layout makes it read and write once (per active cell, fluid cell, face or
 # particle), counted from the world after the step.  Active cells are the
-# active blocks' 64 each.  The fast form's level kernels: per launch on a
-# level of n cells, smoothing one colour 32 n (the colour's cells read their
-# density, four coefficients, diagonal, potentials and right-hand sides and
-# write their potentials, the other colour's potentials read once),
-# restriction 180 n (the four finer cells' ten arrays, the five of the
-# coarse cell written), prolongation 23 n, the one-CTA coarse kernel 28 n on
-# its first level; averaged over the launches of an iteration (s["levels"]:
-# per level, its cells summed over the worlds and whether it is smoothed,
-# restricted by itself, or the coarse kernel's first).
+# active blocks' 64 each.  The fast form's level kernels, per launch on a
+# level of n cells: down (restriction, then both colours of smoothing on
+# chip) 180 n (the four finer cells' ten arrays read, the coarse cell's
+# five written); up (prolongation, then both colours) 51 n (the level's ten
+# arrays read, its potentials written, the coarser level's density and
+# potentials read); the one-CTA coarse kernel 28 n on its first level.
+# Averaged over the launches of an iteration (s["levels"]: per level, its
+# cells summed over the worlds and whether it is smoothed, restricted by
+# itself, or the coarse kernel's first).
 def level_bytes(name, s):
     L = s.get("levels")
     if not L:
@@ -146,12 +146,10 @@ def level_bytes(name, s):
     sm = [n for n, kind in L if kind == "smooth"]
     rs = [n for n, kind in L if kind in ("smooth", "restrict")]
     co = [n for n, kind in L if kind == "restrict"]
-    if name == "F_SMOOTH" and sm:
-        return sum(32 * n for n in sm) // len(sm)
     if name == "F_RESTRICT" and rs:
         return sum(180 * n for n in rs) // len(rs)
     if name == "F_PROLONG" and sm:
-        return sum(23 * n for n in sm) // len(sm)
+        return sum(51 * n for n in sm) // len(sm)
     if name == "F_COARSE" and co:
         return sum(28 * n for n in co)
     return None
@@ -331,17 +329,19 @@ def run_batched(args, rank, world_size, local_rank, dist, torch, emit=True):
     launches_per_step = st[0].launches
 
     # end to end: every step's inputs in, every world's report out
-    cycles, worst = [], 0.0
+    cycles, worst, worst_k = [], 0.0, -1
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         step()
         sts = b.stats(range(n))
         cycles.append(max(x.cycles for x in sts))
-        worst = max(worst, max(x.rel_residual for x in sts))
+        k = max(range(n), key=lambda i: sts[i].rel_residual)
+        if sts[k].rel_residual > worst:
+            worst, worst_k = sts[k].rel_residual, k
     e2e_s = time.perf_counter() - t0
     if worst > TOL:
-        raise SystemExit(f"a world's solve left {worst:.3e} > {TOL}")
+        raise SystemExit(f"world {mine[worst_k]} (side {worlds[worst_k].W}) left {worst:.3e} > {TOL}")
     if dist:
         t = torch.tensor([e2e_s], device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MAX)

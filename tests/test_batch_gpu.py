@@ -163,3 +163,53 @@ def test_batch_refuses_bad_lists():
     with pytest.raises(fluid.WigError):
         b.step([0], P[:1], flags=abi.STEP_PLAIN)
     b.close()
+
+
+def test_batch_of_multi_level_worlds_matches_alone():
+    """Worlds of the batched set whose levels go through the per-level
+    tile kernels (sides 176 to 512: one to three levels above the coarse
+    kernel's) beside one that has none: each the same as stepped alone,
+    converged."""
+    from worldinagrain_b200 import fluid
+    picked = [2, 25, 9, 120, 135]  # sides 96, 176, 272, 400, 512
+    worlds = W.multi_worlds(n=512, seed=2, only=picked)
+    ref = [_alone(w, 3, 0, TOL) for w in worlds]
+    mine = [w.copy() for w in worlds]
+    b = fluid.Batch(mine, W.element_table())
+    ids = list(range(len(mine)))
+    for s in range(1, 4):
+        b.step(ids, [params(w, s) for w in mine], max_cycles=64, flags=TOL, tolerance=1e-6)
+    st = b.stats(ids)
+    for k, w in enumerate(mine):
+        b.download(k)
+        d = _same(w, ref[k][0])
+        assert not d, f"world {picked[k]}: {d}"
+        assert st[k].cycles == ref[k][1].cycles
+        assert st[k].rel_residual <= 1e-6, (picked[k], st[k].rel_residual)
+    b.close()
+
+
+def test_many_world_batch_is_deterministic():
+    """96 worlds of the batched set (many tiles a CTA in each level kernel):
+    two batches stepped alike leave the same buffers and stats, so no kernel
+    reads a cell that another CTA of the same launch writes."""
+    from worldinagrain_b200 import fluid
+    picked = list(range(96))
+    runs = []
+    for _ in range(2):
+        mine = W.multi_worlds(n=512, seed=2, only=picked)
+        b = fluid.Batch(mine, W.element_table())
+        ids = list(range(len(mine)))
+        for s in range(1, 4):
+            b.step(ids, [params(w, s) for w in mine], max_cycles=64, flags=TOL, tolerance=1e-6)
+        st = b.stats(ids)
+        for k in ids:
+            b.download(k)
+        b.close()
+        runs.append((mine, [(x.cycles, x.rel_residual, tuple(x.count)) for x in st]))
+    (wa, sa), (wb, sb) = runs
+    for k in range(len(picked)):
+        assert sa[k] == sb[k], (picked[k], sa[k], sb[k])
+        assert sa[k][1] <= 1e-6, (picked[k], sa[k][1])
+        d = _same(wa[k], wb[k])
+        assert not d, f"world {picked[k]}: {d}"

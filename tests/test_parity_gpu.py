@@ -278,3 +278,27 @@ def test_two_liquids_with_viscosity(form):
         assert not diffs, f"step {s}: " + "; ".join(diffs)
         assert sg.count[abi.COUNT_VISCOUS] == so.count[abi.COUNT_VISCOUS] == 1
     g.close()
+
+
+@pytest.mark.parametrize("k", [9, 120])  # sides 272 and 400 of the batched set, dam breaks
+def test_fast_form_matches_oracle_on_batched_set_worlds(k):
+    """Worlds of the batched set whose first two levels go through the tile
+    kernels, the second with partial tiles at its edge: three steps of the
+    1e-6 form against the oracle."""
+    fluid = _gpu()
+    world = W.multi_worlds(n=512, seed=2, only=[k])[0]
+    ref = world.copy()
+    o = _oracle(ref)
+    g = fluid.LiquidStep(world, W.element_table())
+    got = world.copy()
+    flags = abi.STEP_TOLERANCE | abi.STEP_F64_DOTS
+    for s in range(1, 4):
+        P = params(ref, s)
+        so = o.step(P, max_cycles=64, flags=flags, tolerance=1e-6)
+        g.step(P, max_cycles=64, flags=flags, tolerance=1e-6)
+        sg = g.stats()
+        g.download(got)
+        diffs = compare_worlds(got, ref, scratch=True)
+        assert not diffs, f"step {s}: " + "; ".join(diffs)
+        assert sg.cycles == so.cycles
+    g.close()

@@ -252,7 +252,7 @@ size_t scratch_bytes(const wig::Dev& D) {
     const size_t C = D.C;
     size_t bytes = align256(C) + 17u * align256(C * 4u);
     for (uint32_t l = 1; l <= D.levels; l++) {
-        bytes += 10u * align256((size_t)D.level_w[l] * D.level_h[l] * 4u);
+        bytes += 12u * align256((size_t)D.level_w[l] * D.level_h[l] * 4u);
         bytes += align256(5u * (size_t)D.level_w[l] * D.level_h[l] * 2u);  // the binary16 operator
     }
     bytes += align256(2u * (size_t)D.B * 4u) + 3u * align256(2u * (size_t)D.B * 8u);
@@ -272,6 +272,8 @@ void scratch_take(wig::World& Wd, char* p) {
         wig::Lvl& V = F.L[l];
         V.px = fl(n); V.py = fl(n); V.rx = fl(n); V.ry = fl(n); V.rho = fl(n);
         V.b0 = fl(n); V.b1 = fl(n); V.b2 = fl(n); V.b3 = fl(n); V.diag = fl(n);
+        V.ux = l == 0 ? nullptr : fl(n);
+        V.uy = l == 0 ? nullptr : fl(n);
     }
     F.H[0] = wig::LvlH{nullptr, 0u, 0u};
     for (uint32_t l = 1; l <= D.levels; l++) {
@@ -411,7 +413,7 @@ int make_batch(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, u
         max_items[wig::L_ONE_ALL] += 1;
         max_items[wig::L_ONE] += 1;
         for (uint32_t l = 1; l <= WIG_MG_LEVELS; l++) {
-            const uint64_t ch = cdiv((uint64_t)D.level_w[l] * D.level_h[l], 256);
+            const uint64_t ch = l <= D.levels ? wig::levelTiles(D.level_w[l], D.level_h[l]) : 0u;
             if (l <= lc && l <= D.levels) max_items[wig::L_RES + l - 1] += ch;
             if (l < lc) max_items[wig::L_SM + l - 1] += ch;
             if (l <= D.levels) most_units = std::max<uint64_t>(most_units, ch);
@@ -435,7 +437,7 @@ int make_batch(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, u
         items_total += max_items[l];
     }
     if (items_total > 0xffffffffull) return bail(WIG_E_ARG, "work lists too long");
-    if (S.coarse_smem > 200u * 1024u) return bail(WIG_E_ARG, "coarse levels too large for one CTA");
+    if (S.coarse_smem > 220u * 1024u) return bail(WIG_E_ARG, "coarse levels too large for one CTA");
     if (wig::fast_prepare_attributes(S.coarse_smem) != cudaSuccess) return bail(WIG_E_CUDA, "cudaFuncSetAttribute");
 
     // device memory: elements, step states, reports, world table, scratch

@@ -354,6 +354,7 @@ __device__ __forceinline__ float fineBeta(float a, float b, float da, float db) 
 struct Lvl {
     float *px, *py, *rx, *ry, *rho;
     float *b0, *b1, *b2, *b3, *diag;
+    float *ux, *uy;  // levels >= 1: the potentials after the V-cycle's way up (the way down's stay in px, py)
 };
 
 // A coarse level's operator in binary16 (the mixed-precision form): its
@@ -389,6 +390,11 @@ static_assert(sizeof(World) % 16 == 0, "World copies in 16-byte words");
 // Work lists.  A kernel's CTAs take the items of one list in turn (grid
 // stride); an item is a world of the batch (its index in the world table, the
 // high bits) and a unit of that world's work (the low Batch::lbits bits):
+// The 16x16 tiles of a w x h level: the units of the level lists.
+__host__ __device__ __forceinline__ uint32_t levelTiles(uint32_t w, uint32_t h) {
+    return ((w + 15u) / 16u) * ((h + 15u) / 16u);
+}
+
 enum List : uint32_t {
     L_WB = 0,     // every 8x8 block of the world (sync, syncSeed)
     L_PS,         // 256 particles of `sorted` (syncParticles)
@@ -399,8 +405,8 @@ enum List : uint32_t {
     L_RELAX,      // a relaxation tile: the active blocks, then the shifted tiling's edge tiles
     L_ONE_ALL,    // the world (per-world single-CTA work: compact, report)
     L_ONE,        // the world when it runs the full step (scanTotals, the coarse levels, ...)
-    L_RES,        // + l - 1: 256 cells of level l when the fast form restricts it by itself (l <= lc)
-    L_SM = L_RES + WIG_MG_LEVELS,  // + l - 1: 256 cells of level l below the coarse kernel's (l < lc)
+    L_RES,        // + l - 1: 16x16 tiles of level l when the fast form restricts it by itself (l <= lc)
+    L_SM = L_RES + WIG_MG_LEVELS,  // + l - 1: 16x16 tiles of level l below the coarse kernel's (l < lc)
     L_COUNT = L_SM + WIG_MG_LEVELS
 };
 

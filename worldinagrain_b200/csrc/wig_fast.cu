@@ -72,6 +72,28 @@ __device__ __forceinline__ T tree64x4(T* s, T v) {
     return r;
 }
 
+// The same trees of 64 in two halves, one barrier between them: tilePut,
+// in the upper warp of each tile, leaves its 32 values in s (128 entries);
+// after a barrier, tileSum, in the lower warp, adds them (the tree's first
+// step, lane + 32) and finishes the tree by shuffles (lane + h, h = 16 ..
+// 1): the same additions in the same order.  The tile's sum is in its
+// thread 0.  A kernel alternates two buffers between items, so one item's
+// sums and the next item's puts never share one.
+template <class T>
+__device__ __forceinline__ void tilePut(T* s, T v) {
+    const uint32_t lane = threadIdx.x & 63u;
+    if (lane >= 32u) s[((threadIdx.x >> 6) << 5) + (lane - 32u)] = v;
+}
+template <class T>
+__device__ __forceinline__ T tileSum(const T* s, T v) {
+    if ((threadIdx.x & 32u) == 0u) {  // a whole warp: the tile's lower
+        v = v + s[((threadIdx.x >> 6) << 5) + (threadIdx.x & 31u)];
+#pragma unroll
+        for (int h = 16; h > 0; h >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, h);
+    }
+    return v;
+}
+
 // sumBlocks (fluid.wgsl:2645-2661) by a 256-thread CTA, component comp of 2
 // of the active blocks' partials: thread li adds the partials of blocks li,
 // li + 256, ... in that order (loaded ahead in coalesced batches of 16, the
@@ -97,10 +119,17 @@ __device__ T sumBlocks256(const W& w, const T* part, int comp, T* s) {
     }
     s[li] = acc;
     __syncthreads();
-    for (int h = 128; h > 0; h >>= 1) {
+    for (int h = 128; h > 32; h >>= 1) {
         if ((int)li < h) s[li] = s[li] + s[li + h];
         __syncthreads();
     }
+    if (li < 32u) {
+        T v = s[li] + s[li + 32u];
+#pragma unroll
+        for (int h = 16; h > 0; h >>= 1) v = v + __shfl_down_sync(0xffffffffu, v, h);
+        if (li == 0u) s[0] = v;
+    }
+    __syncthreads();
     T r = s[0];
     __syncthreads();
     return r;
@@ -134,13 +163,26 @@ __device__ void sumBlocks256x2(const W& w, const T* part, T* s0, T* s1, T* out0,
     s0[li] = a0;
     s1[li] = a1;
     __syncthreads();
-    for (int h = 128; h > 0; h >>= 1) {
+    for (int h = 128; h > 32; h >>= 1) {
         if ((int)li < h) {
             s0[li] = s0[li] + s0[li + h];
             s1[li] = s1[li] + s1[li + h];
         }
         __syncthreads();
     }
+    if (li < 32u) {
+        T v0 = s0[li] + s0[li + 32u], v1 = s1[li] + s1[li + 32u];
+#pragma unroll
+        for (int h = 16; h > 0; h >>= 1) {
+            v0 = v0 + __shfl_down_sync(0xffffffffu, v0, h);
+            v1 = v1 + __shfl_down_sync(0xffffffffu, v1, h);
+        }
+        if (li == 0u) {
+            s0[0] = v0;
+            s1[0] = v1;
+        }
+    }
+    __syncthreads();
     *out0 = s0[0];
     *out1 = s1[0];
     __syncthreads();
@@ -527,18 +569,19 @@ __device__ __forceinline__ V2 residualStored(const LRef<T>& V, const float* pin,
     return V2{ld(V.rx + k) - (sx - (dg + pinx) * ld(V.px + k)) / h2, ld(V.ry + k) - (sy - (dg + 0.0f) * ld(V.py + k)) / h2};
 }
 
-// One coarse cell of restrictLevel (fluid.wgsl:2342-2377), level l (stored
-// as TV) from l - 1 (stored as TU).
-template <class TU, class TV>
-__device__ void restrictCellT(const Dev& D, const FastW& F, const W& w, uint32_t l, uint32_t j) {
-    const int lw = (int)D.level_w[l];
-    const int cx = (int)(j % (uint32_t)lw), cy = (int)(j / (uint32_t)lw);
-    const LRef<TV> V = lref<TV>(F, l);
+// restrictLevel's values of level-l cell (cx, cy) from level l - 1, stored
+// as TU (fluid.wgsl:2342-2377): the density and, with `res`, the restricted
+// residuals; all 0 in a block not worked on.
+template <class TU>
+__device__ __forceinline__ void restrictedAt(const Dev& D, const FastW& F, const W& w, uint32_t l, int cx, int cy,
+                                             bool res, float& rho_o, float& rx_o, float& ry_o) {
     const int span = 1 << l;
     if (span <= BLOCK) {
         I2 b{cx * span / BLOCK, cy * span / BLOCK};
         if (w.inBlocks(b) && (D.blocks[w.stateSlot(w.blockIndex(b))] & ACTIVE) == 0u) {
-            st(V.px + j, 0.0f); st(V.py + j, 0.0f); st(V.rx + j, 0.0f); st(V.ry + j, 0.0f); st(V.rho + j, 0.0f);
+            rho_o = 0.0f;
+            rx_o = 0.0f;
+            ry_o = 0.0f;
             return;
         }
     }
@@ -557,16 +600,31 @@ __device__ void restrictCellT(const Dev& D, const FastW& F, const W& w, uint32_t
         else if (rho > 0.0f) {
             fluid = fluid + 1.0f;
             sum = sum + rho;
-            V2 r = residualStored(U, pin, k, kx, ky, uw, uh, h2);
-            rx = rx + r.x;
-            ry = ry + r.y;
+            if (res) {
+                V2 r = residualStored(U, pin, k, kx, ky, uw, uh, h2);
+                rx = rx + r.x;
+                ry = ry + r.y;
+            }
         }
     }
     const float rho = air ? 0.0f : (fluid > 0.0f ? sum / fluid : -1.0f);
+    rho_o = rho;
+    rx_o = rho > 0.0f ? rx * 0.25f : 0.0f;
+    ry_o = rho > 0.0f ? ry * 0.25f : 0.0f;
+}
+
+// One coarse cell of restrictLevel, level l (stored as TV) from l - 1
+// (stored as TU): the cell's values, its potentials zeroed.
+template <class TU, class TV>
+__device__ void restrictCellT(const Dev& D, const FastW& F, const W& w, uint32_t l, uint32_t j) {
+    const int lw = (int)D.level_w[l];
+    const LRef<TV> V = lref<TV>(F, l);
+    float rho, rx, ry;
+    restrictedAt<TU>(D, F, w, l, (int)(j % (uint32_t)lw), (int)(j / (uint32_t)lw), true, rho, rx, ry);
     st(V.px + j, 0.0f);
     st(V.py + j, 0.0f);
-    st(V.rx + j, rho > 0.0f ? rx * 0.25f : 0.0f);
-    st(V.ry + j, rho > 0.0f ? ry * 0.25f : 0.0f);
+    st(V.rx + j, rx);
+    st(V.ry + j, ry);
     st(V.rho + j, rho);
 }
 // Level l from l - 1 with the levels stored as T (level 0 always f32).
@@ -659,93 +717,301 @@ __device__ void prolongCell(const Dev& D, const FastW& F, uint32_t l, uint32_t j
     st(V.py + j, ld(V.py + j) + e.y);
 }
 
-// restrictLevel of level l from level l - 1 (both in the scratch): a thread
-// per coarse cell, 256 cells an item.
+// ---------------------------------------------------------------- level tiles
+//
+// The levels above the coarse kernel's, a 16x16 tile of level l a 256-thread
+// CTA, each pass of one level in one kernel: on the way down the tile's
+// restriction and both colours of smoothing, on the way up its
+// prolongation and both colours.  A tile works a ring of 2 cells around
+// itself again (its neighbours' work, the same arithmetic on the same
+// inputs, so the same bits): the red sweep on the ring of 1 reads the ring
+// of 2, the black sweep on the tile reads the ring of 1.  Shared-memory
+// arrays are 20 x 20, tile cell (0, 0) at (2, 2).
+
+constexpr int LT = 16, LR = LT + 4, LRR = LR * LR;
+
+__device__ __forceinline__ int lsi(int ix, int iy) { return (iy + 2) * LR + (ix + 2); }
+
+// The shared index of neighbour d of tile cell (ix, iy) at level cell
+// (cx, cy): clamped onto the cell past the level's edge, as nbr.
+__device__ __forceinline__ int lsn(int ix, int iy, int cx, int cy, int lw, int lh, int d) {
+    if (!nbrIn(cx, cy, lw, lh, d)) return lsi(ix, iy);
+    switch (d) {
+    case 0: return lsi(ix - 1, iy);
+    case 1: return lsi(ix + 1, iy);
+    case 2: return lsi(ix, iy - 1);
+    default: return lsi(ix, iy + 1);
+    }
+}
+
+// A value as a level of T stores it and reads it back.
+__device__ __forceinline__ float asStored(float v, float) { return v; }
+__device__ __forceinline__ float asStored(float v, __half) { return __half2float(__float2half_rn(v)); }
+
+struct LevelTile {
+    float rho[LRR], px[LRR], py[LRR], rx[LRR], ry[LRR], b[4][LRR], dg[LRR];
+};
+
+// One colour's sweep of smoothAt (fluid.wgsl:2318-2334) over tile cell
+// (ix, iy) held in the tile's arrays.
+__device__ __forceinline__ void tileSweepCell(LevelTile& t, int ix, int iy, int cx, int cy, int lw, int lh, float h2) {
+    const int i = lsi(ix, iy);
+    if (t.rho[i] <= 0.0f) return;
+    const float dg = t.dg[i];
+    if (dg <= 0.0f) return;
+    float sx = 0.0f, sy = 0.0f;
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+        const int n = lsn(ix, iy, cx, cy, lw, lh, d);
+        sx = sx + t.b[d][i] * t.px[n];
+        sy = sy + t.b[d][i] * t.py[n];
+    }
+    t.px[i] = mixf(t.px[i], (sx - h2 * t.rx[i]) / dg, SMOOTH_OMEGA);
+    t.py[i] = mixf(t.py[i], (sy - h2 * t.ry[i]) / dg, SMOOTH_OMEGA);
+}
+
+// The red sweep over the tile's ring of 1, the black over the tile itself.
+__device__ __forceinline__ void tileSmooth(LevelTile& t, int x0, int y0, int lw, int lh, float h2) {
+    for (int k = (int)threadIdx.x; k < (LT + 2) * (LT + 2); k += (int)blockDim.x) {
+        const int ix = k % (LT + 2) - 1, iy = k / (LT + 2) - 1, cx = x0 + ix, cy = y0 + iy;
+        if (cx < 0 || cy < 0 || cx >= lw || cy >= lh || ((cx + cy) & 1) != 0) continue;
+        tileSweepCell(t, ix, iy, cx, cy, lw, lh, h2);
+    }
+    __syncthreads();
+    const int ix = (int)threadIdx.x % LT, iy = (int)threadIdx.x / LT, cx = x0 + ix, cy = y0 + iy;
+    if (cx < lw && cy < lh && ((cx + cy) & 1) == 1) tileSweepCell(t, ix, iy, cx, cy, lw, lh, h2);
+}
+
+// Down, level l: restrictLevel, then smoothRed and smoothBlack when the
+// world smooths level l (l < its coarse kernel's first level; else the
+// restriction alone).  The coefficients of each liquid cell of the ring of 1
+// from the densities (as the step's first iteration works and stores them,
+// and later ones read them back), stored by the tile's own cells on the
+// first iteration.
 template <bool ONE, class T>
-__global__ void k_fRestrict(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
+__global__ void __launch_bounds__(256, ONE ? 3 : 2) k_fDown(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
+    __shared__ LevelTile t;
     FOR_ITEMS(Bt, L_RES + l - 1u, it) {
-        FAST_ITEM(Bt, it, D, F, w, chunk);
+        FAST_ITEM(Bt, it, D, F, w, tile);
         if (D.st->cont == 0u) continue;
-        const uint32_t j = chunk * blockDim.x + threadIdx.x;
-        if (j < D.level_w[l] * D.level_h[l]) restrictCell<T>(D, F, w, l, j);
+        const int lw = (int)D.level_w[l], lh = (int)D.level_h[l], tw = (lw + LT - 1) / LT;
+        const int x0 = (int)(tile % (uint32_t)tw) * LT, y0 = (int)(tile / (uint32_t)tw) * LT;
+        if (l >= F.lc) {
+            const int cx = x0 + (int)threadIdx.x % LT, cy = y0 + (int)threadIdx.x / LT;
+            if (cx < lw && cy < lh) restrictCell<T>(D, F, w, l, (uint32_t)(cy * lw + cx));
+            continue;
+        }
+        const LRef<T> V = lref<T>(F, l);
+        const bool first = D.st->cycle == 0u;
+        for (int k = (int)threadIdx.x; k < LRR; k += (int)blockDim.x) {
+            const int ix = k % LR - 2, iy = k / LR - 2, cx = x0 + ix, cy = y0 + iy;
+            float rho = -1.0f, rx = 0.0f, ry = 0.0f;
+            if (cx >= 0 && cy >= 0 && cx < lw && cy < lh) {
+                const bool res = ix >= -1 && iy >= -1 && ix <= LT && iy <= LT;
+                if (l == 1u) restrictedAt<float>(D, F, w, l, cx, cy, res, rho, rx, ry);
+                else restrictedAt<T>(D, F, w, l, cx, cy, res, rho, rx, ry);
+            }
+            t.rho[k] = asStored(rho, T());
+            t.rx[k] = rx;
+            t.ry[k] = ry;
+            t.px[k] = 0.0f;
+            t.py[k] = 0.0f;
+        }
+        __syncthreads();
+        for (int k = (int)threadIdx.x; k < (LT + 2) * (LT + 2); k += (int)blockDim.x) {
+            const int ix = k % (LT + 2) - 1, iy = k / (LT + 2) - 1, cx = x0 + ix, cy = y0 + iy;
+            if (cx < 0 || cy < 0 || cx >= lw || cy >= lh) continue;
+            const int i = lsi(ix, iy);
+            const float rho = t.rho[i];
+            if (rho <= 0.0f) continue;
+            float b[4];
+            float dg = 0.0f;
+#pragma unroll
+            for (int d = 0; d < 4; d++) {
+                b[d] = 0.0f;
+                if (!nbrIn(cx, cy, lw, lh, d)) continue;
+                const float r = t.rho[lsn(ix, iy, cx, cy, lw, lh, d)];
+                if (r < 0.0f) continue;
+                b[d] = faceBeta(rho, r);
+                dg = dg + b[d];
+            }
+            const bool own = ix >= 0 && iy >= 0 && ix < LT && iy < LT;
+            if (first && own) {
+                const uint32_t j = (uint32_t)(cy * lw + cx);
+                st(V.b0 + j, b[0]); st(V.b1 + j, b[1]); st(V.b2 + j, b[2]); st(V.b3 + j, b[3]);
+                if (V.diag) st(V.diag + j, dg);
+            }
+#pragma unroll
+            for (int d = 0; d < 4; d++) t.b[d][i] = asStored(b[d], T());
+            // the diagonal as diagAt reads it: stored in f32, the rounded
+            // coefficients' sum in binary16
+            t.dg[i] = V.diag ? dg : ((t.b[0][i] + t.b[1][i]) + t.b[2][i]) + t.b[3][i];
+        }
+        __syncthreads();
+        tileSmooth(t, x0, y0, lw, lh, (float)(1u << (2u * l)));
+        {
+            const int ix = (int)threadIdx.x % LT, iy = (int)threadIdx.x / LT, cx = x0 + ix, cy = y0 + iy;
+            if (cx < lw && cy < lh) {
+                const uint32_t j = (uint32_t)(cy * lw + cx);
+                const int i = lsi(ix, iy);
+                st(V.px + j, t.px[i]);
+                st(V.py + j, t.py[i]);
+                st(V.rx + j, t.rx[i]);
+                st(V.ry + j, t.ry[i]);
+                st(V.rho + j, t.rho[i]);
+            }
+        }
+        __syncthreads();  // the tile's arrays are free for the next item
     }
 }
 
-// smoothAt on level l >= 1, one colour.
+// Up, level l (< the coarse kernel's first): prolong from level l + 1
+// (fluid.wgsl:2459-2497), then smoothRed and smoothBlack with the stored
+// coefficients.  The way down's potentials are read from px, py (the ring
+// too) and the results go to ux, uy, so no CTA reads a cell that another
+// writes in the same launch; level l + 1's results are its ux, uy.
 template <bool ONE, class T>
-__global__ void k_fSmooth(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l, int color) {
+__global__ void __launch_bounds__(256, ONE ? 3 : 2) k_fUp(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
+    __shared__ LevelTile t;
     FOR_ITEMS(Bt, L_SM + l - 1u, it) {
-        FAST_ITEM(Bt, it, D, F, w, chunk);
+        FAST_ITEM(Bt, it, D, F, w, tile);
         if (D.st->cont == 0u) continue;
-        const uint32_t j = chunk * blockDim.x + threadIdx.x;
-        if (j < D.level_w[l] * D.level_h[l]) smoothCell<T>(D, F, l, color, D.st->cycle == 0u, j);
-    }
-}
-
-// prolong of level l from l + 1.
-template <bool ONE, class T>
-__global__ void k_fProlong(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
-    __shared__ WorldCopy wc_;
-    if (!ONE) worldCopyInit(wc_);
-    FOR_ITEMS(Bt, L_SM + l - 1u, it) {
-        FAST_ITEM(Bt, it, D, F, w, chunk);
-        if (D.st->cont == 0u) continue;
-        const uint32_t j = chunk * blockDim.x + threadIdx.x;
-        if (j < D.level_w[l] * D.level_h[l]) prolongCell<T>(D, F, l, j);
+        const int lw = (int)D.level_w[l], lh = (int)D.level_h[l], tw = (lw + LT - 1) / LT;
+        const int x0 = (int)(tile % (uint32_t)tw) * LT, y0 = (int)(tile / (uint32_t)tw) * LT;
+        const LRef<T> V = lref<T>(F, l);
+        const T* urho = lref<T>(F, l + 1u).rho;
+        const Lvl& Lu = F.L[l + 1u];
+        const int uw = (int)D.level_w[l + 1], uh = (int)D.level_h[l + 1];
+        for (int k = (int)threadIdx.x; k < LRR; k += (int)blockDim.x) {
+            const int ix = k % LR - 2, iy = k / LR - 2, cx = x0 + ix, cy = y0 + iy;
+            float rho = -1.0f, px = 0.0f, py = 0.0f;
+            if (cx >= 0 && cy >= 0 && cx < lw && cy < lh) {
+                const uint32_t j = (uint32_t)(cy * lw + cx);
+                rho = ld(V.rho + j);
+                px = ld(V.px + j);
+                py = ld(V.py + j);
+                if (rho > 0.0f) {
+                    const V2 e = prolongedFrom(urho, Lu.ux, Lu.uy, uw, uh, cx, cy);
+                    px = px + e.x;
+                    py = py + e.y;
+                    if (ix >= -1 && iy >= -1 && ix <= LT && iy <= LT) {
+                        t.rx[k] = ld(V.rx + j);
+                        t.ry[k] = ld(V.ry + j);
+                        t.b[0][k] = ld(V.b0 + j);
+                        t.b[1][k] = ld(V.b1 + j);
+                        t.b[2][k] = ld(V.b2 + j);
+                        t.b[3][k] = ld(V.b3 + j);
+                        t.dg[k] = diagAt(V, j);
+                    }
+                }
+            }
+            t.rho[k] = rho;
+            t.px[k] = px;
+            t.py[k] = py;
+        }
+        __syncthreads();
+        tileSmooth(t, x0, y0, lw, lh, (float)(1u << (2u * l)));
+        {
+            const int ix = (int)threadIdx.x % LT, iy = (int)threadIdx.x / LT, cx = x0 + ix, cy = y0 + iy;
+            const int i = lsi(ix, iy);
+            if (cx < lw && cy < lh && t.rho[i] > 0.0f) {
+                const uint32_t j = (uint32_t)(cy * lw + cx);
+                F.L[l].ux[j] = t.px[i];
+                F.L[l].uy[j] = t.py[i];
+            }
+        }
+        __syncthreads();
     }
 }
 
 // Named barrier over the first `count` threads (a multiple of 32).
 __device__ __forceinline__ void barSub(uint32_t count) { asm volatile("bar.sync 1, %0;" ::"r"(count) : "memory"); }
 
-// Level l (lc <= l <= levels) of the one-CTA kernel's shared memory: five
-// arrays of the level's cells from sm + off[l].
+// Level l (lc <= l <= levels) of the one-CTA kernel's shared memory: nine
+// arrays of the level's cells from sm + off[l]: the potentials, the
+// right-hand sides, the densities and the four face coefficients.
+constexpr uint32_t SLV_ARRAYS = 9;
 struct SLv {
-    float *px, *py, *rx, *ry, *rho;
+    float *px, *py, *rx, *ry, *rho, *b0, *b1, *b2, *b3;
     int w, h;
 };
 __device__ __forceinline__ SLv slv(float* sm, const uint32_t* off, const Dev& D, uint32_t l) {
     const int n = (int)(D.level_w[l] * D.level_h[l]);
     float* p = sm + off[l];
-    return SLv{p, p + n, p + 2 * n, p + 3 * n, p + 4 * n, (int)D.level_w[l], (int)D.level_h[l]};
+    return SLv{p,         p + n,     p + 2 * n, p + 3 * n, p + 4 * n, p + 5 * n,
+               p + 6 * n, p + 7 * n, p + 8 * n, (int)D.level_w[l], (int)D.level_h[l]};
 }
 
-__device__ __forceinline__ void slv_stencil(const SLv& V, int j, int cx, int cy, float rho, float* sx, float* sy, float* dg) {
-    float ax = 0.0f, ay = 0.0f, d0 = 0.0f;
-    for (int d = 0; d < 4; d++) {
-        if (!nbrIn(cx, cy, V.w, V.h, d)) continue;
-        uint32_t n = nbr((uint32_t)j, cx, cy, V.w, V.h, d);
-        float r = V.rho[n];
-        if (r < 0.0f) continue;
-        float beta = faceBeta(rho, r);
-        ax = ax + beta * V.px[n];
-        ay = ay + beta * V.py[n];
-        d0 = d0 + beta;
+// The face coefficients of level V's cells (smoothAt's stencil,
+// fluid.wgsl:2318-2334): faceBeta to each neighbour inside the level whose
+// density is not negative, else 0; all 0 for a cell that is not liquid.
+__device__ void slv_coefficients(const SLv& V, int tid, int nt) {
+    const int n = V.w * V.h;
+    for (int j = tid; j < n; j += nt) {
+        const int cx = j % V.w, cy = j / V.w;
+        const float rho = V.rho[j];
+        float b[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        if (rho > 0.0f) {
+#pragma unroll
+            for (int d = 0; d < 4; d++) {
+                if (!nbrIn(cx, cy, V.w, V.h, d)) continue;
+                const float r = V.rho[nbr((uint32_t)j, cx, cy, V.w, V.h, d)];
+                if (r >= 0.0f) b[d] = faceBeta(rho, r);
+            }
+        }
+        V.b0[j] = b[0];
+        V.b1[j] = b[1];
+        V.b2[j] = b[2];
+        V.b3[j] = b[3];
     }
-    *sx = ax;
-    *sy = ay;
-    *dg = d0;
+}
+
+// The stencil's sums at liquid cell j from the stored coefficients: the
+// sums of the neighbours taken in order, each beta times the neighbour's
+// potential, and the betas' sum.  A neighbour the stencil skips has beta 0
+// and its index clamped onto j, so adding its term changes no bit.
+__device__ __forceinline__ void slv_stencil(const SLv& V, int j, int cx, int cy, float* sx, float* sy, float* dg) {
+    const float b0 = V.b0[j], b1 = V.b1[j], b2 = V.b2[j], b3 = V.b3[j];
+    const uint32_t n0 = nbr((uint32_t)j, cx, cy, V.w, V.h, 0), n1 = nbr((uint32_t)j, cx, cy, V.w, V.h, 1);
+    const uint32_t n2 = nbr((uint32_t)j, cx, cy, V.w, V.h, 2), n3 = nbr((uint32_t)j, cx, cy, V.w, V.h, 3);
+    *sx = (((0.0f + b0 * V.px[n0]) + b1 * V.px[n1]) + b2 * V.px[n2]) + b3 * V.px[n3];
+    *sy = (((0.0f + b0 * V.py[n0]) + b1 * V.py[n1]) + b2 * V.py[n2]) + b3 * V.py[n3];
+    *dg = (((0.0f + b0) + b1) + b2) + b3;
+}
+
+// One sweep of one colour over level V (smoothRed/Black, fluid.wgsl:2318-
+// 2334, or the solve's SOR sweeps with omega): a thread per cell of that
+// colour.  Of the cells 2k and 2k + 1 exactly one has each colour (in a row,
+// or across a row's end when the width is odd), so pair k gives the cell.
+__device__ void slv_sweep(const SLv& V, uint32_t l, int color, float omega, int tid, int nt) {
+    const int n = V.w * V.h, pairs = (n + 1) / 2;
+    const float h2 = (float)(1u << (2u * l));
+    for (int k = tid; k < pairs; k += nt) {
+        int j = 2 * k, cx = j % V.w, cy = j / V.w;
+        if (((cx + cy) & 1) != color) {
+            j++;
+            if (++cx == V.w) {
+                cx = 0;
+                cy++;
+            }
+        }
+        if (j >= n) continue;
+        if (V.rho[j] <= 0.0f) continue;
+        float sx, sy, dg;
+        slv_stencil(V, j, cx, cy, &sx, &sy, &dg);
+        if (dg <= 0.0f) continue;
+        V.px[j] = mixf(V.px[j], (sx - h2 * V.rx[j]) / dg, omega);
+        V.py[j] = mixf(V.py[j], (sy - h2 * V.ry[j]) / dg, omega);
+    }
 }
 
 __device__ void slv_smooth(const SLv& V, uint32_t l, int tid, int nt) {
-    const int n = V.w * V.h;
-    const float h2 = (float)(1u << (2u * l));
     for (int color = 0; color < 2; color++) {
-        for (int j = tid; j < n; j += nt) {
-            const int cx = j % V.w, cy = j / V.w;
-            if (((cx + cy) & 1) != color) continue;
-            const float rho = V.rho[j];
-            if (rho <= 0.0f) continue;
-            float sx, sy, dg;
-            slv_stencil(V, j, cx, cy, rho, &sx, &sy, &dg);
-            if (dg <= 0.0f) continue;
-            V.px[j] = mixf(V.px[j], (sx - h2 * V.rx[j]) / dg, 1.0f);
-            V.py[j] = mixf(V.py[j], (sy - h2 * V.ry[j]) / dg, 1.0f);
-        }
+        slv_sweep(V, l, color, SMOOTH_OMEGA, tid, nt);
         __syncthreads();
     }
 }
@@ -753,15 +1019,20 @@ __device__ void slv_smooth(const SLv& V, uint32_t l, int tid, int nt) {
 // The levels lc (restricted already, in the scratch) down to the coarsest and
 // back up to lc, in one CTA's shared memory: smoothRed/Black, restrictLevel,
 // solve (40 SOR sweep pairs, omega 1.8), prolong (fluid.wgsl:2318-2470).
+// Each level's face coefficients are worked out once, when its densities
+// are in place, and read by its sweeps and by the restriction below it.
+// Level lc's results go to its ux, uy (`up`, the fast form) or back into its
+// px, py (the persistent form).
 template <class T = float>
-__device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t lc, float* sm, uint32_t* off) {
+__device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t lc, float* sm, uint32_t* off,
+                             bool up) {
     const uint32_t L = D.levels;
     const int tid = (int)threadIdx.x, nt = (int)blockDim.x;
     if (tid == 0) {
         uint32_t o = 0;
         for (uint32_t l = lc; l <= L; l++) {
             off[l] = o;
-            o += 5u * D.level_w[l] * D.level_h[l];
+            o += SLV_ARRAYS * D.level_w[l] * D.level_h[l];
         }
     }
     __syncthreads();
@@ -784,7 +1055,9 @@ __device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t 
         if (l > lc) {
             const SLv U = slv(sm, off, D, l - 1u);
             const int span = 1 << l;
-            const float h2u = (float)(1u << (2u * (l - 1u)));
+            // 1 / h^2 of level l - 1: a power of two, so the product is the
+            // quotient's bits
+            const float inv_h2u = 1.0f / (float)(1u << (2u * (l - 1u)));
             for (int j = tid; j < n; j += nt) {
                 const int cx = j % V.w, cy = j / V.w;
                 if (span <= BLOCK) {
@@ -804,11 +1077,11 @@ __device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t 
                     if (rho == 0.0f) air = true;
                     else if (rho > 0.0f) {
                         float sx, sy, dg;
-                        slv_stencil(U, k, kx, ky, rho, &sx, &sy, &dg);
+                        slv_stencil(U, k, kx, ky, &sx, &sy, &dg);
                         fluid = fluid + 1.0f;
                         sum = sum + rho;
-                        rx = rx + (U.rx[k] - (sx - (dg + 0.0f) * U.px[k]) / h2u);
-                        ry = ry + (U.ry[k] - (sy - (dg + 0.0f) * U.py[k]) / h2u);
+                        rx = rx + (U.rx[k] - (sx - (dg + 0.0f) * U.px[k]) * inv_h2u);
+                        ry = ry + (U.ry[k] - (sy - (dg + 0.0f) * U.py[k]) * inv_h2u);
                     }
                 }
                 const float rho = air ? 0.0f : (fluid > 0.0f ? sum / fluid : -1.0f);
@@ -820,13 +1093,15 @@ __device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t 
             }
             __syncthreads();
         }
+        slv_coefficients(V, tid, nt);
+        __syncthreads();
         if (l < L) slv_smooth(V, l, tid, nt);
     }
     // solve: the coarsest level.  When its cells fit the CTA, a cell a thread
     // of the first warps, the coefficients held in registers across the
     // sweeps and only those warps synchronised (a named barrier over nsolve
-    // <= blockDim threads); else several cells a thread, the CTA
-    // synchronised.
+    // <= blockDim threads); else a thread per cell of the swept colour, the
+    // CTA synchronised.
     {
         const SLv V = slv(sm, off, D, L);
         const int n = min(V.w * V.h, (int)WIG_MG_COARSEST);
@@ -843,14 +1118,9 @@ __device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t 
                     r0 = V.rho[j];
                     hx = h2 * V.rx[j];
                     hy = h2 * V.ry[j];
-                    for (int d = 0; d < 4; d++) {
-                        nb[d] = nbr((uint32_t)j, cx, cy, V.w, V.h, d);
-                        if (!nbrIn(cx, cy, V.w, V.h, d)) continue;
-                        float r = V.rho[nb[d]];
-                        if (r < 0.0f) continue;
-                        b[d] = faceBeta(r0, r);
-                        dg = dg + b[d];
-                    }
+                    b[0] = V.b0[j]; b[1] = V.b1[j]; b[2] = V.b2[j]; b[3] = V.b3[j];
+                    for (int d = 0; d < 4; d++) nb[d] = nbr((uint32_t)j, cx, cy, V.w, V.h, d);
+                    dg = (((0.0f + b[0]) + b[1]) + b[2]) + b[3];
                 }
                 const bool mine = j < n && r0 > 0.0f && dg > 0.0f;
                 const int color = (cx + cy) & 1;
@@ -868,17 +1138,7 @@ __device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t 
             }
         } else {
             for (int s = 0; s < 2 * COARSE_SWEEPS; s++) {
-                for (int j = tid; j < n; j += nt) {
-                    const int cx = j % V.w, cy = j / V.w;
-                    const float r0 = V.rho[j];
-                    if (((cx + cy) & 1) != (s & 1) || r0 <= 0.0f) continue;
-                    float sx, sy, dg;
-                    slv_stencil(V, j, cx, cy, r0, &sx, &sy, &dg);
-                    if (dg > 0.0f) {
-                        V.px[j] = mixf(V.px[j], (sx - h2 * V.rx[j]) / dg, OMEGA);
-                        V.py[j] = mixf(V.py[j], (sy - h2 * V.ry[j]) / dg, OMEGA);
-                    }
-                }
+                slv_sweep(V, L, s & 1, OMEGA, tid, nt);
                 __syncthreads();
             }
         }
@@ -899,11 +1159,12 @@ __device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t 
     }
     {
         const SLv V = slv(sm, off, D, lc);
-        const LRef<T> G = lref<T>(F, lc);
+        float* ox = up ? F.L[lc].ux : F.L[lc].px;
+        float* oy = up ? F.L[lc].uy : F.L[lc].py;
         const int n = V.w * V.h;
         for (int j = tid; j < n; j += nt) {
-            st(G.px + j, V.px[j]);
-            st(G.py + j, V.py[j]);
+            ox[j] = V.px[j];
+            oy[j] = V.py[j];
         }
     }
 }
@@ -918,7 +1179,7 @@ __global__ void __launch_bounds__(1024) k_fCoarse(Batch Bt, const __grid_constan
         FAST_ITEM(Bt, it, D, F, w, unused_);
         (void)unused_;
         if (D.st->cont == 0u) continue;
-        coarseLevels<T>(D, F, w, F.lc, sm, off);
+        coarseLevels<T>(D, F, w, F.lc, sm, off, true);
         __syncthreads();
     }
 }
@@ -932,12 +1193,12 @@ __global__ void k_fProlongFine(Batch Bt, const __grid_constant__ WorldSrc<ONE> s
         FAST_ITEM(Bt, it, D, F, w, wid);
         if (D.st->cont == 0u) continue;
         const Lvl& L0 = F.L[0];
-        const LRef<T> U = lref<T>(F, 1u);
+        const T* urho = lref<T>(F, 1u).rho;
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         uint32_t i = w.cellIndex(c);
         if (L0.rho[i] > 0.0f) {
-            V2 e = prolongedFrom(U.rho, U.px, U.py, (int)D.level_w[1], (int)D.level_h[1], c.x, c.y);
+            V2 e = prolongedFrom(urho, F.L[1].ux, F.L[1].uy, (int)D.level_w[1], (int)D.level_h[1], c.x, c.y);
             float px = L0.px[i] + e.x, py = L0.py[i] + e.y;
             L0.px[i] = px;
             L0.py[i] = py;
@@ -957,7 +1218,10 @@ __global__ void __launch_bounds__(256) k_fRhoBeta(Batch Bt, const __grid_constan
     if (!ONE) worldCopyInit(wc_);
     __shared__ float sx[256], sy[256];
     __shared__ double s64[256], s64b[256];
+    __shared__ float ux[2][128], uy[2][128];
+    __shared__ double ex64[2][128], ey64[2][128];
     uint32_t pend_ = 0;  // tiles finished of the current world, not yet counted
+    uint32_t par = 0;    // the tree buffers of this item
     FOR_ITEMS(Bt, L_ACT4, it) {
         FAST_ITEM(Bt, it, D, F, w, g);
         if (D.st->cont == 0u) continue;
@@ -983,13 +1247,20 @@ __global__ void __launch_bounds__(256) k_fRhoBeta(Batch Bt, const __grid_constan
                 }
             }
         }
-        float tx = tree64x4(sx, vx);
-        float ty = tree64x4(sy, vy);
+        tilePut(ux[par], vx);
+        tilePut(uy[par], vy);
+        if (f64) {
+            tilePut(ex64[par], ex);
+            tilePut(ey64[par], ey);
+        }
+        __syncthreads();
+        const float tx = tileSum(ux[par], vx), ty = tileSum(uy[par], vy);
         double dx = 0.0, dy = 0.0;
         if (f64) {
-            dx = tree64x4(s64, ex);
-            dy = tree64x4(s64, ey);
+            dx = tileSum(ex64[par], ex);
+            dy = tileSum(ey64[par], ey);
         }
+        par ^= 1u;
         if (valid && (threadIdx.x & 63u) == 0u) {
             const uint32_t b = w.blockIndex(w.activeBlock(wid));
             F.part32[2u * b] = tx;
@@ -1054,7 +1325,10 @@ __global__ void __launch_bounds__(256) k_fApplyAlpha(Batch Bt, const __grid_cons
     if (!ONE) worldCopyInit(wc_);
     __shared__ float sx[256];
     __shared__ double s64[256];
+    __shared__ float ux[2][128];
+    __shared__ double ex64[2][128];
     uint32_t pend_ = 0;  // tiles finished of the current world, not yet counted
+    uint32_t par = 0;    // the tree buffers of this item
     FOR_ITEMS(Bt, L_ACT4, it) {
         FAST_ITEM(Bt, it, D, F, w, g);
         if (D.st->cont == 0u) continue;
@@ -1086,9 +1360,13 @@ __global__ void __launch_bounds__(256) k_fApplyAlpha(Batch Bt, const __grid_cons
                 ex = (double)p * (double)q;
             }
         }
-        float tx = tree64x4(sx, vx);
+        tilePut(ux[par], vx);
+        if (f64) tilePut(ex64[par], ex);
+        __syncthreads();
+        const float tx = tileSum(ux[par], vx);
         double dx = 0.0;
-        if (f64) dx = tree64x4(s64, ex);
+        if (f64) dx = tileSum(ex64[par], ex);
+        par ^= 1u;
         if (valid && (threadIdx.x & 63u) == 0u) {
             const uint32_t b = w.blockIndex(w.activeBlock(wid));
             F.part32[2u * b] = tx;
@@ -1126,11 +1404,13 @@ template <bool ONE>
 __global__ void __launch_bounds__(256) k_fUpdate(Batch Bt, const __grid_constant__ WorldSrc<ONE> src) {
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
-    __shared__ uint32_t most[4];
-    __shared__ uint32_t runMost;  // the largest |r| of the current world's run (bits of a non-negative float)
+    __shared__ uint32_t umost[2][4];  // the upper warps' largest |r| (bits of a non-negative float)
+    __shared__ uint32_t runMost;      // the largest |r| of the current world's run
     __shared__ double s64[256];
+    __shared__ double ur2[2][128];
     if (threadIdx.x == 0) runMost = 0u;
     uint32_t pend_ = 0;  // tiles finished of the current world, not yet counted
+    uint32_t par = 0;    // the tree buffers of this item
     FOR_ITEMS(Bt, L_ACT4, it) {
         FAST_ITEM(Bt, it, D, F, w, g);
         if (D.st->cont == 0u) continue;
@@ -1142,8 +1422,7 @@ __global__ void __launch_bounds__(256) k_fUpdate(Batch Bt, const __grid_constant
         const uint32_t na = w.activeCount();
         const uint32_t wid = g * 4u + (threadIdx.x >> 6);
         const bool valid = wid < na;
-        if ((threadIdx.x & 63u) == 0u) most[threadIdx.x >> 6] = 0u;
-        __syncthreads();
+        uint32_t m = 0u;
         double r2 = 0.0;
         if (valid) {
             I2 c = tileCell(w, wid);
@@ -1165,19 +1444,24 @@ __global__ void __launch_bounds__(256) k_fUpdate(Batch Bt, const __grid_constant
                     L0.rx[i] = -r;
                     F.rimx[i] = 0.0f;
                     F.rimy[i] = L0.py[i];
-                    atomicMax(&most[threadIdx.x >> 6], __float_as_uint(fabsf(r)));
+                    m = __float_as_uint(fabsf(r));
                     r2 = (double)r * (double)r;
                 }
             }
         }
-        double t2 = 0.0;
-        if (tol) t2 = tree64x4(s64, r2);
+        // the tile's largest |r| (a max: any order) and its tree of r^2
+        m = __reduce_max_sync(0xffffffffu, m);
+        if ((threadIdx.x & 63u) == 32u) umost[par][threadIdx.x >> 6] = m;
+        if (tol) tilePut(ur2[par], r2);
         __syncthreads();
+        double t2 = 0.0;
+        if (tol) t2 = tileSum(ur2[par], r2);
         if (valid && (threadIdx.x & 63u) == 0u) {
             if (tol) D.norm64[2u * w.blockIndex(w.activeBlock(wid))] = t2;
-            atomicMax(&runMost, most[threadIdx.x >> 6]);
+            atomicMax(&runMost, max(m, umost[par][threadIdx.x >> 6]));
             __threadfence();
         }
+        par ^= 1u;
         pend_ += min(4u, na - g * 4u);
         if (worldRunEnds(Bt, L_ACT4, g_it, e_it, it)) {
             // the run's largest |r| into the world's residual slot (a max of
@@ -1559,7 +1843,7 @@ __global__ void __launch_bounds__(256, 4) k_fSolve(Fast F, int shifted) {
             for (uint32_t j = gt; j < n; j += gn) restrictCell(F.D, F, w, lp, j);
             if (!gridBarrier(st, nb)) return;
         }
-        if (blockIdx.x == 0) coarseLevels(F.D, F, w, lp, sm_coarse, s_off);
+        if (blockIdx.x == 0) coarseLevels(F.D, F, w, lp, sm_coarse, s_off, false);
         if (!gridBarrier(st, nb)) return;
         for (uint32_t l = lp - 1; l >= 1; l--) {
             const uint32_t n = D.level_w[l] * D.level_h[l];
@@ -1802,7 +2086,7 @@ __global__ void __launch_bounds__(256, 4) k_fSolve(Fast F, int shifted) {
 size_t fast_coarse_smem(const Dev& D, uint32_t lc) {
     size_t n = 0;
     for (uint32_t l = lc; l <= D.levels; l++) n += (size_t)D.level_w[l] * D.level_h[l];
-    return 5u * n * sizeof(float);
+    return SLV_ARRAYS * n * sizeof(float);
 }
 
 void fast_zero_level0(const FastW& F, uint32_t cells, cudaStream_t s) { k_fZero<<<148 * 4, 256, 0, s>>>(F, cells); }
@@ -1841,7 +2125,6 @@ uint32_t fast_cycle_t(const Batch& Bt, const BatchShape& S, const World* one, cu
         if (m) m->fn(m->ctx, slot, phase);
         if (phase) launches++;
     };
-    auto cells = [&](uint32_t list) { return list_grid(S, list, 8); };
     mark(WIG_SLOT_F_LOOP, 0);
     k_fLoopStart<<<list_grid(S, L_ONE, 1), 32, 0, s>>>(Bt);
     mark(WIG_SLOT_F_LOOP, 1);
@@ -1849,18 +2132,12 @@ uint32_t fast_cycle_t(const Batch& Bt, const BatchShape& S, const World* one, cu
     LAUNCH(k_fRelax, GR, 128, 0, 0);
     mark(WIG_SLOT_F_RELAX, 1);
     // down: each world restricts its levels 1..lc by themselves and smooths
-    // those above lc, then its levels from lc are the coarse kernel's
+    // those above lc (a kernel a level), then its levels from lc are the
+    // coarse kernel's; up: each level above lc prolonged and smoothed
     for (uint32_t l = 1; l <= S.lc_max; l++) {
         mark(WIG_SLOT_F_RESTRICT, 0);
-        LAUNCH_T(k_fRestrict, T, cells(L_RES + l - 1u), 256, 0, l);
+        LAUNCH_T(k_fDown, T, list_grid(S, L_RES + l - 1u, 8), 256, 0, l);
         mark(WIG_SLOT_F_RESTRICT, 1);
-        if (S.max_items[L_SM + l - 1u] == 0u) continue;
-        mark(WIG_SLOT_F_SMOOTH, 0);
-        LAUNCH_T(k_fSmooth, T, cells(L_SM + l - 1u), 256, 0, l, 0);
-        mark(WIG_SLOT_F_SMOOTH, 1);
-        mark(WIG_SLOT_F_SMOOTH, 0);
-        LAUNCH_T(k_fSmooth, T, cells(L_SM + l - 1u), 256, 0, l, 1);
-        mark(WIG_SLOT_F_SMOOTH, 1);
     }
     mark(WIG_SLOT_F_COARSE, 0);
     LAUNCH_T(k_fCoarse, T, list_grid(S, L_ONE, 1), 1024, S.coarse_smem);
@@ -1868,14 +2145,8 @@ uint32_t fast_cycle_t(const Batch& Bt, const BatchShape& S, const World* one, cu
     for (uint32_t l = S.lc_max; l >= 1; l--) {
         if (S.max_items[L_SM + l - 1u] == 0u) continue;
         mark(WIG_SLOT_F_PROLONG, 0);
-        LAUNCH_T(k_fProlong, T, cells(L_SM + l - 1u), 256, 0, l);
+        LAUNCH_T(k_fUp, T, list_grid(S, L_SM + l - 1u, 8), 256, 0, l);
         mark(WIG_SLOT_F_PROLONG, 1);
-        mark(WIG_SLOT_F_SMOOTH, 0);
-        LAUNCH_T(k_fSmooth, T, cells(L_SM + l - 1u), 256, 0, l, 0);
-        mark(WIG_SLOT_F_SMOOTH, 1);
-        mark(WIG_SLOT_F_SMOOTH, 0);
-        LAUNCH_T(k_fSmooth, T, cells(L_SM + l - 1u), 256, 0, l, 1);
-        mark(WIG_SLOT_F_SMOOTH, 1);
     }
     mark(WIG_SLOT_F_PROLONG_FINE, 0);
     LAUNCH_T(k_fProlongFine, T, G, 64, 0);
@@ -1932,6 +2203,8 @@ cudaError_t fast_solve_grid(const Fast& F, uint32_t* grid) {
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess) return e;
+    e = cudaFuncSetAttribute(k_fSolve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fast_solve_smem(F));
     if (e != cudaSuccess) return e;
     e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_fSolve, 256, fast_solve_smem(F));
     if (e != cudaSuccess) return e;

@@ -8,7 +8,7 @@
 // a world's arithmetic is the same whichever worlds step beside it.
 //
 // Two points of a step write lists: its start (the worlds' blocks, the
-// particles of `sorted`, per-world work, the coarse levels' cells), and
+// particles of `sorted`, per-world work, the coarse levels' tiles), and
 // after `compact` (the blocks worked on and retired, relaxation tiles, the
 // particles of `parts`, whose count syncParticles and syncSeed have set).
 
@@ -42,11 +42,11 @@ __device__ uint32_t unitsOf(const Batch& Bt, const SchedCtl& c, uint32_t s, uint
     }
     if (L >= L_RES && L < L_RES + WIG_MG_LEVELS) {
         const uint32_t l = L - L_RES + 1u;
-        return (!book && l <= Wd.S.lc && l <= D.levels) ? cdiv(D.level_w[l] * D.level_h[l], 256u) : 0u;
+        return (!book && l <= Wd.S.lc && l <= D.levels) ? levelTiles(D.level_w[l], D.level_h[l]) : 0u;
     }
     if (L >= L_SM && L < L_SM + WIG_MG_LEVELS) {
         const uint32_t l = L - L_SM + 1u;
-        return (!book && l < Wd.S.lc) ? cdiv(D.level_w[l] * D.level_h[l], 256u) : 0u;
+        return (!book && l < Wd.S.lc) ? levelTiles(D.level_w[l], D.level_h[l]) : 0u;
     }
     return 0u;
 }
