@@ -197,10 +197,10 @@ def algorithmic_bytes(name, s):
         "PROJECT": A * 2 * (16 + 16 + 8),
         # the fast form's structure-of-arrays kernels (a float a cell per array)
         "F_RELAX": A * (4 + 8) + Cf * (32 + 8),
-        "F_APPLY_ALPHA": A * 4 + Cf * (4 + 16 + 8 + 1 + 4) + (A - Cf) * 8,
+        # cgDirection with cgApply: z and the old p read, the new p and q written
+        "F_APPLY_ALPHA": A * 12 + Cf * (8 + 4 + 16 + 8 + 1 + 4) + (A - Cf) * 8,
         "F_UPDATE": A * 4 + Cf * (16 + 4 + 24),
         "F_RHO_BETA": A * 4 + Cf * 12,
-        "F_DIRECTION": A * 8 + Cf * 8,
         "F_PROLONG_FINE": A * 4 + Cf * (8 + 16) + Cf // 4 * 12,
         "F_SETUP": A * (32 + 12 + 68),
     }

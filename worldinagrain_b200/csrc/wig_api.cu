@@ -250,7 +250,7 @@ void dev_shape(wig::Dev& D, const wig_world_layout& L) {
 // Bytes of a world's fast scratch and FP64 partials.
 size_t scratch_bytes(const wig::Dev& D) {
     const size_t C = D.C;
-    size_t bytes = align256(C) + 17u * align256(C * 4u);
+    size_t bytes = align256(C) + 18u * align256(C * 4u);
     for (uint32_t l = 1; l <= D.levels; l++) {
         bytes += 12u * align256((size_t)D.level_w[l] * D.level_h[l] * 4u);
         bytes += align256(5u * (size_t)D.level_w[l] * D.level_h[l] * 2u);  // the binary16 operator
@@ -281,7 +281,7 @@ void scratch_take(wig::World& Wd, char* p) {
         F.H[l] = wig::LvlH{reinterpret_cast<__half*>(take(5u * n * 2u)), (uint32_t)n, 0u};
     }
     F.pin = fl(C); F.rimx = fl(C); F.rimy = fl(C);
-    F.X = fl(C); F.R = fl(C); F.P = fl(C); F.Q = fl(C);
+    F.X = fl(C); F.R = fl(C); F.P = fl(C); F.Q = fl(C); F.P2 = fl(C);
     F.part32 = fl(2u * (size_t)D.B);
     F.part64 = reinterpret_cast<double*>(take(2u * (size_t)D.B * 8u));
     D.part64 = reinterpret_cast<double*>(take(2u * (size_t)D.B * 8u));
@@ -835,7 +835,7 @@ int record_step_fast(wig_batch* b, Lane& ln, uint32_t max_cycles, uint32_t flags
         }
         *body = 0;
     }
-    wig::fast_finish(ln.Bt, b->S, one, s, prof ? &mk : nullptr);
+    wig::fast_finish(ln.Bt, b->S, one, (flags & WIG_STEP_PERSISTENT) == 0u, s, prof ? &mk : nullptr);
     R.launches++;
     record_post(R);
     *outside = R.launches;

@@ -374,6 +374,7 @@ struct FastW {
     uint8_t* fmask;            // level 0: bit d set when neighbour d is liquid
     float *rimx, *rimy;        // level 0: the relaxation's rim snapshot
     float *X, *R, *P, *Q;      // level 0: CG's x, r, p, A p
+    float* P2;                 // level 0: p of the fast form's odd iterations (p of the even ones in P)
     float* part32;             // 2 per block
     double* part64;            // 2 per block
     uint32_t lc;               // first level the one-CTA coarse kernel solves

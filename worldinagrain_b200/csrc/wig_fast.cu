@@ -1294,31 +1294,12 @@ __global__ void __launch_bounds__(256) k_fRhoBeta(Batch Bt, const __grid_constan
     }
 }
 
-// cgDirection (fluid.wgsl:2767-2776)
-template <bool ONE>
-__global__ void k_fDirection(Batch Bt, const __grid_constant__ WorldSrc<ONE> src) {
-    __shared__ WorldCopy wc_;
-    if (!ONE) worldCopyInit(wc_);
-    FOR_ITEMS(Bt, L_ACT, it) {
-        FAST_ITEM(Bt, it, D, F, w, wid);
-        if (D.st->cont == 0u) continue;
-        const bool f64 = D.st->f64 != 0u;
-        const float beta = D.st->beta32;
-        const double beta64 = D.st->beta;
-        const Lvl& L0 = F.L[0];
-        I2 c = lidCell(w, wid);
-        if (!w.inWorld(c)) continue;
-        uint32_t i = w.cellIndex(c);
-        float p = 0.0f;
-        if (L0.rho[i] > 0.0f) {
-            float z = L0.px[i];
-            p = f64 ? (float)((double)z + beta64 * (double)F.P[i]) : z + beta * F.P[i];
-        }
-        F.P[i] = p;
-    }
-}
-
-// cgApply + cgAlpha (fluid.wgsl:2779-2814)
+// cgDirection + cgApply + cgAlpha (fluid.wgsl:2767-2814): the direction p =
+// z + beta p_old of the cell and of its liquid neighbours (worked again from
+// their z and p_old, the same arithmetic), q = A p, and the tile trees of
+// p q.  p_old is read from one of the two p arrays and p written to the
+// other (by the iteration's parity), so no CTA reads a p that another
+// writes in the launch.
 template <bool ONE>
 __global__ void __launch_bounds__(256) k_fApplyAlpha(Batch Bt, const __grid_constant__ WorldSrc<ONE> src) {
     __shared__ WorldCopy wc_;
@@ -1333,28 +1314,39 @@ __global__ void __launch_bounds__(256) k_fApplyAlpha(Batch Bt, const __grid_cons
         FAST_ITEM(Bt, it, D, F, w, g);
         if (D.st->cont == 0u) continue;
         const bool f64 = D.st->f64 != 0u;
+        const float beta = D.st->beta32;
+        const double beta64 = D.st->beta;
+        const bool odd = (D.st->cycle & 1u) != 0u;
+        const float* Pold = odd ? F.P2 : F.P;
+        float* Pnew = odd ? F.P : F.P2;
         const Lvl& L0 = F.L[0];
         const uint32_t na = w.activeCount();
         const uint32_t wid = g * 4u + (threadIdx.x >> 6);
         const bool valid = wid < na;
+        // cgDirection's p of liquid cell k
+        auto dir = [&](uint32_t k) {
+            const float z = L0.px[k];
+            return f64 ? (float)((double)z + beta64 * (double)Pold[k]) : z + beta * Pold[k];
+        };
         float vx = 0.0f;
         double ex = 0.0;
         if (valid) {
             I2 c = tileCell(w, wid);
             if (w.inWorld(c)) {
                 uint32_t i = w.cellIndex(c);
-                float q = 0.0f;
-                const float p = F.P[i];
+                float p = 0.0f, q = 0.0f;
                 if (L0.rho[i] > 0.0f) {
+                    p = dir(i);
                     const uint8_t m = F.fmask[i];
                     const float b[4] = {L0.b0[i], L0.b1[i], L0.b2[i], L0.b3[i]};
                     float sum = 0.0f;
 #pragma unroll
                     for (int d = 0; d < 4; d++)
-                        if (m & (1u << d)) sum = sum + b[d] * F.P[nbr(i, c.x, c.y, D.W, D.H, d)];
+                        if (m & (1u << d)) sum = sum + b[d] * dir(nbr(i, c.x, c.y, D.W, D.H, d));
                     float dg = L0.diag[i] + F.pin[i];
                     q = dg * p - sum + 0.0f;
                 }
+                Pnew[i] = p;
                 F.Q[i] = q;
                 vx = p * q;
                 ex = (double)p * (double)q;
@@ -1429,7 +1421,7 @@ __global__ void __launch_bounds__(256) k_fUpdate(Batch Bt, const __grid_constant
             if (w.inWorld(c)) {
                 uint32_t i = w.cellIndex(c);
                 if (L0.rho[i] > 0.0f) {
-                    float vx = F.X[i], vy = F.R[i], vz = F.P[i], vw = F.Q[i];
+                    float vx = F.X[i], vy = F.R[i], vz = ((cycle & 1u) ? F.P : F.P2)[i], vw = F.Q[i];
                     float r, x;
                     if (f64) {
                         r = (float)((double)vy - alpha64 * (double)vw);
@@ -1639,7 +1631,7 @@ __global__ void k_fLoopStart(Batch Bt) {
 // iterations the reference still dispatches would clear (cgUpdate's first
 // lines run whether or not the iteration is skipped).
 template <bool ONE>
-__global__ void k_fFinish(Batch Bt, const __grid_constant__ WorldSrc<ONE> src) {
+__global__ void k_fFinish(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, int two_p) {
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
     if (threadIdx.x == 0) {
@@ -1660,7 +1652,9 @@ __global__ void k_fFinish(Batch Bt, const __grid_constant__ WorldSrc<ONE> src) {
         f[0] = F.X[i];
         if (L0.rho[i] > 0.0f) f[1] = L0.rx[i];
         w.fv(2u * i + 1u)[0] = L0.py[i];
-        reinterpret_cast<float4*>(D.cg)[i] = make_float4(F.X[i], F.R[i], F.P[i], F.Q[i]);
+        // the last iteration's p: P2 after an odd number of iterations
+        const float* P = (two_p && (D.st->cycle & 1u)) ? F.P2 : F.P;
+        reinterpret_cast<float4*>(D.cg)[i] = make_float4(F.X[i], F.R[i], P[i], F.Q[i]);
         *w.gwp(i, G_REGION) = 0u;
     }
 }
@@ -2157,9 +2151,6 @@ uint32_t fast_cycle_t(const Batch& Bt, const BatchShape& S, const World* one, cu
     mark(WIG_SLOT_F_RHO_BETA, 0);
     LAUNCH(k_fRhoBeta, G4, 256, 0);
     mark(WIG_SLOT_F_RHO_BETA, 1);
-    mark(WIG_SLOT_F_DIRECTION, 0);
-    LAUNCH(k_fDirection, G, 64, 0);
-    mark(WIG_SLOT_F_DIRECTION, 1);
     mark(WIG_SLOT_F_APPLY_ALPHA, 0);
     LAUNCH(k_fApplyAlpha, G4, 256, 0);
     mark(WIG_SLOT_F_APPLY_ALPHA, 1);
@@ -2181,9 +2172,9 @@ uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, const World* one, cuda
     return Bt.mixed ? fast_cycle_t<__half>(Bt, S, one, s, m) : fast_cycle_t<float>(Bt, S, one, s, m);
 }
 
-void fast_finish(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m) {
+void fast_finish(const Batch& Bt, const BatchShape& S, const World* one, bool two_p, cudaStream_t s, const Marker* m) {
     if (m) m->fn(m->ctx, WIG_SLOT_F_FINISH, 0);
-    LAUNCH(k_fFinish, list_grid(S, L_ACT, 32), 64, 0);
+    LAUNCH(k_fFinish, list_grid(S, L_ACT, 32), 64, 0, two_p ? 1 : 0);
     if (m) m->fn(m->ctx, WIG_SLOT_F_FINISH, 1);
 }
 

@@ -32,7 +32,8 @@ struct Marker {
 // for a batch of several.  fast_cycle returns its launches.
 void fast_setup(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m);
 uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m);
-void fast_finish(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m);
+// cgFinish; `two_p`: the fast form's p is in P or P2 by the iterations' parity.
+void fast_finish(const Batch& Bt, const BatchShape& S, const World* one, bool two_p, cudaStream_t s, const Marker* m);
 // Level 0's arrays of one world zeroed (after its buffers are written by the host).
 void fast_zero_level0(const FastW& F, uint32_t cells, cudaStream_t s);
 // The same for the blocks not worked on, of every world of the step whose
