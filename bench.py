@@ -302,6 +302,24 @@ def run_batched(args, rank, world_size, local_rank, dist, torch, emit=True):
             P[k].frame = step_no
         b.step(ids, P, max_cycles=MAX_CYCLES, flags=FLAGS | extra, tolerance=TOL, stream=stream.cuda_stream)
 
+    # the launch shapes tuned on the batch's first steps (profiled steps of
+    # the same worlds: no result changes), then the warm-up
+    tuned = None
+    if not args.no_tune:
+        from worldinagrain_b200 import tune
+
+        def prof_step():
+            nonlocal step_no
+            step_no += 1
+            for k in range(n):
+                P[k].frame = step_no
+            return b.step_profile(range(n), P, max_cycles=MAX_CYCLES, flags=FLAGS, tolerance=TOL,
+                                  stream=stream.cuda_stream)
+
+        shapes, trials = tune.autotune(b, prof_step)
+        tuned = {"shapes": shapes, "steps": tune.steps_needed(),
+                 "trials_ms_per_iteration": {k: [[v, None if c is None else round(c, 4)] for v, c in r]
+                                             for k, r in trials.items()}}
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -390,6 +408,7 @@ def run_batched(args, rank, world_size, local_rank, dist, torch, emit=True):
         dt = time.perf_counter() - t0
         cpu = {"value": round(done_cells / dt / 1e6, 4), "unit": "Mcells/s", "cores": 1, "kind": "port",
                "sample": f"the first step of {steps_done} of the {n} worlds on one host core, {dt:.1f} s"}
+    b_shapes = b.launch_shapes()
     b.close()
     if rank == 0:
         sides = sorted(w.W for w in worlds)
@@ -401,7 +420,9 @@ def run_batched(args, rank, world_size, local_rank, dist, torch, emit=True):
                        "worlds_on_rank0": n, "sharding": "cell-balanced greedy partition, no data-path collective",
                        "sides": f"log-uniform {sides[0]}..{sides[-1]}, median {sides[n // 2]}", "seed": args.seed,
                        "liquid_per_cell": 4, "tolerance": TOL, "max_cycles": MAX_CYCLES,
-                       "form": "batched fast form: one launch a pass over all worlds, CG loop in a graph WHILE node",
+                       "form": f"batched {args.form} form: one launch a pass over all worlds, CG loop in a graph WHILE node",
+                       "launch": tuned["shapes"] if tuned else b_shapes,
+                       "autotune": tuned,
                        "l2": "inputs larger than L2 (worlds resident in HBM, no flush)", "parallelism": "replicas"},
             "e2e": {"value": round(e2e, 3), "unit": "Mcells/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches_per_step * args.steps,
@@ -525,6 +546,7 @@ def main():
     ap.add_argument("--pool-gb", type=float, default=7.0)
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--serve-max-requests", type=int, default=4000)
+    ap.add_argument("--no-tune", action="store_true", help="the batched workload with the default launch shapes")
     ap.add_argument("--no-forms", action="store_true",
                     help="the single world alone, without the batched and served summaries a one-GPU run adds")
     args = ap.parse_args()

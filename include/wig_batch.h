@@ -101,6 +101,28 @@ uint64_t wig_batch_resident_bytes(const wig_batch* b);
 int wig_batch_set_lane_pool(wig_batch* b, uint32_t lane, uint64_t bytes);
 int wig_batch_world_bytes_split(const wig_world_desc* d, uint64_t* persistent, uint64_t* transient);
 
+/* Launch shapes of the fast form, none of which changes a result bit (every
+ * kernel's arithmetic and order are the same whichever CTA does a unit):
+ * what an autotuner may choose per batch.
+ *   COARSE_CELLS: the one-CTA coarse kernel takes a world's levels from its
+ *     first level of at most this many cells (1 .. 4096; a world with no
+ *     such level above its coarsest: from the coarsest), the tile kernels
+ *     the levels above it: the depth of the V-cycle's on-chip part;
+ *   LEVEL_PER_SM, CG_PER_SM, RELAX_PER_SM: CTAs a multiprocessor (1 .. 64)
+ *     of the level tile kernels, of the three CG kernels, of the fine
+ *     relaxation.
+ * No step of the batch may be in flight; the lanes' graphs are recaptured
+ * at their next step. */
+enum wig_launch_knob {
+    WIG_LAUNCH_COARSE_CELLS = 0,
+    WIG_LAUNCH_LEVEL_PER_SM = 1,
+    WIG_LAUNCH_CG_PER_SM = 2,
+    WIG_LAUNCH_RELAX_PER_SM = 3,
+    WIG_LAUNCH_KNOBS = 4
+};
+int wig_batch_set_launch(wig_batch* b, uint32_t knob, uint32_t value);
+int wig_batch_get_launch(const wig_batch* b, uint32_t knob, uint32_t* value);
+
 #ifdef __cplusplus
 }
 #endif

@@ -213,3 +213,63 @@ def test_many_world_batch_is_deterministic():
         assert sa[k][1] <= 1e-6, (picked[k], sa[k][1])
         d = _same(wa[k], wb[k])
         assert not d, f"world {picked[k]}: {d}"
+
+
+def test_launch_shapes_change_no_result():
+    """Every launch-shape knob at a value other than its default, the V-cycle
+    handed to the coarse kernel at another depth: the same buffers and stats
+    as the default shapes."""
+    from worldinagrain_b200 import fluid
+    picked = [2, 25, 9, 120]
+    runs = []
+    for shapes in ({}, {"coarse_cells": 512, "level_per_sm": 2, "cg_per_sm": 3, "relax_per_sm": 5}):
+        mine = W.multi_worlds(n=512, seed=2, only=picked)
+        b = fluid.Batch(mine, W.element_table())
+        for k, v in shapes.items():
+            b.set_launch(k, v)
+        ids = list(range(len(mine)))
+        for s in range(1, 4):
+            b.step(ids, [params(w, s) for w in mine], max_cycles=64, flags=TOL, tolerance=1e-6)
+        st = b.stats(ids)
+        for k in ids:
+            b.download(k)
+        got = b.launch_shapes()
+        b.close()
+        runs.append((mine, [(x.cycles, x.rel_residual, tuple(x.count)) for x in st], got))
+    (wa, sa, _), (wb, sb, gb) = runs
+    assert gb == {"coarse_cells": 512, "level_per_sm": 2, "cg_per_sm": 3, "relax_per_sm": 5}
+    for k in range(len(picked)):
+        assert sa[k] == sb[k], (picked[k], sa[k], sb[k])
+        d = _same(wa[k], wb[k])
+        assert not d, f"world {picked[k]}: {d}"
+
+
+def test_autotuned_batch_steps_as_the_untuned_one():
+    """The tuner's profiled steps are the batch's steps: a tuned batch and
+    one stepped alike with the default shapes end bit for bit the same."""
+    from worldinagrain_b200 import fluid, tune
+    picked = [2, 25, 9]
+    n_steps = tune.steps_needed() + 2
+    out = []
+    for tuned in (False, True):
+        mine = W.multi_worlds(n=512, seed=2, only=picked)
+        b = fluid.Batch(mine, W.element_table())
+        ids = list(range(len(mine)))
+        s = [0]
+
+        def prof_step():
+            s[0] += 1
+            return b.step_profile(ids, [params(w, s[0]) for w in mine], max_cycles=64, flags=TOL, tolerance=1e-6)
+
+        if tuned:
+            shapes, trials = tune.autotune(b, prof_step)
+            assert set(trials) == {k for k, _, _ in tune.KNOBS}
+        while s[0] < n_steps:
+            prof_step()
+        for k in ids:
+            b.download(k)
+        b.close()
+        out.append(mine)
+    for k in range(len(picked)):
+        d = _same(out[0][k], out[1][k])
+        assert not d, f"world {picked[k]}: {d}"

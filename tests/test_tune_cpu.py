@@ -1,0 +1,60 @@
+"""The launch-shape autotuner's choices, over a fake batch whose profiled
+steps cost what a table says: each knob ends at its cheapest candidate,
+tried in order, each knob tuned with the earlier knobs' choices in place."""
+from worldinagrain_b200 import tune
+
+
+class FakeBatch:
+    def __init__(self, costs):
+        self.shapes = {"coarse_cells": 4096, "level_per_sm": 8, "cg_per_sm": 8, "relax_per_sm": 16}
+        self.costs = costs  # knob -> value -> ms per iteration of its slots
+        self.log = []
+
+    def get_launch(self, name):
+        return self.shapes[name]
+
+    def set_launch(self, name, value):
+        self.shapes[name] = value
+        self.log.append((name, value))
+
+    def launch_shapes(self):
+        return dict(self.shapes)
+
+    def step(self):
+        iters = 7
+        prof = {"F_LOOP": (0.1, iters)}
+        for name, _, slots in tune.KNOBS:
+            share = self.costs[name][self.shapes[name]] * iters / len(slots)
+            for s in slots:
+                ms, n = prof.get(s, (0.0, 0))
+                prof[s] = (ms + share, n + iters)
+        return prof
+
+
+def test_each_knob_ends_at_its_cheapest_candidate():
+    # per knob, its candidates' costs: the second cheapest for the first
+    # knob, the first for the second, and so on
+    costs, want = {}, {}
+    for j, (name, cands, _) in enumerate(tune.KNOBS):
+        cheap = cands[(j + 1) % len(cands)]
+        costs[name] = {v: (1.0 if v == cheap else 2.0 + 0.1 * i) for i, v in enumerate(cands)}
+        want[name] = cheap
+    b = FakeBatch(costs)
+    shapes, trials = tune.autotune(b, b.step)
+    assert shapes == want
+    assert [v for v, _ in trials["coarse_cells"]] == list(tune.KNOBS[0][1])
+    assert len(b.log) == tune.steps_needed() + len(tune.KNOBS)
+
+
+def test_cost_is_per_iteration_and_none_without_iterations():
+    assert tune.cost({"F_LOOP": (0.0, 4), "F_RELAX": (8.0, 8)}, ("F_RELAX",)) == 2.0
+    assert tune.cost({"F_RELAX": (8.0, 8)}, ("F_RELAX",)) is None
+
+
+def test_no_iteration_keeps_the_current_shape():
+    class Idle(FakeBatch):
+        def step(self):
+            return {}
+    b = Idle({})
+    shapes, _ = tune.autotune(b, b.step)
+    assert shapes == {"coarse_cells": 4096, "level_per_sm": 8, "cg_per_sm": 8, "relax_per_sm": 16}

@@ -37,6 +37,14 @@ STEP_PLAIN = 128
 STEP_PERSISTENT = 256
 STEP_MIXED = 512
 
+# wig_launch_knob (include/wig_batch.h): launch shapes that change no result
+LAUNCH_COARSE_CELLS = 0
+LAUNCH_LEVEL_PER_SM = 1
+LAUNCH_CG_PER_SM = 2
+LAUNCH_RELAX_PER_SM = 3
+LAUNCH_KNOBS = {"coarse_cells": LAUNCH_COARSE_CELLS, "level_per_sm": LAUNCH_LEVEL_PER_SM,
+                "cg_per_sm": LAUNCH_CG_PER_SM, "relax_per_sm": LAUNCH_RELAX_PER_SM}
+
 PASSES = [
     "SYNC", "SYNC_MARKS", "SYNC_PARTICLES", "SYNC_SEED", "COMPACT", "RETIRE", "CLEAR", "GATHER",
     "SEAL_JOIN", "SEAL_ANCHOR", "CLASSIFY", "SET_FACES", "VISCOSITY_RED", "VISCOSITY_BLACK", "UNPRESS",

@@ -259,8 +259,9 @@ size_t scratch_bytes(const wig::Dev& D) {
     return bytes;
 }
 
-// Lays a world's scratch out from p (scratch_bytes of it).
-void scratch_take(wig::World& Wd, char* p) {
+// Lays a world's scratch out from p (scratch_bytes of it); the coarse
+// kernel from its first level of at most coarse_cells cells.
+void scratch_take(wig::World& Wd, char* p, uint32_t coarse_cells) {
     wig::Dev& D = Wd.D;
     wig::FastW& F = Wd.S;
     auto take = [&](size_t n) { char* q = p; p += align256(n); return q; };
@@ -286,9 +287,7 @@ void scratch_take(wig::World& Wd, char* p) {
     F.part64 = reinterpret_cast<double*>(take(2u * (size_t)D.B * 8u));
     D.part64 = reinterpret_cast<double*>(take(2u * (size_t)D.B * 8u));
     D.norm64 = reinterpret_cast<double*>(take(2u * (size_t)D.B * 8u));
-    F.lc = D.levels;
-    for (uint32_t l = 1; l <= D.levels; l++)
-        if ((size_t)D.level_w[l] * D.level_h[l] <= wig::COARSE_CTA_CELLS) { F.lc = l; break; }
+    F.lc = wig::coarse_level(D, coarse_cells);
     F.lp = D.levels;
     for (uint32_t l = 1; l <= D.levels; l++)
         if ((size_t)D.level_w[l] * D.level_h[l] <= wig::PERSISTENT_CTA_CELLS) { F.lp = l; break; }
@@ -342,6 +341,32 @@ int upload_world_entry(wig_batch* b, uint32_t k) {
     return WIG_OK;
 }
 
+// The level part of a batch's shape for its coarse_cells: each world's
+// coarse level (into its table entry), the level lists' current lengths,
+// the deepest level restricted by a tile kernel, the coarse kernel's memory.
+void level_shape(wig_batch* b) {
+    wig::BatchShape& S = b->S;
+    for (uint32_t l = 0; l < WIG_MG_LEVELS; l++) {
+        S.max_items[wig::L_RES + l] = 0;
+        S.max_items[wig::L_SM + l] = 0;
+    }
+    S.lc_max = 0;
+    S.coarse_smem = 0;
+    for (uint32_t k = 0; k < b->K; k++) {
+        wig::World& Wd = b->hw[k];
+        const wig::Dev& D = Wd.D;
+        const uint32_t lc = wig::coarse_level(D, S.coarse_cells);
+        Wd.S.lc = lc;
+        for (uint32_t l = 1; l <= D.levels; l++) {
+            const uint32_t ch = wig::levelTiles(D.level_w[l], D.level_h[l]);
+            if (l <= lc) S.max_items[wig::L_RES + l - 1] += ch;
+            if (l < lc) S.max_items[wig::L_SM + l - 1] += ch;
+        }
+        S.lc_max = std::max(S.lc_max, lc);
+        S.coarse_smem = std::max(S.coarse_smem, wig::fast_coarse_smem(D, lc));
+    }
+}
+
 // How a batch holds its worlds' device memory: a single world's scratch with
 // its buffers bound later (wig_fluid_bind); every world's buffers and
 // scratch packed in two allocations; or each world's own allocation, made
@@ -387,21 +412,22 @@ int make_batch(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, u
         }
         dev_shape(b->hw[k].D, b->L[k]);
     }
-    // the shape: list sizes, coarse kernel's memory, item bits
+    // the shape: list sizes, coarse kernel's memory, item bits; the level
+    // lists' room for any coarse level (every level above the coarsest)
     wig::BatchShape& S = b->S;
     std::memset(&S, 0, sizeof(S));
     S.worlds = n;
+    S.coarse_cells = wig::COARSE_CTA_CELLS;
+    S.level_per_sm = 8;
+    S.cg_per_sm = 8;
+    S.relax_per_sm = 16;
     uint64_t most_units = 1, max_items[wig::L_COUNT] = {0};
     size_t scratch_total = 0;
     for (uint32_t k = 0; k < n; k++) {
         wig::World& Wd = b->hw[k];
         const wig::Dev& D = Wd.D;
         scratch_total += scratch_bytes(D);
-        // lc for the shape (scratch_take sets it again on the real layout)
-        uint32_t lc = D.levels;
-        for (uint32_t l = 1; l <= D.levels; l++)
-            if ((size_t)D.level_w[l] * D.level_h[l] <= wig::COARSE_CTA_CELLS) { lc = l; break; }
-        Wd.S.lc = lc;
+        const uint32_t lc = D.levels;
         const uint64_t pch = cdiv(D.cap, 256);
         max_items[wig::L_WB] += D.B;
         max_items[wig::L_PS] += pch;
@@ -420,8 +446,6 @@ int make_batch(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, u
         }
         most_units = std::max<uint64_t>(most_units, std::max<uint64_t>(D.B + D.edge_tiles, pch));
         S.levels = std::max(S.levels, D.levels);
-        S.lc_max = std::max(S.lc_max, lc);
-        S.coarse_smem = std::max(S.coarse_smem, wig::fast_coarse_smem(D, lc));
     }
     uint32_t bits = 1;
     while (bits < 31 && (1ull << bits) <= most_units) bits++;
@@ -437,6 +461,7 @@ int make_batch(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, u
         items_total += max_items[l];
     }
     if (items_total > 0xffffffffull) return bail(WIG_E_ARG, "work lists too long");
+    level_shape(b);
     if (S.coarse_smem > 220u * 1024u) return bail(WIG_E_ARG, "coarse levels too large for one CTA");
     if (wig::fast_prepare_attributes(S.coarse_smem) != cudaSuccess) return bail(WIG_E_CUDA, "cudaFuncSetAttribute");
 
@@ -462,7 +487,7 @@ int make_batch(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, u
         cudaMemset(b->scratch, 0, scratch_total);
         char* p = static_cast<char*>(b->scratch);
         for (uint32_t k = 0; k < n; k++) {
-            scratch_take(b->hw[k], p);
+            scratch_take(b->hw[k], p, b->S.coarse_cells);
             p += scratch_bytes(b->hw[k].D);
         }
     } else {
@@ -938,7 +963,7 @@ int push_inputs(wig_batch* b, Lane& ln, const StepArgs& a, bool* viscous, bool* 
             q += align256(buffer_bytes(b->L[k], 2));
             e.D.cg = reinterpret_cast<float*>(q);
             q += align256(buffer_bytes(b->L[k], 6));
-            scratch_take(e, q);
+            scratch_take(e, q, b->S.coarse_cells);
             ent[i] = e;
             at += need;
         }
@@ -1364,7 +1389,7 @@ int wig_batch_admit(wig_batch* b, uint32_t world, void* stream) {
         *buffer_slot(Wd.D, w) = q;
         q += align256(b->pooled ? persistent_buffer_bytes(b->L[world], w) : buffer_bytes(b->L[world], w));
     }
-    if (!b->pooled) scratch_take(Wd, q);
+    if (!b->pooled) scratch_take(Wd, q, b->S.coarse_cells);
     CUDA_TRY(cudaMemcpyAsync(b->d_worlds + world, &Wd, sizeof(wig::World), cudaMemcpyHostToDevice, s));
     for (auto& ln : b->lane)
         if (ln.d_table) CUDA_TRY(cudaMemcpyAsync(ln.d_table + world, &Wd, sizeof(wig::World), cudaMemcpyHostToDevice, s));
@@ -1405,6 +1430,39 @@ int wig_batch_world_bytes_split(const wig_world_desc* d, uint64_t* persistent, u
     dev_shape(D, L);
     *persistent = persistent_bytes(L);
     *transient = transient_bytes(L, D);
+    return WIG_OK;
+}
+
+int wig_batch_set_launch(wig_batch* b, uint32_t knob, uint32_t value) {
+    if (!b) return fail(WIG_E_ARG, "null batch");
+    if (knob >= WIG_LAUNCH_KNOBS) return fail(WIG_E_ARG, "unknown launch knob");
+    const uint32_t most = knob == WIG_LAUNCH_COARSE_CELLS ? wig::COARSE_CTA_CELLS : 64u;
+    if (value < 1u || value > most) return fail(WIG_E_ARG, "launch knob value out of range");
+    CUDA_TRY(cudaDeviceSynchronize());
+    wig::BatchShape& S = b->S;
+    switch (knob) {
+    case WIG_LAUNCH_COARSE_CELLS:
+        S.coarse_cells = value;
+        level_shape(b);
+        CUDA_TRY(cudaMemcpy(b->d_worlds, b->hw.data(), sizeof(wig::World) * b->K, cudaMemcpyHostToDevice));
+        break;
+    case WIG_LAUNCH_LEVEL_PER_SM: S.level_per_sm = value; break;
+    case WIG_LAUNCH_CG_PER_SM: S.cg_per_sm = value; break;
+    default: S.relax_per_sm = value; break;
+    }
+    for (auto& ln : b->lane) drop_graphs(ln);
+    return WIG_OK;
+}
+
+int wig_batch_get_launch(const wig_batch* b, uint32_t knob, uint32_t* value) {
+    if (!b || !value) return fail(WIG_E_ARG, "null argument");
+    switch (knob) {
+    case WIG_LAUNCH_COARSE_CELLS: *value = b->S.coarse_cells; break;
+    case WIG_LAUNCH_LEVEL_PER_SM: *value = b->S.level_per_sm; break;
+    case WIG_LAUNCH_CG_PER_SM: *value = b->S.cg_per_sm; break;
+    case WIG_LAUNCH_RELAX_PER_SM: *value = b->S.relax_per_sm; break;
+    default: return fail(WIG_E_ARG, "unknown launch knob");
+    }
     return WIG_OK;
 }
 

@@ -2111,9 +2111,8 @@ void fast_setup(const Batch& Bt, const BatchShape& S, const World* one, cudaStre
 
 template <class T>
 uint32_t fast_cycle_t(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m) {
-    const unsigned G = list_grid(S, L_ACT, 32), G4 = list_grid(S, L_ACT4, 8);
-    const unsigned GR = (S.max_items[L_RELAX] + 3u) / 4u < 148u * 16u ? std::max((S.max_items[L_RELAX] + 3u) / 4u, 1u)
-                                                                      : 148u * 16u;
+    const unsigned G = list_grid(S, L_ACT, 32), G4 = list_grid(S, L_ACT4, S.cg_per_sm);
+    const unsigned GR = std::max(std::min((S.max_items[L_RELAX] + 3u) / 4u, 148u * S.relax_per_sm), 1u);
     uint32_t launches = 0;
     auto mark = [&](int slot, int phase) {
         if (m) m->fn(m->ctx, slot, phase);
@@ -2130,7 +2129,7 @@ uint32_t fast_cycle_t(const Batch& Bt, const BatchShape& S, const World* one, cu
     // coarse kernel's; up: each level above lc prolonged and smoothed
     for (uint32_t l = 1; l <= S.lc_max; l++) {
         mark(WIG_SLOT_F_RESTRICT, 0);
-        LAUNCH_T(k_fDown, T, list_grid(S, L_RES + l - 1u, 8), 256, 0, l);
+        LAUNCH_T(k_fDown, T, list_grid(S, L_RES + l - 1u, S.level_per_sm), 256, 0, l);
         mark(WIG_SLOT_F_RESTRICT, 1);
     }
     mark(WIG_SLOT_F_COARSE, 0);
@@ -2139,7 +2138,7 @@ uint32_t fast_cycle_t(const Batch& Bt, const BatchShape& S, const World* one, cu
     for (uint32_t l = S.lc_max; l >= 1; l--) {
         if (S.max_items[L_SM + l - 1u] == 0u) continue;
         mark(WIG_SLOT_F_PROLONG, 0);
-        LAUNCH_T(k_fUp, T, list_grid(S, L_SM + l - 1u, 8), 256, 0, l);
+        LAUNCH_T(k_fUp, T, list_grid(S, L_SM + l - 1u, S.level_per_sm), 256, 0, l);
         mark(WIG_SLOT_F_PROLONG, 1);
     }
     mark(WIG_SLOT_F_PROLONG_FINE, 0);

@@ -19,6 +19,14 @@ struct Fast : FastW {
 // The one-CTA coarse kernel holds levels of at most this many cells; CTA 0
 // of the persistent solve, of at most PERSISTENT_CTA_CELLS.
 constexpr uint32_t COARSE_CTA_CELLS = 4096;
+
+// A world's first level of at most `cells` cells (its coarsest when none
+// above it is): where the coarse kernel takes over.
+inline uint32_t coarse_level(const Dev& D, uint32_t cells) {
+    for (uint32_t l = 1; l <= D.levels; l++)
+        if ((size_t)D.level_w[l] * D.level_h[l] <= cells) return l;
+    return D.levels;
+}
 constexpr uint32_t PERSISTENT_CTA_CELLS = 1024;
 
 // A profiler's hook around each launch: fn(ctx, slot, 0) before, (ctx, slot, 1) after.

@@ -46,6 +46,8 @@ FUNCS = {
                                 C.POINTER(C.c_uint32), C.c_uint32, C.c_uint32, C.c_double, C.c_void_p,
                                 C.POINTER(C.c_float), C.POINTER(C.c_uint32)], C.c_int),
     "wig_batch_destroy": ([C.c_void_p], None),
+    "wig_batch_set_launch": ([C.c_void_p, C.c_uint32, C.c_uint32], C.c_int),
+    "wig_batch_get_launch": ([C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)], C.c_int),
 }
 
 
@@ -243,3 +245,18 @@ class Batch:
         out = (abi.Stats * len(ids))()
         check(lib().wig_batch_read_stats(self.h, _u32s(ids), len(ids), out), "wig_batch_read_stats")
         return list(out)
+
+    def set_launch(self, knob, value):
+        """One launch shape (abi.LAUNCH_KNOBS: a name or its number); no
+        result changes."""
+        k = abi.LAUNCH_KNOBS.get(knob, knob)
+        check(lib().wig_batch_set_launch(self.h, k, int(value)), f"wig_batch_set_launch {knob}")
+
+    def get_launch(self, knob):
+        k = abi.LAUNCH_KNOBS.get(knob, knob)
+        v = C.c_uint32()
+        check(lib().wig_batch_get_launch(self.h, k, C.byref(v)), f"wig_batch_get_launch {knob}")
+        return v.value
+
+    def launch_shapes(self):
+        return {name: self.get_launch(name) for name in abi.LAUNCH_KNOBS}
