@@ -256,7 +256,7 @@ def run_reference(args, rank, world_size):
     line = {
         "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "Mcells/s", "n_gpus": world_size,
         "steps": steps, "warmup": args.warmup, "ms_per_step": round(dt / steps * 1e3, 3), "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": dtype_of(args.form), "data": "synthetic",
         "config": config_of(world, args),
         "cpu_baseline": {"value": round(value, 4), "unit": "Mcells/s", "cores": 1, "kind": "port", "sample": sample},
         "e2e": {"value": round(value, 4), "unit": "Mcells/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -415,7 +415,7 @@ def run_batched(args, rank, world_size, local_rank, dist, torch, emit=True):
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "Mcells/s", "n_gpus": world_size,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype_of(args.form), "data": "synthetic",
             "config": {"workload": f"multi_worlds_{args.worlds}_per_gpu", "worlds": n_all, "cells": sum(all_cells),
                        "worlds_on_rank0": n, "sharding": "cell-balanced greedy partition, no data-path collective",
                        "sides": f"log-uniform {sides[0]}..{sides[-1]}, median {sides[n // 2]}", "seed": args.seed,
@@ -467,7 +467,16 @@ def run_served(args, rank, world_size, local_rank, dist, torch, emit=True):
     srv.preload()
     t_preload = time.perf_counter() - t0
     resident = len(srv.resident)
-    srv.run(serve.poisson_arrivals(1000.0, 200, len(worlds), seed=99))  # graphs captured, first steps seeded
+    # launch shapes tuned on profiled steps of the resident worlds (as many
+    # as a lane's pool takes), then graphs captured and first steps seeded
+    tuned = None
+    if args.tune_served:
+        from worldinagrain_b200 import tune
+        shapes, trials = be.autotune(list(srv.resident))
+        tuned = {"shapes": shapes, "steps": tune.steps_needed(),
+                 "trials_ms_per_iteration": {k: [[v, None if c is None else round(c, 4)] for v, c in r]
+                                             for k, r in trials.items()}}
+    srv.run(serve.poisson_arrivals(1000.0, 200, len(worlds), seed=99))
     rates = [float(r) for r in args.rates.split(",")]
     points = []
     with Clocks(gpu_index_of(torch, local_rank)) as clk:
@@ -501,13 +510,15 @@ def run_served(args, rank, world_size, local_rank, dist, torch, emit=True):
         line = {
             "metric": METRIC + "; served p50/p99 step latency", "value": best["mcells_per_s"], "unit": "Mcells/s",
             "n_gpus": world_size, "steps": sum(p["requests"] for p in points), "warmup": 200,
-            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype_of(args.form),
             "data": "synthetic",
             "config": {"workload": f"served_{args.worlds}_worlds_per_gpu", "worlds": n_all,
                        "cells": sum(s_[0] * s_[0] for s_ in specs), "worlds_on_rank0": len(worlds),
                        "sides": "log-uniform 64..1024", "budget_gb": args.budget_gb, "lane_pool_gb": args.pool_gb,
                        "resident_worlds": resident, "resident_gb": round(srv.resident_bytes / 1e9, 2),
                        "build_s": round(t_build, 1), "preload_s": round(t_preload, 1), "tolerance": TOL,
+                       "form": f"served {args.form} form: continuous batching over two lanes",
+                       "autotune": tuned,
                        "arrivals": "Poisson, worlds uniform", "parallelism": "replicas"},
             "served": points,
             "one_at_a_time": base,
@@ -516,6 +527,12 @@ def run_served(args, rank, world_size, local_rank, dist, torch, emit=True):
         if emit:
             print(json.dumps(line), flush=True)
         return line
+
+
+def dtype_of(form):
+    """The arithmetic the form computes in: FP32 grids and vectors, FP64
+    dots; the mixed form stores its coarse operator in binary16."""
+    return "f16+f32+f64" if form == "mixed" else "f32+f64"
 
 
 def config_of(world, args):
@@ -547,6 +564,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--serve-max-requests", type=int, default=4000)
     ap.add_argument("--no-tune", action="store_true", help="the batched workload with the default launch shapes")
+    ap.add_argument("--tune-served", action="store_true",
+                    help="tune the served workload's launch shapes on profiled steps of its resident worlds")
     ap.add_argument("--no-forms", action="store_true",
                     help="the single world alone, without the batched and served summaries a one-GPU run adds")
     args = ap.parse_args()
@@ -682,7 +701,7 @@ def main():
         line = {
             "metric": METRIC, "value": round(value, 3), "unit": "Mcells/s", "n_gpus": world_size,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype_of(args.form), "data": "synthetic",
             "config": config_of(world, args),
             "e2e": {"value": round(e2e, 3), "unit": "Mcells/s", "h2d_bytes_per_step": 152, "d2h_bytes_per_step": 64},
             "gpu_launches": launches_per_step * args.steps,
@@ -708,24 +727,31 @@ def main():
 
 def run_forms(args, rank, world_size, local_rank, dist, torch):
     """The one-GPU run's summaries of the batched and served forms, beside
-    the single world: each its own workload (run_batched, run_served), made
-    smaller in steps and rates so the whole run stays within minutes."""
+    the single world: each its own workload (run_batched, run_served), in
+    the mixed-precision form with tuned launch shapes, made smaller in steps
+    and rates so the whole run stays within minutes."""
     import argparse as ap_
+    global FLAGS
     out = {}
     b = ap_.Namespace(**vars(args))
-    b.worlds, b.steps, b.warmup, b.no_cpu, b.profile_steps = 512, 10, 3, True, 1
+    b.worlds, b.steps, b.warmup, b.no_cpu, b.profile_steps, b.form = 512, 10, 3, True, 1, "mixed"
     s = ap_.Namespace(**vars(args))
-    s.worlds, s.rates, s.no_cpu = 2000, "1000,2000,20000", True
-    for name, fn, a in (("batched", run_batched, b), ("served", run_served, s)):
-        try:
-            ln = fn(a, rank, world_size, local_rank, dist, torch, emit=False)
-            keep = ("value", "unit", "ms_per_step", "e2e", "config", "roofline", "solve", "served", "one_at_a_time",
-                    "gpu_launches", "clocks")
-            out[name] = {k: ln[k] for k in keep if k in ln}
-        except Exception as e:  # a form that cannot run here is reported, not fatal
-            out[name] = {"error": f"{type(e).__name__}: {e}"}
-        torch.cuda.synchronize()
-        torch.cuda.empty_cache()
+    s.worlds, s.rates, s.no_cpu, s.form = 2000, "1000,2000,20000", True, "mixed"
+    saved = FLAGS
+    FLAGS = abi.STEP_TOLERANCE | abi.STEP_F64_DOTS | abi.STEP_MIXED
+    try:
+        for name, fn, a in (("batched", run_batched, b), ("served", run_served, s)):
+            try:
+                ln = fn(a, rank, world_size, local_rank, dist, torch, emit=False)
+                keep = ("value", "unit", "ms_per_step", "e2e", "config", "roofline", "solve", "served",
+                        "one_at_a_time", "gpu_launches", "clocks")
+                out[name] = {k: ln[k] for k in keep if k in ln}
+            except Exception as e:  # a form that cannot run here is reported, not fatal
+                out[name] = {"error": f"{type(e).__name__}: {e}"}
+            torch.cuda.synchronize()
+            torch.cuda.empty_cache()
+    finally:
+        FLAGS = saved
     return out
 
 

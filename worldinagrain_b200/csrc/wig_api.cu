@@ -13,6 +13,7 @@
 // (js/sim.js:1975-1995, :1763, :1882-1900).
 
 #include <algorithm>
+#include <cmath>
 #include <array>
 #include <cstdio>
 #include <cstring>
@@ -109,6 +110,7 @@ struct Lane {
     uint64_t pool_bytes = 0;
     wig::Batch Bt{};
     wig::SchedCtl ctl{};
+    wig::BatchShape S{};           // the shape the lane's step records with (step_shape)
     std::map<uint64_t, Graph> graphs;
     cudaStream_t cap = nullptr, cap2 = nullptr;
     cudaStream_t last_stream = nullptr;
@@ -121,6 +123,7 @@ size_t align256(size_t x) { return (x + 255u) & ~(size_t)255u; }
 
 struct wig_batch {
     uint32_t K = 0;
+    uint64_t blocks_all = 0;  // the worlds' blocks, summed
     int device = 0;
     std::vector<wig_world_layout> L;
     std::vector<wig::World> hw;       // host copy of the world table
@@ -462,6 +465,7 @@ int make_batch(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, u
     }
     if (items_total > 0xffffffffull) return bail(WIG_E_ARG, "work lists too long");
     level_shape(b);
+    for (uint32_t k = 0; k < n; k++) b->blocks_all += b->hw[k].D.B;
     if (S.coarse_smem > 220u * 1024u) return bail(WIG_E_ARG, "coarse levels too large for one CTA");
     if (wig::fast_prepare_attributes(S.coarse_smem) != cudaSuccess) return bail(WIG_E_CUDA, "cudaFuncSetAttribute");
 
@@ -645,7 +649,7 @@ struct Rec {
         }
     }
     void run(int pass, uint32_t level = 0, uint32_t cycle = 0) {
-        timed(pass, [&] { wig::launch_pass(ln.Bt, b->S, b->hw[0].D, pass, level, cycle, s); });
+        timed(pass, [&] { wig::launch_pass(ln.Bt, ln.S, b->hw[0].D, pass, level, cycle, s); });
     }
     void norm(int which, uint32_t cycle) {
         timed(WIG_SLOT_NORM, [&] { wig::launch_norm(b->hw[0].D, which, cycle, s); });
@@ -657,7 +661,7 @@ struct Rec {
             cudaEventCreate(&e);
             cudaEventRecord(a, s);
         }
-        wig::sched_lists(ln.Bt, ln.ctl, b->S, phase, s);
+        wig::sched_lists(ln.Bt, ln.ctl, ln.S, phase, s);
         launches += 2;
         if (prof) {
             cudaEventRecord(e, s);
@@ -666,7 +670,7 @@ struct Rec {
     }
     void report() {
         timed(WIG_SLOT_REPORT, [&] {
-            k_report<<<wig::list_grid(b->S, wig::L_ONE_ALL, 4), 32, 0, s>>>(ln.Bt, b->d_report, ln.d_rsub);
+            k_report<<<wig::list_grid(ln.S, wig::L_ONE_ALL, 4), 32, 0, s>>>(ln.Bt, b->d_report, ln.d_rsub);
         });
     }
     // the fast form's marker hook: events around each of its launches
@@ -812,10 +816,10 @@ int record_step_fast(wig_batch* b, Lane& ln, uint32_t max_cycles, uint32_t flags
     ln.Bt.mixed = (flags & WIG_STEP_MIXED) ? 1u : 0u;
     const wig::World* one = b->K == 1 ? &b->hw[0] : nullptr;
     if (b->pooled) {
-        wig::fast_zero_idle(ln.Bt, b->S, s);
+        wig::fast_zero_idle(ln.Bt, ln.S, s);
         R.launches++;
     }
-    wig::fast_setup(ln.Bt, b->S, one, s, prof ? &mk : nullptr);
+    wig::fast_setup(ln.Bt, ln.S, one, s, prof ? &mk : nullptr);
     R.launches++;
     if (flags & WIG_STEP_PERSISTENT) {
         wig::Fast F0;
@@ -847,20 +851,20 @@ int record_step_fast(wig_batch* b, Lane& ln, uint32_t max_cycles, uint32_t flags
         CUDA_TRY(cudaStreamBeginCaptureToGraph(ln.cap2, bodyGraph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
         wig::Batch Bc = ln.Bt;
         Bc.cond = (unsigned long long)handle;
-        *body = wig::fast_cycle(Bc, b->S, one, ln.cap2, nullptr);
+        *body = wig::fast_cycle(Bc, ln.S, one, ln.cap2, nullptr);
         cudaGraph_t captured = nullptr;
         CUDA_TRY(cudaStreamEndCapture(ln.cap2, &captured));
     } else {
         uint32_t* cont = reinterpret_cast<uint32_t*>(ln.h_rsub);  // a word of pinned scratch
         for (uint32_t c = 0; c < max_cycles; c++) {
-            R.launches += wig::fast_cycle(ln.Bt, b->S, one, s, prof ? &mk : nullptr);
+            R.launches += wig::fast_cycle(ln.Bt, ln.S, one, s, prof ? &mk : nullptr);
             CUDA_TRY(cudaMemcpyAsync(cont, ln.d_loop, sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
             CUDA_TRY(cudaStreamSynchronize(s));
             if (!*cont) break;
         }
         *body = 0;
     }
-    wig::fast_finish(ln.Bt, b->S, one, (flags & WIG_STEP_PERSISTENT) == 0u, s, prof ? &mk : nullptr);
+    wig::fast_finish(ln.Bt, ln.S, one, (flags & WIG_STEP_PERSISTENT) == 0u, s, prof ? &mk : nullptr);
     R.launches++;
     record_post(R);
     *outside = R.launches;
@@ -988,6 +992,27 @@ void zero_dirty(wig_batch* b, const StepArgs& a) {
     }
 }
 
+// The shape a step records with: every list's grid sized for the step's
+// worlds rather than the whole batch's, by their blocks rounded up to a
+// power of two (`bucket`, part of the graph's key) against all the
+// batch's blocks, so a small step of a large batch launches no idle CTAs
+// by the thousand.  A grid's size changes no result.
+wig::BatchShape step_shape(const wig_batch* b, const StepArgs& a, uint32_t* bucket) {
+    wig::BatchShape S = b->S;
+    uint64_t blocks = 0;
+    for (uint32_t i = 0; i < a.count; i++) blocks += b->hw[a.worlds[i]].D.B;
+    uint32_t e = 0;
+    while (e < 48u && (1ull << e) < blocks) e++;
+    *bucket = e;
+    const double f = (double)(1ull << e) / (double)std::max<uint64_t>(b->blocks_all, 1);
+    if (f < 1.0) {
+        for (uint32_t l = 0; l < wig::L_COUNT; l++)
+            S.max_items[l] = (uint32_t)std::max(1.0, std::ceil((double)S.max_items[l] * f));
+        S.worlds = (uint32_t)std::max(1.0, std::ceil((double)S.worlds * f));
+    }
+    return S;
+}
+
 int batch_step(wig_batch* b, const StepArgs& a) {
     int rc = check_step(b, a);
     if (rc) return rc;
@@ -1002,7 +1027,10 @@ int batch_step(wig_batch* b, const StepArgs& a) {
     if (viscous) shape |= WIG_STEP_VISCOUS;
     if (book1) shape |= WIG_STEP_BOOKKEEPING_ONLY;
     const bool parity_keyed = plain || (a.flags & WIG_STEP_PERSISTENT);
-    const uint64_t key = ((uint64_t)a.max_cycles << 32) | ((uint64_t)shape << 1) | ((parity_keyed && sh) ? 1u : 0u);
+    uint32_t bucket = 0;
+    ln.S = step_shape(b, a, &bucket);
+    const uint64_t key = ((uint64_t)a.max_cycles << 32) | ((uint64_t)bucket << 24) | ((uint64_t)shape << 1) |
+                         ((parity_keyed && sh) ? 1u : 0u);
     auto it = ln.graphs.find(key);
     if (it == ln.graphs.end()) {
         Graph G;
@@ -1059,6 +1087,8 @@ int batch_step_profile(wig_batch* b, const StepArgs& a, float* ms_out, uint32_t*
     if (book1) shape |= WIG_STEP_BOOKKEEPING_ONLY;
     Prof prof;
     ln.last_body = 0;
+    uint32_t bucket = 0;
+    ln.S = step_shape(b, a, &bucket);
     if (plain) {
         ln.last_launches = record_step(b, ln, a.max_cycles, shape, sh, a.s, &prof);
     } else {

@@ -1237,9 +1237,10 @@ __global__ void __launch_bounds__(256) k_fRhoBeta(Batch Bt, const __grid_constan
             I2 c = tileCell(w, wid);
             if (w.inWorld(c)) {
                 uint32_t i = w.cellIndex(c);
-                if (L0.rho[i] > 0.0f) {
-                    float z = L0.px[i];
-                    float r = F.R[i], q = F.Q[i];
+                // loaded beside the density, not after it: one dependent
+                // load fewer on the item's path
+                const float rho = L0.rho[i], z = L0.px[i], r = F.R[i], q = F.Q[i];
+                if (rho > 0.0f) {
                     vx = r * z;
                     vy = q * z;
                     ex = (double)r * (double)z;
@@ -1335,16 +1336,23 @@ __global__ void __launch_bounds__(256) k_fApplyAlpha(Batch Bt, const __grid_cons
             if (w.inWorld(c)) {
                 uint32_t i = w.cellIndex(c);
                 float p = 0.0f, q = 0.0f;
-                if (L0.rho[i] > 0.0f) {
-                    p = dir(i);
-                    const uint8_t m = F.fmask[i];
-                    const float b[4] = {L0.b0[i], L0.b1[i], L0.b2[i], L0.b3[i]};
+                // the cell's and its neighbours' words loaded beside the
+                // density (neighbour indices clamp onto the cell), not after
+                const float rho = L0.rho[i];
+                const uint8_t m = F.fmask[i];
+                const float b[4] = {L0.b0[i], L0.b1[i], L0.b2[i], L0.b3[i]};
+                const float dgp = L0.diag[i] + F.pin[i];
+                const float pi = dir(i);
+                float pn[4];
+#pragma unroll
+                for (int d = 0; d < 4; d++) pn[d] = dir(nbr(i, c.x, c.y, D.W, D.H, d));
+                if (rho > 0.0f) {
+                    p = pi;
                     float sum = 0.0f;
 #pragma unroll
                     for (int d = 0; d < 4; d++)
-                        if (m & (1u << d)) sum = sum + b[d] * dir(nbr(i, c.x, c.y, D.W, D.H, d));
-                    float dg = L0.diag[i] + F.pin[i];
-                    q = dg * p - sum + 0.0f;
+                        if (m & (1u << d)) sum = sum + b[d] * pn[d];
+                    q = dgp * p - sum + 0.0f;
                 }
                 Pnew[i] = p;
                 F.Q[i] = q;
@@ -1420,8 +1428,10 @@ __global__ void __launch_bounds__(256) k_fUpdate(Batch Bt, const __grid_constant
             I2 c = tileCell(w, wid);
             if (w.inWorld(c)) {
                 uint32_t i = w.cellIndex(c);
-                if (L0.rho[i] > 0.0f) {
-                    float vx = F.X[i], vy = F.R[i], vz = ((cycle & 1u) ? F.P : F.P2)[i], vw = F.Q[i];
+                // loaded beside the density, not after it
+                const float rho = L0.rho[i], vx = F.X[i], vy = F.R[i], vz = ((cycle & 1u) ? F.P : F.P2)[i];
+                const float vw = F.Q[i], py = L0.py[i];
+                if (rho > 0.0f) {
                     float r, x;
                     if (f64) {
                         r = (float)((double)vy - alpha64 * (double)vw);
@@ -1435,7 +1445,7 @@ __global__ void __launch_bounds__(256) k_fUpdate(Batch Bt, const __grid_constant
                     L0.px[i] = 0.0f;
                     L0.rx[i] = -r;
                     F.rimx[i] = 0.0f;
-                    F.rimy[i] = L0.py[i];
+                    F.rimy[i] = py;
                     m = __float_as_uint(fabsf(r));
                     r2 = (double)r * (double)r;
                 }

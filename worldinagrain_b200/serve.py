@@ -150,10 +150,9 @@ class GpuBackend:
         self.fluid.check(self.fluid.lib().wig_batch_evict(self.h, k, C.c_void_p(self.streams[0].cuda_stream)),
                          "wig_batch_evict")
 
-    def launch(self, lane, ids):
-        """One batched step of worlds `ids` on `lane`; returns a token."""
-        n = len(ids)
-        P = (abi.Params * n)()
+    def _next_params(self, ids):
+        """The next step's Params of worlds `ids` (their frames advanced)."""
+        P = (abi.Params * len(ids))()
         for i, k in enumerate(ids):
             self.frames[k] += 1
             w = self.worlds[k]
@@ -164,6 +163,12 @@ class GpuBackend:
             p.dx = 1.0
             p.earth_g = w.config["earth_g"]
             p.dt = 1.0 / 120.0
+        return P
+
+    def launch(self, lane, ids):
+        """One batched step of worlds `ids` on `lane`; returns a token."""
+        n = len(ids)
+        P = self._next_params(ids)
         ids_a = (C.c_uint32 * n)(*ids)
         stream = self.streams[lane]
         self.fluid.check(self.fluid.lib().wig_batch_step(self.h, lane, ids_a, n, P, None, self.max_cycles, self.flags,
@@ -175,6 +180,47 @@ class GpuBackend:
 
     def done(self, token):
         return token.query()
+
+    # -- launch shapes (tune.autotune's interface)
+    def get_launch(self, knob):
+        v = C.c_uint32()
+        self.fluid.check(self.fluid.lib().wig_batch_get_launch(self.h, abi.LAUNCH_KNOBS[knob], C.byref(v)),
+                         "wig_batch_get_launch")
+        return v.value
+
+    def set_launch(self, knob, value):
+        self.torch.cuda.synchronize()
+        self.fluid.check(self.fluid.lib().wig_batch_set_launch(self.h, abi.LAUNCH_KNOBS[knob], int(value)),
+                         "wig_batch_set_launch")
+
+    def launch_shapes(self):
+        return {name: self.get_launch(name) for name in abi.LAUNCH_KNOBS}
+
+    def autotune(self, resident, lane=0):
+        """Tunes the batch's launch shapes (tune.autotune) on profiled steps
+        of resident worlds, as many as one lane's pool takes; those worlds
+        step as they would in service. Returns the shapes and the trials."""
+        from . import tune
+        ids, used = [], 0
+        for k in resident:
+            b = self.step_bytes_[k]
+            if self.pool is not None and used + b > self.pool:
+                continue
+            ids.append(k)
+            used += b
+        ms = (C.c_float * abi.PROFILE_SLOTS)()
+        calls = (C.c_uint32 * abi.PROFILE_SLOTS)()
+        ids_a = (C.c_uint32 * len(ids))(*ids)
+        stream = self.streams[lane]
+
+        def prof_step():
+            P = self._next_params(ids)
+            self.fluid.check(self.fluid.lib().wig_batch_step_profile(
+                self.h, lane, ids_a, len(ids), P, None, self.max_cycles, self.flags, self.tolerance,
+                C.c_void_p(stream.cuda_stream), ms, calls), "wig_batch_step_profile")
+            return {abi.PROFILE_NAMES[k]: (ms[k], calls[k]) for k in range(abi.PROFILE_SLOTS) if calls[k]}
+
+        return tune.autotune(self, prof_step)
 
     def stats(self, ids):
         out = (abi.Stats * len(ids))()
