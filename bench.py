@@ -470,7 +470,7 @@ def run_served(args, rank, world_size, local_rank, dist, torch, emit=True):
     # launch shapes tuned on profiled steps of the resident worlds (as many
     # as a lane's pool takes), then graphs captured and first steps seeded
     tuned = None
-    if args.tune_served:
+    if not args.no_tune:
         from worldinagrain_b200 import tune
         shapes, trials = be.autotune(list(srv.resident))
         tuned = {"shapes": shapes, "steps": tune.steps_needed(),
@@ -563,9 +563,7 @@ def main():
     ap.add_argument("--pool-gb", type=float, default=7.0)
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--serve-max-requests", type=int, default=4000)
-    ap.add_argument("--no-tune", action="store_true", help="the batched workload with the default launch shapes")
-    ap.add_argument("--tune-served", action="store_true",
-                    help="tune the served workload's launch shapes on profiled steps of its resident worlds")
+    ap.add_argument("--no-tune", action="store_true", help="the default launch shapes, not the autotuner's")
     ap.add_argument("--no-forms", action="store_true",
                     help="the single world alone, without the batched and served summaries a one-GPU run adds")
     args = ap.parse_args()
@@ -614,6 +612,22 @@ def main():
         return FLAGS | abi.STEP_SHIFTED_SET | (abi.STEP_SHIFTED_FIRST if step % 2 else 0)
 
     step_no = 0
+    # the fast forms' launch shapes tuned on the world's first steps
+    # (profiled steps of its own trajectory: no result changes)
+    tuned = None
+    if not args.no_tune and args.form in ("fast", "mixed"):
+        from worldinagrain_b200 import tune
+
+        def prof_step():
+            nonlocal step_no
+            step_no += 1
+            return g.step_profile(params(world, step_no, args.seed), max_cycles=MAX_CYCLES, flags=flags_of(step_no),
+                                  tolerance=TOL)
+
+        shapes, trials = tune.autotune(g, prof_step)
+        tuned = {"shapes": shapes, "steps": tune.steps_needed(),
+                 "trials_ms_per_iteration": {k: [[v, None if c is None else round(c, 4)] for v, c in r]
+                                             for k, r in trials.items()}}
     for _ in range(args.warmup):
         step_no += 1
         g.step(params(world, step_no, args.seed), max_cycles=MAX_CYCLES, flags=flags_of(step_no), tolerance=TOL)
@@ -702,7 +716,7 @@ def main():
             "metric": METRIC, "value": round(value, 3), "unit": "Mcells/s", "n_gpus": world_size,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms / args.steps, 4),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": dtype_of(args.form), "data": "synthetic",
-            "config": config_of(world, args),
+            "config": dict(config_of(world, args), launch=g.launch_shapes(), autotune=tuned),
             "e2e": {"value": round(e2e, 3), "unit": "Mcells/s", "h2d_bytes_per_step": 152, "d2h_bytes_per_step": 64},
             "gpu_launches": launches_per_step * args.steps,
             "roofline": {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak,

@@ -322,6 +322,11 @@ enum wig_profile_slot {
 int wig_fluid_step_profile(wig_fluid* h, const wig_params* P, uint32_t max_cycles, uint32_t flags, double tolerance,
                            void* stream, float* ms_out, uint32_t* calls_out);
 
+/* The fast form's launch shapes of this world (knob: enum wig_launch_knob of
+ * wig_batch.h, the same values and ranges): none changes a result. */
+int wig_fluid_set_launch(wig_fluid* h, uint32_t knob, uint32_t value);
+int wig_fluid_get_launch(const wig_fluid* h, uint32_t knob, uint32_t* value);
+
 /* Replaces readReport (js/sim.js:1882-1900): waits for the stream and reads
  * the FLUID_COUNT words and the solve's statistics of the last step. */
 int wig_fluid_read_stats(wig_fluid* h, wig_fluid_stats* out);

@@ -64,3 +64,39 @@ def test_served_worlds_match_stepping_alone(pooled):
         d = compare_worlds(w, ref, grid=grid, particles=("sorted",), region_links=True, scratch=True)
         assert not d, f"world {k} ({counts[k]} steps): {d}"
     be.close()
+
+
+@pytest.mark.parametrize("pooled", [False, True])
+def test_launch_shape_changes_between_served_steps(pooled):
+    """Launch shapes changed twice between requests (the coarse kernel's depth
+    among them, worlds with levels above it included): every world still
+    ends as stepping it alone."""
+    from worldinagrain_b200 import fluid
+    base = _worlds()[:5] + [W.dam_break(256, 256, seed=3), W.dam_break(160, 128, seed=4)]
+    mine = [w.copy() for w in base]
+    sizes = [fluid.world_bytes(w.W, w.H, w.L["liquid_per_cell"], w.cap) for w in mine]
+    be = serve.GpuBackend(mine, W.element_table(), FLAGS, 64, 1e-6, pool_bytes=3 * max(sizes) if pooled else None)
+    srv = serve.Server(be, len(mine), sum(be.bytes))
+    srv.preload()
+    counts = [0] * len(mine)
+    phases = ({"coarse_cells": 1024, "level_per_sm": 2, "cg_per_sm": 3, "relax_per_sm": 5},
+              {"coarse_cells": 4096, "level_per_sm": 8, "cg_per_sm": 8, "relax_per_sm": 16}, None)
+    for i, shapes in enumerate(phases):
+        arr = serve.poisson_arrivals(rate=400.0, n_requests=20, n_worlds=len(mine), seed=11 + i)
+        assert len(srv.run(arr)) == 20
+        for _, k in arr:
+            counts[k] += 1
+        if shapes:
+            for name, v in shapes.items():
+                be.set_launch(name, v)
+    for k in list(srv.resident):
+        be.fetch(k)
+    grid = ("cells", "counters", "field", "blocks") if pooled else ("cells", "counters", "field", "blocks", "cg")
+    for k, w in enumerate(mine):
+        ref = _alone(base[k], counts[k])
+        if pooled:
+            n = 4 * (2 * w.C + w.L["face_count"] + 2 * ((w.L["face_count"] + 3) // 4))
+            w.field[n:] = ref.field[n:]
+        d = compare_worlds(w, ref, grid=grid, particles=("sorted",), region_links=True, scratch=True)
+        assert not d, f"world {k} ({counts[k]} steps): {d}"
+    be.close()

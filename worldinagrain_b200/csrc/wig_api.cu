@@ -1310,6 +1310,16 @@ int wig_fluid_step_profile(wig_fluid* h, const wig_params* P, uint32_t max_cycle
     return batch_step_profile(h->b, a, ms_out, calls_out);
 }
 
+int wig_fluid_set_launch(wig_fluid* h, uint32_t knob, uint32_t value) {
+    if (!h || !h->b) return fail(WIG_E_ARG, "null handle");
+    return wig_batch_set_launch(h->b, knob, value);
+}
+
+int wig_fluid_get_launch(const wig_fluid* h, uint32_t knob, uint32_t* value) {
+    if (!h || !h->b) return fail(WIG_E_ARG, "null handle");
+    return wig_batch_get_launch(h->b, knob, value);
+}
+
 int wig_fluid_read_stats(wig_fluid* h, wig_fluid_stats* out) {
     if (!h || !h->b) return fail(WIG_E_ARG, "null argument");
     const uint32_t w0 = 0;

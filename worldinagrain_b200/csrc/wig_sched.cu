@@ -19,9 +19,12 @@ namespace {
 
 __device__ __forceinline__ uint32_t cdiv(uint32_t a, uint32_t b) { return (a + b - 1u) / b; }
 
-// The units world k (entry s of the step's subset) has in list L.
+// The units world k (entry s of the step's subset) has in list L: its
+// shape from this step's entry in a pooled batch (the lane's table holds its
+// last step's entry until k_schedFill copies this one in, and a world's
+// coarse level may have changed since), else from the batch's table.
 __device__ uint32_t unitsOf(const Batch& Bt, const SchedCtl& c, uint32_t s, uint32_t L) {
-    const World& Wd = Bt.worlds[c.sub[s]];
+    const World& Wd = c.entries ? c.entries[s] : Bt.worlds[c.sub[s]];
     const Dev& D = Wd.D;
     const bool book = (c.heads ? c.heads[s].book : D.st->book) != 0u;
     // the blocks' counts as compact left them, held to the world's blocks
@@ -122,8 +125,8 @@ __global__ void __launch_bounds__(256) k_schedFill(Batch Bt, SchedCtl c, int pha
             st->bar_gen = 0u;
         }
         if (phase == 0 && c.entries && q == 0u) {
-            // the world's table entry for this step (the scan above read only
-            // its shape and persistent buffers, the same in every entry)
+            // the world's table entry for this step (the scan above read it
+            // from the entries)
             const uint4* src = reinterpret_cast<const uint4*>(&c.entries[s]);
             uint4* dst = reinterpret_cast<uint4*>(&c.table[k]);
             for (uint32_t i = threadIdx.x; i < sizeof(World) / 16u; i += blockDim.x) dst[i] = src[i];

@@ -47,6 +47,8 @@ FUNCS = {
                                 C.POINTER(C.c_float), C.POINTER(C.c_uint32)], C.c_int),
     "wig_batch_destroy": ([C.c_void_p], None),
     "wig_batch_set_launch": ([C.c_void_p, C.c_uint32, C.c_uint32], C.c_int),
+    "wig_fluid_set_launch": ([C.c_void_p, C.c_uint32, C.c_uint32], C.c_int),
+    "wig_fluid_get_launch": ([C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)], C.c_int),
     "wig_batch_get_launch": ([C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)], C.c_int),
 }
 
@@ -138,6 +140,21 @@ class LiquidStep:
         check(lib().wig_fluid_step_profile(self.h, C.byref(P), max_cycles, flags, tolerance, self.stream, ms, calls),
               "wig_fluid_step_profile")
         return {abi.PROFILE_NAMES[k]: (ms[k], calls[k]) for k in range(abi.PROFILE_SLOTS) if calls[k]}
+
+    def set_launch(self, knob, value):
+        """One launch shape of the fast form (abi.LAUNCH_KNOBS); no result
+        changes."""
+        k = abi.LAUNCH_KNOBS.get(knob, knob)
+        check(lib().wig_fluid_set_launch(self.h, k, int(value)), f"wig_fluid_set_launch {knob}")
+
+    def get_launch(self, knob):
+        k = abi.LAUNCH_KNOBS.get(knob, knob)
+        v = C.c_uint32()
+        check(lib().wig_fluid_get_launch(self.h, k, C.byref(v)), f"wig_fluid_get_launch {knob}")
+        return v.value
+
+    def launch_shapes(self):
+        return {name: self.get_launch(name) for name in abi.LAUNCH_KNOBS}
 
     def dispatch(self, P, name, level=0, cycle=0):
         check(lib().wig_fluid_dispatch(self.h, C.byref(P), abi.PASS[name], level, cycle, self.stream), f"dispatch {name}")
