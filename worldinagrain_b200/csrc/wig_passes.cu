@@ -548,7 +548,46 @@ __global__ void k_clear(Batch Bt) {
 // ================================================================ splat
 
 // splatAxis (fluid.wgsl:1000-1015)
-__device__ __forceinline__ void splatAxis(const W& w, float sx, float sy, float vel, float gx, float gy, bool isU) {
+// Where the splat's fixed-point adds go.  DirectSink: global atomics, a site
+// at a time.  WinSink: a warp's window in shared memory, summed there and
+// added to the global words once a site (WarpGather); the sums are
+// integers, so the words end as with every add made alone.
+struct DirectSink {
+    const W& w;
+    __device__ __forceinline__ void face(bool isU, I2 at, uint32_t a, uint32_t b) const {
+        uint32_t slot = w.sumSlot(w.faceIndex(at, isU));
+        atomicAdd(&w.D.counters[slot], a);
+        atomicAdd(&w.D.counters[slot + 1u], b);
+    }
+    __device__ __forceinline__ void cell(uint32_t g, I2 at, uint32_t v) const { atomicAdd(w.gwp(w.cellIndex(at), g), v); }
+};
+
+// A warp's window: the sites of (GWX + 1) x (GWY + 1) coordinates from
+// (x0, y0): per u face and v face its two sums, per cell its count, mass
+// and density words.
+constexpr int GWX = 16, GWY = 8, GWN = (GWX + 1) * (GWY + 1);
+struct GatherWin {
+    uint32_t u[2][GWN], v[2][GWN], c[3][GWN];
+};
+struct WinSink {
+    GatherWin& win;
+    int x0, y0;
+    __device__ __forceinline__ int at_(I2 at) const { return (at.y - y0) * (GWX + 1) + (at.x - x0); }
+    __device__ __forceinline__ void face(bool isU, I2 at, uint32_t a, uint32_t b) const {
+        const int e = at_(at);
+        uint32_t(*arr)[GWN] = isU ? win.u : win.v;
+        atomicAdd(&arr[0][e], a);
+        atomicAdd(&arr[1][e], b);
+    }
+    __device__ __forceinline__ void cell(uint32_t g, I2 at, uint32_t v) const {
+        atomicAdd(&win.c[g == G_COUNT ? 0 : g == G_MASS ? 1 : 2][at_(at)], v);
+    }
+};
+
+// splatAxis (fluid.wgsl:1041-1067): a face's fixed-point sums of v w and w.
+template <class Sink>
+__device__ __forceinline__ void splatAxis(const W& w, const Sink& k, float sx, float sy, float vel, float gx, float gy,
+                                          bool isU) {
     float fx0 = floorf(sx), fy0 = floorf(sy);
     int bx = f2i(fx0), by = f2i(fy0);
     float fx = sx - fx0, fy = sy - fy0;
@@ -558,10 +597,8 @@ __device__ __forceinline__ void splatAxis(const W& w, float sx, float sy, float 
         float wgt = (ox == 1 ? fx : 1.0f - fx) * (oy == 1 ? fy : 1.0f - fy);
         I2 at{bx + ox, by + oy};
         if (wgt <= 0.0f || !w.faceInWorld(at, isU)) continue;
-        uint32_t slot = w.sumSlot(w.faceIndex(at, isU));
         float there = vel + (gx * ((float)at.x - sx) + gy * ((float)at.y - sy));
-        atomicAdd(&w.D.counters[slot], (uint32_t)f2i(rnd_even(there * wgt * FIX)));
-        atomicAdd(&w.D.counters[slot + 1u], (uint32_t)f2i(rnd_even(wgt * FIX)));
+        k.face(isU, at, (uint32_t)f2i(rnd_even(there * wgt * FIX)), (uint32_t)f2i(rnd_even(wgt * FIX)));
     }
 }
 __device__ __forceinline__ bool walls(const W& w, I2 c) {
@@ -570,7 +607,8 @@ __device__ __forceinline__ bool walls(const W& w, I2 c) {
     return k == WIG_KIND_SOLID || k == WIG_KIND_POWDER;
 }
 // splatDensity (fluid.wgsl:1069-1087)
-__device__ __forceinline__ void splatDensity(const W& w, float px, float py, float room) {
+template <class Sink>
+__device__ __forceinline__ void splatDensity(const W& w, const Sink& k, float px, float py, float room) {
     float sx = px - 0.5f, sy = py - 0.5f;
     float fx0 = floorf(sx), fy0 = floorf(sy);
     int bx = f2i(fx0), by = f2i(fy0);
@@ -587,33 +625,103 @@ __device__ __forceinline__ void splatDensity(const W& w, float px, float py, flo
             else if (!walls(w, xy)) at = xy;
             else at = I2{-1, -1};
         }
-        if (w.inWorld(at) && wgt > 0.0f) atomicAdd(w.gwp(w.cellIndex(at), G_DENSITY), f2u(rnd_even(wgt * room * FIX)));
+        if (w.inWorld(at) && wgt > 0.0f) k.cell(G_DENSITY, at, f2u(rnd_even(wgt * room * FIX)));
     }
 }
 
-// gather (fluid.wgsl:1017-1039), no air bound: no air push.
-__device__ __forceinline__ void gatherOne(const Dev& D, const W& w, uint32_t chunk) {
-    uint32_t live = min(D.parts[0], D.cap);
-    uint32_t k = chunk * blockDim.x + threadIdx.x;
-    if (k >= live) return;
-    const uint4* it = w.items(D.parts);
-    uint4 mo = it[k], stt = it[D.cap + k], af = it[2u * D.cap + k];
-    float px = __uint_as_float(mo.x), py = __uint_as_float(mo.y);
-    float vx = __uint_as_float(mo.z), vy = __uint_as_float(mo.w);
-    float temp = __uint_as_float(stt.y);
-    splatAxis(w, px - 0.0f, py - 0.5f, vx, __uint_as_float(af.x), __uint_as_float(af.y), true);
-    splatAxis(w, px - 0.5f, py - 0.0f, vy, __uint_as_float(af.z), __uint_as_float(af.w), false);
-    uint32_t home = w.cellIndex(w.cellOf(px, py));
-    atomicAdd(w.gwp(home, G_COUNT), 1u);
-    atomicAdd(w.gwp(home, G_MASS), f2u(rnd_even(w.liquidDensity(stt.x, temp) * FIX)));
-    splatDensity(w, px, py, w.liquidVolume(stt.x, temp));
+// gather (fluid.wgsl:1017-1039) of one particle, no air bound: no air push.
+struct GatherIn {
+    float px, py, vx, vy, temp;
+    uint4 stt, af;
+};
+template <class Sink>
+__device__ __forceinline__ void gatherTo(const W& w, const Sink& k, const GatherIn& p) {
+    splatAxis(w, k, p.px - 0.0f, p.py - 0.5f, p.vx, __uint_as_float(p.af.x), __uint_as_float(p.af.y), true);
+    splatAxis(w, k, p.px - 0.5f, p.py - 0.0f, p.vy, __uint_as_float(p.af.z), __uint_as_float(p.af.w), false);
+    const I2 home = w.cellOf(p.px, p.py);
+    k.cell(G_COUNT, home, 1u);
+    k.cell(G_MASS, home, f2u(rnd_even(w.liquidDensity(p.stt.x, p.temp) * FIX)));
+    splatDensity(w, k, p.px, p.py, w.liquidVolume(p.stt.x, p.temp));
 }
-__global__ void k_gather(Batch Bt) {
+
+// A warp's 32 particles of `parts` (in cell order, so mostly a few
+// neighbouring cells): when every site they add to fits one window, summed
+// there and flushed once a site; else each particle's adds straight to the
+// global words.
+__device__ __forceinline__ void gatherWarp(const Dev& D, const W& w, uint32_t k, GatherWin& win) {
+    const uint32_t live = min(D.parts[0], D.cap);
+    const bool has = k < live;
+    GatherIn p{};
+    int lx = 0x3fffffff, ly = 0x3fffffff, hx = -0x3fffffff, hy = -0x3fffffff;
+    if (has) {
+        const uint4* it = w.items(D.parts);
+        const uint4 mo = it[k];
+        p.stt = it[D.cap + k];
+        p.af = it[2u * D.cap + k];
+        p.px = __uint_as_float(mo.x);
+        p.py = __uint_as_float(mo.y);
+        p.vx = __uint_as_float(mo.z);
+        p.vy = __uint_as_float(mo.w);
+        p.temp = __uint_as_float(p.stt.y);
+        // the sites' coordinates: x from floor(px - 1/2) to floor(px) + 1,
+        // y likewise, and the (clamped) home cell; a position far outside
+        // any world (or not a number) sends the warp the direct way
+        if (fabsf(p.px) < 1.0e6f && fabsf(p.py) < 1.0e6f) {
+            const I2 home = w.cellOf(p.px, p.py);
+            lx = min(f2i(floorf(p.px - 0.5f)), home.x);
+            ly = min(f2i(floorf(p.py - 0.5f)), home.y);
+            hx = max(f2i(floorf(p.px)) + 1, home.x);
+            hy = max(f2i(floorf(p.py)) + 1, home.y);
+        } else {
+            lx = ly = -0x3fffffff;
+            hx = hy = 0x3fffffff;
+        }
+    }
+    const int x0 = __reduce_min_sync(0xffffffffu, lx), y0 = __reduce_min_sync(0xffffffffu, ly);
+    const int x1 = __reduce_max_sync(0xffffffffu, hx), y1 = __reduce_max_sync(0xffffffffu, hy);
+    if (x1 - x0 > GWX || y1 - y0 > GWY) {  // (warp-uniform; none here: x1 < x0)
+        if (has) gatherTo(w, DirectSink{w}, p);
+        return;
+    }
+    if (has) gatherTo(w, WinSink{win, x0, y0}, p);
+    __syncwarp();
+    const uint32_t lane = threadIdx.x & 31u;
+    for (uint32_t e = lane; e < (uint32_t)GWN; e += 32u) {
+        const I2 at{x0 + (int)(e % (GWX + 1)), y0 + (int)(e / (GWX + 1))};
+        for (int isU = 1; isU >= 0; isU--) {
+            uint32_t(*arr)[GWN] = isU ? win.u : win.v;
+            const uint32_t a = arr[0][e], b = arr[1][e];
+            if ((a | b) == 0u) continue;
+            arr[0][e] = 0u;
+            arr[1][e] = 0u;
+            const uint32_t slot = w.sumSlot(w.faceIndex(at, isU != 0));
+            atomicAdd(&D.counters[slot], a);
+            atomicAdd(&D.counters[slot + 1u], b);
+        }
+        const uint32_t g3[3] = {G_COUNT, G_MASS, G_DENSITY};
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const uint32_t v = win.c[j][e];
+            if (v == 0u) continue;
+            win.c[j][e] = 0u;
+            atomicAdd(w.gwp(w.cellIndex(at), g3[j]), v);
+        }
+    }
+    __syncwarp();
+}
+__global__ void __launch_bounds__(256) k_gather(Batch Bt) {
     __shared__ WorldCopy wc_;
+    __shared__ GatherWin win_[8];
     worldCopyInit(wc_);
+    GatherWin& win = win_[threadIdx.x >> 5];
+    {
+        uint32_t* z = &win.u[0][0];
+        for (uint32_t i = threadIdx.x & 31u; i < sizeof(GatherWin) / 4u; i += 32u) z[i] = 0u;
+        __syncwarp();
+    }
     FOR_ITEMS(Bt, L_PP, qi) {
         ITEM_WORLD_C(Bt, qi, D, w, chunk);
-        gatherOne(D, w, chunk);
+        gatherWarp(D, w, chunk * blockDim.x + threadIdx.x, win);
     }
 }
 
