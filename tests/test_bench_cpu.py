@@ -1,0 +1,54 @@
+"""bench.py's bookkeeping on the CPU: the byte models behind the roofline
+figures, the arithmetic a form reports, the reference arm's core count, and
+one bounded run of the reference arm on a small world."""
+import json
+import os
+import subprocess
+import sys
+
+import bench
+from worldinagrain_b200 import abi
+
+
+def test_level_byte_models():
+    s = {"levels": [(262144, "smooth"), (65536, "smooth"), (16384, "restrict")]}
+    # down: 180 B a cell averaged over the levels restricted by tile kernels
+    assert bench.level_bytes("F_RESTRICT", s) == (180 * 262144 + 180 * 65536 + 180 * 16384) // 3
+    # up: 51 B a cell over the levels above the coarse kernel's
+    assert bench.level_bytes("F_PROLONG", s) == (51 * 262144 + 51 * 65536) // 2
+    # the coarse kernel: 28 B a cell of its first level
+    assert bench.level_bytes("F_COARSE", s) == 28 * 16384
+    assert bench.level_bytes("F_RELAX", s) is None
+    assert bench.level_bytes("F_RESTRICT", {}) is None
+
+
+def test_algorithmic_bytes_of_the_cg_kernels():
+    s = {"active_cells": 640, "fluid_cells": 512, "particles": 2048, "levels": []}
+    assert bench.algorithmic_bytes("F_UPDATE", s) == 640 * 4 + 512 * (16 + 4 + 24)
+    assert bench.algorithmic_bytes("F_APPLY_ALPHA", s) == 640 * 12 + 512 * (8 + 4 + 16 + 8 + 1 + 4) + 128 * 8
+    assert bench.algorithmic_bytes("NO_SUCH_PASS", s) is None
+
+
+def test_form_arithmetic():
+    assert bench.dtype_of("mixed") == "f16+f32+f64"
+    assert bench.dtype_of("fast") == bench.dtype_of("plain") == "f32+f64"
+    assert bench.FLAGS & abi.STEP_TOLERANCE and bench.FLAGS & abi.STEP_F64_DOTS
+
+
+def test_reference_cores_bounded_by_memory_and_cap():
+    n = bench.reference_cores(1)
+    assert 1 <= n <= 64
+    assert bench.reference_cores(1 << 62) == 1  # no room for a second replica
+
+
+def test_reference_arm_prints_one_line(tmp_path):
+    env = dict(os.environ, PYTHONPATH=bench.ROOT)
+    out = subprocess.run([sys.executable, os.path.join(bench.ROOT, "bench.py"), "--impl", "reference", "--config",
+                          "dam", "--steps", "1", "--warmup", "1", "--cpu-budget", "1"],
+                         capture_output=True, text=True, timeout=600, env=env, cwd=str(tmp_path))
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d["impl"] == "reference" and d["value"] > 0 and d["cpu_baseline"]["cores"] >= 1
+    assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["value"] == d["value"]
