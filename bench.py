@@ -173,6 +173,27 @@ def level_stats(worlds):
     return [(cells[l], kind[l]) for l in sorted(cells)]
 
 
+# DRAM bytes (read + written) per algorithmic byte of a kernel, from one
+# `ncu --set full` capture each of the disks 1024x1024 world (the summaries
+# under profiles/ give the commands). roofline.traffic is this ratio times a
+# launch's algorithmic bytes: the capture's traffic scaled to the launch by
+# the units it processes.
+TRAFFIC_PER_ALG_BYTE = {
+    # k_fDown on level 1: 22.8 MB read, 256 B written; 262,144 cells x 180 B
+    "F_RESTRICT": ((22.8e6 + 256) / (262144 * 180), "k_fDown level 1 (512x512), k_fDown_level1_disks1024.md"),
+    # k_fRelax: 25.0 MB read, 0 written; 24.5 MB algorithmic
+    "F_RELAX": (25.0e6 / 24.5e6, "k_fRelax, k_fRelax_disks1024.md"),
+}
+
+
+def traffic_of(name, alg):
+    """(DRAM bytes a launch moves, where the figure comes from), or (None, None)."""
+    t = TRAFFIC_PER_ALG_BYTE.get(name)
+    if t is None or not alg:
+        return None, None
+    return int(round(t[0] * alg)), "ncu capture " + t[1] + ", scaled to this launch's algorithmic bytes"
+
+
 def algorithmic_bytes(name, s):
     A, Cf, N = s["active_cells"], s["fluid_cells"], s["particles"]
     lb = level_bytes(name, s)
@@ -465,7 +486,8 @@ def run_batched(args, rank, world_size, local_rank, dist, torch, emit=True):
             "e2e": {"value": round(e2e, 3), "unit": "Mcells/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches_per_step * args.steps,
             "roofline": {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic_of(top, alg)[0],
+                         "traffic_source": traffic_of(top, alg)[1],
                          "algorithmic_bytes_per_launch": alg, "launch_ms": round(per_launch_s * 1e3, 5)},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
@@ -758,7 +780,8 @@ def main():
             "e2e": {"value": round(e2e, 3), "unit": "Mcells/s", "h2d_bytes_per_step": 152, "d2h_bytes_per_step": 64},
             "gpu_launches": launches_per_step * args.steps,
             "roofline": {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": None,
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic_of(top, alg)[0],
+                         "traffic_source": traffic_of(top, alg)[1],
                          "algorithmic_bytes_per_launch": alg, "launch_ms": round(per_launch_s * 1e3, 5)},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),

@@ -29,6 +29,17 @@ def test_algorithmic_bytes_of_the_cg_kernels():
     assert bench.algorithmic_bytes("NO_SUCH_PASS", s) is None
 
 
+def test_traffic_scales_the_captured_ratio():
+    """roofline.traffic: a captured launch's DRAM bytes per algorithmic byte
+    times this launch's algorithmic bytes; none for kernels not captured."""
+    alg = 262144 * 180
+    t, src = bench.traffic_of("F_RESTRICT", alg)
+    assert abs(t - (22.8e6 + 256)) < 2 and "k_fDown" in src
+    assert bench.traffic_of("F_RESTRICT", alg // 2)[0] == round(t / 2)
+    assert bench.traffic_of("F_COARSE", 10 ** 6) == (None, None)
+    assert bench.traffic_of("F_RELAX", 0) == (None, None)
+
+
 def test_form_arithmetic():
     assert bench.dtype_of("mixed") == "f16+f32+f64"
     assert bench.dtype_of("fast") == bench.dtype_of("plain") == "f32+f64"

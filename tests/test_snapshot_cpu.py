@@ -45,7 +45,7 @@ def test_reference_shaped_snapshot_loads_and_saves_back():
               "state": {"cur": 1, "frameNo": 3, "shiftedFirst": False}}
     got = snapshot.load(snapshot.write(header, parts))
     assert np.array_equal(got.cells, w.cells)          # cells1: the current one
-    assert np.array_equal(got.cg, np.zeros_like(w.cg))  # fluidCg not kept: zero
+    assert not got.cg.any()  # the CG vectors are written before they are read: not a part
     again_h, again = snapshot.read(snapshot.save(got))
     assert np.array_equal(again["air"].view(np.uint32), air)  # outside the liquid: kept as it was
     assert np.array_equal(again["cells0"].view(np.uint32), w.cells)
@@ -69,12 +69,68 @@ def test_bad_files_are_refused():
     with pytest.raises(ValueError, match="cut short"):
         snapshot.read(_raw({"format": 1, "parts": [{"name": "x", "bytes": 64}]}, b"\0" * 8))
     header, parts = snapshot.read(snapshot.save(w))
-    parts["field"] = parts["field"][:-4]
-    with pytest.raises(ValueError, match="field"):
-        snapshot.world_from(header, parts)
-    del parts["counters"]
-    with pytest.raises(ValueError, match="counters"):
-        snapshot.world_from(header, parts)
+    bad = dict(parts, field=parts["field"][:-4])
+    with pytest.raises(ValueError, match="lays out field differently"):
+        snapshot.world_from(header, bad)
+    bad = {k: v for k, v in parts.items() if k != "particles0"}
+    with pytest.raises(ValueError, match="particles0"):
+        snapshot.world_from(header, bad)
+    other = W.World(40, 40)
+    before = other.cells.copy()
+    with pytest.raises(ValueError, match="48x40 world"):
+        snapshot.restore(other, header, parts)
+    assert np.array_equal(other.cells, before)  # nothing changed
+
+
+def test_particles_laid_out_otherwise_load_empty_with_the_liquid_undrawn():
+    """A snapshot whose particle buffers are of another capacity loads as
+    migrateLiquid has it: no particles, counters or blocks, its liquid cells
+    undrawn with the run word cleared, everything else as saved."""
+    w = _world()
+    from oracle.oracle import Oracle
+    o = Oracle(w, W.element_table())
+    for s in range(1, 3):
+        o.step(params(w, s))
+    header, parts = snapshot.read(snapshot.save(w))
+    parts["particles0"] = parts["particles0"][:-48]
+    parts["particles1"] = parts["particles1"][:-48]
+    got = snapshot.world_from(header, parts)
+    assert got.snapshot_migrated
+    for buf in ("sorted", "parts", "counters", "blocks"):
+        assert not getattr(got, buf).any(), buf
+    assert np.array_equal(got.field, w.field)
+    cw, gw = w.cell_view(), got.cell_view()
+    liquid = (cw[..., 0] & 0xFF) == abi.WATER
+    assert liquid.any() and (cw[liquid, 0] >> 28 & 4).any()
+    assert not (gw[liquid, 0] >> 28 & 4).any() and not gw[liquid, 3].any()
+    assert np.array_equal(gw[liquid, 0] | (4 << 28), cw[liquid, 0] | (4 << 28))
+    assert np.array_equal(gw[~liquid], cw[~liquid])
+    b = Oracle(got, W.element_table())
+    b.step(params(got, 3), flags=snapshot.step_flags(got))
+    assert got.sorted[0] >= 4 * liquid.sum() * 0.9  # the liquid seeded afresh
+
+
+def test_older_blocks_and_field_are_widened_with_zeros():
+    w = _world()
+    w.blocks[:] = np.arange(w.blocks.size, dtype=np.uint32) + 1
+    w.field[:] = np.arange(w.field.size, dtype=np.float32) + 1
+    header, parts = snapshot.read(snapshot.save(w))
+    B, F = w.L["block_count"], w.L["face_count"]
+    at = 4 * B + 4
+    blocks = parts["blocks"].view(np.uint32)
+    parts["blocks"] = np.concatenate([blocks[:at], blocks[at + abi.FLUID_STATS - 4:]]).view(np.uint8)
+    q = (F + 3) // 4 * 4
+    f0 = w.C * 8 + F * 4 + q
+    field = parts["field"].view(np.float32)
+    parts["field"] = np.concatenate([field[:f0], field[f0 + q:]]).view(np.uint8)
+    got = snapshot.world_from(header, parts)
+    assert not got.snapshot_migrated
+    want = w.blocks.copy()
+    want[at:at + abi.FLUID_STATS - 4] = 0
+    assert np.array_equal(got.blocks, want)
+    want = w.field.copy()
+    want[f0:f0 + q] = 0
+    assert np.array_equal(got.field, want)
 
 
 def test_loaded_world_steps_on_as_the_saved_one():

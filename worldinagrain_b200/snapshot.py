@@ -12,18 +12,32 @@ A snapshot is gzipped (js/snapshot.js:4-8, :127-156, :163-189):
 - each part's bytes in the header's order, each padded to 4.
 
 The parts are the GPU buffers that carry over from one step to the next
-(Simulation.snapshotParts, js/sim.js:1429-1438), a pair named name0 and
-name1. The liquid's are:
+(Simulation.snapshotParts, js/sim.js:1429-1438: what js/passes.js:161-182
+finds read before it is written), a pair named name0 and name1. The
+liquid's are:
 
 - cells0 and cells1, the state's `cur` the one the next step reads;
 - particles0 and particles1 (this library's sorted and parts);
-- counters, field, blocks;
-- fluidCg, when the snapshot keeps it.
+- counters, field, blocks.
 
-They are laid out as here, so they load as they are. As in the reference, a
-part of another size than this layout gives is refused, not misread
-(js/snapshot.js:9-12). A snapshot's other parts (air, heat, bodies, ...)
-are outside the liquid step: they are kept, untouched, and written back.
+The CG vectors (fluidCg) are not one: the liquid's pass writes them before
+it reads them (js/passes.js:83).
+
+They are laid out as here, so they load as they are. Loading follows
+restoreSnapshot (js/snapshot.js:510-548) for these parts:
+
+- a snapshot of another world size is refused;
+- one whose particles or counters are laid out otherwise (another
+  LIQUID_PER_CELL, an older layout) loads with no particles, its liquid
+  cells undrawn so that the next step seeds them afresh (migrateLiquid,
+  js/snapshot.js:335-373);
+- blocks from before the V-cycle's counts, and a field from before
+  viscosity's last sweep, are widened with zeros (migrateBlocks, :391-409;
+  migrateField, :448-470);
+- any other liquid part of another size is refused, with nothing changed.
+
+A snapshot's other parts (air, heat, bodies, ...) are outside the liquid
+step: they are kept, untouched, and written back.
 """
 import gzip
 import json
@@ -39,7 +53,12 @@ FORMAT = 1
 
 # this library's buffer name -> the reference's part name (cells: cells{cur})
 PART_OF = {"sorted": "particles0", "parts": "particles1", "counters": "counters", "field": "field",
-           "blocks": "blocks", "cg": "fluidCg"}
+           "blocks": "blocks"}
+# the parts dropped, to load empty, when the particles are laid out otherwise
+# (js/snapshot.js:61)
+LIQUID_PARTS = ("particles0", "particles1", "counters", "blocks")
+# the cell word's flags (js/shared.js:79-91)
+FLAG_SHIFT, FL_DRAWN = 28, 4
 
 
 def _align4(n):
@@ -90,44 +109,124 @@ def write(header, parts):
     return gzip.compress(bytes(out))
 
 
-def world_from(header, parts, liquid_per_cell=4):
-    """A World holding a snapshot's liquid: its size from the header, its
-    particle capacity from the particle parts, each buffer the part's bytes.
-    The snapshot's state (frame, tiling parity, iteration count, ...) is
-    kept as world.snapshot_state and its other parts as world.snapshot_rest.
-    Raises ValueError when a liquid part's size differs from this layout's."""
+def _liquid_types(elems):
+    """Per cell type id (8 bits), whether the element is a liquid."""
+    out = np.zeros(256, dtype=bool)
+    for i, e in enumerate(elems):
+        out[i] = e.kind == abi.KIND_LIQUID
+    return out
+
+
+def migrate_liquid(world, parts, elems):
+    """The parts with the liquid's left out, and its liquid cells undrawn
+    with their run word cleared, when particles0 or counters is laid out
+    otherwise than world's (js/snapshot.js:335-373). Returns (parts,
+    migrated)."""
+    saved, counters = parts.get("particles0"), parts.get("counters")
+    if saved is None or (saved.nbytes == world.sorted.nbytes and counters is not None
+                         and counters.nbytes == world.counters.nbytes):
+        return parts, False
+    out = {k: v for k, v in parts.items() if k not in LIQUID_PARTS}
+    liquid = _liquid_types(elems)
+    for name in ("cells0", "cells1"):
+        b = parts.get(name)
+        if b is None or b.nbytes < 16 * world.C or b.nbytes % 4:
+            continue
+        u = b.view(np.uint32).copy()
+        cell = u[: 4 * world.C].reshape(world.C, 4)
+        m = liquid[cell[:, 0] & 0xFF]
+        cell[m, 0] &= np.uint32(~(FL_DRAWN << FLAG_SHIFT) & 0xFFFFFFFF)
+        cell[m, 3] = 0
+        out[name] = u.view(np.uint8)
+    return out, True
+
+
+def migrate_blocks(world, parts):
+    """blocks saved with 4 count words after the block lists, not
+    FLUID_STATS: the V-cycle's words put in after them, zero
+    (js/snapshot.js:391-409)."""
+    saved = parts.get("blocks")
+    added = (abi.FLUID_STATS - 4) * 4
+    if saved is None or saved.nbytes != world.blocks.nbytes - added:
+        return parts
+    at = (4 * world.L["block_count"] + 4) * 4
+    grown = np.zeros(world.blocks.nbytes, dtype=np.uint8)
+    grown[:at] = saved[:at]
+    grown[at + added:] = saved[at:]
+    return dict(parts, blocks=grown)
+
+
+def migrate_field(world, parts):
+    """field saved without viscosity's last sweep per face (a quarter word a
+    face after the velocities before viscosity): put in, zero
+    (js/snapshot.js:448-470)."""
+    saved = parts.get("field")
+    F = world.L["face_count"]
+    quarter = (F + 3) // 4 * 16
+    if saved is None or saved.nbytes != world.field.nbytes - quarter:
+        return parts
+    at = world.C * 32 + F * 16 + quarter
+    grown = np.zeros(world.field.nbytes, dtype=np.uint8)
+    grown[:at] = saved[:at]
+    grown[at + quarter:] = saved[at:]
+    return dict(parts, field=grown)
+
+
+def restore(world, header, parts, elems=None):
+    """Load a snapshot (read's header and parts) into `world`, a World of its
+    size, as restoreSnapshot does for the liquid's parts
+    (js/snapshot.js:510-548). Raises ValueError, with world unchanged, when
+    the size differs or a liquid part doesn't fit. The snapshot's state
+    (frame, tiling parity, iteration count, ...) is kept as
+    world.snapshot_state and its other parts as world.snapshot_rest."""
     width, height = int(header["width"]), int(header["height"])
+    if (width, height) != (world.W, world.H):
+        raise ValueError(f"the snapshot is of a {width}x{height} world, this one is {world.W}x{world.H}")
     state = header.get("state", {})
     cur = int(state.get("cur", 0))
-    p0 = parts.get("particles0")
-    if p0 is None or p0.nbytes < 16 or (p0.nbytes - 16) % 48:
-        raise ValueError("the snapshot has no particle buffer of this layout")
-    cap = (p0.nbytes - 16) // 48
-    w = W.World(width, height, liquid_per_cell, cap)
+    elems = W.element_table() if elems is None else elems
+    parts, migrated = migrate_liquid(world, parts, elems)
+    parts = migrate_field(world, migrate_blocks(world, parts))
     names = dict(PART_OF, cells=f"cells{cur}")
+    misfits = []
     for buf, part in names.items():
-        dst = getattr(w, buf)
+        src = parts.get(part)
+        if src is None and migrated and part in LIQUID_PARTS:
+            continue
+        if src is None or src.nbytes != getattr(world, buf).nbytes:
+            misfits.append(part)
+    if misfits:
+        raise ValueError(f"saved by a version that lays out {', '.join(misfits)} differently")
+    for buf, part in names.items():
+        dst = getattr(world, buf)
         src = parts.get(part)
         if src is None:
-            if buf == "cg":  # not kept: cgStart writes it before any pass reads it
-                continue
-            raise ValueError(f"the snapshot has no {part}")
-        if src.nbytes != dst.nbytes:
-            raise ValueError(f"{part} is {src.nbytes} bytes; this layout's {buf} is {dst.nbytes}")
-        dst[:] = src.view(dst.dtype)
-    w.config = dict(workload="snapshot", grid=f"{width}x{height}", seed=0, earth_g=W.earth_g_cells())
-    w.snapshot_state = dict(state)
-    w.snapshot_elements = list(header.get("elements", []))
-    w.snapshot_rest = {k: v for k, v in parts.items()
-                       if k not in set(names.values()) and not (k.startswith("cells") and k[5:] in ("0", "1"))}
-    w.snapshot_other_cells = parts.get(f"cells{1 - cur}")
-    return w
+            dst[:] = 0
+        else:
+            dst[:] = src.view(dst.dtype)
+    world.cg[:] = 0
+    world.snapshot_state = dict(state)
+    world.snapshot_elements = list(header.get("elements", []))
+    kept = set(names.values()) | {"cells0", "cells1"} | set(LIQUID_PARTS)
+    world.snapshot_rest = {k: v for k, v in parts.items() if k not in kept}
+    world.snapshot_other_cells = parts.get(f"cells{1 - cur}")
+    world.snapshot_migrated = migrated
+    return world
 
 
-def load(data, liquid_per_cell=4):
+def world_from(header, parts, liquid_per_cell=4, capacity=0, elems=None):
+    """A World of the snapshot's size, with the reference's particle
+    capacity for it (or `capacity`), holding the snapshot's liquid
+    (restore)."""
+    w = W.World(int(header["width"]), int(header["height"]), liquid_per_cell, capacity)
+    w.config = dict(workload="snapshot", grid=f"{w.W}x{w.H}", seed=0, earth_g=W.earth_g_cells())
+    return restore(w, header, parts, elems)
+
+
+def load(data, liquid_per_cell=4, capacity=0, elems=None):
     """world_from(read(data))."""
     header, parts = read(data)
-    return world_from(header, parts, liquid_per_cell)
+    return world_from(header, parts, liquid_per_cell, capacity, elems)
 
 
 def save(world, state=None, elements=None):
