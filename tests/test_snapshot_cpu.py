@@ -41,8 +41,8 @@ def test_reference_shaped_snapshot_loads_and_saves_back():
     air = np.arange(100, dtype=np.uint32)
     parts = {"cells0": stale, "cells1": w.cells, "air": air, "particles0": w.sorted, "particles1": w.parts,
              "counters": w.counters, "field": w.field, "blocks": w.blocks}
-    header = {"format": 1, "width": 48, "height": 40, "elements": [0, 1, 2, 3, 4],
-              "state": {"cur": 1, "frameNo": 3, "shiftedFirst": False}}
+    header = {"format": 1, "width": 48, "height": 40, "elements": [0, 1, 2, 3, 4], "gas": 2, "bodies": 1,
+              "water": {"vapour20": 1.0}, "state": {"cur": 1, "frameNo": 3, "shiftedFirst": False}}
     got = snapshot.load(snapshot.write(header, parts))
     assert np.array_equal(got.cells, w.cells)          # cells1: the current one
     assert not got.cg.any()  # the CG vectors are written before they are read: not a part
@@ -51,6 +51,10 @@ def test_reference_shaped_snapshot_loads_and_saves_back():
     assert np.array_equal(again["cells0"].view(np.uint32), w.cells)
     assert np.array_equal(again["cells1"].view(np.uint32), stale)
     assert again_h["state"]["cur"] == 0 and again_h["elements"] == [0, 1, 2, 3, 4]
+    # the header keys the other parts' loaders read, written back as loaded
+    assert again_h["gas"] == 2 and again_h["bodies"] == 1 and again_h["water"] == {"vapour20": 1.0}
+    with pytest.raises(ValueError, match="different set of elements"):
+        snapshot.load(snapshot.write(header, parts), element_ids=[0, 1, 2, 3])
 
 
 def _raw(header, body=b""):

@@ -172,13 +172,19 @@ def migrate_field(world, parts):
     return dict(parts, field=grown)
 
 
-def restore(world, header, parts, elems=None):
+def restore(world, header, parts, elems=None, element_ids=None):
     """Load a snapshot (read's header and parts) into `world`, a World of its
     size, as restoreSnapshot does for the liquid's parts
-    (js/snapshot.js:510-548). Raises ValueError, with world unchanged, when
-    the size differs or a liquid part doesn't fit. The snapshot's state
-    (frame, tiling parity, iteration count, ...) is kept as
-    world.snapshot_state and its other parts as world.snapshot_rest."""
+    (js/snapshot.js:510-548). `elems` is the element table the cells' type
+    ids index (this library's by default); element_ids, when given, the
+    host's element ids in that order, which the snapshot's must equal
+    (js/snapshot.js:179-181). Raises ValueError, with world unchanged, when
+    the elements or the size differ or a liquid part doesn't fit. The
+    snapshot's state (frame, tiling parity, iteration count, ...) is kept as
+    world.snapshot_state, the rest of its header as world.snapshot_header
+    and its other parts as world.snapshot_rest."""
+    if element_ids is not None and list(header.get("elements", [])) != list(element_ids):
+        raise ValueError("saved with a different set of elements")
     width, height = int(header["width"]), int(header["height"])
     if (width, height) != (world.W, world.H):
         raise ValueError(f"the snapshot is of a {width}x{height} world, this one is {world.W}x{world.H}")
@@ -207,6 +213,7 @@ def restore(world, header, parts, elems=None):
     world.cg[:] = 0
     world.snapshot_state = dict(state)
     world.snapshot_elements = list(header.get("elements", []))
+    world.snapshot_header = {k: v for k, v in header.items() if k not in ("parts", "state")}
     kept = set(names.values()) | {"cells0", "cells1"} | set(LIQUID_PARTS)
     world.snapshot_rest = {k: v for k, v in parts.items() if k not in kept}
     world.snapshot_other_cells = parts.get(f"cells{1 - cur}")
@@ -214,26 +221,27 @@ def restore(world, header, parts, elems=None):
     return world
 
 
-def world_from(header, parts, liquid_per_cell=4, capacity=0, elems=None):
+def world_from(header, parts, liquid_per_cell=4, capacity=0, elems=None, element_ids=None):
     """A World of the snapshot's size, with the reference's particle
     capacity for it (or `capacity`), holding the snapshot's liquid
     (restore)."""
     w = W.World(int(header["width"]), int(header["height"]), liquid_per_cell, capacity)
     w.config = dict(workload="snapshot", grid=f"{w.W}x{w.H}", seed=0, earth_g=W.earth_g_cells())
-    return restore(w, header, parts, elems)
+    return restore(w, header, parts, elems, element_ids)
 
 
-def load(data, liquid_per_cell=4, capacity=0, elems=None):
+def load(data, liquid_per_cell=4, capacity=0, elems=None, element_ids=None):
     """world_from(read(data))."""
     header, parts = read(data)
-    return world_from(header, parts, liquid_per_cell, capacity, elems)
+    return world_from(header, parts, liquid_per_cell, capacity, elems, element_ids)
 
 
 def save(world, state=None, elements=None):
-    """A snapshot of `world`'s liquid (and the other parts it was loaded
-    with, unchanged): its cells as cells0 with `cur` 0 (the other cell
-    buffer as loaded, or a copy), the state as given (or as loaded, cur set
-    to 0), the elements as loaded (or ids 0..n-1 of this library's table)."""
+    """A snapshot of `world`'s liquid (and the other parts and header keys
+    it was loaded with, unchanged): its cells as cells0 with `cur` 0 (the
+    other cell buffer as loaded, or a copy), the state as given (or as
+    loaded, cur set to 0), the elements as loaded (or ids 0..n-1 of this
+    library's table)."""
     st = dict(getattr(world, "snapshot_state", {}) if state is None else state)
     st["cur"] = 0
     other = getattr(world, "snapshot_other_cells", None)
@@ -244,7 +252,8 @@ def save(world, state=None, elements=None):
     els = elements if elements is not None else getattr(world, "snapshot_elements", None)
     if els is None:
         els = list(range(len(W.element_table())))
-    header = {"format": FORMAT, "width": world.W, "height": world.H, "elements": els, "state": st}
+    header = dict(getattr(world, "snapshot_header", {}))
+    header.update(format=FORMAT, width=world.W, height=world.H, elements=els, state=st)
     return write(header, parts)
 
 

@@ -17,8 +17,8 @@ another, each given the choices made before it.
 
 KNOBS = (
     ("coarse_cells", (4096, 2048, 1024, 512), ("F_RESTRICT", "F_PROLONG", "F_COARSE")),
-    ("level_per_sm", (8, 16, 32), ("F_RESTRICT", "F_PROLONG")),
-    ("cg_per_sm", (8, 16, 32), ("F_RHO_BETA", "F_APPLY_ALPHA", "F_UPDATE")),
+    ("level_per_sm", (4, 8, 16, 32), ("F_RESTRICT", "F_PROLONG")),
+    ("cg_per_sm", (2, 4, 8, 16, 32), ("F_RHO_BETA", "F_APPLY_ALPHA", "F_UPDATE")),
     ("relax_per_sm", (16, 32, 64), ("F_RELAX",)),
 )
 
