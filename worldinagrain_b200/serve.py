@@ -29,7 +29,7 @@ from dataclasses import dataclass, field
 
 import numpy as np
 
-from . import abi
+from . import abi, snapshot
 
 
 @dataclass
@@ -74,7 +74,12 @@ class GpuBackend:
                     "wig_batch_create_deferred")
         self.h = h
         self.streams = [torch.cuda.Stream(), torch.cuda.Stream()]
-        self.frames = [0] * len(worlds)
+        # a world loaded from a snapshot (snapshot.load) holds a state: all of
+        # its buffers go up at its first admission, its frames count on from
+        # the saved one, and its first step sets the saved tiling parity
+        self.has_state = [hasattr(w, "snapshot_state") for w in worlds]
+        self.frames = [int(w.snapshot_state.get("frameNo", 0)) if s else 0 for w, s in zip(worlds, self.has_state)]
+        self.first_flags = [snapshot.step_flags(w) if s else 0 for w, s in zip(worlds, self.has_state)]
         self.pooled = pool_bytes is not None
         self.pool = pool_bytes
         split = [self._split(w) for w in worlds]
@@ -124,13 +129,13 @@ class GpuBackend:
 
     def admit(self, k):
         """Allocates world k on the device and uploads its host state (only
-        its cells when it has never stepped: the rest is zero, as the new
-        memory is)."""
+        its cells when it has never stepped and was not loaded from a
+        snapshot: the rest is zero, as the new memory is)."""
         L = self.fluid.lib()
         s = C.c_void_p(self.streams[0].cuda_stream)
         self.fluid.check(L.wig_batch_admit(self.h, k, s), "wig_batch_admit")
         w = self.worlds[k]
-        for which, name in (self.names if self.frames[k] else [(0, "cells")]):
+        for which, name in (self.names if self.has_state[k] else [(0, "cells")]):
             arr = np.ascontiguousarray(getattr(w, name))
             self.fluid.check(L.wig_batch_upload(self.h, k, which, arr.ctypes.data, 0, arr.nbytes, s), "upload")
 
@@ -155,6 +160,7 @@ class GpuBackend:
         P = (abi.Params * len(ids))()
         for i, k in enumerate(ids):
             self.frames[k] += 1
+            self.has_state[k] = True
             w = self.worlds[k]
             p = P[i]
             p.size[0], p.size[1] = w.W, w.H
@@ -165,13 +171,22 @@ class GpuBackend:
             p.dt = 1.0 / 120.0
         return P
 
+    def _world_flags(self, ids):
+        """The per-world flags of the next step of worlds `ids` (the saved
+        tiling parity of a snapshot's first step), or None when all are 0."""
+        wf = [self.first_flags[k] for k in ids]
+        for k in ids:
+            self.first_flags[k] = 0
+        return (C.c_uint32 * len(ids))(*wf) if any(wf) else None
+
     def launch(self, lane, ids):
         """One batched step of worlds `ids` on `lane`; returns a token."""
         n = len(ids)
+        wf_a = self._world_flags(ids)
         P = self._next_params(ids)
         ids_a = (C.c_uint32 * n)(*ids)
         stream = self.streams[lane]
-        self.fluid.check(self.fluid.lib().wig_batch_step(self.h, lane, ids_a, n, P, None, self.max_cycles, self.flags,
+        self.fluid.check(self.fluid.lib().wig_batch_step(self.h, lane, ids_a, n, P, wf_a, self.max_cycles, self.flags,
                                                          self.tolerance, C.c_void_p(stream.cuda_stream)),
                          "wig_batch_step")
         ev = self.torch.cuda.Event()
@@ -214,9 +229,10 @@ class GpuBackend:
         stream = self.streams[lane]
 
         def prof_step():
+            wf_a = self._world_flags(ids)
             P = self._next_params(ids)
             self.fluid.check(self.fluid.lib().wig_batch_step_profile(
-                self.h, lane, ids_a, len(ids), P, None, self.max_cycles, self.flags, self.tolerance,
+                self.h, lane, ids_a, len(ids), P, wf_a, self.max_cycles, self.flags, self.tolerance,
                 C.c_void_p(stream.cuda_stream), ms, calls), "wig_batch_step_profile")
             return {abi.PROFILE_NAMES[k]: (ms[k], calls[k]) for k in range(abi.PROFILE_SLOTS) if calls[k]}
 
