@@ -361,21 +361,27 @@ def run_batched(args, rank, world_size, local_rank, dist, torch, emit=True):
             P[k].frame = step_no
         b.step(ids, P, max_cycles=MAX_CYCLES, flags=FLAGS | extra, tolerance=TOL, stream=stream.cuda_stream)
 
-    # the launch shapes tuned on the batch's first steps (profiled steps of
-    # the same worlds: no result changes), then the warm-up
+    # the launch shapes tuned on the worlds' first steps, stepped by a batch
+    # of their own (no result changes), so the timed trajectory is the one
+    # the default shapes would step; then the warm-up
     tuned = None
     if not args.no_tune:
         from worldinagrain_b200 import tune
+        tb = fluid.Batch(worlds, W.element_table())
+        tune_no = 0
 
         def prof_step():
-            nonlocal step_no
-            step_no += 1
+            nonlocal tune_no
+            tune_no += 1
             for k in range(n):
-                P[k].frame = step_no
-            return b.step_profile(range(n), P, max_cycles=MAX_CYCLES, flags=FLAGS, tolerance=TOL,
-                                  stream=stream.cuda_stream)
+                P[k].frame = tune_no
+            return tb.step_profile(range(n), P, max_cycles=MAX_CYCLES, flags=FLAGS, tolerance=TOL,
+                                   stream=stream.cuda_stream)
 
-        shapes, trials = tune.autotune(b, prof_step)
+        shapes, trials = tune.autotune(tb, prof_step)
+        tb.close()
+        for name, v in shapes.items():
+            b.set_launch(name, v)
         tuned = {"shapes": shapes, "steps": tune.steps_needed(),
                  "trials_ms_per_iteration": {k: [[v, None if c is None else round(c, 4)] for v, c in r]
                                              for k, r in trials.items()}}
@@ -672,19 +678,25 @@ def main():
         return FLAGS | abi.STEP_SHIFTED_SET | (abi.STEP_SHIFTED_FIRST if step % 2 else 0)
 
     step_no = 0
-    # the fast forms' launch shapes tuned on the world's first steps
-    # (profiled steps of its own trajectory: no result changes)
+    # the fast forms' launch shapes tuned on the world's first steps, stepped
+    # by a handle of their own (no result changes), so the timed trajectory
+    # is the one the default shapes would step
     tuned = None
     if not args.no_tune and args.form in ("fast", "mixed"):
         from worldinagrain_b200 import tune
+        tg = fluid.LiquidStep(world, W.element_table(), stream=stream.cuda_stream)
+        tune_no = 0
 
         def prof_step():
-            nonlocal step_no
-            step_no += 1
-            return g.step_profile(params(world, step_no, args.seed), max_cycles=MAX_CYCLES, flags=flags_of(step_no),
-                                  tolerance=TOL)
+            nonlocal tune_no
+            tune_no += 1
+            return tg.step_profile(params(world, tune_no, args.seed), max_cycles=MAX_CYCLES,
+                                   flags=flags_of(tune_no), tolerance=TOL)
 
-        shapes, trials = tune.autotune(g, prof_step)
+        shapes, trials = tune.autotune(tg, prof_step)
+        tg.close()
+        for name, v in shapes.items():
+            g.set_launch(name, v)
         tuned = {"shapes": shapes, "steps": tune.steps_needed(),
                  "trials_ms_per_iteration": {k: [[v, None if c is None else round(c, 4)] for v, c in r]
                                              for k, r in trials.items()}}

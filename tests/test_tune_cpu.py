@@ -1,6 +1,7 @@
 """The launch-shape autotuner's choices, over a fake batch whose profiled
 steps cost what a table says: each knob ends at its cheapest candidate,
-tried in order, each knob tuned with the earlier knobs' choices in place."""
+tried in order, each knob tuned with the earlier knobs' choices in place,
+and a cost that drifts from step to step does not decide the choice."""
 from worldinagrain_b200 import tune
 
 
@@ -58,3 +59,27 @@ def test_no_iteration_keeps_the_current_shape():
     b = Idle({})
     shapes, _ = tune.autotune(b, b.step)
     assert shapes == {"coarse_cells": 4096, "level_per_sm": 8, "cg_per_sm": 8, "relax_per_sm": 16}
+
+
+def test_a_drift_over_the_steps_weighs_the_same_on_every_candidate():
+    """The steps' cost falls by 0.2 ms an iteration a step (the worlds move
+    on); the first candidate is cheapest by 0.1. One pass in order would
+    pick the last candidate; the two passes pick the first."""
+    name, cands, slots = tune.KNOBS[0]
+
+    class Drifting(FakeBatch):
+        def __init__(self):
+            super().__init__({})
+            self.n = 0
+
+        def step(self):
+            c = (1.0 if self.shapes[name] == cands[0] else 1.1) - 0.2 * self.n
+            self.n += 1
+            return {"F_LOOP": (0.1, 7), slots[0]: (c * 7, 7)}
+
+    b = Drifting()
+    shapes, trials = tune.autotune(b, b.step, knobs=(tune.KNOBS[0],))
+    assert shapes[name] == cands[0] and b.n == 2 * len(cands)
+    b = Drifting()
+    shapes, _ = tune.autotune(b, b.step, knobs=(tune.KNOBS[0],), passes=1)
+    assert shapes[name] == cands[-1]

@@ -9,10 +9,17 @@ shaped is the batch's choice (include/wig_batch.h, wig_launch_knob):
   level tile kernels, the CG kernels and the fine relaxation.
 
 No knob changes a result bit, so the tuner tunes on the batch's own steps.
-Each candidate runs one profiled step (device timestamps around every
-launch). Its cost is the time, per solver iteration, of the kernels the
-knob shapes. The cheapest candidate is kept. Knobs are tuned one after
-another, each given the choices made before it.
+Each candidate runs profiled steps (device timestamps around every launch).
+Its cost is the time, per solver iteration, of the kernels the knob shapes.
+The cheapest candidate is kept. Knobs are tuned one after another, each
+given the choices made before it.
+
+Successive steps are different steps of the worlds: their solves take
+other iterations, and a batch's worlds stop iterating at other times, so a
+step's cost per iteration drifts as the worlds move on. The candidates are
+therefore tried in two passes, in order and then in reverse, and each
+candidate's cost is taken over both of its steps: a drift that is linear
+over the knob's steps weighs the same on every candidate.
 """
 
 KNOBS = (
@@ -26,26 +33,37 @@ KNOBS = (
 def cost(profile, slots):
     """Milliseconds per solver iteration of `slots` in one profiled step
     (profile: slot name -> (ms, launches)); None when no iteration ran."""
+    ms, iters = slot_time(profile, slots)
+    return ms / iters if iters else None
+
+
+def slot_time(profile, slots):
+    """(milliseconds of `slots`, solver iterations) of one profiled step."""
     iters = profile.get("F_LOOP", (0.0, 0))[1]
-    if not iters:
-        return None
-    return sum(profile.get(s, (0.0, 0))[0] for s in slots) / iters
+    return sum(profile.get(s, (0.0, 0))[0] for s in slots), iters
 
 
-def autotune(batch, step, knobs=KNOBS):
+def autotune(batch, step, knobs=KNOBS, passes=2):
     """Tune `batch` (fluid.Batch or anything with get_launch, set_launch and
     launch_shapes) on its own steps: step() runs one profiled step of the
-    caller's worlds and returns Batch.step_profile's dict. Returns the chosen
-    shapes and, per knob, the (value, cost) of each candidate tried. The
-    batch keeps the chosen shapes."""
+    caller's worlds and returns Batch.step_profile's dict. Each candidate is
+    stepped once a pass, the passes alternating in order and in reverse.
+    Returns the chosen shapes and, per knob, the (value, cost) of each
+    candidate in the knob's order. The batch keeps the chosen shapes."""
     trials = {}
     for name, candidates, slots in knobs:
-        best_v, best_c = batch.get_launch(name), None
-        rows = []
-        for v in candidates:
-            batch.set_launch(name, v)
-            c = cost(step(), slots)
-            rows.append((v, c))
+        keep = batch.get_launch(name)
+        ms = {v: 0.0 for v in candidates}
+        its = {v: 0 for v in candidates}
+        for p in range(passes):
+            for v in (candidates if p % 2 == 0 else tuple(reversed(candidates))):
+                batch.set_launch(name, v)
+                t, n = slot_time(step(), slots)
+                ms[v] += t
+                its[v] += n
+        rows = [(v, ms[v] / its[v] if its[v] else None) for v in candidates]
+        best_v, best_c = keep, None
+        for v, c in rows:
             if c is not None and (best_c is None or c < best_c):
                 best_v, best_c = v, c
         batch.set_launch(name, best_v)
@@ -53,6 +71,6 @@ def autotune(batch, step, knobs=KNOBS):
     return batch.launch_shapes(), trials
 
 
-def steps_needed(knobs=KNOBS):
+def steps_needed(knobs=KNOBS, passes=2):
     """Profiled steps autotune runs."""
-    return sum(len(c) for _, c, _ in knobs)
+    return passes * sum(len(c) for _, c, _ in knobs)
