@@ -131,64 +131,79 @@ def params(world, step, seed):
 # layout makes it read and write once (per active cell, fluid cell, face or
 # particle), counted from the world after the step.  Active cells are the
 # active blocks' 64 each.  The fast form's level kernels, per launch on a
-# level of n cells: down (restriction, then both colours of smoothing on
-# chip) 180 n (the four finer cells' ten arrays read, the coarse cell's
-# five written); up (prolongation, then both colours) 51 n (the level's ten
-# arrays read, its potentials written, the coarser level's density and
-# potentials read); the one-CTA coarse kernel 28 n on its first level.
-# Averaged over the launches of an iteration (s["levels"]: per level, its
-# cells summed over the worlds and whether it is smoothed, restricted by
-# itself, or the coarse kernel's first).
+# level of n cells.  A level cell holds four FP32 words (px, py, rx, ry),
+# five operator words of e bytes (rho, b0..b3: 4, or 2 in the mixed form's
+# binary16 levels) and, stored only in FP32, its diagonal (d = 4, mixed 0);
+# level 0 is all FP32 (40 B a cell).  Down (restriction, then both colours
+# of smoothing on chip): the four finer cells read, the coarse cell's px, py,
+# rx, ry and rho written, 180 n in FP32; up (prolongation, then both
+# colours): the level's words read, its potentials written, the coarser
+# level's density and potentials read a quarter each, 51 n in FP32; the
+# one-CTA coarse kernel on its first level 24 + e a cell, 28 n in FP32.
+# Averaged over the launches of an iteration (s["levels"]: level_stats'
+# cells of each level's launches; s["mixed"]: the mixed form).
 def level_bytes(name, s):
     L = s.get("levels")
     if not L:
         return None
-    sm = [n for n, kind in L if kind == "smooth"]
-    rs = [n for n, kind in L if kind in ("smooth", "restrict")]
-    co = [n for n, kind in L if kind == "restrict"]
-    if name == "F_RESTRICT" and rs:
-        return sum(180 * n for n in rs) // len(rs)
-    if name == "F_PROLONG" and sm:
-        return sum(51 * n for n in sm) // len(sm)
+    e, d = (2, 0) if s.get("mixed") else (4, 4)
+    cell = 16 + 5 * e + d
+    down = [(4 * (40 if i == 0 else cell) + 16 + e) * r for i, (r, _, _) in enumerate(L) if r]
+    up = [(cell + 8 + (e + 8) / 4) * m for _, m, _ in L if m]
+    co = [(24 + e) * c for _, _, c in L if c]
+    if name == "F_RESTRICT" and down:
+        return int(sum(down)) // len(down)
+    if name == "F_PROLONG" and up:
+        return int(sum(up)) // len(up)
     if name == "F_COARSE" and co:
-        return sum(28 * n for n in co)
+        return int(sum(co))
     return None
 
 
-def level_stats(worlds):
-    """Per level index: (cells over the worlds, what the fast form does there)."""
+def level_stats(worlds, coarse_cells=4096):
+    """Per level index l from 1: (cells a down launch takes, cells an up
+    launch takes, cells the coarse kernel starts from), summed over the
+    worlds, for the launch shape coarse_cells: a world's coarse kernel
+    starts at its first level lc of at most that many cells (else its
+    coarsest); its levels up to lc are restricted by the down kernel, those
+    above lc also smoothed on the way up."""
     from collections import defaultdict
-    cells, kind = defaultdict(int), {}
+    res, smooth, coarse = defaultdict(int), defaultdict(int), defaultdict(int)
     for w in worlds:
         lv = w.L["levels"]
-        lc = next((i + 1 for i, (a, b) in enumerate(lv) if a * b <= 4096), len(lv))
-        for i, (a, b) in enumerate(lv):
+        lc = next((i + 1 for i, (a, b) in enumerate(lv) if a * b <= coarse_cells), len(lv))
+        for i, (a, b) in enumerate(lv[:lc]):
             l = i + 1
+            res[l] += a * b
             if l < lc:
-                cells[l] += a * b
-                kind[l] = "smooth"
-            elif l == lc:
-                cells[l] += a * b
-                kind.setdefault(l, "restrict")
-    return [(cells[l], kind[l]) for l in sorted(cells)]
+                smooth[l] += a * b
+            else:
+                coarse[l] += a * b
+    return [(res[l], smooth[l], coarse[l]) for l in sorted(res)]
 
 
 # DRAM bytes (read + written) per algorithmic byte of a kernel, from one
-# `ncu --set full` capture each of the disks 1024x1024 world (the summaries
-# under profiles/ give the commands). roofline.traffic is this ratio times a
-# launch's algorithmic bytes: the capture's traffic scaled to the launch by
-# the units it processes.
+# ncu capture each (the summaries under profiles/ give the commands), keyed
+# by (slot, mixed form). roofline.traffic is this ratio times a launch's
+# algorithmic bytes: the capture's traffic scaled to the launch by the units
+# it processes.
 TRAFFIC_PER_ALG_BYTE = {
-    # k_fDown on level 1: 22.8 MB read, 256 B written; 262,144 cells x 180 B
-    "F_RESTRICT": ((22.8e6 + 256) / (262144 * 180), "k_fDown level 1 (512x512), k_fDown_level1_disks1024.md"),
-    # k_fRelax: 25.0 MB read, 0 written; 24.5 MB algorithmic
-    "F_RELAX": (25.0e6 / 24.5e6, "k_fRelax, k_fRelax_disks1024.md"),
+    # k_fDown on level 1 of the disks 1024x1024 world: 22.8 MB read, 256 B
+    # written; 262,144 cells x 180 B
+    ("F_RESTRICT", False): ((22.8e6 + 256) / (262144 * 180), "k_fDown level 1 (512x512), k_fDown_level1_disks1024.md"),
+    # k_fDown on levels 1-3 of one iteration of a 64-world batch, mixed form:
+    # 117.1 MB read and written; 222.2 MB algorithmic
+    ("F_RESTRICT", True): (117145856 / 222247528, "k_fDown levels 1-3 of a 64-world batch, k_fDown_batch64_mixed.md"),
+    # k_fRelax on the disks 1024x1024 world: 25.0 MB read, 0 written; 24.5 MB
+    # algorithmic (the fine level is FP32 in both forms)
+    ("F_RELAX", False): (25.0e6 / 24.5e6, "k_fRelax, k_fRelax_disks1024.md"),
+    ("F_RELAX", True): (25.0e6 / 24.5e6, "k_fRelax, k_fRelax_disks1024.md"),
 }
 
 
-def traffic_of(name, alg):
+def traffic_of(name, alg, mixed=False):
     """(DRAM bytes a launch moves, where the figure comes from), or (None, None)."""
-    t = TRAFFIC_PER_ALG_BYTE.get(name)
+    t = TRAFFIC_PER_ALG_BYTE.get((name, bool(mixed)))
     if t is None or not alg:
         return None, None
     return int(round(t[0] * alg)), "ncu capture " + t[1] + ", scaled to this launch's algorithmic bytes"
@@ -228,13 +243,13 @@ def algorithmic_bytes(name, s):
     return table.get(name)
 
 
-def world_stats(world):
+def world_stats(world, coarse_cells=4096):
     blocks = world.blocks
     B = world.L["block_count"]
     active = int(blocks[4 * B + abi.COUNT_ACTIVE])
     rho = world.field_cells()[:, 0, 2]
     return {"active_cells": active * 64, "fluid_cells": int(np.sum(rho > 0)), "particles": int(world.sorted[0]),
-            "levels": level_stats([world])}
+            "levels": level_stats([world], coarse_cells)}
 
 
 def cpu_baseline(world, args, budget_s):
@@ -449,7 +464,8 @@ def run_batched(args, rank, world_size, local_rank, dist, torch, emit=True):
         ws["active_cells"] += int(w.blocks[4 * B + abi.COUNT_ACTIVE]) * 64
         ws["fluid_cells"] += int(np.sum(w.field_cells()[:, 0, 2] > 0))
     ws["particles"] = int(sum(x.particles for x in b.stats(range(n))))
-    ws["levels"] = level_stats(worlds)
+    ws["levels"] = level_stats(worlds, b.get_launch("coarse_cells"))
+    ws["mixed"] = args.form == "mixed"
     total = sum(v[0] for v in prof.values())
     ranked = sorted(prof.items(), key=lambda kv: -kv[1][0])
     top = next((k for k, _ in ranked if algorithmic_bytes(k, ws) is not None), ranked[0][0])
@@ -492,8 +508,8 @@ def run_batched(args, rank, world_size, local_rank, dist, torch, emit=True):
             "e2e": {"value": round(e2e, 3), "unit": "Mcells/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches_per_step * args.steps,
             "roofline": {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic_of(top, alg)[0],
-                         "traffic_source": traffic_of(top, alg)[1],
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic_of(top, alg, ws["mixed"])[0],
+                         "traffic_source": traffic_of(top, alg, ws["mixed"])[1],
                          "algorithmic_bytes_per_launch": alg, "launch_ms": round(per_launch_s * 1e3, 5)},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
@@ -767,7 +783,8 @@ def main():
             a, b = prof.get(k, (0.0, 0))
             prof[k] = (a + t_ms, b + n)
     g.download(world)
-    ws = world_stats(world)
+    ws = world_stats(world, g.get_launch("coarse_cells"))
+    ws["mixed"] = args.form == "mixed"
     total = sum(v[0] for v in prof.values())
     ranked = sorted(prof.items(), key=lambda kv: -kv[1][0])
     top = next((k for k, _ in ranked if algorithmic_bytes(k, ws) is not None), ranked[0][0])
@@ -792,8 +809,8 @@ def main():
             "e2e": {"value": round(e2e, 3), "unit": "Mcells/s", "h2d_bytes_per_step": 152, "d2h_bytes_per_step": 64},
             "gpu_launches": launches_per_step * args.steps,
             "roofline": {"bound": "hbm", "kernel": top, "achieved": round(achieved, 1), "peak": peak,
-                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic_of(top, alg)[0],
-                         "traffic_source": traffic_of(top, alg)[1],
+                         "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4), "traffic": traffic_of(top, alg, ws["mixed"])[0],
+                         "traffic_source": traffic_of(top, alg, ws["mixed"])[1],
                          "algorithmic_bytes_per_launch": alg, "launch_ms": round(per_launch_s * 1e3, 5)},
             "cpu_baseline": cpu,
             "clocks": clk.summary(),

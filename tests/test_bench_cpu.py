@@ -11,7 +11,8 @@ from worldinagrain_b200 import abi
 
 
 def test_level_byte_models():
-    s = {"levels": [(262144, "smooth"), (65536, "smooth"), (16384, "restrict")]}
+    # per level: (down launch cells, up launch cells, coarse kernel's first)
+    s = {"levels": [(262144, 262144, 0), (65536, 65536, 0), (16384, 0, 16384)]}
     # down: 180 B a cell averaged over the levels restricted by tile kernels
     assert bench.level_bytes("F_RESTRICT", s) == (180 * 262144 + 180 * 65536 + 180 * 16384) // 3
     # up: 51 B a cell over the levels above the coarse kernel's
@@ -20,6 +21,29 @@ def test_level_byte_models():
     assert bench.level_bytes("F_COARSE", s) == 28 * 16384
     assert bench.level_bytes("F_RELAX", s) is None
     assert bench.level_bytes("F_RESTRICT", {}) is None
+    # the mixed form: the operator words of levels 1 down in binary16, no
+    # stored diagonal there; level 0 all FP32
+    m = dict(s, mixed=True)
+    assert bench.level_bytes("F_RESTRICT", m) == (178 * 262144 + 122 * 65536 + 122 * 16384) // 3
+    assert bench.level_bytes("F_PROLONG", m) == int(36.5 * 262144 + 36.5 * 65536) // 2
+    assert bench.level_bytes("F_COARSE", m) == 26 * 16384
+
+
+def test_level_stats_follow_the_coarse_kernels_first_level():
+    """The level list the byte models average over: the tile kernels' levels
+    end where the batch's coarse_cells launch shape starts the coarse
+    kernel, per world."""
+    from types import SimpleNamespace
+    w512 = SimpleNamespace(L=abi.layout_py(512, 512))
+    w64 = SimpleNamespace(L=abi.layout_py(64, 64))
+    assert bench.level_stats([w512]) == [(65536, 65536, 0), (16384, 16384, 0), (4096, 0, 4096)]
+    assert bench.level_stats([w512], 2048) == [(65536, 65536, 0), (16384, 16384, 0), (4096, 4096, 0),
+                                                (1024, 0, 1024)]
+    # a 64x64 world's coarse kernel starts at its level 1 (1024 cells): the
+    # level-1 down launch takes it, the up launch doesn't
+    assert bench.level_stats([w512, w64]) == [(65536 + 1024, 65536, 1024), (16384, 16384, 0), (4096, 0, 4096)]
+    s = {"levels": bench.level_stats([w512, w64])}
+    assert bench.level_bytes("F_COARSE", s) == 28 * (1024 + 4096)
 
 
 def test_algorithmic_bytes_of_the_cg_kernels():
