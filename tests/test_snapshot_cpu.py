@@ -76,6 +76,9 @@ def test_bad_files_are_refused():
     bad = dict(parts, field=parts["field"][:-4])
     with pytest.raises(ValueError, match="lays out field differently"):
         snapshot.world_from(header, bad)
+    bad = dict(parts, cells1=parts["cells1"][:-16])  # the pair's other buffer must fit too
+    with pytest.raises(ValueError, match="cells1"):
+        snapshot.world_from(header, bad)
     bad = {k: v for k, v in parts.items() if k != "particles0"}
     with pytest.raises(ValueError, match="particles0"):
         snapshot.world_from(header, bad)

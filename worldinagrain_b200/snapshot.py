@@ -201,6 +201,9 @@ def restore(world, header, parts, elems=None, element_ids=None):
             continue
         if src is None or src.nbytes != getattr(world, buf).nbytes:
             misfits.append(part)
+    other = parts.get(f"cells{1 - cur}")
+    if other is not None and other.nbytes != world.cells.nbytes:
+        misfits.append(f"cells{1 - cur}")
     if misfits:
         raise ValueError(f"saved by a version that lays out {', '.join(misfits)} differently")
     for buf, part in names.items():
