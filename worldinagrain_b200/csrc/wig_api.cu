@@ -422,7 +422,11 @@ int make_batch(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, u
     S.worlds = n;
     S.coarse_cells = wig::COARSE_CTA_CELLS;
     S.level_per_sm = 8;
-    S.cg_per_sm = 8;
+    // a single world's CG kernels run fastest with fewer CTAs, each taking
+    // more tiles and fewer of them counting into the world's last-tile
+    // counter (0.074 against 0.079 ms an iteration at 1024x1024, the
+    // autotuner's measurement); a batch's with more
+    S.cg_per_sm = n == 1 ? 4 : 8;
     S.relax_per_sm = 16;
     uint64_t most_units = 1, max_items[wig::L_COUNT] = {0};
     size_t scratch_total = 0;
