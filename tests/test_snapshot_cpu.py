@@ -72,7 +72,21 @@ def test_bad_files_are_refused():
         snapshot.read(_raw({"format": 2, "parts": []}))
     with pytest.raises(ValueError, match="cut short"):
         snapshot.read(_raw({"format": 1, "parts": [{"name": "x", "bytes": 64}]}, b"\0" * 8))
+    # malformed headers and part lists: a ValueError, never another error
+    for h, body in (({"format": 1, "parts": [{"name": "x", "bytes": -5}]}, b"\0" * 16),
+                    ({"format": 1, "parts": [{"name": "x", "bytes": "4"}]}, b"\0" * 16),
+                    ({"format": 1, "parts": [{"bytes": 4}]}, b"\0" * 16),
+                    ({"format": 1, "parts": 5}, b""),
+                    ([1, 2], b"")):
+        with pytest.raises(ValueError):
+            snapshot.read(_raw(h, body))
+    with pytest.raises(ValueError, match="cut short"):
+        snapshot.read(gzip.compress(b"SANDSNAP" + struct.pack("<I", 10 ** 9) + b"{}"))
     header, parts = snapshot.read(snapshot.save(w))
+    for h in ({k: v for k, v in header.items() if k != "width"}, dict(header, height="tall"),
+              dict(header, width=0), dict(header, state=[]), dict(header, state={"cur": 2})):
+        with pytest.raises(ValueError):
+            snapshot.world_from(h, parts)
     bad = dict(parts, field=parts["field"][:-4])
     with pytest.raises(ValueError, match="lays out field differently"):
         snapshot.world_from(header, bad)

@@ -76,16 +76,25 @@ def read(data):
     if len(raw) < len(MAGIC) + 4 or raw[:len(MAGIC)] != MAGIC:
         raise ValueError("not a snapshot")
     (length,) = struct.unpack_from("<I", raw, len(MAGIC))
+    if len(MAGIC) + 4 + length > len(raw):
+        raise ValueError("the snapshot is cut short")
     try:
         header = json.loads(raw[len(MAGIC) + 4:len(MAGIC) + 4 + length].decode())
     except (UnicodeDecodeError, json.JSONDecodeError) as e:
         raise ValueError("not a snapshot") from e
+    if not isinstance(header, dict):
+        raise ValueError("not a snapshot")
     if header.get("format") != FORMAT:
         raise ValueError(f"saved in snapshot format {header.get('format')}; this reads format {FORMAT}")
+    listed = header.get("parts", [])
+    if not isinstance(listed, list) or not all(
+            isinstance(p, dict) and isinstance(p.get("name"), str) and isinstance(p.get("bytes"), int)
+            and not isinstance(p.get("bytes"), bool) and p["bytes"] >= 0 for p in listed):
+        raise ValueError("the snapshot's list of parts is malformed")
     parts = {}
     at = len(MAGIC) + 4 + _align4(length)
-    for part in header.get("parts", []):
-        n = int(part["bytes"])
+    for part in listed:
+        n = part["bytes"]
         if at + n > len(raw):
             raise ValueError("the snapshot is cut short")
         parts[part["name"]] = np.frombuffer(raw, dtype=np.uint8, count=n, offset=at).copy()
@@ -172,6 +181,17 @@ def migrate_field(world, parts):
     return dict(parts, field=grown)
 
 
+def _size(header):
+    """The header's world size (width, height); ValueError when it has none."""
+    try:
+        width, height = int(header["width"]), int(header["height"])
+    except (KeyError, TypeError, ValueError) as e:
+        raise ValueError("the snapshot's header gives no world size") from e
+    if width <= 0 or height <= 0:
+        raise ValueError(f"the snapshot's world is {width}x{height}")
+    return width, height
+
+
 def restore(world, header, parts, elems=None, element_ids=None):
     """Load a snapshot (read's header and parts) into `world`, a World of its
     size, as restoreSnapshot does for the liquid's parts
@@ -185,10 +205,12 @@ def restore(world, header, parts, elems=None, element_ids=None):
     and its other parts as world.snapshot_rest."""
     if element_ids is not None and list(header.get("elements", [])) != list(element_ids):
         raise ValueError("saved with a different set of elements")
-    width, height = int(header["width"]), int(header["height"])
+    width, height = _size(header)
     if (width, height) != (world.W, world.H):
         raise ValueError(f"the snapshot is of a {width}x{height} world, this one is {world.W}x{world.H}")
     state = header.get("state", {})
+    if not isinstance(state, dict) or state.get("cur", 0) not in (0, 1):
+        raise ValueError("the snapshot's state names no current cell buffer")
     cur = int(state.get("cur", 0))
     elems = W.element_table() if elems is None else elems
     parts, migrated = migrate_liquid(world, parts, elems)
@@ -228,7 +250,7 @@ def world_from(header, parts, liquid_per_cell=4, capacity=0, elems=None, element
     """A World of the snapshot's size, with the reference's particle
     capacity for it (or `capacity`), holding the snapshot's liquid
     (restore)."""
-    w = W.World(int(header["width"]), int(header["height"]), liquid_per_cell, capacity)
+    w = W.World(*_size(header), liquid_per_cell, capacity)
     w.config = dict(workload="snapshot", grid=f"{w.W}x{w.H}", seed=0, earth_g=W.earth_g_cells())
     return restore(w, header, parts, elems, element_ids)
 
