@@ -400,6 +400,8 @@ def run_batched(args, rank, world_size, local_rank, dist, torch, emit=True):
         tuned = {"shapes": shapes, "steps": tune.steps_needed(),
                  "trials_ms_per_iteration": {k: [[v, None if c is None else round(c, 4)] for v, c in r]
                                              for k, r in trials.items()}}
+    for name, v in args.launch.items():
+        b.set_launch(name, v)
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
@@ -611,6 +613,18 @@ def run_served(args, rank, world_size, local_rank, dist, torch, emit=True):
         return line
 
 
+def launch_overrides(items):
+    """--launch KNOB=VALUE arguments as {knob: value}; SystemExit on an
+    unknown knob or a value that is not a positive integer."""
+    out = {}
+    for it in items:
+        name, _, v = it.partition("=")
+        if name not in abi.LAUNCH_KNOBS or not v.isdigit() or int(v) <= 0:
+            raise SystemExit(f"--launch {it}: want one of {', '.join(abi.LAUNCH_KNOBS)} = a positive integer")
+        out[name] = int(v)
+    return out
+
+
 def dtype_of(form):
     """The arithmetic the form computes in: FP32 grids and vectors, FP64
     dots; the mixed form stores its coarse operator in binary16."""
@@ -648,7 +662,11 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="the default launch shapes, not the autotuner's")
     ap.add_argument("--no-forms", action="store_true",
                     help="the single world alone, without the batched and served summaries a one-GPU run adds")
+    ap.add_argument("--launch", action="append", default=[], metavar="KNOB=VALUE",
+                    help="a launch shape set on the measured handle after any tuning (coarse_cells, "
+                         "level_per_sm, cg_per_sm, relax_per_sm); repeatable")
     args = ap.parse_args()
+    args.launch = launch_overrides(args.launch)
     args.warmup = max(args.warmup, 3)
     global FLAGS
     if args.form == "plain":
@@ -716,6 +734,8 @@ def main():
         tuned = {"shapes": shapes, "steps": tune.steps_needed(),
                  "trials_ms_per_iteration": {k: [[v, None if c is None else round(c, 4)] for v, c in r]
                                              for k, r in trials.items()}}
+    for name, v in args.launch.items():
+        g.set_launch(name, v)
     for _ in range(args.warmup):
         step_no += 1
         g.step(params(world, step_no, args.seed), max_cycles=MAX_CYCLES, flags=flags_of(step_no), tolerance=TOL)

@@ -6,6 +6,8 @@ import os
 import subprocess
 import sys
 
+import pytest
+
 import bench
 from worldinagrain_b200 import abi
 
@@ -62,6 +64,13 @@ def test_traffic_scales_the_captured_ratio():
     assert bench.traffic_of("F_RESTRICT", alg // 2)[0] == round(t / 2)
     assert bench.traffic_of("F_COARSE", 10 ** 6) == (None, None)
     assert bench.traffic_of("F_RELAX", 0) == (None, None)
+
+
+def test_launch_overrides():
+    assert bench.launch_overrides(["cg_per_sm=8", "coarse_cells=2048"]) == {"cg_per_sm": 8, "coarse_cells": 2048}
+    for bad in (["cg=8"], ["cg_per_sm=0"], ["cg_per_sm=x"], ["cg_per_sm"]):
+        with pytest.raises(SystemExit):
+            bench.launch_overrides(bad)
 
 
 def test_form_arithmetic():
