@@ -859,6 +859,7 @@ def run_forms(args, rank, world_size, local_rank, dist, torch):
     out = {}
     b = ap_.Namespace(**vars(args))
     b.worlds, b.steps, b.warmup, b.no_cpu, b.profile_steps, b.form = 512, 10, 3, True, 1, "mixed"
+    b.launch = {}  # the forms keep their own tuned shapes
     s = ap_.Namespace(**vars(args))
     s.worlds, s.rates, s.no_cpu, s.form = 2000, "1000,2000,20000", True, "mixed"
     saved = FLAGS
