@@ -141,3 +141,28 @@ def test_merge_parts_pools_latencies_and_sums_throughput():
     assert m["p50_ms"] == 2.5
     assert m["mcells_per_s"] == round((300 / 1.0 + 100 / 0.5) / 1e6, 3)
     assert m["swapped_requests"] == 1 and m["p50_ms_resident"] == 2.0
+
+
+def test_snapshot_worlds_carry_their_state_into_the_backend():
+    """The GPU backend's bookkeeping for worlds loaded from snapshots, without
+    a device: such a world uploads whole at its first admission, its frames
+    count on from the saved one, and only its first step carries the saved
+    tiling parity."""
+    from worldinagrain_b200 import abi, snapshot
+    from worldinagrain_b200 import world as W
+    fresh = W.small_world(32, 32, seed=1, kind="dam")
+    loaded = snapshot.load(snapshot.save(W.small_world(48, 40, seed=2, kind="dam"),
+                                         state={"frameNo": 7, "shiftedFirst": True}))
+    be = serve.GpuBackend.__new__(serve.GpuBackend)  # the bookkeeping only, no device
+    be.worlds = [fresh, loaded]
+    be.seed = 1
+    be._init_states(be.worlds)
+    assert be.has_state == [False, True] and be.frames == [0, 7]
+    # the saved parity: shiftedFirst True, flipped before the step's first relaxation
+    assert be.first_flags == [0, abi.STEP_SHIFTED_SET]
+    wf = be._world_flags([1, 0])
+    assert list(wf) == [abi.STEP_SHIFTED_SET, 0]
+    P = be._next_params([1, 0])
+    assert [p.frame for p in P] == [8, 1]
+    assert be.has_state == [True, True]
+    assert be._world_flags([0, 1]) is None  # later steps: the handle flips the parity itself

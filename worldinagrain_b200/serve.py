@@ -74,12 +74,7 @@ class GpuBackend:
                     "wig_batch_create_deferred")
         self.h = h
         self.streams = [torch.cuda.Stream(), torch.cuda.Stream()]
-        # a world loaded from a snapshot (snapshot.load) holds a state: all of
-        # its buffers go up at its first admission, its frames count on from
-        # the saved one, and its first step sets the saved tiling parity
-        self.has_state = [hasattr(w, "snapshot_state") for w in worlds]
-        self.frames = [int(w.snapshot_state.get("frameNo", 0)) if s else 0 for w, s in zip(worlds, self.has_state)]
-        self.first_flags = [snapshot.step_flags(w) if s else 0 for w, s in zip(worlds, self.has_state)]
+        self._init_states(worlds)
         self.pooled = pool_bytes is not None
         self.pool = pool_bytes
         split = [self._split(w) for w in worlds]
@@ -93,6 +88,16 @@ class GpuBackend:
             self.step_bytes_ = [0] * len(worlds)
         self.names = [(which, name) for which, name in enumerate(abi.BUFFER_NAMES)
                       if not (self.pooled and name in ("parts", "cg"))]
+
+    def _init_states(self, worlds):
+        """Per world: whether it holds a state, its frame count, the flags of
+        its first step. A world loaded from a snapshot (snapshot.load) holds
+        one: all of its buffers go up at its first admission, its frames
+        count on from the saved one, and its first step sets the saved
+        tiling parity."""
+        self.has_state = [hasattr(w, "snapshot_state") for w in worlds]
+        self.frames = [int(w.snapshot_state.get("frameNo", 0)) if s else 0 for w, s in zip(worlds, self.has_state)]
+        self.first_flags = [snapshot.step_flags(w) if s else 0 for w, s in zip(worlds, self.has_state)]
 
     @staticmethod
     def _setup_funcs(L):
