@@ -323,7 +323,9 @@ int wig_fluid_step_profile(wig_fluid* h, const wig_params* P, uint32_t max_cycle
                            void* stream, float* ms_out, uint32_t* calls_out);
 
 /* The fast form's launch shapes of this world (knob: enum wig_launch_knob of
- * wig_batch.h, the same values and ranges): none changes a result. */
+ * wig_batch.h, the same values and ranges): none changes a result.  No
+ * counterpart in the reference, whose dispatch sizes are fixed per pipeline
+ * (encodeFluid's run and blocks, js/sim.js:2473-2478). */
 int wig_fluid_set_launch(wig_fluid* h, uint32_t knob, uint32_t value);
 int wig_fluid_get_launch(const wig_fluid* h, uint32_t knob, uint32_t* value);
 
