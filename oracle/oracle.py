@@ -37,6 +37,7 @@ def lib():
         L.wo_solve_f64.argtypes = [C.POINTER(abi.WorldDesc), C.POINTER(abi.Params), C.POINTER(abi.Elem), C.c_uint32,
                                    C.POINTER(abi.Buffers), C.c_double, C.c_uint32, C.c_void_p,
                                    C.POINTER(C.c_double)]
+        L.wo_solve_f64_mg.argtypes = L.wo_solve_f64.argtypes
         L.wo_true_residual.argtypes = [C.POINTER(abi.WorldDesc), C.POINTER(abi.Params), C.POINTER(abi.Elem),
                                        C.c_uint32, C.POINTER(abi.Buffers), C.c_void_p]
         L.wo_true_residual.restype = C.c_double
@@ -77,13 +78,19 @@ class Oracle:
         assert rc == 0, rc
         return st
 
-    def solve_f64(self, P, rel_tol=1e-12, max_iter=100000):
+    def solve_f64(self, P, rel_tol=1e-12, max_iter=100000, multigrid=False):
+        """The FP64 solve of the step's pressure system (the world stopped
+        after cgAnchor): (x per cell, iterations, relative residual).
+        multigrid: flexible CG preconditioned by one of the oracle's V-cycles
+        (tens of iterations; leaves the V-cycle's scratch in the buffers),
+        else Jacobi-preconditioned CG."""
         d = self.world.desc()
         b = _buffers(self.world)
         x = np.zeros(self.world.C, dtype=np.float64)
         rel = C.c_double(0.0)
-        it = lib().wo_solve_f64(C.byref(d), C.byref(P), self.elems, len(self.elems), C.byref(b), rel_tol, max_iter,
-                                x.ctypes.data, C.byref(rel))
+        f = lib().wo_solve_f64_mg if multigrid else lib().wo_solve_f64
+        it = f(C.byref(d), C.byref(P), self.elems, len(self.elems), C.byref(b), rel_tol, max_iter,
+               x.ctypes.data, C.byref(rel))
         return x, it, rel.value
 
     def true_residual(self, P, x):

@@ -90,7 +90,14 @@ inline uint32_t f2u(float f) {
     if (f >= 4294967296.0f) return 0xffffffffu;
     return (uint32_t)f;
 }
-inline float clampf(float x, float lo, float hi) { return std::min(std::max(x, lo), hi); }
+// WGSL's min and max: of two f32, a NaN operand gives the other one (as the
+// GPU's fminf and fmaxf do), otherwise the smaller or larger; any other type
+// as std::min and std::max.
+template <class T> inline T wmax(T a, T b) { return std::max(a, b); }
+template <class T> inline T wmin(T a, T b) { return std::min(a, b); }
+inline float wmax(float a, float b) { return a != a ? b : (b != b ? a : std::max(a, b)); }
+inline float wmin(float a, float b) { return a != a ? b : (b != b ? a : std::min(a, b)); }
+inline float clampf(float x, float lo, float hi) { return wmin(wmax(x, lo), hi); }
 inline float mixf(float a, float b, float t) { return a * (1.0f - t) + b * t; }
 
 // IEEE binary16 from f32, rounding to nearest even (pack2x16float).
@@ -174,7 +181,7 @@ inline uint32_t wordSolute(uint32_t x) { return holdsSolute(wordType(x)) ? wordA
 inline uint32_t wordStrength(uint32_t x) { return holdsSolute(wordType(x)) ? wordLife(x) : 0u; }
 inline uint32_t liquidHome(uint32_t w) { return w >> LIQUID_COUNT_BITS; }
 inline uint32_t liquidCount(uint32_t w) { return w & LIQUID_COUNT_MAX; }
-inline uint32_t liquidW(uint32_t home, uint32_t count) { return (home << LIQUID_COUNT_BITS) | std::min(count, LIQUID_COUNT_MAX); }
+inline uint32_t liquidW(uint32_t home, uint32_t count) { return (home << LIQUID_COUNT_BITS) | wmin(count, LIQUID_COUNT_MAX); }
 inline uint32_t claimOf(uint32_t i) { return DEST_CELL | (DEST_SPAN - i); }
 inline uint32_t claimedCell(uint32_t d) { return DEST_SPAN - (d & DEST_SPAN); }
 inline bool isClaim(uint32_t d) { return d != DEST_KEEP && (d & DEST_ASIDE) == 0u && (d & DEST_CELL) != 0u; }
@@ -223,7 +230,7 @@ struct Ctx {
     uint32_t cellIndex(I2 c) const { return (uint32_t)c.y * (uint32_t)W + (uint32_t)c.x; }
     I2 cellOf(V2 p) const {
         int x = f2i(std::floor(p.x)), y = f2i(std::floor(p.y));
-        return I2{std::min(std::max(x, 0), W - 1), std::min(std::max(y, 0), H - 1)};
+        return I2{wmin(wmax(x, 0), W - 1), wmin(wmax(y, 0), H - 1)};
     }
     static I2 beside(I2 c, int d) {
         if (d < 2) return I2{c.x + (d & 1) * 2 - 1, c.y};
@@ -313,7 +320,7 @@ struct Ctx {
         uint32_t* a = item(parts, 2u * cap + k);
         a[0] = bits(q.affine.x); a[1] = bits(q.affine.y); a[2] = bits(q.affine.z); a[3] = bits(q.affine.w);
     }
-    uint32_t partsLive() const { return std::min(parts[0], cap); }
+    uint32_t partsLive() const { return wmin(parts[0], cap); }
 
     // RNG (common.wgsl:1415-1432)
     void seedRng(uint32_t a, uint32_t b, uint32_t c) { rng = pcg(a ^ pcg(b ^ pcg(c))); }
@@ -341,8 +348,8 @@ struct Ctx {
     // elements (common.wgsl:981-997, :1469-1564)
     float effTempIn(uint32_t t, float stored, float hiT, float loT) {
         const wig_elem& e = elem(t);
-        return clampf(stored, loT, hiT) + std::max(stored - hiT - e.up_span, 0.0f)
-            - std::max(loT - e.down_span - stored, 0.0f) * e.down_scale;
+        return clampf(stored, loT, hiT) + wmax(stored - hiT - e.up_span, 0.0f)
+            - wmax(loT - e.down_span - stored, 0.0f) * e.down_scale;
     }
     float actsAt(uint32_t x, float temp) {  // effTempIn(t, temp, phaseOf(t, solute, strength, 0))
         uint32_t t = wordType(x);
@@ -351,7 +358,7 @@ struct Ctx {
     }
     float expandedAt(uint32_t t, float temp) {
         const wig_elem& e = elem(t);
-        float d = temp - std::max(AMBIENT_T, e.lo_t);
+        float d = temp - wmax(AMBIENT_T, e.lo_t);
         return clampf(1.0f - e.expansion * d - e.expansion2 * d * d, 0.8f, 1.05f);
     }
     float liquidDensity(uint32_t x, float temp) {
@@ -370,7 +377,7 @@ struct Ctx {
     }
     float viscosityAt(const wig_elem& e, float temp) {
         if (e.viscosity_e <= 0.0f) return e.viscosity;
-        return std::min(e.viscosity * std::exp((e.viscosity_t - temp) / e.viscosity_e), 1e4f);
+        return wmin(e.viscosity * std::exp((e.viscosity_t - temp) / e.viscosity_e), 1e4f);
     }
     float wordTempOf(const uint32_t* v) { return actsAt(v[0], cellTemp(v)); }
 
@@ -386,9 +393,9 @@ struct Ctx {
 // faceBeta, surfaceShare, fineBeta (fluid.wgsl:369-405)
 float faceBeta(float a, float b) {
     if (a < 0.0f || b < 0.0f || (a <= 0.0f && b <= 0.0f)) return 0.0f;
-    return (a > 0.0f && b > 0.0f) ? 2.0f / (a + b) : 1.0f / std::max(a, b);
+    return (a > 0.0f && b > 0.0f) ? 2.0f / (a + b) : 1.0f / wmax(a, b);
 }
-float surfaceShare(float da, float db) { return clampf((da - 0.5f) / std::max(da - db, 1e-3f), THETA_MIN, 1.0f); }
+float surfaceShare(float da, float db) { return clampf((da - 0.5f) / wmax(da - db, 1e-3f), THETA_MIN, 1.0f); }
 float fineBeta(float a, float b, float da, float db) {
     float beta = faceBeta(a, b);
     if (a > 0.0f && b == 0.0f) return beta / (da > 0.0f ? surfaceShare(da, db) : 0.5f);
@@ -413,10 +420,10 @@ void ufJoin(Ctx& X, uint32_t i, uint32_t j) {
         a = ufFind(X, a);
         b = ufFind(X, b);
         if (a == b) return;
-        uint32_t lo = std::min(a, b), hi = std::max(a, b);
+        uint32_t lo = wmin(a, b), hi = wmax(a, b);
         uint32_t& w = X.gw(hi, G_REGION);
         uint32_t old = w;
-        w = std::min(w, lo);
+        w = wmin(w, lo);
         if (old == hi) return;
         a = old;
         b = lo;
@@ -551,7 +558,7 @@ V2 prolonged(Ctx& X, uint32_t l, I2 c) {
             sum.y = sum.y + wt[k] * p.y;
         }
     }
-    float w = std::max(weight, 1e-6f);
+    float w = wmax(weight, 1e-6f);
     return V2{sum.x / w, sum.y / w};
 }
 
@@ -590,7 +597,7 @@ void pass_sync(Ctx& X, bool claims) {
                         uint32_t home = liquidHome(v[3]);
                         if (claims && wordHas(v[0], FL_DRAWN) && home < X.C) {
                             uint32_t& d = X.gw(home, G_DEST);
-                            d = std::max(d, claimOf(i));
+                            d = wmax(d, claimOf(i));
                         }
                         here = true;
                     }
@@ -605,7 +612,7 @@ void markBlockOf(Ctx& X, V2 pos) {
 }
 
 V2 pairWay(uint32_t a, uint32_t b) {
-    uint32_t h = pcg(std::min(a, b) ^ pcg(std::max(a, b)));
+    uint32_t h = pcg(wmin(a, b) ^ pcg(wmax(a, b)));
     float angle = (float)h * (float)(6.2831853 / 4294967296.0);
     float s, c;
     sincos_own(angle, &s, &c);
@@ -658,12 +665,12 @@ uint32_t sharedLife(Ctx& X, uint32_t life, uint32_t was, uint32_t now, uint32_t 
     if (now < was) l = l * (float)now / (float)was;
     else l = 255.0f - (255.0f - l) * (255.0f - (float)now) / (255.0f - (float)was);
     X.seedRng(id, X.P->frame, X.P->seed ^ 0x5a17u);
-    return std::min(f2u(std::floor(l + X.rnd())), 255u);
+    return wmin(f2u(std::floor(l + X.rnd())), 255u);
 }
 
 // syncParticles (fluid.wgsl:767-831); parts filled in sorted's order.
 void pass_syncParticles(Ctx& X) {
-    uint32_t live = std::min(X.sorted[0], X.cap);
+    uint32_t live = wmin(X.sorted[0], X.cap);
     for (uint32_t k = 0; k < live; k++) {
         bool keep = false;
         Particle q = X.toParticle(X.sorted, k);
@@ -745,7 +752,7 @@ void pass_syncSeed(Ctx& X) {
             if (!wordHas(v[0], FL_DRAWN)) {
                 n = X.ppc;
             } else if (home >= X.C || X.gw(home, G_DEST) != claimOf(i)) {
-                n = std::max(want, 1u);
+                n = wmax(want, 1u);
             } else if (want > X.gw(home, G_SORT) && want < LIQUID_COUNT_MAX) {
                 n = want - X.gw(home, G_SORT);
             }
@@ -1023,7 +1030,7 @@ float obstacleVelAxis(Ctx& X, I2 c, int axis) {
 float faceViscosity(V4 ga, V4 gb) {
     if (ga.z < 0.0f || gb.z < 0.0f) return 0.0f;
     float fa = ga.z > 0.0f ? 1.0f : 0.0f, fb = gb.z > 0.0f ? 1.0f : 0.0f;
-    return (fa * ga.w + fb * gb.w) / std::max(fa + fb, 1.0f);
+    return (fa * ga.w + fb * gb.w) / wmax(fa + fb, 1.0f);
 }
 bool wasLiquid(Ctx& X, I2 c) {
     uint32_t sb = 1u << ((X.P->frame + 1u) & 1u);
@@ -1100,7 +1107,7 @@ void viscousFace(Ctx& X, I2 at, bool isU, int color) {
             other = V4{op[0], op[1], op[2], op[3]};
         }
         float k = (d & 1) == 1 ? through.y : through.x;
-        if (across) k = other.z < 0.0f ? nu : 2.0f * nu * other.w / std::max(nu + other.w, 1e-12f);
+        if (across) k = other.z < 0.0f ? nu : 2.0f * nu * other.w / wmax(nu + other.w, 1e-12f);
         if (other.z < 0.0f) n = n + k * (across ? 2.0f : 1.0f);
         else if (other.z > 0.0f) { sum = sum + k * other.x; n = n + k; }
     }
@@ -1304,7 +1311,7 @@ void relaxTile(Ctx& X, uint32_t wid, int shift) {
             s.diag = s.bx + s.by + s.bz + s.bw;
             bool pinned = rho > 0.0f && pinnedAt(X, X.cellIndex(me));
             s.dx = s.diag + (pinned ? PIN : 0.0f);
-            s.dy = std::max(s.diag, 1e-30f);
+            s.dy = wmax(s.diag, 1e-30f);
             s.solving = s.dx > 0.0f;
             s.color = (me.x + me.y) & 1;
             s.t = t;
@@ -1402,7 +1409,7 @@ void pass_solve(Ctx& X) {
     if (X.converged()) return;
     uint32_t l = X.level;
     I2 size = levelSize(X, l);
-    uint32_t n = std::min((uint32_t)(size.x * size.y), WIG_MG_COARSEST);
+    uint32_t n = wmin((uint32_t)(size.x * size.y), WIG_MG_COARSEST);
     std::vector<V2> pot(n), rhs(n);
     std::vector<float> rho(n);
     for (uint32_t j = 0; j < n; j++) {
@@ -1674,10 +1681,10 @@ void pass_cgUpdate(Ctx& X) {
         g[0] = x; g[1] = r; g[2] = v.z; g[3] = v.w;
         X.fv(2u * i)[0] = 0.0f;
         X.fv(2u * i)[1] = -r;
-        most = std::max(most, bits(std::fabs(r)));
+        most = wmax(most, bits(std::fabs(r)));
     });
     uint32_t& slot = X.blocks[X.countSlot(COUNT_RESIDUAL + X.cycle % 3u)];
-    slot = std::max(slot, most);
+    slot = wmax(slot, most);
     if (X.tol_mode) {
         double rr = norm2Blocks(X, [&](I2 c) -> double {
             uint32_t i = X.cellIndex(c);
@@ -1698,7 +1705,7 @@ void pass_cgFinish(Ctx& X) {
 // projectFace, project (fluid.wgsl:2897-2942), no bodies.
 void pass_project(Ctx& X) {
     uint32_t& most = X.blocks[X.countSlot(COUNT_MOST_CYCLES)];
-    most = std::max(most, X.blocks[X.countSlot(COUNT_CYCLES)]);
+    most = wmax(most, X.blocks[X.countSlot(COUNT_CYCLES)]);
     forActiveCells(X, [&](uint32_t, I2 c, uint32_t) {
         if (!X.inWorld(c)) return;
         int fs[4][3];
@@ -1834,7 +1841,7 @@ V2 slipOf(Ctx& X, const Particle& q) {
     uint32_t n = X.gw(i, G_COUNT);
     if (n < 2u) return V2{0, 0};
     float mean = (float)X.gw(i, G_MASS) / (FIX * (float)n);
-    float lighter = (mean - X.liquidDensity(q.word, q.temp)) / std::max(mean, 1e-3f);
+    float lighter = (mean - X.liquidDensity(q.word, q.temp)) / wmax(mean, 1e-3f);
     V2 pull = X.pullAt(q.pos);
     float wgt = X.elem(WATER).weight;
     return V2{-pull.x / wgt * SLIP * lighter, -pull.y / wgt * SLIP * lighter};
@@ -1854,19 +1861,19 @@ void pass_advect(Ctx& X) {
         V2 cs = clampSpeed(vel);
         V2 sl = slipOf(X, q);
         V2 travel{cs.x + clampf(u.drift + sl.x, -MAX_DRIFT, MAX_DRIFT), cs.y + clampf(v.drift + sl.y, -MAX_DRIFT, MAX_DRIFT)};
-        int steps = std::min(std::max(f2i(std::ceil(std::max(std::fabs(travel.x), std::fabs(travel.y)) * 2.0f)), 1), ADVECT_STEPS);
+        int steps = wmin(wmax(f2i(std::ceil(wmax(std::fabs(travel.x), std::fabs(travel.y)) * 2.0f)), 1), ADVECT_STEPS);
         V2 d{travel.x / (float)steps, travel.y / (float)steps};
         V2 pos = q.pos;
         float impact = 0.0f;
         for (int s = 0; s < steps; s++) {
             V2 nx{pos.x + d.x, pos.y + 0.0f};
             if (d.x != 0.0f && isObstacle(X, nx)) {
-                if (vel.x * d.x > 0.0f) { impact = std::max(impact, std::fabs(vel.x)); vel.x = 0.0f; }
+                if (vel.x * d.x > 0.0f) { impact = wmax(impact, std::fabs(vel.x)); vel.x = 0.0f; }
                 d.x = 0.0f;
             } else pos = nx;
             V2 ny{pos.x + 0.0f, pos.y + d.y};
             if (d.y != 0.0f && isObstacle(X, ny)) {
-                if (vel.y * d.y > 0.0f) { impact = std::max(impact, std::fabs(vel.y)); vel.y = 0.0f; }
+                if (vel.y * d.y > 0.0f) { impact = wmax(impact, std::fabs(vel.y)); vel.y = 0.0f; }
                 d.y = 0.0f;
             } else pos = ny;
         }
@@ -1980,7 +1987,7 @@ void pass_rasterClaims(Ctx& X) {
         X.gw(i, G_AIR_TO) = to;
         if (to != NONE) {
             uint32_t& w = X.gw(to, G_TAKEN);
-            w = std::max(w, takenBy(i));
+            w = wmax(w, takenBy(i));
         }
     });
 }
@@ -2087,7 +2094,7 @@ void pass_raster(Ctx& X) {
             } else if (pt == most && solutes && wordAux(st[0]) == 0u) {
                 ly = ly + 1.0f;
             }
-            float hc = std::max(X.elem(pt).heat_cap, 1e-6f);
+            float hc = wmax(X.elem(pt).heat_cap, 1e-6f);
             heat = exact_add(heat, hc * flt(st[1]));
             capa = exact_add(capa, hc);
             uint32_t* mo = X.item(X.sorted, k);
@@ -2095,7 +2102,7 @@ void pass_raster(Ctx& X) {
             vy = exact_add(vy, flt(mo[3]));
         }
         X.seedRng(i, X.P->frame, X.P->seed ^ 0x7a57u);
-        uint32_t life = std::min(f2u(std::floor(lx / ly + X.rnd())), 255u);
+        uint32_t life = wmin(f2u(std::floor(lx / ly + X.rnd())), 255u);
         word = packWord(wordType(word), wordAux(word), life, wordShade(word), wordFlags(word));
         float temp = exact_value(heat, EXACT_FINE) / exact_value(capa, EXACT_FINE);
         float velx = exact_value(vx, EXACT_FINE) / (float)n, vely = exact_value(vy, EXACT_FINE) / (float)n;
@@ -2221,6 +2228,58 @@ void run_pass(Ctx& X, int pass) {
     default: break;
     }
 }
+
+// The pressure operator of the FP64 solves: per fluid cell (in cell order)
+// its four neighbours' rows and betas (fineBeta, the liquid neighbours
+// only), its diagonal (the betas of every non-solid side, PIN at the root
+// of a closed region) and the right-hand side -b.
+struct F64System {
+    struct Row { int32_t nb[4]; double beta[4]; double diag; };
+    std::vector<uint32_t> cellsOf;
+    std::vector<Row> rows;
+    std::vector<double> rhs;
+    size_t n() const { return cellsOf.size(); }
+    void build(Ctx& X) {
+        std::vector<int32_t> idx(X.C, -1);
+        for (uint32_t i = 0; i < X.C; i++)
+            if (X.fv(2u * i)[2] > 0.0f) { idx[i] = (int32_t)cellsOf.size(); cellsOf.push_back(i); }
+        rows.resize(n());
+        rhs.resize(n());
+        for (size_t k = 0; k < n(); k++) {
+            uint32_t i = cellsOf[k];
+            I2 c{(int)(i % (uint32_t)X.W), (int)(i / (uint32_t)X.W)};
+            float rho = X.fv(2u * i)[2];
+            Row& r = rows[k];
+            r.diag = 0.0;
+            float share = X.shareAt(c);
+            for (int dd = 0; dd < 4; dd++) {
+                I2 nn = Ctx::beside(c, dd);
+                r.nb[dd] = -1;
+                r.beta[dd] = 0.0;
+                float rr = rhoAt(X, 0, nn);
+                if (rr < 0.0f) continue;
+                double beta = (double)fineBeta(rho, rr, share, X.shareAt(nn));
+                if (rr > 0.0f) { r.nb[dd] = idx[X.cellIndex(nn)]; r.beta[dd] = beta; }
+                r.diag += beta;
+            }
+            if (pinnedAt(X, i)) r.diag += (double)PIN;
+            rhs[k] = -(double)X.fv(2u * i)[1];
+        }
+    }
+    void apply(const std::vector<double>& p, std::vector<double>& q) const {
+        for (size_t k = 0; k < n(); k++) {
+            double s = rows[k].diag * p[k];
+            for (int dd = 0; dd < 4; dd++)
+                if (rows[k].nb[dd] >= 0) s -= rows[k].beta[dd] * p[rows[k].nb[dd]];
+            q[k] = s;
+        }
+    }
+    void scatter(const std::vector<double>& x, uint32_t C, double* out) const {
+        if (!out) return;
+        for (uint32_t i = 0; i < C; i++) out[i] = 0.0;
+        for (size_t k = 0; k < n(); k++) out[cellsOf[k]] = x[k];
+    }
+};
 
 }  // namespace
 
@@ -2356,56 +2415,22 @@ int wo_solve_f64(const wig_world_desc* d, const wig_params* P, const wig_elem* E
     if (rc) return rc;
     Ctx X;
     setup(X, L, P, E, nE, b);
-    uint32_t C = X.C;
-    std::vector<int32_t> idx(C, -1);
-    std::vector<uint32_t> cellsOf;
-    for (uint32_t i = 0; i < C; i++)
-        if (X.fv(2u * i)[2] > 0.0f) { idx[i] = (int32_t)cellsOf.size(); cellsOf.push_back(i); }
-    size_t n = cellsOf.size();
-    struct Row { int32_t nb[4]; double beta[4]; double diag; };
-    std::vector<Row> rows(n);
-    std::vector<double> rhs(n);
-    for (size_t k = 0; k < n; k++) {
-        uint32_t i = cellsOf[k];
-        I2 c{(int)(i % (uint32_t)X.W), (int)(i / (uint32_t)X.W)};
-        float rho = X.fv(2u * i)[2];
-        Row& r = rows[k];
-        r.diag = 0.0;
-        float share = X.shareAt(c);
-        for (int dd = 0; dd < 4; dd++) {
-            I2 nn = Ctx::beside(c, dd);
-            r.nb[dd] = -1;
-            r.beta[dd] = 0.0;
-            float rr = rhoAt(X, 0, nn);
-            if (rr < 0.0f) continue;
-            double beta = (double)fineBeta(rho, rr, share, X.shareAt(nn));
-            if (rr > 0.0f) { r.nb[dd] = idx[X.cellIndex(nn)]; r.beta[dd] = beta; }
-            r.diag += beta;
-        }
-        if (pinnedAt(X, i)) r.diag += (double)PIN;
-        rhs[k] = -(double)X.fv(2u * i)[1];
-    }
-    auto apply = [&](const std::vector<double>& p, std::vector<double>& q) {
-        for (size_t k = 0; k < n; k++) {
-            double s = rows[k].diag * p[k];
-            for (int dd = 0; dd < 4; dd++)
-                if (rows[k].nb[dd] >= 0) s -= rows[k].beta[dd] * p[rows[k].nb[dd]];
-            q[k] = s;
-        }
-    };
-    std::vector<double> x(n, 0.0), r(rhs), z(n), p(n), q(n);
+    F64System S;
+    S.build(X);
+    const size_t n = S.n();
+    std::vector<double> x(n, 0.0), r(S.rhs), z(n), p(n), q(n);
     double bn = 0.0;
-    for (double v : rhs) bn += v * v;
+    for (double v : S.rhs) bn += v * v;
     bn = std::sqrt(bn);
     uint32_t it = 0;
     double rel = 0.0;
     if (bn > 0.0) {
-        for (size_t k = 0; k < n; k++) z[k] = rows[k].diag > 0.0 ? r[k] / rows[k].diag : r[k];
+        for (size_t k = 0; k < n; k++) z[k] = S.rows[k].diag > 0.0 ? r[k] / S.rows[k].diag : r[k];
         p = z;
         double rz = 0.0;
         for (size_t k = 0; k < n; k++) rz += r[k] * z[k];
         for (it = 0; it < max_iter; it++) {
-            apply(p, q);
+            S.apply(p, q);
             double pq = 0.0;
             for (size_t k = 0; k < n; k++) pq += p[k] * q[k];
             if (pq <= 0.0) break;
@@ -2415,16 +2440,101 @@ int wo_solve_f64(const wig_world_desc* d, const wig_params* P, const wig_elem* E
             rel = std::sqrt(rr) / bn;
             if (rel <= rel_tol) { it++; break; }
             double rz2 = 0.0;
-            for (size_t k = 0; k < n; k++) { z[k] = rows[k].diag > 0.0 ? r[k] / rows[k].diag : r[k]; rz2 += r[k] * z[k]; }
+            for (size_t k = 0; k < n; k++) { z[k] = S.rows[k].diag > 0.0 ? r[k] / S.rows[k].diag : r[k]; rz2 += r[k] * z[k]; }
             double beta = rz2 / rz;
             rz = rz2;
             for (size_t k = 0; k < n; k++) p[k] = z[k] + beta * p[k];
         }
     }
-    if (x_out) {
-        for (uint32_t i = 0; i < C; i++) x_out[i] = 0.0;
-        for (size_t k = 0; k < n; k++) x_out[cellsOf[k]] = x[k];
+    S.scatter(x, X.C, x_out);
+    if (rel_out) *rel_out = rel;
+    return (int)it;
+}
+
+// The same FP64 solve (operator, right-hand side, output) with one V-cycle
+// of this oracle's own FP32 passes as the preconditioner, for worlds where
+// the Jacobi form needs thousands of iterations (2048 x 2048).  The outer
+// iteration is flexible CG in double: beta = -(z . q_prev) / (p_prev . q_prev)
+// (the reference's flexible beta, fluid.wgsl:2752-2764), alpha = (p . r) /
+// (p . q), every vector, dot product and residual FP64.  The preconditioner
+// puts r, scaled to a largest entry of 1, into field's right-hand sides
+// (-r, as cgPrepare and cgUpdate leave them, fluid.wgsl:2721-2732,
+// :2852-2880), zeroes the potentials, runs relaxRims, relax, restrict and
+// smooth down the levels, solve, prolong and smooth up, prolongFine,
+// relaxRims, relax (encodeFluid's cycle, js/sim.js:2557-2588), and reads z
+// back from the potentials.  Its FP32 rounding bounds how much one
+// iteration gains, not the accuracy reached: the residual is FP64 and the
+// solve runs to rel_tol.  The buffers hold the V-cycle's scratch afterwards
+// (potentials, coarse levels, rims), so callers solve on a copy.
+int wo_solve_f64_mg(const wig_world_desc* d, const wig_params* P, const wig_elem* E, uint32_t nE, wig_fluid_buffers* b,
+                    double rel_tol, uint32_t max_iter, double* x_out, double* rel_out) {
+    wig_world_layout L;
+    int rc = layout(d, &L);
+    if (rc) return rc;
+    Ctx X;
+    setup(X, L, P, E, nE, b);
+    F64System S;
+    S.build(X);
+    const size_t n = S.n();
+    // every pass of the cycle runs: the tolerance form's test with rel above tol
+    X.tol_mode = true;
+    X.tol = 0.0;
+    X.rel = 1.0;
+    X.cycle = 0;
+    bool sh = false;
+    auto vcycle = [&](const std::vector<double>& r, std::vector<double>& z) {
+        double scale = 0.0;
+        for (double v : r) scale = wmax(scale, std::fabs(v));
+        if (scale == 0.0) scale = 1.0;
+        for (uint32_t i = 0; i < X.C; i++) X.fv(2u * i)[0] = 0.0f;
+        for (size_t k = 0; k < n; k++) X.fv(2u * S.cellsOf[k])[1] = (float)(-r[k] / scale);
+        auto run = [&](int pass, uint32_t level) { X.level = level; run_pass(X, pass); };
+        const uint32_t deepest = L.levels;
+        run(WIG_PASS_RELAX_RIMS, 0);
+        run(sh ? WIG_PASS_RELAX_SHIFTED : WIG_PASS_RELAX, 0);
+        sh = !sh;
+        for (uint32_t l = 1; l <= deepest; l++) {
+            run(WIG_PASS_RESTRICT, l);
+            if (l < deepest) { run(WIG_PASS_SMOOTH_RED, l); run(WIG_PASS_SMOOTH_BLACK, l); }
+        }
+        run(WIG_PASS_SOLVE, deepest);
+        for (uint32_t l = deepest - 1; l >= 1; l--) {
+            run(WIG_PASS_PROLONG, l);
+            run(WIG_PASS_SMOOTH_RED, l);
+            run(WIG_PASS_SMOOTH_BLACK, l);
+        }
+        run(WIG_PASS_PROLONG_FINE, 0);
+        run(WIG_PASS_RELAX_RIMS, 0);
+        run(sh ? WIG_PASS_RELAX_SHIFTED : WIG_PASS_RELAX, 0);
+        sh = !sh;
+        for (size_t k = 0; k < n; k++) z[k] = scale * (double)X.fv(2u * S.cellsOf[k])[0];
+    };
+    auto dot = [&](const std::vector<double>& a, const std::vector<double>& c) {
+        double s = 0.0;
+        for (size_t k = 0; k < n; k++) s += a[k] * c[k];
+        return s;
+    };
+    std::vector<double> x(n, 0.0), r(S.rhs), z(n), p(n, 0.0), q(n, 0.0);
+    const double bn = std::sqrt(dot(S.rhs, S.rhs));
+    uint32_t it = 0;
+    double rel = bn > 0.0 ? 1.0 : 0.0, pq_prev = 0.0;
+    if (bn > 0.0) {
+        for (it = 0; it < max_iter; it++) {
+            vcycle(r, z);
+            const double beta = (it == 0 || pq_prev <= 0.0) ? 0.0 : -dot(z, q) / pq_prev;
+            for (size_t k = 0; k < n; k++) p[k] = z[k] + beta * p[k];
+            S.apply(p, q);
+            const double pq = dot(p, q);
+            if (pq <= 0.0) break;
+            const double a = dot(p, r) / pq;
+            double rr = 0.0;
+            for (size_t k = 0; k < n; k++) { x[k] += a * p[k]; r[k] -= a * q[k]; rr += r[k] * r[k]; }
+            pq_prev = pq;
+            rel = std::sqrt(rr) / bn;
+            if (rel <= rel_tol) { it++; break; }
+        }
     }
+    S.scatter(x, X.C, x_out);
     if (rel_out) *rel_out = rel;
     return (int)it;
 }

@@ -126,6 +126,42 @@ def test_fp32_solve_against_fp64_solve():
     assert true_rel < 1e-3
 
 
+@pytest.mark.parametrize("builder", [lambda: W.dam_break(128, 128), lambda: W.small_world(96, 80, seed=4, kind="obstacles")])
+def test_multigrid_fp64_solve_matches_jacobi_fp64_solve(builder):
+    """The FP64 solve preconditioned by the oracle's V-cycle (for the large
+    worlds) reaches the same solution as the Jacobi-preconditioned one, in
+    far fewer iterations."""
+    world = builder()
+    _run(world, 3, flags=abi.STEP_TOLERANCE | abi.STEP_F64_DOTS, max_cycles=48)
+    P = params(world, 4)
+    seq = ("SYNC", "SYNC_PARTICLES", "SYNC_SEED", "COMPACT", "RETIRE", "CLEAR", "GATHER", "SEAL_JOIN",
+           "SEAL_ANCHOR", "CLASSIFY", "SET_FACES", "UNPRESS", "DIVERGENCE", "CG_START", "CG_JOIN", "CG_ANCHOR")
+    po = Oracle(world, W.element_table())
+    for name in seq:
+        po.pass_(P, name)
+    xj, itj, relj = Oracle(world.copy(), W.element_table()).solve_f64(P, rel_tol=1e-12)
+    xm, itm, relm = Oracle(world.copy(), W.element_table()).solve_f64(P, rel_tol=1e-12, multigrid=True)
+    assert relj <= 1e-12 and relm <= 1e-12
+    assert itm < itj / 4, (itm, itj)
+    assert np.linalg.norm(xm - xj) <= 1e-9 * np.linalg.norm(xj)
+
+
+def test_min_max_take_wgsl_nan_rule():
+    """f32 min and max in the oracle follow WGSL's builtins (a NaN operand
+    gives the other one), as the GPU's fminf and fmaxf do, so non-finite
+    particles step alike on both: checked through the sub-step count of a
+    travel with one NaN component, which a std::max would make NaN."""
+    world = W.small_world(32, 32, seed=7, kind="dam")
+    _run(world, 2)
+    m = world.sorted[4:].reshape(3, world.cap, 4)[0].view(np.float32)
+    n = int(world.sorted[0])
+    m[n // 2, 2] = np.float32("nan")
+    o = Oracle(world, W.element_table())
+    o.step(params(world, 3))
+    assert int(world.sorted[0]) > 0
+    assert np.all(np.isfinite(world.pressure()))
+
+
 @pytest.mark.parametrize("case", [c[0] for c in CASES])
 def test_oracle_matches_golden_fixtures(case):
     with open(os.path.join(HERE, "golden", "oracle_steps.json")) as f:
