@@ -330,7 +330,18 @@ int wig_fluid_set_launch(wig_fluid* h, uint32_t knob, uint32_t value);
 int wig_fluid_get_launch(const wig_fluid* h, uint32_t knob, uint32_t* value);
 
 /* Replaces readReport (js/sim.js:1882-1900): waits for the stream and reads
- * the FLUID_COUNT words and the solve's statistics of the last step. */
+ * the FLUID_COUNT words and the solve's statistics of the last step.  The
+ * report is filled in whatever the return code.  WIG_E_NOT_CONVERGED: the
+ * step ran WIG_STEP_TOLERANCE with a nonzero right-hand side and its solve
+ * stopped after max_cycles with rel_residual above the tolerance (the step
+ * is complete; a host that adapts max_cycles from the report, as
+ * js/sim.js:1896-1900 adapts fluidCycles, raises it).  The reference's own
+ * criterion (max|r| < 1e-2, without WIG_STEP_TOLERANCE) reports no such
+ * error: it stops at max_cycles as the reference does.  WIG_E_CAPACITY: the
+ * step's sync and seeding put more particles into `parts` than its
+ * capacity (fluid.wgsl:104-107, :827-830); those past the room are lost.
+ * WIG_E_STATE (a device loop gave up at its bound) takes precedence over
+ * WIG_E_CAPACITY, which takes precedence over WIG_E_NOT_CONVERGED. */
 int wig_fluid_read_stats(wig_fluid* h, wig_fluid_stats* out);
 
 void wig_fluid_destroy(wig_fluid* h);
@@ -353,6 +364,25 @@ void wig_fluid_destroy(wig_fluid* h);
 #define WIG_NOALLOC_MAX_BLOCKS 16384u
 int wig_fluid_residual_norm2_noalloc(const wig_world_desc* d, const void* field, const void* blocks, const void* cg,
                                      double* out, void* stream);
+
+/* No counterpart in the reference.  The allocation-free entry point keeps
+ * its array's device address per device for the process's life; a host that
+ * destroys and recreates the current device's primary context
+ * (cudaDeviceReset) calls this afterwards, so the next call looks the
+ * address up again in the new context. */
+int wig_fluid_noalloc_forget_device(void);
+
+/* No counterpart in the reference.  Lowers the bounds of the device's
+ * waits on the current device, for every kernel launched after the call
+ * (graphs already captured included): loop_limit bounds each lock-free
+ * retry loop (the union-find of sealJoin and cgJoin, label.wgsl:27-55),
+ * spin_limit the polls of the persistent form's grid barrier.  0 restores a
+ * default (2^22 retries; 2^23 polls of about 64 ns).  A loop that runs out
+ * gives up, and the step's stats read returns WIG_E_STATE; nothing hangs
+ * and the device stays usable.  For tests of those failure paths: a host
+ * has no other reason to call it.  Limits above the defaults are refused
+ * with WIG_E_ARG.  Synchronous (it writes two device words). */
+int wig_fluid_set_wait_limits(uint32_t loop_limit, uint32_t spin_limit);
 
 /* One-line description of the last error on this thread ("" if none). */
 const char* wig_fluid_last_error(void);

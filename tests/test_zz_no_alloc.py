@@ -32,7 +32,14 @@ def _entry():
     return fluid, f
 
 
-def test_noalloc_norm_matches_the_step_on_two_calls():
+# the step's forms: one kernel a reference pass, the fast form (the default),
+# and the mixed-precision form, whose residual reaches cg through the fast
+# form's write-back and may have been replaced by the true residual
+FORMS = {"plain": abi.STEP_PLAIN, "fast": 0, "mixed": abi.STEP_MIXED}
+
+
+@pytest.mark.parametrize("form", ["plain", "fast", "mixed"])
+def test_noalloc_norm_matches_the_step_on_two_calls(form):
     import torch
     fluid, f = _entry()
     world = W.dam_break(64, 64)
@@ -40,7 +47,8 @@ def test_noalloc_norm_matches_the_step_on_two_calls():
     out = torch.full((1,), -1.0, dtype=torch.float64, device="cuda")
     d = world.desc()
     for s in (1, 2):
-        g.step(params(world, s), max_cycles=48, flags=abi.STEP_TOLERANCE | abi.STEP_F64_DOTS, tolerance=1e-6)
+        g.step(params(world, s), max_cycles=48, flags=abi.STEP_TOLERANCE | abi.STEP_F64_DOTS | FORMS[form],
+               tolerance=1e-6)
         st = g.stats()
         b = g.buffers()
         rc = f(C.byref(d), b.field, b.blocks, b.cg, C.c_void_p(out.data_ptr()), None)

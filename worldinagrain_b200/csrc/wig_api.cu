@@ -40,6 +40,8 @@ int fail(int code, const std::string& msg) {
 
 namespace wig {
 void set_last_error(const std::string& msg) { g_last_error = msg; }
+__device__ uint32_t g_loop_limit = LOOP_LIMIT;
+__device__ uint32_t g_spin_limit = BARRIER_SPIN_LIMIT;
 }  // namespace wig
 
 namespace {
@@ -56,7 +58,8 @@ struct Report {
     uint32_t count[WIG_FLUID_STATS];
     uint32_t particles;
     uint32_t err;
-    uint32_t pad;
+    uint32_t short_of_tol;  // a tolerance-form solve of a nonzero b stopped above its tolerance
+    uint32_t tried;         // particles the step's sync and seeding put into `parts` (past its room: lost)
     double rel;
     double bnorm2;
     double rel_true;
@@ -72,8 +75,11 @@ __global__ void k_report(wig::Batch Bt, Report* by_world, Report* by_entry) {
         Report r;
         for (uint32_t c = 0; c < WIG_FLUID_STATS; c++) r.count[c] = D.blocks[4u * D.B + c];
         r.particles = D.sorted[0];
+        r.tried = D.parts[0];
         r.err = D.st->err;
-        r.pad = 0u;
+        // a full step of the tolerance form whose solve stopped (max_cycles
+        // run) with the residual still above the tolerance
+        r.short_of_tol = (D.st->tol_mode && !D.st->book && D.st->bnorm2 > 0.0 && D.st->rel > D.st->tol) ? 1u : 0u;
         r.rel = D.st->rel;
         r.bnorm2 = D.st->bnorm2;
         r.rel_true = D.st->rel_true;
@@ -1121,6 +1127,15 @@ int batch_step_profile(wig_batch* b, const StepArgs& a, float* ms_out, uint32_t*
     return WIG_OK;
 }
 
+int severity(int rc) {
+    switch (rc) {
+    case WIG_OK: return 0;
+    case WIG_E_NOT_CONVERGED: return 1;
+    case WIG_E_CAPACITY: return 2;
+    default: return 3;
+    }
+}
+
 int batch_read_stats(wig_batch* b, const uint32_t* worlds, uint32_t count, wig_fluid_stats* out) {
     if (!b || !worlds || !out) return fail(WIG_E_ARG, "null argument");
     std::vector<cudaStream_t> waited;
@@ -1152,10 +1167,26 @@ int batch_read_stats(wig_batch* b, const uint32_t* worlds, uint32_t count, wig_f
         o.rel_residual = r.rel;
         o.b_norm = r.bnorm2 > 0.0 ? __builtin_sqrt(r.bnorm2) : 0.0;
         o.true_residual = r.rel_true;
-        if (rc == WIG_OK) {
-            if (r.err & wig::ERR_BARRIER) rc = fail(WIG_E_STATE, "the persistent solve's grid barrier waited past its limit");
-            else if (r.err) rc = fail(WIG_E_STATE, "a device loop hit its iteration limit (union-find)");
-            else if (r.particles > b->L[k].capacity) rc = fail(WIG_E_CAPACITY, "more particles than the buffers hold");
+        // the most severe of the worlds' conditions is returned, every
+        // world's report filled in all the same: a device loop that gave up,
+        // then particles past the capacity, then a solve short of its
+        // tolerance
+        if (r.err & wig::ERR_BARRIER) {
+            if (severity(rc) < severity(WIG_E_STATE))
+                rc = fail(WIG_E_STATE, "the persistent solve's grid barrier waited past its limit");
+        } else if (r.err) {
+            if (severity(rc) < severity(WIG_E_STATE))
+                rc = fail(WIG_E_STATE, "a device loop hit its iteration limit (union-find)");
+        } else if (r.tried > b->L[k].capacity) {
+            if (severity(rc) < severity(WIG_E_CAPACITY))
+                rc = fail(WIG_E_CAPACITY, "world " + std::to_string(k) + ": " + std::to_string(r.tried) +
+                                              " particles for room for " + std::to_string(b->L[k].capacity) +
+                                              "; those past the room were lost");
+        } else if (r.short_of_tol) {
+            if (severity(rc) < severity(WIG_E_NOT_CONVERGED))
+                rc = fail(WIG_E_NOT_CONVERGED, "world " + std::to_string(k) + ": the solve left a relative residual of " +
+                                                   std::to_string(r.rel) + " after " +
+                                                   std::to_string(r.count[WIG_COUNT_CYCLES]) + " iterations");
         }
     }
     return rc;
@@ -1189,6 +1220,16 @@ int copy_world(wig_batch* b, uint32_t k, int which, void* host, uint64_t offset,
 extern "C" {
 
 uint32_t wig_fluid_abi_version(void) { return WIG_ABI_VERSION; }
+
+int wig_fluid_set_wait_limits(uint32_t loop_limit, uint32_t spin_limit) {
+    const uint32_t lo = loop_limit ? loop_limit : wig::LOOP_LIMIT;
+    const uint32_t sp = spin_limit ? spin_limit : wig::BARRIER_SPIN_LIMIT;
+    if (lo > wig::LOOP_LIMIT || sp > wig::BARRIER_SPIN_LIMIT)
+        return fail(WIG_E_ARG, "wait limits may only be lowered");
+    CUDA_TRY(cudaMemcpyToSymbol(wig::g_loop_limit, &lo, sizeof(lo)));
+    CUDA_TRY(cudaMemcpyToSymbol(wig::g_spin_limit, &sp, sizeof(sp)));
+    return WIG_OK;
+}
 
 const char* wig_fluid_last_error(void) { return g_last_error.c_str(); }
 

@@ -61,6 +61,11 @@ constexpr uint32_t ERR_LOOP = 1u, ERR_CAPACITY = 2u, ERR_BARRIER = 4u;
 // A grid barrier's wait: at most this many polls of ~64 ns (about half a
 // second), past which the kernel records ERR_BARRIER and returns.
 constexpr uint32_t BARRIER_SPIN_LIMIT = 1u << 23;
+// The bounds in force on a device (the two above unless
+// wig_fluid_set_wait_limits lowered them, which the failure-path tests do to
+// see the error come back); read by the loops at run time.
+extern __device__ uint32_t g_loop_limit;
+extern __device__ uint32_t g_spin_limit;
 
 // What the host writes for a world before each step: its Params, the
 // solve's stopping rule, and its part of the step (a batch steps worlds with

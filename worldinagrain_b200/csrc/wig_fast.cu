@@ -1680,7 +1680,7 @@ __global__ void k_fFinish(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, i
 // same order of every sum as the passes.
 
 // A grid barrier (all CTAs are resident: cooperative launch).  Each wait is
-// bounded: past BARRIER_SPIN_LIMIT polls it records ERR_BARRIER and every CTA
+// bounded: past g_spin_limit polls it records ERR_BARRIER and every CTA
 // returns false from here on.
 __device__ bool gridBarrier(StepState* st, uint32_t nblocks) {
     __shared__ int s_ok;
@@ -1697,8 +1697,9 @@ __device__ bool gridBarrier(StepState* st, uint32_t nblocks) {
             atomicAdd(&st->bar_gen, 1u);
         } else {
             uint32_t it = 0;
+            const uint32_t limit = g_spin_limit;
             while (*gen == g0) {
-                if (++it > BARRIER_SPIN_LIMIT) {
+                if (++it > limit) {
                     atomicOr(&st->err, ERR_BARRIER);
                     ok = 0;
                     break;

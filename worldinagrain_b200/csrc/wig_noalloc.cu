@@ -18,7 +18,8 @@
 // exits.  The array's name in host code is only a host-side stand-in, so the
 // host takes the array's device address once per device with
 // cudaGetSymbolAddress (the first call on a device does that set-up) and
-// passes it to the kernels.  Every call shares the one array: calls whose
+// passes it to the kernels.  That address is kept until
+// wig_fluid_noalloc_forget_device, which a host that resets a device calls.  Every call shares the one array: calls whose
 // work overlaps on the GPU (two streams, or two host threads) race on it.
 
 #include <cstdint>
@@ -46,14 +47,15 @@ int set_error(int code, const std::string& msg) {
 
 // Squared residual of the liquid cells of each block worked on (cg's y,
 // the CG residual r, where field's z > 0), a tree of 64 per block, as the
-// step's tolerance form sums it (k_cgUpdate).
+// step's tolerance form sums it (k_cgUpdate).  The blocks worked on are
+// those whose state word has ACTIVE set, the same set k_sum_partials reads,
+// so no partial left from an earlier call (of this world or another) can
+// enter the sum, whatever the active list holds.
 __global__ void __launch_bounds__(64) k_block_r2(uint32_t W, uint32_t H, uint32_t B, uint32_t BW, const uint32_t* blocks,
                                                  const float4* field, const float4* cg, double* partials) {
     __shared__ double s[64];
-    const uint32_t na = min(blocks[4u * B + WIG_COUNT_ACTIVE], B);
-    for (uint32_t wid = blockIdx.x; wid < na; wid += gridDim.x) {
-        const uint32_t n = blocks[2u * B + wid];
-        if (n >= B) continue;  // a corrupt list entry: skipped (uniform in the CTA)
+    for (uint32_t n = blockIdx.x; n < B; n += gridDim.x) {
+        if ((blocks[B + n] & 1u) == 0u) continue;  // not worked on (uniform in the CTA)
         const uint32_t bx = n % BW, by = n / BW;
         const uint32_t x = bx * 8u + (threadIdx.x & 7u), y = by * 8u + (threadIdx.x >> 3);
         double v = 0.0;
@@ -92,7 +94,9 @@ __global__ void __launch_bounds__(256) k_sum_partials(uint32_t B, const uint32_t
 }
 
 // The device address of g_block_partials on the current device, looked up
-// once per device.
+// once per device and kept for the process's life: a host that destroys and
+// recreates a device's primary context (cudaDeviceReset) loads the module
+// anew, so it must call wig_fluid_noalloc_forget_device afterwards.
 int partials_on_current_device(double** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
@@ -133,6 +137,16 @@ int wig_fluid_residual_norm2_noalloc(const wig_world_desc* d, const void* field,
     k_sum_partials<<<1, 256, 0, s>>>((uint32_t)B, (const uint32_t*)blocks, partials, out);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(WIG_E_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+    return WIG_OK;
+}
+
+int wig_fluid_noalloc_forget_device(void) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return set_error(WIG_E_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
+    if (dev < 0 || (uint32_t)dev >= MAX_DEVICES) return set_error(WIG_E_ARG, "device ordinal past the ones this entry point keeps");
+    std::lock_guard<std::mutex> lock(g_mutex);
+    g_partials_of[dev] = nullptr;
     return WIG_OK;
 }
 

@@ -37,7 +37,8 @@ __device__ __forceinline__ uint32_t vload(const uint32_t* p) { return *(const vo
 // union-find over G_REGION words (label.wgsl:27-55), lock-free by atomicMin.
 __device__ uint32_t ufFind(const W& w, uint32_t i) {
     uint32_t x = i;
-    for (uint32_t it = 0; it < LOOP_LIMIT; it++) {
+    const uint32_t limit = g_loop_limit;
+    for (uint32_t it = 0; it < limit; it++) {
         uint32_t up = vload(w.gwp(x, G_REGION));
         if (up >= x) return x;
         x = up;
@@ -47,7 +48,8 @@ __device__ uint32_t ufFind(const W& w, uint32_t i) {
 }
 __device__ void ufJoin(const W& w, uint32_t i, uint32_t j) {
     uint32_t a = i, b = j;
-    for (uint32_t it = 0; it < LOOP_LIMIT; it++) {
+    const uint32_t limit = g_loop_limit;
+    for (uint32_t it = 0; it < limit; it++) {
         a = ufFind(w, a);
         b = ufFind(w, b);
         if (a == b) return;

@@ -50,11 +50,25 @@ FUNCS = {
     "wig_fluid_set_launch": ([C.c_void_p, C.c_uint32, C.c_uint32], C.c_int),
     "wig_fluid_get_launch": ([C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)], C.c_int),
     "wig_batch_get_launch": ([C.c_void_p, C.c_uint32, C.POINTER(C.c_uint32)], C.c_int),
+    "wig_fluid_set_wait_limits": ([C.c_uint32, C.c_uint32], C.c_int),
 }
 
 
 class WigError(RuntimeError):
     pass
+
+
+class NotConverged(WigError):
+    """WIG_E_NOT_CONVERGED from a stats read: a tolerance-form solve stopped
+    after max_cycles above its tolerance.  The step itself is complete;
+    `stats` holds the report (one Stats, or a list for a batch)."""
+
+    def __init__(self, msg, stats):
+        super().__init__(msg)
+        self.stats = stats
+
+
+E_NOT_CONVERGED = -5
 
 
 def lib(path=None):
@@ -159,10 +173,28 @@ class LiquidStep:
     def dispatch(self, P, name, level=0, cycle=0):
         check(lib().wig_fluid_dispatch(self.h, C.byref(P), abi.PASS[name], level, cycle, self.stream), f"dispatch {name}")
 
-    def stats(self):
+    def stats(self, unconverged_ok=False):
+        """The last step's report (wig_fluid_read_stats).  A solve short of
+        its tolerance raises NotConverged unless unconverged_ok."""
         st = abi.Stats()
-        check(lib().wig_fluid_read_stats(self.h, C.byref(st)), "wig_fluid_read_stats")
-        return st
+        rc = lib().wig_fluid_read_stats(self.h, C.byref(st))
+        return _stats_or_raise(rc, st, unconverged_ok, "wig_fluid_read_stats")
+
+
+def set_wait_limits(loop_limit=0, spin_limit=0):
+    """Lowers the device's retry and barrier-wait bounds on the current
+    device (0: the default) so a failure-path test sees them run out."""
+    check(lib().wig_fluid_set_wait_limits(loop_limit, spin_limit), "wig_fluid_set_wait_limits")
+
+
+def _stats_or_raise(rc, stats, unconverged_ok, what):
+    if rc == E_NOT_CONVERGED:
+        if unconverged_ok:
+            return stats
+        msg = lib().wig_fluid_last_error().decode(errors="replace")
+        raise NotConverged(f"{what}: WIG_E_NOT_CONVERGED: {msg}", stats)
+    check(rc, what)
+    return stats
 
 
 def world_bytes(width, height, liquid_per_cell=4, capacity=0):
@@ -257,11 +289,13 @@ class Batch:
                                            C.c_void_p(stream or None), ms, calls), "wig_batch_step_profile")
         return {abi.PROFILE_NAMES[k]: (ms[k], calls[k]) for k in range(abi.PROFILE_SLOTS) if calls[k]}
 
-    def stats(self, ids):
+    def stats(self, ids, unconverged_ok=False):
+        """The worlds' reports (wig_batch_read_stats); NotConverged as for
+        LiquidStep.stats."""
         ids = list(ids)
         out = (abi.Stats * len(ids))()
-        check(lib().wig_batch_read_stats(self.h, _u32s(ids), len(ids), out), "wig_batch_read_stats")
-        return list(out)
+        rc = lib().wig_batch_read_stats(self.h, _u32s(ids), len(ids), out)
+        return _stats_or_raise(rc, list(out), unconverged_ok, "wig_batch_read_stats")
 
     def set_launch(self, knob, value):
         """One launch shape (abi.LAUNCH_KNOBS: a name or its number); no
