@@ -166,3 +166,27 @@ def test_snapshot_worlds_carry_their_state_into_the_backend():
     assert [p.frame for p in P] == [8, 1]
     assert be.has_state == [True, True]
     assert be._world_flags([0, 1]) is None  # later steps: the handle flips the parity itself
+
+
+def test_requests_that_can_never_fit_are_refused_not_left_pending():
+    """A world larger than the whole budget, or whose step borrows more than
+    a lane pool holds, can never be admitted: its requests are refused on
+    arrival (the loop ends, the budget holds) and the rest are served."""
+    clock = FakeClock()
+    sizes = [50, 50, 5000, 50]
+    be = FakeBackend(sizes, step_s=0.002, clock=clock, step_sizes=[3, 30, 3, 3], pool=12)
+    srv = serve.Server(be, len(sizes), 1000, clock=clock)
+    srv.preload()
+    assert 2 not in srv.resident
+    arr = [(0.0005 * i, i % 4) for i in range(40)]
+    done = srv.run(arr)
+    assert len(done) == 40
+    refused = [r for r in done if r.refused]
+    assert {r.world for r in refused} == {1, 2} and len(refused) == 20
+    assert "budget" in next(r for r in refused if r.world == 2).refused
+    assert "lane pool" in next(r for r in refused if r.world == 1).refused
+    assert all(ev[0] != "admit" or ev[1] != 2 for ev in be.log)
+    s = serve.latency_summary(done, lambda k: 1)
+    assert s["requests"] == 20 and s["refused_requests"] == 20
+    part = serve.latency_part(done, lambda k: 1)
+    assert serve.merge_parts([part])["refused_requests"] == 20

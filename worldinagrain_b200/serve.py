@@ -41,6 +41,7 @@ class Request:
     t_done: float = 0.0
     lane: int = -1
     swapped: bool = False
+    refused: str = ""  # why the request was refused on arrival ("" if served)
 
 
 @dataclass
@@ -327,6 +328,18 @@ class Server:
         self.swaps_in += 1
         return True, True
 
+    def refusal(self, k):
+        """Why a request for world k can never be served ("" if it can): its
+        world's memory is above the whole budget, or its step's borrowed
+        memory above a lane pool."""
+        need = self.be.world_bytes(k)
+        if need > self.budget:
+            return f"world {k} needs {need} bytes resident, above the {self.budget}-byte budget"
+        cap = self.be.lane_capacity(0)
+        if cap is not None and self.be.step_bytes(k) > cap:
+            return f"a step of world {k} borrows {self.be.step_bytes(k)} bytes, above a lane pool's {cap}"
+        return ""
+
     # -- the loop
     def _complete(self, lane_id, now, finished):
         lane = self.lanes[lane_id]
@@ -385,7 +398,15 @@ class Server:
         while len(finished) < total:
             now = self.clock() - t0
             while i < total and reqs[i].t_arrival <= now:
-                pending.append(reqs[i])
+                # a request that no eviction can make room for is refused at
+                # once, not left pending for ever
+                why = self.refusal(reqs[i].world)
+                if why:
+                    reqs[i].refused = why
+                    reqs[i].t_start = reqs[i].t_done = now
+                    finished.append(reqs[i])
+                else:
+                    pending.append(reqs[i])
                 i += 1
             for lane_id, lane in enumerate(self.lanes):
                 if lane.busy and self.be.done(lane.token):
@@ -413,7 +434,12 @@ def poisson_arrivals(rate, n_requests, n_worlds, seed):
 def latency_summary(finished, cells_of):
     """p50 / p99 / mean latency (ms, arrival to completion seen by the
     host), throughput (Mcells/s and steps/s over the run) and the requests
-    that waited for their world to be swapped in."""
+    that waited for their world to be swapped in, over the requests served
+    (refused ones are counted apart)."""
+    refused = sum(1 for r in finished if r.refused)
+    finished = [r for r in finished if not r.refused]
+    if not finished:
+        return {"requests": 0, "refused_requests": refused}
     lat = np.array([r.t_done - r.t_arrival for r in finished]) * 1e3
     span = max(r.t_done for r in finished) - min(r.t_arrival for r in finished)
     cells = sum(cells_of(r.world) for r in finished)
@@ -427,6 +453,8 @@ def latency_summary(finished, cells_of):
         "steps_per_s": round(len(finished) / max(span, 1e-9), 1),
         "swapped_requests": int((~hit).sum()),
     }
+    if refused:
+        out["refused_requests"] = refused
     if hit.any() and not hit.all():
         out["p50_ms_resident"] = round(float(np.percentile(lat[hit], 50)), 3)
         out["p99_ms_resident"] = round(float(np.percentile(lat[hit], 99)), 3)
@@ -436,21 +464,29 @@ def latency_summary(finished, cells_of):
 def latency_part(finished, cells_of):
     """One rank's raw results, for merge_parts on rank 0: latencies (ms),
     swapped flags, cells stepped, and the run's first arrival and last
-    completion (the ranks' clocks start together at a barrier)."""
+    completion (the ranks' clocks start together at a barrier); refused
+    requests only counted."""
+    refused = sum(1 for r in finished if r.refused)
+    finished = [r for r in finished if not r.refused]
     return {
+        "refused": refused,
         "lat_ms": [(r.t_done - r.t_arrival) * 1e3 for r in finished],
         "swapped": [bool(r.swapped) for r in finished],
         "cells": int(sum(cells_of(r.world) for r in finished)),
-        "t0": min(r.t_arrival for r in finished),
-        "t1": max(r.t_done for r in finished),
+        "t0": min((r.t_arrival for r in finished), default=0.0),
+        "t1": max((r.t_done for r in finished), default=0.0),
     }
 
 
 def merge_parts(parts):
     """latency_summary over several ranks' latency_part results: the
     percentiles of all requests, the throughput summed over the ranks."""
-    lat = np.concatenate([np.asarray(p["lat_ms"]) for p in parts])
+    lat = np.concatenate([np.asarray(p["lat_ms"], dtype=np.float64) for p in parts])
     hit = ~np.concatenate([np.asarray(p["swapped"], dtype=bool) for p in parts])
+    refused = sum(p.get("refused", 0) for p in parts)
+    if lat.size == 0:
+        return {"requests": 0, "refused_requests": refused}
+    parts = [p for p in parts if p["lat_ms"]]
     out = {
         "requests": int(lat.size),
         "p50_ms": round(float(np.percentile(lat, 50)), 3),
@@ -460,6 +496,8 @@ def merge_parts(parts):
         "steps_per_s": round(sum(len(p["lat_ms"]) / max(p["t1"] - p["t0"], 1e-9) for p in parts), 1),
         "swapped_requests": int((~hit).sum()),
     }
+    if refused:
+        out["refused_requests"] = refused
     if hit.any() and not hit.all():
         out["p50_ms_resident"] = round(float(np.percentile(lat[hit], 50)), 3)
         out["p99_ms_resident"] = round(float(np.percentile(lat[hit], 99)), 3)
