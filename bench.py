@@ -183,21 +183,21 @@ def level_stats(worlds, coarse_cells=4096):
 
 
 # DRAM bytes (read + written) per algorithmic byte of a kernel, from one
-# ncu capture each (the summaries under profiles/ give the commands), keyed
-# by (slot, mixed form). roofline.traffic is this ratio times a launch's
+# ncu capture each (dram__bytes_read.sum + dram__bytes_write.sum), keyed by
+# (slot, mixed form). roofline.traffic is this ratio times a launch's
 # algorithmic bytes: the capture's traffic scaled to the launch by the units
 # it processes.
 TRAFFIC_PER_ALG_BYTE = {
     # k_fDown on level 1 of the disks 1024x1024 world: 22.8 MB read, 256 B
     # written; 262,144 cells x 180 B
-    ("F_RESTRICT", False): ((22.8e6 + 256) / (262144 * 180), "k_fDown level 1 (512x512), k_fDown_level1_disks1024.md"),
+    ("F_RESTRICT", False): ((22.8e6 + 256) / (262144 * 180), "k_fDown, level 1 (512x512) of the disks 1024x1024 world"),
     # k_fDown on levels 1-3 of one iteration of a 64-world batch, mixed form:
     # 117.1 MB read and written; 222.2 MB algorithmic
-    ("F_RESTRICT", True): (117145856 / 222247528, "k_fDown levels 1-3 of a 64-world batch, k_fDown_batch64_mixed.md"),
+    ("F_RESTRICT", True): (117145856 / 222247528, "k_fDown, levels 1-3 of one iteration of a 64-world mixed batch"),
     # k_fRelax on the disks 1024x1024 world: 25.0 MB read, 0 written; 24.5 MB
     # algorithmic (the fine level is FP32 in both forms)
-    ("F_RELAX", False): (25.0e6 / 24.5e6, "k_fRelax, k_fRelax_disks1024.md"),
-    ("F_RELAX", True): (25.0e6 / 24.5e6, "k_fRelax, k_fRelax_disks1024.md"),
+    ("F_RELAX", False): (25.0e6 / 24.5e6, "k_fRelax, the disks 1024x1024 world"),
+    ("F_RELAX", True): (25.0e6 / 24.5e6, "k_fRelax, the disks 1024x1024 world"),
 }
 
 
@@ -206,7 +206,8 @@ def traffic_of(name, alg, mixed=False):
     t = TRAFFIC_PER_ALG_BYTE.get((name, bool(mixed)))
     if t is None or not alg:
         return None, None
-    return int(round(t[0] * alg)), "ncu capture " + t[1] + ", scaled to this launch's algorithmic bytes"
+    return int(round(t[0] * alg)), ("ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of " + t[1] +
+                                    ", scaled to this launch's algorithmic bytes")
 
 
 def algorithmic_bytes(name, s):
@@ -397,9 +398,7 @@ def run_batched(args, rank, world_size, local_rank, dist, torch, emit=True):
         tb.close()
         for name, v in shapes.items():
             b.set_launch(name, v)
-        tuned = {"shapes": shapes, "steps": tune.steps_needed(),
-                 "trials_ms_per_iteration": {k: [[v, None if c is None else round(c, 4)] for v, c in r]
-                                             for k, r in trials.items()}}
+        tuned = tuned_summary(shapes, trials)
     for name, v in args.launch.items():
         b.set_launch(name, v)
     for _ in range(args.warmup):
@@ -557,9 +556,7 @@ def run_served(args, rank, world_size, local_rank, dist, torch, emit=True):
     if not args.no_tune:
         from worldinagrain_b200 import tune
         shapes, trials = be.autotune(list(srv.resident))
-        tuned = {"shapes": shapes, "steps": tune.steps_needed(),
-                 "trials_ms_per_iteration": {k: [[v, None if c is None else round(c, 4)] for v, c in r]
-                                             for k, r in trials.items()}}
+        tuned = tuned_summary(shapes, trials)
     srv.run(serve.poisson_arrivals(1000.0, 200, len(worlds), seed=99))
     rates = [float(r) for r in args.rates.split(",")]
     points = []
@@ -611,6 +608,16 @@ def run_served(args, rank, world_size, local_rank, dist, torch, emit=True):
         if emit:
             print(json.dumps(line), flush=True)
         return line
+
+
+def tuned_summary(shapes, trials):
+    """The autotuner's picks for the bench line; its per-candidate trial
+    costs go to stderr as one JSON line (they would fill the line)."""
+    print(json.dumps({"autotune_trials_ms_per_iteration": {
+        k: [[v, None if c is None else round(c, 4)] for v, c in r] for k, r in trials.items()}}),
+        file=sys.stderr, flush=True)
+    from worldinagrain_b200 import tune
+    return {"shapes": shapes, "steps": tune.steps_needed()}
 
 
 def launch_overrides(items):
@@ -731,9 +738,7 @@ def main():
         tg.close()
         for name, v in shapes.items():
             g.set_launch(name, v)
-        tuned = {"shapes": shapes, "steps": tune.steps_needed(),
-                 "trials_ms_per_iteration": {k: [[v, None if c is None else round(c, 4)] for v, c in r]
-                                             for k, r in trials.items()}}
+        tuned = tuned_summary(shapes, trials)
     for name, v in args.launch.items():
         g.set_launch(name, v)
     for _ in range(args.warmup):
@@ -814,6 +819,35 @@ def main():
     peak, peak_kind = peaks()
     achieved = alg / per_launch_s / 1e9 if per_launch_s > 0 else 0.0
 
+    # ---- the plain drop-in (a kernel a reference pass) over the same steps
+    # of the same trajectory, device-timed as above: the one-world baseline
+    # the batched and served forms are compared with
+    plain = None
+    if world_size == 1 and not args.no_forms and args.form != "plain":
+        def pflags(k):
+            return flags_of(k) | abi.STEP_PLAIN
+        g.upload(saved)
+        g.step(params(world, step_saved + 1, args.seed), max_cycles=MAX_CYCLES, flags=pflags(step_saved + 1),
+               tolerance=TOL)  # captures the plain form's graph
+        g.stats()
+        g.upload(saved)
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            p0.record(stream)
+        for k in range(step_saved + 1, step_saved + 1 + args.steps):
+            g.step(params(world, k, args.seed), max_cycles=MAX_CYCLES, flags=pflags(k), tolerance=TOL)
+        with torch.cuda.stream(stream):
+            p1.record(stream)
+        torch.cuda.synchronize()
+        pst = g.stats()
+        pms = p0.elapsed_time(p1)
+        plain = {"value": round(cells * args.steps / (pms / 1e3) / 1e6, 3), "unit": "Mcells/s",
+                 "ms_per_step": round(pms / args.steps, 4), "steps": args.steps,
+                 "form": "plain drop-in: a kernel a reference pass, in one CUDA graph a step",
+                 "same_steps_as": "value (the same saved state and trajectory)",
+                 "rel_residual_last": pst.rel_residual, "gpu_launches": pst.launches * args.steps}
+
     cpu = None
     if rank == 0 and not args.no_cpu:
         v, nsteps, dt = cpu_baseline(world, args, args.cpu_budget)
@@ -842,7 +876,8 @@ def main():
         }
     g.close()
     if rank == 0 and world_size == 1 and not args.no_forms:
-        line["forms"] = run_forms(args, rank, world_size, local_rank, dist, torch)
+        line["forms"] = {"plain": plain} if plain else {}
+        line["forms"].update(run_forms(args, rank, world_size, local_rank, dist, torch))
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
