@@ -118,7 +118,7 @@ struct Lane {
     wig::SchedCtl ctl{};
     wig::BatchShape S{};           // the shape the lane's step records with (step_shape)
     std::map<uint64_t, Graph> graphs;
-    cudaStream_t cap = nullptr, cap2 = nullptr;
+    cudaStream_t cap = nullptr, cap2 = nullptr, cap3 = nullptr;
     cudaStream_t last_stream = nullptr;
     uint32_t last_launches = 0, last_body = 0;
 };
@@ -566,6 +566,7 @@ int make_batch(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, u
         if (cudaMallocHost(&ln.h_rsub, sizeof(Report) * n) != cudaSuccess) return bail(WIG_E_OOM, "cudaMallocHost lane reports");
         if (cudaStreamCreateWithFlags(&ln.cap, cudaStreamNonBlocking) != cudaSuccess) return bail(WIG_E_CUDA, "stream");
         if (cudaStreamCreateWithFlags(&ln.cap2, cudaStreamNonBlocking) != cudaSuccess) return bail(WIG_E_CUDA, "stream");
+        if (cudaStreamCreateWithFlags(&ln.cap3, cudaStreamNonBlocking) != cudaSuccess) return bail(WIG_E_CUDA, "stream");
         wig::Batch& Bt = ln.Bt;
         Bt.worlds = b->d_worlds;
         Bt.items = ln.d_items;
@@ -575,6 +576,8 @@ int make_batch(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, u
         Bt.single = n == 1 ? 1u : 0u;
         Bt.max_cycles = 1;
         Bt.cond = 0;
+        Bt.cond_check = 0;
+        Bt.cond_drift = 0;
         Bt.loop = ln.d_loop;
         wig::SchedCtl& c = ln.ctl;
         c.nsub = reinterpret_cast<const uint32_t*>(ln.d_up);
@@ -609,6 +612,7 @@ void destroy_batch(wig_batch* b) {
         if (ln.h_rsub) cudaFreeHost(ln.h_rsub);
         if (ln.cap) cudaStreamDestroy(ln.cap);
         if (ln.cap2) cudaStreamDestroy(ln.cap2);
+        if (ln.cap3) cudaStreamDestroy(ln.cap3);
         if (ln.d_table) cudaFree(ln.d_table);
         if (ln.d_pool) cudaFree(ln.d_pool);
     }
@@ -823,6 +827,8 @@ int record_step_fast(wig_batch* b, Lane& ln, uint32_t max_cycles, uint32_t flags
     wig::Marker mk{&Rec::mark, &R};
     ln.Bt.max_cycles = max_cycles;
     ln.Bt.cond = 0;
+    ln.Bt.cond_check = 0;
+    ln.Bt.cond_drift = 0;
     ln.Bt.mixed = (flags & WIG_STEP_MIXED) ? 1u : 0u;
     const wig::World* one = b->K == 1 ? &b->hw[0] : nullptr;
     if (b->pooled) {
@@ -861,9 +867,11 @@ int record_step_fast(wig_batch* b, Lane& ln, uint32_t max_cycles, uint32_t flags
         CUDA_TRY(cudaStreamBeginCaptureToGraph(ln.cap2, bodyGraph, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
         wig::Batch Bc = ln.Bt;
         Bc.cond = (unsigned long long)handle;
-        *body = wig::fast_cycle(Bc, ln.S, one, ln.cap2, nullptr);
+        wig::NestCapture nest{ln.cap3, cudaSuccess};
+        *body = wig::fast_cycle(Bc, ln.S, one, ln.cap2, nullptr, &nest);
         cudaGraph_t captured = nullptr;
         CUDA_TRY(cudaStreamEndCapture(ln.cap2, &captured));
+        CUDA_TRY(nest.err);
     } else {
         uint32_t* cont = reinterpret_cast<uint32_t*>(ln.h_rsub);  // a word of pinned scratch
         for (uint32_t c = 0; c < max_cycles; c++) {

@@ -429,6 +429,8 @@ struct Batch {
     uint32_t mixed;           // the mixed-precision form (coarse operators in binary16, true-residual checks)
     uint32_t max_cycles;
     unsigned long long cond;  // cudaGraphConditionalHandle of the iteration loop (0: none)
+    unsigned long long cond_check;  // the mixed form's IF node of the true-residual check (0: none)
+    unsigned long long cond_drift;  // the IF node of its fix (0: none)
     uint32_t* loop;           // the loop's verdict: 1 when a world iterates again
 
     __device__ __forceinline__ uint32_t n(uint32_t list) const { return count[list]; }

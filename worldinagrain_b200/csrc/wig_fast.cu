@@ -188,10 +188,14 @@ __device__ void sumBlocks256x2(const W& w, const T* part, T* s0, T* s1, T* out0,
     __syncthreads();
 }
 
-// Whether this CTA counted the last of `total` tiles (its writers fenced
-// their partials before the barrier): a threadfence reduction's test.
+// Whether this CTA counted the last of `total` tiles: a threadfence
+// reduction's test.  The partials of the counted tiles were written by the
+// tiles' first threads (threadIdx.x % 64 == 0), each with no fence of its
+// own: those threads fence here, once for all the tiles of the run, before
+// the count.
 __device__ bool lastOf4(uint32_t* counter, uint32_t inc, uint32_t total) {
     __shared__ int last;
+    if ((threadIdx.x & 63u) == 0u) __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
         uint32_t old = atomicAdd(counter, inc);
@@ -337,7 +341,6 @@ __global__ void __launch_bounds__(256) k_fSetup(Batch Bt, const __grid_constant_
             double v = tree64x4(s64, b2);
             if (valid && (threadIdx.x & 63u) == 0u) {
                 D.norm64[2u * w.blockIndex(w.activeBlock(wid))] = v;
-                __threadfence();
             }
             pend_ += min(4u, na - g * 4u);
             if (flushTiles(Bt, g_it, e_it, it, pend_, &D.st->fdone[0], na)) {
@@ -1270,7 +1273,6 @@ __global__ void __launch_bounds__(256) k_fRhoBeta(Batch Bt, const __grid_constan
                 F.part64[2u * b] = dx;
                 F.part64[2u * b + 1u] = dy;
             }
-            __threadfence();
         }
         pend_ += min(4u, na - g * 4u);
         if (flushTiles(Bt, g_it, e_it, it, pend_, &D.st->fdone[1], na)) {
@@ -1375,7 +1377,6 @@ __global__ void __launch_bounds__(256) k_fApplyAlpha(Batch Bt, const __grid_cons
                 F.part64[2u * b] = dx;
                 F.part64[2u * b + 1u] = 0.0;
             }
-            __threadfence();
         }
         pend_ += min(4u, na - g * 4u);
         if (flushTiles(Bt, g_it, e_it, it, pend_, &D.st->fdone[2], na)) {
@@ -1461,7 +1462,6 @@ __global__ void __launch_bounds__(256) k_fUpdate(Batch Bt, const __grid_constant
         if (valid && (threadIdx.x & 63u) == 0u) {
             if (tol) D.norm64[2u * w.blockIndex(w.activeBlock(wid))] = t2;
             atomicMax(&runMost, max(m, umost[par][threadIdx.x >> 6]));
-            __threadfence();
         }
         par ^= 1u;
         pend_ += min(4u, na - g * 4u);
@@ -1494,6 +1494,7 @@ __global__ void __launch_bounds__(256) k_fUpdate(Batch Bt, const __grid_constant
                 D.st->cycle = next;
                 D.st->cont = cont;
                 D.st->check = check ? 1u : 0u;
+                if (check && Bt.cond_check) cudaGraphSetConditional(Bt.cond_check, 1u);
                 if (cont) {
                     *Bt.loop = 1u;
                     if (Bt.cond) cudaGraphSetConditional(Bt.cond, 1u);
@@ -1561,7 +1562,6 @@ __global__ void __launch_bounds__(256) k_fTrueCheck(Batch Bt, const __grid_const
             const uint32_t b = w.blockIndex(w.activeBlock(wid));
             D.norm64[2u * b] = t2;
             D.norm64[2u * b + 1u] = u2;
-            __threadfence();
         }
         pend_ += min(4u, na - g * 4u);
         if (flushTiles(Bt, g_it, e_it, it, pend_, &D.st->fdone[4], na)) {
@@ -1574,6 +1574,7 @@ __global__ void __launch_bounds__(256) k_fTrueCheck(Batch Bt, const __grid_const
                 D.st->check = 0u;
                 if (rel > 2.0 * D.st->rel + 4.0 * flo) {
                     D.st->drift = 1u;
+                    if (Bt.cond_drift) cudaGraphSetConditional(Bt.cond_drift, 1u);
                     const uint32_t cont = D.st->cycle < Bt.max_cycles ? 1u : 0u;
                     D.st->cont = cont;
                     if (cont) {
@@ -1617,6 +1618,8 @@ __global__ void k_fLoopStart(Batch Bt) {
     if (blockIdx.x == 0) {
         *Bt.loop = 0u;
         if (Bt.cond) cudaGraphSetConditional(Bt.cond, 0u);
+        if (Bt.cond_check) cudaGraphSetConditional(Bt.cond_check, 0u);
+        if (Bt.cond_drift) cudaGraphSetConditional(Bt.cond_drift, 0u);
     }
     FOR_ITEMS(Bt, L_ONE, it) {
         ITEM_WORLD(Bt, it, D, w, unused_);
@@ -2120,8 +2123,52 @@ void fast_setup(const Batch& Bt, const BatchShape& S, const World* one, cudaStre
     if (m) m->fn(m->ctx, WIG_SLOT_F_SETUP, 1);
 }
 
+// An IF node at the capture point of stream `outer`, on condition `h`; its
+// body captured from `body` (launches on the given stream).
+template <class Body>
+cudaError_t captureIf(cudaStream_t outer, cudaGraphConditionalHandle h, cudaStream_t inner, Body body) {
+    cudaStreamCaptureStatus cs;
+    cudaGraph_t g = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t nd = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(outer, &cs, nullptr, &g, &deps, &nd);
+    if (e != cudaSuccess) return e;
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeIf;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node;
+    e = cudaGraphAddNode(&node, g, deps, nd, &cp);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamUpdateCaptureDependencies(outer, &node, 1, cudaStreamSetCaptureDependencies);
+    if (e != cudaSuccess) return e;
+    e = cudaStreamBeginCaptureToGraph(inner, cp.conditional.phGraph_out[0], nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) return e;
+    body(inner);
+    cudaGraph_t captured = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(inner, &captured);
+    e = cudaGetLastError();
+    return e != cudaSuccess ? e : e2;
+}
+
 template <class T>
-uint32_t fast_cycle_t(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m) {
+uint32_t fast_cycle_t(const Batch& Bt0, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m,
+                      NestCapture* nest) {
+    // the mixed form's check and fix: under IF nodes when captured, with
+    // their conditions' handles in the kernels' Batch from the iteration's
+    // start (k_fLoopStart clears them, k_fUpdate and k_fTrueCheck set them)
+    Batch Bt = Bt0;
+    cudaGraphConditionalHandle hc = 0, hd = 0;
+    if (Bt.mixed && nest && nest->err == cudaSuccess) {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t g = nullptr;
+        nest->err = cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, nullptr, nullptr);
+        if (nest->err == cudaSuccess) nest->err = cudaGraphConditionalHandleCreate(&hc, g, 0, cudaGraphCondAssignDefault);
+        if (nest->err == cudaSuccess) nest->err = cudaGraphConditionalHandleCreate(&hd, g, 0, cudaGraphCondAssignDefault);
+        Bt.cond_check = (unsigned long long)hc;
+        Bt.cond_drift = (unsigned long long)hd;
+    }
     const unsigned G = list_grid(S, L_ACT, 32), G4 = list_grid(S, L_ACT4, S.cg_per_sm);
     const unsigned GR = std::max(std::min((S.max_items[L_RELAX] + 3u) / 4u, 148u * S.relax_per_sm), 1u);
     uint32_t launches = 0;
@@ -2167,7 +2214,14 @@ uint32_t fast_cycle_t(const Batch& Bt, const BatchShape& S, const World* one, cu
     mark(WIG_SLOT_F_UPDATE, 0);
     LAUNCH(k_fUpdate, G4, 256, 0);
     mark(WIG_SLOT_F_UPDATE, 1);
-    if (Bt.mixed) {
+    if (Bt.mixed && hc && hd) {
+        // captured: launched only on the iterations that check (not counted
+        // among every iteration's launches)
+        if (nest->err == cudaSuccess)
+            nest->err = captureIf(s, hc, nest->s, [&](cudaStream_t s) { LAUNCH(k_fTrueCheck, G4, 256, 0); });
+        if (nest->err == cudaSuccess)
+            nest->err = captureIf(s, hd, nest->s, [&](cudaStream_t s) { LAUNCH(k_fTrueFix, G, 64, 0); });
+    } else if (Bt.mixed) {
         mark(WIG_SLOT_F_UPDATE, 0);
         LAUNCH(k_fTrueCheck, G4, 256, 0);
         mark(WIG_SLOT_F_UPDATE, 1);
@@ -2178,8 +2232,9 @@ uint32_t fast_cycle_t(const Batch& Bt, const BatchShape& S, const World* one, cu
     return launches;
 }
 
-uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m) {
-    return Bt.mixed ? fast_cycle_t<__half>(Bt, S, one, s, m) : fast_cycle_t<float>(Bt, S, one, s, m);
+uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m,
+                    NestCapture* nest) {
+    return Bt.mixed ? fast_cycle_t<__half>(Bt, S, one, s, m, nest) : fast_cycle_t<float>(Bt, S, one, s, m, nest);
 }
 
 void fast_finish(const Batch& Bt, const BatchShape& S, const World* one, bool two_p, cudaStream_t s, const Marker* m) {

@@ -35,11 +35,24 @@ struct Marker {
     void* ctx;
 };
 
+// While an iteration is captured into the loop's body graph: a stream for
+// the bodies of the conditional nodes inside it (the mixed form's
+// true-residual check and fix run in IF nodes, so the iterations that need
+// neither launch neither), and the first CUDA error met.
+struct NestCapture {
+    cudaStream_t s;
+    cudaError_t err;
+};
+
 // Launchers over a batch (stream-ordered; all capturable).  `one`: the
 // batch's only world (host copy), passed to the kernels as a parameter; null
-// for a batch of several.  fast_cycle returns its launches.
+// for a batch of several.  fast_cycle returns the launches every iteration
+// makes; `nest`: the capture's stream for conditional bodies (null when
+// launched eagerly: the check and the fix are then launched every
+// iteration and return at once when not needed).
 void fast_setup(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m);
-uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m);
+uint32_t fast_cycle(const Batch& Bt, const BatchShape& S, const World* one, cudaStream_t s, const Marker* m,
+                    NestCapture* nest = nullptr);
 // cgFinish; `two_p`: the fast form's p is in P or P2 by the iterations' parity.
 void fast_finish(const Batch& Bt, const BatchShape& S, const World* one, bool two_p, cudaStream_t s, const Marker* m);
 // Level 0's arrays of one world zeroed (after its buffers are written by the host).
