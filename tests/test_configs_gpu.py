@@ -190,7 +190,7 @@ def test_column_2048_forms_match_oracle_and_fp64_solve():
         print(f"\ncolumn 2048x2048 {form}: pressure {e[0]:.3e}, velocity {e[1]:.3e} relative L2 against the FP64 "
               f"solve ({e[4]:.3e} of the velocity projected); {sg.cycles} iterations, residual {sg.rel_residual:.2e}")
     assert out["plain"][0] == out["fast"][0]
-    assert out["fast"][0] < 1e-3 and out["fast"][4] < 1e-4
+    assert out["fast"][0] < 1e-3 and out["fast"][4] < 1e-3
     assert out["mixed"][0] <= 2 * out["fast"][0] + 1e-5
     assert out["mixed"][4] <= 2 * out["fast"][4] + 1e-5
 
