@@ -665,6 +665,11 @@ struct Rec {
     void run(int pass, uint32_t level = 0, uint32_t cycle = 0) {
         timed(pass, [&] { wig::launch_pass(ln.Bt, ln.S, b->hw[0].D, pass, level, cycle, s); });
     }
+    // cgStart + cgJoin as the fast forms run them (profiled as the two passes)
+    void labels() {
+        timed(WIG_PASS_CG_START, [&] { wig::launch_labels(ln.Bt, ln.S, s, 0); });
+        timed(WIG_PASS_CG_JOIN, [&] { wig::launch_labels(ln.Bt, ln.S, s, 1); });
+    }
     void norm(int which, uint32_t cycle) {
         timed(WIG_SLOT_NORM, [&] { wig::launch_norm(b->hw[0].D, which, cycle, s); });
     }
@@ -821,8 +826,7 @@ int record_step_fast(wig_batch* b, Lane& ln, uint32_t max_cycles, uint32_t flags
         return WIG_OK;
     }
     record_pre(R, (flags & WIG_STEP_VISCOUS) != 0u);
-    R.run(WIG_PASS_CG_START);
-    R.run(WIG_PASS_CG_JOIN);
+    R.labels();
     R.run(WIG_PASS_CG_ANCHOR);
     wig::Marker mk{&Rec::mark, &R};
     ln.Bt.max_cycles = max_cycles;

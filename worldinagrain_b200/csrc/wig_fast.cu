@@ -477,17 +477,35 @@ __global__ void __launch_bounds__(128) k_fRelax(Batch Bt, const __grid_constant_
         }
         // the tile and its rim: the snapshot's values for liquid cells, the
         // potentials elsewhere
-        for (int k = (int)lane; k < RIM * RIM; k += 32) {
-            I2 c{ox - 1 + k % RIM, oy - 1 + k / RIM};
-            float px = 0.0f, py = 0.0f;
-            if (w.inWorld(c)) {
-                uint32_t i = w.cellIndex(c);
-                const float r = L0.rho[i], ax = F.rimx[i], ay = F.rimy[i], qx = L0.px[i], qy = L0.py[i];
-                px = r > 0.0f ? ax : qx;
-                py = r > 0.0f ? ay : qy;
+        // (the four rounds of the lane's loads issued together)
+        {
+            constexpr int NR = (RIM * RIM + 31) / 32;
+            float rr[NR], ax[NR], ay[NR], qx[NR], qy[NR];
+            bool inw[NR];
+#pragma unroll
+            for (int u = 0; u < NR; u++) {
+                const int k = (int)lane + 32 * u;
+                const I2 c{ox - 1 + k % RIM, oy - 1 + k / RIM};
+                inw[u] = k < RIM * RIM && w.inWorld(c);
+                const uint32_t i = inw[u] ? w.cellIndex(c) : 0u;
+                rr[u] = L0.rho[i];
+                ax[u] = F.rimx[i];
+                ay[u] = F.rimy[i];
+                qx[u] = L0.px[i];
+                qy[u] = L0.py[i];
             }
-            sx_[k] = px;
-            sy_[k] = py;
+#pragma unroll
+            for (int u = 0; u < NR; u++) {
+                const int k = (int)lane + 32 * u;
+                if (k >= RIM * RIM) continue;
+                float px = 0.0f, py = 0.0f;
+                if (inw[u]) {
+                    px = rr[u] > 0.0f ? ax[u] : qx[u];
+                    py = rr[u] > 0.0f ? ay[u] : qy[u];
+                }
+                sx_[k] = px;
+                sy_[k] = py;
+            }
         }
         __syncwarp();
         for (int sw = 0; sw < 2 * SWEEPS; sw++) {
@@ -555,10 +573,12 @@ __device__ __forceinline__ float diagAt(const LRef<__half>& V, uint32_t k) {
 }
 
 // residualAt (fluid.wgsl:2306-2315) of cell k on a level held in arrays with
-// stored coefficients (level 0's pinned roots held at PIN).
+// stored coefficients (level 0's pinned roots held at PIN).  The division by
+// h2, a power of two, is the multiplication by its exact inverse: the same
+// real number rounded once either way, so the same bits.
 template <class T>
 __device__ __forceinline__ V2 residualStored(const LRef<T>& V, const float* pin, uint32_t k, int x, int y, int lw, int lh,
-                                             float h2) {
+                                             float inv_h2) {
     float sx = 0.0f, sy = 0.0f;
     const float b[4] = {ld(V.b0 + k), ld(V.b1 + k), ld(V.b2 + k), ld(V.b3 + k)};
 #pragma unroll
@@ -569,12 +589,17 @@ __device__ __forceinline__ V2 residualStored(const LRef<T>& V, const float* pin,
     }
     const float dg = diagAt(V, k);
     const float pinx = pin ? pin[k] : 0.0f;
-    return V2{ld(V.rx + k) - (sx - (dg + pinx) * ld(V.px + k)) / h2, ld(V.ry + k) - (sy - (dg + 0.0f) * ld(V.py + k)) / h2};
+    return V2{ld(V.rx + k) - (sx - (dg + pinx) * ld(V.px + k)) * inv_h2,
+              ld(V.ry + k) - (sy - (dg + 0.0f) * ld(V.py + k)) * inv_h2};
 }
 
 // restrictLevel's values of level-l cell (cx, cy) from level l - 1, stored
 // as TU (fluid.wgsl:2342-2377): the density and, with `res`, the restricted
-// residuals; all 0 in a block not worked on.
+// residuals; all 0 in a block not worked on.  The four finer cells' words
+// are all loaded before any is used (a cell past the level's edge reads
+// the level's first cell and is then left out; a cell not liquid has its
+// residual worked and dropped), so their loads are in flight together; the
+// sums then take the liquid cells in the reference's order.
 template <class TU>
 __device__ __forceinline__ void restrictedAt(const Dev& D, const FastW& F, const W& w, uint32_t l, int cx, int cy,
                                              bool res, float& rho_o, float& rx_o, float& ry_o) {
@@ -590,23 +615,33 @@ __device__ __forceinline__ void restrictedAt(const Dev& D, const FastW& F, const
     }
     const LRef<TU> U = lref<TU>(F, l - 1u);
     const int uw = (int)D.level_w[l - 1], uh = (int)D.level_h[l - 1];
-    const float h2 = (float)(1u << (2u * (l - 1u)));
+    const float inv_h2 = 1.0f / (float)(1u << (2u * (l - 1u)));
     const float* pin = l == 1u ? F.pin : nullptr;
+    float rq[4];
+    V2 eq[4];
+    bool inq[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int kx = 2 * cx + (q & 1), ky = 2 * cy + (q >> 1);
+        inq[q] = kx < uw && ky < uh;  // rhoAt outside the level: -1
+        const int sx = inq[q] ? kx : 0, sy = inq[q] ? ky : 0;
+        const uint32_t k = (uint32_t)sy * (uint32_t)uw + (uint32_t)sx;
+        rq[q] = ld(U.rho + k);
+        eq[q] = res ? residualStored(U, pin, k, sx, sy, uw, uh, inv_h2) : V2{0.0f, 0.0f};
+    }
     float fluid = 0.0f, sum = 0.0f, rx = 0.0f, ry = 0.0f;
     bool air = false;
+#pragma unroll
     for (int q = 0; q < 4; q++) {
-        int kx = 2 * cx + (q & 1), ky = 2 * cy + (q >> 1);
-        if (kx >= uw || ky >= uh) continue;  // rhoAt outside the level: -1
-        uint32_t k = (uint32_t)ky * (uint32_t)uw + (uint32_t)kx;
-        float rho = ld(U.rho + k);
+        if (!inq[q]) continue;
+        const float rho = rq[q];
         if (rho == 0.0f) air = true;
         else if (rho > 0.0f) {
             fluid = fluid + 1.0f;
             sum = sum + rho;
             if (res) {
-                V2 r = residualStored(U, pin, k, kx, ky, uw, uh, h2);
-                rx = rx + r.x;
-                ry = ry + r.y;
+                rx = rx + eq[q].x;
+                ry = ry + eq[q].y;
             }
         }
     }
@@ -682,25 +717,37 @@ __device__ void smoothCell(const Dev& D, const FastW& F, uint32_t l, int color, 
     st(V.py + j, mixf(ey, (sy - h2 * ld(V.ry + j)) / dg, 1.0f));
 }
 
-// prolonged (fluid.wgsl:2478-2497) from level l + 1's arrays.
+// prolonged (fluid.wgsl:2478-2497) from level l + 1's arrays.  The four
+// coarse cells' words are loaded before any is used (a cell past the
+// level's edge reads a clamped one and is left out), then weighed in the
+// reference's order.
 template <class T>
 __device__ __forceinline__ V2 prolongedFrom(const T* rho, const float* px, const float* py, int lw, int lh, int cx, int cy) {
     const int kx = cx / 2, ky = cy / 2;
     const int sx = (cx & 1) == 1 ? 1 : -1, sy = (cy & 1) == 1 ? 1 : -1;
     const int ox[4] = {0, sx, 0, sx}, oy[4] = {0, 0, sy, sy};
     const float wt[4] = {9.0f, 3.0f, 3.0f, 1.0f};
+    float rq[4], xq[4], yq[4];
+    bool inq[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int ax_ = kx + ox[q], ay_ = ky + oy[q];
+        inq[q] = !(ax_ < 0 || ay_ < 0 || ax_ >= lw || ay_ >= lh);
+        const uint32_t k = inq[q] ? (uint32_t)ay_ * (uint32_t)lw + (uint32_t)ax_ : 0u;
+        rq[q] = ld(rho + k);
+        xq[q] = ld(px + k);
+        yq[q] = ld(py + k);
+    }
     float ax = 0.0f, ay = 0.0f, weight = 0.0f;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-        int ax_ = kx + ox[q], ay_ = ky + oy[q];
-        if (ax_ < 0 || ay_ < 0 || ax_ >= lw || ay_ >= lh) continue;
-        uint32_t k = (uint32_t)ay_ * (uint32_t)lw + (uint32_t)ax_;
-        float r = ld(rho + k);
+        if (!inq[q]) continue;
+        const float r = rq[q];
         if (r < 0.0f) continue;
         weight = weight + wt[q];
         if (r > 0.0f) {
-            ax = ax + wt[q] * ld(px + k);
-            ay = ay + wt[q] * ld(py + k);
+            ax = ax + wt[q] * xq[q];
+            ay = ay + wt[q] * yq[q];
         }
     }
     const float ww = fmaxf(weight, 1e-6f);
@@ -893,22 +940,35 @@ __global__ void __launch_bounds__(256, ONE ? 3 : 2) k_fUp(Batch Bt, const __grid
             const int ix = k % LR - 2, iy = k / LR - 2, cx = x0 + ix, cy = y0 + iy;
             float rho = -1.0f, px = 0.0f, py = 0.0f;
             if (cx >= 0 && cy >= 0 && cx < lw && cy < lh) {
+                // every word the cell may need loaded before any is used (a
+                // cell not liquid drops them)
                 const uint32_t j = (uint32_t)(cy * lw + cx);
+                const bool ring1 = ix >= -1 && iy >= -1 && ix <= LT && iy <= LT;
                 rho = ld(V.rho + j);
                 px = ld(V.px + j);
                 py = ld(V.py + j);
+                const V2 e = prolongedFrom(urho, Lu.ux, Lu.uy, uw, uh, cx, cy);
+                float rx = 0.0f, ry = 0.0f, b0 = 0.0f, b1 = 0.0f, b2 = 0.0f, b3 = 0.0f, dg = 0.0f;
+                if (ring1) {
+                    rx = ld(V.rx + j);
+                    ry = ld(V.ry + j);
+                    b0 = ld(V.b0 + j);
+                    b1 = ld(V.b1 + j);
+                    b2 = ld(V.b2 + j);
+                    b3 = ld(V.b3 + j);
+                    dg = diagAt(V, j);
+                }
                 if (rho > 0.0f) {
-                    const V2 e = prolongedFrom(urho, Lu.ux, Lu.uy, uw, uh, cx, cy);
                     px = px + e.x;
                     py = py + e.y;
-                    if (ix >= -1 && iy >= -1 && ix <= LT && iy <= LT) {
-                        t.rx[k] = ld(V.rx + j);
-                        t.ry[k] = ld(V.ry + j);
-                        t.b[0][k] = ld(V.b0 + j);
-                        t.b[1][k] = ld(V.b1 + j);
-                        t.b[2][k] = ld(V.b2 + j);
-                        t.b[3][k] = ld(V.b3 + j);
-                        t.dg[k] = diagAt(V, j);
+                    if (ring1) {
+                        t.rx[k] = rx;
+                        t.ry[k] = ry;
+                        t.b[0][k] = b0;
+                        t.b[1][k] = b1;
+                        t.b[2][k] = b2;
+                        t.b[3][k] = b3;
+                        t.dg[k] = dg;
                     }
                 }
             }
@@ -941,12 +1001,20 @@ constexpr uint32_t SLV_ARRAYS = 9;
 struct SLv {
     float *px, *py, *rx, *ry, *rho, *b0, *b1, *b2, *b3;
     int w, h;
+    uint32_t mw;  // ceil(2^32 / w) (0 for w = 1): j / w = umulhi(j, mw) for the level's indices
 };
 __device__ __forceinline__ SLv slv(float* sm, const uint32_t* off, const Dev& D, uint32_t l) {
     const int n = (int)(D.level_w[l] * D.level_h[l]);
     float* p = sm + off[l];
+    const uint32_t w = D.level_w[l];
     return SLv{p,         p + n,     p + 2 * n, p + 3 * n, p + 4 * n, p + 5 * n,
-               p + 6 * n, p + 7 * n, p + 8 * n, (int)D.level_w[l], (int)D.level_h[l]};
+               p + 6 * n, p + 7 * n, p + 8 * n, (int)w, (int)D.level_h[l], w == 1u ? 0u : 0xffffffffu / w + 1u};
+}
+// The row of index j < 2 n of level V: j / w by a multiply-high with
+// ceil(2^32 / w), exact while j w < 2^32 (the coarse kernel's levels hold at
+// most 4096 cells), in place of an integer division's instruction sequence.
+__device__ __forceinline__ int slvRow(const SLv& V, int j) {
+    return V.w == 1 ? j : (int)__umulhi((uint32_t)j, V.mw);
 }
 
 // The face coefficients of level V's cells (smoothAt's stencil,
@@ -955,7 +1023,7 @@ __device__ __forceinline__ SLv slv(float* sm, const uint32_t* off, const Dev& D,
 __device__ void slv_coefficients(const SLv& V, int tid, int nt) {
     const int n = V.w * V.h;
     for (int j = tid; j < n; j += nt) {
-        const int cx = j % V.w, cy = j / V.w;
+        const int cy = slvRow(V, j), cx = j - cy * V.w;
         const float rho = V.rho[j];
         float b[4] = {0.0f, 0.0f, 0.0f, 0.0f};
         if (rho > 0.0f) {
@@ -994,7 +1062,7 @@ __device__ void slv_sweep(const SLv& V, uint32_t l, int color, float omega, int 
     const int n = V.w * V.h, pairs = (n + 1) / 2;
     const float h2 = (float)(1u << (2u * l));
     for (int k = tid; k < pairs; k += nt) {
-        int j = 2 * k, cx = j % V.w, cy = j / V.w;
+        int j = 2 * k, cy = slvRow(V, j), cx = j - cy * V.w;
         if (((cx + cy) & 1) != color) {
             j++;
             if (++cx == V.w) {
@@ -1062,7 +1130,7 @@ __device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t 
             // quotient's bits
             const float inv_h2u = 1.0f / (float)(1u << (2u * (l - 1u)));
             for (int j = tid; j < n; j += nt) {
-                const int cx = j % V.w, cy = j / V.w;
+                const int cy = slvRow(V, j), cx = j - cy * V.w;
                 if (span <= BLOCK) {
                     I2 b{cx * span / BLOCK, cy * span / BLOCK};
                     if (w.inBlocks(b) && (D.blocks[w.stateSlot(w.blockIndex(b))] & ACTIVE) == 0u) {
@@ -1153,7 +1221,8 @@ __device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t 
         const int n = V.w * V.h;
         for (int j = tid; j < n; j += nt) {
             if (V.rho[j] <= 0.0f) continue;
-            V2 e = prolongedFrom(U.rho, U.px, U.py, U.w, U.h, j % V.w, j / V.w);
+            const int cy = slvRow(V, j);
+            V2 e = prolongedFrom(U.rho, U.px, U.py, U.w, U.h, j - cy * V.w, cy);
             V.px[j] = V.px[j] + e.x;
             V.py[j] = V.py[j] + e.y;
         }
@@ -1200,9 +1269,12 @@ __global__ void k_fProlongFine(Batch Bt, const __grid_constant__ WorldSrc<ONE> s
         I2 c = lidCell(w, wid);
         if (!w.inWorld(c)) continue;
         uint32_t i = w.cellIndex(c);
-        if (L0.rho[i] > 0.0f) {
-            V2 e = prolongedFrom(urho, F.L[1].ux, F.L[1].uy, (int)D.level_w[1], (int)D.level_h[1], c.x, c.y);
-            float px = L0.px[i] + e.x, py = L0.py[i] + e.y;
+        // the cell's words and the prolongation's loaded together, then used
+        // for a liquid cell only
+        const float rho = L0.rho[i], px0 = L0.px[i], py0 = L0.py[i];
+        const V2 e = prolongedFrom(urho, F.L[1].ux, F.L[1].uy, (int)D.level_w[1], (int)D.level_h[1], c.x, c.y);
+        if (rho > 0.0f) {
+            float px = px0 + e.x, py = py0 + e.y;
             L0.px[i] = px;
             L0.py[i] = py;
             F.rimx[i] = px;

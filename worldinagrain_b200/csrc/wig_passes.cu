@@ -1033,6 +1033,70 @@ __global__ void k_cgJoin(Batch Bt) {
         }
     }
 }
+// cgStart with the block's own part of cgJoin's labelling, for the fast
+// forms' steps (the per-pass dispatch and the plain form keep k_cgStart and
+// k_cgJoin): each liquid cell's region link goes straight to the smallest
+// index of the liquid cells its block joins it to (min-label propagation
+// over the block's 4-neighbour liquid edges in shared memory, at most 63
+// rounds), every other cell its own root.  The union-find's links always
+// point to lower indices and its roots are the smallest indices of their
+// regions, so after k_cgJoinAcross has joined the edges between blocks the
+// regions, their roots and every ufFind are those of cgJoin's; only the
+// intermediate links, a lock-free union-find's timing in the reference too,
+// differ (cgFinish clears them all).
+__global__ void k_cgStartLocal(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
+    __shared__ uint32_t lab[64];
+    FOR_ITEMS(Bt, L_ACT, it) {
+        ITEM_WORLD_C(Bt, it, D, w, wid);
+        const I2 c = lidCell(w, wid);
+        const bool in = w.inWorld(c);
+        const uint32_t i = in ? w.cellIndex(c) : 0u;
+        bool fluid = false;
+        if (in) {
+            const float4 g = w.gridAt(c);
+            reinterpret_cast<float4*>(D.cg)[i] = make_float4(g.x, 0.0f, 0.0f, 0.0f);
+            fluid = g.z > 0.0f;
+        }
+        const int t = (int)threadIdx.x, lx = t & 7, ly = t >> 3;
+        lab[t] = fluid ? i : 0xffffffffu;
+        __syncthreads();
+        for (int round = 0; round < 64; round++) {
+            uint32_t m = lab[t];
+            if (fluid) {
+                if (lx > 0) m = min(m, lab[t - 1]);
+                if (lx < 7) m = min(m, lab[t + 1]);
+                if (ly > 0) m = min(m, lab[t - 8]);
+                if (ly < 7) m = min(m, lab[t + 8]);
+            }
+            __syncthreads();
+            const bool changed = m < lab[t];
+            lab[t] = m;
+            if (!__syncthreads_or(changed)) break;
+        }
+        if (in) *w.gwp(i, G_REGION) = fluid ? lab[t] : i;
+        __syncthreads();
+    }
+}
+// cgJoin's edges between blocks (to the right and below, from the block's
+// last column and row), after k_cgStartLocal has linked each block's own.
+__global__ void k_cgJoinAcross(Batch Bt) {
+    __shared__ WorldCopy wc_;
+    worldCopyInit(wc_);
+    FOR_ITEMS(Bt, L_ACT, it) {
+        ITEM_WORLD_C(Bt, it, D, w, wid);
+        const int lx = (int)(threadIdx.x & 7u), ly = (int)(threadIdx.x >> 3);
+        if (lx != 7 && ly != 7) continue;
+        I2 c = lidCell(w, wid);
+        if (!w.inWorld(c) || w.gridAt(c).z <= 0.0f) continue;
+        for (int d = 0; d < 2; d++) {
+            if ((d == 0 && lx != 7) || (d == 1 && ly != 7)) continue;
+            I2 n = d == 0 ? I2{c.x + 1, c.y} : I2{c.x, c.y + 1};
+            if (rhoAt(w, 0, n) > 0.0f) ufJoin(w, w.cellIndex(c), w.cellIndex(n));
+        }
+    }
+}
 // cgAnchor (fluid.wgsl:2692-2705)
 __global__ void k_cgAnchor(Batch Bt) {
     __shared__ WorldCopy wc_;
@@ -2291,6 +2355,12 @@ int launch_pass(const Batch& Bt, const BatchShape& S, const Dev& D0, int pass, u
     default: return WIG_E_ARG;
     }
     return WIG_OK;
+}
+
+void launch_labels(const Batch& Bt, const BatchShape& S, cudaStream_t s, int part) {
+    const unsigned A = list_grid(S, L_ACT, 32);
+    if (part == 0) k_cgStartLocal<<<A, 64, 0, s>>>(Bt);
+    else k_cgJoinAcross<<<A, 64, 0, s>>>(Bt);
 }
 
 int launch_norm(const Dev& D, int which, uint32_t cycle, cudaStream_t s) {

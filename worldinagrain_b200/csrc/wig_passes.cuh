@@ -25,6 +25,10 @@ unsigned list_grid(const BatchShape& S, uint32_t list, unsigned per_sm);
 // world 0, whose descriptor D0 is.
 int launch_pass(const Batch& Bt, const BatchShape& S, const Dev& D0, int pass, uint32_t level, uint32_t cycle,
                 cudaStream_t s);
+// The fast forms' cgStart + cgJoin: part 0 cgStart with each block's own
+// labelling (k_cgStartLocal), part 1 the joins between blocks; the same
+// regions and roots as the two passes.
+void launch_labels(const Batch& Bt, const BatchShape& S, cudaStream_t s, int part);
 // The plain form's tolerance norms on world 0: which 0 = ||b||^2 after
 // cgResidual, 1 = ||r||/||b|| after cgUpdate.
 int launch_norm(const Dev& D, int which, uint32_t cycle, cudaStream_t s);
