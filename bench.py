@@ -131,26 +131,28 @@ def params(world, step, seed):
 # layout makes it read and write once (per active cell, fluid cell, face or
 # particle), counted from the world after the step.  Active cells are the
 # active blocks' 64 each.  The fast form's level kernels, per launch on a
-# level of n cells.  A level cell holds four FP32 words (px, py, rx, ry),
-# five operator words of e bytes (rho, b0..b3: 4, or 2 in the mixed form's
-# binary16 levels) and, stored only in FP32, its diagonal (d = 4, mixed 0);
-# level 0 is all FP32 (40 B a cell).  Down (restriction, then both colours
-# of smoothing on chip): the four finer cells read, the coarse cell's px, py,
-# rx, ry and rho written, 180 n in FP32; up (prolongation, then both
-# colours): the level's words read, its potentials written, the coarser
-# level's density and potentials read a quarter each, 51 n in FP32; the
-# one-CTA coarse kernel on its first level 24 + e a cell, 28 n in FP32.
+# level of n cells.  A level cell holds four potential words of p bytes
+# (px, py, rx, ry: FP32, 4; the mixed form's bf16, 2), five operator words
+# of e bytes (rho, b0..b3: 4, or 2 in the mixed form's binary16) and,
+# stored only in FP32, its diagonal (d = 4, mixed 0); level 0 is all FP32
+# (40 B a cell).  Down (restriction, then both colours of smoothing on
+# chip): the four finer cells read, the coarse cell's px, py, rx, ry and
+# rho written, 180 n in FP32; up (prolongation, then both colours): the
+# level's words read, its way-up potentials written, the coarser level's
+# density and way-up potentials read a quarter each, 51 n in FP32; the
+# one-CTA coarse kernel on its first level: its potentials, right-hand
+# sides and density read, its way-up potentials written, 28 n in FP32.
 # Averaged over the launches of an iteration (s["levels"]: level_stats'
 # cells of each level's launches; s["mixed"]: the mixed form).
 def level_bytes(name, s):
     L = s.get("levels")
     if not L:
         return None
-    e, d = (2, 0) if s.get("mixed") else (4, 4)
-    cell = 16 + 5 * e + d
-    down = [(4 * (40 if i == 0 else cell) + 16 + e) * r for i, (r, _, _) in enumerate(L) if r]
-    up = [(cell + 8 + (e + 8) / 4) * m for _, m, _ in L if m]
-    co = [(24 + e) * c for _, _, c in L if c]
+    p, e, d = (2, 2, 0) if s.get("mixed") else (4, 4, 4)
+    cell = 4 * p + 5 * e + d
+    down = [(4 * (40 if i == 0 else cell) + 4 * p + e) * r for i, (r, _, _) in enumerate(L) if r]
+    up = [(cell + 2 * p + (e + 2 * p) / 4) * m for _, m, _ in L if m]
+    co = [(6 * p + e) * c for _, _, c in L if c]
     if name == "F_RESTRICT" and down:
         return int(sum(down)) // len(down)
     if name == "F_PROLONG" and up:
@@ -634,8 +636,9 @@ def launch_overrides(items):
 
 def dtype_of(form):
     """The arithmetic the form computes in: FP32 grids and vectors, FP64
-    dots; the mixed form stores its coarse operator in binary16."""
-    return "f16+f32+f64" if form == "mixed" else "f32+f64"
+    dots; the mixed form stores its coarse operator in binary16 and its
+    levels' potentials in bf16."""
+    return "bf16+f16+f32+f64" if form == "mixed" else "f32+f64"
 
 
 def config_of(world, args):

@@ -180,9 +180,11 @@ typedef struct wig_fluid_buffers {
 #define WIG_STEP_SYNC_STATS 64u       /* copy the stats to the host at the end of the step */
 #define WIG_STEP_PLAIN 128u           /* the solve as one kernel per reference pass (else the fast form) */
 #define WIG_STEP_PERSISTENT 256u      /* the fast form's iterations as one persistent cooperative kernel (else kernels in a graph WHILE loop) */
-#define WIG_STEP_MIXED 512u           /* mixed precision (fast form, with TOLERANCE and F64_DOTS): each coarse level's
-                                         operator (density, stencil coefficients) stored in binary16 and worked in FP32,
-                                         potentials, right-hand sides and CG vectors FP32, dots and norms FP64; every 8th
+#define WIG_STEP_MIXED 512u           /* mixed precision (fast form, with TOLERANCE and F64_DOTS): the multigrid levels
+                                         stored in 16 bits and worked in FP32 (each coarse level's density and stencil
+                                         coefficients in binary16, its potentials, right-hand sides and way-up potentials
+                                         in bf16; the fine smoother's coefficients in binary16 copies), the fine level's
+                                         potentials and the CG vectors and operator FP32, dots and norms FP64; every 8th
                                          iteration and before the solve stops, the true residual b + A x worked in FP64
                                          and put in for the recursive one when it has drifted above it and above the
                                          FP32 rounding floor of A x; not bit-exact with the other forms */

@@ -23,12 +23,12 @@ def test_level_byte_models():
     assert bench.level_bytes("F_COARSE", s) == 28 * 16384
     assert bench.level_bytes("F_RELAX", s) is None
     assert bench.level_bytes("F_RESTRICT", {}) is None
-    # the mixed form: the operator words of levels 1 down in binary16, no
-    # stored diagonal there; level 0 all FP32
+    # the mixed form: the operator words of levels 1 down in binary16 and
+    # their potentials in bf16, no stored diagonal there; level 0 all FP32
     m = dict(s, mixed=True)
-    assert bench.level_bytes("F_RESTRICT", m) == (178 * 262144 + 122 * 65536 + 122 * 16384) // 3
-    assert bench.level_bytes("F_PROLONG", m) == int(36.5 * 262144 + 36.5 * 65536) // 2
-    assert bench.level_bytes("F_COARSE", m) == 26 * 16384
+    assert bench.level_bytes("F_RESTRICT", m) == (170 * 262144 + 82 * 65536 + 82 * 16384) // 3
+    assert bench.level_bytes("F_PROLONG", m) == int(23.5 * 262144 + 23.5 * 65536) // 2
+    assert bench.level_bytes("F_COARSE", m) == 14 * 16384
 
 
 def test_level_stats_follow_the_coarse_kernels_first_level():
@@ -74,7 +74,7 @@ def test_launch_overrides():
 
 
 def test_form_arithmetic():
-    assert bench.dtype_of("mixed") == "f16+f32+f64"
+    assert bench.dtype_of("mixed") == "bf16+f16+f32+f64"
     assert bench.dtype_of("fast") == bench.dtype_of("plain") == "f32+f64"
     assert bench.FLAGS & abi.STEP_TOLERANCE and bench.FLAGS & abi.STEP_F64_DOTS
 

@@ -259,7 +259,7 @@ void dev_shape(wig::Dev& D, const wig_world_layout& L) {
 // Bytes of a world's fast scratch and FP64 partials.
 size_t scratch_bytes(const wig::Dev& D) {
     const size_t C = D.C;
-    size_t bytes = align256(C) + 18u * align256(C * 4u);
+    size_t bytes = align256(C) + 18u * align256(C * 4u) + align256(4u * C * 2u);  // + level 0's binary16 copies
     for (uint32_t l = 1; l <= D.levels; l++) {
         bytes += 12u * align256((size_t)D.level_w[l] * D.level_h[l] * 4u);
         bytes += align256(5u * (size_t)D.level_w[l] * D.level_h[l] * 2u);  // the binary16 operator
@@ -285,7 +285,7 @@ void scratch_take(wig::World& Wd, char* p, uint32_t coarse_cells) {
         V.ux = l == 0 ? nullptr : fl(n);
         V.uy = l == 0 ? nullptr : fl(n);
     }
-    F.H[0] = wig::LvlH{nullptr, 0u, 0u};
+    F.H[0] = wig::LvlH{reinterpret_cast<__half*>(take(4u * C * 2u)), (uint32_t)C, 0u};
     for (uint32_t l = 1; l <= D.levels; l++) {
         const size_t n = (size_t)D.level_w[l] * D.level_h[l];
         F.H[l] = wig::LvlH{reinterpret_cast<__half*>(take(5u * n * 2u)), (uint32_t)n, 0u};

@@ -362,9 +362,12 @@ struct Lvl {
     float *ux, *uy;  // levels >= 1: the potentials after the V-cycle's way up (the way down's stay in px, py)
 };
 
-// A coarse level's operator in binary16 (the mixed-precision form): its
-// density and four stencil coefficients (rho, b0, b1, b2, b3), n values each,
-// from base; its potentials and right-hand sides stay in Lvl's f32 arrays.
+// A level's operator in binary16 (the mixed-precision form), n values an
+// array from base: on a coarse level its density and four stencil
+// coefficients (rho, b0, b1, b2, b3), whose potentials and right-hand sides
+// are stored as bf16 in the first half of Lvl's f32 arrays; on level 0 the
+// four coefficients alone, the copies the smoother reads (the CG's A p reads
+// Lvl's f32 ones).
 struct LvlH {
     __half* base;
     uint32_t n;
@@ -374,7 +377,7 @@ struct LvlH {
 // A world's fast-form scratch.
 struct FastW {
     Lvl L[WIG_MG_LEVELS + 1];  // level 0 (the cells) .. levels
-    LvlH H[WIG_MG_LEVELS + 1]; // levels 1 .. levels: the operator in binary16 (the mixed form)
+    LvlH H[WIG_MG_LEVELS + 1]; // the operator in binary16 (the mixed form): level 0's coefficients, levels 1 ..
     float* pin;                // level 0: PIN at a pinned root, else 0
     uint8_t* fmask;            // level 0: bit d set when neighbour d is liquid
     float *rimx, *rimy;        // level 0: the relaxation's rim snapshot

@@ -22,6 +22,8 @@
 
 #include <algorithm>
 
+#include <cuda_bf16.h>
+
 #include "wig_fast.cuh"
 
 namespace wig {
@@ -332,6 +334,15 @@ __global__ void __launch_bounds__(256) k_fSetup(Batch Bt, const __grid_constant_
             }
             L0.b0[i] = bb[0]; L0.b1[i] = bb[1]; L0.b2[i] = bb[2]; L0.b3[i] = bb[3];
             L0.diag[i] = bb[0] + bb[1] + bb[2] + bb[3];
+            if (Bt.mixed) {
+                // the smoother's copies of the coefficients (the mixed form)
+                __half* h = F.H[0].base;
+                const uint32_t n = F.H[0].n;
+                h[i] = __float2half_rn(bb[0]);
+                h[n + i] = __float2half_rn(bb[1]);
+                h[2u * n + i] = __float2half_rn(bb[2]);
+                h[3u * n + i] = __float2half_rn(bb[3]);
+            }
             F.pin[i] = pinv;
             F.fmask[i] = mask;
             F.R[i] = R;
@@ -394,6 +405,97 @@ __global__ void k_fZero(FastW F, uint32_t C) {
     }
 }
 
+// ================================================================ level storage
+
+// A level's arrays as stored, the operator (density, stencil coefficients,
+// diagonal) in T: f32 (the plain precision) or binary16 (the mixed form);
+// values are read into and worked in f32.  The potentials, right-hand sides and way-up potentials of a level whose
+// operator is stored as T: f32 with an f32 operator; bf16 (8 bits of
+// mantissa, f32's range, so no scaling as a residual shrinks) with the mixed
+// form's binary16 operator.  Both are stored in the level's f32 arrays (a
+// bf16 array fills the first half of one).
+template <class T>
+struct PotOf {
+    using type = float;
+};
+template <>
+struct PotOf<__half> {
+    using type = __nv_bfloat16;
+};
+// A level's arrays: potentials and right-hand sides of P, densities of R,
+// the stencil's coefficients (and, when B is f32, their stored sum) of B.
+template <class P, class R, class B>
+struct LRefX {
+    P *px, *py, *rx, *ry;
+    R* rho;
+    B *b0, *b1, *b2, *b3, *diag;
+};
+// Levels 1 down as the form stores them (operator T).
+template <class T>
+using LRef = LRefX<typename PotOf<T>::type, T, T>;
+// Level 0 as the form's smoother reads it: all f32, or (the mixed form) its
+// coefficients from their binary16 copies, the potentials, right-hand sides
+// and densities f32 (the CG's A p keeps the f32 coefficients).
+template <class T>
+using L0Ref = LRefX<float, float, T>;
+__device__ __forceinline__ float ld(const float* p) { return *p; }
+__device__ __forceinline__ float ld(const __half* p) { return __half2float(*p); }
+__device__ __forceinline__ float ld(const __nv_bfloat16* p) { return __bfloat162float(*p); }
+__device__ __forceinline__ void st(float* p, float v) { *p = v; }
+__device__ __forceinline__ void st(__half* p, float v) { *p = __float2half_rn(v); }
+__device__ __forceinline__ void st(__nv_bfloat16* p, float v) { *p = __float2bfloat16_rn(v); }
+
+template <class T>
+__device__ __forceinline__ LRef<T> lref(const FastW& F, uint32_t l);
+template <>
+__device__ __forceinline__ LRef<float> lref<float>(const FastW& F, uint32_t l) {
+    const Lvl& V = F.L[l];
+    return LRef<float>{V.px, V.py, V.rx, V.ry, V.rho, V.b0, V.b1, V.b2, V.b3, V.diag};
+}
+template <>
+__device__ __forceinline__ LRef<__half> lref<__half>(const FastW& F, uint32_t l) {
+    const Lvl& V = F.L[l];
+    __half* b = F.H[l].base;
+    const uint32_t n = F.H[l].n;
+    using P = __nv_bfloat16;
+    return LRef<__half>{reinterpret_cast<P*>(V.px), reinterpret_cast<P*>(V.py), reinterpret_cast<P*>(V.rx),
+                        reinterpret_cast<P*>(V.ry), b, b + n, b + 2u * n, b + 3u * n, b + 4u * n, nullptr};
+}
+template <class T>
+__device__ __forceinline__ L0Ref<T> lref0(const FastW& F);
+template <>
+__device__ __forceinline__ L0Ref<float> lref0<float>(const FastW& F) {
+    return lref<float>(F, 0u);
+}
+template <>
+__device__ __forceinline__ L0Ref<__half> lref0<__half>(const FastW& F) {
+    const Lvl& V = F.L[0];
+    __half* b = F.H[0].base;
+    const uint32_t n = F.H[0].n;
+    return L0Ref<__half>{V.px, V.py, V.rx, V.ry, V.rho, b, b + n, b + 2u * n, b + 3u * n, nullptr};
+}
+// Level l's way-up potentials (l >= 1) as a level of operator T stores them.
+template <class T>
+__device__ __forceinline__ typename PotOf<T>::type* upx(const FastW& F, uint32_t l) {
+    return reinterpret_cast<typename PotOf<T>::type*>(F.L[l].ux);
+}
+template <class T>
+__device__ __forceinline__ typename PotOf<T>::type* upy(const FastW& F, uint32_t l) {
+    return reinterpret_cast<typename PotOf<T>::type*>(F.L[l].uy);
+}
+
+// A cell's diagonal: stored in f32 (the sum of its four coefficients, in
+// that order); in binary16 not stored but the sum of the rounded
+// coefficients, so the rounded operator keeps its diagonal equal to the sum
+// of its off-diagonals (a separately rounded diagonal could fall below it
+// and make a region with no free surface indefinite).
+template <class P, class R>
+__device__ __forceinline__ float diagAt(const LRefX<P, R, float>& V, uint32_t k) { return V.diag[k]; }
+template <class P, class R>
+__device__ __forceinline__ float diagAt(const LRefX<P, R, __half>& V, uint32_t k) {
+    return ((ld(V.b0 + k) + ld(V.b1 + k)) + ld(V.b2 + k)) + ld(V.b3 + k);
+}
+
 // ================================================================ relaxation
 
 __device__ I2 tileBlockF(const W& w, uint32_t wid, int shift) {
@@ -412,7 +514,7 @@ __device__ I2 tileBlockF(const W& w, uint32_t wid, int shift) {
 // independent, so each keeps the reference's arithmetic and order.
 // `second`: the iteration's relaxation after the V-cycle, on the other
 // tiling from the first (each world's first tiling is its step's).
-template <bool ONE>
+template <bool ONE, class T>
 __global__ void __launch_bounds__(128) k_fRelax(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, int second) {
     __shared__ float tpx[4][RIM * RIM], tpy[4][RIM * RIM];
     const uint32_t warp = threadIdx.x >> 5, lane = threadIdx.x & 31u;
@@ -455,14 +557,15 @@ __global__ void __launch_bounds__(128) k_fRelax(Batch Bt, const __grid_constant_
             bool fluid = false;
             if (w.inWorld(me)) {
                 id = w.cellIndex(me);
+                const L0Ref<T> S0 = lref0<T>(F);
                 fluid = L0.rho[id] > 0.0f;
                 r_x = L0.rx[id];
                 r_y = L0.ry[id];
-                b0 = L0.b0[id];
-                b1 = L0.b1[id];
-                b2 = L0.b2[id];
-                b3 = L0.b3[id];
-                dg = L0.diag[id];
+                b0 = ld(S0.b0 + id);
+                b1 = ld(S0.b1 + id);
+                b2 = ld(S0.b2 + id);
+                b3 = ld(S0.b3 + id);
+                dg = diagAt(S0, id);
                 pv = F.pin[id];
             }
             if (!fluid) {
@@ -533,51 +636,12 @@ __global__ void __launch_bounds__(128) k_fRelax(Batch Bt, const __grid_constant_
 
 // ================================================================ the levels
 
-// A level's arrays as stored: the potentials and right-hand sides in f32,
-// the operator (density, stencil coefficients, diagonal) in T: f32 (the
-// plain precision) or binary16 (the coarse levels of the mixed form); values
-// are read into and worked in f32.
-template <class T>
-struct LRef {
-    float *px, *py, *rx, *ry;
-    T *rho, *b0, *b1, *b2, *b3, *diag;
-};
-__device__ __forceinline__ float ld(const float* p) { return *p; }
-__device__ __forceinline__ float ld(const __half* p) { return __half2float(*p); }
-__device__ __forceinline__ void st(float* p, float v) { *p = v; }
-__device__ __forceinline__ void st(__half* p, float v) { *p = __float2half_rn(v); }
-
-template <class T>
-__device__ __forceinline__ LRef<T> lref(const FastW& F, uint32_t l);
-template <>
-__device__ __forceinline__ LRef<float> lref<float>(const FastW& F, uint32_t l) {
-    const Lvl& V = F.L[l];
-    return LRef<float>{V.px, V.py, V.rx, V.ry, V.rho, V.b0, V.b1, V.b2, V.b3, V.diag};
-}
-template <>
-__device__ __forceinline__ LRef<__half> lref<__half>(const FastW& F, uint32_t l) {
-    const Lvl& V = F.L[l];
-    __half* b = F.H[l].base;
-    const uint32_t n = F.H[l].n;
-    return LRef<__half>{V.px, V.py, V.rx, V.ry, b, b + n, b + 2u * n, b + 3u * n, b + 4u * n, nullptr};
-}
-
-// A cell's diagonal: stored in f32 (the sum of its four coefficients, in
-// that order); in binary16 not stored but the sum of the rounded
-// coefficients, so the rounded operator keeps its diagonal equal to the sum
-// of its off-diagonals (a separately rounded diagonal could fall below it
-// and make a region with no free surface indefinite).
-__device__ __forceinline__ float diagAt(const LRef<float>& V, uint32_t k) { return V.diag[k]; }
-__device__ __forceinline__ float diagAt(const LRef<__half>& V, uint32_t k) {
-    return ((ld(V.b0 + k) + ld(V.b1 + k)) + ld(V.b2 + k)) + ld(V.b3 + k);
-}
-
 // residualAt (fluid.wgsl:2306-2315) of cell k on a level held in arrays with
 // stored coefficients (level 0's pinned roots held at PIN).  The division by
 // h2, a power of two, is the multiplication by its exact inverse: the same
 // real number rounded once either way, so the same bits.
-template <class T>
-__device__ __forceinline__ V2 residualStored(const LRef<T>& V, const float* pin, uint32_t k, int x, int y, int lw, int lh,
+template <class VT>
+__device__ __forceinline__ V2 residualStored(const VT& V, const float* pin, uint32_t k, int x, int y, int lw, int lh,
                                              float inv_h2) {
     float sx = 0.0f, sy = 0.0f;
     const float b[4] = {ld(V.b0 + k), ld(V.b1 + k), ld(V.b2 + k), ld(V.b3 + k)};
@@ -600,9 +664,9 @@ __device__ __forceinline__ V2 residualStored(const LRef<T>& V, const float* pin,
 // the level's first cell and is then left out; a cell not liquid has its
 // residual worked and dropped), so their loads are in flight together; the
 // sums then take the liquid cells in the reference's order.
-template <class TU>
-__device__ __forceinline__ void restrictedAt(const Dev& D, const FastW& F, const W& w, uint32_t l, int cx, int cy,
-                                             bool res, float& rho_o, float& rx_o, float& ry_o) {
+template <class VT>
+__device__ __forceinline__ void restrictedFrom(const Dev& D, const FastW& F, const W& w, uint32_t l, const VT& U, int cx,
+                                               int cy, bool res, float& rho_o, float& rx_o, float& ry_o) {
     const int span = 1 << l;
     if (span <= BLOCK) {
         I2 b{cx * span / BLOCK, cy * span / BLOCK};
@@ -613,7 +677,6 @@ __device__ __forceinline__ void restrictedAt(const Dev& D, const FastW& F, const
             return;
         }
     }
-    const LRef<TU> U = lref<TU>(F, l - 1u);
     const int uw = (int)D.level_w[l - 1], uh = (int)D.level_h[l - 1];
     const float inv_h2 = 1.0f / (float)(1u << (2u * (l - 1u)));
     const float* pin = l == 1u ? F.pin : nullptr;
@@ -651,14 +714,23 @@ __device__ __forceinline__ void restrictedAt(const Dev& D, const FastW& F, const
     ry_o = rho > 0.0f ? ry * 0.25f : 0.0f;
 }
 
+// restrictedFrom for level l of a form whose levels store operator T: from
+// level 0 as its smoother reads it, or from level l - 1.
+template <class T>
+__device__ __forceinline__ void restrictedAt(const Dev& D, const FastW& F, const W& w, uint32_t l, int cx, int cy,
+                                             bool res, float& rho_o, float& rx_o, float& ry_o) {
+    if (l == 1u) restrictedFrom(D, F, w, l, lref0<T>(F), cx, cy, res, rho_o, rx_o, ry_o);
+    else restrictedFrom(D, F, w, l, lref<T>(F, l - 1u), cx, cy, res, rho_o, rx_o, ry_o);
+}
+
 // One coarse cell of restrictLevel, level l (stored as TV) from l - 1
 // (stored as TU): the cell's values, its potentials zeroed.
-template <class TU, class TV>
+template <class T>
 __device__ void restrictCellT(const Dev& D, const FastW& F, const W& w, uint32_t l, uint32_t j) {
     const int lw = (int)D.level_w[l];
-    const LRef<TV> V = lref<TV>(F, l);
+    const LRef<T> V = lref<T>(F, l);
     float rho, rx, ry;
-    restrictedAt<TU>(D, F, w, l, (int)(j % (uint32_t)lw), (int)(j / (uint32_t)lw), true, rho, rx, ry);
+    restrictedAt<T>(D, F, w, l, (int)(j % (uint32_t)lw), (int)(j / (uint32_t)lw), true, rho, rx, ry);
     st(V.px + j, 0.0f);
     st(V.py + j, 0.0f);
     st(V.rx + j, rx);
@@ -668,8 +740,7 @@ __device__ void restrictCellT(const Dev& D, const FastW& F, const W& w, uint32_t
 // Level l from l - 1 with the levels stored as T (level 0 always f32).
 template <class T = float>
 __device__ __forceinline__ void restrictCell(const Dev& D, const FastW& F, const W& w, uint32_t l, uint32_t j) {
-    if (l == 1u) restrictCellT<float, T>(D, F, w, l, j);
-    else restrictCellT<T, T>(D, F, w, l, j);
+    restrictCellT<T>(D, F, w, l, j);
 }
 
 // One cell of smoothAt (fluid.wgsl:2318-2334) on level l >= 1, the
@@ -721,8 +792,8 @@ __device__ void smoothCell(const Dev& D, const FastW& F, uint32_t l, int color, 
 // coarse cells' words are loaded before any is used (a cell past the
 // level's edge reads a clamped one and is left out), then weighed in the
 // reference's order.
-template <class T>
-__device__ __forceinline__ V2 prolongedFrom(const T* rho, const float* px, const float* py, int lw, int lh, int cx, int cy) {
+template <class T, class P>
+__device__ __forceinline__ V2 prolongedFrom(const T* rho, const P* px, const P* py, int lw, int lh, int cx, int cy) {
     const int kx = cx / 2, ky = cy / 2;
     const int sx = (cx & 1) == 1 ? 1 : -1, sy = (cy & 1) == 1 ? 1 : -1;
     const int ox[4] = {0, sx, 0, sx}, oy[4] = {0, 0, sy, sy};
@@ -860,8 +931,7 @@ __global__ void __launch_bounds__(256, ONE ? 3 : 2) k_fDown(Batch Bt, const __gr
             float rho = -1.0f, rx = 0.0f, ry = 0.0f;
             if (cx >= 0 && cy >= 0 && cx < lw && cy < lh) {
                 const bool res = ix >= -1 && iy >= -1 && ix <= LT && iy <= LT;
-                if (l == 1u) restrictedAt<float>(D, F, w, l, cx, cy, res, rho, rx, ry);
-                else restrictedAt<T>(D, F, w, l, cx, cy, res, rho, rx, ry);
+                restrictedAt<T>(D, F, w, l, cx, cy, res, rho, rx, ry);
             }
             t.rho[k] = asStored(rho, T());
             t.rx[k] = rx;
@@ -934,7 +1004,8 @@ __global__ void __launch_bounds__(256, ONE ? 3 : 2) k_fUp(Batch Bt, const __grid
         const int x0 = (int)(tile % (uint32_t)tw) * LT, y0 = (int)(tile / (uint32_t)tw) * LT;
         const LRef<T> V = lref<T>(F, l);
         const T* urho = lref<T>(F, l + 1u).rho;
-        const Lvl& Lu = F.L[l + 1u];
+        const auto* lux = upx<T>(F, l + 1u);
+        const auto* luy = upy<T>(F, l + 1u);
         const int uw = (int)D.level_w[l + 1], uh = (int)D.level_h[l + 1];
         for (int k = (int)threadIdx.x; k < LRR; k += (int)blockDim.x) {
             const int ix = k % LR - 2, iy = k / LR - 2, cx = x0 + ix, cy = y0 + iy;
@@ -947,7 +1018,7 @@ __global__ void __launch_bounds__(256, ONE ? 3 : 2) k_fUp(Batch Bt, const __grid
                 rho = ld(V.rho + j);
                 px = ld(V.px + j);
                 py = ld(V.py + j);
-                const V2 e = prolongedFrom(urho, Lu.ux, Lu.uy, uw, uh, cx, cy);
+                const V2 e = prolongedFrom(urho, lux, luy, uw, uh, cx, cy);
                 float rx = 0.0f, ry = 0.0f, b0 = 0.0f, b1 = 0.0f, b2 = 0.0f, b3 = 0.0f, dg = 0.0f;
                 if (ring1) {
                     rx = ld(V.rx + j);
@@ -983,8 +1054,8 @@ __global__ void __launch_bounds__(256, ONE ? 3 : 2) k_fUp(Batch Bt, const __grid
             const int i = lsi(ix, iy);
             if (cx < lw && cy < lh && t.rho[i] > 0.0f) {
                 const uint32_t j = (uint32_t)(cy * lw + cx);
-                F.L[l].ux[j] = t.px[i];
-                F.L[l].uy[j] = t.py[i];
+                st(upx<T>(F, l) + j, t.px[i]);
+                st(upy<T>(F, l) + j, t.py[i]);
             }
         }
         __syncthreads();
@@ -1231,12 +1302,12 @@ __device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t 
     }
     {
         const SLv V = slv(sm, off, D, lc);
-        float* ox = up ? F.L[lc].ux : F.L[lc].px;
-        float* oy = up ? F.L[lc].uy : F.L[lc].py;
+        auto* ox = up ? upx<T>(F, lc) : lref<T>(F, lc).px;
+        auto* oy = up ? upy<T>(F, lc) : lref<T>(F, lc).py;
         const int n = V.w * V.h;
         for (int j = tid; j < n; j += nt) {
-            ox[j] = V.px[j];
-            oy[j] = V.py[j];
+            st(ox + j, V.px[j]);
+            st(oy + j, V.py[j]);
         }
     }
 }
@@ -1272,7 +1343,7 @@ __global__ void k_fProlongFine(Batch Bt, const __grid_constant__ WorldSrc<ONE> s
         // the cell's words and the prolongation's loaded together, then used
         // for a liquid cell only
         const float rho = L0.rho[i], px0 = L0.px[i], py0 = L0.py[i];
-        const V2 e = prolongedFrom(urho, F.L[1].ux, F.L[1].uy, (int)D.level_w[1], (int)D.level_h[1], c.x, c.y);
+        const V2 e = prolongedFrom(urho, upx<T>(F, 1u), upy<T>(F, 1u), (int)D.level_w[1], (int)D.level_h[1], c.x, c.y);
         if (rho > 0.0f) {
             float px = px0 + e.x, py = py0 + e.y;
             L0.px[i] = px;
@@ -2252,7 +2323,7 @@ uint32_t fast_cycle_t(const Batch& Bt0, const BatchShape& S, const World* one, c
     k_fLoopStart<<<list_grid(S, L_ONE, 1), 32, 0, s>>>(Bt);
     mark(WIG_SLOT_F_LOOP, 1);
     mark(WIG_SLOT_F_RELAX, 0);
-    LAUNCH(k_fRelax, GR, 128, 0, 0);
+    LAUNCH_T(k_fRelax, T, GR, 128, 0, 0);
     mark(WIG_SLOT_F_RELAX, 1);
     // down: each world restricts its levels 1..lc by themselves and smooths
     // those above lc (a kernel a level), then its levels from lc are the
@@ -2275,7 +2346,7 @@ uint32_t fast_cycle_t(const Batch& Bt0, const BatchShape& S, const World* one, c
     LAUNCH_T(k_fProlongFine, T, G, 64, 0);
     mark(WIG_SLOT_F_PROLONG_FINE, 1);
     mark(WIG_SLOT_F_RELAX, 0);
-    LAUNCH(k_fRelax, GR, 128, 0, 1);
+    LAUNCH_T(k_fRelax, T, GR, 128, 0, 1);
     mark(WIG_SLOT_F_RELAX, 1);
     mark(WIG_SLOT_F_RHO_BETA, 0);
     LAUNCH(k_fRhoBeta, G4, 256, 0);
