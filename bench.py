@@ -134,8 +134,10 @@ def params(world, step, seed):
 # level of n cells.  A level cell holds four potential words of p bytes
 # (px, py, rx, ry: FP32, 4; the mixed form's bf16, 2), five operator words
 # of e bytes (rho, b0..b3: 4, or 2 in the mixed form's binary16) and,
-# stored only in FP32, its diagonal (d = 4, mixed 0); level 0 is all FP32
-# (40 B a cell).  Down (restriction, then both colours of smoothing on
+# stored only in FP32, its diagonal (d = 4, mixed 0); level 0's restriction
+# reads 40 B a cell in FP32 (the potentials, right-hand sides, density,
+# coefficients and diagonal), 28 in the mixed form (its coefficients from
+# their binary16 copies, no diagonal).  Down (restriction, then both colours of smoothing on
 # chip): the four finer cells read, the coarse cell's px, py, rx, ry and
 # rho written, 180 n in FP32; up (prolongation, then both colours): the
 # level's words read, its way-up potentials written, the coarser level's
@@ -148,9 +150,9 @@ def level_bytes(name, s):
     L = s.get("levels")
     if not L:
         return None
-    p, e, d = (2, 2, 0) if s.get("mixed") else (4, 4, 4)
+    p, e, d, c0 = (2, 2, 0, 28) if s.get("mixed") else (4, 4, 4, 40)
     cell = 4 * p + 5 * e + d
-    down = [(4 * (40 if i == 0 else cell) + 4 * p + e) * r for i, (r, _, _) in enumerate(L) if r]
+    down = [(4 * (c0 if i == 0 else cell) + 4 * p + e) * r for i, (r, _, _) in enumerate(L) if r]
     up = [(cell + 2 * p + (e + 2 * p) / 4) * m for _, m, _ in L if m]
     co = [(6 * p + e) * c for _, _, c in L if c]
     if name == "F_RESTRICT" and down:
@@ -192,14 +194,15 @@ def level_stats(worlds, coarse_cells=4096):
 TRAFFIC_PER_ALG_BYTE = {
     # k_fDown on level 1 of the disks 1024x1024 world: 22.8 MB read, 256 B
     # written; 262,144 cells x 180 B
-    ("F_RESTRICT", False): ((22.8e6 + 256) / (262144 * 180), "k_fDown, level 1 (512x512) of the disks 1024x1024 world"),
+    ("F_RESTRICT", False): ((23.902e6 + 3584) / (262144 * 180), "k_fDown, level 1 (512x512) of the disks 1024x1024 world"),
     # k_fDown on levels 1-3 of one iteration of a 64-world batch, mixed form:
-    # 117.1 MB read and written; 222.2 MB algorithmic
-    ("F_RESTRICT", True): (117145856 / 222247528, "k_fDown, levels 1-3 of one iteration of a 64-world mixed batch"),
-    # k_fRelax on the disks 1024x1024 world: 25.0 MB read, 0 written; 24.5 MB
-    # algorithmic (the fine level is FP32 in both forms)
-    ("F_RELAX", False): (25.0e6 / 24.5e6, "k_fRelax, the disks 1024x1024 world"),
-    ("F_RELAX", True): (25.0e6 / 24.5e6, "k_fRelax, the disks 1024x1024 world"),
+    # 90.9 MB read and written; 151.8 MB algorithmic
+    ("F_RESTRICT", True): (90.86e6 / 151.8e6, "k_fDown, levels 1-3 of one iteration of a 64-world mixed batch"),
+    # k_fRelax on the disks 1024x1024 world: 28.0 MB read, 0 written; 24.5 MB
+    # algorithmic (the mixed form reads 12 B a cell less: its coefficients'
+    # binary16 copies, no diagonal)
+    ("F_RELAX", False): (28.0e6 / 24.5e6, "k_fRelax, the disks 1024x1024 world"),
+    ("F_RELAX", True): (28.0e6 / 24.5e6, "k_fRelax, the disks 1024x1024 world"),
 }
 
 
