@@ -239,6 +239,7 @@ void dev_shape(wig::Dev& D, const wig_world_layout& L) {
     D.F = L.face_count;
     D.B = L.block_count;
     D.BW = L.blocks_wide;
+    D.bw_mul = 0xffffffffu / L.blocks_wide;
     D.BH = L.block_count / L.blocks_wide;
     D.cap = L.capacity;
     D.ppc = L.liquid_per_cell;

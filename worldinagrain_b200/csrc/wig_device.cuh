@@ -122,6 +122,7 @@ static_assert(sizeof(StepHead) == offsetof(StepState, err), "StepHead is StepSta
 struct Dev {
     int W, H;
     uint32_t C, F, B, BW, BH, cap, ppc, edge_tiles, levels;
+    uint32_t bw_mul;  // floor((2^32 - 1) / BW): a block index's row by a multiply-high and one correction
     uint32_t level_w[WIG_MG_LEVELS + 1];
     uint32_t level_h[WIG_MG_LEVELS + 1];
     uint32_t level_start[WIG_MG_LEVELS + 1];
@@ -270,10 +271,18 @@ struct W {
                 if (inBlocks(I2{x, y})) r |= D.blocks[stateSlot(blockIndex(I2{x, y}))];
         return r;
     }
-    __device__ I2 activeBlock(uint32_t wid) const {
-        uint32_t n = D.blocks[activeSlot(wid)];
-        return I2{(int)(n % D.BW), (int)(n / D.BW)};
+    // Block n's (column, row): n / BW as umulhi(n, floor((2^32 - 1) / BW)),
+    // which is the quotient or one below it for any 32-bit n, corrected by
+    // the remainder (in place of an integer division's instruction sequence).
+    __device__ __forceinline__ I2 blockAt(uint32_t n) const {
+        uint32_t q = __umulhi(n, D.bw_mul), r = n - q * D.BW;
+        if (r >= D.BW) {
+            q += 1u;
+            r -= D.BW;
+        }
+        return I2{(int)r, (int)q};
     }
+    __device__ I2 activeBlock(uint32_t wid) const { return blockAt(D.blocks[activeSlot(wid)]); }
     // facesOf (fluid.wgsl:296-303)
     __device__ void facesOf(I2 c, int out[4][3]) const {
         bool right = c.x == D.W - 1 || (c.x % BLOCK == BLOCK - 1 && !isActiveBlock(I2{c.x / BLOCK + 1, c.y / BLOCK}));

@@ -370,7 +370,8 @@ __global__ void __launch_bounds__(256) k_fSetup(Batch Bt, const __grid_constant_
         const uint32_t it = Bt.item(L_RET, t);
         FAST_ITEM_G(Bt, it, D, F, w, j);
         uint32_t n = D.blocks[w.retiredSlot(j)];
-        I2 c{(int)(n % D.BW) * BLOCK + (int)(threadIdx.x & 7u), (int)(n / D.BW) * BLOCK + (int)((threadIdx.x >> 3) & 7u)};
+        const I2 bq_ = w.blockAt(n);
+        I2 c{bq_.x * BLOCK + (int)(threadIdx.x & 7u), bq_.y * BLOCK + (int)((threadIdx.x >> 3) & 7u)};
         if (w.inWorld(c)) {
             uint32_t i = w.cellIndex(c);
             const Lvl& L0 = F.L[0];
@@ -388,7 +389,8 @@ __global__ void k_fZeroIdle(Batch Bt) {
         FAST_ITEM_G(Bt, it, D, F, w, n);
         if (D.st->book != 0u || (D.blocks[w.stateSlot(n)] & ACTIVE) != 0u) continue;
         for (uint32_t t = threadIdx.x; t < 64u; t += blockDim.x) {
-            I2 c{(int)(n % D.BW) * BLOCK + (int)(t & 7u), (int)(n / D.BW) * BLOCK + (int)(t >> 3)};
+            const I2 bq_ = w.blockAt(n);
+            I2 c{bq_.x * BLOCK + (int)(t & 7u), bq_.y * BLOCK + (int)(t >> 3)};
             if (!w.inWorld(c)) continue;
             const uint32_t i = w.cellIndex(c);
             F.L[0].px[i] = 0.0f; F.L[0].py[i] = 0.0f; F.L[0].rho[i] = 0.0f;
@@ -500,7 +502,7 @@ __device__ __forceinline__ float diagAt(const LRefX<P, R, __half>& V, uint32_t k
 
 __device__ I2 tileBlockF(const W& w, uint32_t wid, int shift) {
     if (wid < w.activeCount()) return w.activeBlock(wid);
-    int wide = (int)w.D.BW, high = (int)(w.D.B / w.D.BW);
+    int wide = (int)w.D.BW, high = (int)w.D.BH;
     int j = (int)wid - (int)w.D.B;
     if (shift == 0 || j < 0 || j > high + wide) return I2{-1, -1};
     return j <= high ? I2{wide, j} : I2{j - high - 1, high};
@@ -910,7 +912,7 @@ __device__ __forceinline__ void tileSmooth(LevelTile& t, int x0, int y0, int lw,
 // and later ones read them back), stored by the tile's own cells on the
 // first iteration.
 template <bool ONE, class T>
-__global__ void __launch_bounds__(256, ONE ? 3 : 2) k_fDown(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
+__global__ void __launch_bounds__(256, ONE ? 4 : 2) k_fDown(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
     __shared__ LevelTile t;
@@ -993,7 +995,7 @@ __global__ void __launch_bounds__(256, ONE ? 3 : 2) k_fDown(Batch Bt, const __gr
 // too) and the results go to ux, uy, so no CTA reads a cell that another
 // writes in the same launch; level l + 1's results are its ux, uy.
 template <bool ONE, class T>
-__global__ void __launch_bounds__(256, ONE ? 3 : 2) k_fUp(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
+__global__ void __launch_bounds__(256, ONE ? 4 : 2) k_fUp(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
     __shared__ LevelTile t;
@@ -1394,27 +1396,33 @@ __global__ void __launch_bounds__(256) k_fRhoBeta(Batch Bt, const __grid_constan
                 }
             }
         }
-        tilePut(ux[par], vx);
-        tilePut(uy[par], vy);
+        // the f32 trees only without FP64 dots, which read none of them
         if (f64) {
             tilePut(ex64[par], ex);
             tilePut(ey64[par], ey);
+        } else {
+            tilePut(ux[par], vx);
+            tilePut(uy[par], vy);
         }
         __syncthreads();
-        const float tx = tileSum(ux[par], vx), ty = tileSum(uy[par], vy);
+        float tx = 0.0f, ty = 0.0f;
         double dx = 0.0, dy = 0.0;
         if (f64) {
             dx = tileSum(ex64[par], ex);
             dy = tileSum(ey64[par], ey);
+        } else {
+            tx = tileSum(ux[par], vx);
+            ty = tileSum(uy[par], vy);
         }
         par ^= 1u;
         if (valid && (threadIdx.x & 63u) == 0u) {
             const uint32_t b = w.blockIndex(w.activeBlock(wid));
-            F.part32[2u * b] = tx;
-            F.part32[2u * b + 1u] = ty;
             if (f64) {
                 F.part64[2u * b] = dx;
                 F.part64[2u * b + 1u] = dy;
+            } else {
+                F.part32[2u * b] = tx;
+                F.part32[2u * b + 1u] = ty;
             }
         }
         pend_ += min(4u, na - g * 4u);
@@ -1505,20 +1513,22 @@ __global__ void __launch_bounds__(256) k_fApplyAlpha(Batch Bt, const __grid_cons
                 ex = (double)p * (double)q;
             }
         }
-        tilePut(ux[par], vx);
         if (f64) tilePut(ex64[par], ex);
+        else tilePut(ux[par], vx);
         __syncthreads();
-        const float tx = tileSum(ux[par], vx);
+        float tx = 0.0f;
         double dx = 0.0;
         if (f64) dx = tileSum(ex64[par], ex);
+        else tx = tileSum(ux[par], vx);
         par ^= 1u;
         if (valid && (threadIdx.x & 63u) == 0u) {
             const uint32_t b = w.blockIndex(w.activeBlock(wid));
-            F.part32[2u * b] = tx;
-            F.part32[2u * b + 1u] = 0.0f;
             if (f64) {
                 F.part64[2u * b] = dx;
                 F.part64[2u * b + 1u] = 0.0;
+            } else {
+                F.part32[2u * b] = tx;
+                F.part32[2u * b + 1u] = 0.0f;
             }
         }
         pend_ += min(4u, na - g * 4u);

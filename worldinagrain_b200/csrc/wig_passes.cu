@@ -199,7 +199,7 @@ __global__ void k_sync(Batch Bt, int sync_claims) {
   FOR_ITEMS(Bt, L_WB, it) {
     ITEM_WORLD_C(Bt, it, D, w, n);
     const bool claims = sync_claims && D.st->book == 0u;
-    const I2 b{(int)(n % D.BW), (int)(n / D.BW)};
+    const I2 b = w.blockAt(n);
     I2 c{b.x * BLOCK + (int)(threadIdx.x & 7u), b.y * BLOCK + (int)(threadIdx.x >> 3)};
     bool here = false;
     if (w.inWorld(c)) {
@@ -392,7 +392,8 @@ __global__ void k_syncSeed(Batch Bt) {
   FOR_ITEMS(Bt, L_WB, qi) {
     ITEM_WORLD_C(Bt, qi, D, w, blk);
     if (D.st->book) continue;
-    I2 c{(int)(blk % D.BW) * BLOCK + (int)(threadIdx.x & 7u), (int)(blk / D.BW) * BLOCK + (int)(threadIdx.x >> 3)};
+    const I2 bq_ = w.blockAt(blk);
+    I2 c{bq_.x * BLOCK + (int)(threadIdx.x & 7u), bq_.y * BLOCK + (int)(threadIdx.x >> 3)};
     uint32_t n = 0;
     uint4 v = make_uint4(0, 0, 0, 0);
     Rng g;
@@ -447,7 +448,7 @@ __global__ void __launch_bounds__(1024) k_compact(Batch Bt) {
     const uint32_t lo = min(threadIdx.x * per, D.B), hi = min(lo + per, D.B);
     uint32_t na = 0, nr = 0;
     for (uint32_t n = lo; n < hi; n++) {
-        I2 b{(int)(n % D.BW), (int)(n / D.BW)};
+        I2 b = w.blockAt(n);
         uint32_t marks = 0;
         for (int y = -1; y <= 1; y++)
             for (int x = -1; x <= 1; x++) {
@@ -474,7 +475,7 @@ __global__ void __launch_bounds__(1024) k_compact(Batch Bt) {
     // All states are read above before any is written below.
     __syncthreads();
     for (uint32_t n = lo; n < hi; n++) {
-        I2 b{(int)(n % D.BW), (int)(n / D.BW)};
+        I2 b = w.blockAt(n);
         uint32_t marks = 0;
         for (int y = -1; y <= 1; y++)
             for (int x = -1; x <= 1; x++) {
@@ -503,7 +504,8 @@ __global__ void k_retire(Batch Bt) {
     FOR_ITEMS(Bt, L_RET, it) {
         ITEM_WORLD_C(Bt, it, D, w, wid);
         uint32_t n = D.blocks[w.retiredSlot(wid)];
-        I2 c{(int)(n % D.BW) * BLOCK + (int)(threadIdx.x & 7u), (int)(n / D.BW) * BLOCK + (int)(threadIdx.x >> 3)};
+        const I2 bq_ = w.blockAt(n);
+        I2 c{bq_.x * BLOCK + (int)(threadIdx.x & 7u), bq_.y * BLOCK + (int)(threadIdx.x >> 3)};
         if (!w.inWorld(c)) continue;
         uint32_t i = w.cellIndex(c);
         reinterpret_cast<float4*>(D.field)[2u * i] = make_float4(0, 0, 0, 0);
@@ -1227,7 +1229,7 @@ __global__ void k_relaxRims(Dev D, uint32_t cycle) {
 // tileBlock (fluid.wgsl:2080-2091)
 __device__ I2 tileBlock(const W& w, uint32_t wid, int shift) {
     if (wid < w.activeCount()) return w.activeBlock(wid);
-    int wide = (int)w.D.BW, high = (int)(w.D.B / w.D.BW);
+    int wide = (int)w.D.BW, high = (int)w.D.BH;
     int j = (int)wid - (int)w.D.B;
     if (shift == 0 || j < 0 || j > high + wide) return I2{-1, -1};
     return j <= high ? I2{wide, j} : I2{j - high - 1, high};
