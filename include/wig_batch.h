@@ -101,13 +101,18 @@ uint64_t wig_batch_resident_bytes(const wig_batch* b);
 int wig_batch_set_lane_pool(wig_batch* b, uint32_t lane, uint64_t bytes);
 int wig_batch_world_bytes_split(const wig_world_desc* d, uint64_t* persistent, uint64_t* transient);
 
-/* Launch shapes of the fast form, none of which changes a result bit (every
- * kernel's arithmetic and order are the same whichever CTA does a unit):
- * what an autotuner may choose per batch.
+/* Launch shapes of the fast form, none of which changes a result bit of
+ * the FP32 forms (every kernel's arithmetic and order are the same whichever
+ * CTA does a unit; in the mixed form COARSE_CELLS also decides which levels
+ * stay FP32 on chip rather than stored in 16 bits): what an autotuner may
+ * choose per batch.
  *   COARSE_CELLS: the one-CTA coarse kernel takes a world's levels from its
  *     first level of at most this many cells (1 .. 4096; a world with no
  *     such level above its coarsest: from the coarsest), the tile kernels
- *     the levels above it: the depth of the V-cycle's on-chip part;
+ *     the levels above it: the depth of the V-cycle's on-chip part.  A
+ *     batch of one world takes up to 16384: from a level of more than 4096
+ *     cells its coarse levels run on a cluster of 8 CTAs (WIG_E_ARG when
+ *     they do not fit its shared memory);
  *   LEVEL_PER_SM, CG_PER_SM, RELAX_PER_SM: CTAs a multiprocessor (1 .. 64)
  *     of the level tile kernels, of the three CG kernels, of the fine
  *     relaxation.

@@ -83,3 +83,22 @@ def test_a_drift_over_the_steps_weighs_the_same_on_every_candidate():
     b = Drifting()
     shapes, _ = tune.autotune(b, b.step, knobs=(tune.KNOBS[0],), passes=1)
     assert shapes[name] == cands[-1]
+
+
+def test_a_refused_candidate_is_left_out():
+    """A batch of several worlds refuses coarse cells above 4096 (the
+    single world's cluster range): that candidate gets no cost and no step,
+    and the choice falls among the others."""
+    from worldinagrain_b200.fluid import WigError
+
+    class Several(FakeBatch):
+        def set_launch(self, name, value):
+            if name == "coarse_cells" and value > 4096:
+                raise WigError("launch knob value out of range")
+            super().set_launch(name, value)
+    costs = {name: {v: 1.0 + 0.1 * i for i, v in enumerate(c)} for name, c, _ in tune.KNOBS}
+    b = Several(costs)
+    shapes, trials = tune.autotune(b, b.step)
+    assert dict(trials["coarse_cells"])[16384] is None
+    assert shapes["coarse_cells"] == 4096
+    assert all(v <= 4096 for n, v in b.log if n == "coarse_cells")

@@ -353,7 +353,9 @@ int upload_world_entry(wig_batch* b, uint32_t k) {
 
 // The level part of a batch's shape for its coarse_cells: each world's
 // coarse level (into its table entry), the level lists' current lengths,
-// the deepest level restricted by a tile kernel, the coarse kernel's memory.
+// the deepest level restricted by a tile kernel, the coarse kernel's memory
+// (a single world's from a level too large for one CTA: the cluster
+// kernel's).
 void level_shape(wig_batch* b) {
     wig::BatchShape& S = b->S;
     for (uint32_t l = 0; l < WIG_MG_LEVELS; l++) {
@@ -362,6 +364,7 @@ void level_shape(wig_batch* b) {
     }
     S.lc_max = 0;
     S.coarse_smem = 0;
+    S.cluster = 0;
     for (uint32_t k = 0; k < b->K; k++) {
         wig::World& Wd = b->hw[k];
         const wig::Dev& D = Wd.D;
@@ -373,7 +376,9 @@ void level_shape(wig_batch* b) {
             if (l < lc) S.max_items[wig::L_SM + l - 1] += ch;
         }
         S.lc_max = std::max(S.lc_max, lc);
-        S.coarse_smem = std::max(S.coarse_smem, wig::fast_coarse_smem(D, lc));
+        const size_t c = b->K == 1 ? wig::fast_cluster_smem(D, lc) : 0;
+        if (c) S.cluster = 1;
+        S.coarse_smem = std::max(S.coarse_smem, c ? c : wig::fast_coarse_smem(D, lc));
     }
 }
 
@@ -1534,16 +1539,26 @@ int wig_batch_world_bytes_split(const wig_world_desc* d, uint64_t* persistent, u
 int wig_batch_set_launch(wig_batch* b, uint32_t knob, uint32_t value) {
     if (!b) return fail(WIG_E_ARG, "null batch");
     if (knob >= WIG_LAUNCH_KNOBS) return fail(WIG_E_ARG, "unknown launch knob");
-    const uint32_t most = knob == WIG_LAUNCH_COARSE_CELLS ? wig::COARSE_CTA_CELLS : 64u;
+    // a single world's coarse levels may start higher: on a cluster
+    const uint32_t most = knob != WIG_LAUNCH_COARSE_CELLS ? 64u
+                          : b->K == 1                    ? wig::COARSE_CLUSTER_CELLS
+                                                         : wig::COARSE_CTA_CELLS;
     if (value < 1u || value > most) return fail(WIG_E_ARG, "launch knob value out of range");
     CUDA_TRY(cudaDeviceSynchronize());
     wig::BatchShape& S = b->S;
     switch (knob) {
-    case WIG_LAUNCH_COARSE_CELLS:
+    case WIG_LAUNCH_COARSE_CELLS: {
+        const uint32_t was = S.coarse_cells;
         S.coarse_cells = value;
         level_shape(b);
+        if (S.coarse_smem > 220u * 1024u || wig::fast_prepare_attributes(S.coarse_smem) != cudaSuccess) {
+            S.coarse_cells = was;
+            level_shape(b);
+            return fail(WIG_E_ARG, "coarse levels too large for the coarse kernel");
+        }
         CUDA_TRY(cudaMemcpy(b->d_worlds, b->hw.data(), sizeof(wig::World) * b->K, cudaMemcpyHostToDevice));
         break;
+    }
     case WIG_LAUNCH_LEVEL_PER_SM: S.level_per_sm = value; break;
     case WIG_LAUNCH_CG_PER_SM: S.cg_per_sm = value; break;
     default: S.relax_per_sm = value; break;

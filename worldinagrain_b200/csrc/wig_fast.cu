@@ -22,6 +22,7 @@
 
 #include <algorithm>
 
+#include <cooperative_groups.h>
 #include <cuda_bf16.h>
 
 #include "wig_fast.cuh"
@@ -912,7 +913,7 @@ __device__ __forceinline__ void tileSmooth(LevelTile& t, int x0, int y0, int lw,
 // and later ones read them back), stored by the tile's own cells on the
 // first iteration.
 template <bool ONE, class T>
-__global__ void __launch_bounds__(256, ONE ? 4 : 2) k_fDown(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
+__global__ void __launch_bounds__(256, 4) k_fDown(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
     __shared__ LevelTile t;
@@ -995,7 +996,7 @@ __global__ void __launch_bounds__(256, ONE ? 4 : 2) k_fDown(Batch Bt, const __gr
 // too) and the results go to ux, uy, so no CTA reads a cell that another
 // writes in the same launch; level l + 1's results are its ux, uy.
 template <bool ONE, class T>
-__global__ void __launch_bounds__(256, ONE ? 4 : 2) k_fUp(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
+__global__ void __launch_bounds__(256, 4) k_fUp(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
     __shared__ LevelTile t;
@@ -1160,39 +1161,15 @@ __device__ void slv_smooth(const SLv& V, uint32_t l, int tid, int nt) {
     }
 }
 
-// The levels lc (restricted already, in the scratch) down to the coarsest and
-// back up to lc, in one CTA's shared memory: smoothRed/Black, restrictLevel,
-// solve (40 SOR sweep pairs, omega 1.8), prolong (fluid.wgsl:2318-2470).
-// Each level's face coefficients are worked out once, when its densities
-// are in place, and read by its sweeps and by the restriction below it.
-// Level lc's results go to its ux, uy (`up`, the fast form) or back into its
-// px, py (the persistent form).
-template <class T = float>
-__device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t lc, float* sm, uint32_t* off,
-                             bool up) {
+// The levels from lc (in sm from offsets off[]: just loaded, or restricted
+// already) down to the coarsest and back up to lc: each level's
+// coefficients worked out once its densities are in place, smoothRed/Black,
+// restrictLevel, solve (40 SOR sweep pairs, omega 1.8), prolong
+// (fluid.wgsl:2318-2470); the result in level lc's px, py.  Every thread of
+// the CTA takes part.
+__device__ void coarseCore(const Dev& D, const W& w, uint32_t lc, float* sm, const uint32_t* off) {
     const uint32_t L = D.levels;
     const int tid = (int)threadIdx.x, nt = (int)blockDim.x;
-    if (tid == 0) {
-        uint32_t o = 0;
-        for (uint32_t l = lc; l <= L; l++) {
-            off[l] = o;
-            o += SLV_ARRAYS * D.level_w[l] * D.level_h[l];
-        }
-    }
-    __syncthreads();
-    {
-        const SLv V = slv(sm, off, D, lc);
-        const LRef<T> G = lref<T>(F, lc);
-        const int n = V.w * V.h;
-        for (int j = tid; j < n; j += nt) {
-            V.px[j] = ld(G.px + j);
-            V.py[j] = ld(G.py + j);
-            V.rx[j] = ld(G.rx + j);
-            V.ry[j] = ld(G.ry + j);
-            V.rho[j] = ld(G.rho + j);
-        }
-        __syncthreads();
-    }
     for (uint32_t l = lc; l <= L; l++) {
         const SLv V = slv(sm, off, D, l);
         const int n = V.w * V.h;
@@ -1302,6 +1279,42 @@ __device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t 
         __syncthreads();
         slv_smooth(V, (uint32_t)l, tid, nt);
     }
+}
+
+// The levels lc (restricted already, in the scratch) down to the coarsest and
+// back up to lc, in one CTA's shared memory: smoothRed/Black, restrictLevel,
+// solve (40 SOR sweep pairs, omega 1.8), prolong (fluid.wgsl:2318-2470).
+// Each level's face coefficients are worked out once, when its densities
+// are in place, and read by its sweeps and by the restriction below it.
+// Level lc's results go to its ux, uy (`up`, the fast form) or back into its
+// px, py (the persistent form).
+template <class T = float>
+__device__ void coarseLevels(const Dev& D, const FastW& F, const W& w, uint32_t lc, float* sm, uint32_t* off,
+                             bool up) {
+    const uint32_t L = D.levels;
+    const int tid = (int)threadIdx.x, nt = (int)blockDim.x;
+    if (tid == 0) {
+        uint32_t o = 0;
+        for (uint32_t l = lc; l <= L; l++) {
+            off[l] = o;
+            o += SLV_ARRAYS * D.level_w[l] * D.level_h[l];
+        }
+    }
+    __syncthreads();
+    {
+        const SLv V = slv(sm, off, D, lc);
+        const LRef<T> G = lref<T>(F, lc);
+        const int n = V.w * V.h;
+        for (int j = tid; j < n; j += nt) {
+            V.px[j] = ld(G.px + j);
+            V.py[j] = ld(G.py + j);
+            V.rx[j] = ld(G.rx + j);
+            V.ry[j] = ld(G.ry + j);
+            V.rho[j] = ld(G.rho + j);
+        }
+        __syncthreads();
+    }
+    coarseCore(D, w, lc, sm, off);
     {
         const SLv V = slv(sm, off, D, lc);
         auto* ox = up ? upx<T>(F, lc) : lref<T>(F, lc).px;
@@ -1326,6 +1339,366 @@ __global__ void __launch_bounds__(1024) k_fCoarse(Batch Bt, const __grid_constan
         if (D.st->cont == 0u) continue;
         coarseLevels<T>(D, F, w, F.lc, sm, off, true);
         __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------- the coarse levels on a cluster
+//
+// A single world whose coarse kernel starts at a level of more than
+// COARSE_CTA_CELLS cells (at 1024 x 1024: 128 x 128, with the coarse_cells
+// knob at 16384) runs its coarse levels on one thread-block cluster of
+// CLUSTER_CTAS CTAs instead of one CTA, in their distributed shared memory.
+// Each level of more than RANK0_CELLS cells is cut into strips of rows, a
+// strip a CTA, its nine arrays (px, py, rx, ry, rho, b0..b3) in that CTA's
+// shared memory at the same offsets in every CTA; a neighbour's row across a
+// strip's edge is read from the owning CTA (cluster.map_shared_rank).  The
+// levels of at most RANK0_CELLS cells are CTA 0's alone (coarseCore, as in
+// the one-CTA kernel).  Every pass is the one-CTA kernel's, cell for cell, in
+// the same arithmetic and order (the cells of a colour are independent), and
+// a cluster barrier ends each pass whose results another CTA reads.  The
+// levels it takes over from the tile kernels (the restrict-only launch of
+// its first level stays) would each have been a launch of one wave of a few
+// CTAs.
+constexpr int CLUSTER_CTAS = 8;
+constexpr uint32_t RANK0_CELLS = 1024;
+
+enum { A_PX = 0, A_PY, A_RX, A_RY, A_RHO, A_B0, A_B1, A_B2, A_B3 };
+
+// n / d for any 32-bit n, with mul = floor((2^32 - 1) / d): the multiply-high
+// is the quotient or one below it.
+__device__ __forceinline__ uint32_t divq(uint32_t n, uint32_t d, uint32_t mul) {
+    uint32_t q = __umulhi(n, mul);
+    if (n - q * d >= d) q += 1u;
+    return q;
+}
+
+// A level cut into strips: this CTA's rows r0 .. r1 - 1 of rpr a CTA; array
+// k of a CTA's rows at base + k n (n = rpr w floats).
+struct DLv {
+    float* base;
+    int n, w, h, rpr, r0, r1;
+    uint32_t wmul, rmul;
+    __device__ float* a(int k) const { return base + k * n; }
+};
+// The strip levels' shared memory: level lc's from sm, each next level's
+// after the one above it.
+__host__ __device__ inline size_t stripFloats(uint32_t w, uint32_t h) {
+    return (size_t)SLV_ARRAYS * ((h + CLUSTER_CTAS - 1) / CLUSTER_CTAS) * w;
+}
+__device__ __forceinline__ DLv dlv(float* sm, const Dev& D, uint32_t lc, uint32_t l, unsigned me) {
+    for (uint32_t k = lc; k < l; k++) sm += stripFloats(D.level_w[k], D.level_h[k]);
+    DLv V;
+    V.base = sm;
+    V.w = (int)D.level_w[l];
+    V.h = (int)D.level_h[l];
+    V.rpr = (V.h + CLUSTER_CTAS - 1) / CLUSTER_CTAS;
+    V.n = V.rpr * V.w;
+    V.r0 = min((int)me * V.rpr, V.h);
+    V.r1 = min(V.r0 + V.rpr, V.h);
+    V.wmul = 0xffffffffu / (uint32_t)V.w;
+    V.rmul = 0xffffffffu / (uint32_t)V.rpr;
+    return V;
+}
+// Row y of a strip level (its array 0; array k at + k n), in whichever CTA
+// holds it.
+__device__ __forceinline__ float* dlRow(const DLv& V, int y, unsigned me) {
+    const unsigned o = divq((uint32_t)y, (uint32_t)V.rpr, V.rmul);
+    float* p = V.base + (y - (int)o * V.rpr) * V.w;
+    return o == me ? p : cooperative_groups::this_cluster().map_shared_rank(p, o);
+}
+// This CTA's own cell j (of (r1 - r0) w): its coordinates.
+__device__ __forceinline__ void dlCell(const DLv& V, int j, int* x, int* y) {
+    const int q = (int)divq((uint32_t)j, (uint32_t)V.w, V.wmul);
+    *x = j - q * V.w;
+    *y = V.r0 + q;
+}
+
+// slv_stencil of a strip level's cell (x, y) in row r (its rows above and
+// below from whichever CTAs hold them): the neighbours clamped onto the cell
+// past the level's edge (nbr), each beta times its potential, in order.
+__device__ __forceinline__ void dl_stencil(const DLv& V, const float* r, int x, int y, unsigned me, float* sx, float* sy,
+                                           float* dg) {
+    const float* u = y > 0 ? dlRow(V, y - 1, me) : r;
+    const float* d = y < V.h - 1 ? dlRow(V, y + 1, me) : r;
+    const int xl = x > 0 ? x - 1 : x, xr = x < V.w - 1 ? x + 1 : x;
+    const int n = V.n;
+    const float b0 = r[A_B0 * n + x], b1 = r[A_B1 * n + x], b2 = r[A_B2 * n + x], b3 = r[A_B3 * n + x];
+    *sx = (((0.0f + b0 * r[xl]) + b1 * r[xr]) + b2 * u[x]) + b3 * d[x];
+    *sy = (((0.0f + b0 * r[n + xl]) + b1 * r[n + xr]) + b2 * u[n + x]) + b3 * d[n + x];
+    *dg = (((0.0f + b0) + b1) + b2) + b3;
+}
+
+// slv_coefficients over this CTA's strip.
+__device__ void dl_coefficients(const DLv& V, unsigned me) {
+    const int n = (V.r1 - V.r0) * V.w;
+    for (int j = (int)threadIdx.x; j < n; j += (int)blockDim.x) {
+        int x, y;
+        dlCell(V, j, &x, &y);
+        const float* own = V.a(A_RHO);
+        const float rho = own[j];
+        float b[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        if (rho > 0.0f) {
+            const float* u = y > 0 ? dlRow(V, y - 1, me) + A_RHO * V.n : nullptr;
+            const float* d = y < V.h - 1 ? dlRow(V, y + 1, me) + A_RHO * V.n : nullptr;
+            const float rn[4] = {x > 0 ? own[j - 1] : 0.0f, x < V.w - 1 ? own[j + 1] : 0.0f, u ? u[x] : 0.0f,
+                                 d ? d[x] : 0.0f};
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                if (!nbrIn(x, y, V.w, V.h, q)) continue;
+                if (rn[q] >= 0.0f) b[q] = faceBeta(rho, rn[q]);
+            }
+        }
+        V.a(A_B0)[j] = b[0];
+        V.a(A_B1)[j] = b[1];
+        V.a(A_B2)[j] = b[2];
+        V.a(A_B3)[j] = b[3];
+    }
+}
+
+// slv_sweep of one colour over this CTA's strip: of its cells 2k and
+// 2k + 1 exactly one has each colour, so pair k gives the cell.
+__device__ void dl_sweep(const DLv& V, uint32_t l, int color, float omega, unsigned me) {
+    const int n = (V.r1 - V.r0) * V.w, pairs = (n + 1) / 2;
+    const float h2 = (float)(1u << (2u * l));
+    for (int k = (int)threadIdx.x; k < pairs; k += (int)blockDim.x) {
+        int j = 2 * k, x, y;
+        dlCell(V, j, &x, &y);
+        if (((x + y) & 1) != color) {
+            j++;
+            if (++x == V.w) {
+                x = 0;
+                y++;
+            }
+        }
+        if (j >= n) continue;
+        if (V.a(A_RHO)[j] <= 0.0f) continue;
+        float* r = V.base + (j - x);
+        float sx, sy, dg;
+        dl_stencil(V, r, x, y, me, &sx, &sy, &dg);
+        if (dg <= 0.0f) continue;
+        float* px = V.a(A_PX);
+        float* py = V.a(A_PY);
+        px[j] = mixf(px[j], (sx - h2 * V.a(A_RX)[j]) / dg, omega);
+        py[j] = mixf(py[j], (sy - h2 * V.a(A_RY)[j]) / dg, omega);
+    }
+}
+
+// restrictLevel into coarse cell (cx, cy) of level l from strip level U
+// (level l - 1), as coarseCore restricts: the stencil from U's stored
+// coefficients.
+__device__ __forceinline__ void dl_restricted(const Dev& D, const W& w, uint32_t l, const DLv& U, int cx, int cy, unsigned me,
+                                              float* px, float* py, float* rx_o, float* ry_o, float* rho_o) {
+    const int span = 1 << l;
+    if (span <= BLOCK) {
+        I2 b{cx * span / BLOCK, cy * span / BLOCK};
+        if (w.inBlocks(b) && (D.blocks[w.stateSlot(w.blockIndex(b))] & ACTIVE) == 0u) {
+            *px = 0.0f; *py = 0.0f; *rx_o = 0.0f; *ry_o = 0.0f; *rho_o = 0.0f;
+            return;
+        }
+    }
+    const float inv_h2u = 1.0f / (float)(1u << (2u * (l - 1u)));
+    const int n = U.n;
+    float fluid = 0.0f, sum = 0.0f, rx = 0.0f, ry = 0.0f;
+    bool air = false;
+    for (int q = 0; q < 4; q++) {
+        const int kx = 2 * cx + (q & 1), ky = 2 * cy + (q >> 1);
+        if (kx >= U.w || ky >= U.h) continue;
+        const float* r = dlRow(U, ky, me);
+        const float rho = r[A_RHO * n + kx];
+        if (rho == 0.0f) air = true;
+        else if (rho > 0.0f) {
+            float sx, sy, dg;
+            dl_stencil(U, r, kx, ky, me, &sx, &sy, &dg);
+            fluid = fluid + 1.0f;
+            sum = sum + rho;
+            rx = rx + (r[A_RX * n + kx] - (sx - (dg + 0.0f) * r[kx]) * inv_h2u);
+            ry = ry + (r[A_RY * n + kx] - (sy - (dg + 0.0f) * r[n + kx]) * inv_h2u);
+        }
+    }
+    const float rho = air ? 0.0f : (fluid > 0.0f ? sum / fluid : -1.0f);
+    *px = 0.0f;
+    *py = 0.0f;
+    *rx_o = rho > 0.0f ? rx * 0.25f : 0.0f;
+    *ry_o = rho > 0.0f ? ry * 0.25f : 0.0f;
+    *rho_o = rho;
+}
+
+// prolonged (fluid.wgsl:2478-2497) of fine cell (cx, cy) from strip level
+// U: prolongedFrom's loads and weights, U's two rows from their CTAs.
+__device__ __forceinline__ V2 dl_prolonged(const DLv& U, int cx, int cy, unsigned me) {
+    const int kx = cx / 2, ky = cy / 2;
+    const int sx = (cx & 1) == 1 ? 1 : -1, sy = (cy & 1) == 1 ? 1 : -1;
+    const int ox[4] = {0, sx, 0, sx}, oy[4] = {0, 0, sy, sy};
+    const float wt[4] = {9.0f, 3.0f, 3.0f, 1.0f};
+    const bool row2 = ky + sy >= 0 && ky + sy < U.h;
+    const float* r0 = dlRow(U, ky, me);
+    const float* r1 = row2 ? dlRow(U, ky + sy, me) : r0;
+    const int n = U.n;
+    float rq[4], xq[4], yq[4];
+    bool inq[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        const int ax_ = kx + ox[q], ay_ = ky + oy[q];
+        inq[q] = !(ax_ < 0 || ay_ < 0 || ax_ >= U.w || ay_ >= U.h);
+        const float* r = oy[q] == 0 ? r0 : r1;
+        const int c = inq[q] ? ax_ : kx;
+        rq[q] = r[A_RHO * n + c];
+        xq[q] = r[c];
+        yq[q] = r[n + c];
+    }
+    float ax = 0.0f, ay = 0.0f, weight = 0.0f;
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        if (!inq[q]) continue;
+        const float r = rq[q];
+        if (r < 0.0f) continue;
+        weight = weight + wt[q];
+        if (r > 0.0f) {
+            ax = ax + wt[q] * xq[q];
+            ay = ay + wt[q] * yq[q];
+        }
+    }
+    const float ww = fmaxf(weight, 1e-6f);
+    return V2{ax / ww, ay / ww};
+}
+
+// The cluster's shared memory (floats a CTA) for a world from level lc: each
+// strip level's rows of one CTA, then CTA 0's levels ls .. L; 0 when the
+// coarsest level has more than RANK0_CELLS cells.
+__host__ __device__ inline size_t clusterFloats(const uint32_t* lw, const uint32_t* lh, uint32_t lc, uint32_t L,
+                                                uint32_t* ls_out) {
+    size_t n = 0;
+    uint32_t l = lc;
+    for (; l <= L && lw[l] * lh[l] > RANK0_CELLS; l++) n += stripFloats(lw[l], lh[l]);
+    if (ls_out) *ls_out = l;
+    if (l > L) return 0;
+    for (uint32_t k = l; k <= L; k++) n += (size_t)SLV_ARRAYS * lw[k] * lh[k];
+    return n;
+}
+
+template <class T>
+__global__ void __launch_bounds__(1024) k_fCoarseCluster(Batch Bt, const __grid_constant__ WorldSrc<true> src) {
+    extern __shared__ float sm[];
+    __shared__ uint32_t off[WIG_MG_LEVELS + 1];
+    namespace cgs = cooperative_groups;
+    cgs::cluster_group cl = cgs::this_cluster();
+    const unsigned me = cl.block_rank();
+    const World& Wd = src.w;
+    const Dev& D = Wd.D;
+    const FastW& F = Wd.S;
+    const W w(D);
+    (void)Bt;
+    // every CTA reads the same word: all go on, or all return, together
+    if (D.st->cont == 0u) return;
+    const uint32_t lc = F.lc, L = D.levels;
+    uint32_t ls = lc;
+    clusterFloats(D.level_w, D.level_h, lc, L, &ls);
+    // CTA 0's levels ls .. L after the strip levels lc .. ls - 1
+    float* sm0 = sm;
+    for (uint32_t l = lc; l < ls; l++) sm0 += stripFloats(D.level_w[l], D.level_h[l]);
+    if (threadIdx.x == 0) {
+        uint32_t o = 0;
+        for (uint32_t l = ls; l <= L; l++) {
+            off[l] = o;
+            o += SLV_ARRAYS * D.level_w[l] * D.level_h[l];
+        }
+    }
+    // level lc's rows from the scratch (restricted by the down kernel)
+    {
+        const DLv A = dlv(sm, D, lc, lc, me);
+        const LRef<T> G = lref<T>(F, lc);
+        const int n = (A.r1 - A.r0) * A.w;
+        for (int j = (int)threadIdx.x; j < n; j += (int)blockDim.x) {
+            const int g = A.r0 * A.w + j;
+            A.a(A_PX)[j] = ld(G.px + g);
+            A.a(A_PY)[j] = ld(G.py + g);
+            A.a(A_RX)[j] = ld(G.rx + g);
+            A.a(A_RY)[j] = ld(G.ry + g);
+            A.a(A_RHO)[j] = ld(G.rho + g);
+        }
+    }
+    cl.sync();
+    // down the strip levels
+    for (uint32_t l = lc; l < ls; l++) {
+        const DLv A = dlv(sm, D, lc, l, me);
+        if (l > lc) {
+            const DLv U = dlv(sm, D, lc, l - 1u, me);
+            const int n = (A.r1 - A.r0) * A.w;
+            for (int j = (int)threadIdx.x; j < n; j += (int)blockDim.x) {
+                int x, y;
+                dlCell(A, j, &x, &y);
+                dl_restricted(D, w, l, U, x, y, me, &A.a(A_PX)[j], &A.a(A_PY)[j], &A.a(A_RX)[j], &A.a(A_RY)[j],
+                              &A.a(A_RHO)[j]);
+            }
+            cl.sync();
+        }
+        dl_coefficients(A, me);
+        __syncthreads();
+        dl_sweep(A, l, 0, SMOOTH_OMEGA, me);
+        cl.sync();
+        dl_sweep(A, l, 1, SMOOTH_OMEGA, me);
+        cl.sync();
+    }
+    // CTA 0: level ls restricted from the last strip level, then the levels
+    // below it and back up, in its own shared memory
+    if (me == 0u) {
+        const DLv U = dlv(sm, D, lc, ls - 1u, me);
+        const SLv S = slv(sm0, off, D, ls);
+        const int n = S.w * S.h;
+        for (int j = (int)threadIdx.x; j < n; j += (int)blockDim.x) {
+            const int cy = slvRow(S, j), cx = j - cy * S.w;
+            dl_restricted(D, w, ls, U, cx, cy, me, &S.px[j], &S.py[j], &S.rx[j], &S.ry[j], &S.rho[j]);
+        }
+        __syncthreads();
+        coarseCore(D, w, ls, sm0, off);
+    }
+    cl.sync();
+    // up the strip levels: prolong from the level below (CTA 0's or a strip
+    // level), then both colours
+    for (int l = (int)ls - 1; l >= (int)lc; l--) {
+        const DLv A = dlv(sm, D, lc, (uint32_t)l, me);
+        const int n = (A.r1 - A.r0) * A.w;
+        if (l + 1 == (int)ls) {
+            // CTA 0's level ls, at offset 0 of its levels there
+            const int lw = (int)D.level_w[ls], lh = (int)D.level_h[ls];
+            const int nl = lw * lh;
+            const float* b0 = cl.map_shared_rank(sm0, 0u);
+            for (int j = (int)threadIdx.x; j < n; j += (int)blockDim.x) {
+                if (A.a(A_RHO)[j] <= 0.0f) continue;
+                int x, y;
+                dlCell(A, j, &x, &y);
+                const V2 e = prolongedFrom(b0 + 4 * nl, b0, b0 + nl, lw, lh, x, y);
+                A.a(A_PX)[j] = A.a(A_PX)[j] + e.x;
+                A.a(A_PY)[j] = A.a(A_PY)[j] + e.y;
+            }
+        } else {
+            const DLv U = dlv(sm, D, lc, (uint32_t)l + 1u, me);
+            for (int j = (int)threadIdx.x; j < n; j += (int)blockDim.x) {
+                if (A.a(A_RHO)[j] <= 0.0f) continue;
+                int x, y;
+                dlCell(A, j, &x, &y);
+                const V2 e = dl_prolonged(U, x, y, me);
+                A.a(A_PX)[j] = A.a(A_PX)[j] + e.x;
+                A.a(A_PY)[j] = A.a(A_PY)[j] + e.y;
+            }
+        }
+        cl.sync();
+        dl_sweep(A, (uint32_t)l, 0, SMOOTH_OMEGA, me);
+        cl.sync();
+        dl_sweep(A, (uint32_t)l, 1, SMOOTH_OMEGA, me);
+        cl.sync();
+    }
+    // level lc's rows to its way-up potentials
+    {
+        const DLv A = dlv(sm, D, lc, lc, me);
+        const int n = (A.r1 - A.r0) * A.w;
+        auto* ox = upx<T>(F, lc);
+        auto* oy = upy<T>(F, lc);
+        for (int j = (int)threadIdx.x; j < n; j += (int)blockDim.x) {
+            const int g = A.r0 * A.w + j;
+            st(ox + g, A.a(A_PX)[j]);
+            st(oy + g, A.a(A_PY)[j]);
+        }
     }
 }
 
@@ -2250,6 +2623,11 @@ size_t fast_coarse_smem(const Dev& D, uint32_t lc) {
     return SLV_ARRAYS * n * sizeof(float);
 }
 
+size_t fast_cluster_smem(const Dev& D, uint32_t lc) {
+    if (lc < 1u || lc > D.levels || (size_t)D.level_w[lc] * D.level_h[lc] <= COARSE_CTA_CELLS) return 0;
+    return clusterFloats(D.level_w, D.level_h, lc, D.levels, nullptr) * sizeof(float);
+}
+
 void fast_zero_level0(const FastW& F, uint32_t cells, cudaStream_t s) { k_fZero<<<148 * 4, 256, 0, s>>>(F, cells); }
 
 void fast_zero_idle(const Batch& Bt, const BatchShape& S, cudaStream_t s) {
@@ -2344,7 +2722,24 @@ uint32_t fast_cycle_t(const Batch& Bt0, const BatchShape& S, const World* one, c
         mark(WIG_SLOT_F_RESTRICT, 1);
     }
     mark(WIG_SLOT_F_COARSE, 0);
-    LAUNCH_T(k_fCoarse, T, list_grid(S, L_ONE, 1), 1024, S.coarse_smem);
+    if (S.cluster && one) {
+        // one cluster of CLUSTER_CTAS CTAs
+        cudaLaunchConfig_t c = {};
+        c.gridDim = dim3(CLUSTER_CTAS);
+        c.blockDim = dim3(1024);
+        c.dynamicSmemBytes = S.coarse_smem;
+        c.stream = s;
+        cudaLaunchAttribute at[1];
+        at[0].id = cudaLaunchAttributeClusterDimension;
+        at[0].val.clusterDim.x = CLUSTER_CTAS;
+        at[0].val.clusterDim.y = 1;
+        at[0].val.clusterDim.z = 1;
+        c.attrs = at;
+        c.numAttrs = 1;
+        (void)cudaLaunchKernelEx(&c, k_fCoarseCluster<T>, Bt, WorldSrc<true>{*one});
+    } else {
+        LAUNCH_T(k_fCoarse, T, list_grid(S, L_ONE, 1), 1024, S.coarse_smem);
+    }
     mark(WIG_SLOT_F_COARSE, 1);
     for (uint32_t l = S.lc_max; l >= 1; l--) {
         if (S.max_items[L_SM + l - 1u] == 0u) continue;
@@ -2402,6 +2797,8 @@ cudaError_t fast_prepare_attributes(size_t smem) {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fCoarse<false, float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fCoarse<true, __half>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fCoarse<false, __half>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fCoarseCluster<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_fCoarseCluster<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize, b);
     return e;
 }
 

@@ -19,6 +19,9 @@ struct Fast : FastW {
 // The one-CTA coarse kernel holds levels of at most this many cells; CTA 0
 // of the persistent solve, of at most PERSISTENT_CTA_CELLS.
 constexpr uint32_t COARSE_CTA_CELLS = 4096;
+// A single world's coarse levels from a level of up to this many cells run
+// on a thread-block cluster (k_fCoarseCluster).
+constexpr uint32_t COARSE_CLUSTER_CELLS = 16384;
 
 // A world's first level of at most `cells` cells (its coarsest when none
 // above it is): where the coarse kernel takes over.
@@ -62,6 +65,10 @@ void fast_zero_level0(const FastW& F, uint32_t cells, cudaStream_t s);
 void fast_zero_idle(const Batch& Bt, const BatchShape& S, cudaStream_t s);
 // Shared memory of the coarse kernel for a world, and the kernel's limit set.
 size_t fast_coarse_smem(const Dev& D, uint32_t lc);
+// Shared memory a CTA of the cluster coarse kernel takes for a single world
+// from level lc; 0 when that kernel does not apply (level lc fits the one-CTA
+// kernel, or the world's coarsest level does not fit one CTA of the cluster).
+size_t fast_cluster_smem(const Dev& D, uint32_t lc);
 cudaError_t fast_prepare_attributes(size_t smem);
 // The persistent solve of one world: all iterations in one cooperative launch.
 size_t fast_solve_smem(const Fast& F);

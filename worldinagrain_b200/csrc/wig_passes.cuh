@@ -11,7 +11,8 @@ struct BatchShape {
     uint32_t worlds;
     uint32_t levels;       // deepest coarse level of any world
     uint32_t lc_max;       // deepest level any world restricts by itself
-    size_t coarse_smem;    // the coarse kernel's shared memory for the largest world
+    size_t coarse_smem;    // the coarse kernel's shared memory for the largest world (a CTA's, on a cluster)
+    uint32_t cluster;      // a single world's coarse levels on a thread-block cluster
     // launch shapes (wig_launch_knob): none changes a result
     uint32_t coarse_cells;  // the coarse kernel from a world's first level of at most this many cells
     uint32_t level_per_sm, cg_per_sm, relax_per_sm;

@@ -3,8 +3,10 @@
 A batch steps its worlds with one launch a pass; how those launches are
 shaped is the batch's choice (include/wig_batch.h, wig_launch_knob):
 
-- coarse_cells: from which level the one-CTA coarse kernel takes over a
-  world's V-cycle (the depth of its on-chip part);
+- coarse_cells: from which level the coarse kernel takes over a world's
+  V-cycle (the depth of its on-chip part; above 4096, a single world's on a
+  cluster of CTAs, a value a batch of several worlds refuses and the tuner
+  leaves out);
 - level_per_sm, cg_per_sm, relax_per_sm: the CTAs a multiprocessor of the
   level tile kernels, the CG kernels and the fine relaxation.
 
@@ -22,8 +24,10 @@ candidate's cost is taken over both of its steps: a drift that is linear
 over the knob's steps weighs the same on every candidate.
 """
 
+from .fluid import WigError
+
 KNOBS = (
-    ("coarse_cells", (4096, 2048, 1024, 512), ("F_RESTRICT", "F_PROLONG", "F_COARSE")),
+    ("coarse_cells", (16384, 4096, 2048, 1024, 512), ("F_RESTRICT", "F_PROLONG", "F_COARSE")),
     ("level_per_sm", (4, 8, 16, 32), ("F_RESTRICT", "F_PROLONG")),
     ("cg_per_sm", (2, 4, 8, 16, 32), ("F_RHO_BETA", "F_APPLY_ALPHA", "F_UPDATE")),
     ("relax_per_sm", (16, 32, 64), ("F_RELAX",)),
@@ -55,9 +59,18 @@ def autotune(batch, step, knobs=KNOBS, passes=2):
         keep = batch.get_launch(name)
         ms = {v: 0.0 for v in candidates}
         its = {v: 0 for v in candidates}
+        refused = set()
         for p in range(passes):
             for v in (candidates if p % 2 == 0 else tuple(reversed(candidates))):
-                batch.set_launch(name, v)
+                if v in refused:
+                    continue
+                try:
+                    batch.set_launch(name, v)
+                except WigError:
+                    # out of this batch's range (coarse cells above 4096 on
+                    # more than one world): no cost
+                    refused.add(v)
+                    continue
                 t, n = slot_time(step(), slots)
                 ms[v] += t
                 its[v] += n
