@@ -435,66 +435,87 @@ __global__ void k_syncSeed(Batch Bt) {
   }
 }
 
-// compact (fluid.wgsl:896-921): one CTA of 1024 threads, a contiguous run of
-// blocks each, so the lists come out in block-index order.
+// The marks of block b's 3x3 neighbourhood (OR of the blocks inside the world).
+__device__ __forceinline__ uint32_t marksAround(const W& w, I2 b) {
+    uint32_t m[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) {
+        const I2 o{b.x + k % 3 - 1, b.y + k / 3 - 1};
+        m[k] = w.inBlocks(o) ? w.D.blocks[w.blockIndex(o)] : 0u;
+    }
+    uint32_t marks = 0;
+#pragma unroll
+    for (int k = 0; k < 9; k++) marks |= m[k];
+    return marks;
+}
+
+// compact (fluid.wgsl:896-921): one 1024-thread CTA a world, each thread a
+// run of consecutive blocks, so the lists come out in block-index order.  The first pass reads every block's marks and
+// state (four blocks' loads issued together) and keeps what it found, a bit
+// a block, for the second (runs of up to 64 blocks; a longer run reads them
+// again), which writes the states and the lists in block order after the
+// scan of the runs' counts.
 __global__ void __launch_bounds__(1024) k_compact(Batch Bt) {
     __shared__ WorldCopy wc_;
     worldCopyInit(wc_);
-  __shared__ uint32_t sa[1024], sr[1024];
-  FOR_ITEMS(Bt, L_ONE_ALL, it) {
-    ITEM_WORLD_C(Bt, it, D, w, unused_);
-    (void)unused_;
-    const uint32_t per = (D.B + 1023u) / 1024u;
-    const uint32_t lo = min(threadIdx.x * per, D.B), hi = min(lo + per, D.B);
-    uint32_t na = 0, nr = 0;
-    for (uint32_t n = lo; n < hi; n++) {
-        I2 b = w.blockAt(n);
-        uint32_t marks = 0;
-        for (int y = -1; y <= 1; y++)
-            for (int x = -1; x <= 1; x++) {
-                I2 o{b.x + x, b.y + y};
-                if (w.inBlocks(o)) marks |= D.blocks[w.blockIndex(o)];
-            }
-        bool liquid = (marks & (MARK_LIQUID | MARK_REGION)) != 0u;
-        bool was = (D.blocks[w.stateSlot(n)] & ACTIVE) != 0u;
-        na += liquid ? 1u : 0u;
-        nr += (!liquid && was) ? 1u : 0u;
-    }
-    sa[threadIdx.x] = na;
-    sr[threadIdx.x] = nr;
-    __syncthreads();
-    for (uint32_t o = 1; o < 1024u; o <<= 1) {
-        uint32_t a = threadIdx.x >= o ? sa[threadIdx.x - o] : 0u;
-        uint32_t r = threadIdx.x >= o ? sr[threadIdx.x - o] : 0u;
+    __shared__ uint32_t sa[1024], sr[1024];
+    FOR_ITEMS(Bt, L_ONE_ALL, it) {
+        ITEM_WORLD_C(Bt, it, D, w, unused_);
+        (void)unused_;
+        const uint32_t per = (D.B + 1023u) / 1024u;
+        const uint32_t lo = min(threadIdx.x * per, D.B), hi = min(lo + per, D.B);
+        const bool keep = per <= 64u;
+        uint64_t liq = 0, nea = 0, wasm = 0;
+        uint32_t na = 0, nr = 0;
+#pragma unroll 4
+        for (uint32_t n = lo; n < hi; n++) {
+            const uint32_t marks = marksAround(w, w.blockAt(n));
+            const bool liquid = (marks & (MARK_LIQUID | MARK_REGION)) != 0u;
+            const bool was = (D.blocks[w.stateSlot(n)] & ACTIVE) != 0u;
+            const uint64_t bit = 1ull << ((n - lo) & 63u);
+            if (liquid) liq |= bit;
+            if ((marks & MARK_LIQUID) != 0u) nea |= bit;
+            if (was) wasm |= bit;
+            na += liquid ? 1u : 0u;
+            nr += (!liquid && was) ? 1u : 0u;
+        }
+        sa[threadIdx.x] = na;
+        sr[threadIdx.x] = nr;
         __syncthreads();
-        sa[threadIdx.x] += a;
-        sr[threadIdx.x] += r;
+        for (uint32_t o = 1; o < 1024u; o <<= 1) {
+            uint32_t a = threadIdx.x >= o ? sa[threadIdx.x - o] : 0u;
+            uint32_t r = threadIdx.x >= o ? sr[threadIdx.x - o] : 0u;
+            __syncthreads();
+            sa[threadIdx.x] += a;
+            sr[threadIdx.x] += r;
+            __syncthreads();
+        }
+        uint32_t ai = sa[threadIdx.x] - na, ri = sr[threadIdx.x] - nr;
+        // All states are read above before any is written below.
+        __syncthreads();
+        for (uint32_t n = lo; n < hi; n++) {
+            bool liquid, near, was;
+            if (keep) {
+                const uint64_t bit = 1ull << (n - lo);
+                liquid = (liq & bit) != 0u;
+                near = (nea & bit) != 0u;
+                was = (wasm & bit) != 0u;
+            } else {
+                const uint32_t marks = marksAround(w, w.blockAt(n));
+                liquid = (marks & (MARK_LIQUID | MARK_REGION)) != 0u;
+                near = (marks & MARK_LIQUID) != 0u;
+                was = (D.blocks[w.stateSlot(n)] & ACTIVE) != 0u;
+            }
+            D.blocks[w.stateSlot(n)] = (liquid ? ACTIVE : 0u) | (near ? NEAR_LIQUID : 0u);
+            if (liquid) D.blocks[w.activeSlot(ai++)] = n;
+            else if (was) D.blocks[w.retiredSlot(ri++)] = n;
+        }
+        if (threadIdx.x == 1023u) {
+            D.blocks[w.countSlot(COUNT_ACTIVE)] = sa[1023];
+            D.blocks[w.countSlot(COUNT_RETIRED)] = sr[1023];
+        }
         __syncthreads();
     }
-    uint32_t ai = sa[threadIdx.x] - na, ri = sr[threadIdx.x] - nr;
-    // All states are read above before any is written below.
-    __syncthreads();
-    for (uint32_t n = lo; n < hi; n++) {
-        I2 b = w.blockAt(n);
-        uint32_t marks = 0;
-        for (int y = -1; y <= 1; y++)
-            for (int x = -1; x <= 1; x++) {
-                I2 o{b.x + x, b.y + y};
-                if (w.inBlocks(o)) marks |= D.blocks[w.blockIndex(o)];
-            }
-        bool near = (marks & MARK_LIQUID) != 0u;
-        bool liquid = (marks & (MARK_LIQUID | MARK_REGION)) != 0u;
-        bool was = (D.blocks[w.stateSlot(n)] & ACTIVE) != 0u;
-        D.blocks[w.stateSlot(n)] = (liquid ? ACTIVE : 0u) | (near ? NEAR_LIQUID : 0u);
-        if (liquid) D.blocks[w.activeSlot(ai++)] = n;
-        else if (was) D.blocks[w.retiredSlot(ri++)] = n;
-    }
-    if (threadIdx.x == 1023u) {
-        D.blocks[w.countSlot(COUNT_ACTIVE)] = sa[1023];
-        D.blocks[w.countSlot(COUNT_RETIRED)] = sr[1023];
-    }
-    __syncthreads();
-  }
 }
 
 // retire (fluid.wgsl:924-951)
@@ -769,13 +790,40 @@ __global__ void k_sealAnchor(Batch Bt) {
     }
 }
 
-// columnWeight (fluid.wgsl:1566-1575)
+// columnWeight (fluid.wgsl:1566-1575): the cells with particles straight
+// above p, counted up to the first without (at most COLUMN_MOST).  The
+// column is read COLUMN_RUN cells at a time, their type and count words
+// loaded together; each cell's countAt then follows from those words (the
+// full test only for a gas cell, which may be a bubble), and the cells are
+// taken in order, as the walk takes them.
+constexpr int COLUMN_RUN = 8;
 __device__ float columnWeight(const W& w, I2 p, float density) {
     int over = 0;
-    I2 q{p.x, p.y - 1};
-    while (over < COLUMN_MOST && countAt(w, q) > 0) {
-        over += 1;
-        q.y -= 1;
+    int y = p.y - 1;
+    bool more = true;
+    while (more && over < COLUMN_MOST) {
+        uint32_t t[COLUMN_RUN], n[COLUMN_RUN];
+        bool in[COLUMN_RUN];
+#pragma unroll
+        for (int k = 0; k < COLUMN_RUN; k++) {
+            const I2 q{p.x, y - k};
+            in[k] = w.inWorld(q);
+            const uint32_t i = in[k] ? w.cellIndex(q) : 0u;
+            t[k] = w.cellType(i);
+            n[k] = w.gw(i, G_COUNT);
+        }
+#pragma unroll
+        for (int k = 0; k < COLUMN_RUN; k++) {
+            int m = -1;
+            if (in[k]) {
+                const uint32_t kind = w.kindOf(t[k]);
+                if (kind == WIG_KIND_GAS) m = countAt(w, I2{p.x, y - k});
+                else if (kind != WIG_KIND_SOLID && kind != WIG_KIND_POWDER) m = (int32_t)n[k];
+            }
+            if (more && over < COLUMN_MOST && m > 0) over += 1;
+            else more = false;
+        }
+        y -= COLUMN_RUN;
     }
     return density * w.D.st->P.earth_g * ((float)over + 0.5f);
 }
