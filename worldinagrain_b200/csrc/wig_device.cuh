@@ -151,6 +151,27 @@ __device__ __forceinline__ float clampf(float x, float lo, float hi) { return fm
 __device__ __forceinline__ float mixf(float a, float b, float t) { return a * (1.0f - t) + b * t; }
 __device__ __forceinline__ float len2(float x, float y) { return __fsqrt_rn(x * x + y * y); }
 
+// a / d rounded to float (IEEE, round to nearest even) for a divisor d that
+// divides many times: quotBy(a, recipOf(d)) is a times the FP64 reciprocal
+// of d, rounded to float.  Why it is the quotient's bits:
+// - recipOf(d) = (1/d)(1 + e1) and the FP64 product (a/d)(1 + e1)(1 + e2),
+//   |e1|, |e2| <= 2^-53: within 2^-51.9 of a/d, relative.
+// - With a = A 2^i and d = D 2^k (A, D < 2^24 integers), a float rounding
+//   boundary m near a/d (a midpoint between two floats, the overflow
+//   threshold, or a subnormal midpoint) has a - d m a multiple of
+//   2^min(i, k + ulp exponent), so a/d is at least 2^-49 from m, relative,
+//   or 2^-174 absolute below the normal range, and never on m (d m would
+//   need an odd factor above 2^24 that A lacks).
+// - So no boundary lies between a/d and the product: both round to the
+//   same float.  Zeros, infinities and NaNs follow IEEE's products as the
+//   quotient's special cases do (1/0 = inf, 0 inf = NaN, a / inf = a 0).
+// The method is this bound on the gap between a quotient of p-bit numbers
+// and the rounding points (the argument of double-rounding results for
+// division with a 2p + 2-bit intermediate format), checked in the tests
+// against the GPU's and the host's IEEE division on random bit patterns.
+__device__ __forceinline__ double recipOf(float d) { return 1.0 / (double)d; }
+__device__ __forceinline__ float quotBy(float a, double rd) { return __double2float_rn((double)a * rd); }
+
 __device__ __forceinline__ float f16_value(uint32_t h) { return __half2float(__ushort_as_half((unsigned short)h)); }
 __device__ __forceinline__ uint32_t pack2x16(float a, float b) {
     return (uint32_t)__half_as_ushort(__float2half_rn(a)) | ((uint32_t)__half_as_ushort(__float2half_rn(b)) << 16);

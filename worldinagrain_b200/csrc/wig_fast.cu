@@ -1161,6 +1161,56 @@ __device__ void slv_smooth(const SLv& V, uint32_t l, int tid, int nt) {
     }
 }
 
+// A coarsest-level cell of the solve, held in registers: its index, its
+// four neighbours (clamped, nbr), their coefficients, the diagonal's FP64
+// reciprocal (quotBy: the 80 sweeps' divisions by it), h^2 times its
+// right-hand sides, and whether it is updated (a liquid cell with a
+// positive diagonal, j < n).
+struct SolveCell {
+    uint32_t j, nb[4];
+    float b[4], dg, hx, hy;
+    double rd;
+    int color;
+    bool mine;
+};
+__device__ __forceinline__ SolveCell solveCell(const SLv& V, int j, int n, float h2) {
+    SolveCell c;
+    const int cy = slvRow(V, j), cx = j - cy * V.w;
+    c.j = (uint32_t)j;
+    c.color = (cx + cy) & 1;
+    float r0 = -1.0f;
+    c.dg = 0.0f;
+    c.hx = 0.0f;
+    c.hy = 0.0f;
+#pragma unroll
+    for (int d = 0; d < 4; d++) {
+        c.b[d] = 0.0f;
+        c.nb[d] = 0u;
+    }
+    if (j < n) {
+        r0 = V.rho[j];
+        c.hx = h2 * V.rx[j];
+        c.hy = h2 * V.ry[j];
+        c.b[0] = V.b0[j]; c.b[1] = V.b1[j]; c.b[2] = V.b2[j]; c.b[3] = V.b3[j];
+#pragma unroll
+        for (int d = 0; d < 4; d++) c.nb[d] = nbr((uint32_t)j, cx, cy, V.w, V.h, d);
+        c.dg = (((0.0f + c.b[0]) + c.b[1]) + c.b[2]) + c.b[3];
+    }
+    c.mine = j < n && r0 > 0.0f && c.dg > 0.0f;
+    c.rd = recipOf(c.dg);
+    return c;
+}
+// One SOR update (omega 1.8) of a solve cell from its neighbours' potentials.
+__device__ __forceinline__ void solveUpdate(const SLv& V, const SolveCell& c) {
+    if (!c.mine) return;
+    float* px = V.px;
+    float* py = V.py;
+    float sx = c.b[0] * px[c.nb[0]] + c.b[1] * px[c.nb[1]] + c.b[2] * px[c.nb[2]] + c.b[3] * px[c.nb[3]];
+    float sy = c.b[0] * py[c.nb[0]] + c.b[1] * py[c.nb[1]] + c.b[2] * py[c.nb[2]] + c.b[3] * py[c.nb[3]];
+    px[c.j] = mixf(px[c.j], quotBy(sx - c.hx, c.rd), OMEGA);
+    py[c.j] = mixf(py[c.j], quotBy(sy - c.hy, c.rd), OMEGA);
+}
+
 // The levels from lc (in sm from offsets off[]: just loaded, or restricted
 // already) down to the coarsest and back up to lc: each level's
 // coefficients worked out once its densities are in place, smoothRed/Black,
@@ -1218,43 +1268,33 @@ __device__ void coarseCore(const Dev& D, const W& w, uint32_t lc, float* sm, con
         __syncthreads();
         if (l < L) slv_smooth(V, l, tid, nt);
     }
-    // solve: the coarsest level.  When its cells fit the CTA, a cell a thread
-    // of the first warps, the coefficients held in registers across the
-    // sweeps and only those warps synchronised (a named barrier over nsolve
-    // <= blockDim threads); else a thread per cell of the swept colour, the
-    // CTA synchronised.
+    // solve: the coarsest level.  When its cells fit the CTA, thread k of the
+    // first warps holds cells 2k and 2k + 1, one of each colour (in a row, or
+    // across a row's end when the width is odd), their coefficients in
+    // registers across the sweeps: every thread of those warps updates a
+    // cell each sweep, and only they are synchronised (a named barrier over
+    // npair <= blockDim threads); else a thread per cell of the swept
+    // colour, the CTA synchronised.
     {
         const SLv V = slv(sm, off, D, L);
         const int n = min(V.w * V.h, (int)WIG_MG_COARSEST);
         const float h2 = (float)(1u << (2u * L));
-        const uint32_t nsolve = (uint32_t)((n + 31) & ~31);
-        if (nsolve <= (uint32_t)nt) {
-            if (tid < (int)nsolve) {
-                const int j = tid;
-                const int cx = j % V.w, cy = j / V.w;
-                float b[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-                uint32_t nb[4] = {0u, 0u, 0u, 0u};
-                float dg = 0.0f, r0 = -1.0f, hx = 0.0f, hy = 0.0f;
-                if (j < n) {
-                    r0 = V.rho[j];
-                    hx = h2 * V.rx[j];
-                    hy = h2 * V.ry[j];
-                    b[0] = V.b0[j]; b[1] = V.b1[j]; b[2] = V.b2[j]; b[3] = V.b3[j];
-                    for (int d = 0; d < 4; d++) nb[d] = nbr((uint32_t)j, cx, cy, V.w, V.h, d);
-                    dg = (((0.0f + b[0]) + b[1]) + b[2]) + b[3];
+        const int pairs = (n + 1) / 2;
+        const uint32_t npair = (uint32_t)((pairs + 31) & ~31);
+        if (npair <= (uint32_t)nt) {
+            if (tid < (int)npair) {
+                SolveCell c0 = solveCell(V, 2 * tid, n, h2), c1 = solveCell(V, 2 * tid + 1, n, h2);
+                // c0 the colour-0 cell, c1 the colour-1 one
+                if (c0.color != 0) {
+                    const SolveCell t = c0;
+                    c0 = c1;
+                    c1 = t;
                 }
-                const bool mine = j < n && r0 > 0.0f && dg > 0.0f;
-                const int color = (cx + cy) & 1;
-                float* px = V.px;
-                float* py = V.py;
-                for (int s = 0; s < 2 * COARSE_SWEEPS; s++) {
-                    if (mine && color == (s & 1)) {
-                        float sx = b[0] * px[nb[0]] + b[1] * px[nb[1]] + b[2] * px[nb[2]] + b[3] * px[nb[3]];
-                        float sy = b[0] * py[nb[0]] + b[1] * py[nb[1]] + b[2] * py[nb[2]] + b[3] * py[nb[3]];
-                        px[j] = mixf(px[j], (sx - hx) / dg, OMEGA);
-                        py[j] = mixf(py[j], (sy - hy) / dg, OMEGA);
-                    }
-                    barSub(nsolve);
+                for (int s = 0; s < COARSE_SWEEPS; s++) {
+                    solveUpdate(V, c0);
+                    barSub(npair);
+                    solveUpdate(V, c1);
+                    barSub(npair);
                 }
             }
         } else {
