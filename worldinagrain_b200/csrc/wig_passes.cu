@@ -704,15 +704,21 @@ __device__ __forceinline__ void gatherWarp(const Dev& D, const W& w, uint32_t k,
     }
     const int x0 = __reduce_min_sync(0xffffffffu, lx), y0 = __reduce_min_sync(0xffffffffu, ly);
     const int x1 = __reduce_max_sync(0xffffffffu, hx), y1 = __reduce_max_sync(0xffffffffu, hy);
-    if (x1 - x0 > GWX || y1 - y0 > GWY) {  // (warp-uniform; none here: x1 < x0)
+    if (x1 - x0 > GWX || y1 - y0 > GWY) {  // (warp-uniform)
         if (has) gatherTo(w, DirectSink{w}, p);
         return;
     }
+    if (x1 < x0) return;  // no particle in the warp
     if (has) gatherTo(w, WinSink{win, x0, y0}, p);
     __syncwarp();
+    // the flush: the sites' box alone (every add fell inside it), a lane a
+    // window entry; each nonzero sum added to its global word and cleared
     const uint32_t lane = threadIdx.x & 31u;
-    for (uint32_t e = lane; e < (uint32_t)GWN; e += 32u) {
-        const I2 at{x0 + (int)(e % (GWX + 1)), y0 + (int)(e / (GWX + 1))};
+    const uint32_t bw = (uint32_t)(x1 - x0 + 1), nbox = bw * (uint32_t)(y1 - y0 + 1);
+    for (uint32_t q = lane; q < nbox; q += 32u) {
+        const uint32_t qy = q / bw, qx = q - qy * bw;
+        const uint32_t e = qy * (uint32_t)(GWX + 1) + qx;
+        const I2 at{x0 + (int)qx, y0 + (int)qy};
         for (int isU = 1; isU >= 0; isU--) {
             uint32_t(*arr)[GWN] = isU ? win.u : win.v;
             const uint32_t a = arr[0][e], b = arr[1][e];
