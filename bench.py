@@ -192,12 +192,13 @@ def level_stats(worlds, coarse_cells=4096):
 # algorithmic bytes: the capture's traffic scaled to the launch by the units
 # it processes.
 TRAFFIC_PER_ALG_BYTE = {
-    # k_fDown on level 1 of the disks 1024x1024 world: 22.8 MB read, 256 B
+    # k_fDown on level 1 of the disks 1024x1024 world: 23.9 MB read, none
     # written; 262,144 cells x 180 B
-    ("F_RESTRICT", False): ((23.902e6 + 3584) / (262144 * 180), "k_fDown, level 1 (512x512) of the disks 1024x1024 world"),
-    # k_fDown on levels 1-3 of one iteration of a 64-world batch, mixed form:
-    # 90.9 MB read and written; 151.8 MB algorithmic
-    ("F_RESTRICT", True): (90.86e6 / 151.8e6, "k_fDown, levels 1-3 of one iteration of a 64-world mixed batch"),
+    ("F_RESTRICT", False): (23.90272e6 / (262144 * 180), "k_fDown, level 1 (512x512) of the disks 1024x1024 world"),
+    # k_fDown on levels 1-3 of one iteration of a 64-world batch, mixed form,
+    # coarse cells 2048: 94.2 MB read and written; 153.3 MB algorithmic
+    # (122 B a level-1 cell, 82 below: 1,043,904, 257,952 and 58,312 cells)
+    ("F_RESTRICT", True): (94.191616e6 / 153.289936e6, "k_fDown, levels 1-3 of one iteration of a 64-world mixed batch"),
     # k_fRelax on the disks 1024x1024 world: 28.0 MB read, 0 written; 24.5 MB
     # algorithmic (the mixed form reads 12 B a cell less: its coefficients'
     # binary16 copies, no diagonal)

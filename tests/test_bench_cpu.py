@@ -61,7 +61,7 @@ def test_traffic_scales_the_captured_ratio():
     times this launch's algorithmic bytes; none for kernels not captured."""
     alg = 262144 * 180
     t, src = bench.traffic_of("F_RESTRICT", alg)
-    assert abs(t - (23.902e6 + 3584)) < 2 and "k_fDown" in src
+    assert abs(t - 23.90272e6) < 2 and "k_fDown" in src
     assert bench.traffic_of("F_RESTRICT", alg // 2)[0] == round(t / 2)
     assert bench.traffic_of("F_COARSE", 10 ** 6) == (None, None)
     assert bench.traffic_of("F_RELAX", 0) == (None, None)
