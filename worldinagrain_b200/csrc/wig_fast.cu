@@ -902,6 +902,7 @@ __device__ __forceinline__ void tileSmooth(LevelTile& t, int x0, int y0, int lw,
         tileSweepCell(t, ix, iy, cx, cy, lw, lh, h2);
     }
     __syncthreads();
+    if (threadIdx.x >= (unsigned)(LT * LT)) return;  // a wide CTA's threads past the tile's cells
     const int ix = (int)threadIdx.x % LT, iy = (int)threadIdx.x / LT, cx = x0 + ix, cy = y0 + iy;
     if (cx < lw && cy < lh && ((cx + cy) & 1) == 1) tileSweepCell(t, ix, iy, cx, cy, lw, lh, h2);
 }
@@ -912,8 +913,8 @@ __device__ __forceinline__ void tileSmooth(LevelTile& t, int x0, int y0, int lw,
 // from the densities (as the step's first iteration works and stores them,
 // and later ones read them back), stored by the tile's own cells on the
 // first iteration.
-template <bool ONE, class T>
-__global__ void __launch_bounds__(256, 4) k_fDown(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
+template <bool ONE, class T, int NT = 256>
+__global__ void __launch_bounds__(NT, NT == 256 ? 4 : 1) k_fDown(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
     __shared__ LevelTile t;
@@ -924,7 +925,8 @@ __global__ void __launch_bounds__(256, 4) k_fDown(Batch Bt, const __grid_constan
         const int x0 = (int)(tile % (uint32_t)tw) * LT, y0 = (int)(tile / (uint32_t)tw) * LT;
         if (l >= F.lc) {
             const int cx = x0 + (int)threadIdx.x % LT, cy = y0 + (int)threadIdx.x / LT;
-            if (cx < lw && cy < lh) restrictCell<T>(D, F, w, l, (uint32_t)(cy * lw + cx));
+            if (threadIdx.x < (unsigned)(LT * LT) && cx < lw && cy < lh)
+                restrictCell<T>(D, F, w, l, (uint32_t)(cy * lw + cx));
             continue;
         }
         const LRef<T> V = lref<T>(F, l);
@@ -974,7 +976,7 @@ __global__ void __launch_bounds__(256, 4) k_fDown(Batch Bt, const __grid_constan
         }
         __syncthreads();
         tileSmooth(t, x0, y0, lw, lh, (float)(1u << (2u * l)));
-        {
+        if (threadIdx.x < (unsigned)(LT * LT)) {
             const int ix = (int)threadIdx.x % LT, iy = (int)threadIdx.x / LT, cx = x0 + ix, cy = y0 + iy;
             if (cx < lw && cy < lh) {
                 const uint32_t j = (uint32_t)(cy * lw + cx);
@@ -995,8 +997,8 @@ __global__ void __launch_bounds__(256, 4) k_fDown(Batch Bt, const __grid_constan
 // coefficients.  The way down's potentials are read from px, py (the ring
 // too) and the results go to ux, uy, so no CTA reads a cell that another
 // writes in the same launch; level l + 1's results are its ux, uy.
-template <bool ONE, class T>
-__global__ void __launch_bounds__(256, 4) k_fUp(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
+template <bool ONE, class T, int NT = 256>
+__global__ void __launch_bounds__(NT, NT == 256 ? 4 : 1) k_fUp(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
     __shared__ LevelTile t;
@@ -1052,7 +1054,7 @@ __global__ void __launch_bounds__(256, 4) k_fUp(Batch Bt, const __grid_constant_
         }
         __syncthreads();
         tileSmooth(t, x0, y0, lw, lh, (float)(1u << (2u * l)));
-        {
+        if (threadIdx.x < (unsigned)(LT * LT)) {
             const int ix = (int)threadIdx.x % LT, iy = (int)threadIdx.x / LT, cx = x0 + ix, cy = y0 + iy;
             const int i = lsi(ix, iy);
             if (cx < lw && cy < lh && t.rho[i] > 0.0f) {
@@ -2756,9 +2758,16 @@ uint32_t fast_cycle_t(const Batch& Bt0, const BatchShape& S, const World* one, c
     // down: each world restricts its levels 1..lc by themselves and smooths
     // those above lc (a kernel a level), then its levels from lc are the
     // coarse kernel's; up: each level above lc prolonged and smoothed
+    // a single world's levels of at most one tile a multiprocessor: 512
+    // threads a tile, so each thread takes fewer of its cells in turn
+    auto wide = [&](uint32_t list) { return one != nullptr && S.max_items[list] <= 148u; };
     for (uint32_t l = 1; l <= S.lc_max; l++) {
         mark(WIG_SLOT_F_RESTRICT, 0);
-        LAUNCH_T(k_fDown, T, list_grid(S, L_RES + l - 1u, S.level_per_sm), 256, 0, l);
+        const uint32_t list = L_RES + l - 1u;
+        if (wide(list))
+            k_fDown<true, T, 512><<<list_grid(S, list, S.level_per_sm), 512, 0, s>>>(Bt, WorldSrc<true>{*one}, l);
+        else
+            LAUNCH_T(k_fDown, T, list_grid(S, list, S.level_per_sm), 256, 0, l);
         mark(WIG_SLOT_F_RESTRICT, 1);
     }
     mark(WIG_SLOT_F_COARSE, 0);
@@ -2784,7 +2793,11 @@ uint32_t fast_cycle_t(const Batch& Bt0, const BatchShape& S, const World* one, c
     for (uint32_t l = S.lc_max; l >= 1; l--) {
         if (S.max_items[L_SM + l - 1u] == 0u) continue;
         mark(WIG_SLOT_F_PROLONG, 0);
-        LAUNCH_T(k_fUp, T, list_grid(S, L_SM + l - 1u, S.level_per_sm), 256, 0, l);
+        const uint32_t list = L_SM + l - 1u;
+        if (wide(list))
+            k_fUp<true, T, 512><<<list_grid(S, list, S.level_per_sm), 512, 0, s>>>(Bt, WorldSrc<true>{*one}, l);
+        else
+            LAUNCH_T(k_fUp, T, list_grid(S, list, S.level_per_sm), 256, 0, l);
         mark(WIG_SLOT_F_PROLONG, 1);
     }
     mark(WIG_SLOT_F_PROLONG_FINE, 0);
