@@ -914,7 +914,7 @@ __device__ __forceinline__ void tileSmooth(LevelTile& t, int x0, int y0, int lw,
 // and later ones read them back), stored by the tile's own cells on the
 // first iteration.
 template <bool ONE, class T, int NT = 256>
-__global__ void __launch_bounds__(NT, NT == 256 ? 4 : 1) k_fDown(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
+__global__ void __launch_bounds__(NT, NT == 256 ? 4 : 2) k_fDown(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
     __shared__ LevelTile t;
@@ -998,7 +998,7 @@ __global__ void __launch_bounds__(NT, NT == 256 ? 4 : 1) k_fDown(Batch Bt, const
 // too) and the results go to ux, uy, so no CTA reads a cell that another
 // writes in the same launch; level l + 1's results are its ux, uy.
 template <bool ONE, class T, int NT = 256>
-__global__ void __launch_bounds__(NT, NT == 256 ? 4 : 1) k_fUp(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
+__global__ void __launch_bounds__(NT, NT == 256 ? 4 : 2) k_fUp(Batch Bt, const __grid_constant__ WorldSrc<ONE> src, uint32_t l) {
     __shared__ WorldCopy wc_;
     if (!ONE) worldCopyInit(wc_);
     __shared__ LevelTile t;
@@ -2758,9 +2758,9 @@ uint32_t fast_cycle_t(const Batch& Bt0, const BatchShape& S, const World* one, c
     // down: each world restricts its levels 1..lc by themselves and smooths
     // those above lc (a kernel a level), then its levels from lc are the
     // coarse kernel's; up: each level above lc prolonged and smoothed
-    // a single world's levels of at most one tile a multiprocessor: 512
+    // a single world's levels of at most two tiles a multiprocessor: 512
     // threads a tile, so each thread takes fewer of its cells in turn
-    auto wide = [&](uint32_t list) { return one != nullptr && S.max_items[list] <= 148u; };
+    auto wide = [&](uint32_t list) { return one != nullptr && S.max_items[list] <= 2u * 148u; };
     for (uint32_t l = 1; l <= S.lc_max; l++) {
         mark(WIG_SLOT_F_RESTRICT, 0);
         const uint32_t list = L_RES + l - 1u;
