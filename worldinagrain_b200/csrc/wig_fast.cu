@@ -2683,6 +2683,12 @@ void fast_zero_idle(const Batch& Bt, const BatchShape& S, cudaStream_t s) {
         if (one) K<true><<<(grid), (block), (smem), s>>>(Bt, WorldSrc<true>{*one}, ##__VA_ARGS__); \
         else K<false><<<(grid), (block), (smem), s>>>(Bt, WorldSrc<false>{}, ##__VA_ARGS__);       \
     } while (0)
+// The same for a kernel over levels stored as T with N threads a CTA.
+#define LAUNCH_TN(K, T, N, grid, smem, ...)                                                            \
+    do {                                                                                               \
+        if (one) K<true, T, N><<<(grid), (N), (smem), s>>>(Bt, WorldSrc<true>{*one}, ##__VA_ARGS__);    \
+        else K<false, T, N><<<(grid), (N), (smem), s>>>(Bt, WorldSrc<false>{}, ##__VA_ARGS__);          \
+    } while (0)
 // The same for a kernel over levels stored as T.
 #define LAUNCH_T(K, T, grid, block, smem, ...)                                                        \
     do {                                                                                              \
@@ -2765,7 +2771,7 @@ uint32_t fast_cycle_t(const Batch& Bt0, const BatchShape& S, const World* one, c
         mark(WIG_SLOT_F_RESTRICT, 0);
         const uint32_t list = L_RES + l - 1u;
         if (wide(list))
-            k_fDown<true, T, 512><<<list_grid(S, list, S.level_per_sm), 512, 0, s>>>(Bt, WorldSrc<true>{*one}, l);
+            LAUNCH_TN(k_fDown, T, 512, list_grid(S, list, S.level_per_sm), 0, l);
         else
             LAUNCH_T(k_fDown, T, list_grid(S, list, S.level_per_sm), 256, 0, l);
         mark(WIG_SLOT_F_RESTRICT, 1);
@@ -2795,7 +2801,7 @@ uint32_t fast_cycle_t(const Batch& Bt0, const BatchShape& S, const World* one, c
         mark(WIG_SLOT_F_PROLONG, 0);
         const uint32_t list = L_SM + l - 1u;
         if (wide(list))
-            k_fUp<true, T, 512><<<list_grid(S, list, S.level_per_sm), 512, 0, s>>>(Bt, WorldSrc<true>{*one}, l);
+            LAUNCH_TN(k_fUp, T, 512, list_grid(S, list, S.level_per_sm), 0, l);
         else
             LAUNCH_T(k_fUp, T, list_grid(S, list, S.level_per_sm), 256, 0, l);
         mark(WIG_SLOT_F_PROLONG, 1);
