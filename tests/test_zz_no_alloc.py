@@ -68,3 +68,25 @@ def test_noalloc_refuses_worlds_past_its_maximum():
     rc = f(C.byref(d), one, one, one, one, None)
     assert rc == -1
     assert b"at most 16384" in fluid.lib().wig_fluid_last_error()
+
+
+def test_noalloc_norm_at_its_maximum_world():
+    """A 1024x1024 world: 128 x 128 = 16384 blocks, exactly the static
+    scratch's size (WIG_NOALLOC_MAX_BLOCKS)."""
+    import torch
+    fluid, f = _entry()
+    world = W.disks_world(1024, 1024, seed=2)
+    assert world.L["block_count"] == 16384
+    g = fluid.LiquidStep(world, W.element_table())
+    out = torch.full((1,), -1.0, dtype=torch.float64, device="cuda")
+    d = world.desc()
+    g.step(params(world, 1), max_cycles=64, flags=abi.STEP_TOLERANCE | abi.STEP_F64_DOTS, tolerance=1e-6)
+    st = g.stats()
+    b = g.buffers()
+    rc = f(C.byref(d), b.field, b.blocks, b.cg, C.c_void_p(out.data_ptr()), None)
+    assert rc == 0, fluid.lib().wig_fluid_last_error()
+    torch.cuda.synchronize()
+    want = (st.rel_residual * st.b_norm) ** 2
+    assert want > 0.0
+    assert abs(float(out.item()) - want) <= REL * want
+    g.close()
