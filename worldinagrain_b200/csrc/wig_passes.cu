@@ -2024,7 +2024,12 @@ __global__ void k_advect(Batch Bt) {
 
 // ================================================================ sort
 
-// sortCount (fluid.wgsl:3700-3708)
+// sortCount (fluid.wgsl:3700-3708): each particle's slot among its cell's.
+// The lanes of a warp whose particles share a cell (parts is in cell order
+// from the last sort, so mostly neighbours) take their slots with one atomic
+// add by the lowest of them, each lane its rank among them past the base;
+// the slots within a cell are any order of 0..n-1, as the reference's
+// atomics give them.
 __device__ __forceinline__ void sortCountOne(const Dev& D, const W& w, uint32_t chunk) {
     uint32_t live = min(D.parts[0], D.cap);
     uint32_t k = chunk * blockDim.x + threadIdx.x;
@@ -2032,7 +2037,13 @@ __device__ __forceinline__ void sortCountOne(const Dev& D, const W& w, uint32_t 
     uint4* it = w.items(D.parts);
     uint4 mo = it[k];
     uint32_t i = w.cellIndex(w.cellOf(__uint_as_float(mo.x), __uint_as_float(mo.y)));
-    it[D.cap + k].w = atomicAdd(w.gwp(i, G_SORT), 1u);
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t peers = __match_any_sync(__activemask(), i);
+    const int leader = __ffs(peers) - 1;
+    uint32_t base = 0u;
+    if ((int)lane == leader) base = atomicAdd(w.gwp(i, G_SORT), (uint32_t)__popc(peers));
+    base = __shfl_sync(peers, base, leader);
+    it[D.cap + k].w = base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
 }
 __global__ void k_sortCount(Batch Bt) {
     __shared__ WorldCopy wc_;
