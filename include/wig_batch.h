@@ -116,8 +116,9 @@ int wig_batch_world_bytes_split(const wig_world_desc* d, uint64_t* persistent, u
  *   LEVEL_PER_SM, CG_PER_SM, RELAX_PER_SM: CTAs a multiprocessor (1 .. 64)
  *     of the level tile kernels, of the three CG kernels, of the fine
  *     relaxation.
- * Defaults: COARSE_CELLS 4096, LEVEL_PER_SM 8, CG_PER_SM 8 (4 for a batch of
- * one world, as every wig_fluid handle is), RELAX_PER_SM 16.
+ * Defaults: COARSE_CELLS 4096, LEVEL_PER_SM 8, CG_PER_SM 8, RELAX_PER_SM 16;
+ * for a batch of one world, as every wig_fluid handle is: COARSE_CELLS 2048,
+ * LEVEL_PER_SM 32, CG_PER_SM 4, RELAX_PER_SM 64.
  * No step of the batch may be in flight; the lanes' graphs are recaptured
  * at their next step. */
 enum wig_launch_knob {

@@ -112,6 +112,10 @@ def test_mixed_batch_matches_each_world_alone():
     for w in worlds:
         r = w.copy()
         h = fluid.LiquidStep(r, W.element_table())
+        # the mixed form's coarse kernel keeps its levels in FP32, the tile
+        # kernels store theirs in 16 bits: alone, the world starts its coarse
+        # kernel where the batch does (a batch's default, 4096 cells)
+        h.set_launch("coarse_cells", 4096)
         for s in range(1, 4):
             h.step(params(r, s), max_cycles=64, flags=MIXED, tolerance=1e-6)
         h.download()

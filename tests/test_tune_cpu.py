@@ -106,10 +106,24 @@ def test_a_refused_candidate_is_left_out():
 
 def test_the_profiled_steps_launch_floor_is_not_counted():
     """A candidate with fewer launches is not credited with the profiled
-    step's per-launch floor (the loop-start kernel's time a launch): 6
-    launches of 0.02 ms against 8 of 0.016 ms, floor 0.01 ms, cost 0.06
-    against 0.048 ms; counting the floor would pick the first."""
+    step's per-launch overhead (FLOOR_SHARE of the loop-start kernel's time
+    a launch): 6 launches of 0.02 ms against 8 of 0.016 ms, floor 0.005 ms
+    of the loop start's 0.01, cost 0.09 against 0.088 ms; counting the whole
+    time would pick the first."""
+    assert tune.FLOOR_SHARE == 0.5
     few = {"F_LOOP": (0.01, 1), "F_COARSE": (0.12, 6)}
     many = {"F_LOOP": (0.01, 1), "F_COARSE": (0.128, 8)}
-    assert abs(tune.cost(few, ("F_COARSE",)) - 0.06) < 1e-12
-    assert abs(tune.cost(many, ("F_COARSE",)) - 0.048) < 1e-12
+    assert abs(tune.cost(few, ("F_COARSE",)) - 0.09) < 1e-12
+    assert abs(tune.cost(many, ("F_COARSE",)) - 0.088) < 1e-12
+
+
+def test_the_current_shape_stays_unless_clearly_beaten():
+    """A candidate 2% cheaper than the batch's own shape does not replace it
+    (the profiled steps' spread is about 3%); one 5% cheaper does."""
+    name, cands, slots = tune.KNOBS[1]  # level_per_sm, current 8
+    for cheaper, want in ((0.98, 8), (0.95, cands[0])):
+        costs = {n: {v: 1.0 for v in c} for n, c, _ in tune.KNOBS}
+        costs[name][cands[0]] = cheaper
+        b = FakeBatch(costs)
+        shapes, _ = tune.autotune(b, b.step, knobs=(tune.KNOBS[1],))
+        assert shapes[name] == want

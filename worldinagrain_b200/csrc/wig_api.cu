@@ -432,14 +432,17 @@ int make_batch(const wig_world_desc* descs, uint32_t n, const wig_elem* elems, u
     wig::BatchShape& S = b->S;
     std::memset(&S, 0, sizeof(S));
     S.worlds = n;
-    S.coarse_cells = wig::COARSE_CTA_CELLS;
-    S.level_per_sm = 8;
-    // a single world's CG kernels run fastest with fewer CTAs, each taking
-    // more tiles and fewer of them counting into the world's last-tile
-    // counter (0.074 against 0.079 ms an iteration at 1024x1024, the
-    // autotuner's measurement); a batch's with more
-    S.cg_per_sm = n == 1 ? 4 : 8;
-    S.relax_per_sm = 16;
+    // a single world's defaults are the shapes measured fastest on the
+    // 1024x1024 world in its step graph (coarse kernel from 32x32, 32 CTAs a
+    // multiprocessor for the level kernels, 64 for the relaxation: 170.5
+    // Mcells/s against 168.8 from 64x64 and 166.8 from 16x16); its CG
+    // kernels run fastest with fewer CTAs, each taking more tiles and fewer
+    // of them counting into the world's last-tile counter.  A batch's are
+    // the autotuner's starting point.
+    S.coarse_cells = n == 1 ? 2048u : wig::COARSE_CTA_CELLS;
+    S.level_per_sm = n == 1 ? 32u : 8u;
+    S.cg_per_sm = n == 1 ? 4u : 8u;
+    S.relax_per_sm = n == 1 ? 64u : 16u;
     uint64_t most_units = 1, max_items[wig::L_COUNT] = {0};
     size_t scratch_total = 0;
     for (uint32_t k = 0; k < n; k++) {
