@@ -21,11 +21,11 @@
  *   binding 9  Level         -> (level, cycle) arguments of wig_fluid_dispatch
  *   binding 10 gravity       -> (not bound: Earth's pull P.earthG straight down)
  *   binding 11 airSource     -> (not bound)
- *   binding 12 bodyMotion    -> (not bound: no free bodies)
+ *   binding 12 bodyMotion    -> motion     (u32: the body table, wig_fluid_bind_bodies; optional)
  *   binding 13 occupants     -> (not bound: no people)
- *   binding 14 bodies        -> (not bound)
+ *   binding 14 bodies        -> (not bound: no swept stamps, so no body seams or cups)
  *   binding 15 fluidCg       -> cg         (vec4<f32>: per cell, per block, sums)
- *   binding 16 bodyPushes    -> (not bound)
+ *   binding 16 bodyPushes    -> pushes     (u32: WIG_BODY_PUSH_WORDS per body; optional)
  *
  * All entry points return 0 on success and a negative WIG_E* code on error;
  * wig_fluid_last_error() gives a one-line description of the last error on
@@ -85,6 +85,44 @@ extern "C" {
 #define WIG_ELEM_SAND 2u
 #define WIG_ELEM_WATER 3u
 #define WIG_MAX_ELEMS 256u
+#define WIG_NO_ELEM 255u      /* js/shared.js:113 */
+#define WIG_FL_LOOSE 8u       /* a cell's flag: moving with a free body (shaders/common.wgsl:160) */
+
+/* Free bodies (js/shared.js:294-333).  The body table `motion` (binding 12)
+ * holds MAX_BODIES list words, then MAX_BODIES slots of BODY_TABLE_WORDS
+ * (word WIG_BW_* of body b at MAX_BODIES + b * BODY_TABLE_WORDS + k), the
+ * contacts, and BODY_LIQUID_WORDS a body of what the liquid did to it this
+ * step (velocity x, y and spin in RIGID_FIX fixed point, and LIQUID_WET).
+ * `pushes` (binding 16) is the solve's scratch: BODY_PUSH_SETS sets a body
+ * of a force x, y and a torque, each an exact sum in two words. */
+#define WIG_MAX_BODIES 1024u
+#define WIG_BODY_TABLE_WORDS 116u
+#define WIG_BODY_CONTACTS 16384u
+#define WIG_BODY_CONTACT_WORDS 12u
+#define WIG_BODY_LIQUID_WORDS 4u
+#define WIG_BODY_PUSH_SETS 6u
+#define WIG_BODY_PUSH_WORDS (6u * WIG_BODY_PUSH_SETS)
+#define WIG_BODY_MOTION_WORDS (WIG_MAX_BODIES * (1u + WIG_BODY_TABLE_WORDS) + \
+                               WIG_BODY_CONTACTS * WIG_BODY_CONTACT_WORDS + WIG_MAX_BODIES * WIG_BODY_LIQUID_WORDS)
+#define WIG_BODY_LIQUID_BASE (WIG_MAX_BODIES * (1u + WIG_BODY_TABLE_WORDS) + WIG_BODY_CONTACTS * WIG_BODY_CONTACT_WORDS)
+#define WIG_BW_POS 0u            /* vec2 f32: the centre of mass, cells */
+#define WIG_BW_VEL 3u            /* vec2 f32: cells/step */
+#define WIG_BW_SPIN 5u           /* f32: radians/step */
+#define WIG_BW_MASS 6u
+#define WIG_BW_INERTIA 7u
+#define WIG_BW_CELLS 13u         /* u32 */
+#define WIG_BW_FLAGS 18u         /* u32: WIG_BF_* */
+#define WIG_BW_SUBCELL 25u       /* 2 x f16: the pose's offset from the stamp, cells */
+#define WIG_BW_CARGO 105u
+#define WIG_BW_CARGO_INERTIA 106u
+#define WIG_BW_MOBILITY 108u     /* 6 f32: a symmetric 3 x 3 (the contacts' give) */
+#define WIG_BW_MOBILITY_AT 114u  /* u32: the step MOBILITY was worked out */
+#define WIG_BF_ALIVE 1u
+#define WIG_BF_NEW 2u
+#define WIG_BF_HELD 32u
+#define WIG_BF_WET 64u
+#define WIG_RIGID_FIX 16777216.0f
+#define WIG_LIQUID_WET 0x80000000u
 
 /* Params (shaders/common.wgsl:5-40), 80 bytes, written per step by the host
  * (js/sim.js:1975-1995).  Field for field the reference's uniform. */
@@ -130,7 +168,9 @@ typedef struct wig_elem {
     float sol_density;
     uint32_t flags;     /* F_* (js/elements.js:10-21); F_IMPACT = 32 */
     float wetting;
-    float pad[2];
+    uint32_t break_to;  /* breakTo (js/elements.js:160): WIG_NO_ELEM for none; a loose solid
+                           with one is a free body's cell (fluid.wgsl:1233-1248) */
+    float pad;
 } wig_elem;
 
 /* A world: its size and the liquid's particles per cell (LIQUID_PER_CELL,
@@ -254,6 +294,15 @@ enum wig_pass {
     WIG_PASS_RASTER_CLAIMS,       /* fluid.wgsl:3928 */
     WIG_PASS_RASTER,              /* fluid.wgsl:3983 */
     WIG_PASS_UNPAINT,             /* fluid.wgsl:4163 */
+    WIG_PASS_BODY_START,          /* fluid.wgsl:3079 */
+    WIG_PASS_BODY_LOADS,          /* fluid.wgsl:3094 */
+    WIG_PASS_BODY_DRAG,           /* fluid.wgsl:3149 */
+    WIG_PASS_BODY_FACES,          /* fluid.wgsl:3180 */
+    WIG_PASS_CG_BODY_X,           /* fluid.wgsl:2820 */
+    WIG_PASS_CG_BODY_P,           /* fluid.wgsl:2828 */
+    WIG_PASS_CG_BODY_F,           /* fluid.wgsl:2840 */
+    WIG_PASS_RIGIDIFY,            /* fluid.wgsl:3034 */
+    WIG_PASS_BODY_PUSH,           /* fluid.wgsl:3205 */
     WIG_PASS_COUNT
 };
 
@@ -270,6 +319,17 @@ int wig_fluid_create(const wig_world_desc* d, const wig_elem* elems, uint32_t n_
  * buffers (null fields are allocated by the handle and zeroed, as
  * js/sim.js:1259 `clear` leaves them). */
 int wig_fluid_bind(wig_fluid* h, const wig_fluid_buffers* b);
+
+/* Binds the free bodies' buffers (bindings 12 and 16, js/sim.js:1159): the
+ * body table `motion` (WIG_BODY_MOTION_WORDS u32, caller-owned, read for
+ * the bodies' poses and written in its liquid words) and `pushes`
+ * (WIG_MAX_BODIES * WIG_BODY_PUSH_WORDS u32, caller-owned scratch).  With
+ * them bound, each step couples the bodies into the solve (A = L + J^T M^-1 J,
+ * fluid.wgsl:1181-1470, :2819-2845, :2949-3218) and runs in the plain form
+ * (a kernel per reference pass), whatever the form flags ask; the body
+ * table's swept stamps (binding 14) are not read, so no body has seams or
+ * a cup.  Both null unbinds them.  Single-world handles only. */
+int wig_fluid_bind_bodies(wig_fluid* h, void* motion, void* pushes);
 
 /* The bound (or allocated) device buffers. */
 int wig_fluid_buffers_of(wig_fluid* h, wig_fluid_buffers* out);

@@ -42,6 +42,7 @@ def lib():
                                        C.c_uint32, C.POINTER(abi.Buffers), C.c_void_p]
         L.wo_true_residual.restype = C.c_double
         L.wo_sincos.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
+        L.wo_bind_bodies.argtypes = [C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -58,23 +59,42 @@ def _buffers(world):
 class Oracle:
     """Runs the oracle's passes and steps over a World's host buffers in place."""
 
-    def __init__(self, world, elems):
+    def __init__(self, world, elems, bodies=None):
+        """bodies: a world.Bodies whose table and push sums the passes read
+        and write in place (None: no free bodies)."""
         self.world = world
         self.elems = elems
+        self.bodies = bodies
         self.shifted = C.c_uint32(0)
+
+    def _bind(self):
+        if self.bodies is None:
+            lib().wo_bind_bodies(None, None)
+        else:
+            assert self.bodies.motion.flags["C_CONTIGUOUS"] and self.bodies.pushes.flags["C_CONTIGUOUS"]
+            lib().wo_bind_bodies(self.bodies.motion.ctypes.data, self.bodies.pushes.ctypes.data)
 
     def pass_(self, P, name, level=0, cycle=0):
         d = self.world.desc()
         b = _buffers(self.world)
-        rc = lib().wo_pass(C.byref(d), C.byref(P), self.elems, len(self.elems), C.byref(b), abi.PASS[name], level, cycle)
+        self._bind()
+        try:
+            rc = lib().wo_pass(C.byref(d), C.byref(P), self.elems, len(self.elems), C.byref(b), abi.PASS[name],
+                               level, cycle)
+        finally:
+            lib().wo_bind_bodies(None, None)
         assert rc == 0, rc
 
     def step(self, P, max_cycles=abi.FLUID_CYCLES, flags=0, tolerance=1e-6):
         d = self.world.desc()
         b = _buffers(self.world)
         st = abi.Stats()
-        rc = lib().wo_step(C.byref(d), C.byref(P), self.elems, len(self.elems), C.byref(b), max_cycles, flags,
-                           tolerance, C.byref(self.shifted), C.byref(st))
+        self._bind()
+        try:
+            rc = lib().wo_step(C.byref(d), C.byref(P), self.elems, len(self.elems), C.byref(b), max_cycles, flags,
+                               tolerance, C.byref(self.shifted), C.byref(st))
+        finally:
+            lib().wo_bind_bodies(None, None)
         assert rc == 0, rc
         return st
 

@@ -19,8 +19,9 @@
 //
 // Scope: the element subset AIR, WALL, WATER (and any element table given),
 // no air motion (binding 3 unbound: no air push in gather, no wind drag in
-// setFace), no free bodies (bindings 12, 14, 16 unbound: rigidAt, seamOf,
-// cupOf are NONE), no people (binding 13 unbound: isOccupant is false), and
+// setFace), free bodies only when their table and sums are bound (bindings
+// 12 and 16, wo_bind_bodies; else rigidAt and heldAt are NONE) and never
+// their swept stamps (binding 14 unbound: seamOf and cupOf are NONE), no people (binding 13 unbound: isOccupant is false), and
 // the Earth's pull alone (binding 10 unbound: pullAt = (0, P.earthG), down is
 // +y).  Surface tension's pass runs only when sim.js's surfaceTension() holds
 // (capillary length over dx >= 0.3 cells), which no config reaches.
@@ -162,6 +163,7 @@ void sincos_own(float a, float* s, float* c) {
 struct I2 { int x, y; };
 struct V2 { float x, y; };
 struct V4 { float x, y, z, w; };
+struct V3 { float x, y, z; };
 
 // Word fields (js/shared.js:79): type [0,8), aux [8,16), life [16,24),
 // shade [24,28), flags [28,32).
@@ -210,6 +212,8 @@ struct Ctx {
     float* field;
     uint32_t* blocks;
     float* cg;
+    uint32_t* motion = nullptr;   // binding 12, the body table (null: no free bodies)
+    uint32_t* pushes = nullptr;   // binding 16, the solve's sums of what it does to each body
     uint32_t level = 0, cycle = 0;
     uint32_t rng = 0;
     int W, H;
@@ -577,6 +581,221 @@ void forActiveCells(Ctx& X, Fn fn) {
     }
 }
 
+// ---------------------------------------------------------------- free bodies (fluid.wgsl:1181-1470)
+
+constexpr uint32_t MAX_BODIES = WIG_MAX_BODIES, BODY_TABLE_WORDS = WIG_BODY_TABLE_WORDS;
+constexpr uint32_t PUSH_P0 = 0, PUSH_X = 2, PUSH_F = 3, PUSH_SURFACE = 4, PUSH_DRAG = 5;
+constexpr float EXACT_COARSE = 16777216.0f, RIGID_FIX = WIG_RIGID_FIX;
+constexpr int SEEP_REACH = 128;
+
+uint32_t bodyWord(Ctx& X, uint32_t b, uint32_t k) { return X.motion[MAX_BODIES + b * BODY_TABLE_WORDS + k]; }
+float bodyF(Ctx& X, uint32_t b, uint32_t k) { return flt(bodyWord(X, b, k)); }
+V2 bodyV(Ctx& X, uint32_t b, uint32_t k) { return V2{bodyF(X, b, k), bodyF(X, b, k + 1u)}; }
+uint32_t liquidSlot(uint32_t b, uint32_t w) { return WIG_BODY_LIQUID_BASE + b * WIG_BODY_LIQUID_WORDS + w; }
+// alive, weighed and not just found (rigidBodyOf's, cupOf's test, fluid.wgsl:1243-1246)
+bool bodyInSolve(Ctx& X, uint32_t b) {
+    uint32_t flags = bodyWord(X, b, WIG_BW_FLAGS);
+    return !((flags & WIG_BF_ALIVE) == 0u || (flags & WIG_BF_NEW) != 0u || bodyF(X, b, WIG_BW_MASS) <= 0.0f);
+}
+// rigidBodyOf (fluid.wgsl:1233-1248)
+uint32_t rigidBodyOf(Ctx& X, const uint32_t* v) {
+    uint32_t t = wordType(v[0]);
+    if (!wordHas(v[0], WIG_FL_LOOSE) || X.elem(t).kind != WIG_KIND_SOLID || X.elem(t).break_to == WIG_NO_ELEM) return NONE;
+    float id = f16_value(v[3] & 0xffffu);
+    if (id < 0.0f || id >= (float)MAX_BODIES) return NONE;
+    uint32_t b = f2u(id);
+    return bodyInSolve(X, b) ? b : NONE;
+}
+float rigidMass(Ctx& X, uint32_t b) { return bodyF(X, b, WIG_BW_MASS) + bodyF(X, b, WIG_BW_CARGO); }
+float rigidInertia(Ctx& X, uint32_t b) { return bodyF(X, b, WIG_BW_INERTIA) + bodyF(X, b, WIG_BW_CARGO_INERTIA); }
+float bodyDensity(Ctx& X, uint32_t b) { return rigidMass(X, b) / wmax((float)bodyWord(X, b, WIG_BW_CELLS), 1.0f); }
+bool isHeld(Ctx& X, uint32_t b) { return (bodyWord(X, b, WIG_BW_FLAGS) & WIG_BF_HELD) != 0u; }
+// wetRegionAt (fluid.wgsl:592-595)
+bool wetRegionAt(Ctx& X, const uint32_t* v) {
+    if (!X.motion) return false;
+    uint32_t b = rigidBodyOf(X, v);
+    return b != NONE && (bodyWord(X, b, WIG_BW_FLAGS) & (WIG_BF_WET | WIG_BF_HELD)) == (WIG_BF_WET | WIG_BF_HELD);
+}
+// rigidAt, heldAt (fluid.wgsl:1422-1458): the body classify put in the drift's z
+uint32_t rigidAt(Ctx& X, I2 c) {
+    if (!X.motion || !X.inWorld(c)) return NONE;
+    float z = X.fv(2u * X.cellIndex(c) + 1u)[2];
+    uint32_t b = f2u(wmax(-z, 1.0f)) - 1u;
+    return (z < 0.0f && b < MAX_BODIES) ? b : NONE;
+}
+uint32_t heldAt(Ctx& X, I2 c) {
+    if (!X.motion || !X.inWorld(c)) return NONE;
+    float z = X.fv(2u * X.cellIndex(c) + 1u)[2];
+    uint32_t b = f2u(wmax(-z, 1.0f)) - 1u;
+    // (a slot past the table, from a drift word classify did not write, is none)
+    return (z < 0.0f && b >= MAX_BODIES && b < 2u * MAX_BODIES) ? b - MAX_BODIES : NONE;
+}
+
+// exactParts, exactCarry, exactValue (common.wgsl:1378-1412)
+void exactParts(float x, float scale, uint32_t* lo, uint32_t* hi) {
+    float s = rnd_even(clampf(x * scale, -9.2e18f, 9.2e18f));
+    if (std::fabs(s) < 2147483648.0f) {
+        int32_t v = f2i(s);
+        *lo = (uint32_t)v;
+        *hi = v < 0 ? 0xffffffffu : 0u;
+        return;
+    }
+    float h = std::floor(s / 4294967296.0f);
+    *lo = f2u(s - h * 4294967296.0f);
+    *hi = (uint32_t)f2i(h);
+}
+float exactValue(uint32_t lo, uint32_t hi, float scale) {
+    int32_t l = (int32_t)lo, h = (int32_t)hi;
+    if ((h == 0 && l >= 0) || (h == -1 && l < 0)) return (float)l / scale;
+    return ((float)h * 4294967296.0f + (float)lo) / scale;
+}
+// pushSlot, addPush, pushOf (fluid.wgsl:1318-1338)
+uint32_t pushSlot(uint32_t b, uint32_t which, uint32_t k) { return b * WIG_BODY_PUSH_WORDS + 6u * which + 2u * k; }
+void addPush(Ctx& X, uint32_t b, uint32_t which, V3 v) {
+    float c[3] = {v.x, v.y, v.z};
+    for (uint32_t k = 0; k < 3; k++) {
+        uint32_t lo, hi;
+        exactParts(c[k], EXACT_COARSE, &lo, &hi);
+        uint32_t at = pushSlot(b, which, k);
+        uint32_t old = X.pushes[at];
+        X.pushes[at] = old + lo;
+        X.pushes[at + 1u] += hi + (old + lo < old ? 1u : 0u);
+    }
+}
+V3 pushOf(Ctx& X, uint32_t b, uint32_t which) {
+    float c[3];
+    for (uint32_t k = 0; k < 3; k++) {
+        uint32_t at = pushSlot(b, which, k);
+        c[k] = exactValue(X.pushes[at], X.pushes[at + 1u], EXACT_COARSE);
+    }
+    return V3{c[0], c[1], c[2]};
+}
+// giveWay, pushChange, pushChangeFree (fluid.wgsl:1348-1372)
+V3 giveWay(Ctx& X, uint32_t b, V3 g) {
+    if (bodyWord(X, b, WIG_BW_MOBILITY_AT) != X.P->frame - 1u)
+        return V3{g.x / rigidMass(X, b), g.y / rigidMass(X, b), g.z / rigidInertia(X, b)};
+    float m[6];
+    for (uint32_t k = 0; k < 6; k++) m[k] = bodyF(X, b, WIG_BW_MOBILITY + k);
+    return V3{m[0] * g.x + m[1] * g.y + m[2] * g.z, m[1] * g.x + m[3] * g.y + m[4] * g.z,
+              m[2] * g.x + m[4] * g.y + m[5] * g.z};
+}
+V3 pushChange(Ctx& X, uint32_t b, uint32_t which) { return giveWay(X, b, pushOf(X, b, which)); }
+V3 pushChangeFree(Ctx& X, uint32_t b, uint32_t which) {
+    V3 g = pushOf(X, b, which);
+    return V3{g.x / rigidMass(X, b), g.y / rigidMass(X, b), g.z / rigidInertia(X, b)};
+}
+// bodyFaceJ (fluid.wgsl:1374-1379): the face from cell c to body b's cell q
+V3 bodyFaceJ(Ctx& X, I2 c, I2 q, uint32_t b) {
+    V2 n{(float)(q.x - c.x), (float)(q.y - c.y)};
+    V2 pos = bodyV(X, b, WIG_BW_POS);
+    V2 r{(((float)c.x + 0.5f) + 0.5f * n.x) - pos.x, (((float)c.y + 0.5f) + 0.5f * n.y) - pos.y};
+    return V3{n.x, n.y, r.x * n.y - r.y * n.x};
+}
+inline V3 scale3(V3 v, float s) { return V3{v.x * s, v.y * s, v.z * s}; }
+inline V3 add3(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline float dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// addPressurePush, couplingAt (fluid.wgsl:1381-1403)
+void addPressurePush(Ctx& X, I2 c, float p, uint32_t which) {
+    for (int d = 0; d < 4; d++) {
+        I2 q = Ctx::beside(c, d);
+        uint32_t b = rigidAt(X, q);
+        if (b != NONE) addPush(X, b, which, scale3(bodyFaceJ(X, c, q, b), p));
+    }
+}
+float couplingAt(Ctx& X, I2 c, uint32_t which) {
+    float sum = 0.0f;
+    if (!X.motion) return sum;
+    for (int d = 0; d < 4; d++) {
+        I2 q = Ctx::beside(c, d);
+        uint32_t b = rigidAt(X, q);
+        if (b != NONE) sum = sum + dot3(bodyFaceJ(X, c, q, b), pushChange(X, b, which));
+    }
+    return sum;
+}
+// rigidVel (fluid.wgsl:1460-1465), bodyMoving (fluid.wgsl:1410-1419)
+V2 rigidVel(Ctx& X, uint32_t b, V2 x) {
+    V2 pos = bodyV(X, b, WIG_BW_POS);
+    V2 r{x.x - pos.x, x.y - pos.y};
+    float spin = bodyF(X, b, WIG_BW_SPIN);
+    V2 v = bodyV(X, b, WIG_BW_VEL);
+    return V2{v.x + -spin * r.y, v.y + spin * r.x};
+}
+V2 bodyMoving(Ctx& X, uint32_t b, V2 x, bool drag) {
+    V2 pos = bodyV(X, b, WIG_BW_POS);
+    V2 pull = X.pullAt(pos);
+    float m = rigidMass(X, b);
+    V3 ch = add3(pushChange(X, b, PUSH_SURFACE), giveWay(X, b, V3{m * pull.x, m * pull.y, 0.0f}));
+    if (drag) ch = add3(ch, pushChange(X, b, PUSH_DRAG));
+    V2 r{x.x - pos.x, x.y - pos.y};
+    V2 rv = rigidVel(X, b, x);
+    V2 px = X.pullAt(x);
+    return V2{(((rv.x + px.x) - pull.x) + ch.x) + -ch.z * r.y, (((rv.y + px.y) - pull.y) + ch.y) + ch.z * r.x};
+}
+// bodyReach (fluid.wgsl:413-415)
+float bodyReach(Ctx& X, uint32_t b, I2 n) {
+    uint32_t w = bodyWord(X, b, WIG_BW_SUBCELL);
+    float sx = f16_value(w & 0xffffu), sy = f16_value(w >> 16);
+    return clampf(0.5f + (sx * (float)n.x + sy * (float)n.y), 0.0f, 1.0f);
+}
+// posedRoom (fluid.wgsl:2035-2045)
+float posedRoom(Ctx& X, I2 c) {
+    float room = 1.0f;
+    for (int d = 0; d < 4; d++) {
+        I2 q = Ctx::beside(c, d);
+        uint32_t b = rigidAt(X, q);
+        if (b != NONE) room = room + (0.5f - bodyReach(X, b, I2{c.x - q.x, c.y - q.y}));
+    }
+    return clampf(room, 0.1f, 1.9f);
+}
+// faceMiddle (fluid.wgsl:1473-1475)
+V2 faceMiddle(I2 at, bool isU) { return isU ? V2{(float)at.x + 0.0f, (float)at.y + 0.5f} : V2{(float)at.x + 0.5f, (float)at.y + 0.0f}; }
+// potentialAt (fluid.wgsl:2958-2960), the masses' potential none (binding 10 unbound)
+float potentialAt(Ctx& X, V2 pos) { return X.P->earth_g * ((float)X.H - pos.y) + 0.0f; }
+// seepAt (fluid.wgsl:2977-3000)
+float seepAt(Ctx& X, I2 c, I2 n, uint32_t h, bool held, V2 x) {
+    I2 ways[2] = {I2{-1, 0}, I2{1, 0}};
+    int count = 2;
+    if (n.x != 0) { ways[0] = I2{-n.x, -n.y}; count = 1; }
+    int nearest = SEEP_REACH + 1;
+    float p = 0.0f;
+    for (int w = 0; w < count; w++) {
+        for (int k = 1; k < nearest; k++) {
+            I2 q{c.x + ways[w].x * k, c.y + ways[w].y * k};
+            if ((held ? heldAt(X, q) : rigidAt(X, q)) == h) continue;
+            V4 g = X.gridAt(q);
+            if (g.z > 0.0f) {
+                nearest = k;
+                p = g.x + g.z * (potentialAt(X, V2{(float)q.x + 0.5f, (float)q.y + 0.5f}) - potentialAt(X, x));
+            }
+            break;
+        }
+    }
+    return p;
+}
+// heldPush (fluid.wgsl:3007-3031)
+void heldPush(Ctx& X, I2 c, uint32_t h, int32_t out[3]) {
+    V2 pos = bodyV(X, h, WIG_BW_POS);
+    V2 f{0.0f, 0.0f};
+    float torque = 0.0f;
+    for (int d = 0; d < 4; d++) {
+        I2 q = Ctx::beside(c, d);
+        I2 n{q.x - c.x, q.y - c.y};
+        if (heldAt(X, q) == h) continue;
+        V4 g = X.gridAt(q);
+        V2 x{((float)c.x + 0.5f) + 0.5f * (float)n.x, ((float)c.y + 0.5f) + 0.5f * (float)n.y};
+        float p = g.x;
+        if (g.z > 0.0f) p = p + g.z * (potentialAt(X, V2{(float)q.x + 0.5f, (float)q.y + 0.5f}) - potentialAt(X, x));
+        else if (g.z < 0.0f) p = seepAt(X, c, n, h, true, x);
+        V2 push{-p * (float)n.x, -p * (float)n.y};
+        f = V2{f.x + push.x, f.y + push.y};
+        V2 r{x.x - pos.x, x.y - pos.y};
+        torque = torque + (r.x * push.y - r.y * push.x);
+    }
+    out[0] = f2i(rnd_even((f.x / rigidMass(X, h)) * RIGID_FIX));
+    out[1] = f2i(rnd_even((f.y / rigidMass(X, h)) * RIGID_FIX));
+    out[2] = f2i(rnd_even((torque / rigidInertia(X, h)) * RIGID_FIX));
+}
+
 // sync / syncMarks (fluid.wgsl:608-659)
 void pass_sync(Ctx& X, bool claims) {
     X.parts[0] = 0u;
@@ -586,7 +805,7 @@ void pass_sync(Ctx& X, bool claims) {
     int bh = (X.H + BLOCK - 1) / BLOCK;
     for (int by = 0; by < bh; by++)
         for (int bx = 0; bx < (int)X.BW; bx++) {
-            bool here = false;
+            bool here = false, region = false;
             for (int ly = 0; ly < BLOCK; ly++)
                 for (int lx = 0; lx < BLOCK; lx++) {
                     I2 c{bx * BLOCK + lx, by * BLOCK + ly};
@@ -600,9 +819,12 @@ void pass_sync(Ctx& X, bool claims) {
                             d = wmax(d, claimOf(i));
                         }
                         here = true;
+                    } else if (wetRegionAt(X, v)) {
+                        region = true;
                     }
                 }
             if (here) X.blocks[X.blockIndex(I2{bx, by})] |= MARK_LIQUID;
+            if (region) X.blocks[X.blockIndex(I2{bx, by})] |= MARK_REGION;
         }
 }
 
@@ -973,8 +1195,12 @@ void pass_classify(Ctx& X) {
                 V4 wasDrift{wdp[0], wdp[1], wdp[2], wdp[3]};
                 bool sealed = false;
                 if (n == 0 && mayBeSealed(X, p)) sealed = (ufLink(X, ufFind(X, i)) & REGION_OPEN) == 0u;
+                uint32_t rigid = NONE, held = NONE;
                 if (n < 0) {
                     c.z = -1.0f;
+                    // a free body's cell (fluid.wgsl:1614-1627; no cups: binding 14 unbound)
+                    if (X.motion) rigid = rigidBodyOf(X, X.cellv(i));
+                    if (rigid != NONE && isHeld(X, rigid)) { held = rigid; rigid = NONE; }
                 } else if (n > 0) {
                     V2 li = liquidIn(X, i);
                     c = V4{0, 0, li.x, li.y};
@@ -998,8 +1224,10 @@ void pass_classify(Ctx& X) {
                         c = fluid > 0.0f ? V4{0, 0, mean.x / fluid, mean.y / fluid} : V4{0, 0, 1.0f, 0.0f};
                     }
                 }
-                uint32_t liquid = c.z > 0.0f ? mine : 0u;
+                uint32_t liquid = (c.z > 0.0f || rigid != NONE || held != NONE) ? mine : 0u;
                 V4 drift{0.0f, 0.0f, sealed ? 1.0f : 0.0f, (float)((f2u(wasDrift.w) & ~(mine | fall0)) | liquid)};
+                if (rigid != NONE) drift.z = -1.0f - (float)rigid;
+                else if (held != NONE) drift.z = -1.0f - (float)(held + MAX_BODIES);
                 if (c.z > 0.0f) {
                     if (was.z > 0.0f) {
                         c.x = was.x;
@@ -1041,12 +1269,39 @@ float lastPush(Ctx& X, I2 a, I2 at, V4 ga, V4 gb) {
     return fineBeta(ga.z, gb.z, X.shareAt(a), X.shareAt(at)) * (gb.x - ga.x);
 }
 
+// setBodyFace (fluid.wgsl:1840-1859)
+void setBodyFace(Ctx& X, uint32_t f, I2 at, bool isU, V4 ga, V4 gb, uint32_t ra, uint32_t rb, bool drag) {
+    V2 x = faceMiddle(at, isU);
+    float now = 0.0f, u = 0.0f;
+    if (ra != NONE && rb != NONE) {
+        V2 ma = bodyMoving(X, ra, x, drag), mb = bodyMoving(X, rb, x, drag);
+        V2 va = rigidVel(X, ra, x), vb = rigidVel(X, rb, x);
+        now = 0.5f * (isU ? ma.x + mb.x : ma.y + mb.y);
+        u = 0.5f * (isU ? va.x + vb.x : va.y + vb.y);
+    } else {
+        uint32_t b = ra != NONE ? ra : rb;
+        V2 m = bodyMoving(X, b, x, drag), v = rigidVel(X, b, x);
+        now = isU ? m.x : m.y;
+        u = isU ? v.x : v.y;
+    }
+    V4 other = ra != NONE ? gb : ga;
+    float nu = ((ra == NONE || rb == NONE) && other.z > 0.0f) ? other.w : 0.0f;
+    float* fp = X.fv(X.faceSlot(f));
+    fp[0] = now; fp[1] = u; fp[2] = 1.0f; fp[3] = nu;
+    X.viscRhs(f) = now;
+}
+
 // setFace (fluid.wgsl:1936-1980), the wind's drag none (no air bound).
 void setFace(Ctx& X, I2 at, bool isU) {
     uint32_t f = X.faceIndex(at, isU);
     I2 a = isU ? I2{at.x - 1, at.y} : I2{at.x, at.y - 1};
     int axis = isU ? 0 : 1;
     V4 ga = X.gridAt(a), gb = X.gridAt(at);
+    uint32_t ra = rigidAt(X, a), rb = rigidAt(X, at);
+    if (ra != NONE || rb != NONE) {
+        setBodyFace(X, f, at, isU, ga, gb, ra, rb, false);
+        return;
+    }
     uint32_t slot = X.sumSlot(f);
     int32_t weight = (int32_t)X.counters[slot + 1u];
     float u = 0.0f, held = 0.0f;
@@ -1085,17 +1340,23 @@ void pass_setFaces(Ctx& X) {
     });
 }
 
-// viscousFace (fluid.wgsl:3347-3403), no bodies.
+// viscousFace (fluid.wgsl:3347-3403)
 void viscousFace(Ctx& X, I2 at, bool isU, int color) {
     if (((at.x + at.y) & 1) != color) return;
     I2 a = isU ? I2{at.x - 1, at.y} : I2{at.x, at.y - 1};
     V4 ga = X.gridAt(a), gb = X.gridAt(at);
-    if (ga.z < 0.0f || gb.z < 0.0f) return;
+    uint32_t ra = rigidAt(X, a), rb = rigidAt(X, at);
+    bool surface = (ra != NONE) != (rb != NONE) && (ra != NONE ? gb.z : ga.z) > 0.0f;
+    if (!surface && (ga.z < 0.0f || gb.z < 0.0f || ra != NONE || rb != NONE)) return;
     uint32_t fi = X.faceIndex(at, isU);
     float* fp = X.fv(X.faceSlot(fi));
     float nu = fp[3];
     if (nu <= 0.0f) return;
     float heavy = 1.0f;
+    if (surface) {
+        float liquid = ra != NONE ? gb.z : ga.z;
+        heavy = 2.0f * liquid / (liquid + bodyDensity(X, ra != NONE ? ra : rb));
+    }
     V2 through{ga.z > 0.0f ? ga.w : 0.0f, gb.z > 0.0f ? gb.w : 0.0f};
     float sum = 0.0f, n = 0.0f;
     for (int d = 0; d < 4; d++) {
@@ -1134,7 +1395,7 @@ void pass_viscosity(Ctx& X, int color) {
                     I2 a = isU ? I2{at.x - 1, at.y} : I2{at.x, at.y - 1};
                     V4 ga = X.gridAt(a), gb = X.gridAt(at);
                     uint32_t fi = X.faceIndex(at, isU);
-                    if (faceViscosity(ga, gb) > 0.0f) {
+                    if (rigidAt(X, a) == NONE && rigidAt(X, at) == NONE && faceViscosity(ga, gb) > 0.0f) {
                         float* fp = X.fv(X.faceSlot(fi));
                         X.viscLast(fi) = fp[0] - X.viscRhs(fi);
                         fp[0] = fp[0] + lastPush(X, a, at, ga, gb);
@@ -1146,7 +1407,7 @@ void pass_viscosity(Ctx& X, int color) {
     }
 }
 
-// divergence (fluid.wgsl:1996-2025), posedRoom 1 with no bodies.
+// divergence (fluid.wgsl:1996-2025)
 void pass_divergence(Ctx& X) {
     X.blocks[X.countSlot(COUNT_RESIDUAL)] = 0u;
     X.blocks[X.countSlot(COUNT_CYCLES)] = 0u;
@@ -1158,7 +1419,7 @@ void pass_divergence(Ctx& X) {
                     X.fv(X.faceSlot(X.vFace(c.x, c.y + 1)))[0] - X.fv(X.faceSlot(X.vFace(c.x, c.y)))[0];
         X.fv(2u * i)[1] = out;
         float n = X.densityAt(c);
-        float room = clampf(1.0f, 0.1f, 1.9f);
+        float room = posedRoom(X, c);
         X.fv(2u * i + 1u)[1] = X.fv(2u * i + 1u)[2] < 0.0f ? 0.0f : -SPREAD * (n - room);
     });
 }
@@ -1224,7 +1485,7 @@ double norm2Blocks(Ctx& X, Fn value) {
 void pass_cgResidual(Ctx& X) {
     forActiveCells(X, [&](uint32_t, I2 c, uint32_t) {
         if (!X.inWorld(c)) return;
-        if (X.gridAt(c).z > 0.0f) X.cg[4u * (size_t)X.cellIndex(c) + 1u] = -residualAt(X, 0, c).x - 0.0f;
+        if (X.gridAt(c).z > 0.0f) X.cg[4u * (size_t)X.cellIndex(c) + 1u] = -residualAt(X, 0, c).x - couplingAt(X, c, PUSH_X);
     });
     X.bnorm2 = norm2Blocks(X, [&](I2 c) -> double {
         uint32_t i = X.cellIndex(c);
@@ -1631,7 +1892,7 @@ void pass_cgApply(Ctx& X) {
             if (!X.inWorld(c)) continue;
             float rho = X.gridAt(c).z;
             uint32_t i = X.cellIndex(c);
-            float q = rho > 0.0f ? applyA(X, c, rho) + 0.0f : 0.0f;
+            float q = rho > 0.0f ? applyA(X, c, rho) + couplingAt(X, c, PUSH_P0 + X.cycle % 2u) : 0.0f;
             float* g = X.cg + 4u * (size_t)i;
             g[3] = q;
             vx[li] = g[2] * q;
@@ -1644,6 +1905,13 @@ void pass_cgApply(Ctx& X) {
         }
     }
 }
+// The bodies' sums of this iteration's direction emptied for the iteration
+// after next (fluid.wgsl:2808-2813).
+void clearDirectionPushes(Ctx& X) {
+    if (!X.pushes) return;
+    uint32_t which = PUSH_P0 + X.cycle % 2u;
+    for (uint32_t k = 0; k < MAX_BODIES * 6u; k++) X.pushes[pushSlot(k / 6u, which, 0u) + k % 6u] = 0u;
+}
 void pass_cgAlpha(Ctx& X) {
     if (X.converged() || X.activeCount() == 0u) return;
     float* at = X.cg + 4u * (size_t)(X.C + X.B);
@@ -1653,11 +1921,13 @@ void pass_cgAlpha(Ctx& X) {
         g_pq = pq;
         g_alpha = pq <= 0.0 ? 0.0 : g_rz / pq;
         at[1] = (float)g_alpha; at[3] = (float)pq;
+        clearDirectionPushes(X);
         return;
     }
     float pq = sumBlocks(X).x;
     V4 was{at[0], at[1], at[2], at[3]};
     at[0] = was.x; at[1] = pq <= 0.0f ? 0.0f : was.x / pq; at[2] = was.z; at[3] = pq;
+    clearDirectionPushes(X);
 }
 void pass_cgUpdate(Ctx& X) {
     X.blocks[X.countSlot(COUNT_RESIDUAL + (X.cycle + 1u) % 3u)] = 0u;
@@ -1702,7 +1972,7 @@ void pass_cgFinish(Ctx& X) {
     });
 }
 
-// projectFace, project (fluid.wgsl:2897-2942), no bodies.
+// projectFace, project (fluid.wgsl:2897-2942)
 void pass_project(Ctx& X) {
     uint32_t& most = X.blocks[X.countSlot(COUNT_MOST_CYCLES)];
     most = wmax(most, X.blocks[X.countSlot(COUNT_CYCLES)]);
@@ -1718,13 +1988,166 @@ void pass_project(Ctx& X) {
             I2 a = isU ? I2{at.x - 1, at.y} : I2{at.x, at.y - 1};
             V4 ga = X.gridAt(a), gb = X.gridAt(at);
             float beta = fineBeta(ga.z, gb.z, X.shareAt(a), X.shareAt(at));
+            uint32_t ra = rigidAt(X, a), rb = rigidAt(X, at);
             if (beta > 0.0f) {
                 face[0] = face[0] - beta * (gb.x - ga.x);
                 face[2] = PROJECTED;
-                face[3] = clampf(-beta * (X.driftAt(at) - X.driftAt(a)), -MAX_DRIFT, MAX_DRIFT);
+                bool rigid = ra != NONE || rb != NONE;
+                face[3] = rigid ? 0.0f : clampf(-beta * (X.driftAt(at) - X.driftAt(a)), -MAX_DRIFT, MAX_DRIFT);
+            }
+            // a face between the liquid and a free body moves with the body's push (PUSH_F)
+            if ((ra == NONE) != (rb == NONE) && (ra != NONE ? gb.z : ga.z) > 0.0f) {
+                uint32_t bb = ra != NONE ? ra : rb;
+                V3 ch = pushChange(X, bb, PUSH_F);
+                V2 m = faceMiddle(at, isU);
+                V2 pos = bodyV(X, bb, WIG_BW_POS);
+                V2 r{m.x - pos.x, m.y - pos.y};
+                face[0] = face[0] + (isU ? ch.x - ch.z * r.y : ch.y + ch.z * r.x);
+                face[2] = PROJECTED;
             }
         }
     });
+}
+
+// ---------------------------------------------------------------- the bodies' passes
+
+// bodyStart (fluid.wgsl:3079-3084)
+void pass_bodyStart(Ctx& X) {
+    if (!X.pushes) return;
+    for (uint32_t k = 0; k < MAX_BODIES * WIG_BODY_PUSH_WORDS; k++) X.pushes[k] = 0u;
+}
+// seepLoads, bodyLoads (fluid.wgsl:3094-3139)
+void seepLoads(Ctx& X, I2 c, uint32_t b) {
+    for (int d = 0; d < 4; d++) {
+        I2 q = Ctx::beside(c, d);
+        if (!X.inWorld(q) || rigidAt(X, q) == b || X.gridAt(q).z >= 0.0f) continue;
+        I2 n{q.x - c.x, q.y - c.y};
+        V2 x{((float)c.x + 0.5f) + 0.5f * (float)n.x, ((float)c.y + 0.5f) + 0.5f * (float)n.y};
+        addPush(X, b, PUSH_SURFACE, scale3(bodyFaceJ(X, q, c, b), seepAt(X, c, n, b, false, x)));
+    }
+}
+void pass_bodyLoads(Ctx& X) {
+    if (!X.motion) return;
+    forActiveCells(X, [&](uint32_t, I2 c, uint32_t) {
+        if (!X.inWorld(c)) return;
+        uint32_t own = rigidAt(X, c);
+        if (own != NONE) { seepLoads(X, c, own); return; }
+        V4 g = X.gridAt(c);
+        if (g.z <= 0.0f) return;
+        V2 mid{(float)c.x + 0.5f, (float)c.y + 0.5f};
+        for (int d = 0; d < 4; d++) {
+            I2 q = Ctx::beside(c, d);
+            uint32_t b = rigidAt(X, q);
+            if (b == NONE) continue;
+            I2 n{q.x - c.x, q.y - c.y};
+            float reach = 1.0f - bodyReach(X, b, I2{-n.x, -n.y});
+            V2 surface{mid.x + (float)n.x * reach, mid.y + (float)n.y * reach};
+            addPush(X, b, PUSH_SURFACE,
+                    scale3(scale3(bodyFaceJ(X, c, q, b), g.z), potentialAt(X, mid) - potentialAt(X, surface)));
+        }
+    });
+}
+// bodyDrag (fluid.wgsl:3149-3176)
+void pass_bodyDrag(Ctx& X) {
+    if (!X.motion) return;
+    forActiveCells(X, [&](uint32_t, I2 c, uint32_t) {
+        uint32_t b = rigidAt(X, c);
+        if (!X.inWorld(c) || b == NONE) return;
+        V2 pos = bodyV(X, b, WIG_BW_POS);
+        float rho = bodyDensity(X, b);
+        V3 push{0.0f, 0.0f, 0.0f};
+        for (int k = 0; k < 4; k++) {
+            bool isU = k < 2;
+            int sg = (k & 1) == 1 ? 1 : -1;
+            I2 n = isU ? I2{sg, 0} : I2{0, sg};
+            if (X.gridAt(I2{c.x + n.x, c.y + n.y}).z <= 0.0f) continue;
+            I2 at = isU ? I2{c.x + (k & 1), c.y} : I2{c.x, c.y + (k & 1)};
+            V2 x = faceMiddle(at, isU);
+            V2 mv = bodyMoving(X, b, x, false);
+            float du = (bodyReach(X, b, n) * rho) * (X.fv(X.faceSlot(X.faceIndex(at, isU)))[0] - (isU ? mv.x : mv.y));
+            V2 r{x.x - pos.x, x.y - pos.y};
+            if (isU) push.x = push.x + du; else push.y = push.y + du;
+            push.z = push.z + (isU ? -r.y * du : r.x * du);
+        }
+        if (push.x != 0.0f || push.y != 0.0f || push.z != 0.0f) addPush(X, b, PUSH_DRAG, push);
+    });
+}
+// bodyFaces (fluid.wgsl:3180-3200)
+void pass_bodyFaces(Ctx& X) {
+    if (!X.motion) return;
+    forActiveCells(X, [&](uint32_t, I2 c, uint32_t) {
+        if (!X.inWorld(c)) return;
+        int fs[4][3];
+        X.facesOf(c, fs);
+        for (int j = 0; j < 4; j++) {
+            if (fs[j][2] < 0) continue;
+            I2 at{fs[j][0], fs[j][1]};
+            bool isU = fs[j][2] == 1;
+            I2 a = isU ? I2{at.x - 1, at.y} : I2{at.x, at.y - 1};
+            uint32_t ra = rigidAt(X, a), rb = rigidAt(X, at);
+            if (ra != NONE || rb != NONE) setBodyFace(X, X.faceIndex(at, isU), at, isU, X.gridAt(a), X.gridAt(at), ra, rb, true);
+        }
+    });
+}
+// cgBodyX, cgBodyP, cgBodyF (fluid.wgsl:2819-2845)
+void pass_cgBodyX(Ctx& X) {
+    if (!X.motion) return;
+    forActiveCells(X, [&](uint32_t, I2 c, uint32_t) {
+        if (X.inWorld(c) && X.gridAt(c).z > 0.0f) addPressurePush(X, c, X.cg[4u * (size_t)X.cellIndex(c)], PUSH_X);
+    });
+}
+void pass_cgBodyP(Ctx& X) {
+    if (!X.motion || X.converged()) return;
+    forActiveCells(X, [&](uint32_t, I2 c, uint32_t) {
+        if (X.inWorld(c) && X.gridAt(c).z > 0.0f)
+            addPressurePush(X, c, X.cg[4u * (size_t)X.cellIndex(c) + 2u], PUSH_P0 + X.cycle % 2u);
+    });
+}
+void pass_cgBodyF(Ctx& X) {
+    if (!X.motion) return;
+    forActiveCells(X, [&](uint32_t, I2 c, uint32_t) {
+        if (X.inWorld(c) && X.gridAt(c).z > 0.0f) addPressurePush(X, c, X.fv(2u * X.cellIndex(c))[0], PUSH_F);
+    });
+}
+// rigidify (fluid.wgsl:3033-3076): each block's cells of its lowest held
+// body summed once, the others' added straight into their bodies' words.
+void pass_rigidify(Ctx& X) {
+    if (!X.motion) return;
+    uint32_t na = X.activeCount();
+    for (uint32_t wid = 0; wid < na; wid++) {
+        I2 b = X.activeBlock(wid);
+        uint32_t first = NONE;
+        for (int li = 0; li < 64; li++) {
+            uint32_t h = heldAt(X, I2{b.x * BLOCK + li % BLOCK, b.y * BLOCK + li / BLOCK});
+            if (h != NONE) first = wmin(first, h);
+        }
+        uint32_t sums[3] = {0u, 0u, 0u};
+        for (int li = 0; li < 64; li++) {
+            I2 c{b.x * BLOCK + li % BLOCK, b.y * BLOCK + li / BLOCK};
+            uint32_t h = heldAt(X, c);
+            if (h == NONE) continue;
+            int32_t d[3];
+            heldPush(X, c, h, d);
+            if ((X.blocks[X.stateSlot(X.blockIndex(b))] & NEAR_LIQUID) != 0u) X.motion[liquidSlot(h, 3u)] |= WIG_LIQUID_WET;
+            for (int k = 0; k < 3; k++) {
+                if (h == first) sums[k] += (uint32_t)d[k];
+                else X.motion[liquidSlot(h, (uint32_t)k)] += (uint32_t)d[k];
+            }
+        }
+        if (first != NONE)
+            for (uint32_t k = 0; k < 3; k++) X.motion[liquidSlot(first, k)] += sums[k];
+    }
+}
+// bodyPush (fluid.wgsl:3205-3218)
+void pass_bodyPush(Ctx& X) {
+    if (!X.motion) return;
+    for (uint32_t b = 0; b < MAX_BODIES; b++) {
+        V3 ch = add3(add3(pushChangeFree(X, b, PUSH_SURFACE), pushChangeFree(X, b, PUSH_DRAG)), pushChangeFree(X, b, PUSH_F));
+        if (ch.x == 0.0f && ch.y == 0.0f && ch.z == 0.0f) continue;
+        X.motion[liquidSlot(b, 0u)] += (uint32_t)f2i(rnd_even(ch.x * RIGID_FIX));
+        X.motion[liquidSlot(b, 1u)] += (uint32_t)f2i(rnd_even(ch.y * RIGID_FIX));
+        X.motion[liquidSlot(b, 2u)] += (uint32_t)f2i(rnd_even(ch.z * RIGID_FIX));
+    }
 }
 
 // extrapolateFace (fluid.wgsl:3226-3265)
@@ -2159,8 +2582,14 @@ int layout(const wig_world_desc* d, wig_world_layout* L) {
     return WIG_OK;
 }
 
+// The bodies' buffers bound by wo_bind_bodies (null: none).
+uint32_t* g_motion = nullptr;
+uint32_t* g_pushes = nullptr;
+
 void setup(Ctx& X, const wig_world_layout& L, const wig_params* P, const wig_elem* E, uint32_t nE, wig_fluid_buffers* b) {
     X.L = L; X.P = P; X.E = E; X.nE = nE;
+    X.motion = g_motion;
+    X.pushes = g_pushes;
     X.cells = (uint32_t*)b->cells; X.sorted = (uint32_t*)b->sorted; X.parts = (uint32_t*)b->parts;
     X.counters = (uint32_t*)b->counters; X.field = (float*)b->field; X.blocks = (uint32_t*)b->blocks; X.cg = (float*)b->cg;
     X.W = (int)L.width; X.H = (int)L.height;
@@ -2225,6 +2654,15 @@ void run_pass(Ctx& X, int pass) {
     case WIG_PASS_RASTER_CLAIMS: pass_rasterClaims(X); break;
     case WIG_PASS_RASTER: pass_raster(X); break;
     case WIG_PASS_UNPAINT: pass_unpaint(X); break;
+    case WIG_PASS_BODY_START: pass_bodyStart(X); break;
+    case WIG_PASS_BODY_LOADS: pass_bodyLoads(X); break;
+    case WIG_PASS_BODY_DRAG: pass_bodyDrag(X); break;
+    case WIG_PASS_BODY_FACES: pass_bodyFaces(X); break;
+    case WIG_PASS_CG_BODY_X: pass_cgBodyX(X); break;
+    case WIG_PASS_CG_BODY_P: pass_cgBodyP(X); break;
+    case WIG_PASS_CG_BODY_F: pass_cgBodyF(X); break;
+    case WIG_PASS_RIGIDIFY: pass_rigidify(X); break;
+    case WIG_PASS_BODY_PUSH: pass_bodyPush(X); break;
     default: break;
     }
 }
@@ -2289,6 +2727,16 @@ extern "C" {
 
 int wo_layout(const wig_world_desc* d, wig_world_layout* out) { return layout(d, out); }
 
+// Binds the free bodies' host buffers for the passes and steps that follow
+// (motion: WIG_BODY_MOTION_WORDS, pushes: WIG_MAX_BODIES * WIG_BODY_PUSH_WORDS
+// u32); both null unbinds them.
+int wo_bind_bodies(uint32_t* motion, uint32_t* pushes) {
+    if ((motion == nullptr) != (pushes == nullptr)) return WIG_E_ARG;
+    g_motion = motion;
+    g_pushes = pushes;
+    return WIG_OK;
+}
+
 // One pass (a reference pipeline dispatch) over host buffers.
 int wo_pass(const wig_world_desc* d, const wig_params* P, const wig_elem* E, uint32_t nE, wig_fluid_buffers* b,
             int pass, uint32_t level, uint32_t cycle) {
@@ -2338,10 +2786,13 @@ int wo_step(const wig_world_desc* d, const wig_params* P, const wig_elem* E, uin
         run(WIG_PASS_SEAL_JOIN);
         run(WIG_PASS_SEAL_ANCHOR);
         run(WIG_PASS_CLASSIFY);
+        const bool bodies = X.motion != nullptr;
+        if (bodies) { run(WIG_PASS_BODY_START); run(WIG_PASS_BODY_LOADS); }
         run(WIG_PASS_SET_FACES);
         if (flags & WIG_STEP_VISCOUS)
             for (int i = 0; i < 8; i++) { run(WIG_PASS_VISCOSITY_RED); run(WIG_PASS_VISCOSITY_BLACK); }
         run(WIG_PASS_UNPRESS);
+        if (bodies && (flags & WIG_STEP_VISCOUS)) { run(WIG_PASS_BODY_DRAG); run(WIG_PASS_BODY_FACES); }
         run(WIG_PASS_DIVERGENCE);
         bool sh;
         if (flags & WIG_STEP_SHIFTED_SET) sh = (flags & WIG_STEP_SHIFTED_FIRST) != 0u;
@@ -2350,6 +2801,7 @@ int wo_step(const wig_world_desc* d, const wig_params* P, const wig_elem* E, uin
         run(WIG_PASS_CG_START);
         run(WIG_PASS_CG_JOIN);
         run(WIG_PASS_CG_ANCHOR);
+        if (bodies) run(WIG_PASS_CG_BODY_X);
         run(WIG_PASS_CG_RESIDUAL);
         run(WIG_PASS_CG_PREPARE);
         for (uint32_t cycle = 0; cycle < max_cycles; cycle++) {
@@ -2373,12 +2825,15 @@ int wo_step(const wig_world_desc* d, const wig_params* P, const wig_elem* E, uin
             run(WIG_PASS_CG_RHO, 0, cycle);
             run(WIG_PASS_CG_BETA, 0, cycle);
             run(WIG_PASS_CG_DIRECTION, 0, cycle);
+            if (bodies) run(WIG_PASS_CG_BODY_P, 0, cycle);
             run(WIG_PASS_CG_APPLY, 0, cycle);
             run(WIG_PASS_CG_ALPHA, 0, cycle);
             run(WIG_PASS_CG_UPDATE, 0, cycle);
         }
         run(WIG_PASS_CG_FINISH);
+        if (bodies) run(WIG_PASS_CG_BODY_F);
         run(WIG_PASS_PROJECT);
+        if (bodies) { run(WIG_PASS_RIGIDIFY); run(WIG_PASS_BODY_PUSH); }
         run(WIG_PASS_EXTRAPOLATE);
         run(WIG_PASS_EXTRAPOLATE_FURTHER);
         run(WIG_PASS_ADVECT);

@@ -1,0 +1,112 @@
+"""The oracle's free-body coupling (fluid.wgsl:1181-1470, :2819-2845,
+:2949-3218) on a tank with synthetic bodies, checked on the CPU by what the
+coupled solve must do: the liquid beside a moving body is left as divergence
+free as the rest (the body's faces moving with its push, PUSH_F), the bodies
+the reference leaves out of the solve (just found, not alive) get nothing,
+a held body's push is summed and it is marked wet, and no particle ends in a
+body's cell."""
+import numpy as np
+import pytest
+
+from worldinagrain_b200 import abi
+from worldinagrain_b200 import world as W
+
+from .common import params
+
+FLAGS = abi.STEP_TOLERANCE | abi.STEP_F64_DOTS
+
+
+def _oracle(world, bodies):
+    from oracle.oracle import Oracle
+    return Oracle(world, W.body_element_table(), bodies)
+
+
+def _face_divergence(w):
+    C, Wd, H, F = w.C, w.W, w.H, w.L["face_count"]
+    faces = w.field.view(np.float32)[4 * 2 * C:4 * (2 * C + F)].reshape(F, 4)
+    u = faces[:(Wd + 1) * H, 0].reshape(H, Wd + 1)
+    v = faces[(Wd + 1) * H:, 0].reshape(H + 1, Wd)
+    return (u[:, 1:] - u[:, :-1]) + (v[1:, :] - v[:-1, :])
+
+
+def _solve_and_project(o, w, P, max_cycles=64):
+    """The second half of a step, pass by pass, up to and including project."""
+    for p in ["SYNC", "SYNC_PARTICLES", "SYNC_SEED", "COMPACT", "RETIRE", "CLEAR", "GATHER", "SEAL_JOIN",
+              "SEAL_ANCHOR", "CLASSIFY", "BODY_START", "BODY_LOADS", "SET_FACES", "UNPRESS", "DIVERGENCE",
+              "CG_START", "CG_JOIN", "CG_ANCHOR", "CG_BODY_X", "CG_RESIDUAL", "CG_PREPARE"]:
+        o.pass_(P, p)
+    levels = len(w.L["levels"])
+    sh = True
+    for cyc in range(max_cycles):
+        for p in ("RELAX_RIMS", "RELAX_SHIFTED" if sh else "RELAX"):
+            o.pass_(P, p, 0, cyc)
+        sh = not sh
+        for l in range(1, levels + 1):
+            o.pass_(P, "RESTRICT", l, cyc)
+            if l < levels:
+                o.pass_(P, "SMOOTH_RED", l, cyc)
+                o.pass_(P, "SMOOTH_BLACK", l, cyc)
+        o.pass_(P, "SOLVE", levels, cyc)
+        for l in range(levels - 1, 0, -1):
+            for p in ("PROLONG", "SMOOTH_RED", "SMOOTH_BLACK"):
+                o.pass_(P, p, l, cyc)
+        for p in ("PROLONG_FINE", "RELAX_RIMS", "RELAX_SHIFTED" if sh else "RELAX"):
+            o.pass_(P, p, 0, cyc)
+        sh = not sh
+        for p in ("CG_RHO", "CG_BETA", "CG_DIRECTION", "CG_BODY_P", "CG_APPLY", "CG_ALPHA", "CG_UPDATE"):
+            o.pass_(P, p, 0, cyc)
+    o.pass_(P, "CG_FINISH")
+    o.pass_(P, "CG_BODY_F")
+    before = _face_divergence(w)
+    o.pass_(P, "PROJECT")
+    return before, _face_divergence(w)
+
+
+def test_coupled_projection_leaves_the_liquid_beside_bodies_divergence_free():
+    w, bodies = W.bodies_world()
+    o = _oracle(w, bodies)
+    o.step(params(w, 1), max_cycles=64, flags=FLAGS, tolerance=1e-6)
+    before, after = _solve_and_project(o, w, params(w, 2))
+    rho = w.field_cells()[:, 0, 2].reshape(w.H, w.W)
+    rigid = w.field_cells()[:, 1, 2].reshape(w.H, w.W) < -0.5
+    near = np.zeros_like(rigid)
+    near[:, 1:] |= rigid[:, :-1]
+    near[:, :-1] |= rigid[:, 1:]
+    near[1:, :] |= rigid[:-1, :]
+    near[:-1, :] |= rigid[1:, :]
+    liquid = rho > 0
+    assert np.any(liquid & near)
+    beside = np.abs(after[liquid & near]).max()
+    elsewhere = np.abs(after[liquid & ~near]).max()
+    assert beside < 0.05 * np.abs(before[liquid & near]).max()
+    assert beside <= 2.0 * elsewhere, (beside, elsewhere)
+
+
+@pytest.mark.parametrize("liquid,flags", [(abi.WATER, FLAGS), (W.MUD, FLAGS | abi.STEP_VISCOUS), (abi.WATER, 0)])
+def test_bodies_in_and_out_of_the_solve(liquid, flags):
+    w, bodies = W.bodies_world(liquid=liquid)
+    o = _oracle(w, bodies)
+    for s in range(1, 4):
+        st = o.step(params(w, s), max_cycles=64, flags=flags, tolerance=1e-6)
+        if flags & abi.STEP_TOLERANCE:
+            assert st.rel_residual <= 1e-6
+    drift_z = w.field_cells()[:, 1, 2]
+    # the free bodies and the held one are in the solve, classified by slot (fluid.wgsl:1657-1661)
+    for b, cells in ((0, 42), (1, 36)):
+        assert int(np.sum(drift_z == np.float32(-1.0 - b))) == cells
+    assert int(np.sum(drift_z == np.float32(-1.0 - (2 + abi.MAX_BODIES)))) == 40
+    for b in (0, 1, 2):
+        assert np.any(bodies.liquid(b)[:3] != 0), b
+    assert bodies.liquid(2)[3] & 0x80000000  # held and by the liquid: wet (LIQUID_WET)
+    for b in (3, 4):  # just found, not alive: walls standing still, nothing done to them
+        assert not np.any(bodies.liquid(b)), b
+    pushes = bodies.pushes.reshape(abi.MAX_BODIES, 6, 6)
+    assert np.any(pushes[0, 4] != 0)  # the pressure at the plank's surface as posed (PUSH_SURFACE)
+    if flags & abi.STEP_VISCOUS:
+        assert np.any(pushes[0, 5] != 0)  # the viscous liquid's drag (PUSH_DRAG)
+    # particles stop at a body's cells as at any solid
+    motion, _, _ = w.particles("sorted")
+    cx = np.clip(np.floor(motion[:, 0]).astype(int), 0, w.W - 1)
+    cy = np.clip(np.floor(motion[:, 1]).astype(int), 0, w.H - 1)
+    kinds = w.cell_view()[cy, cx, 0] & 0xff
+    assert not np.any(kinds == W.WOOD)

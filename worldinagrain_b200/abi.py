@@ -19,6 +19,22 @@ COUNT_RESIDUAL, COUNT_CYCLES, COUNT_MOST_CYCLES = 4, 7, 8
 
 KIND_SOLID, KIND_POWDER, KIND_LIQUID, KIND_GAS = 1, 2, 3, 4
 AIR, WALL, SAND, WATER = 0, 1, 2, 3
+NO_ELEM = 255
+FL_LOOSE = 8
+
+# Free bodies (include/wig_fluid.h, js/shared.js:294-333)
+MAX_BODIES = 1024
+BODY_TABLE_WORDS = 116
+BODY_CONTACTS = 16384
+BODY_CONTACT_WORDS = 12
+BODY_LIQUID_WORDS = 4
+BODY_PUSH_WORDS = 36
+BODY_LIQUID_BASE = MAX_BODIES * (1 + BODY_TABLE_WORDS) + BODY_CONTACTS * BODY_CONTACT_WORDS
+BODY_MOTION_WORDS = BODY_LIQUID_BASE + MAX_BODIES * BODY_LIQUID_WORDS
+BW = dict(POS=0, VEL=3, SPIN=5, MASS=6, INERTIA=7, CELLS=13, FLAGS=18, SUBCELL=25, CARGO=105, CARGO_INERTIA=106,
+          MOBILITY=108, MOBILITY_AT=114)
+BF_ALIVE, BF_NEW, BF_HELD, BF_WET = 1, 2, 32, 64
+RIGID_FIX = 16777216.0
 
 WIG_OK = 0
 ERRORS = {
@@ -53,6 +69,8 @@ PASSES = [
     "CG_RHO", "CG_BETA", "CG_DIRECTION", "CG_APPLY", "CG_ALPHA", "CG_UPDATE", "CG_FINISH", "PROJECT",
     "EXTRAPOLATE", "EXTRAPOLATE_FURTHER", "ADVECT", "SORT_COUNT", "SCAN_BLOCKS", "SCAN_TOTALS",
     "SCAN_FINISH", "SCATTER", "RASTER_CLAIMS", "RASTER", "UNPAINT",
+    "BODY_START", "BODY_LOADS", "BODY_DRAG", "BODY_FACES", "CG_BODY_X", "CG_BODY_P", "CG_BODY_F",
+    "RIGIDIFY", "BODY_PUSH",
 ]
 PASS = {name: i for i, name in enumerate(PASSES)}
 PROFILE_NAMES = PASSES + ["NORM", "REPORT", "F_SETUP", "F_LOOP", "F_RELAX", "F_RESTRICT", "F_SMOOTH", "F_COARSE",
@@ -80,7 +98,7 @@ class Elem(C.Structure):
         ("tension", C.c_float), ("expansion", C.c_float), ("expansion2", C.c_float),
         ("hi_t", C.c_float), ("lo_t", C.c_float), ("up_span", C.c_float), ("down_span", C.c_float),
         ("down_scale", C.c_float), ("sol_density", C.c_float), ("flags", C.c_uint32),
-        ("wetting", C.c_float), ("pad", C.c_float * 2),
+        ("wetting", C.c_float), ("break_to", C.c_uint32), ("pad", C.c_float),
     ]
 
 

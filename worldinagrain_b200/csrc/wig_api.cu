@@ -719,7 +719,11 @@ struct Rec {
 
 // encodeFluid's passes before the solve (js/sim.js:2486-2521), with the
 // work lists written at the step's start and after compact.
+// Whether the batch is one world with its free bodies bound.
+bool has_bodies(const wig_batch* b) { return b->K == 1 && b->hw[0].D.motion != nullptr; }
+
 void record_pre(Rec& R, bool viscous) {
+    const bool bodies = has_bodies(R.b);
     R.sched(0);
     R.run(WIG_PASS_SYNC);
     R.run(WIG_PASS_SYNC_PARTICLES);
@@ -732,6 +736,10 @@ void record_pre(Rec& R, bool viscous) {
     R.run(WIG_PASS_SEAL_JOIN);
     R.run(WIG_PASS_SEAL_ANCHOR);
     R.run(WIG_PASS_CLASSIFY);
+    if (bodies) {
+        R.run(WIG_PASS_BODY_START);
+        R.run(WIG_PASS_BODY_LOADS);
+    }
     R.run(WIG_PASS_SET_FACES);
     if (viscous)
         for (int i = 0; i < 8; i++) {
@@ -739,12 +747,20 @@ void record_pre(Rec& R, bool viscous) {
             R.run(WIG_PASS_VISCOSITY_BLACK);
         }
     R.run(WIG_PASS_UNPRESS);
+    if (bodies && viscous) {
+        R.run(WIG_PASS_BODY_DRAG);
+        R.run(WIG_PASS_BODY_FACES);
+    }
     R.run(WIG_PASS_DIVERGENCE);
 }
 
 // encodeFluid's passes after the solve (js/sim.js:2592-2611) and the report.
 void record_post(Rec& R) {
     R.run(WIG_PASS_PROJECT);
+    if (has_bodies(R.b)) {
+        R.run(WIG_PASS_RIGIDIFY);
+        R.run(WIG_PASS_BODY_PUSH);
+    }
     R.run(WIG_PASS_EXTRAPOLATE);
     R.run(WIG_PASS_EXTRAPOLATE_FURTHER);
     R.run(WIG_PASS_ADVECT);
@@ -781,6 +797,8 @@ uint32_t record_step(wig_batch* b, Lane& ln, uint32_t max_cycles, uint32_t flags
     R.run(WIG_PASS_CG_START);
     R.run(WIG_PASS_CG_JOIN);
     R.run(WIG_PASS_CG_ANCHOR);
+    const bool bodies = has_bodies(b);
+    if (bodies) R.run(WIG_PASS_CG_BODY_X);
     R.run(WIG_PASS_CG_RESIDUAL);
     if (tol) R.norm(0, 0);
     R.run(WIG_PASS_CG_PREPARE);
@@ -809,12 +827,14 @@ uint32_t record_step(wig_batch* b, Lane& ln, uint32_t max_cycles, uint32_t flags
         R.run(WIG_PASS_CG_RHO, 0, cycle);
         R.run(WIG_PASS_CG_BETA, 0, cycle);
         R.run(WIG_PASS_CG_DIRECTION, 0, cycle);
+        if (bodies) R.run(WIG_PASS_CG_BODY_P, 0, cycle);
         R.run(WIG_PASS_CG_APPLY, 0, cycle);
         R.run(WIG_PASS_CG_ALPHA, 0, cycle);
         R.run(WIG_PASS_CG_UPDATE, 0, cycle);
         if (tol) R.norm(1, cycle);
     }
     R.run(WIG_PASS_CG_FINISH);
+    if (bodies) R.run(WIG_PASS_CG_BODY_F);
     record_post(R);
     return R.launches;
 }
@@ -1306,6 +1326,25 @@ int wig_fluid_bind(wig_fluid* h, const wig_fluid_buffers* bufs) {
     return WIG_OK;
 }
 
+int wig_fluid_bind_bodies(wig_fluid* h, void* motion, void* pushes) {
+    if (!h || !h->b) return fail(WIG_E_ARG, "null handle");
+    if ((motion == nullptr) != (pushes == nullptr)) return fail(WIG_E_ARG, "bind both body buffers or neither");
+    if (((uintptr_t)motion & 15u) != 0u || ((uintptr_t)pushes & 15u) != 0u)
+        return fail(WIG_E_ARG, "body buffer not 16-byte aligned");
+    wig_batch* b = h->b;
+    for (auto& ln : b->lane) drop_graphs(ln);
+    b->hw[0].D.motion = static_cast<uint32_t*>(motion);
+    b->hw[0].D.pushes = static_cast<uint32_t*>(pushes);
+    return upload_world_entry(b, 0);
+}
+
+// A world with its free bodies bound steps in the plain form (the coupled
+// operator is the reference's pass sequence, fluid.wgsl:2819-2845).
+uint32_t step_flags_of(const wig_fluid* h, uint32_t flags) {
+    if (!has_bodies(h->b)) return flags;
+    return (flags | WIG_STEP_PLAIN) & ~(WIG_STEP_PERSISTENT | WIG_STEP_MIXED);
+}
+
 int wig_fluid_buffers_of(wig_fluid* h, wig_fluid_buffers* out) {
     if (!h || !h->b) return fail(WIG_E_ARG, "null argument");
     return wig_batch_buffers_of(h->b, 0, out);
@@ -1364,7 +1403,7 @@ int wig_fluid_dispatch(wig_fluid* h, const wig_params* P, int pass, uint32_t lev
 int wig_fluid_step(wig_fluid* h, const wig_params* P, uint32_t max_cycles, uint32_t flags, double tolerance, void* stream) {
     if (!h || !h->b || !P) return fail(WIG_E_ARG, "null argument");
     const uint32_t w0 = 0;
-    StepArgs a{0, &w0, 1, P, nullptr, max_cycles, flags, tolerance, (cudaStream_t)stream};
+    StepArgs a{0, &w0, 1, P, nullptr, max_cycles, step_flags_of(h, flags), tolerance, (cudaStream_t)stream};
     return batch_step(h->b, a);
 }
 
@@ -1372,7 +1411,7 @@ int wig_fluid_step_profile(wig_fluid* h, const wig_params* P, uint32_t max_cycle
                            void* stream, float* ms_out, uint32_t* calls_out) {
     if (!h || !h->b || !P) return fail(WIG_E_ARG, "null argument");
     const uint32_t w0 = 0;
-    StepArgs a{0, &w0, 1, P, nullptr, max_cycles, flags, tolerance, (cudaStream_t)stream};
+    StepArgs a{0, &w0, 1, P, nullptr, max_cycles, step_flags_of(h, flags), tolerance, (cudaStream_t)stream};
     return batch_step_profile(h->b, a, ms_out, calls_out);
 }
 

@@ -138,6 +138,8 @@ struct Dev {
     StepState* st;
     double* part64;   // 2 doubles per block: FP64 partial sums
     double* norm64;   // 2 doubles per block: FP64 norms' partials
+    uint32_t* motion; // binding 12, the free bodies' table (null: no free bodies)
+    uint32_t* pushes; // binding 16, the solve's exact sums of what it does to each body
 };
 
 struct I2 { int x, y; };

@@ -189,6 +189,235 @@ __device__ V2 prolonged(const W& w, uint32_t l, I2 c) {
     return V2{sum.x / ww, sum.y / ww};
 }
 
+// ================================================================ free bodies
+// (fluid.wgsl:1181-1470; the body table's words, js/shared.js:294-333).  The
+// pushes are exact two-word sums (common.wgsl:1378-1412) added by atomics, so
+// their totals do not depend on the order the cells add them in.
+
+constexpr uint32_t MAX_BODIES = WIG_MAX_BODIES;
+constexpr uint32_t PUSH_P0 = 0, PUSH_X = 2, PUSH_F = 3, PUSH_SURFACE = 4, PUSH_DRAG = 5;
+constexpr float EXACT_COARSE = 16777216.0f;
+constexpr int SEEP_REACH = 128;
+struct V3 { float x, y, z; };
+
+__device__ __forceinline__ uint32_t bodyWord(const W& w, uint32_t b, uint32_t k) {
+    return w.D.motion[MAX_BODIES + b * WIG_BODY_TABLE_WORDS + k];
+}
+__device__ __forceinline__ float bodyF(const W& w, uint32_t b, uint32_t k) { return __uint_as_float(bodyWord(w, b, k)); }
+__device__ __forceinline__ V2 bodyV(const W& w, uint32_t b, uint32_t k) { return V2{bodyF(w, b, k), bodyF(w, b, k + 1u)}; }
+__device__ __forceinline__ uint32_t liquidSlot(uint32_t b, uint32_t k) { return WIG_BODY_LIQUID_BASE + b * WIG_BODY_LIQUID_WORDS + k; }
+__device__ __forceinline__ bool bodyInSolve(const W& w, uint32_t b) {
+    uint32_t flags = bodyWord(w, b, WIG_BW_FLAGS);
+    return !((flags & WIG_BF_ALIVE) == 0u || (flags & WIG_BF_NEW) != 0u || bodyF(w, b, WIG_BW_MASS) <= 0.0f);
+}
+// rigidBodyOf (fluid.wgsl:1233-1248)
+__device__ uint32_t rigidBodyOf(const W& w, uint4 v) {
+    const uint32_t t = wordType(v.x);
+    const wig_elem& e = w.elem(t);
+    if (!wordHas(v.x, WIG_FL_LOOSE) || e.kind != WIG_KIND_SOLID || e.break_to == WIG_NO_ELEM) return NONE;
+    const float id = f16_value(v.w & 0xffffu);
+    if (id < 0.0f || id >= (float)MAX_BODIES) return NONE;
+    const uint32_t b = f2u(id);
+    return bodyInSolve(w, b) ? b : NONE;
+}
+__device__ __forceinline__ float rigidMass(const W& w, uint32_t b) { return bodyF(w, b, WIG_BW_MASS) + bodyF(w, b, WIG_BW_CARGO); }
+__device__ __forceinline__ float rigidInertia(const W& w, uint32_t b) {
+    return bodyF(w, b, WIG_BW_INERTIA) + bodyF(w, b, WIG_BW_CARGO_INERTIA);
+}
+__device__ __forceinline__ float bodyDensity(const W& w, uint32_t b) {
+    return rigidMass(w, b) / fmaxf((float)bodyWord(w, b, WIG_BW_CELLS), 1.0f);
+}
+__device__ __forceinline__ bool isHeld(const W& w, uint32_t b) { return (bodyWord(w, b, WIG_BW_FLAGS) & WIG_BF_HELD) != 0u; }
+// wetRegionAt (fluid.wgsl:592-595)
+__device__ bool wetRegionAt(const W& w, uint4 v) {
+    if (!w.D.motion) return false;
+    const uint32_t b = rigidBodyOf(w, v);
+    return b != NONE && (bodyWord(w, b, WIG_BW_FLAGS) & (WIG_BF_WET | WIG_BF_HELD)) == (WIG_BF_WET | WIG_BF_HELD);
+}
+// rigidAt, heldAt (fluid.wgsl:1422-1458): the body classify put in the drift's z
+__device__ uint32_t rigidAt(const W& w, I2 c) {
+    if (!w.D.motion || !w.inWorld(c)) return NONE;
+    const float z = w.fv(2u * w.cellIndex(c) + 1u)[2];
+    const uint32_t b = f2u(fmaxf(-z, 1.0f)) - 1u;
+    return (z < 0.0f && b < MAX_BODIES) ? b : NONE;
+}
+__device__ uint32_t heldAt(const W& w, I2 c) {
+    if (!w.D.motion || !w.inWorld(c)) return NONE;
+    const float z = w.fv(2u * w.cellIndex(c) + 1u)[2];
+    const uint32_t b = f2u(fmaxf(-z, 1.0f)) - 1u;
+    // (a slot past the table, from a drift word classify did not write, is none)
+    return (z < 0.0f && b >= MAX_BODIES && b < 2u * MAX_BODIES) ? b - MAX_BODIES : NONE;
+}
+// exactParts, exactValue (common.wgsl:1378-1412)
+__device__ __forceinline__ void exactParts(float x, float scale, uint32_t* lo, uint32_t* hi) {
+    const float s = rnd_even(clampf(x * scale, -9.2e18f, 9.2e18f));
+    if (fabsf(s) < 2147483648.0f) {
+        const int32_t v = f2i(s);
+        *lo = (uint32_t)v;
+        *hi = v < 0 ? 0xffffffffu : 0u;
+        return;
+    }
+    const float h = floorf(s / 4294967296.0f);
+    *lo = f2u(s - h * 4294967296.0f);
+    *hi = (uint32_t)f2i(h);
+}
+__device__ __forceinline__ float exactValue(uint32_t lo, uint32_t hi, float scale) {
+    const int32_t l = (int32_t)lo, h = (int32_t)hi;
+    if ((h == 0 && l >= 0) || (h == -1 && l < 0)) return __int2float_rn(l) / scale;
+    return (__int2float_rn(h) * 4294967296.0f + __uint2float_rn(lo)) / scale;
+}
+// pushSlot, addPush, pushOf (fluid.wgsl:1318-1338)
+__device__ __forceinline__ uint32_t pushSlot(uint32_t b, uint32_t which, uint32_t k) {
+    return b * WIG_BODY_PUSH_WORDS + 6u * which + 2u * k;
+}
+__device__ void addPush(const W& w, uint32_t b, uint32_t which, V3 v) {
+    const float c[3] = {v.x, v.y, v.z};
+    for (uint32_t k = 0; k < 3; k++) {
+        uint32_t lo, hi;
+        exactParts(c[k], EXACT_COARSE, &lo, &hi);
+        uint32_t* at = w.D.pushes + pushSlot(b, which, k);
+        const uint32_t old = atomicAdd(at, lo);
+        atomicAdd(at + 1, hi + (old + lo < old ? 1u : 0u));
+    }
+}
+__device__ V3 pushOf(const W& w, uint32_t b, uint32_t which) {
+    const uint32_t* at = w.D.pushes + pushSlot(b, which, 0u);
+    return V3{exactValue(at[0], at[1], EXACT_COARSE), exactValue(at[2], at[3], EXACT_COARSE),
+              exactValue(at[4], at[5], EXACT_COARSE)};
+}
+// giveWay, pushChange, pushChangeFree (fluid.wgsl:1348-1372)
+__device__ V3 giveWay(const W& w, uint32_t b, V3 g) {
+    if (bodyWord(w, b, WIG_BW_MOBILITY_AT) != w.D.st->P.frame - 1u)
+        return V3{g.x / rigidMass(w, b), g.y / rigidMass(w, b), g.z / rigidInertia(w, b)};
+    float m[6];
+    for (uint32_t k = 0; k < 6; k++) m[k] = bodyF(w, b, WIG_BW_MOBILITY + k);
+    return V3{m[0] * g.x + m[1] * g.y + m[2] * g.z, m[1] * g.x + m[3] * g.y + m[4] * g.z,
+              m[2] * g.x + m[4] * g.y + m[5] * g.z};
+}
+__device__ __forceinline__ V3 pushChange(const W& w, uint32_t b, uint32_t which) { return giveWay(w, b, pushOf(w, b, which)); }
+__device__ V3 pushChangeFree(const W& w, uint32_t b, uint32_t which) {
+    const V3 g = pushOf(w, b, which);
+    return V3{g.x / rigidMass(w, b), g.y / rigidMass(w, b), g.z / rigidInertia(w, b)};
+}
+// bodyFaceJ (fluid.wgsl:1374-1379): the face from cell c to body b's cell q
+__device__ V3 bodyFaceJ(const W& w, I2 c, I2 q, uint32_t b) {
+    const V2 n{(float)(q.x - c.x), (float)(q.y - c.y)};
+    const V2 pos = bodyV(w, b, WIG_BW_POS);
+    const V2 r{(((float)c.x + 0.5f) + 0.5f * n.x) - pos.x, (((float)c.y + 0.5f) + 0.5f * n.y) - pos.y};
+    return V3{n.x, n.y, r.x * n.y - r.y * n.x};
+}
+__device__ __forceinline__ V3 scale3(V3 v, float s) { return V3{v.x * s, v.y * s, v.z * s}; }
+__device__ __forceinline__ V3 add3(V3 a, V3 b) { return V3{a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ float dot3(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+// addPressurePush, couplingAt (fluid.wgsl:1381-1403)
+__device__ void addPressurePush(const W& w, I2 c, float p, uint32_t which) {
+    for (int d = 0; d < 4; d++) {
+        const I2 q = beside(c, d);
+        const uint32_t b = rigidAt(w, q);
+        if (b != NONE) addPush(w, b, which, scale3(bodyFaceJ(w, c, q, b), p));
+    }
+}
+__device__ float couplingAt(const W& w, I2 c, uint32_t which) {
+    float sum = 0.0f;
+    if (!w.D.motion) return sum;
+    for (int d = 0; d < 4; d++) {
+        const I2 q = beside(c, d);
+        const uint32_t b = rigidAt(w, q);
+        if (b != NONE) sum = sum + dot3(bodyFaceJ(w, c, q, b), pushChange(w, b, which));
+    }
+    return sum;
+}
+// rigidVel (fluid.wgsl:1460-1465), bodyMoving (fluid.wgsl:1410-1419)
+__device__ V2 rigidVel(const W& w, uint32_t b, V2 x) {
+    const V2 pos = bodyV(w, b, WIG_BW_POS);
+    const V2 r{x.x - pos.x, x.y - pos.y};
+    const float spin = bodyF(w, b, WIG_BW_SPIN);
+    const V2 v = bodyV(w, b, WIG_BW_VEL);
+    return V2{v.x + -spin * r.y, v.y + spin * r.x};
+}
+__device__ V2 bodyMoving(const W& w, uint32_t b, V2 x, bool drag) {
+    const V2 pos = bodyV(w, b, WIG_BW_POS);
+    const V2 pull = w.pull();
+    const float m = rigidMass(w, b);
+    V3 ch = add3(pushChange(w, b, PUSH_SURFACE), giveWay(w, b, V3{m * pull.x, m * pull.y, 0.0f}));
+    if (drag) ch = add3(ch, pushChange(w, b, PUSH_DRAG));
+    const V2 r{x.x - pos.x, x.y - pos.y};
+    const V2 rv = rigidVel(w, b, x);
+    const V2 px = w.pull();
+    return V2{(((rv.x + px.x) - pull.x) + ch.x) + -ch.z * r.y, (((rv.y + px.y) - pull.y) + ch.y) + ch.z * r.x};
+}
+// bodyReach (fluid.wgsl:413-415)
+__device__ float bodyReach(const W& w, uint32_t b, I2 n) {
+    const uint32_t s = bodyWord(w, b, WIG_BW_SUBCELL);
+    const float sx = f16_value(s & 0xffffu), sy = f16_value(s >> 16);
+    return clampf(0.5f + (sx * (float)n.x + sy * (float)n.y), 0.0f, 1.0f);
+}
+// posedRoom (fluid.wgsl:2035-2045)
+__device__ float posedRoom(const W& w, I2 c) {
+    float room = 1.0f;
+    for (int d = 0; d < 4; d++) {
+        const I2 q = beside(c, d);
+        const uint32_t b = rigidAt(w, q);
+        if (b != NONE) room = room + (0.5f - bodyReach(w, b, I2{c.x - q.x, c.y - q.y}));
+    }
+    return clampf(room, 0.1f, 1.9f);
+}
+// faceMiddle (fluid.wgsl:1473-1475)
+__device__ __forceinline__ V2 faceMiddle(I2 at, bool isU) {
+    return isU ? V2{(float)at.x + 0.0f, (float)at.y + 0.5f} : V2{(float)at.x + 0.5f, (float)at.y + 0.0f};
+}
+// potentialAt (fluid.wgsl:2958-2960): the masses' potential none (binding 10 unbound)
+__device__ __forceinline__ float potentialAt(const W& w, V2 pos) {
+    return w.D.st->P.earth_g * ((float)w.D.H - pos.y) + 0.0f;
+}
+// seepAt (fluid.wgsl:2977-3000)
+__device__ float seepAt(const W& w, I2 c, I2 n, uint32_t h, bool held, V2 x) {
+    I2 ways[2] = {I2{-1, 0}, I2{1, 0}};
+    int count = 2;
+    if (n.x != 0) {
+        ways[0] = I2{-n.x, -n.y};
+        count = 1;
+    }
+    int nearest = SEEP_REACH + 1;
+    float p = 0.0f;
+    for (int k2 = 0; k2 < count; k2++) {
+        for (int k = 1; k < nearest; k++) {
+            const I2 q{c.x + ways[k2].x * k, c.y + ways[k2].y * k};
+            if ((held ? heldAt(w, q) : rigidAt(w, q)) == h) continue;
+            const float4 g = w.gridAt(q);
+            if (g.z > 0.0f) {
+                nearest = k;
+                p = g.x + g.z * (potentialAt(w, V2{(float)q.x + 0.5f, (float)q.y + 0.5f}) - potentialAt(w, x));
+            }
+            break;
+        }
+    }
+    return p;
+}
+// heldPush (fluid.wgsl:3007-3031)
+__device__ void heldPush(const W& w, I2 c, uint32_t h, int32_t out[3]) {
+    const V2 pos = bodyV(w, h, WIG_BW_POS);
+    V2 f{0.0f, 0.0f};
+    float torque = 0.0f;
+    for (int d = 0; d < 4; d++) {
+        const I2 q = beside(c, d);
+        const I2 n{q.x - c.x, q.y - c.y};
+        if (heldAt(w, q) == h) continue;
+        const float4 g = w.gridAt(q);
+        const V2 x{((float)c.x + 0.5f) + 0.5f * (float)n.x, ((float)c.y + 0.5f) + 0.5f * (float)n.y};
+        float p = g.x;
+        if (g.z > 0.0f) p = p + g.z * (potentialAt(w, V2{(float)q.x + 0.5f, (float)q.y + 0.5f}) - potentialAt(w, x));
+        else if (g.z < 0.0f) p = seepAt(w, c, n, h, true, x);
+        const V2 push{-p * (float)n.x, -p * (float)n.y};
+        f = V2{f.x + push.x, f.y + push.y};
+        const V2 r{x.x - pos.x, x.y - pos.y};
+        torque = torque + (r.x * push.y - r.y * push.x);
+    }
+    out[0] = f2i(rnd_even((f.x / rigidMass(w, h)) * WIG_RIGID_FIX));
+    out[1] = f2i(rnd_even((f.y / rigidMass(w, h)) * WIG_RIGID_FIX));
+    out[2] = f2i(rnd_even((torque / rigidInertia(w, h)) * WIG_RIGID_FIX));
+}
+
 // ================================================================ bookkeeping
 
 // sync / syncMarks (fluid.wgsl:608-659): a CTA per block of the world
@@ -201,7 +430,7 @@ __global__ void k_sync(Batch Bt, int sync_claims) {
     const bool claims = sync_claims && D.st->book == 0u;
     const I2 b = w.blockAt(n);
     I2 c{b.x * BLOCK + (int)(threadIdx.x & 7u), b.y * BLOCK + (int)(threadIdx.x >> 3)};
-    bool here = false;
+    bool here = false, region = false;
     if (w.inWorld(c)) {
         uint32_t i = w.cellIndex(c);
         if (i == 0u) {
@@ -215,9 +444,12 @@ __global__ void k_sync(Batch Bt, int sync_claims) {
             uint32_t home = liquidHome(v.w);
             if (claims && wordHas(v.x, FL_DRAWN) && home < D.C) atomicMax(w.gwp(home, G_DEST), claimOf(i));
             here = true;
+        } else if (wetRegionAt(w, v)) {
+            region = true;
         }
     }
     if (__syncthreads_or(here) && threadIdx.x == 0) atomicOr(&D.blocks[n], MARK_LIQUID);
+    if (__syncthreads_or(region) && threadIdx.x == 0) atomicOr(&D.blocks[n], MARK_REGION);
   }
 }
 
@@ -853,8 +1085,15 @@ __global__ void k_classify(Batch Bt) {
             float4 was = w.f4(2u * i), wasDrift = w.f4(2u * i + 1u);
             bool sealed = false;
             if (n == 0 && mayBeSealed(w, p)) sealed = (vload(w.gwp(ufFind(w, i), G_REGION)) & REGION_OPEN) == 0u;
+            uint32_t rigid = NONE, held = NONE;
             if (n < 0) {
                 c.z = -1.0f;
+                // a free body's cell (fluid.wgsl:1614-1627; no cups: binding 14 unbound)
+                if (D.motion) rigid = rigidBodyOf(w, w.cell(i));
+                if (rigid != NONE && isHeld(w, rigid)) {
+                    held = rigid;
+                    rigid = NONE;
+                }
             } else if (n > 0) {
                 V2 li = liquidIn(w, i);
                 c = make_float4(0.0f, 0.0f, li.x, li.y);
@@ -875,8 +1114,10 @@ __global__ void k_classify(Batch Bt) {
                 if (fluid >= 2.0f && fluid + wallsN >= 3.0f) c = make_float4(0.0f, 0.0f, mean.x / fluid, mean.y / fluid);
                 else if (sealed) c = fluid > 0.0f ? make_float4(0.0f, 0.0f, mean.x / fluid, mean.y / fluid) : make_float4(0.0f, 0.0f, 1.0f, 0.0f);
             }
-            uint32_t liquid = c.z > 0.0f ? mine : 0u;
+            uint32_t liquid = (c.z > 0.0f || rigid != NONE || held != NONE) ? mine : 0u;
             float4 drift = make_float4(0.0f, 0.0f, sealed ? 1.0f : 0.0f, (float)((f2u(wasDrift.w) & ~(mine | fall0)) | liquid));
+            if (rigid != NONE) drift.z = -1.0f - (float)rigid;
+            else if (held != NONE) drift.z = -1.0f - (float)(held + MAX_BODIES);
             if (c.z > 0.0f) {
                 if (was.z > 0.0f) {
                     c.x = was.x;
@@ -923,12 +1164,41 @@ __device__ float lastPush(const W& w, I2 a, I2 at, float4 ga, float4 gb) {
     return fineBeta(ga.z, gb.z, w.densityAt(a), w.densityAt(at)) * (gb.x - ga.x);
 }
 
+// setBodyFace (fluid.wgsl:1840-1859)
+__device__ void setBodyFace(const W& w, uint32_t f, I2 at, bool isU, float4 ga, float4 gb, uint32_t ra, uint32_t rb,
+                            bool drag) {
+    const V2 x = faceMiddle(at, isU);
+    float now = 0.0f, u = 0.0f;
+    if (ra != NONE && rb != NONE) {
+        const V2 ma = bodyMoving(w, ra, x, drag), mb = bodyMoving(w, rb, x, drag);
+        const V2 va = rigidVel(w, ra, x), vb = rigidVel(w, rb, x);
+        now = 0.5f * (isU ? ma.x + mb.x : ma.y + mb.y);
+        u = 0.5f * (isU ? va.x + vb.x : va.y + vb.y);
+    } else {
+        const uint32_t b = ra != NONE ? ra : rb;
+        const V2 m = bodyMoving(w, b, x, drag), v = rigidVel(w, b, x);
+        now = isU ? m.x : m.y;
+        u = isU ? v.x : v.y;
+    }
+    const float4 other = ra != NONE ? gb : ga;
+    const float nu = ((ra == NONE || rb == NONE) && other.z > 0.0f) ? other.w : 0.0f;
+    reinterpret_cast<float4*>(w.D.field)[w.faceSlot(f)] = make_float4(now, u, 1.0f, nu);
+    *w.viscRhsP(f) = now;
+}
+
 // setFace (fluid.wgsl:1936-1980), no air bound: no wind drag.
 __device__ void setFace(const W& w, I2 at, bool isU) {
     uint32_t f = w.faceIndex(at, isU);
     I2 a = isU ? I2{at.x - 1, at.y} : I2{at.x, at.y - 1};
     int axis = isU ? 0 : 1;
     float4 ga = w.gridAt(a), gb = w.gridAt(at);
+    if (w.D.motion) {
+        const uint32_t ra = rigidAt(w, a), rb = rigidAt(w, at);
+        if (ra != NONE || rb != NONE) {
+            setBodyFace(w, f, at, isU, ga, gb, ra, rb, false);
+            return;
+        }
+    }
     uint32_t slot = w.sumSlot(f);
     int32_t weight = (int32_t)w.D.counters[slot + 1u];
     float u = 0.0f, held = 0.0f;
@@ -971,17 +1241,23 @@ __global__ void k_setFaces(Batch Bt) {
     }
 }
 
-// viscousFace (fluid.wgsl:3347-3403), no bodies.
+// viscousFace (fluid.wgsl:3347-3403)
 __device__ void viscousFace(const W& w, I2 at, bool isU, int color) {
     if (((at.x + at.y) & 1) != color) return;
     I2 a = isU ? I2{at.x - 1, at.y} : I2{at.x, at.y - 1};
     float4 ga = w.gridAt(a), gb = w.gridAt(at);
-    if (ga.z < 0.0f || gb.z < 0.0f) return;
+    const uint32_t ra = rigidAt(w, a), rb = rigidAt(w, at);
+    const bool surface = (ra != NONE) != (rb != NONE) && (ra != NONE ? gb.z : ga.z) > 0.0f;
+    if (!surface && (ga.z < 0.0f || gb.z < 0.0f || ra != NONE || rb != NONE)) return;
     uint32_t fi = w.faceIndex(at, isU);
     float* fp = w.fv(w.faceSlot(fi));
     float nu = fp[3];
     if (nu <= 0.0f) return;
     float heavy = 1.0f;
+    if (surface) {
+        const float liquid = ra != NONE ? gb.z : ga.z;
+        heavy = 2.0f * liquid / (liquid + bodyDensity(w, ra != NONE ? ra : rb));
+    }
     float tx = ga.z > 0.0f ? ga.w : 0.0f, ty = gb.z > 0.0f ? gb.w : 0.0f;
     float sum = 0.0f, n = 0.0f;
     for (int d = 0; d < 4; d++) {
@@ -1021,7 +1297,7 @@ __global__ void k_viscosity(Batch Bt, int color) {
             I2 a = isU ? I2{at.x - 1, at.y} : I2{at.x, at.y - 1};
             float4 ga = w.gridAt(a), gb = w.gridAt(at);
             uint32_t fi = w.faceIndex(at, isU);
-            if (faceViscosity(ga, gb) > 0.0f) {
+            if (rigidAt(w, a) == NONE && rigidAt(w, at) == NONE && faceViscosity(ga, gb) > 0.0f) {
                 float* fp = w.fv(w.faceSlot(fi));
                 *w.viscLastP(fi) = fp[0] - *w.viscRhsP(fi);
                 fp[0] = fp[0] + lastPush(w, a, at, ga, gb);
@@ -1032,7 +1308,7 @@ __global__ void k_viscosity(Batch Bt, int color) {
     }
 }
 
-// divergence (fluid.wgsl:1996-2025), posedRoom 1 with no bodies.
+// divergence (fluid.wgsl:1996-2025)
 __global__ void k_divergence(Batch Bt) {
     __shared__ WorldCopy wc_;
     worldCopyInit(wc_);
@@ -1055,7 +1331,7 @@ __global__ void k_divergence(Batch Bt) {
                     w.fv(w.faceSlot(w.vFace(c.x, c.y + 1)))[0] - w.fv(w.faceSlot(w.vFace(c.x, c.y)))[0];
         w.fv(2u * i)[1] = out;
         float n = w.densityAt(c);
-        float room = clampf(1.0f, 0.1f, 1.9f);
+        float room = posedRoom(w, c);
         w.fv(2u * i + 1u)[1] = w.fv(2u * i + 1u)[2] < 0.0f ? 0.0f : -SPREAD * (n - room);
     }
 }
@@ -1191,7 +1467,7 @@ __global__ void k_cgResidual(Dev D) {
         double b2 = 0.0;
         if (w.inWorld(c) && w.gridAt(c).z > 0.0f) {
             uint32_t i = w.cellIndex(c);
-            D.cg[4u * (size_t)i + 1u] = -residualAt(w, 0, c).x - 0.0f;
+            D.cg[4u * (size_t)i + 1u] = -residualAt(w, 0, c).x - couplingAt(w, c, PUSH_X);
             double b = (double)w.fv(2u * i)[1];
             b2 = b * b;
         }
@@ -1609,6 +1885,13 @@ __global__ void __launch_bounds__(256) k_cgBeta(Dev D, uint32_t cycle) {
     __shared__ float sx[256], sy[256];
     __shared__ double s64[256];
     if (w.converged(cycle) || w.activeCount() == 0u) return;
+    // the bodies' sums of this iteration's direction, done with, emptied for
+    // the iteration after next (fluid.wgsl:2808-2813)
+    if (D.pushes) {
+        const uint32_t which = PUSH_P0 + cycle % 2u;
+        for (uint32_t k = threadIdx.x; k < MAX_BODIES * 6u; k += blockDim.x)
+            D.pushes[pushSlot(k / 6u, which, 0u) + k % 6u] = 0u;
+    }
     float* at = D.cg + 4u * (size_t)(D.C + D.B);
     if (D.st->f64) {
         double rz = sumBlocks64(w, D.part64, 0, s64);
@@ -1682,7 +1965,7 @@ __global__ void __launch_bounds__(64) k_cgApply(Dev D, uint32_t cycle) {
         if (w.inWorld(c)) {
             float rho = w.gridAt(c).z;
             uint32_t i = w.cellIndex(c);
-            float q = rho > 0.0f ? applyA(w, c, rho) + 0.0f : 0.0f;
+            float q = rho > 0.0f ? applyA(w, c, rho) + couplingAt(w, c, PUSH_P0 + cycle % 2u) : 0.0f;
             float* g = D.cg + 4u * (size_t)i;
             g[3] = q;
             vx = g[2] * q;
@@ -1790,7 +2073,7 @@ __global__ void k_cgFinish(Dev D) {
 
 // ================================================================ projection, extrapolation
 
-// project / projectFace (fluid.wgsl:2897-2942), no bodies.
+// project / projectFace (fluid.wgsl:2897-2942)
 __global__ void k_project(Batch Bt) {
     __shared__ WorldCopy wc_;
     worldCopyInit(wc_);
@@ -1817,11 +2100,24 @@ __global__ void k_project(Batch Bt) {
             I2 a = isU ? I2{at.x - 1, at.y} : I2{at.x, at.y - 1};
             float4 ga = w.gridAt(a), gb = w.gridAt(at);
             float beta = fineBeta(ga.z, gb.z, w.densityAt(a), w.densityAt(at));
+            const uint32_t ra = rigidAt(w, a), rb = rigidAt(w, at);
             if (beta > 0.0f) {
                 float4 face = *fp;
                 face.x = face.x - beta * (gb.x - ga.x);
                 face.z = PROJECTED;
-                face.w = clampf(-beta * (w.driftAt(at) - w.driftAt(a)), -MAX_DRIFT, MAX_DRIFT);
+                const bool rigid = ra != NONE || rb != NONE;
+                face.w = rigid ? 0.0f : clampf(-beta * (w.driftAt(at) - w.driftAt(a)), -MAX_DRIFT, MAX_DRIFT);
+                *fp = face;
+            }
+            // a face between the liquid and a free body moves with the body's push (PUSH_F)
+            if ((ra == NONE) != (rb == NONE) && (ra != NONE ? gb.z : ga.z) > 0.0f) {
+                const uint32_t bb = ra != NONE ? ra : rb;
+                const V3 ch = pushChange(w, bb, PUSH_F);
+                const V2 m = faceMiddle(at, isU), pos = bodyV(w, bb, WIG_BW_POS);
+                const V2 r{m.x - pos.x, m.y - pos.y};
+                float4 face = *fp;
+                face.x = face.x + (isU ? ch.x - ch.z * r.y : ch.y + ch.z * r.x);
+                face.z = PROJECTED;
                 *fp = face;
             }
         }
@@ -2347,6 +2643,161 @@ __global__ void k_unpaint(Batch Bt) {
 
 // ================================================================ launch
 
+// ================================================================ the bodies' passes (world 0)
+
+// bodyStart (fluid.wgsl:3079-3084)
+__global__ void k_bodyStart(Dev D) {
+    const uint32_t n = MAX_BODIES * WIG_BODY_PUSH_WORDS;
+    for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) D.pushes[k] = 0u;
+}
+
+// seepLoads, bodyLoads (fluid.wgsl:3094-3139)
+__device__ void seepLoads(const W& w, I2 c, uint32_t b) {
+    for (int d = 0; d < 4; d++) {
+        const I2 q = beside(c, d);
+        if (!w.inWorld(q) || rigidAt(w, q) == b || w.gridAt(q).z >= 0.0f) continue;
+        const I2 n{q.x - c.x, q.y - c.y};
+        const V2 x{((float)c.x + 0.5f) + 0.5f * (float)n.x, ((float)c.y + 0.5f) + 0.5f * (float)n.y};
+        addPush(w, b, PUSH_SURFACE, scale3(bodyFaceJ(w, q, c, b), seepAt(w, c, n, b, false, x)));
+    }
+}
+__global__ void __launch_bounds__(64) k_bodyLoads(Dev D) {
+    W w(D);
+    FOR_ACTIVE(D, w, wid) {
+        const I2 c = lidCell(w, wid);
+        if (!w.inWorld(c)) continue;
+        const uint32_t own = rigidAt(w, c);
+        if (own != NONE) {
+            seepLoads(w, c, own);
+            continue;
+        }
+        const float4 g = w.gridAt(c);
+        if (g.z <= 0.0f) continue;
+        const V2 mid{(float)c.x + 0.5f, (float)c.y + 0.5f};
+        for (int d = 0; d < 4; d++) {
+            const I2 q = beside(c, d);
+            const uint32_t b = rigidAt(w, q);
+            if (b == NONE) continue;
+            const I2 n{q.x - c.x, q.y - c.y};
+            const float reach = 1.0f - bodyReach(w, b, I2{-n.x, -n.y});
+            const V2 surface{mid.x + (float)n.x * reach, mid.y + (float)n.y * reach};
+            addPush(w, b, PUSH_SURFACE,
+                    scale3(scale3(bodyFaceJ(w, c, q, b), g.z), potentialAt(w, mid) - potentialAt(w, surface)));
+        }
+    }
+}
+
+// bodyDrag (fluid.wgsl:3149-3176)
+__global__ void __launch_bounds__(64) k_bodyDrag(Dev D) {
+    W w(D);
+    FOR_ACTIVE(D, w, wid) {
+        const I2 c = lidCell(w, wid);
+        const uint32_t b = rigidAt(w, c);
+        if (!w.inWorld(c) || b == NONE) continue;
+        const V2 pos = bodyV(w, b, WIG_BW_POS);
+        const float rho = bodyDensity(w, b);
+        V3 push{0.0f, 0.0f, 0.0f};
+        for (int k = 0; k < 4; k++) {
+            const bool isU = k < 2;
+            const int sg = (k & 1) == 1 ? 1 : -1;
+            const I2 n = isU ? I2{sg, 0} : I2{0, sg};
+            if (w.gridAt(I2{c.x + n.x, c.y + n.y}).z <= 0.0f) continue;
+            const I2 at = isU ? I2{c.x + (k & 1), c.y} : I2{c.x, c.y + (k & 1)};
+            const V2 x = faceMiddle(at, isU);
+            const V2 mv = bodyMoving(w, b, x, false);
+            const float du = (bodyReach(w, b, n) * rho) * (w.fv(w.faceSlot(w.faceIndex(at, isU)))[0] - (isU ? mv.x : mv.y));
+            const V2 r{x.x - pos.x, x.y - pos.y};
+            if (isU) push.x = push.x + du;
+            else push.y = push.y + du;
+            push.z = push.z + (isU ? -r.y * du : r.x * du);
+        }
+        if (push.x != 0.0f || push.y != 0.0f || push.z != 0.0f) addPush(w, b, PUSH_DRAG, push);
+    }
+}
+
+// bodyFaces (fluid.wgsl:3180-3200)
+__global__ void __launch_bounds__(64) k_bodyFaces(Dev D) {
+    W w(D);
+    FOR_ACTIVE(D, w, wid) {
+        const I2 c = lidCell(w, wid);
+        if (!w.inWorld(c)) continue;
+        int fs[4][3];
+        w.facesOf(c, fs);
+        for (int j = 0; j < 4; j++) {
+            if (fs[j][2] < 0) continue;
+            const I2 at{fs[j][0], fs[j][1]};
+            const bool isU = fs[j][2] == 1;
+            const I2 a = isU ? I2{at.x - 1, at.y} : I2{at.x, at.y - 1};
+            const uint32_t ra = rigidAt(w, a), rb = rigidAt(w, at);
+            if (ra != NONE || rb != NONE) setBodyFace(w, w.faceIndex(at, isU), at, isU, w.gridAt(a), w.gridAt(at), ra, rb, true);
+        }
+    }
+}
+
+// cgBodyX, cgBodyP, cgBodyF (fluid.wgsl:2819-2845): the pressure's push on
+// the bodies beside each liquid cell, of the solve's start (x), of this
+// iteration's direction (p, into the set of the iteration's parity) and of
+// the pressure it ends with.
+__global__ void __launch_bounds__(64) k_cgBody(Dev D, int which, uint32_t cycle) {
+    W w(D);
+    if (which == 1 && w.converged(cycle)) return;
+    FOR_ACTIVE(D, w, wid) {
+        const I2 c = lidCell(w, wid);
+        if (!w.inWorld(c) || w.gridAt(c).z <= 0.0f) continue;
+        const uint32_t i = w.cellIndex(c);
+        if (which == 0) addPressurePush(w, c, D.cg[4u * (size_t)i], PUSH_X);
+        else if (which == 1) addPressurePush(w, c, D.cg[4u * (size_t)i + 2u], PUSH_P0 + cycle % 2u);
+        else addPressurePush(w, c, w.fv(2u * i)[0], PUSH_F);
+    }
+}
+
+// rigidify (fluid.wgsl:3033-3076): each block's cells of its lowest held
+// body summed in shared memory and added once, the others' straight into
+// their bodies' words (integer adds: the totals are the same in any order).
+__global__ void __launch_bounds__(64) k_rigidify(Dev D) {
+    W w(D);
+    __shared__ uint32_t first;
+    __shared__ uint32_t sums[3];
+    FOR_ACTIVE(D, w, wid) {
+        if (threadIdx.x == 0) {
+            first = NONE;
+            sums[0] = sums[1] = sums[2] = 0u;
+        }
+        __syncthreads();
+        const I2 c = lidCell(w, wid);
+        const uint32_t h = heldAt(w, c);
+        if (h != NONE) atomicMin(&first, h);
+        __syncthreads();
+        const uint32_t f0 = first;
+        if (h != NONE) {
+            int32_t d[3];
+            heldPush(w, c, h, d);
+            if ((D.blocks[w.stateSlot(w.blockIndex(w.activeBlock(wid)))] & NEAR_LIQUID) != 0u)
+                atomicOr(&D.motion[liquidSlot(h, 3u)], WIG_LIQUID_WET);
+            for (uint32_t k = 0; k < 3; k++) {
+                if (h == f0) atomicAdd(&sums[k], (uint32_t)d[k]);
+                else atomicAdd(&D.motion[liquidSlot(h, k)], (uint32_t)d[k]);
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0 && f0 != NONE)
+            for (uint32_t k = 0; k < 3; k++) atomicAdd(&D.motion[liquidSlot(f0, k)], sums[k]);
+        __syncthreads();
+    }
+}
+
+// bodyPush (fluid.wgsl:3205-3218): a thread a body.
+__global__ void k_bodyPush(Dev D) {
+    W w(D);
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= MAX_BODIES) return;
+    const V3 ch = add3(add3(pushChangeFree(w, b, PUSH_SURFACE), pushChangeFree(w, b, PUSH_DRAG)), pushChangeFree(w, b, PUSH_F));
+    if (ch.x == 0.0f && ch.y == 0.0f && ch.z == 0.0f) return;
+    atomicAdd(&D.motion[liquidSlot(b, 0u)], (uint32_t)f2i(rnd_even(ch.x * WIG_RIGID_FIX)));
+    atomicAdd(&D.motion[liquidSlot(b, 1u)], (uint32_t)f2i(rnd_even(ch.y * WIG_RIGID_FIX)));
+    atomicAdd(&D.motion[liquidSlot(b, 2u)], (uint32_t)f2i(rnd_even(ch.z * WIG_RIGID_FIX)));
+}
+
 static inline unsigned block_grid(const Dev& D, unsigned per_sm) {
     unsigned g = 148u * per_sm;
     return D.B < g ? (D.B ? D.B : 1u) : g;
@@ -2419,7 +2870,23 @@ int launch_pass(const Batch& Bt, const BatchShape& S, const Dev& D0, int pass, u
     case WIG_PASS_RASTER_CLAIMS: k_rasterClaims<<<A, 64, 0, s>>>(Bt); break;
     case WIG_PASS_RASTER: k_raster<<<A, 64, 0, s>>>(Bt); break;
     case WIG_PASS_UNPAINT: k_unpaint<<<A, 64, 0, s>>>(Bt); break;
-    default: return WIG_E_ARG;
+    default:
+        // the bodies' passes: world 0 with its bodies bound (no-ops without)
+        if (pass < WIG_PASS_BODY_START || pass > WIG_PASS_BODY_PUSH) return WIG_E_ARG;
+        if (!D.motion || !D.pushes) return WIG_OK;
+        switch (pass) {
+        case WIG_PASS_BODY_START: k_bodyStart<<<(MAX_BODIES * WIG_BODY_PUSH_WORDS + 255u) / 256u, 256, 0, s>>>(D); break;
+        case WIG_PASS_BODY_LOADS: k_bodyLoads<<<G, 64, 0, s>>>(D); break;
+        case WIG_PASS_BODY_DRAG: k_bodyDrag<<<G, 64, 0, s>>>(D); break;
+        case WIG_PASS_BODY_FACES: k_bodyFaces<<<G, 64, 0, s>>>(D); break;
+        case WIG_PASS_CG_BODY_X: k_cgBody<<<G, 64, 0, s>>>(D, 0, cycle); break;
+        case WIG_PASS_CG_BODY_P: k_cgBody<<<G, 64, 0, s>>>(D, 1, cycle); break;
+        case WIG_PASS_CG_BODY_F: k_cgBody<<<G, 64, 0, s>>>(D, 2, cycle); break;
+        case WIG_PASS_RIGIDIFY: k_rigidify<<<G, 64, 0, s>>>(D); break;
+        case WIG_PASS_BODY_PUSH: k_bodyPush<<<(MAX_BODIES + 255u) / 256u, 256, 0, s>>>(D); break;
+        default: break;
+        }
+        break;
     }
     return WIG_OK;
 }

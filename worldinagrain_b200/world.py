@@ -18,6 +18,7 @@ New liquid is painted as undrawn WATER cells, and the first step's syncSeed
 (shaders/fluid.wgsl:863-890) turns each into LIQUID_PER_CELL particles, as a
 scene painted by js/scenes.js is (`dam`, js/scenes.js:404-407).
 """
+import ctypes as C
 import math
 import struct
 
@@ -46,7 +47,7 @@ def element_table():
         base = dict(kind=abi.KIND_SOLID, density=1000.0, weight=GRAVITY, heat_cap=2.0, viscosity=0.0,
                     viscosity_t=20.0, viscosity_e=0.0, tension=0.0, expansion=0.0, expansion2=0.0,
                     hi_t=T_NEVER, lo_t=-T_NEVER, up_span=1e30, down_span=1e30, down_scale=0.0,
-                    sol_density=0.0, flags=0, wetting=0.5)
+                    sol_density=0.0, flags=0, wetting=0.5, break_to=abi.NO_ELEM)
         base.update(kw)
         for k, v in base.items():
             setattr(e, k, v)
@@ -321,3 +322,128 @@ def small_world(width=32, height=32, seed=7, kind="dam"):
     w.paint(water, abi.WATER, vel=vel)
     w.config = dict(workload=f"small_{kind}", grid=f"{width}x{height}", seed=seed, earth_g=earth_g_cells())
     return w
+
+
+# ---------------------------------------------------------------- free bodies
+
+WOOD = 5  # a structural solid of this table's own that the test bodies are made of
+
+
+def body_element_table():
+    """element_table() and a sixth row: a structural solid lighter than water
+    on the lines of the reference's wood (density 60, breakTo an element,
+    js/elements.js:608-614).  A breakTo is what lets a loose cell of it be a
+    free body's (fluid.wgsl:1233-1248); SAND stands in for the sawdust this
+    table does not have."""
+    base = element_table()
+    rows = (abi.Elem * 6)()
+    for k in range(5):
+        C.memmove(C.byref(rows[k]), C.byref(base[k]), C.sizeof(abi.Elem))
+    C.memmove(C.byref(rows[WOOD]), C.byref(base[abi.WALL]), C.sizeof(abi.Elem))
+    rows[WOOD].density = 60.0
+    rows[WOOD].break_to = abi.SAND
+    return rows
+
+
+class Bodies:
+    """A free-body table (binding 12, `motion`) and the solve's push sums
+    (binding 16, `pushes`) in the reference's layouts (js/shared.js:294-333),
+    host side.  The liquid step reads a body's pose, motion, mass and flags
+    and adds what it does to the body into the body's liquid words."""
+
+    def __init__(self):
+        self.motion = np.zeros(abi.BODY_MOTION_WORDS, dtype=np.uint32)
+        self.pushes = np.zeros(abi.MAX_BODIES * abi.BODY_PUSH_WORDS, dtype=np.uint32)
+
+    def words(self, b):
+        at = abi.MAX_BODIES + b * abi.BODY_TABLE_WORDS
+        return self.motion[at:at + abi.BODY_TABLE_WORDS]
+
+    def liquid(self, b):
+        """The body's liquid words: its change in velocity x, y and spin in
+        RIGID_FIX fixed point (i32), and the wet word."""
+        at = abi.BODY_LIQUID_BASE + b * abi.BODY_LIQUID_WORDS
+        return self.motion[at:at + abi.BODY_LIQUID_WORDS]
+
+    def set_f32(self, b, k, *values):
+        self.words(b)[k:k + len(values)] = np.asarray(values, dtype=np.float32).view(np.uint32)
+
+    def copy(self):
+        o = Bodies.__new__(Bodies)
+        o.motion = self.motion.copy()
+        o.pushes = self.pushes.copy()
+        return o
+
+
+def stamp_body(world, bodies, b, mask, density, vel=(0.0, 0.0), spin=0.0, subcell=(0.0, 0.0), flags=abi.BF_ALIVE,
+               mobility=None, mobility_at=0xffffffff):
+    """Body b's cells (mask, H x W) stamped as loose WOOD cells carrying its
+    slot in frac.x (shaders/common.wgsl:113-160), and its table slot: pose
+    at the cells' centre of mass, velocity and spin, mass (density in water
+    cells a cell) and moment of inertia about the centre, flags, the pose's
+    sub-cell offset, and optionally a contact mobility (6 f32 of a symmetric
+    3 x 3) worked out at step mobility_at."""
+    ys, xs = np.nonzero(mask)
+    cx, cy = xs + 0.5, ys + 0.5
+    n = len(xs)
+    m = np.float32(density) * np.float32(n)
+    pos = (np.float32(cx.mean()), np.float32(cy.mean()))
+    inertia = np.float32(density * np.sum((cx - pos[0]) ** 2 + (cy - pos[1]) ** 2 + 1.0 / 6.0))
+    cv = world.cell_view()
+    cv[mask, 0] = WOOD | (abi.FL_LOOSE << 28)
+    cv[mask, 1] = f32_bits(world.temperature)
+    cv[mask, 2] = 0
+    cv[mask, 3] = f16x2(np.full(n, float(b)), np.zeros(n))
+    bodies.set_f32(b, abi.BW["POS"], *pos)
+    bodies.set_f32(b, abi.BW["VEL"], *vel)
+    bodies.set_f32(b, abi.BW["SPIN"], spin)
+    bodies.set_f32(b, abi.BW["MASS"], m)
+    bodies.set_f32(b, abi.BW["INERTIA"], inertia)
+    bodies.words(b)[abi.BW["CELLS"]] = n
+    bodies.words(b)[abi.BW["FLAGS"]] = flags
+    bodies.words(b)[abi.BW["SUBCELL"]] = f16x2(np.array([subcell[0]]), np.array([subcell[1]]))[0]
+    if mobility is not None:
+        bodies.set_f32(b, abi.BW["MOBILITY"], *mobility)
+    bodies.words(b)[abi.BW["MOBILITY_AT"]] = mobility_at & 0xffffffff
+
+
+def bodies_world(width=96, height=80, seed=6, liquid=abi.WATER):
+    """A tank of water with synthetic free bodies in it (none of the
+    reference's configs has any): a plank afloat at the surface, moving and
+    spinning, with a sub-cell pose; a block under the water whose contact
+    mobility was worked out the step before the first; a heavy block held
+    on the floor, wet; a body just found (NEW, a wall until weighed); and
+    cells of a slot that is not alive.  liquid: the tank's liquid (MUD for
+    the viscous sweeps and the liquid's drag on the bodies).  Returns
+    (world, bodies)."""
+    rng = np.random.default_rng(seed)
+    w = World(width, height)
+    bodies = Bodies()
+    wall = np.zeros((height, width), dtype=bool)
+    wall[-1, :] = True
+    wall[:, 0] = wall[:, -1] = True
+    w.paint(wall, abi.WALL)
+    surface = height // 3
+    used = wall.copy()
+
+    def box(x0, y0, bw, bh):
+        m = np.zeros((height, width), dtype=bool)
+        m[y0:y0 + bh, x0:x0 + bw] = True
+        assert not np.any(m & used)
+        used[m] = True
+        return m
+
+    stamp_body(w, bodies, 0, box(width // 6, surface - 1, 14, 3), 0.6, vel=(0.05, 0.03), spin=0.002,
+               subcell=(0.25, -0.125))
+    stamp_body(w, bodies, 1, box(width // 2, surface + 12, 6, 6), 0.9, vel=(-0.02, 0.01), spin=-0.001,
+               subcell=(-0.1875, 0.0625), mobility=(0.5, 0.01, 0.002, 0.45, -0.003, 0.02), mobility_at=0)
+    stamp_body(w, bodies, 2, box(width // 2 + 14, height - 5, 10, 4), 7.8, flags=abi.BF_ALIVE | abi.BF_HELD | abi.BF_WET)
+    stamp_body(w, bodies, 3, box(width // 6 + 4, height - 12, 4, 4), 0.6, flags=abi.BF_ALIVE | abi.BF_NEW)
+    stamp_body(w, bodies, 4, box(width - 14, surface + 4, 3, 5), 0.6, flags=0)
+    water = np.zeros((height, width), dtype=bool)
+    water[surface:height - 1, 1:width - 1] = True
+    water &= ~used
+    vel = rng.normal(0.0, 0.3, (height, width, 2)).astype(np.float32)
+    w.paint(water, liquid, vel=vel)
+    w.config = dict(workload="bodies_tank", grid=f"{width}x{height}", seed=seed, earth_g=earth_g_cells())
+    return w, bodies
