@@ -33,12 +33,13 @@ def _body_diffs(got, ref):
     return out
 
 
-def _sequence(levels, max_cycles, shifted):
-    """encodeFluid's dispatches with the bodies' passes (js/sim.js:2486-2611)."""
+def _sequence(levels, max_cycles, shifted, drag=False):
+    """encodeFluid's dispatches with the bodies' passes (js/sim.js:2486-2611);
+    drag: the liquid's drag on the bodies after unpress (a viscous world's)."""
     seq = [(p, 0, 0) for p in ("SYNC", "SYNC_PARTICLES", "SYNC_SEED", "COMPACT", "RETIRE", "CLEAR", "GATHER",
                                "SEAL_JOIN", "SEAL_ANCHOR", "CLASSIFY", "BODY_START", "BODY_LOADS", "SET_FACES",
-                               "UNPRESS", "DIVERGENCE", "CG_START", "CG_JOIN", "CG_ANCHOR", "CG_BODY_X",
-                               "CG_RESIDUAL", "CG_PREPARE")]
+                               "UNPRESS") + (("BODY_DRAG", "BODY_FACES") if drag else ()) +
+           ("DIVERGENCE", "CG_START", "CG_JOIN", "CG_ANCHOR", "CG_BODY_X", "CG_RESIDUAL", "CG_PREPARE")]
     sh = shifted
     for cyc in range(max_cycles):
         seq += [("RELAX_RIMS", 0, cyc), ("RELAX_SHIFTED" if sh else "RELAX", 0, cyc)]
@@ -60,20 +61,22 @@ def _sequence(levels, max_cycles, shifted):
     return seq
 
 
-def test_each_pass_with_bodies_matches_oracle():
+@pytest.mark.parametrize("liquid", ["water", "mud"])
+def test_each_pass_with_bodies_matches_oracle(liquid):
     """Each pass, the bodies' own among them, from the same state (a tank
     stepped twice) leaves the same buffers and body words."""
     from worldinagrain_b200 import fluid
-    world, bodies = W.bodies_world()
+    mud = liquid == "mud"
+    world, bodies = W.bodies_world(liquid=W.MUD if mud else abi.WATER)
     o = _oracle(world, bodies)
     for s in (1, 2):
-        o.step(params(world, s), max_cycles=64, flags=TOL, tolerance=1e-6)
+        o.step(params(world, s), max_cycles=64, flags=TOL | (abi.STEP_VISCOUS if mud else 0), tolerance=1e-6)
     g = fluid.LiquidStep(world.copy(), W.body_element_table())
     g.bind_bodies(bodies)
     P = params(world, 3)
     got, got_b = world.copy(), bodies.copy()
     labelling = False
-    for name, level, cycle in _sequence(len(world.L["levels"]), 3, shifted=True):
+    for name, level, cycle in _sequence(len(world.L["levels"]), 3, shifted=True, drag=mud):
         if name == "SEAL_JOIN":
             labelling = True
         if name == "CG_FINISH":

@@ -1885,13 +1885,6 @@ __global__ void __launch_bounds__(256) k_cgBeta(Dev D, uint32_t cycle) {
     __shared__ float sx[256], sy[256];
     __shared__ double s64[256];
     if (w.converged(cycle) || w.activeCount() == 0u) return;
-    // the bodies' sums of this iteration's direction, done with, emptied for
-    // the iteration after next (fluid.wgsl:2808-2813)
-    if (D.pushes) {
-        const uint32_t which = PUSH_P0 + cycle % 2u;
-        for (uint32_t k = threadIdx.x; k < MAX_BODIES * 6u; k += blockDim.x)
-            D.pushes[pushSlot(k / 6u, which, 0u) + k % 6u] = 0u;
-    }
     float* at = D.cg + 4u * (size_t)(D.C + D.B);
     if (D.st->f64) {
         double rz = sumBlocks64(w, D.part64, 0, s64);
@@ -1991,6 +1984,13 @@ __global__ void __launch_bounds__(256) k_cgAlpha(Dev D, uint32_t cycle) {
     __shared__ float sx[256], sy[256];
     __shared__ double s64[256];
     if (w.converged(cycle) || w.activeCount() == 0u) return;
+    // the bodies' sums of this iteration's direction, done with, emptied for
+    // the iteration after next (fluid.wgsl:2808-2813)
+    if (D.pushes) {
+        const uint32_t which = PUSH_P0 + cycle % 2u;
+        for (uint32_t k = threadIdx.x; k < MAX_BODIES * 6u; k += blockDim.x)
+            D.pushes[pushSlot(k / 6u, which, 0u) + k % 6u] = 0u;
+    }
     float* at = D.cg + 4u * (size_t)(D.C + D.B);
     if (D.st->f64) {
         double pq = sumBlocks64(w, D.part64, 0, s64);
