@@ -1,5 +1,7 @@
 """Writes tests/golden/oracle_steps.json: SHA-256 digests of the CPU oracle's
-buffers after steps of small seeded worlds.
+buffers after steps of small seeded worlds; and tests/golden/bodies_steps.json,
+the same for the tank of synthetic free bodies with its body table and push
+sums.
 
 The reference ships no test vectors for the liquid step (its test/*.mjs
 scripts are named in comments but absent), so these fixtures pin the oracle
@@ -35,6 +37,14 @@ CASES = [
 ]
 
 
+BODY_CASES = [
+    # name, liquid, flags, max_cycles, steps recorded
+    ("bodies_water_tol", abi.WATER, abi.STEP_TOLERANCE | abi.STEP_F64_DOTS, 64, (1, 3, 6)),
+    ("bodies_water_ref", abi.WATER, 0, 16, (1, 4)),
+    ("bodies_mud_tol", W.MUD, abi.STEP_TOLERANCE | abi.STEP_F64_DOTS | abi.STEP_VISCOUS, 64, (1, 4)),
+]
+
+
 def digest(a):
     return hashlib.sha256(memoryview(a).cast("B")).hexdigest()
 
@@ -64,13 +74,35 @@ def run_case(builder, flags, max_cycles, record):
     return got
 
 
+def run_body_case(liquid, flags, max_cycles, record):
+    world, bodies = W.bodies_world(liquid=liquid)
+    o = Oracle(world, W.body_element_table(), bodies)
+    got = {}
+    for s in range(1, max(record) + 1):
+        P = W.make_params(world, frame=s, seed=0x1234, earth_g=world.config["earth_g"])
+        st = o.step(P, max_cycles=max_cycles, flags=flags, tolerance=1e-6)
+        if s in record:
+            d = world_digests(world)
+            d["motion"] = digest(bodies.motion)
+            d["pushes"] = digest(bodies.pushes)
+            d["cycles"] = int(st.cycles)
+            got[str(s)] = d
+    return got
+
+
 def main():
     fixtures = {}
     for name, builder, flags, max_cycles, record in CASES:
         fixtures[name] = {"flags": flags, "max_cycles": max_cycles, "steps": run_case(builder, flags, max_cycles, record)}
     with open(os.path.join(HERE, "oracle_steps.json"), "w") as f:
         json.dump(fixtures, f, indent=1, sort_keys=True)
-    print("wrote", len(fixtures), "cases")
+    bodies = {}
+    for name, liquid, flags, max_cycles, record in BODY_CASES:
+        bodies[name] = {"flags": flags, "max_cycles": max_cycles,
+                        "steps": run_body_case(liquid, flags, max_cycles, record)}
+    with open(os.path.join(HERE, "bodies_steps.json"), "w") as f:
+        json.dump(bodies, f, indent=1, sort_keys=True)
+    print("wrote", len(fixtures) + len(bodies), "cases")
 
 
 if __name__ == "__main__":

@@ -5,6 +5,9 @@ free as the rest (the body's faces moving with its push, PUSH_F), the bodies
 the reference leaves out of the solve (just found, not alive) get nothing,
 a held body's push is summed and it is marked wet, and no particle ends in a
 body's cell."""
+import json
+import os
+
 import numpy as np
 import pytest
 
@@ -12,6 +15,9 @@ from worldinagrain_b200 import abi
 from worldinagrain_b200 import world as W
 
 from .common import params
+from .golden.make_golden import BODY_CASES, run_body_case
+
+HERE = os.path.dirname(os.path.abspath(__file__))
 
 FLAGS = abi.STEP_TOLERANCE | abi.STEP_F64_DOTS
 
@@ -110,3 +116,13 @@ def test_bodies_in_and_out_of_the_solve(liquid, flags):
     cy = np.clip(np.floor(motion[:, 1]).astype(int), 0, w.H - 1)
     kinds = w.cell_view()[cy, cx, 0] & 0xff
     assert not np.any(kinds == W.WOOD)
+
+
+@pytest.mark.parametrize("case", [c[0] for c in BODY_CASES])
+def test_oracle_with_bodies_matches_golden_fixtures(case):
+    """The oracle's steps of the body tank against its committed digests
+    (grid buffers, particles, body table, push sums)."""
+    with open(os.path.join(HERE, "golden", "bodies_steps.json")) as f:
+        fixture = json.load(f)[case]
+    _, liquid, flags, max_cycles, record = next(c for c in BODY_CASES if c[0] == case)
+    assert run_body_case(liquid, flags, max_cycles, record) == fixture["steps"]
