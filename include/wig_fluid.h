@@ -23,7 +23,7 @@
  *   binding 11 airSource     -> (not bound)
  *   binding 12 bodyMotion    -> motion     (u32: the body table, wig_fluid_bind_bodies; optional)
  *   binding 13 occupants     -> (not bound: no people)
- *   binding 14 bodies        -> (not bound: no swept stamps, so no body seams or cups)
+ *   binding 14 bodies        -> stamps     (u32: the bodies' buffer, read for its swept stamps; optional)
  *   binding 15 fluidCg       -> cg         (vec4<f32>: per cell, per block, sums)
  *   binding 16 bodyPushes    -> pushes     (u32: WIG_BODY_PUSH_WORDS per body; optional)
  *
@@ -122,6 +122,18 @@ extern "C" {
 #define WIG_BF_HELD 32u
 #define WIG_BF_WET 64u
 #define WIG_RIGID_FIX 16777216.0f
+/* The bodies' buffer (binding 14, js/sim.js:796-799) of a W x H world: its
+ * header (4 T + BODY_STAT_WORDS + BODY_COUNTERS + MAX_BODIES words, T the
+ * 8 x 8 body tiles), 2 + BODY_SUM_WORDS words a cell, structure's words
+ * (1 + T + 2 W H), and per cell two swept stamps, one for even steps and one
+ * for odd (shaders/common.wgsl:316-380): which body last moved over the cell
+ * as its cup (bit 0 clear) or a seam of its wall (bit 0 set), the stamp's
+ * step in the top 20 bits. */
+#define WIG_BODY_TILE 8u
+#define WIG_BODY_STAT_WORDS 8u
+#define WIG_BODY_COUNTERS 9u
+#define WIG_BODY_SUM_WORDS 8u
+#define WIG_CLAIM_PERIOD 0xfffffu
 #define WIG_LIQUID_WET 0x80000000u
 
 /* Params (shaders/common.wgsl:5-40), 80 bytes, written per step by the host
@@ -320,16 +332,18 @@ int wig_fluid_create(const wig_world_desc* d, const wig_elem* elems, uint32_t n_
  * js/sim.js:1259 `clear` leaves them). */
 int wig_fluid_bind(wig_fluid* h, const wig_fluid_buffers* b);
 
-/* Binds the free bodies' buffers (bindings 12 and 16, js/sim.js:1159): the
- * body table `motion` (WIG_BODY_MOTION_WORDS u32, caller-owned, read for
- * the bodies' poses and written in its liquid words) and `pushes`
- * (WIG_MAX_BODIES * WIG_BODY_PUSH_WORDS u32, caller-owned scratch).  With
- * them bound, each step couples the bodies into the solve (A = L + J^T M^-1 J,
+/* Binds the free bodies' buffers (bindings 12, 14 and 16, js/sim.js:1159):
+ * the body table `motion` (WIG_BODY_MOTION_WORDS u32, caller-owned, read for
+ * the bodies' poses and written in its liquid words), `pushes`
+ * (WIG_MAX_BODIES * WIG_BODY_PUSH_WORDS u32, caller-owned scratch), and
+ * optionally `stamps`, the bodies' buffer (layout above, read only: the
+ * swept stamps of last step and the one before, by which a body's seams
+ * and cup are found; null: no body has seams or a cup).  With them bound,
+ * each step couples the bodies into the solve (A = L + J^T M^-1 J,
  * fluid.wgsl:1181-1470, :2819-2845, :2949-3218) and runs in the plain form
- * (a kernel per reference pass), whatever the form flags ask; the body
- * table's swept stamps (binding 14) are not read, so no body has seams or
- * a cup.  Both null unbinds them.  Single-world handles only. */
-int wig_fluid_bind_bodies(wig_fluid* h, void* motion, void* pushes);
+ * (a kernel per reference pass), whatever the form flags ask.  motion and
+ * pushes null unbind all three.  Single-world handles only. */
+int wig_fluid_bind_bodies(wig_fluid* h, void* motion, void* pushes, void* stamps);
 
 /* The bound (or allocated) device buffers. */
 int wig_fluid_buffers_of(wig_fluid* h, wig_fluid_buffers* out);

@@ -42,7 +42,7 @@ def lib():
                                        C.c_uint32, C.POINTER(abi.Buffers), C.c_void_p]
         L.wo_true_residual.restype = C.c_double
         L.wo_sincos.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
-        L.wo_bind_bodies.argtypes = [C.c_void_p, C.c_void_p]
+        L.wo_bind_bodies.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = L
     return _lib
 
@@ -69,10 +69,11 @@ class Oracle:
 
     def _bind(self):
         if self.bodies is None:
-            lib().wo_bind_bodies(None, None)
+            lib().wo_bind_bodies(None, None, None)
         else:
-            assert self.bodies.motion.flags["C_CONTIGUOUS"] and self.bodies.pushes.flags["C_CONTIGUOUS"]
-            lib().wo_bind_bodies(self.bodies.motion.ctypes.data, self.bodies.pushes.ctypes.data)
+            b = self.bodies
+            assert b.motion.flags["C_CONTIGUOUS"] and b.pushes.flags["C_CONTIGUOUS"] and b.stamps.flags["C_CONTIGUOUS"]
+            lib().wo_bind_bodies(b.motion.ctypes.data, b.pushes.ctypes.data, b.stamps.ctypes.data)
 
     def pass_(self, P, name, level=0, cycle=0):
         d = self.world.desc()
@@ -82,7 +83,7 @@ class Oracle:
             rc = lib().wo_pass(C.byref(d), C.byref(P), self.elems, len(self.elems), C.byref(b), abi.PASS[name],
                                level, cycle)
         finally:
-            lib().wo_bind_bodies(None, None)
+            lib().wo_bind_bodies(None, None, None)
         assert rc == 0, rc
 
     def step(self, P, max_cycles=abi.FLUID_CYCLES, flags=0, tolerance=1e-6):
@@ -94,7 +95,7 @@ class Oracle:
             rc = lib().wo_step(C.byref(d), C.byref(P), self.elems, len(self.elems), C.byref(b), max_cycles, flags,
                                tolerance, C.byref(self.shifted), C.byref(st))
         finally:
-            lib().wo_bind_bodies(None, None)
+            lib().wo_bind_bodies(None, None, None)
         assert rc == 0, rc
         return st
 

@@ -20,8 +20,9 @@
 // Scope: the element subset AIR, WALL, WATER (and any element table given),
 // no air motion (binding 3 unbound: no air push in gather, no wind drag in
 // setFace), free bodies only when their table and sums are bound (bindings
-// 12 and 16, wo_bind_bodies; else rigidAt and heldAt are NONE) and never
-// their swept stamps (binding 14 unbound: seamOf and cupOf are NONE), no people (binding 13 unbound: isOccupant is false), and
+// 12 and 16, wo_bind_bodies; else rigidAt and heldAt are NONE) and their
+// seams and cups only when the bodies' buffer is too (binding 14; else
+// seamOf, cupOf and cupBefore are NONE), no people (binding 13 unbound: isOccupant is false), and
 // the Earth's pull alone (binding 10 unbound: pullAt = (0, P.earthG), down is
 // +y).  Surface tension's pass runs only when sim.js's surfaceTension() holds
 // (capillary length over dx >= 0.3 cells), which no config reaches.
@@ -214,6 +215,7 @@ struct Ctx {
     float* cg;
     uint32_t* motion = nullptr;   // binding 12, the body table (null: no free bodies)
     uint32_t* pushes = nullptr;   // binding 16, the solve's sums of what it does to each body
+    uint32_t* stamps = nullptr;   // binding 14, the bodies' buffer (its swept stamps; null: none)
     uint32_t level = 0, cycle = 0;
     uint32_t rng = 0;
     int W, H;
@@ -616,6 +618,32 @@ bool wetRegionAt(Ctx& X, const uint32_t* v) {
     uint32_t b = rigidBodyOf(X, v);
     return b != NONE && (bodyWord(X, b, WIG_BW_FLAGS) & (WIG_BF_WET | WIG_BF_HELD)) == (WIG_BF_WET | WIG_BF_HELD);
 }
+// bodySweptSlot, claimStep (common.wgsl:316-385): cell i's stamp of step frame
+uint32_t claimStep(uint32_t frame) { return frame % WIG_CLAIM_PERIOD + 1u; }
+uint32_t bodySweptSlot(Ctx& X, uint32_t i, uint32_t frame) {
+    uint32_t tiles = (((uint32_t)X.W + WIG_BODY_TILE - 1u) / WIG_BODY_TILE) * (((uint32_t)X.H + WIG_BODY_TILE - 1u) / WIG_BODY_TILE);
+    uint32_t base = 4u * tiles + WIG_BODY_STAT_WORDS + WIG_BODY_COUNTERS + MAX_BODIES + (2u + WIG_BODY_SUM_WORDS) * X.C;
+    return base + 1u + tiles + 2u * X.C + X.C + 2u * i + (frame & 1u);
+}
+// cupOf, seamOf (fluid.wgsl:1252-1288): the body whose cup (seam) cell i was
+// stamped last step, alive and weighed; cupBefore (fluid.wgsl:3521-3528):
+// whose cup it was the step before, whatever the body's state now
+uint32_t sweptBody(Ctx& X, uint32_t i, uint32_t frame, uint32_t seam) {
+    if (!X.stamps || !X.motion) return NONE;
+    uint32_t key = X.stamps[bodySweptSlot(X, i, frame)];
+    if ((key >> 12u) != claimStep(frame) || (key & 1u) != seam) return NONE;
+    uint32_t b = 2047u - ((key >> 1u) & 0x7ffu);
+    return b < MAX_BODIES ? b : NONE;
+}
+uint32_t cupOf(Ctx& X, uint32_t i) {
+    uint32_t b = sweptBody(X, i, X.P->frame - 1u, 0u);
+    return b != NONE && bodyInSolve(X, b) ? b : NONE;
+}
+uint32_t seamOf(Ctx& X, uint32_t i) {
+    uint32_t b = sweptBody(X, i, X.P->frame - 1u, 1u);
+    return b != NONE && bodyInSolve(X, b) ? b : NONE;
+}
+uint32_t cupBefore(Ctx& X, uint32_t i) { return sweptBody(X, i, X.P->frame - 2u, 0u); }
 // rigidAt, heldAt (fluid.wgsl:1422-1458): the body classify put in the drift's z
 uint32_t rigidAt(Ctx& X, I2 c) {
     if (!X.motion || !X.inWorld(c)) return NONE;
@@ -903,9 +931,11 @@ void pass_syncParticles(Ctx& X) {
             keep = true;
             markBlockOf(X, q.pos);
         } else if ((d & DEST_ASIDE) != 0u && (d & ~DEST_ASIDE) < X.C) {
-            uint32_t to = d & ~DEST_ASIDE;  // no bodies: no cup is ever in the way
-            q.pos = V2{(float)(to % (uint32_t)X.W) + (q.pos.x - std::floor(q.pos.x)),
-                       (float)(to / (uint32_t)X.W) + (q.pos.y - std::floor(q.pos.y))};
+            uint32_t to = d & ~DEST_ASIDE;
+            // not into another body's cup (fluid.wgsl:785-793)
+            if (cupOf(X, to) == NONE)
+                q.pos = V2{(float)(to % (uint32_t)X.W) + (q.pos.x - std::floor(q.pos.x)),
+                           (float)(to / (uint32_t)X.W) + (q.pos.y - std::floor(q.pos.y))};
             keep = true;
             markBlockOf(X, q.pos);
         } else if (isClaim(d) && claimedCell(d) < X.C) {
@@ -1196,10 +1226,20 @@ void pass_classify(Ctx& X) {
                 bool sealed = false;
                 if (n == 0 && mayBeSealed(X, p)) sealed = (ufLink(X, ufFind(X, i)) & REGION_OPEN) == 0u;
                 uint32_t rigid = NONE, held = NONE;
-                if (n < 0) {
+                uint32_t seam = n < 0 ? NONE : seamOf(X, i);
+                if (seam != NONE) {
+                    // a gap the stamp opened in a body's wall: the body's (fluid.wgsl:1604-1613)
                     c.z = -1.0f;
-                    // a free body's cell (fluid.wgsl:1614-1627; no cups: binding 14 unbound)
-                    if (X.motion) rigid = rigidBodyOf(X, X.cellv(i));
+                    rigid = seam;
+                    if (isHeld(X, seam)) { held = seam; rigid = NONE; }
+                    sealed = false;
+                } else if (n < 0) {
+                    c.z = -1.0f;
+                    // a free body's cell, or powder in its cup, its cargo (fluid.wgsl:1614-1627)
+                    if (X.motion) {
+                        rigid = rigidBodyOf(X, X.cellv(i));
+                        if (rigid == NONE && X.kindOfCell(i) == WIG_KIND_POWDER) rigid = cupOf(X, i);
+                    }
                     if (rigid != NONE && isHeld(X, rigid)) { held = rigid; rigid = NONE; }
                 } else if (n > 0) {
                     V2 li = liquidIn(X, i);
@@ -2219,16 +2259,22 @@ bool isObstacle(Ctx& X, V2 pos) {
     uint32_t k = X.kindOfCell(X.cellIndex(c));
     return k == WIG_KIND_SOLID || k == WIG_KIND_POWDER;
 }
-bool escapesTo(Ctx& X, I2 q) { return X.inWorld(q) && !(X.gridAt(q).z < 0.0f); }
+// shutAt, escapesTo (fluid.wgsl:1468-1470, :3535-3541)
+bool escapesTo(Ctx& X, I2 q, uint32_t side) {
+    if (!X.inWorld(q) || X.gridAt(q).z < 0.0f || rigidAt(X, q) != NONE) return false;
+    uint32_t cup = cupOf(X, X.cellIndex(q));
+    return cup == NONE || cup == side;
+}
 V2 escape(Ctx& X, V2 pos) {
     if (!isObstacle(X, pos)) return pos;
     I2 c{f2i(std::floor(pos.x)), f2i(std::floor(pos.y))};
+    const uint32_t side = X.inWorld(c) ? cupBefore(X, X.cellIndex(c)) : NONE;
     V2 best = pos;
     float bestD = 1e9f;
     for (int n = 0; n < 8; n++) {
         int m = n + (n >= 4 ? 1 : 0);
         I2 at{c.x + m % 3 - 1, c.y + m / 3 - 1};
-        if (!escapesTo(X, at)) continue;
+        if (!escapesTo(X, at, side)) continue;
         V2 inside{clampf(pos.x, (float)at.x + 0.02f, (float)at.x + 0.98f), clampf(pos.y, (float)at.y + 0.02f, (float)at.y + 0.98f)};
         float dx = pos.x - inside.x, dy = pos.y - inside.y;
         float d = std::sqrt(dx * dx + dy * dy);
@@ -2242,7 +2288,7 @@ V2 escape(Ctx& X, V2 pos) {
         I2 dir = ways[n];
         for (int r = 2; r < nearest; r++) {
             I2 q{c.x + dir.x * r, c.y + dir.y * r};
-            if (!isObstacle(X, V2{(float)q.x + 0.5f, (float)q.y + 0.5f}) && escapesTo(X, q)) {
+            if (!isObstacle(X, V2{(float)q.x + 0.5f, (float)q.y + 0.5f}) && escapesTo(X, q, side)) {
                 nearest = r;
                 way = dir;
                 break;
@@ -2585,11 +2631,13 @@ int layout(const wig_world_desc* d, wig_world_layout* L) {
 // The bodies' buffers bound by wo_bind_bodies (null: none).
 uint32_t* g_motion = nullptr;
 uint32_t* g_pushes = nullptr;
+uint32_t* g_stamps = nullptr;
 
 void setup(Ctx& X, const wig_world_layout& L, const wig_params* P, const wig_elem* E, uint32_t nE, wig_fluid_buffers* b) {
     X.L = L; X.P = P; X.E = E; X.nE = nE;
     X.motion = g_motion;
     X.pushes = g_pushes;
+    X.stamps = g_stamps;
     X.cells = (uint32_t*)b->cells; X.sorted = (uint32_t*)b->sorted; X.parts = (uint32_t*)b->parts;
     X.counters = (uint32_t*)b->counters; X.field = (float*)b->field; X.blocks = (uint32_t*)b->blocks; X.cg = (float*)b->cg;
     X.W = (int)L.width; X.H = (int)L.height;
@@ -2729,11 +2777,13 @@ int wo_layout(const wig_world_desc* d, wig_world_layout* out) { return layout(d,
 
 // Binds the free bodies' host buffers for the passes and steps that follow
 // (motion: WIG_BODY_MOTION_WORDS, pushes: WIG_MAX_BODIES * WIG_BODY_PUSH_WORDS
-// u32); both null unbinds them.
-int wo_bind_bodies(uint32_t* motion, uint32_t* pushes) {
+// u32; stamps: the bodies' buffer of the world, or null); motion and pushes
+// null unbinds them all.
+int wo_bind_bodies(uint32_t* motion, uint32_t* pushes, uint32_t* stamps) {
     if ((motion == nullptr) != (pushes == nullptr)) return WIG_E_ARG;
     g_motion = motion;
     g_pushes = pushes;
+    g_stamps = motion ? stamps : nullptr;
     return WIG_OK;
 }
 

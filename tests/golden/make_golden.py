@@ -80,6 +80,8 @@ def run_body_case(liquid, flags, max_cycles, record):
     got = {}
     for s in range(1, max(record) + 1):
         P = W.make_params(world, frame=s, seed=0x1234, earth_g=world.config["earth_g"])
+        bodies.stamp_step(s - 1)
+        W.send_aside(world, bodies, s)
         st = o.step(P, max_cycles=max_cycles, flags=flags, tolerance=1e-6)
         if s in record:
             d = world_digests(world)

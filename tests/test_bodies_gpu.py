@@ -3,8 +3,9 @@
 dispatches of js/sim.js:2499-2600) against the CPU oracle, through the C ABI
 (wig_fluid_bind_bodies).  The tank holds synthetic bodies: a plank afloat,
 moving and spinning with a sub-cell pose; a block under the water with a
-contact mobility; a held, wet block on the floor; a body just found; and a
-slot not alive.  Grid buffers, the body table (its liquid words) and the
+contact mobility and a seam in its wall; a held, wet block on the floor; a
+body just found; a slot not alive; and a hull whose cup (its swept stamps)
+holds sand as cargo, with particles sent aside into and beside it.  Grid buffers, the body table (its liquid words) and the
 push sums must match bit for bit, particles as multisets."""
 import numpy as np
 import pytest
@@ -70,7 +71,11 @@ def test_each_pass_with_bodies_matches_oracle(liquid):
     world, bodies = W.bodies_world(liquid=W.MUD if mud else abi.WATER)
     o = _oracle(world, bodies)
     for s in (1, 2):
+        bodies.stamp_step(s - 1)
+        W.send_aside(world, bodies, s)
         o.step(params(world, s), max_cycles=64, flags=TOL | (abi.STEP_VISCOUS if mud else 0), tolerance=1e-6)
+    bodies.stamp_step(2)
+    W.send_aside(world, bodies, 3)
     g = fluid.LiquidStep(world.copy(), W.body_element_table())
     g.bind_bodies(bodies)
     P = params(world, 3)
@@ -113,6 +118,12 @@ def test_steps_with_bodies_match_oracle(case):
     gpu_flags = (flags | abi.STEP_MIXED) if case == "fast_flags" else (flags | abi.STEP_PLAIN)
     for s in range(1, steps + 1):
         P = params(ref, s)
+        # what the bodies' pass would leave: this step's stamps, particles sent aside
+        for wd, bd in ((ref, ref_b), (got, got_b)):
+            bd.stamp_step(s - 1)
+            W.send_aside(wd, bd, s)
+        g.upload(got)
+        g.upload_bodies(got_b)
         ost = o.step(P, max_cycles=cycles, flags=flags, tolerance=1e-6)
         g.step(P, max_cycles=cycles, flags=gpu_flags, tolerance=1e-6)
         st = g.stats(unconverged_ok=not (flags & abi.STEP_TOLERANCE))
@@ -124,6 +135,6 @@ def test_steps_with_bodies_match_oracle(case):
         assert st.cycles == ost.cycles
         if flags & abi.STEP_TOLERANCE:
             assert st.rel_residual <= 1e-6
-    for b in (0, 1, 2):
+    for b in (0, 1, 2, 5):
         assert np.any(got_b.liquid(b)[:3] != 0)
     g.close()

@@ -35,6 +35,19 @@ BW = dict(POS=0, VEL=3, SPIN=5, MASS=6, INERTIA=7, CELLS=13, FLAGS=18, SUBCELL=2
           MOBILITY=108, MOBILITY_AT=114)
 BF_ALIVE, BF_NEW, BF_HELD, BF_WET = 1, 2, 32, 64
 RIGID_FIX = 16777216.0
+BODY_TILE, BODY_STAT_WORDS, BODY_COUNTERS, BODY_SUM_WORDS = 8, 8, 9, 8
+CLAIM_PERIOD = 0xfffff
+
+
+def body_stamps_layout(width, height):
+    """(words of the bodies' buffer, first swept-stamp word) of a world
+    (js/sim.js:796-799, shaders/common.wgsl:316-380): cell i's stamp of step
+    f is at first + 2 i + (f & 1)."""
+    tiles = -(-width // BODY_TILE) * -(-height // BODY_TILE)
+    n = width * height
+    header = 4 * tiles + BODY_STAT_WORDS + BODY_COUNTERS + MAX_BODIES
+    first = header + (2 + BODY_SUM_WORDS) * n + 1 + tiles + 2 * n + n
+    return header + (2 + BODY_SUM_WORDS) * n + 1 + tiles + 5 * n, first
 
 WIG_OK = 0
 ERRORS = {

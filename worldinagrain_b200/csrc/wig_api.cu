@@ -1326,15 +1326,16 @@ int wig_fluid_bind(wig_fluid* h, const wig_fluid_buffers* bufs) {
     return WIG_OK;
 }
 
-int wig_fluid_bind_bodies(wig_fluid* h, void* motion, void* pushes) {
+int wig_fluid_bind_bodies(wig_fluid* h, void* motion, void* pushes, void* stamps) {
     if (!h || !h->b) return fail(WIG_E_ARG, "null handle");
     if ((motion == nullptr) != (pushes == nullptr)) return fail(WIG_E_ARG, "bind both body buffers or neither");
-    if (((uintptr_t)motion & 15u) != 0u || ((uintptr_t)pushes & 15u) != 0u)
+    if (((uintptr_t)motion & 15u) != 0u || ((uintptr_t)pushes & 15u) != 0u || ((uintptr_t)stamps & 15u) != 0u)
         return fail(WIG_E_ARG, "body buffer not 16-byte aligned");
     wig_batch* b = h->b;
     for (auto& ln : b->lane) drop_graphs(ln);
     b->hw[0].D.motion = static_cast<uint32_t*>(motion);
     b->hw[0].D.pushes = static_cast<uint32_t*>(pushes);
+    b->hw[0].D.stamps = motion ? static_cast<uint32_t*>(stamps) : nullptr;
     return upload_world_entry(b, 0);
 }
 

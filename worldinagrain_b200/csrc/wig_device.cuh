@@ -140,6 +140,7 @@ struct Dev {
     double* norm64;   // 2 doubles per block: FP64 norms' partials
     uint32_t* motion; // binding 12, the free bodies' table (null: no free bodies)
     uint32_t* pushes; // binding 16, the solve's exact sums of what it does to each body
+    uint32_t* stamps; // binding 14, the bodies' buffer, read for its swept stamps (null: no seams or cups)
 };
 
 struct I2 { int x, y; };

@@ -234,6 +234,33 @@ __device__ bool wetRegionAt(const W& w, uint4 v) {
     const uint32_t b = rigidBodyOf(w, v);
     return b != NONE && (bodyWord(w, b, WIG_BW_FLAGS) & (WIG_BF_WET | WIG_BF_HELD)) == (WIG_BF_WET | WIG_BF_HELD);
 }
+// bodySweptSlot, claimStep (common.wgsl:316-385): cell i's stamp of step frame
+__device__ __forceinline__ uint32_t claimStep(uint32_t frame) { return frame % WIG_CLAIM_PERIOD + 1u; }
+__device__ __forceinline__ uint32_t bodySweptSlot(const W& w, uint32_t i, uint32_t frame) {
+    const uint32_t tiles = (((uint32_t)w.D.W + WIG_BODY_TILE - 1u) / WIG_BODY_TILE) *
+                           (((uint32_t)w.D.H + WIG_BODY_TILE - 1u) / WIG_BODY_TILE);
+    const uint32_t base = 4u * tiles + WIG_BODY_STAT_WORDS + WIG_BODY_COUNTERS + MAX_BODIES + (2u + WIG_BODY_SUM_WORDS) * w.D.C;
+    return base + 1u + tiles + 2u * w.D.C + w.D.C + 2u * i + (frame & 1u);
+}
+// cupOf, seamOf (fluid.wgsl:1252-1288): the body whose cup (seam) cell i was
+// stamped last step, alive and weighed; cupBefore (fluid.wgsl:3521-3528):
+// whose cup it was the step before, whatever the body's state now
+__device__ uint32_t sweptBody(const W& w, uint32_t i, uint32_t frame, uint32_t seam) {
+    if (!w.D.stamps || !w.D.motion) return NONE;
+    const uint32_t key = w.D.stamps[bodySweptSlot(w, i, frame)];
+    if ((key >> 12u) != claimStep(frame) || (key & 1u) != seam) return NONE;
+    const uint32_t b = 2047u - ((key >> 1u) & 0x7ffu);
+    return b < MAX_BODIES ? b : NONE;
+}
+__device__ uint32_t cupOf(const W& w, uint32_t i) {
+    const uint32_t b = sweptBody(w, i, w.D.st->P.frame - 1u, 0u);
+    return b != NONE && bodyInSolve(w, b) ? b : NONE;
+}
+__device__ uint32_t seamOf(const W& w, uint32_t i) {
+    const uint32_t b = sweptBody(w, i, w.D.st->P.frame - 1u, 1u);
+    return b != NONE && bodyInSolve(w, b) ? b : NONE;
+}
+__device__ __forceinline__ uint32_t cupBefore(const W& w, uint32_t i) { return sweptBody(w, i, w.D.st->P.frame - 2u, 0u); }
 // rigidAt, heldAt (fluid.wgsl:1422-1458): the body classify put in the drift's z
 __device__ uint32_t rigidAt(const W& w, I2 c) {
     if (!w.D.motion || !w.inWorld(c)) return NONE;
@@ -577,7 +604,9 @@ __global__ void k_syncParticles(Batch Bt) {
             markBlockOf(w, pos.x, pos.y);
         } else if ((d & DEST_ASIDE) != 0u && (d & ~DEST_ASIDE) < D.C) {
             uint32_t to = d & ~DEST_ASIDE;
-            pos = V2{(float)(to % (uint32_t)D.W) + (pos.x - floorf(pos.x)), (float)(to / (uint32_t)D.W) + (pos.y - floorf(pos.y))};
+            // not into another body's cup (fluid.wgsl:785-793)
+            if (cupOf(w, to) == NONE)
+                pos = V2{(float)(to % (uint32_t)D.W) + (pos.x - floorf(pos.x)), (float)(to / (uint32_t)D.W) + (pos.y - floorf(pos.y))};
             keep = true;
             markBlockOf(w, pos.x, pos.y);
         } else if (isClaim(d) && claimedCell(d) < D.C) {
@@ -1086,10 +1115,23 @@ __global__ void k_classify(Batch Bt) {
             bool sealed = false;
             if (n == 0 && mayBeSealed(w, p)) sealed = (vload(w.gwp(ufFind(w, i), G_REGION)) & REGION_OPEN) == 0u;
             uint32_t rigid = NONE, held = NONE;
-            if (n < 0) {
+            const uint32_t seam = n < 0 ? NONE : seamOf(w, i);
+            if (seam != NONE) {
+                // a gap the stamp opened in a body's wall: the body's (fluid.wgsl:1604-1613)
                 c.z = -1.0f;
-                // a free body's cell (fluid.wgsl:1614-1627; no cups: binding 14 unbound)
-                if (D.motion) rigid = rigidBodyOf(w, w.cell(i));
+                rigid = seam;
+                if (isHeld(w, seam)) {
+                    held = seam;
+                    rigid = NONE;
+                }
+                sealed = false;
+            } else if (n < 0) {
+                c.z = -1.0f;
+                // a free body's cell, or powder in its cup, its cargo (fluid.wgsl:1614-1627)
+                if (D.motion) {
+                    rigid = rigidBodyOf(w, w.cell(i));
+                    if (rigid == NONE && w.kindOfCell(i) == WIG_KIND_POWDER) rigid = cupOf(w, i);
+                }
                 if (rigid != NONE && isHeld(w, rigid)) {
                     held = rigid;
                     rigid = NONE;
@@ -2197,17 +2239,23 @@ __device__ __forceinline__ bool isObstacle(const W& w, float px, float py) {
     uint32_t k = w.kindOfCell(w.cellIndex(c));
     return k == WIG_KIND_SOLID || k == WIG_KIND_POWDER;
 }
-__device__ __forceinline__ bool escapesTo(const W& w, I2 q) { return w.inWorld(q) && !(w.gridAt(q).z < 0.0f); }
+// shutAt, escapesTo (fluid.wgsl:1468-1470, :3535-3541)
+__device__ __forceinline__ bool escapesTo(const W& w, I2 q, uint32_t side) {
+    if (!w.inWorld(q) || w.gridAt(q).z < 0.0f || rigidAt(w, q) != NONE) return false;
+    const uint32_t cup = cupOf(w, w.cellIndex(q));
+    return cup == NONE || cup == side;
+}
 // escape (fluid.wgsl:3552-3594), no bodies, the Earth's down.
 __device__ V2 escape(const W& w, V2 pos) {
     if (!isObstacle(w, pos.x, pos.y)) return pos;
     I2 c{f2i(floorf(pos.x)), f2i(floorf(pos.y))};
+    const uint32_t side = w.inWorld(c) ? cupBefore(w, w.cellIndex(c)) : NONE;
     V2 best = pos;
     float bestD = 1e9f;
     for (int n = 0; n < 8; n++) {
         int m = n + (n >= 4 ? 1 : 0);
         I2 at{c.x + m % 3 - 1, c.y + m / 3 - 1};
-        if (!escapesTo(w, at)) continue;
+        if (!escapesTo(w, at, side)) continue;
         float ix = clampf(pos.x, (float)at.x + 0.02f, (float)at.x + 0.98f);
         float iy = clampf(pos.y, (float)at.y + 0.02f, (float)at.y + 0.98f);
         float d = len2(pos.x - ix, pos.y - iy);
@@ -2220,7 +2268,7 @@ __device__ V2 escape(const W& w, V2 pos) {
     for (int n = 0; n < 4; n++) {
         for (int r = 2; r < nearest; r++) {
             I2 q{c.x + wx[n] * r, c.y + wy[n] * r};
-            if (!isObstacle(w, (float)q.x + 0.5f, (float)q.y + 0.5f) && escapesTo(w, q)) {
+            if (!isObstacle(w, (float)q.x + 0.5f, (float)q.y + 0.5f) && escapesTo(w, q, side)) {
                 nearest = r;
                 wayx = wx[n];
                 wayy = wy[n];

@@ -22,7 +22,7 @@ FUNCS = {
     "wig_fluid_layout": ([C.POINTER(abi.WorldDesc), C.POINTER(abi.WorldLayout)], C.c_int),
     "wig_fluid_create": ([C.POINTER(abi.WorldDesc), C.POINTER(abi.Elem), C.c_uint32, C.POINTER(C.c_void_p)], C.c_int),
     "wig_fluid_bind": ([C.c_void_p, C.POINTER(abi.Buffers)], C.c_int),
-    "wig_fluid_bind_bodies": ([C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
+    "wig_fluid_bind_bodies": ([C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p], C.c_int),
     "wig_fluid_buffers_of": ([C.c_void_p, C.POINTER(abi.Buffers)], C.c_int),
     "wig_fluid_step": ([C.c_void_p, C.POINTER(abi.Params), C.c_uint32, C.c_uint32, C.c_double, C.c_void_p], C.c_int),
     "wig_fluid_dispatch": ([C.c_void_p, C.POINTER(abi.Params), C.c_int, C.c_uint32, C.c_uint32, C.c_void_p], C.c_int),
@@ -145,33 +145,34 @@ class LiquidStep:
         return b
 
     def bind_bodies(self, bodies):
-        """Binds a free-body table and push sums (world.Bodies) in device
-        memory of their own (bindings 12 and 16, js/sim.js:1159); the steps
-        after couple the bodies into the solve.  None unbinds them."""
+        """Binds a free-body table, push sums and bodies' buffer
+        (world.Bodies) in device memory of their own (bindings 12, 16 and
+        14, js/sim.js:1159); the steps after couple the bodies into the
+        solve.  None unbinds them."""
         import torch
         if bodies is None:
-            check(lib().wig_fluid_bind_bodies(self.h, None, None), "wig_fluid_bind_bodies")
+            check(lib().wig_fluid_bind_bodies(self.h, None, None, None), "wig_fluid_bind_bodies")
             self._bodies = None
             return
-        motion = torch.from_numpy(bodies.motion.view(np.int32).copy()).to("cuda")
-        pushes = torch.from_numpy(bodies.pushes.view(np.int32).copy()).to("cuda")
+        devs = tuple(torch.from_numpy(a.view(np.int32).copy()).to("cuda")
+                     for a in (bodies.motion, bodies.pushes, bodies.stamps))
         torch.cuda.synchronize()
-        check(lib().wig_fluid_bind_bodies(self.h, C.c_void_p(motion.data_ptr()), C.c_void_p(pushes.data_ptr())),
-              "wig_fluid_bind_bodies")
-        self._bodies = (motion, pushes)
+        check(lib().wig_fluid_bind_bodies(self.h, *(C.c_void_p(t.data_ptr()) for t in devs)), "wig_fluid_bind_bodies")
+        self._bodies = devs
 
     def upload_bodies(self, bodies):
-        """bodies' table and push sums copied into the bound device buffers."""
+        """bodies' table, push sums and stamps copied into the bound device
+        buffers."""
         import torch
-        motion, pushes = self._bodies
-        motion.copy_(torch.from_numpy(bodies.motion.view(np.int32).copy()))
-        pushes.copy_(torch.from_numpy(bodies.pushes.view(np.int32).copy()))
+        for t, a in zip(self._bodies, (bodies.motion, bodies.pushes, bodies.stamps)):
+            t.copy_(torch.from_numpy(a.view(np.int32).copy()))
         torch.cuda.synchronize()
 
     def download_bodies(self, bodies):
-        """The bound body table and push sums copied back into bodies."""
+        """The bound body table and push sums copied back into bodies (the
+        stamps the step only reads)."""
         import torch
-        motion, pushes = self._bodies
+        motion, pushes, _ = self._bodies
         torch.cuda.synchronize()
         bodies.motion[:] = motion.cpu().numpy().view(np.uint32)
         bodies.pushes[:] = pushes.cpu().numpy().view(np.uint32)

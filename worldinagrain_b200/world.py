@@ -346,14 +346,33 @@ def body_element_table():
 
 
 class Bodies:
-    """A free-body table (binding 12, `motion`) and the solve's push sums
-    (binding 16, `pushes`) in the reference's layouts (js/shared.js:294-333),
-    host side.  The liquid step reads a body's pose, motion, mass and flags
-    and adds what it does to the body into the body's liquid words."""
+    """A free-body table (binding 12, `motion`), the solve's push sums
+    (binding 16, `pushes`) and the bodies' buffer of a world (binding 14,
+    `stamps`, of which the liquid step reads the swept stamps) in the
+    reference's layouts (js/shared.js:294-333, js/sim.js:796-799), host
+    side.  The liquid step reads a body's pose, motion, mass and flags and
+    adds what it does to the body into the body's liquid words."""
 
-    def __init__(self):
+    def __init__(self, width, height):
         self.motion = np.zeros(abi.BODY_MOTION_WORDS, dtype=np.uint32)
         self.pushes = np.zeros(abi.MAX_BODIES * abi.BODY_PUSH_WORDS, dtype=np.uint32)
+        words, self.stamp_at = abi.body_stamps_layout(width, height)
+        self.stamps = np.zeros(words, dtype=np.uint32)
+        self.width = width
+        self.swept = []  # (cells' flat indices, body, seam) stamped every step (stamp_step)
+
+    def stamp(self, frame, cells, b, seam):
+        """Cells (flat indices) swept by body b at step `frame`, as its cup or
+        as seams of its wall (bodies.wgsl's stamp: claimStep(frame) << 12 |
+        (2047 - b) << 1 | seam)."""
+        key = ((frame % abi.CLAIM_PERIOD + 1) << 12) | ((2047 - b) << 1) | (1 if seam else 0)
+        self.stamps[self.stamp_at + 2 * np.asarray(cells, dtype=np.int64) + (frame & 1)] = key
+
+    def stamp_step(self, frame):
+        """The stamps the bodies would leave at step `frame` (the bodies
+        here stand still, so the same cells each step)."""
+        for cells, b, seam in self.swept:
+            self.stamp(frame, cells, b, seam)
 
     def words(self, b):
         at = abi.MAX_BODIES + b * abi.BODY_TABLE_WORDS
@@ -370,8 +389,10 @@ class Bodies:
 
     def copy(self):
         o = Bodies.__new__(Bodies)
+        o.__dict__.update(self.__dict__)
         o.motion = self.motion.copy()
         o.pushes = self.pushes.copy()
+        o.stamps = self.stamps.copy()
         return o
 
 
@@ -407,18 +428,21 @@ def stamp_body(world, bodies, b, mask, density, vel=(0.0, 0.0), spin=0.0, subcel
     bodies.words(b)[abi.BW["MOBILITY_AT"]] = mobility_at & 0xffffffff
 
 
-def bodies_world(width=96, height=80, seed=6, liquid=abi.WATER):
+def bodies_world(width=96, height=80, seed=6, liquid=abi.WATER, stamps=True):
     """A tank of water with synthetic free bodies in it (none of the
     reference's configs has any): a plank afloat at the surface, moving and
     spinning, with a sub-cell pose; a block under the water whose contact
-    mobility was worked out the step before the first; a heavy block held
-    on the floor, wet; a body just found (NEW, a wall until weighed); and
-    cells of a slot that is not alive.  liquid: the tank's liquid (MUD for
-    the viscous sweeps and the liquid's drag on the bodies).  Returns
-    (world, bodies)."""
+    mobility was worked out the step before the first, with a seam its stamp
+    opened in its wall; a heavy block held on the floor, wet; a body just
+    found (NEW, a wall until weighed); cells of a slot that is not alive;
+    and a hull afloat whose cup holds sand (its cargo) and the water over
+    its rim.  liquid: the tank's liquid (MUD for the viscous sweeps and the
+    liquid's drag on the bodies).  stamps: the hull's cup and the block's
+    seam in the swept stamps (Bodies.stamp_step writes them a step).
+    Returns (world, bodies)."""
     rng = np.random.default_rng(seed)
     w = World(width, height)
-    bodies = Bodies()
+    bodies = Bodies(width, height)
     wall = np.zeros((height, width), dtype=bool)
     wall[-1, :] = True
     wall[:, 0] = wall[:, -1] = True
@@ -435,15 +459,52 @@ def bodies_world(width=96, height=80, seed=6, liquid=abi.WATER):
 
     stamp_body(w, bodies, 0, box(width // 6, surface - 1, 14, 3), 0.6, vel=(0.05, 0.03), spin=0.002,
                subcell=(0.25, -0.125))
-    stamp_body(w, bodies, 1, box(width // 2, surface + 12, 6, 6), 0.9, vel=(-0.02, 0.01), spin=-0.001,
+    block = box(width // 2, surface + 12, 6, 6)
+    seam = np.zeros_like(block)
+    seam[surface + 14, width // 2 + 2] = True  # a gap in the block's wall, left to the liquid
+    block &= ~seam
+    stamp_body(w, bodies, 1, block, 0.9, vel=(-0.02, 0.01), spin=-0.001,
                subcell=(-0.1875, 0.0625), mobility=(0.5, 0.01, 0.002, 0.45, -0.003, 0.02), mobility_at=0)
     stamp_body(w, bodies, 2, box(width // 2 + 14, height - 5, 10, 4), 7.8, flags=abi.BF_ALIVE | abi.BF_HELD | abi.BF_WET)
     stamp_body(w, bodies, 3, box(width // 6 + 4, height - 12, 4, 4), 0.6, flags=abi.BF_ALIVE | abi.BF_NEW)
     stamp_body(w, bodies, 4, box(width - 14, surface + 4, 3, 5), 0.6, flags=0)
+    # a hull: a floor 10 wide and sides 5 high, its hold 8 x 4 over the floor
+    hx, hy = width // 2 - 6, surface - 3
+    hull = np.zeros((height, width), dtype=bool)
+    hull[hy + 4, hx:hx + 10] = True
+    hull[hy:hy + 4, hx] = hull[hy:hy + 4, hx + 9] = True
+    assert not np.any(hull & used)
+    used[hull] = True
+    stamp_body(w, bodies, 5, hull, 0.6, vel=(0.01, -0.02), spin=0.001, subcell=(0.0625, 0.125))
+    hold = np.zeros((height, width), dtype=bool)
+    hold[hy:hy + 4, hx + 1:hx + 9] = True
+    cargo = np.zeros_like(hold)
+    cargo[hy + 3, hx + 2:hx + 4] = True  # sand on the hold's floor: the hull's cargo
+    w.paint(cargo, abi.SAND)
+    used[cargo] = True
     water = np.zeros((height, width), dtype=bool)
     water[surface:height - 1, 1:width - 1] = True
     water &= ~used
     vel = rng.normal(0.0, 0.3, (height, width, 2)).astype(np.float32)
     w.paint(water, liquid, vel=vel)
     w.config = dict(workload="bodies_tank", grid=f"{width}x{height}", seed=seed, earth_g=earth_g_cells())
+    if stamps:
+        bodies.swept = [(np.flatnonzero(hold.ravel()), 5, False), (np.flatnonzero(seam.ravel()), 1, True)]
     return w, bodies
+
+
+def send_aside(world, bodies, frame):
+    """What bodies.wgsl leaves for the liquid's next step where a body pushed
+    particles aside: their cell's G_DEST says DEST_ASIDE and the cell they
+    go to.  Cells of the water under the hull are sent into its hold (which
+    syncParticles refuses: another body's cup) and beside it (which it
+    takes)."""
+    if not bodies.swept:
+        return
+    cc = world.counters_cells()
+    hold = bodies.swept[0][0]
+    rows = hold // world.W
+    below = (rows.max() + 2) * world.W + (hold % world.W)
+    for k, src in enumerate(below[:4]):
+        dst = hold[k] if k % 2 == 0 else src + 3 * world.W
+        cc[src, 4] = 0x80000000 | int(dst)
