@@ -172,3 +172,110 @@ def test_loaded_world_steps_on_as_the_saved_one():
     d = compare_worlds(loaded, full, region_links=True)
     assert not d, "; ".join(d)
     assert snapshot.step_flags(loaded) & abi.STEP_SHIFTED_SET
+
+
+# ---------------------------------------------------------------- free bodies' parts
+
+def _body_snapshot(w, bodies, header_bodies=True, motion=None, stamps=None):
+    """A snapshot of w with the bodies' parts (bodyMotion, bodies) as given
+    (the current layouts by default); header_bodies: whether its header says
+    the bodies were kept whole (BODIES)."""
+    w.snapshot_rest = {"bodyMotion": (bodies.motion if motion is None else motion).view(np.uint8),
+                       "bodies": (bodies.stamps if stamps is None else stamps).view(np.uint8)}
+    data = snapshot.save(w, state={"frameNo": 2})
+    header, parts = snapshot.read(data)
+    if not header_bodies:
+        del header["bodies"]
+    return header, parts
+
+
+def _oracle(world, bodies):
+    from oracle.oracle import Oracle
+    return Oracle(world, W.body_element_table(), bodies)
+
+
+def test_bodies_round_trip_and_step_on_as_saved():
+    """A world with free bodies saved after two steps and loaded again holds
+    the same buffers and body table, and steps on (the oracle, coupled) as
+    the world it was saved from."""
+    w, bodies = W.bodies_world()
+    o = _oracle(w, bodies)
+    flags = abi.STEP_TOLERANCE | abi.STEP_F64_DOTS | abi.STEP_SHIFTED_SET
+    for s in (1, 2):
+        bodies.stamp_step(s - 1)
+        o.step(params(w, s), max_cycles=64, flags=flags, tolerance=1e-6)
+    snapshot.keep_bodies(w, bodies)
+    header, parts = _body_snapshot(w, bodies)
+    assert header["bodies"] == snapshot.BODIES
+    got = snapshot.world_from(header, parts, elems=W.body_element_table())
+    got_b = snapshot.bodies_from(got)
+    assert got_b is not None
+    assert np.array_equal(got_b.motion, bodies.motion) and np.array_equal(got_b.stamps, bodies.stamps)
+    assert not compare_worlds(got, w, grid=("cells", "counters", "field", "blocks"))  # cg is no part
+    got_b.swept = bodies.swept
+    o2 = _oracle(got, got_b)
+    bodies.stamp_step(2)
+    got_b.stamp_step(2)
+    o.step(params(w, 3), max_cycles=64, flags=flags, tolerance=1e-6)
+    o2.step(params(got, 3), max_cycles=64, flags=flags, tolerance=1e-6)
+    assert not compare_worlds(got, w)
+    assert np.array_equal(got_b.motion, bodies.motion) and np.array_equal(got_b.pushes, bodies.pushes)
+
+
+def test_narrow_body_tables_are_widened():
+    """Body slots saved OLD_TABLE_WORDS wide are widened with zeros, the
+    contacts and the liquid's words moved along (migrateTable)."""
+    w, bodies = W.bodies_world()
+    nb, tw, ow = abi.MAX_BODIES, abi.BODY_TABLE_WORDS, snapshot.OLD_TABLE_WORDS
+    bodies.motion[nb:nb * (1 + tw)].reshape(nb, tw)[:, ow:] = 0  # what an old table could not hold
+    bodies.motion[nb * (1 + tw):] = np.arange(bodies.motion.size - nb * (1 + tw), dtype=np.uint32)
+    old = np.concatenate([bodies.motion[:nb], bodies.motion[nb:nb * (1 + tw)].reshape(nb, tw)[:, :ow].ravel(),
+                          bodies.motion[nb * (1 + tw):]])
+    header, parts = _body_snapshot(w, bodies, motion=old)
+    got = snapshot.bodies_from(snapshot.world_from(header, parts, elems=W.body_element_table()))
+    assert np.array_equal(got.motion, bodies.motion)
+
+
+def test_swept_words_at_the_start_of_the_table_are_moved():
+    """Two words a cell saved at the start of bodyMotion, from before the
+    stamps moved to the end of the bodies buffer: dropped there, none at the
+    end (migrateSwept)."""
+    w, bodies = W.bodies_world()
+    cell_words = 2 * w.C
+    bodies.stamps[-cell_words:] = 0
+    old_motion = np.concatenate([np.full(cell_words, 0xABCDEF, dtype=np.uint32), bodies.motion])
+    header, parts = _body_snapshot(w, bodies, motion=old_motion, stamps=bodies.stamps[:-cell_words])
+    got = snapshot.bodies_from(snapshot.world_from(header, parts, elems=W.body_element_table()))
+    assert np.array_equal(got.motion, bodies.motion) and np.array_equal(got.stamps, bodies.stamps)
+
+
+def test_bodies_not_kept_whole_let_go_of_cells_they_did_not_stamp():
+    """A snapshot from before its bodies were kept whole: live bodies are
+    looked at whole (PARTS), and loose cells their body did not claim in
+    its last step are let go, FREE_BODY in their slot (migrateBodies); the
+    liquid step then takes them as no body's."""
+    w, bodies = W.bodies_world()
+    nb, tw = abi.MAX_BODIES, abi.BODY_TABLE_WORDS
+    frame = 5
+    bodies.words(0)[abi.BW["FRAME"]] = frame
+    tiles = -(-w.W // abi.BODY_TILE) * -(-w.H // abi.BODY_TILE)
+    claims_at = 4 * tiles + abi.BODY_STAT_WORDS + abi.BODY_COUNTERS + nb + w.C
+    cv = w.cell_view().reshape(w.C, 4)
+    slot = (cv[:, 3] & 0xFFFF).astype(np.uint16).view(np.float16)
+    loose = ((cv[:, 0] >> 28) & abi.FL_LOOSE) != 0
+    mine = np.flatnonzero(loose & (slot == 0))
+    bodies.stamps[claims_at + mine] = ((frame & 0xFFFFF) << 12) | ((2047 - 0) << 1)
+    header, parts = _body_snapshot(w, bodies, header_bodies=False)
+    got = snapshot.world_from(header, parts, elems=W.body_element_table())
+    gslot = (got.cell_view().reshape(w.C, 4)[:, 3] & 0xFFFF).astype(np.uint16).view(np.float16)
+    assert np.all(gslot[mine] == 0)
+    others = np.flatnonzero(loose & (slot != 0))
+    assert others.size and np.all(gslot[others] == np.float16(snapshot.FREE_BODY))
+    gb = snapshot.bodies_from(got)
+    flags = gb.motion[nb:nb * (1 + tw)].reshape(nb, tw)[:, abi.BW["FLAGS"]]
+    live = (bodies.motion[nb:nb * (1 + tw)].reshape(nb, tw)[:, abi.BW["FLAGS"]] & abi.BF_ALIVE) != 0
+    assert np.all((flags[live] & 8) != 0) and not np.any(flags[~live] & 8)
+    # kept whole: nothing let go
+    header, parts = _body_snapshot(w, bodies)
+    kept = snapshot.world_from(header, parts, elems=W.body_element_table())
+    assert np.array_equal(kept.cells, w.cells)

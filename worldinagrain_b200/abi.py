@@ -31,7 +31,7 @@ BODY_LIQUID_WORDS = 4
 BODY_PUSH_WORDS = 36
 BODY_LIQUID_BASE = MAX_BODIES * (1 + BODY_TABLE_WORDS) + BODY_CONTACTS * BODY_CONTACT_WORDS
 BODY_MOTION_WORDS = BODY_LIQUID_BASE + MAX_BODIES * BODY_LIQUID_WORDS
-BW = dict(POS=0, VEL=3, SPIN=5, MASS=6, INERTIA=7, CELLS=13, FLAGS=18, SUBCELL=25, CARGO=105, CARGO_INERTIA=106,
+BW = dict(POS=0, VEL=3, SPIN=5, MASS=6, INERTIA=7, CELLS=13, FLAGS=18, FRAME=19, SUBCELL=25, CARGO=105, CARGO_INERTIA=106,
           MOBILITY=108, MOBILITY_AT=114)
 BF_ALIVE, BF_NEW, BF_HELD, BF_WET = 1, 2, 32, 64
 RIGID_FIX = 16777216.0

@@ -36,7 +36,13 @@ restoreSnapshot (js/snapshot.js:510-548) for these parts:
   migrateField, :448-470);
 - any other liquid part of another size is refused, with nothing changed.
 
-A snapshot's other parts (air, heat, bodies, ...) are outside the liquid
+The free bodies' parts (bodyMotion, the body table; bodies, the bodies'
+buffer with its swept stamps) are migrated as restoreSnapshot migrates
+them (migrateSwept, migrateTable, migrateBodies, js/snapshot.js:411-507:
+the last one lets go the loose cells of a snapshot from before its bodies
+were kept whole, which the liquid step reads), kept, and handed to a host
+that binds them (bodies_from); keep_bodies puts the stepped table back for
+`save`. A snapshot's other parts (air, heat, ...) are outside the liquid
 step: they are kept, untouched, and written back.
 """
 import gzip
@@ -181,6 +187,118 @@ def migrate_field(world, parts):
     return dict(parts, field=grown)
 
 
+# The bodies' parts (js/snapshot.js:411-507): header.bodies, whether the
+# snapshot's bodies were kept whole; the width of a body's slot before the
+# contacts' mobility was added; a loose cell's slot once its body let it go.
+BODIES = 1
+OLD_TABLE_WORDS = 108
+FREE_BODY = 2047.0
+
+
+def _body_sizes(world):
+    """(bytes of bodyMotion, of the bodies buffer, of a cell's two swept
+    words over the world, of the table's growth past OLD_TABLE_WORDS)."""
+    stamps_words, _ = abi.body_stamps_layout(world.W, world.H)
+    return (4 * abi.BODY_MOTION_WORDS, 4 * stamps_words, 2 * 4 * world.C,
+            4 * abi.MAX_BODIES * (abi.BODY_TABLE_WORDS - OLD_TABLE_WORDS))
+
+
+def migrate_swept(world, parts):
+    """A snapshot from before the swept stamps moved to the end of the
+    bodies buffer (two words a cell at the start of bodyMotion then): those
+    dropped from bodyMotion, and none at the end of bodies, so no cell is
+    taken as a cup of last step's (migrateSwept, js/snapshot.js:411-426)."""
+    motion_bytes, bodies_bytes, cell_bytes, growth = _body_sizes(world)
+    bodies, motion = parts.get("bodies"), parts.get("bodyMotion")
+    if (bodies is None or motion is None or bodies.nbytes != bodies_bytes - cell_bytes
+            or motion.nbytes not in (motion_bytes + cell_bytes, motion_bytes - growth + cell_bytes)):
+        return parts
+    grown = np.zeros(bodies_bytes, dtype=np.uint8)
+    grown[:bodies.nbytes] = bodies
+    return dict(parts, bodies=grown, bodyMotion=motion[cell_bytes:].copy())
+
+
+def migrate_table(world, parts):
+    """A snapshot whose body slots were OLD_TABLE_WORDS wide: each slot
+    widened with zeros (no contact mobility worked out: a body gives way by
+    its mass alone until the bodies' pass has run), the contacts and the
+    liquid's words after the table moved along (migrateTable,
+    js/snapshot.js:428-450)."""
+    motion_bytes, _, _, growth = _body_sizes(world)
+    saved = parts.get("bodyMotion")
+    if saved is None or saved.nbytes != motion_bytes - growth:
+        return parts
+    nb, old_w, new_w = abi.MAX_BODIES, OLD_TABLE_WORDS, abi.BODY_TABLE_WORDS
+    old = saved.view(np.uint32)
+    grown = np.zeros(abi.BODY_MOTION_WORDS, dtype=np.uint32)
+    grown[:nb] = old[:nb]
+    grown[nb:nb * (1 + new_w)].reshape(nb, new_w)[:, :old_w] = old[nb:nb * (1 + old_w)].reshape(nb, old_w)
+    grown[nb * (1 + new_w):] = old[nb * (1 + old_w):]
+    return dict(parts, bodyMotion=grown.view(np.uint8))
+
+
+def migrate_bodies(world, header, parts, cur, elems):
+    """A snapshot from before its bodies were kept whole (header.bodies under
+    BODIES): every live body looked at whole in its first step (BF_PARTS),
+    and each loose solid cell its body did not stamp in its last step (its
+    claim word is not the body's key) let go as a broken body's are, its
+    slot FREE_BODY (migrateBodies, js/snapshot.js:471-507).  The liquid step
+    reads the slot: a cell let go is no body's."""
+    motion_bytes, bodies_bytes, _, _ = _body_sizes(world)
+    name = f"cells{cur}"
+    saved, bodies, motion = parts.get(name), parts.get("bodies"), parts.get("bodyMotion")
+    if (int(header.get("bodies", 0)) >= BODIES or saved is None or bodies is None or motion is None
+            or bodies.nbytes != bodies_bytes or motion.nbytes != motion_bytes or saved.nbytes < 16 * world.C):
+        return parts
+    nb, tw = abi.MAX_BODIES, abi.BODY_TABLE_WORDS
+    table = motion.view(np.uint32).copy()
+    flags = table[nb:nb * (1 + tw)].reshape(nb, tw)[:, abi.BW["FLAGS"]]
+    alive = (flags & abi.BF_ALIVE) != 0
+    flags[alive] |= 8  # BODY_FLAG.PARTS (js/shared.js:327)
+    table[nb:nb * (1 + tw)].reshape(nb, tw)[:, abi.BW["FLAGS"]] = flags
+    tiles = -(-world.W // abi.BODY_TILE) * -(-world.H // abi.BODY_TILE)
+    body_header = 4 * tiles + abi.BODY_STAT_WORDS + abi.BODY_COUNTERS + nb
+    claims = bodies.view(np.uint32)[body_header + world.C:body_header + 2 * world.C]
+    cells = saved.view(np.uint32).copy()
+    cell = cells[:4 * world.C].reshape(world.C, 4)
+    kind = np.array([elems[t].kind if t < len(elems) else elems[0].kind for t in range(256)])
+    slot = (cell[:, 3] & 0xFFFF).astype(np.uint16).view(np.float16).astype(np.float64)
+    loose = (((cell[:, 0] >> FLAG_SHIFT) & abi.FL_LOOSE) != 0) & (kind[cell[:, 0] & 0xFF] == abi.KIND_SOLID) & (slot < nb)
+    for i in np.flatnonzero(loose):
+        # (a slot that is no whole number of the table, which only a damaged
+        # snapshot holds, is let go: its body words are none)
+        b = int(slot[i])
+        whole = slot[i] >= 0 and slot[i] == b
+        body = table[nb + b * tw:nb + (b + 1) * tw] if whole else np.zeros(tw, dtype=np.uint32)
+        key = (((int(body[abi.BW["FRAME"]]) & 0xFFFFF) << 12) | (int(FREE_BODY - slot[i]) << 1)) & 0xFFFFFFFF
+        if not (body[abi.BW["FLAGS"]] & abi.BF_ALIVE) or int(claims[i]) != key:
+            cell[i, 3] = (int(cell[i, 3]) & 0xFFFF0000) | int(np.float16(FREE_BODY).view(np.uint16))
+    return dict(parts, **{name: cells.view(np.uint8), "bodyMotion": table.view(np.uint8)})
+
+
+def bodies_from(world):
+    """The free bodies of a world restored from a snapshot, as a world.Bodies
+    to bind (LiquidStep.bind_bodies): its body table and bodies' buffer as
+    saved (after the migrations above), the push sums empty (a step's
+    scratch, not a part).  None when the snapshot holds no body parts of
+    this world's layout."""
+    rest = getattr(world, "snapshot_rest", {})
+    motion_bytes, bodies_bytes, _, _ = _body_sizes(world)
+    motion, stamps = rest.get("bodyMotion"), rest.get("bodies")
+    if motion is None or stamps is None or motion.nbytes != motion_bytes or stamps.nbytes != bodies_bytes:
+        return None
+    b = W.Bodies(world.W, world.H)
+    b.motion[:] = motion.view(np.uint32)
+    b.stamps[:] = stamps.view(np.uint32)
+    return b
+
+
+def keep_bodies(world, bodies):
+    """The stepped body table (what the liquid did to each body in its
+    liquid words) into the parts `save` writes back."""
+    world.snapshot_rest = dict(getattr(world, "snapshot_rest", {}), bodyMotion=bodies.motion.view(np.uint8).copy())
+
+
 def _size(header):
     """The header's world size (width, height); ValueError when it has none."""
     try:
@@ -214,7 +332,8 @@ def restore(world, header, parts, elems=None, element_ids=None):
     cur = int(state.get("cur", 0))
     elems = W.element_table() if elems is None else elems
     parts, migrated = migrate_liquid(world, parts, elems)
-    parts = migrate_field(world, migrate_blocks(world, parts))
+    parts = migrate_table(world, migrate_swept(world, migrate_blocks(world, parts)))
+    parts = migrate_bodies(world, header, migrate_field(world, parts), cur, elems)
     names = dict(PART_OF, cells=f"cells{cur}")
     misfits = []
     for buf, part in names.items():
@@ -278,7 +397,7 @@ def save(world, state=None, elements=None):
     if els is None:
         els = list(range(len(W.element_table())))
     header = dict(getattr(world, "snapshot_header", {}))
-    header.update(format=FORMAT, width=world.W, height=world.H, elements=els, state=st)
+    header.update(format=FORMAT, width=world.W, height=world.H, elements=els, state=st, bodies=BODIES)
     return write(header, parts)
 
 
