@@ -110,15 +110,24 @@ class Oracle:
         x = np.zeros(self.world.C, dtype=np.float64)
         rel = C.c_double(0.0)
         f = lib().wo_solve_f64_mg if multigrid else lib().wo_solve_f64
-        it = f(C.byref(d), C.byref(P), self.elems, len(self.elems), C.byref(b), rel_tol, max_iter,
-               x.ctypes.data, C.byref(rel))
+        self._bind()
+        try:
+            it = f(C.byref(d), C.byref(P), self.elems, len(self.elems), C.byref(b), rel_tol, max_iter,
+                   x.ctypes.data, C.byref(rel))
+        finally:
+            lib().wo_bind_bodies(None, None, None)
         return x, it, rel.value
 
     def true_residual(self, P, x):
         d = self.world.desc()
         b = _buffers(self.world)
         x = np.ascontiguousarray(x, dtype=np.float32)
-        return lib().wo_true_residual(C.byref(d), C.byref(P), self.elems, len(self.elems), C.byref(b), x.ctypes.data)
+        self._bind()
+        try:
+            return lib().wo_true_residual(C.byref(d), C.byref(P), self.elems, len(self.elems), C.byref(b),
+                                          x.ctypes.data)
+        finally:
+            lib().wo_bind_bodies(None, None, None)
 
 
 def sincos(a):

@@ -30,6 +30,7 @@
 #include "../include/wig_fluid.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -2718,14 +2719,42 @@ void run_pass(Ctx& X, int pass) {
 // The pressure operator of the FP64 solves: per fluid cell (in cell order)
 // its four neighbours' rows and betas (fineBeta, the liquid neighbours
 // only), its diagonal (the betas of every non-solid side, PIN at the root
-// of a closed region) and the right-hand side -b.
+// of a closed region) and the right-hand side -b.  With free bodies bound,
+// the coupling J^T G J assembled on its own (fluid.wgsl:1374-1403, :2779-2795):
+// per face from a fluid cell to a body's cell its J row (the normal and its
+// arm about the body's centre, bodyFaceJ), and per body G, how it gives way
+// (giveWay: the contact mobility worked out last step, else 1/m, 1/m, 1/I),
+// so that (A p)_k = (L p)_k + sum over k's body faces of J . G (sum of J p).
 struct F64System {
     struct Row { int32_t nb[4]; double beta[4]; double diag; };
+    struct Couple { size_t k; uint32_t b; double j[3]; };
     std::vector<uint32_t> cellsOf;
     std::vector<Row> rows;
     std::vector<double> rhs;
+    std::vector<Couple> couples;
+    std::vector<std::array<double, 9>> give;  // per body, G row-major (bodies not coupled: unused)
+    void couple(Ctx& X, size_t k, I2 c) {
+        if (!X.motion) return;
+        for (int dd = 0; dd < 4; dd++) {
+            I2 q = Ctx::beside(c, dd);
+            uint32_t b = rigidAt(X, q);
+            if (b == NONE) continue;
+            V3 j = bodyFaceJ(X, c, q, b);
+            couples.push_back(Couple{k, b, {(double)j.x, (double)j.y, (double)j.z}});
+            std::array<double, 9>& g = give[b];
+            if (bodyWord(X, b, WIG_BW_MOBILITY_AT) != X.P->frame - 1u) {
+                g = {1.0 / (double)rigidMass(X, b), 0, 0, 0, 1.0 / (double)rigidMass(X, b), 0, 0, 0,
+                     1.0 / (double)rigidInertia(X, b)};
+            } else {
+                double m[6];
+                for (uint32_t t = 0; t < 6; t++) m[t] = (double)bodyF(X, b, WIG_BW_MOBILITY + t);
+                g = {m[0], m[1], m[2], m[1], m[3], m[4], m[2], m[4], m[5]};
+            }
+        }
+    }
     size_t n() const { return cellsOf.size(); }
     void build(Ctx& X) {
+        give.assign(X.motion ? MAX_BODIES : 0, std::array<double, 9>{});
         std::vector<int32_t> idx(X.C, -1);
         for (uint32_t i = 0; i < X.C; i++)
             if (X.fv(2u * i)[2] > 0.0f) { idx[i] = (int32_t)cellsOf.size(); cellsOf.push_back(i); }
@@ -2750,6 +2779,7 @@ struct F64System {
             }
             if (pinnedAt(X, i)) r.diag += (double)PIN;
             rhs[k] = -(double)X.fv(2u * i)[1];
+            couple(X, k, c);
         }
     }
     void apply(const std::vector<double>& p, std::vector<double>& q) const {
@@ -2758,6 +2788,16 @@ struct F64System {
             for (int dd = 0; dd < 4; dd++)
                 if (rows[k].nb[dd] >= 0) s -= rows[k].beta[dd] * p[rows[k].nb[dd]];
             q[k] = s;
+        }
+        if (couples.empty()) return;
+        std::vector<std::array<double, 3>> jp(give.size(), std::array<double, 3>{0, 0, 0});
+        for (const Couple& e : couples)
+            for (int t = 0; t < 3; t++) jp[e.b][t] += e.j[t] * p[e.k];
+        for (const Couple& e : couples) {
+            const std::array<double, 9>& g = give[e.b];
+            double v = 0.0;
+            for (int t = 0; t < 3; t++) v += e.j[t] * (g[3 * t] * jp[e.b][0] + g[3 * t + 1] * jp[e.b][1] + g[3 * t + 2] * jp[e.b][2]);
+            q[e.k] += v;
         }
     }
     void scatter(const std::vector<double>& x, uint32_t C, double* out) const {

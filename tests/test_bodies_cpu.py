@@ -148,3 +148,47 @@ def test_cup_and_seam_only_with_the_stamps():
     drift_z = w.field_cells()[:, 1, 2]
     assert int(np.sum(drift_z == np.float32(-2.0))) == 35
     assert int(np.sum(drift_z == np.float32(-6.0))) == 18
+
+
+@pytest.mark.parametrize("liquid", ["water", "mud"])
+def test_coupled_fp32_solve_reaches_the_fp64_solution_of_the_assembled_system(liquid):
+    """The FP32 step's pressure (the coupling applied as the reference does,
+    through the push sums and couplingAt) against an FP64 CG of the same
+    system assembled on its own, L + J^T G J (the oracle's F64System): within
+    the 1e-6 solve's error; and far from the FP64 solution of L alone, the
+    bodies then walls that move but do not give way."""
+    mud = liquid == "mud"
+    w, bodies = W.bodies_world(liquid=W.MUD if mud else abi.WATER)
+    flags = FLAGS | (abi.STEP_VISCOUS if mud else 0)
+    o = _oracle(w, bodies)
+    for s in (1, 2):
+        bodies.stamp_step(s - 1)
+        W.send_aside(w, bodies, s)
+        o.step(params(w, s), max_cycles=64, flags=flags, tolerance=1e-6)
+    bodies.stamp_step(2)
+    P = params(w, 3)
+    probe, probe_b = w.copy(), bodies.copy()
+    po = _oracle(probe, probe_b)
+    pre = ["SYNC", "SYNC_PARTICLES", "SYNC_SEED", "COMPACT", "RETIRE", "CLEAR", "GATHER", "SEAL_JOIN",
+           "SEAL_ANCHOR", "CLASSIFY", "BODY_START", "BODY_LOADS", "SET_FACES", "UNPRESS"]
+    if mud:  # the sweeps' passes, then the drag, as a viscous step runs them
+        pre += ["VISCOSITY_RED", "VISCOSITY_BLACK"] * 8 + ["UNPRESS", "BODY_DRAG", "BODY_FACES"]
+        pre.remove("UNPRESS")
+    pre += ["DIVERGENCE", "CG_START", "CG_JOIN", "CG_ANCHOR"]
+    for name in pre:
+        po.pass_(P, name)
+    x64, _, rel = po.solve_f64(P, rel_tol=1e-12)
+    assert rel <= 1e-12
+    from oracle.oracle import Oracle
+    xl, _, rel_l = Oracle(probe.copy(), W.body_element_table(), None).solve_f64(P, rel_tol=1e-12)
+    assert rel_l <= 1e-12
+    st = o.step(P, max_cycles=64, flags=flags | abi.STEP_SHIFTED_SET, tolerance=1e-6)
+    assert st.rel_residual <= 1e-6
+    fluid = probe.field_cells()[:, 0, 2] > 0
+    p = w.field_cells()[:, 0, 0][fluid].astype(np.float64)
+    err = np.linalg.norm(p - x64[fluid]) / np.linalg.norm(x64[fluid])
+    apart = np.linalg.norm(xl[fluid] - x64[fluid]) / np.linalg.norm(x64[fluid])
+    print(f"\nbodies tank, {liquid}: pressure {err:.3e} relative L2 against the FP64 coupled solve "
+          f"({apart:.3e} between the coupled and the uncoupled solves)")
+    assert err < 1e-4, err
+    assert apart > 100 * err, (apart, err)
