@@ -192,3 +192,55 @@ def test_coupled_fp32_solve_reaches_the_fp64_solution_of_the_assembled_system(li
           f"({apart:.3e} between the coupled and the uncoupled solves)")
     assert err < 1e-4, err
     assert apart > 100 * err, (apart, err)
+
+
+def _still_tank(density, size=64, side=8):
+    """A tank of still water, a quarter of it air, and a square body of the
+    given density (water cells a cell) at rest at mid-depth."""
+    w = W.World(size, size)
+    bodies = W.Bodies(size, size)
+    wall = np.zeros((size, size), dtype=bool)
+    wall[-1, :] = True
+    wall[:, 0] = wall[:, -1] = True
+    w.paint(wall, abi.WALL)
+    surface = size // 4
+    body = np.zeros_like(wall)
+    y0, x0 = (surface + size) // 2 - side // 2, size // 2 - side // 2
+    body[y0:y0 + side, x0:x0 + side] = True
+    W.stamp_body(w, bodies, 0, body, density)
+    water = np.zeros_like(wall)
+    water[surface:size - 1, 1:size - 1] = True
+    w.paint(water & ~(wall | body), abi.WATER)
+    w.config = dict(earth_g=W.earth_g_cells())
+    return w, bodies
+
+
+# The added mass of a square prism moving square to a face in still liquid,
+# by potential flow: C_A = 1.51 on the area pi (b/2)^2, i.e. 1.19 rho b^2
+# (the tabulated potential-flow coefficient of a square section, as in
+# DNV-RP-C205's appendix A and Newman, Marine Hydrodynamics, 1977).
+SQUARE_ADDED_MASS = 1.51 * np.pi / 4.0
+
+
+@pytest.mark.parametrize("density", [1.0, 0.5, 2.0])
+def test_a_body_released_in_still_water_moves_as_its_added_mass_has_it(density):
+    """A physical anchor for the coupling: a square body at rest in still
+    water, its first step.  Held by the liquid against the pull and free to
+    give way, it takes the acceleration a = (rho_w - rho_b) V g / (m + m_A),
+    m_A the liquid it sets moving; what the liquid does to it (its liquid
+    words) is a - g along the pull: -g exactly at the liquid's own density
+    (Archimedes: it neither rises nor sinks), and within 2% of the
+    potential-flow added mass at half and twice it.  Nothing pushes it
+    sideways or turns it."""
+    w, bodies = _still_tank(density)
+    o = _oracle(w, bodies)
+    st = o.step(params(w, 1), max_cycles=64, flags=FLAGS, tolerance=1e-6)
+    assert st.rel_residual <= 1e-6
+    g = w.config["earth_g"]
+    dv = bodies.liquid(0)[:3].view(np.int32).astype(np.float64) / abi.RIGID_FIX
+    expected = -1.0 - (1.0 - density) / (density + SQUARE_ADDED_MASS)
+    print(f"\ndensity {density}: liquid's dv_y {dv[1] / g:+.4f} g, potential flow {expected:+.4f} g")
+    assert abs(dv[1] / g - expected) <= 0.02 * abs(expected), (dv[1] / g, expected)
+    if density == 1.0:
+        assert abs(dv[1] / g + 1.0) < 1e-3
+    assert abs(dv[0]) < 1e-3 * g and abs(dv[2]) < 1e-3 * g
