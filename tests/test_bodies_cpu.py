@@ -244,3 +244,36 @@ def test_a_body_released_in_still_water_moves_as_its_added_mass_has_it(density):
     if density == 1.0:
         assert abs(dv[1] / g + 1.0) < 1e-3
     assert abs(dv[0]) < 1e-3 * g and abs(dv[2]) < 1e-3 * g
+
+
+@pytest.mark.parametrize("density", [7.8, 2.0])
+def test_a_held_block_on_the_floor_is_lifted_as_archimedes_has_it(density):
+    """A held block resting on the floor of a still tank (heldPush, with
+    seepAt finding the liquid's pressure beside it for the faces it rests
+    on, fluid.wgsl:2977-3031): the liquid's push on it is Archimedes' lift,
+    -g rho_w / rho_b along the pull, each step, within 0.5%, and turns it
+    not at all."""
+    size, side = 64, 8
+    w = W.World(size, size)
+    bodies = W.Bodies(size, size)
+    wall = np.zeros((size, size), dtype=bool)
+    wall[-1, :] = True
+    wall[:, 0] = wall[:, -1] = True
+    w.paint(wall, abi.WALL)
+    block = np.zeros_like(wall)
+    block[size - 1 - side:size - 1, size // 2 - side // 2:size // 2 + side // 2] = True
+    W.stamp_body(w, bodies, 0, block, density, flags=abi.BF_ALIVE | abi.BF_HELD | abi.BF_WET)
+    water = np.zeros_like(wall)
+    water[size // 4:size - 1, 1:size - 1] = True
+    w.paint(water & ~(wall | block), abi.WATER)
+    w.config = dict(earth_g=W.earth_g_cells())
+    o = _oracle(w, bodies)
+    g = w.config["earth_g"]
+    before = np.zeros(3)
+    for s in range(1, 4):
+        o.step(params(w, s), max_cycles=64, flags=FLAGS, tolerance=1e-6)
+        now = bodies.liquid(0)[:3].view(np.int32).astype(np.float64) / abi.RIGID_FIX
+        dv, before = now - before, now
+        assert abs(dv[1] / g + 1.0 / density) <= 0.005 / density, (s, dv[1] / g)
+        assert abs(dv[2]) < 1e-3 * g
+    assert bodies.liquid(0)[3] & 0x80000000  # by the liquid: wet
