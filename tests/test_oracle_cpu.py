@@ -177,3 +177,57 @@ def test_oracle_matches_golden_fixtures(case):
             got = world_digests(world)
             got["cycles"] = int(st.cycles)
             assert got == want[str(s)], f"{case} step {s}"
+
+
+def test_free_fall_gains_g_each_step():
+    """A blob of water in open air falls freely: each step's pull on its
+    faces (setFace, fluid.wgsl:1966-1973) leaves no divergence for the
+    pressure to take back, so its particles' mean velocity is s g after s
+    steps, within 0.2%, and nothing pushes them sideways."""
+    world = W.World(48, 128)
+    blob = np.zeros((128, 48), dtype=bool)
+    blob[8:20, 16:32] = True
+    world.paint(blob, abi.WATER)
+    world.config = {"earth_g": W.earth_g_cells()}
+    g = world.config["earth_g"]
+    o = Oracle(world, W.element_table())
+    for s in range(1, 41):
+        o.step(params(world, s), max_cycles=64, flags=abi.STEP_TOLERANCE | abi.STEP_F64_DOTS, tolerance=1e-6)
+        m, _, _ = world.particles()
+        assert len(m) == 12 * 16 * 4
+        assert abs(m[:, 3].mean() / (s * g) - 1.0) < 2e-3, s
+        assert abs(m[:, 2].mean()) < 1e-2 * g
+
+
+def test_slot_in_a_tank_floor_discharges_as_kirchhoff_has_it():
+    """Torricelli through a slot 4 cells wide in the floor of a tank 80 cells
+    deep: the discharge a step, over the slot's width, is C sqrt(2 g h),
+    with C the contraction of a jet from a slot in a wide wall, pi / (pi + 2)
+    = 0.611 (Kirchhoff's free-streamline solution), within 12% (measured
+    0.58)."""
+    H, Wd, floor = 120, 64, 100
+    world = W.World(Wd, H)
+    wall = np.zeros((H, Wd), dtype=bool)
+    wall[-1, :] = True
+    wall[:, 0] = wall[:, -1] = True
+    wall[floor, 1:Wd - 1] = True
+    wall[floor, Wd // 2 - 2:Wd // 2 + 2] = False
+    world.paint(wall, abi.WALL)
+    water = np.zeros((H, Wd), dtype=bool)
+    water[20:floor, 1:Wd - 1] = True
+    world.paint(water, abi.WATER)
+    world.config = {"earth_g": W.earth_g_cells()}
+    g = world.config["earth_g"]
+    o = Oracle(world, W.element_table())
+    held = {}
+    for s in range(1, 141):
+        o.step(params(world, s), max_cycles=64, flags=abi.STEP_TOLERANCE | abi.STEP_F64_DOTS, tolerance=1e-6)
+        if s in (60, 140):
+            m, _, _ = world.particles()
+            inside = m[m[:, 1] < floor]
+            held[s] = (len(inside), floor - np.percentile(inside[:, 1], 0.5))
+    q = (held[60][0] - held[140][0]) / 80.0 / 4.0  # cells of liquid a step, 4 particles a cell
+    h = 0.5 * (held[60][1] + held[140][1])
+    c = q / 4.0 / math.sqrt(2.0 * g * h)
+    kirchhoff = math.pi / (math.pi + 2.0)
+    assert abs(c - kirchhoff) <= 0.12 * kirchhoff, c
