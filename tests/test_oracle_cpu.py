@@ -231,3 +231,54 @@ def test_slot_in_a_tank_floor_discharges_as_kirchhoff_has_it():
     c = q / 4.0 / math.sqrt(2.0 * g * h)
     kirchhoff = math.pi / (math.pi + 2.0)
     assert abs(c - kirchhoff) <= 0.12 * kirchhoff, c
+
+
+def _poiseuille_startup(t, width, nu):
+    """The centre speed of plane Poiseuille flow started from rest, over its
+    steady g W^2 / (8 nu): 1 - (32 / pi^3) sum over odd n of (-1)^((n-1)/2)
+    exp(-n^2 pi^2 nu t / W^2) / n^3 (the series solution of the diffusion of
+    momentum from no-slip walls)."""
+    s = 0.0
+    for n in range(1, 200, 2):
+        s += (-1) ** ((n - 1) // 2) * math.exp(-(n * math.pi) ** 2 * nu * t / width ** 2) / n ** 3
+    return 1.0 - 32.0 / math.pi ** 3 * s
+
+
+def test_viscous_liquid_drains_down_a_channel_as_poiseuille_flow():
+    """A viscous liquid (this table's mud, nu = 0.8 cells^2 a step) falling
+    down a vertical channel 20 cells wide and out of its open end: the
+    viscosity's sweeps with no slip at the walls (viscousFace,
+    fluid.wgsl:3347-3403) give the parabola u = g x (W - x) / (2 nu) across
+    it, within 3% in shape, and its centre speed follows the start-up of
+    Poiseuille flow from rest within 3% after 120 and 200 steps."""
+    Wd, H, x0, x1, bottom = 64, 200, 23, 43, 150
+    world = W.World(Wd, H)
+    wall = np.zeros((H, Wd), dtype=bool)
+    wall[-1, :] = True
+    wall[:, 0] = wall[:, -1] = True
+    wall[:bottom, x0 - 1] = True
+    wall[:bottom, x1] = True
+    world.paint(wall, abi.WALL)
+    mud = np.zeros((H, Wd), dtype=bool)
+    mud[10:140, x0:x1] = True
+    world.paint(mud, W.MUD)
+    world.config = {"earth_g": W.earth_g_cells()}
+    g = world.config["earth_g"]
+    elems = W.element_table()
+    nu = elems[W.MUD].viscosity
+    o = Oracle(world, elems)
+    xc = np.arange(x0, x1) + 0.5
+    steady = g / (2.0 * nu) * (xc - x0) * (x1 - xc)
+    for s in range(1, 201):
+        o.step(params(world, s), max_cycles=64,
+               flags=abi.STEP_TOLERANCE | abi.STEP_F64_DOTS | abi.STEP_VISCOUS, tolerance=1e-6)
+        if s in (120, 200):
+            m, _, _ = world.particles()
+            mid = m[(m[:, 1] > 60) & (m[:, 1] < 100)]
+            cols = np.floor(mid[:, 0]).astype(int)
+            prof = np.array([mid[cols == c, 3].mean() for c in range(x0, x1)])
+            shape = np.linalg.norm(prof / prof.max() - steady / steady.max()) / np.linalg.norm(steady / steady.max())
+            ratio = prof.max() / steady.max()
+            expected = _poiseuille_startup(s, x1 - x0, nu)
+            assert shape < 0.03, (s, shape)
+            assert abs(ratio - expected) < 0.03 * expected, (s, ratio, expected)
