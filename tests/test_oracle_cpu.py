@@ -282,3 +282,34 @@ def test_viscous_liquid_drains_down_a_channel_as_poiseuille_flow():
             expected = _poiseuille_startup(s, x1 - x0, nu)
             assert shape < 0.03, (s, shape)
             assert abs(ratio - expected) < 0.03 * expected, (s, ratio, expected)
+
+
+def test_two_layers_at_rest_hold_each_its_own_hydrostatic_gradient():
+    """Water resting on a denser liquid (this table's mud, 1.6 times water)
+    stays at rest, and the pressure grows by rho g a cell of depth in each
+    layer, water's 1.0 and mud's 1.6, within 1%."""
+    world = W.World(32, 48)
+    wall = np.zeros((48, 32), dtype=bool)
+    wall[-1, :] = True
+    wall[:, 0] = wall[:, -1] = True
+    world.paint(wall, abi.WALL)
+    water = np.zeros((48, 32), dtype=bool)
+    water[12:28, 1:31] = True
+    world.paint(water, abi.WATER)
+    mud = np.zeros((48, 32), dtype=bool)
+    mud[28:47, 1:31] = True
+    world.paint(mud, W.MUD)
+    world.config = {"earth_g": W.earth_g_cells()}
+    g = world.config["earth_g"]
+    elems = W.element_table()
+    o = Oracle(world, elems)
+    for s in range(1, 81):
+        o.step(params(world, s), max_cycles=64,
+               flags=abi.STEP_TOLERANCE | abi.STEP_F64_DOTS | abi.STEP_VISCOUS, tolerance=1e-6)
+    col = world.pressure()[:, 15]
+    for rows, elem in ((slice(15, 26), abi.WATER), (slice(31, 45), W.MUD)):
+        slope = np.mean(np.diff(col[rows])) / g
+        rho = elems[elem].density / 100.0
+        assert abs(slope - rho) < 0.01 * rho, (elem, slope)
+    m, _, _ = world.particles()
+    assert np.abs(m[:, 2:]).max() < 0.01 * 80 * g  # at rest: far below free fall over the run
