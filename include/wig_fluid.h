@@ -112,6 +112,7 @@ extern "C" {
 #define WIG_BW_INERTIA 7u
 #define WIG_BW_CELLS 13u         /* u32 */
 #define WIG_BW_FLAGS 18u         /* u32: WIG_BF_* */
+#define WIG_BW_FRAME 19u         /* u32: the step the body was last stamped */
 #define WIG_BW_SUBCELL 25u       /* 2 x f16: the pose's offset from the stamp, cells */
 #define WIG_BW_CARGO 105u
 #define WIG_BW_CARGO_INERTIA 106u

@@ -105,3 +105,41 @@ def test_noalloc_refuses_large_worlds_without_touching_the_device():
     one = C.c_void_p(16)
     assert f(C.byref(d), one, one, one, one, None) == -1
     assert b"at most 16384" in L.wig_fluid_last_error()
+
+
+def _header_macros():
+    """The integer #defines of include/*.h, evaluated in order (a macro may
+    name the ones before it)."""
+    vals = {}
+    for h in HEADERS:
+        text = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
+        text = text.replace("\\\n", " ")
+        for name, expr in re.findall(r"^#define\s+(WIG_[A-Z0-9_]+)\s+(.+)$", text, flags=re.M):
+            e = re.sub(r"\b(0x[0-9a-fA-F]+|\d+)u\b", r"\1", expr.strip())
+            e = re.sub(r"(\d\.\d*)f\b", r"\1", e)
+            e = re.sub(r"\b(WIG_[A-Z0-9_]+)\b", lambda m: str(vals.get(m.group(1), "None")), e)
+            try:
+                vals[name] = eval(e, {"__builtins__": {}})
+            except Exception:
+                pass
+    return vals
+
+
+def test_body_layout_constants_agree_with_the_header():
+    """The free bodies' layout constants of the Python mirror are the
+    header's (js/shared.js:294-333)."""
+    m = _header_macros()
+    assert m["WIG_MAX_BODIES"] == abi.MAX_BODIES
+    assert m["WIG_BODY_TABLE_WORDS"] == abi.BODY_TABLE_WORDS
+    assert m["WIG_BODY_PUSH_WORDS"] == abi.BODY_PUSH_WORDS
+    assert m["WIG_BODY_MOTION_WORDS"] == abi.BODY_MOTION_WORDS
+    assert m["WIG_BODY_LIQUID_BASE"] == abi.BODY_LIQUID_BASE
+    assert m["WIG_RIGID_FIX"] == abi.RIGID_FIX
+    assert m["WIG_FL_LOOSE"] == abi.FL_LOOSE and m["WIG_NO_ELEM"] == abi.NO_ELEM
+    assert (m["WIG_BF_ALIVE"], m["WIG_BF_NEW"], m["WIG_BF_HELD"], m["WIG_BF_WET"]) == (
+        abi.BF_ALIVE, abi.BF_NEW, abi.BF_HELD, abi.BF_WET)
+    for k, v in abi.BW.items():
+        assert m[f"WIG_BW_{k}"] == v, k
+    assert (m["WIG_BODY_TILE"], m["WIG_BODY_STAT_WORDS"], m["WIG_BODY_COUNTERS"], m["WIG_BODY_SUM_WORDS"]) == (
+        abi.BODY_TILE, abi.BODY_STAT_WORDS, abi.BODY_COUNTERS, abi.BODY_SUM_WORDS)
+    assert m["WIG_CLAIM_PERIOD"] == abi.CLAIM_PERIOD
