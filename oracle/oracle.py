@@ -43,6 +43,9 @@ def lib():
         L.wo_true_residual.restype = C.c_double
         L.wo_sincos.argtypes = [C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]
         L.wo_bind_bodies.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
+        L.wo_exact_parts.argtypes = [C.c_float, C.POINTER(C.c_uint32), C.POINTER(C.c_uint32)]
+        L.wo_exact_value.argtypes = [C.c_uint32, C.c_uint32]
+        L.wo_exact_value.restype = C.c_float
         _lib = L
     return _lib
 
@@ -134,3 +137,14 @@ def sincos(a):
     s, c = C.c_float(), C.c_float()
     lib().wo_sincos(C.c_float(a), C.byref(s), C.byref(c))
     return s.value, c.value
+
+
+def exact_parts(x):
+    """The oracle's exactParts of x at the push sums' scale: (low, high)."""
+    lo, hi = C.c_uint32(), C.c_uint32()
+    lib().wo_exact_parts(C.c_float(x), C.byref(lo), C.byref(hi))
+    return lo.value, hi.value
+
+
+def exact_value(lo, hi):
+    return lib().wo_exact_value(lo, hi)

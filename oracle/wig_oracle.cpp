@@ -3119,4 +3119,9 @@ double wo_true_residual(const wig_world_desc* d, const wig_params* P, const wig_
 // sin/cos of the own implementation, for the tests to compare with.
 void wo_sincos(float a, float* s, float* c) { sincos_own(a, s, c); }
 
+// exactParts and exactValue (common.wgsl:1378-1412) at EXACT_COARSE, the
+// scale of the bodies' push sums, for the tests of their two-word sums.
+void wo_exact_parts(float x, uint32_t* lo, uint32_t* hi) { exactParts(x, EXACT_COARSE, lo, hi); }
+float wo_exact_value(uint32_t lo, uint32_t hi) { return exactValue(lo, hi, EXACT_COARSE); }
+
 }  // extern "C"

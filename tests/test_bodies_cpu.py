@@ -277,3 +277,33 @@ def test_a_held_block_on_the_floor_is_lifted_as_archimedes_has_it(density):
         assert abs(dv[1] / g + 1.0 / density) <= 0.005 / density, (s, dv[1] / g)
         assert abs(dv[2]) < 1e-3 * g
     assert bodies.liquid(0)[3] & 0x80000000  # by the liquid: wet
+
+
+def test_two_word_push_sums_are_exact_and_order_free():
+    """The pushes' sums (common.wgsl:1378-1412): each value split into two
+    words of 2^-24 units, the low added with its carry into the high, as the
+    atomics add them.  In any order the words come out the same, also past
+    2^31 units (|x| >= 128, which a large body in deep water reaches), and
+    read back they are the sum of the rounded values."""
+    from oracle.oracle import exact_parts, exact_value
+    rng = np.random.default_rng(7)
+    x = np.concatenate([rng.normal(0.0, 1e-3, 200), rng.normal(0.0, 30.0, 200), rng.uniform(-3e3, 3e3, 50)])
+    x = x.astype(np.float32)
+    parts = [exact_parts(float(v)) for v in x]
+    assert any(abs(float(v)) >= 128.0 for v in x)
+    units = [int(np.round(np.float64(v) * 16777216.0)) for v in x]
+    for (lo, hi), u in zip(parts, units):  # each part pair is its value's units, two's complement
+        assert ((hi << 32) | lo) == u % (1 << 64)
+    totals = set()
+    for _ in range(5):
+        lo_sum = hi_sum = 0
+        for k in rng.permutation(len(parts)):
+            lo, hi = parts[k]
+            old = lo_sum
+            lo_sum = (old + lo) & 0xFFFFFFFF
+            hi_sum = (hi_sum + hi + (1 if lo_sum < old else 0)) & 0xFFFFFFFF
+        totals.add((lo_sum, hi_sum))
+    assert len(totals) == 1
+    lo_sum, hi_sum = totals.pop()
+    want = sum(units) / 16777216.0
+    assert abs(exact_value(lo_sum, hi_sum) - want) <= 1e-6 * max(1.0, abs(want))
